@@ -1,0 +1,156 @@
+"""CPU oracle for the per-batch operators — TEST INFRASTRUCTURE ONLY.
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
+the checker / CPU baseline; the product never imports it.
+
+``liboracle.so`` (oracle.c) holds the C restatements (stable ORDER BY,
+nested-loop join, the timed query baselines); ``expr_eval`` evaluates
+expression trees with numpy. Parity status: the reference ships no golden
+vectors or known-answer tests; the oracle is pinned against the reference's
+own GPU kernels run on the same inputs (``oracle/_ref``, built by
+``oracle/Makefile`` from the reference sources) by ``tests/test_ref_pin_gpu.py``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+SRC = os.path.join(HERE, "oracle.c")
+
+
+def build() -> str:
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+        subprocess.check_call(["gcc", "-O3", "-march=x86-64-v2", "-shared", "-fPIC", "-pthread", "-o", LIB, SRC,
+                               "-lm"])
+    return LIB
+
+
+class OrcCol(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("nulls", C.c_void_p), ("type", C.c_int), ("width", C.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB)
+        vp, u32, i32, u64 = C.c_void_p, C.c_uint32, C.c_int, C.c_uint64
+        L.orc_sort_perm.argtypes = [i32, vp, vp, i32, u32, i32, i32, vp, i32, vp, vp, i32]
+        L.orc_sort_perm.restype = i32
+        L.orc_join_pairs.argtypes = [C.POINTER(OrcCol), C.POINTER(OrcCol), vp, i32, u32, u32, vp, vp, u64]
+        L.orc_join_pairs.restype = u64
+        L.orc_sales_query.argtypes = [vp, vp, vp, vp, i32, vp, u32, i32, C.POINTER(C.c_double),
+                                      C.POINTER(C.c_int64), C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.orc_sales_query.restype = None
+        L.orc_star_query.argtypes = [vp, vp, vp, vp, u32, vp, i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+        L.orc_star_query.restype = None
+        L.orc_cross_lt.argtypes = [vp, u32, vp, u32, vp, vp, u64]
+        L.orc_cross_lt.restype = u64
+        L.orc_gather.argtypes = [vp, vp, i32, vp, u32]
+        L.orc_gather.restype = None
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+# yq_type codes (0..3 equal the reference's DataType)
+INT32, FLOAT32, DATETIME, TEXT, INT64, FLOAT64, BOOL = range(7)
+
+
+def type_of(a: np.ndarray) -> int:
+    if a.ndim == 2:
+        return TEXT
+    return {np.dtype(np.int32): INT32, np.dtype(np.float32): FLOAT32, np.dtype(np.int64): INT64,
+            np.dtype(np.float64): FLOAT64, np.dtype(np.uint8): BOOL}[a.dtype]
+
+
+def sort_perm(key: np.ndarray, desc=False, nulls=None, nulls_first=False, segments=None, in_perm=None,
+              threads=1, type_=None) -> np.ndarray:
+    """Stable ORDER BY permutation of one key (row ids), per segment."""
+    key = np.ascontiguousarray(key)
+    n = key.shape[0]
+    t = type_ if type_ is not None else type_of(key)
+    width = key.shape[1] if key.ndim == 2 else key.dtype.itemsize
+    out = np.empty(n, dtype=np.uint32)
+    seg = None if segments is None else np.ascontiguousarray(np.asarray(segments, dtype=np.uint32))
+    nl = None if nulls is None else np.ascontiguousarray(nulls.astype(np.uint8))
+    ip = None if in_perm is None else np.ascontiguousarray(in_perm.astype(np.uint32))
+    rc = lib().orc_sort_perm(t, _ptr(key), _ptr(nl), width, n, int(desc), int(nulls_first), _ptr(seg),
+                             0 if seg is None else len(seg) - 1, _ptr(ip), _ptr(out), threads)
+    assert rc == 0
+    return out
+
+
+def sort_perm_multi(keys: list, descs: list, nulls=None, nulls_first=None, threads=1) -> np.ndarray:
+    """ORDER BY k0, k1, ...: stable sorts from the least significant key."""
+    perm = None
+    for i in range(len(keys) - 1, -1, -1):
+        perm = sort_perm(keys[i], descs[i], None if nulls is None else nulls[i],
+                         False if nulls_first is None else nulls_first[i], in_perm=perm, threads=threads)
+    return perm
+
+
+def join_pairs(lcols: list, rcols: list, conds: list, lnulls=None, rnulls=None, cap=None):
+    """Inner join pairs (l, r) in (l, r) order; conds = [(lcol, rcol, cmp)]."""
+    def mk(cols, nulls):
+        arr = (OrcCol * len(cols))()
+        keep = []
+        for i, c in enumerate(cols):
+            c = np.ascontiguousarray(c)
+            keep.append(c)
+            nl = None if nulls is None or nulls[i] is None else np.ascontiguousarray(nulls[i].astype(np.uint8))
+            keep.append(nl)
+            arr[i] = OrcCol(c.ctypes.data, None if nl is None else nl.ctypes.data, type_of(c),
+                            c.shape[1] if c.ndim == 2 else c.dtype.itemsize)
+        return arr, keep
+
+    la, lk = mk(lcols, lnulls)
+    ra, rk = mk(rcols, rnulls)
+    L, R = lcols[0].shape[0], rcols[0].shape[0]
+    cd = np.asarray([x for c in conds for x in c], dtype=np.int32)
+    cap = cap if cap is not None else L * R
+    ol = np.empty(max(1, cap), dtype=np.uint32)
+    orr = np.empty(max(1, cap), dtype=np.uint32)
+    n = lib().orc_join_pairs(la, ra, _ptr(cd), len(conds), L, R, _ptr(ol), _ptr(orr), cap)
+    n = min(n, cap)
+    return ol[:n], orr[:n]
+
+
+def sales_query(t: dict, excluded: bytes, n: int | None = None, threads=1):
+    n = len(t["price"]) if n is None else n
+    ex = np.zeros(t["category"].shape[1], dtype=np.uint8)
+    ex[: len(excluded)] = np.frombuffer(excluded, dtype=np.uint8)
+    s, c, mn, mx = C.c_double(), C.c_int64(), C.c_float(), C.c_float()
+    lib().orc_sales_query(_ptr(t["price"]), _ptr(t["qty"]), _ptr(t["discount"]), _ptr(t["category"]),
+                          t["category"].shape[1], _ptr(ex), n, threads, C.byref(s), C.byref(c), C.byref(mn),
+                          C.byref(mx))
+    return s.value, c.value, mn.value, mx.value
+
+
+def star_query(fact: dict, dim: dict, year: int, n: int | None = None, threads=1):
+    n = len(fact["datekey"]) if n is None else n
+    ok = np.zeros(len(dim["datekey"]), dtype=np.uint8)
+    ok[dim["datekey"][dim["year"] == year]] = 1
+    s, c = C.c_double(), C.c_int64()
+    lib().orc_star_query(_ptr(fact["datekey"]), _ptr(fact["quantity"]), _ptr(fact["discount"]),
+                         _ptr(fact["extendedprice"]), n, _ptr(ok), len(ok), threads, C.byref(s), C.byref(c))
+    return s.value, c.value
+
+
+def cross_lt(x: np.ndarray, y: np.ndarray, cap=None):
+    cap = cap if cap is not None else len(x) * len(y)
+    ox = np.empty(max(1, cap), dtype=np.int32)
+    oy = np.empty(max(1, cap), dtype=np.int32)
+    n = lib().orc_cross_lt(_ptr(x), len(x), _ptr(y), len(y), _ptr(ox), _ptr(oy), cap)
+    return ox[: min(n, cap)], oy[: min(n, cap)], n

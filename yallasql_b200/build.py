@@ -1,0 +1,109 @@
+"""Build the in-tree shared libraries for sm_100a.
+
+``libyq_ops.so``    CUDA kernels + the C ABI declared in ``include/yq_ops.h``.
+``libyq_engine.so`` C++ operator layer (Batch / CacheManager / operators)
+                    declared in ``include/yq_engine.h``, linked against
+                    libyq_ops.so.
+
+Objects are compiled in parallel and only when a source or header changed.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+ENGINE = os.path.join(PKG, "engine")
+INCLUDE = os.path.join(ROOT, "include")
+BUILD = os.path.join(ROOT, "_build")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC",
+              "-I", INCLUDE, "-diag-suppress", "177"]
+OPS_LIB = os.path.join(PKG, "libyq_ops.so")
+ENGINE_LIB = os.path.join(PKG, "libyq_engine.so")
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _headers(d: str) -> list[str]:
+    out = []
+    for base in (d, INCLUDE):
+        for f in os.listdir(base):
+            if f.endswith((".cuh", ".h", ".hpp")):
+                out.append(os.path.join(base, f))
+    return out
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed:\n" + " ".join(cmd) + "\n" + r.stdout)
+
+
+def _compile_all(srcs: list[str], extra: list[str], headers: list[str]) -> list[str]:
+    os.makedirs(BUILD, exist_ok=True)
+    objs, jobs = [], []
+    for s in srcs:
+        o = os.path.join(BUILD, os.path.basename(s) + ".o")
+        objs.append(o)
+        if _stale(o, [s] + headers):
+            jobs.append([nvcc()] + ARCH + NVCC_FLAGS + extra + ["-c", s, "-o", o])
+    if jobs:
+        with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
+            list(ex.map(_run, jobs))
+    return objs
+
+
+def build_ops(verbose: bool = False) -> str:
+    srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    headers = _headers(CSRC)
+    objs = _compile_all(srcs, [], headers)
+    if _stale(OPS_LIB, objs):
+        _run([nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", OPS_LIB] + objs)
+        if verbose:
+            print("built", OPS_LIB)
+    return OPS_LIB
+
+
+def build_engine(verbose: bool = False) -> str:
+    if not os.path.isdir(ENGINE):
+        return ""
+    srcs = sorted(os.path.join(ENGINE, f) for f in os.listdir(ENGINE) if f.endswith((".cpp", ".cu")))
+    if not srcs:
+        return ""
+    headers = _headers(ENGINE)
+    objs = _compile_all(srcs, [], headers)
+    if _stale(ENGINE_LIB, objs + [OPS_LIB]):
+        _run([nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", ENGINE_LIB] + objs +
+             ["-L", PKG, "-lyq_ops", "-Xlinker", "-rpath,$ORIGIN"])
+        if verbose:
+            print("built", ENGINE_LIB)
+    return ENGINE_LIB
+
+
+def build(verbose: bool = False) -> None:
+    build_ops(verbose)
+    build_engine(verbose)
+
+
+if __name__ == "__main__":
+    build(verbose=True)
+    sys.exit(0)

@@ -1,0 +1,885 @@
+// Stable LSD radix argsort for ORDER BY (sm_100a), onesweep style
+// (Adinets & Merrill, "Onesweep: A Faster Least Significant Digit Radix Sort
+// for GPUs", 2022): one upfront histogram kernel computes every pass's digit
+// counts; each pass is then a single kernel that ranks a tile's digits with
+// warp ballots, obtains the tile's global digit offsets through a decoupled
+// look-back over tiles, and scatters through a shared-memory staging buffer so
+// global writes are contiguous per digit run.
+//
+// Replaces BoundRefSortExpression + int_to_uint32/float_to_uint32 +
+// launch_radix_sort (radix_sort_local_kerenl, launch_prefix_sum,
+// radix_sort_shuffle per 4-bit pass) + move_rows_batch
+// (include/engine/operators/expressions/bound_ref_sort.hpp:26-64,
+//  src/kernels/radix_sort_utils.cu:4-53, src/kernels/radix_sort_kernel.cu:65-178,
+//  include/kernels/radix_sort_kernel.hpp:26-73, include/kernels/move_rows_kernel.hpp:51-83).
+//
+// Segmented: rows are split into independent segments (sorted runs); tiles
+// never straddle a segment and the look-back stops at a segment's first tile,
+// so all 4 MB batches of a table (or all tasks of a batch) sort in one set of
+// launches. A single global sort is the one-segment case.
+#include <string.h>
+#include <vector>
+#include "yq_common.cuh"
+
+namespace yq {
+
+constexpr int kSortBlock = 256;
+constexpr uint32_t kStatAgg = 1u << 30;
+constexpr uint32_t kStatIncl = 2u << 30;
+constexpr uint32_t kStatMask = (1u << 30) - 1u;
+constexpr uint32_t kMaxSortRows = (1u << 30) - 1u;
+
+// Where the first pass of a key reads its keys from.
+struct KeySrc {
+  const char* data;
+  const uint8_t* nulls;
+  const uint32_t* in_perm;  // multi-key: this key's row for element e is in_perm[e]
+  int32_t type;
+  int32_t width;
+  int32_t vwords;       // value words in the key (excluding the null word)
+  int32_t desc;
+  int32_t nulls_first;
+  int32_t null_word;    // 1: word `vwords` is the null flag
+};
+
+struct SegInfo {
+  const uint32_t* seg_start;   // nseg + 1 row offsets
+  const uint32_t* tile_start;  // nseg + 1 tile offsets
+  int32_t nseg;
+};
+
+__device__ __forceinline__ uint32_t bswap(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
+
+// Order-preserving unsigned key words of one row (word 0 least significant).
+template <int KW>
+__device__ __forceinline__ void make_key(const KeySrc& s, uint32_t row, uint32_t (&k)[KW]) {
+#pragma unroll
+  for (int j = 0; j < KW; ++j) k[j] = 0u;
+  const bool is_null = s.nulls && s.nulls[row];
+  if (!is_null) {
+    switch (s.type) {
+      case YQ_INT32: {
+        k[0] = __ldg(reinterpret_cast<const uint32_t*>(s.data) + row) ^ 0x80000000u;
+        break;
+      }
+      case YQ_FLOAT32: {
+        uint32_t b = __ldg(reinterpret_cast<const uint32_t*>(s.data) + row);
+        if ((b & 0x7fffffffu) == 0u) b = 0u;                          // -0.0 ties with +0.0
+        else if ((b & 0x7f800000u) == 0x7f800000u && (b & 0x007fffffu)) b = 0x7fc00000u;  // NaN above +inf
+        k[0] = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+        break;
+      }
+      case YQ_INT64:
+      case YQ_DATETIME: {
+        unsigned long long v = __ldg(reinterpret_cast<const unsigned long long*>(s.data) + row);
+        k[0] = (uint32_t)v;
+        if (KW > 1) k[KW > 1 ? 1 : 0] = (uint32_t)(v >> 32) ^ 0x80000000u;
+        break;
+      }
+      case YQ_FLOAT64: {
+        unsigned long long b = __ldg(reinterpret_cast<const unsigned long long*>(s.data) + row);
+        if ((b & 0x7fffffffffffffffull) == 0ull) b = 0ull;
+        else if ((b & 0x7ff0000000000000ull) == 0x7ff0000000000000ull && (b & 0x000fffffffffffffull))
+          b = 0x7ff8000000000000ull;
+        b = (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+        k[0] = (uint32_t)b;
+        if (KW > 1) k[KW > 1 ? 1 : 0] = (uint32_t)(b >> 32);
+        break;
+      }
+      case YQ_BOOL: {
+        k[0] = (uint32_t)(s.data[row] != 0);
+        break;
+      }
+      default: {  // TEXT: the first vwords words of the slot as a big-endian integer
+        const uint32_t* p = reinterpret_cast<const uint32_t*>(s.data + (size_t)row * s.width);
+#pragma unroll
+        for (int j = 0; j < KW; ++j)
+          if (j < s.vwords) k[j] = bswap(__ldg(p + (s.vwords - 1 - j)));
+        break;
+      }
+    }
+    if (s.desc) {
+#pragma unroll
+      for (int j = 0; j < KW; ++j)
+        if (j < s.vwords) k[j] = ~k[j];
+    }
+  }
+  if (s.null_word) {
+    const uint32_t nv = s.nulls_first ? (is_null ? 0u : 1u) : (is_null ? 1u : 0u);
+#pragma unroll
+    for (int j = 0; j < KW; ++j)
+      if (j == s.vwords) k[j] = nv;
+  }
+}
+
+template <int KW, int D>
+__device__ __forceinline__ uint32_t digit_of(const uint32_t (&k)[KW], int shift) {
+  const int w = shift >> 5, o = shift & 31;
+  uint32_t lo = 0u, hi = 0u;
+#pragma unroll
+  for (int j = 0; j < KW; ++j) {
+    if (j == w) lo = k[j];
+    if (j == w + 1) hi = k[j];
+  }
+  uint32_t v = lo >> o;
+  if (o + D > 32) v |= hi << (32 - o);
+  return v & ((1u << D) - 1u);
+}
+
+__device__ __forceinline__ int find_segment(const SegInfo& g, uint32_t tile) {
+  int lo = 0, hi = g.nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(g.tile_start + mid) <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// ------------------------------------------------------------- histogram
+// Each block owns a contiguous range of tiles; per-segment counts for every
+// pass accumulate in shared memory and are flushed when the segment changes.
+template <int KW, int D>
+__global__ void __launch_bounds__(kSortBlock) k_sort_histogram(const KeySrc src, const SegInfo seg, uint32_t tile_rows,
+                                                               uint32_t ntiles, uint32_t* __restrict__ hist) {
+  constexpr int RADIX = 1 << D;
+  constexpr int P = (KW * 32 + D - 1) / D;
+  extern __shared__ uint32_t s_hist[];  // [P][RADIX]
+  const int lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < P * RADIX; i += kSortBlock) s_hist[i] = 0u;
+  __syncthreads();
+  const uint32_t per = ceil_div<uint32_t>(ntiles, gridDim.x);
+  const uint32_t t0 = blockIdx.x * per;
+  const uint32_t t1 = min(ntiles, t0 + per);
+  int cur = -1;
+  for (uint32_t t = t0; t < t1; ++t) {
+    const int sg = find_segment(seg, t);
+    if (sg != cur) {
+      if (cur >= 0) {
+        __syncthreads();
+        uint32_t* h = hist + (size_t)cur * P * RADIX;
+        for (int i = threadIdx.x; i < P * RADIX; i += kSortBlock) {
+          if (s_hist[i]) atomicAdd(h + i, s_hist[i]);
+          s_hist[i] = 0u;
+        }
+        __syncthreads();
+      }
+      cur = sg;
+    }
+    const uint32_t lt = t - __ldg(seg.tile_start + sg);
+    const uint32_t r0 = __ldg(seg.seg_start + sg) + lt * tile_rows;
+    const uint32_t r1 = min(__ldg(seg.seg_start + sg + 1), r0 + tile_rows);
+    for (uint32_t base = r0; base < r1; base += kSortBlock) {
+      const uint32_t e = base + threadIdx.x;
+      const bool valid = e < r1;
+      uint32_t k[KW];
+      if (valid) make_key<KW>(src, src.in_perm ? __ldg(src.in_perm + e) : e, k);
+      else {
+#pragma unroll
+        for (int j = 0; j < KW; ++j) k[j] = 0u;
+      }
+      const uint32_t vb = __ballot_sync(0xffffffffu, valid);
+      const int first = __ffs(vb) - 1;
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        const uint32_t d = digit_of<KW, D>(k, p * D);
+        const uint32_t d0 = __shfl_sync(0xffffffffu, d, first);
+        if (__all_sync(0xffffffffu, !valid || d == d0)) {
+          if (lane == first) atomicAdd(&s_hist[p * RADIX + d0], (uint32_t)__popc(vb));
+        } else if (valid) {
+          atomicAdd(&s_hist[p * RADIX + d], 1u);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (cur >= 0) {
+    uint32_t* h = hist + (size_t)cur * P * RADIX;
+    for (int i = threadIdx.x; i < P * RADIX; i += kSortBlock)
+      if (s_hist[i]) atomicAdd(h + i, s_hist[i]);
+  }
+}
+
+// --------------------------------------------------------------- onesweep
+struct SweepParams {
+  const uint32_t* keys_in;  // null on a key's first pass (keys come from src)
+  const uint32_t* vals_in;  // null on a key's first pass (vals = source row)
+  uint32_t* keys_out;       // null on the last pass
+  uint32_t* vals_out;
+  KeySrc src;
+  SegInfo seg;
+  const uint32_t* hist;  // [nseg][P][RADIX] of this key
+  uint32_t* status;      // [ntiles][RADIX], zero on entry
+  uint32_t* tile_counter;
+  uint32_t* err;
+  int32_t pass;          // index of this pass's digit (bit offset = pass * D)
+  int32_t npass;         // P
+};
+
+template <int KW, int D, int ITEMS>
+__global__ void __launch_bounds__(kSortBlock) k_sort_onesweep(const __grid_constant__ SweepParams S) {
+  constexpr int RADIX = 1 << D;
+  constexpr int NW = kSortBlock / 32;
+  constexpr uint32_t TILE = kSortBlock * ITEMS;
+  constexpr int DPT = (RADIX + kSortBlock - 1) / kSortBlock;  // digits per thread (1 here)
+  static_assert(RADIX <= kSortBlock, "one digit per thread");
+  (void)DPT;
+
+  extern __shared__ uint32_t smem[];
+  uint32_t* s_whist = smem;                       // [NW][RADIX]
+  uint32_t* s_tile_base = s_whist + NW * RADIX;   // [RADIX]
+  uint32_t* s_glob = s_tile_base + RADIX;         // [RADIX]
+  uint32_t* s_scan = s_glob + RADIX;              // [NW + 1]
+  uint32_t* s_misc = s_scan + NW + 1;             // [4]
+  uint32_t* s_keys = s_misc + 4;                  // [TILE][KW]
+  uint32_t* s_vals = s_keys + TILE * KW;          // [TILE]
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_misc[0] = atomicAdd(S.tile_counter, 1u);
+  for (int i = threadIdx.x; i < NW * RADIX; i += kSortBlock) s_whist[i] = 0u;
+  __syncthreads();
+  const uint32_t tile = s_misc[0];
+  const int sg = find_segment(S.seg, tile);
+  const uint32_t lt = tile - __ldg(S.seg.tile_start + sg);
+  const uint32_t seg0 = __ldg(S.seg.seg_start + sg);
+  const uint32_t seg1 = __ldg(S.seg.seg_start + sg + 1);
+  const uint32_t r0 = seg0 + lt * TILE;
+  const uint32_t tile_n = min(TILE, seg1 - r0);
+  const int shift = S.pass * D;
+
+  // 1. load (warp-striped: element = r0 + warp*ITEMS*32 + k*32 + lane)
+  uint32_t key[ITEMS][KW];
+  uint32_t val[ITEMS];
+  uint32_t dig[ITEMS];
+  uint32_t rank[ITEMS];
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint32_t off = (uint32_t)(warp * ITEMS * 32 + k * 32 + lane);
+    const uint32_t e = r0 + off;
+    const bool valid = off < tile_n;
+    if (valid) {
+      if (S.keys_in) {
+        if (KW == 1) {
+          key[k][0] = __ldg(S.keys_in + e);
+        } else if (KW == 2) {
+          uint2 q = __ldg(reinterpret_cast<const uint2*>(S.keys_in) + e);
+          key[k][0] = q.x;
+          key[k][KW > 1 ? 1 : 0] = q.y;
+        } else {
+#pragma unroll
+          for (int j = 0; j < KW; j += 4) {
+            uint4 q = ldg_nc_v4(S.keys_in + (size_t)e * KW + j);
+            key[k][j] = q.x;
+            key[k][j + 1 < KW ? j + 1 : 0] = q.y;
+            key[k][j + 2 < KW ? j + 2 : 0] = q.z;
+            key[k][j + 3 < KW ? j + 3 : 0] = q.w;
+          }
+        }
+        val[k] = __ldg(S.vals_in + e);
+      } else {
+        const uint32_t row = S.src.in_perm ? __ldg(S.src.in_perm + e) : e;
+        make_key<KW>(S.src, row, key[k]);
+        val[k] = row;
+      }
+      dig[k] = digit_of<KW, D>(key[k], shift);
+    } else {
+#pragma unroll
+      for (int j = 0; j < KW; ++j) key[k][j] = 0u;
+      val[k] = 0u;
+      dig[k] = 0u;
+    }
+  }
+
+  // 2. warp-level stable ranking (order within a warp = (k, lane))
+  const uint32_t lt_mask = lanemask_lt();
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint32_t off = (uint32_t)(warp * ITEMS * 32 + k * 32 + lane);
+    const bool valid = off < tile_n;
+    uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+    for (int b = 0; b < D; ++b) {
+      const bool bit = (dig[k] >> b) & 1u;
+      const uint32_t bb = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? bb : ~bb;
+    }
+    const int leader = __ffs(peers) - 1;
+    uint32_t old = 0u;
+    if (valid && lane == leader) {
+      old = s_whist[warp * RADIX + dig[k]];
+      s_whist[warp * RADIX + dig[k]] = old + __popc(peers);
+    }
+    old = __shfl_sync(0xffffffffu, old, leader < 0 ? 0 : leader);
+    rank[k] = old + __popc(peers & lt_mask);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // 3. per-digit: warp offsets, tile count, global digit base of the segment
+  const int t = threadIdx.x;
+  uint32_t tile_count = 0u, seg_count = 0u;
+  if (t < RADIX) {
+    for (int w = 0; w < NW; ++w) {
+      const uint32_t c = s_whist[w * RADIX + t];
+      s_whist[w * RADIX + t] = tile_count;
+      tile_count += c;
+    }
+    seg_count = __ldg(S.hist + ((size_t)sg * S.npass + S.pass) * RADIX + t);
+  }
+  uint32_t total;
+  const uint32_t tile_excl = block_exclusive_sum<kSortBlock>(t < RADIX ? tile_count : 0u, s_scan, total);
+  const uint32_t seg_excl = block_exclusive_sum<kSortBlock>(t < RADIX ? seg_count : 0u, s_scan, total);
+
+  // 4. decoupled look-back per digit over the segment's earlier tiles
+  if (t < RADIX) {
+    s_tile_base[t] = tile_excl;
+    uint32_t* st = S.status + (size_t)tile * RADIX + t;
+    uint32_t excl = 0u;
+    if (lt == 0) {
+      st_relaxed_u32(st, kStatIncl | tile_count);
+    } else {
+      st_relaxed_u32(st, kStatAgg | tile_count);
+      const uint32_t* p = st - RADIX;
+      uint32_t back = lt;
+      uint32_t spins = 0;
+      while (back > 0) {
+        const uint32_t v = ld_relaxed_u32(p);
+        const uint32_t f = v & ~kStatMask;
+        if (f == 0u) {
+          if (++spins > kSpinLimit || ((spins & 63u) == 0u && ld_relaxed_u32(S.err) != 0u)) {
+            atomicOr(S.err, kErrTimeout);
+            break;
+          }
+          __nanosleep(spins < 64 ? 32 : 128);
+          continue;
+        }
+        excl += v & kStatMask;
+        if (f == kStatIncl) break;
+        p -= RADIX;
+        --back;
+      }
+      st_relaxed_u32(st, kStatIncl | ((excl + tile_count) & kStatMask));
+    }
+    s_glob[t] = seg0 + seg_excl + excl;
+  }
+  __syncthreads();
+
+  // 5. stage the tile in shared memory in digit order
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint32_t off = (uint32_t)(warp * ITEMS * 32 + k * 32 + lane);
+    if (off < tile_n) {
+      const uint32_t lp = s_tile_base[dig[k]] + s_whist[warp * RADIX + dig[k]] + rank[k];
+      if (lp >= tile_n) {
+        atomicOr(S.err, kErrBounds);
+        continue;
+      }
+#pragma unroll
+      for (int j = 0; j < KW; ++j) s_keys[lp * KW + j] = key[k][j];
+      s_vals[lp] = val[k];
+    }
+  }
+  __syncthreads();
+
+  // 6. contiguous scatter per digit run
+  for (uint32_t i = threadIdx.x; i < tile_n; i += kSortBlock) {
+    uint32_t kk[KW];
+#pragma unroll
+    for (int j = 0; j < KW; ++j) kk[j] = s_keys[i * KW + j];
+    const uint32_t d = digit_of<KW, D>(kk, shift);
+    const uint32_t g = s_glob[d] + (i - s_tile_base[d]);
+    if (g < seg0 || g >= seg1) {  // offsets inconsistent with the histogram: skip, report
+      atomicOr(S.err, kErrBounds);
+      continue;
+    }
+    if (S.keys_out) {
+      if (KW == 1) {
+        S.keys_out[g] = kk[0];
+      } else if (KW == 2) {
+        reinterpret_cast<uint2*>(S.keys_out)[g] = make_uint2(kk[0], kk[KW > 1 ? 1 : 0]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < KW; j += 4)
+          *reinterpret_cast<uint4*>(S.keys_out + (size_t)g * KW + j) =
+              make_uint4(kk[j], kk[j + 1 < KW ? j + 1 : 0], kk[j + 2 < KW ? j + 2 : 0], kk[j + 3 < KW ? j + 3 : 0]);
+      }
+    }
+    S.vals_out[g] = s_vals[i];
+  }
+}
+
+__global__ void k_iota_segments(uint32_t* out, const uint32_t* in_perm, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = in_perm ? in_perm[i] : i;
+}
+
+// Number of significant 4-byte words of a text column (index of the last
+// nonzero word + 1 over all rows).
+__global__ void k_text_words(const char* data, const uint8_t* nulls, int width, uint32_t n, uint32_t* out) {
+  uint32_t best = 0;
+  const int words = width >> 2;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    if (nulls && nulls[r]) continue;
+    const uint32_t* p = reinterpret_cast<const uint32_t*>(data + (size_t)r * width);
+    for (int j = words - 1; j >= (int)best; --j)
+      if (__ldg(p + j)) {
+        best = j + 1;
+        break;
+      }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, d));
+  if ((threadIdx.x & 31) == 0 && best) atomicMax(out, best);
+}
+
+// ------------------------------------------------------------------ gather
+struct GatherCol {
+  const char* src;
+  const uint8_t* src_nulls;
+  char* dst;
+  uint8_t* dst_nulls;
+  int32_t width;
+};
+struct GatherParams {
+  GatherCol c[YQ_MAX_BATCH_COLUMNS];
+  int32_t ncols;
+};
+
+__device__ __forceinline__ void copy_bytes(char* dst, const char* src, int width) {
+  if (width == 4) *reinterpret_cast<uint32_t*>(dst) = __ldg(reinterpret_cast<const uint32_t*>(src));
+  else if (width == 8)
+    *reinterpret_cast<unsigned long long*>(dst) = __ldg(reinterpret_cast<const unsigned long long*>(src));
+  else if (width == 1) *dst = *src;
+  else if ((width & 15) == 0 && ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0)
+    for (int i = 0; i < width; i += 16) *reinterpret_cast<uint4*>(dst + i) = ldg_nc_v4(src + i);
+  else
+    for (int i = 0; i < width; i += 4)
+      *reinterpret_cast<uint32_t*>(dst + i) = __ldg(reinterpret_cast<const uint32_t*>(src + i));
+}
+
+__global__ void __launch_bounds__(256) k_gather(const __grid_constant__ GatherParams G, const uint32_t* __restrict__ perm,
+                                                uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t r = __ldg(perm + i);
+    if (r >= n) continue;  // perm must be a permutation of [0, n): skip anything else
+    for (int c = 0; c < G.ncols; ++c) {
+      const GatherCol& g = G.c[c];
+      copy_bytes(g.dst + (size_t)i * g.width, g.src + (size_t)r * g.width, g.width);
+      if (g.dst_nulls) g.dst_nulls[i] = g.src_nulls ? g.src_nulls[r] : 0;
+    }
+  }
+}
+
+// -------------------------------------------------------------- host side
+struct SortShape {
+  int kw;     // key words (1, 2, 4, 8)
+  int vwords;
+  int null_word;
+};
+
+static int key_value_words(const yq_column& c) {
+  switch (c.type) {
+    case YQ_INT32:
+    case YQ_FLOAT32:
+    case YQ_BOOL: return 1;
+    case YQ_INT64:
+    case YQ_DATETIME:
+    case YQ_FLOAT64: return 2;
+    case YQ_TEXT: return c.width / 4;
+    default: return -1;
+  }
+}
+
+static bool valid_key_column(const yq_column& c) {
+  if (!c.data) return false;
+  switch (c.type) {
+    case YQ_INT32:
+    case YQ_FLOAT32: return c.width == 4;
+    case YQ_INT64:
+    case YQ_DATETIME:
+    case YQ_FLOAT64: return c.width == 8;
+    case YQ_BOOL: return c.width == 1;
+    case YQ_TEXT: return c.width >= 4 && c.width <= YQ_MAX_TEXT_WIDTH && c.width % 4 == 0;
+    default: return false;
+  }
+}
+
+static int round_kw(int w) { return w <= 1 ? 1 : (w <= 2 ? 2 : (w <= 4 ? 4 : (w <= 8 ? 8 : -1))); }
+
+static int items_for(int kw) { return kw == 1 ? 16 : (kw == 2 ? 12 : (kw == 4 ? 8 : 4)); }
+
+template <int KW, int D, int ITEMS>
+static size_t sweep_smem() {
+  constexpr int RADIX = 1 << D;
+  constexpr int NW = kSortBlock / 32;
+  return sizeof(uint32_t) * ((size_t)NW * RADIX + 2 * RADIX + NW + 1 + 4 + (size_t)kSortBlock * ITEMS * (KW + 1));
+}
+
+template <int KW, int D, int ITEMS>
+static int launch_sweep(const SweepParams& P, uint32_t ntiles, cudaStream_t s) {
+  const size_t smem = sweep_smem<KW, D, ITEMS>();
+  static bool attr = false;
+  if (!attr) {
+    YQ_TRY_CUDA(cudaFuncSetAttribute(k_sort_onesweep<KW, D, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    attr = true;
+  }
+  k_sort_onesweep<KW, D, ITEMS><<<ntiles, kSortBlock, smem, s>>>(P);
+  YQ_CHECK_LAUNCH();
+  return YQ_OK;
+}
+
+template <int KW, int D>
+static int launch_hist(const KeySrc& src, const SegInfo& seg, uint32_t tile_rows, uint32_t ntiles, uint32_t* hist,
+                       cudaStream_t s) {
+  constexpr int P = (KW * 32 + D - 1) / D;
+  const size_t smem = sizeof(uint32_t) * P * (1 << D);
+  static bool attr = false;
+  if (!attr) {
+    YQ_TRY_CUDA(cudaFuncSetAttribute(k_sort_histogram<KW, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = true;
+  }
+  int grid = sm_count() * 4;
+  if ((uint32_t)grid > ntiles) grid = (int)ntiles;
+  if (grid < 1) grid = 1;
+  k_sort_histogram<KW, D><<<grid, kSortBlock, smem, s>>>(src, seg, tile_rows, ntiles, hist);
+  YQ_CHECK_LAUNCH();
+  return YQ_OK;
+}
+
+// Dispatch table over (KW, D).
+struct SortKernels {
+  int (*hist)(const KeySrc&, const SegInfo&, uint32_t, uint32_t, uint32_t*, cudaStream_t);
+  int (*sweep)(const SweepParams&, uint32_t, cudaStream_t);
+  int items;
+};
+
+template <int KW, int D, int ITEMS>
+static SortKernels make_kernels() {
+  SortKernels k;
+  k.hist = &launch_hist<KW, D>;
+  k.sweep = &launch_sweep<KW, D, ITEMS>;
+  k.items = ITEMS;
+  return k;
+}
+
+static bool pick_kernels(int kw, int d, SortKernels& k) {
+  switch (kw * 100 + d) {
+    case 108: k = make_kernels<1, 8, 16>(); return true;
+    case 106: k = make_kernels<1, 6, 16>(); return true;
+    case 104: k = make_kernels<1, 4, 16>(); return true;
+    case 208: k = make_kernels<2, 8, 12>(); return true;
+    case 206: k = make_kernels<2, 6, 12>(); return true;
+    case 204: k = make_kernels<2, 4, 12>(); return true;
+    case 408: k = make_kernels<4, 8, 8>(); return true;
+    case 808: k = make_kernels<8, 8, 4>(); return true;
+    default: return false;
+  }
+}
+
+struct SegPlan {
+  std::vector<uint32_t> seg;    // nseg + 1
+  std::vector<uint32_t> tiles;  // nseg + 1
+  uint32_t ntiles = 0;
+};
+
+static void plan_segments(const uint32_t* offsets, int nseg, uint32_t tile_rows, SegPlan& sp) {
+  sp.seg.assign(offsets, offsets + nseg + 1);
+  sp.tiles.resize(nseg + 1);
+  uint32_t t = 0;
+  for (int i = 0; i < nseg; ++i) {
+    sp.tiles[i] = t;
+    const uint32_t len = offsets[i + 1] - offsets[i];
+    t += ceil_div<uint32_t>(len, tile_rows);
+  }
+  sp.tiles[nseg] = t;
+  sp.ntiles = t;
+}
+
+// One key of a (possibly multi-key) segmented sort: perm_in (null = identity) -> perm_out.
+struct KeyJob {
+  yq_column key;
+  int desc, nulls_first;
+};
+
+// Resolved plan for one key: words, digit width, tiling.
+struct KeyPlan {
+  SortShape sh;
+  int D, P, R;
+  SortKernels K;
+  uint32_t tile_rows, ntiles;
+};
+
+static int plan_key(const yq_column& c, int vwords_override, int want_d, const uint32_t* seg_offsets, int nseg,
+                    KeyPlan& kp) {
+  kp.sh.vwords = vwords_override >= 0 ? vwords_override : key_value_words(c);
+  kp.sh.null_word = c.nulls != nullptr;
+  kp.sh.kw = round_kw(kp.sh.vwords + kp.sh.null_word);
+  if (kp.sh.kw < 0) return YQ_ERR_UNSUPPORTED;
+  kp.D = want_d;
+  if (!pick_kernels(kp.sh.kw, kp.D, kp.K)) {
+    kp.D = 8;
+    if (!pick_kernels(kp.sh.kw, 8, kp.K)) return YQ_ERR_UNSUPPORTED;
+  }
+  kp.P = (kp.sh.kw * 32 + kp.D - 1) / kp.D;
+  kp.R = 1 << kp.D;
+  kp.tile_rows = (uint32_t)kSortBlock * kp.K.items;
+  kp.ntiles = 0;
+  for (int i = 0; i < nseg; ++i) kp.ntiles += ceil_div<uint32_t>(seg_offsets[i + 1] - seg_offsets[i], kp.tile_rows);
+  return YQ_OK;
+}
+
+// Workspace: [seg offsets][tile offsets][histograms][look-back status per pass]
+//            [counters][keys A/B][vals A/B][perm between keys]
+int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint32_t* seg_offsets_host, int nseg,
+                       uint32_t* out_perm, const yq_sort_config* cfg, void* workspace, size_t workspace_bytes,
+                       cudaStream_t s, size_t* size_only) {
+  if (njobs <= 0 || nseg <= 0 || !seg_offsets_host) return YQ_ERR_INVALID_ARG;
+  if (rows > kMaxSortRows) return YQ_ERR_UNSUPPORTED;
+  if (seg_offsets_host[0] != 0 || seg_offsets_host[nseg] != rows) return YQ_ERR_INVALID_ARG;
+  for (int i = 0; i < nseg; ++i)
+    if (seg_offsets_host[i + 1] < seg_offsets_host[i]) return YQ_ERR_INVALID_ARG;
+  const int want_d = (cfg && cfg->digit_bits) ? cfg->digit_bits : 8;
+  if (want_d != 4 && want_d != 6 && want_d != 8) return YQ_ERR_INVALID_ARG;
+  const bool keep_trivial = cfg && cfg->keep_trivial;
+
+  // Size buffers for the widest plan any key can take (text keys are sized
+  // for their full slot, up to 8 words; their significant width is measured
+  // on the device before they are sorted).
+  size_t max_kw = 1, max_hist = 1, max_status = 1;
+  for (int j = 0; j < njobs; ++j) {
+    const yq_column& c = jobs[j].key;
+    if (!valid_key_column(c)) return YQ_ERR_INVALID_ARG;
+    KeyPlan kp;
+    int vw = key_value_words(c);
+    if (c.type == YQ_TEXT && vw > 8 - (c.nulls ? 1 : 0)) vw = 8 - (c.nulls ? 1 : 0);
+    int st = plan_key(c, vw, want_d, seg_offsets_host, nseg, kp);
+    if (st != YQ_OK) return st;
+    // For a text key this is the plan at its full (clamped) width, which
+    // bounds every narrower plan: fewer words mean fewer passes and larger tiles.
+    max_kw = kp.sh.kw > (int)max_kw ? kp.sh.kw : max_kw;
+    const size_t h = (size_t)nseg * kp.P * kp.R, sz = (size_t)kp.P * kp.ntiles * kp.R;
+    if (h > max_hist) max_hist = h;
+    if (sz > max_status) max_status = sz;
+  }
+
+  WsSize w;
+  w.add<uint32_t>(nseg + 1);
+  w.add<uint32_t>(nseg + 1);
+  w.add<uint32_t>(max_hist);
+  w.add<uint32_t>(max_status);
+  w.add<uint32_t>(80);
+  w.add<uint32_t>((size_t)rows * max_kw);
+  w.add<uint32_t>((size_t)rows * max_kw);
+  w.add<uint32_t>(rows);
+  w.add<uint32_t>(rows);
+  w.add<uint32_t>(rows);
+  if (size_only) {
+    *size_only = w.total();
+    return YQ_OK;
+  }
+  if (!out_perm) return YQ_ERR_INVALID_ARG;
+  if (rows == 0) return YQ_OK;
+
+  Workspace ws;
+  YQ_TRY(ws.acquire(workspace, workspace_bytes, w.total(), s));
+  uint32_t* d_seg = ws.take<uint32_t>(nseg + 1);
+  uint32_t* d_tiles = ws.take<uint32_t>(nseg + 1);
+  uint32_t* d_hist = ws.take<uint32_t>(max_hist);
+  uint32_t* d_status = ws.take<uint32_t>(max_status);
+  uint32_t* d_misc = ws.take<uint32_t>(80);  // [0..63] tile counters, [64] error, [65] text words
+  uint32_t* d_keys[2] = {ws.take<uint32_t>((size_t)rows * max_kw), ws.take<uint32_t>((size_t)rows * max_kw)};
+  uint32_t* d_vals[2] = {ws.take<uint32_t>(rows), ws.take<uint32_t>(rows)};
+  uint32_t* d_perm_tmp = ws.take<uint32_t>(rows);
+  uint32_t* d_err = d_misc + 64;
+  uint32_t* d_textw = d_misc + 65;
+  YQ_TRY_CUDA(cudaMemsetAsync(d_misc, 0, 80 * sizeof(uint32_t), s));
+
+  const uint32_t* perm_in = nullptr;  // order from the less significant keys (null = identity)
+  for (int jj = njobs - 1; jj >= 0; --jj) {
+    const KeyJob& job = jobs[jj];
+    const yq_column& c = job.key;
+    int vw = -1;
+    if (c.type == YQ_TEXT) {
+      // Only the significant prefix of the slot takes part: trailing all-zero
+      // words are equal for every row.
+      uint32_t tw = 0;
+      YQ_TRY_CUDA(cudaMemsetAsync(d_textw, 0, sizeof(uint32_t), s));
+      k_text_words<<<sm_count() * 4, 256, 0, s>>>(static_cast<const char*>(c.data), c.nulls, c.width, rows, d_textw);
+      YQ_CHECK_LAUNCH();
+      YQ_TRY_CUDA(cudaMemcpyAsync(&tw, d_textw, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      YQ_TRY_CUDA(cudaStreamSynchronize(s));
+      vw = (int)tw;
+      if (vw == 0 && !c.nulls) continue;  // every key equal: order unchanged
+    }
+    KeyPlan kp;
+    YQ_TRY(plan_key(c, vw, want_d, seg_offsets_host, nseg, kp));
+    SegPlan sp;
+    plan_segments(seg_offsets_host, nseg, kp.tile_rows, sp);
+    YQ_TRY_CUDA(cudaMemcpyAsync(d_seg, sp.seg.data(), (nseg + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    YQ_TRY_CUDA(cudaMemcpyAsync(d_tiles, sp.tiles.data(), (nseg + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    YQ_TRY_CUDA(cudaMemsetAsync(d_hist, 0, (size_t)nseg * kp.P * kp.R * sizeof(uint32_t), s));
+    YQ_TRY_CUDA(cudaMemsetAsync(d_status, 0, (size_t)kp.P * sp.ntiles * kp.R * sizeof(uint32_t), s));
+    YQ_TRY_CUDA(cudaMemsetAsync(d_misc, 0, 64 * sizeof(uint32_t), s));
+
+    KeySrc src;
+    src.data = static_cast<const char*>(c.data);
+    src.nulls = c.nulls;
+    src.in_perm = perm_in;
+    src.type = c.type;
+    src.width = c.width;
+    src.vwords = kp.sh.vwords;
+    src.desc = job.desc;
+    src.nulls_first = job.nulls_first;
+    src.null_word = kp.sh.null_word;
+    SegInfo seg;
+    seg.seg_start = d_seg;
+    seg.tile_start = d_tiles;
+    seg.nseg = nseg;
+    YQ_TRY(kp.K.hist(src, seg, kp.tile_rows, sp.ntiles, d_hist, s));
+
+    std::vector<int> passes;
+    if (keep_trivial) {
+      for (int p = 0; p < kp.P; ++p) passes.push_back(p);
+    } else {
+      // A pass whose digit is the same for every key of every segment leaves
+      // the order unchanged and is skipped.
+      std::vector<uint32_t> h((size_t)nseg * kp.P * kp.R);
+      YQ_TRY_CUDA(cudaMemcpyAsync(h.data(), d_hist, h.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      YQ_TRY_CUDA(cudaStreamSynchronize(s));
+      for (int p = 0; p < kp.P; ++p) {
+        bool trivial = true;
+        for (int g = 0; g < nseg && trivial; ++g) {
+          const uint32_t len = seg_offsets_host[g + 1] - seg_offsets_host[g];
+          if (len == 0) continue;
+          const uint32_t* hp = h.data() + ((size_t)g * kp.P + p) * kp.R;
+          bool one = false;
+          for (int d = 0; d < kp.R && !one; ++d) one = (hp[d] == len);
+          trivial = one;
+        }
+        if (!trivial) passes.push_back(p);
+      }
+    }
+    if (passes.empty()) continue;  // order unchanged by this key
+    if (passes.size() > 64) return YQ_ERR_UNSUPPORTED;
+    uint32_t* dst_perm = (perm_in == out_perm) ? d_perm_tmp : out_perm;
+    for (size_t i = 0; i < passes.size(); ++i) {
+      const bool first = (i == 0), last = (i + 1 == passes.size());
+      SweepParams Sp;
+      Sp.keys_in = first ? nullptr : d_keys[(i - 1) & 1];
+      Sp.vals_in = first ? nullptr : d_vals[(i - 1) & 1];
+      Sp.keys_out = last ? nullptr : d_keys[i & 1];
+      Sp.vals_out = last ? dst_perm : d_vals[i & 1];
+      Sp.src = src;
+      Sp.seg = seg;
+      Sp.hist = d_hist;
+      Sp.status = d_status + (size_t)i * sp.ntiles * kp.R;
+      Sp.tile_counter = d_misc + i;
+      Sp.err = d_err;
+      Sp.pass = passes[i];
+      Sp.npass = kp.P;
+      YQ_TRY(kp.K.sweep(Sp, sp.ntiles, s));
+    }
+    perm_in = dst_perm;
+  }
+  if (perm_in != out_perm) {
+    if (perm_in) {
+      YQ_TRY_CUDA(cudaMemcpyAsync(out_perm, perm_in, (size_t)rows * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    } else {
+      k_iota_segments<<<sm_count() * 4, 256, 0, s>>>(out_perm, nullptr, rows);
+      YQ_CHECK_LAUNCH();
+    }
+  }
+  if (!keep_trivial) {
+    uint32_t err = 0;
+    YQ_TRY_CUDA(cudaMemcpyAsync(&err, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    YQ_TRY_CUDA(cudaStreamSynchronize(s));
+    if (err & kErrTimeout) return YQ_ERR_TIMEOUT;
+    if (err & kErrBounds) return YQ_ERR_INVALID_ARG;
+  }
+  return YQ_OK;
+}
+
+}  // namespace yq
+
+using namespace yq;
+
+extern "C" {
+
+size_t yq_sort_workspace_size(const yq_column* key, uint32_t rows) {
+  if (!key) return 0;
+  KeyJob j{*key, 0, 0};
+  uint32_t offs[2] = {0, rows};
+  size_t bytes = 0;
+  if (sort_segments_impl(&j, 1, rows, offs, 1, nullptr, nullptr, nullptr, 0, nullptr, &bytes) != YQ_OK) return 0;
+  return bytes;
+}
+
+int yq_sort_indices(const yq_column* key, uint32_t rows, int32_t descending, int32_t nulls_first, uint32_t* out_perm,
+                    const yq_sort_config* config, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!key) return YQ_ERR_INVALID_ARG;
+  KeyJob j{*key, descending != 0, nulls_first != 0};
+  uint32_t offs[2] = {0, rows};
+  return sort_segments_impl(&j, 1, rows, offs, 1, out_perm, config, workspace, workspace_bytes, as_stream(stream),
+                            nullptr);
+}
+
+int yq_sort_indices_multi(const yq_column* keys, const int32_t* descending, const int32_t* nulls_first, int32_t nkeys,
+                          uint32_t rows, uint32_t* out_perm, const yq_sort_config* config, void* workspace,
+                          size_t workspace_bytes, void* stream) {
+  if (!keys || nkeys <= 0 || nkeys > YQ_MAX_BATCH_COLUMNS) return YQ_ERR_INVALID_ARG;
+  std::vector<KeyJob> jobs(nkeys);
+  for (int i = 0; i < nkeys; ++i) {
+    jobs[i].key = keys[i];
+    jobs[i].desc = descending ? descending[i] != 0 : 0;
+    jobs[i].nulls_first = nulls_first ? nulls_first[i] != 0 : 0;
+  }
+  uint32_t offs[2] = {0, rows};
+  return sort_segments_impl(jobs.data(), nkeys, rows, offs, 1, out_perm, config, workspace, workspace_bytes,
+                            as_stream(stream), nullptr);
+}
+
+size_t yq_sort_segments_workspace_size(const yq_column* key, uint32_t rows, const uint32_t* seg_offsets, int32_t nseg) {
+  if (!key) return 0;
+  KeyJob j{*key, 0, 0};
+  size_t bytes = 0;
+  if (sort_segments_impl(&j, 1, rows, seg_offsets, nseg, nullptr, nullptr, nullptr, 0, nullptr, &bytes) != YQ_OK)
+    return 0;
+  return bytes;
+}
+
+int yq_sort_segments(const yq_column* key, uint32_t rows, const uint32_t* seg_offsets, int32_t nseg, int32_t descending,
+                     int32_t nulls_first, uint32_t* out_perm, const yq_sort_config* config, void* workspace,
+                     size_t workspace_bytes, void* stream) {
+  if (!key) return YQ_ERR_INVALID_ARG;
+  KeyJob j{*key, descending != 0, nulls_first != 0};
+  return sort_segments_impl(&j, 1, rows, seg_offsets, nseg, out_perm, config, workspace, workspace_bytes,
+                            as_stream(stream), nullptr);
+}
+
+int yq_gather(const yq_column* in, int32_t ncols, const uint32_t* perm, uint32_t rows, yq_column* out, void* stream) {
+  if (ncols < 0 || ncols > YQ_MAX_BATCH_COLUMNS || (ncols > 0 && (!in || !out)) || (rows > 0 && !perm))
+    return YQ_ERR_INVALID_ARG;
+  if (rows == 0 || ncols == 0) return YQ_OK;
+  GatherParams G;
+  memset(&G, 0, sizeof(G));
+  G.ncols = ncols;
+  for (int c = 0; c < ncols; ++c) {
+    if (!in[c].data || !out[c].data || in[c].width != out[c].width || in[c].width <= 0) return YQ_ERR_INVALID_ARG;
+    if (in[c].width != 1 && in[c].width % 4 != 0) return YQ_ERR_INVALID_ARG;
+    G.c[c].src = static_cast<const char*>(in[c].data);
+    G.c[c].src_nulls = in[c].nulls;
+    G.c[c].dst = static_cast<char*>(out[c].data);
+    G.c[c].dst_nulls = const_cast<uint8_t*>(out[c].nulls);
+    G.c[c].width = in[c].width;
+  }
+  cudaStream_t s = as_stream(stream);
+  int grid = (int)ceil_div<uint32_t>(rows, 256);
+  const int cap = sm_count() * 16;
+  if (grid > cap) grid = cap;
+  k_gather<<<grid, 256, 0, s>>>(G, perm, rows);
+  YQ_CHECK_LAUNCH();
+  return YQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,294 @@
+// Host-side loader for expression programs: validates a client's postfix
+// program against the batch schema, applies peephole fusions, and annotates
+// each instruction with the stack moves it needs (see yq_vm.cuh).
+#pragma once
+
+#include <string.h>
+#include "yq_vm.cuh"
+
+namespace yq {
+
+struct ProgramBuilder {
+  VmProgram P;
+  int len = 0;
+  int nconsts = 0;
+  int ntext = 0;
+
+  ProgramBuilder() { memset(&P, 0, sizeof(P)); }
+
+  int set_columns(const yq_column* cols, int ncols) {
+    if (ncols < 0 || ncols > YQ_MAX_BATCH_COLUMNS || (ncols > 0 && !cols)) return YQ_ERR_INVALID_ARG;
+    P.ncols = ncols;
+    for (int i = 0; i < ncols; ++i) {
+      const yq_column& c = cols[i];
+      if (!valid_column(c)) return YQ_ERR_INVALID_ARG;
+      DevCol& d = P.cols[i];
+      d.data = static_cast<const char*>(c.data);
+      d.nulls = c.nulls;
+      d.type = c.type;
+      d.width = c.width;
+      d.vec = ((reinterpret_cast<uintptr_t>(c.data) & 15u) == 0);
+      d.nvec = ((reinterpret_cast<uintptr_t>(c.nulls) & 3u) == 0);
+    }
+    return YQ_OK;
+  }
+
+  static bool valid_column(const yq_column& c) {
+    switch (c.type) {
+      case YQ_INT32:
+      case YQ_FLOAT32: return c.width == 4;
+      case YQ_INT64:
+      case YQ_DATETIME:
+      case YQ_FLOAT64: return c.width == 8;
+      case YQ_BOOL: return c.width == 1;
+      case YQ_TEXT: return c.width >= 4 && c.width <= YQ_MAX_TEXT_WIDTH && (c.width % 4) == 0;
+      default: return false;
+    }
+  }
+
+  int set_constants(const yq_constants* k) {
+    if (!k) return YQ_OK;
+    if (k->count < 0 || k->count > YQ_MAX_CONSTANTS || (k->count > 0 && !k->values)) return YQ_ERR_INVALID_ARG;
+    for (int i = 0; i < k->count; ++i) P.consts[i] = k->values[i];
+    nconsts = k->count;
+    if (k->text_count < 0 || k->text_count > YQ_MAX_TEXT_CONSTANTS) return YQ_ERR_INVALID_ARG;
+    if (k->text_count > 0) {
+      if (!k->text || k->text_width <= 0 || k->text_width > YQ_MAX_TEXT_WIDTH) return YQ_ERR_INVALID_ARG;
+      const int words = (k->text_width + 3) / 4;
+      P.text_words = words;
+      for (int s = 0; s < k->text_count; ++s) {
+        const unsigned char* src = reinterpret_cast<const unsigned char*>(k->text) + (size_t)s * k->text_width;
+        for (int w = 0; w < words; ++w) {
+          uint32_t v = 0;
+          for (int b = 0; b < 4; ++b) {
+            int idx = w * 4 + b;
+            v = (v << 8) | (idx < k->text_width ? src[idx] : 0u);
+          }
+          P.text[s][w] = v;
+        }
+      }
+      ntext = k->text_count;
+    }
+    return YQ_OK;
+  }
+
+  static bool numeric(int t) {
+    return t == YQ_INT32 || t == YQ_FLOAT32 || t == YQ_INT64 || t == YQ_DATETIME || t == YQ_FLOAT64;
+  }
+  static bool loadable(int t) { return numeric(t) || t == YQ_BOOL; }
+  static bool castable(int from, int to) { return loadable(from) && loadable(to); }
+
+  int col_type(int c) const { return (c >= 0 && c < P.ncols) ? P.cols[c].type : -1; }
+
+  // Append one client program; on success `result_type` is the type left on
+  // the stack (exactly one value).
+  int append(const yq_program* prog, int& result_type) {
+    if (!prog || prog->len <= 0 || !prog->code) return YQ_ERR_INVALID_ARG;
+    int types[8];
+    int depth = 0;
+    const int start = len;
+    for (int i = 0; i < prog->len; ++i) {
+      Insn I;
+      I.op = prog->code[i].op;
+      I.type = prog->code[i].type;
+      I.a = prog->code[i].a;
+      I.b = prog->code[i].b;
+      I.imm = prog->code[i].imm;
+      int pushes = 0, pops = 0, out_t = -1;
+      switch (I.op) {
+        case OP_COL: {
+          int ct = col_type(I.a);
+          if (ct < 0 || !castable(ct, I.type)) return YQ_ERR_INVALID_ARG;
+          pushes = 1; out_t = I.type;
+          break;
+        }
+        case OP_CONST:
+          if (I.imm < 0 || I.imm >= nconsts || !loadable(I.type)) return YQ_ERR_INVALID_ARG;
+          pushes = 1; out_t = I.type;
+          break;
+        case OP_NULL:
+          if (!loadable(I.type)) return YQ_ERR_INVALID_ARG;
+          pushes = 1; out_t = I.type;
+          break;
+        case OP_CAST:
+          if (depth < 1 || types[depth - 1] != I.type || !castable(I.type, I.a)) return YQ_ERR_INVALID_ARG;
+          pops = 1; pushes = 1; out_t = I.a;
+          break;
+        case OP_ARITH:
+          if (depth < 2 || types[depth - 1] != I.type || types[depth - 2] != I.type || !numeric(I.type) || I.a > YQ_MOD)
+            return YQ_ERR_INVALID_ARG;
+          pops = 2; pushes = 1; out_t = I.type;
+          break;
+        case OP_ARITH_COL: {
+          int ct = col_type(I.b);
+          if (depth < 1 || types[depth - 1] != I.type || !numeric(I.type) || ct < 0 || !castable(ct, I.type) || I.a > YQ_MOD)
+            return YQ_ERR_INVALID_ARG;
+          pops = 1; pushes = 1; out_t = I.type;
+          break;
+        }
+        case OP_ARITH_CONST:
+          if (depth < 1 || types[depth - 1] != I.type || !numeric(I.type) || I.imm < 0 || I.imm >= nconsts || I.a > YQ_MOD)
+            return YQ_ERR_INVALID_ARG;
+          pops = 1; pushes = 1; out_t = I.type;
+          break;
+        case OP_CMP:
+          if (depth < 2 || types[depth - 1] != I.type || types[depth - 2] != I.type || !loadable(I.type) || I.a > YQ_NE)
+            return YQ_ERR_INVALID_ARG;
+          pops = 2; pushes = 1; out_t = YQ_BOOL;
+          break;
+        case OP_CMP_COL_CONST:
+        case OP_AND_CMP_COL_CONST: {
+          int ct = col_type(I.b);
+          if (ct < 0 || I.a > YQ_NE) return YQ_ERR_INVALID_ARG;
+          if (ct == YQ_TEXT) {
+            if (I.imm < 0 || I.imm >= ntext) return YQ_ERR_INVALID_ARG;
+            I.type = YQ_TEXT;
+          } else if (!castable(ct, I.type) || I.imm < 0 || I.imm >= nconsts) {
+            return YQ_ERR_INVALID_ARG;
+          }
+          if (I.op == OP_AND_CMP_COL_CONST) {
+            if (depth < 1 || types[depth - 1] != YQ_BOOL) return YQ_ERR_INVALID_ARG;
+            pops = 1;
+          }
+          pushes = 1; out_t = YQ_BOOL;
+          break;
+        }
+        case OP_CMP_COL_COL: {
+          int ct = col_type(I.b), dt = col_type(I.imm);
+          if (ct < 0 || dt < 0 || I.a > YQ_NE) return YQ_ERR_INVALID_ARG;
+          if ((ct == YQ_TEXT) != (dt == YQ_TEXT)) return YQ_ERR_INVALID_ARG;
+          if (ct == YQ_TEXT) I.type = YQ_TEXT;
+          else if (!castable(ct, I.type) || !castable(dt, I.type)) return YQ_ERR_INVALID_ARG;
+          pushes = 1; out_t = YQ_BOOL;
+          break;
+        }
+        case OP_AND:
+        case OP_OR:
+          if (depth < 2 || types[depth - 1] != YQ_BOOL || types[depth - 2] != YQ_BOOL) return YQ_ERR_INVALID_ARG;
+          pops = 2; pushes = 1; out_t = YQ_BOOL;
+          break;
+        case OP_NOT:
+          if (depth < 1 || types[depth - 1] != YQ_BOOL) return YQ_ERR_INVALID_ARG;
+          pops = 1; pushes = 1; out_t = YQ_BOOL;
+          break;
+        case OP_IS_NULL:
+        case OP_IS_NOT_NULL:
+          if (depth < 1) return YQ_ERR_INVALID_ARG;
+          pops = 1; pushes = 1; out_t = YQ_BOOL;
+          break;
+        default: return YQ_ERR_INVALID_ARG;
+      }
+      depth -= pops;
+      if (depth + pushes > 4) return YQ_ERR_UNSUPPORTED;  // deeper than the register stack
+      for (int p = 0; p < pushes; ++p) types[depth++] = out_t;
+      if (len >= kMaxInsns - 1) return YQ_ERR_UNSUPPORTED;
+      P.code[len++] = I;
+      peephole(start);
+    }
+    if (depth != 1) return YQ_ERR_INVALID_ARG;
+    result_type = types[0];
+    return YQ_OK;
+  }
+
+  // Fuse the last instructions of the current program where possible.
+  void peephole(int start) {
+    for (;;) {
+      if (len - start >= 2) {
+        Insn& x = P.code[len - 2];
+        Insn& y = P.code[len - 1];
+        // COL c ; CAST c.type->t   =>  COL c as t (only from the column's own type)
+        if (x.op == OP_COL && y.op == OP_CAST && x.type == y.type && x.type == col_type(x.a)) {
+          x.type = y.a;
+          --len;
+          continue;
+        }
+      }
+      if (len - start >= 3) {
+        Insn& x = P.code[len - 3];
+        Insn& y = P.code[len - 2];
+        Insn& z = P.code[len - 1];
+        // <bool> ; CMP_COL_CONST ; AND  =>  <bool> ; AND_CMP_COL_CONST
+        if (y.op == OP_CMP_COL_CONST && z.op == OP_AND && produces_value(x)) {
+          y.op = OP_AND_CMP_COL_CONST;
+          --len;
+          continue;
+        }
+        // <v> ; COL c ; ARITH op  =>  <v> ; ARITH_COL op c
+        if (y.op == OP_COL && z.op == OP_ARITH && z.type == y.type && produces_value(x)) {
+          Insn f;
+          f.op = OP_ARITH_COL;
+          f.type = z.type;
+          f.a = z.a;
+          f.b = y.a;
+          f.imm = 0;
+          y = f;
+          --len;
+          continue;
+        }
+        // <v> ; CONST k ; ARITH op  =>  <v> ; ARITH_CONST op k
+        if (y.op == OP_CONST && z.op == OP_ARITH && z.type == y.type && produces_value(x)) {
+          Insn f;
+          f.op = OP_ARITH_CONST;
+          f.type = z.type;
+          f.a = z.a;
+          f.b = 0;
+          f.imm = y.imm;
+          y = f;
+          --len;
+          continue;
+        }
+      }
+      break;
+    }
+  }
+  // True when x leaves a value on the stack that the next instruction's
+  // fused form may consume (any non-emit instruction).
+  static bool produces_value(const Insn& x) {
+    uint8_t op = x.op & OP_MASK;
+    return op != OP_EMIT_PRED && op != OP_EMIT_AGG && op != OP_EMIT_PROJ && op != OP_END;
+  }
+
+  int emit(uint8_t op, uint8_t a, uint8_t b, uint8_t type) {
+    if (len >= kMaxInsns) return YQ_ERR_UNSUPPORTED;
+    Insn I;
+    I.op = op; I.a = a; I.b = b; I.type = type; I.imm = 0;
+    P.code[len++] = I;
+    return YQ_OK;
+  }
+
+  // Set the stack-move flags from the depth before each instruction.
+  void finalize() {
+    int depth = 0;
+    for (int i = 0; i < len; ++i) {
+      Insn& I = P.code[i];
+      const uint8_t op = I.op & OP_MASK;
+      I.op = op;
+      switch (op) {
+        case OP_COL:
+        case OP_CONST:
+        case OP_NULL:
+        case OP_CMP_COL_CONST:
+        case OP_CMP_COL_COL:
+          if (depth >= 1) I.op |= OPF_PUSH;
+          ++depth;
+          break;
+        case OP_ARITH:
+        case OP_CMP:
+        case OP_AND:
+        case OP_OR:
+          if (depth >= 3) I.op |= OPF_POPSHIFT;
+          --depth;
+          break;
+        case OP_EMIT_PRED:
+        case OP_EMIT_AGG:
+        case OP_EMIT_PROJ:
+          if (depth >= 2) I.op |= OPF_POPSHIFT;
+          --depth;
+          break;
+        default: break;  // in-place ops keep the depth
+      }
+    }
+  }
+};
+
+}  // namespace yq

@@ -1,0 +1,173 @@
+// Shared device/host plumbing for the yq kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "../../include/yq_ops.h"
+
+namespace yq {
+
+// ------------------------------------------------------------------ errors
+void set_cuda_error(cudaError_t e);
+void count_launch(int n = 1);
+
+#define YQ_TRY_CUDA(expr)                                   \
+  do {                                                      \
+    cudaError_t _e = (expr);                                \
+    if (_e != cudaSuccess) {                                \
+      ::yq::set_cuda_error(_e);                             \
+      return YQ_ERR_CUDA;                                   \
+    }                                                       \
+  } while (0)
+
+#define YQ_TRY(expr)                                        \
+  do {                                                      \
+    int _s = (expr);                                        \
+    if (_s != YQ_OK) return _s;                             \
+  } while (0)
+
+// After a kernel launch: picks up launch-configuration errors.
+#define YQ_CHECK_LAUNCH()                                   \
+  do {                                                      \
+    ::yq::count_launch();                                   \
+    cudaError_t _e = cudaGetLastError();                    \
+    if (_e != cudaSuccess) {                                \
+      ::yq::set_cuda_error(_e);                             \
+      return YQ_ERR_CUDA;                                   \
+    }                                                       \
+  } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int sm_count();
+
+template <typename T>
+__host__ __device__ inline T ceil_div(T a, T b) { return (a + b - 1) / b; }
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Bump allocator over one workspace region. When the caller passes no
+// workspace, `Workspace::acquire` allocates it stream-ordered and the
+// destructor frees it stream-ordered (cudaFreeAsync), so a call never blocks
+// on allocation and the memory returns to the pool after the work it backs.
+struct Workspace {
+  char* base = nullptr;
+  size_t bytes = 0;
+  size_t used = 0;
+  bool owned = false;
+  cudaStream_t stream = nullptr;
+
+  int acquire(void* user, size_t user_bytes, size_t need, cudaStream_t s) {
+    stream = s;
+    if (user) {
+      if (user_bytes < need) return YQ_ERR_INVALID_ARG;
+      base = static_cast<char*>(user);
+      bytes = user_bytes;
+      return YQ_OK;
+    }
+    if (need == 0) return YQ_OK;
+    void* p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, need, s);
+    if (e != cudaSuccess) {
+      set_cuda_error(e);
+      return YQ_ERR_ALLOC;
+    }
+    base = static_cast<char*>(p);
+    bytes = need;
+    owned = true;
+    return YQ_OK;
+  }
+  template <typename T>
+  T* take(size_t count) {
+    size_t off = align_up(used, 256);
+    used = off + count * sizeof(T);
+    return reinterpret_cast<T*>(base + off);
+  }
+  ~Workspace() {
+    if (owned && base) cudaFreeAsync(base, stream);
+  }
+};
+
+// Size helper mirroring Workspace::take's alignment.
+struct WsSize {
+  size_t used = 0;
+  template <typename T>
+  void add(size_t count) { used = align_up(used, 256) + count * sizeof(T); }
+  size_t total() const { return align_up(used, 256) + 256; }
+};
+
+// ---------------------------------------------------------- device helpers
+// Bound on every spin wait: ~2^22 polls with a 64-256 ns back-off is well
+// over a second, far beyond any legitimate wait on a predecessor tile.
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+// Error word layout inside workspaces: bit 0 = a bounded wait ran out,
+// bit 1 = a computed index fell outside its buffer (the access was skipped).
+constexpr uint32_t kErrTimeout = 1u;
+constexpr uint32_t kErrBounds = 2u;
+
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u32(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ uint4 ldg_nc_v4(const void* p) {
+  uint4 v;
+  asm volatile("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p));
+  return v;
+}
+
+// Block-wide exclusive sum over one value per thread (BLOCK threads).
+template <int BLOCK>
+__device__ __forceinline__ uint32_t block_exclusive_sum(uint32_t x, uint32_t* s_warp, uint32_t& total) {
+  constexpr int NW = BLOCK / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t inc = x;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc += y;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < NW ? s_warp[lane] : 0u;
+    uint32_t wi = w;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, wi, d);
+      if (lane >= d) wi += y;
+    }
+    if (lane < NW) s_warp[lane] = wi - w;  // exclusive warp offsets
+    if (lane == NW - 1) s_warp[NW] = wi;   // block total
+  }
+  __syncthreads();
+  uint32_t excl = s_warp[warp] + inc - x;
+  total = s_warp[NW];
+  __syncthreads();
+  return excl;
+}
+
+}  // namespace yq

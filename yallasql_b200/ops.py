@@ -1,0 +1,271 @@
+"""Python entry points over the C ABI, on torch CUDA tensors.
+
+PyTorch supplies device memory and streams only; every operator runs in
+libyq_ops.so. There is no CPU fallback: without the library (or a GPU) these
+functions raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import torch
+
+from . import _abi as A
+from .expr import Aggregate, ConstPool, Expr, compile_expr, Compiled
+
+TORCH_DTYPE = {A.INT32: torch.int32, A.FLOAT32: torch.float32, A.INT64: torch.int64, A.DATETIME: torch.int64,
+               A.FLOAT64: torch.float64, A.BOOL: torch.uint8, A.TEXT: torch.uint8}
+
+
+def lib():
+    return A.load()
+
+
+def _stream(stream=None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+@dataclass
+class DeviceColumn:
+    """One column of a batch in HBM: values plus an optional null-byte array
+    (the reference's Batch::columnData[i] + NullBitSet, include/batch.hpp:21-60)."""
+    data: torch.Tensor
+    type: int
+    nulls: torch.Tensor | None = None
+
+    @property
+    def width(self) -> int:
+        if self.type == A.TEXT:
+            return int(self.data.shape[1])
+        return self.data.element_size()
+
+    @property
+    def rows(self) -> int:
+        return int(self.data.shape[0])
+
+    def c(self) -> A.Column:
+        return A.Column(self.data.data_ptr(), self.nulls.data_ptr() if self.nulls is not None else None,
+                        self.type, self.width)
+
+    @staticmethod
+    def empty(type_: int, rows: int, width: int | None = None, nulls: bool = False, device="cuda"):
+        if type_ == A.TEXT:
+            data = torch.empty((rows, width), dtype=torch.uint8, device=device)
+        else:
+            data = torch.empty(rows, dtype=TORCH_DTYPE[type_], device=device)
+        n = torch.empty(rows, dtype=torch.uint8, device=device) if nulls else None
+        return DeviceColumn(data, type_, n)
+
+    def slice(self, start: int, stop: int) -> "DeviceColumn":
+        return DeviceColumn(self.data[start:stop], self.type, None if self.nulls is None else self.nulls[start:stop])
+
+
+@dataclass
+class DeviceBatch:
+    columns: list
+
+    @property
+    def rows(self) -> int:
+        return self.columns[0].rows if self.columns else 0
+
+    def c(self):
+        arr = (A.Column * max(1, len(self.columns)))(*[c.c() for c in self.columns])
+        b = A.Batch(arr, len(self.columns), self.rows)
+        return b, arr
+
+    def slice(self, start: int, stop: int) -> "DeviceBatch":
+        return DeviceBatch([c.slice(start, stop) for c in self.columns])
+
+
+def _check(st: int, where: str):
+    A.check(st, where)
+
+
+# ----------------------------------------------------------- aggregates
+class AggState:
+    """Device accumulator for a list of aggregates (AggregateExpression's
+    accumlator/counter, include/engine/operators/expressions/aggregate.hpp:20-40)."""
+
+    def __init__(self, aggs: list[Aggregate], stream=None):
+        self.aggs = aggs
+        self.buf = torch.empty(max(256, lib().yq_agg_state_bytes(len(aggs))), dtype=torch.uint8, device="cuda")
+        self._specs = _agg_specs_stub(aggs)
+        _check(lib().yq_agg_state_init(self.buf.data_ptr(), self._specs, len(aggs), _stream(stream)),
+               "yq_agg_state_init")
+
+    def read(self, stream=None) -> list:
+        out = (A.AggResult * max(1, len(self.aggs)))()
+        _check(lib().yq_agg_state_read(self.buf.data_ptr(), self._specs, len(self.aggs), out, _stream(stream)),
+               "yq_agg_state_read")
+        vals = []
+        for a, r in zip(self.aggs, out):
+            if r.is_null:
+                vals.append(None)
+            elif a.kind in (A.AGG_COUNT, A.AGG_COUNT_STAR):
+                vals.append(int(r.i))
+            elif a.kind == A.AGG_AVG or a.input_type in (A.FLOAT32, A.FLOAT64):
+                vals.append(float(r.f))
+            else:
+                vals.append(int(r.i))
+        return vals
+
+
+def _agg_specs_stub(aggs):
+    arr = (A.AggSpec * max(1, len(aggs)))()
+    for i, a in enumerate(aggs):
+        arr[i].kind = a.kind
+        arr[i].input_type = a.input_type
+    return arr
+
+
+class AggPlan:
+    """Compiled predicate + aggregate inputs, reusable across batches."""
+
+    def __init__(self, col_types: list[int], predicate: Expr | None, aggs: list[Aggregate]):
+        self.pool = ConstPool()
+        self.pred = Compiled(compile_expr(predicate, self.pool, col_types) if predicate is not None else [])
+        self.inputs = [Compiled(compile_expr(a.arg, self.pool, col_types) if a.arg is not None else [])
+                       for a in aggs]
+        self.aggs = aggs
+        self.specs = (A.AggSpec * max(1, len(aggs)))()
+        for i, (a, p) in enumerate(zip(aggs, self.inputs)):
+            self.specs[i].kind = a.kind
+            self.specs[i].input_type = a.input_type
+            self.specs[i].input = p.prog
+        self.consts, self._keep = self.pool.to_c()
+
+    def run(self, batch: DeviceBatch, state: AggState, stream=None, workspace: torch.Tensor | None = None):
+        b, keep = batch.c()
+        ws = workspace.data_ptr() if workspace is not None else None
+        wsb = workspace.numel() if workspace is not None else 0
+        _check(lib().yq_filter_aggregate(C.byref(b), C.byref(self.pred.prog), C.byref(self.consts), self.specs,
+                                         len(self.aggs), state.buf.data_ptr(), ws, wsb, _stream(stream)),
+               "yq_filter_aggregate")
+
+
+def filter_aggregate(batch: DeviceBatch, predicate: Expr | None, aggs: list[Aggregate], stream=None) -> list:
+    plan = AggPlan([c.type for c in batch.columns], predicate, aggs)
+    st = AggState(aggs, stream)
+    plan.run(batch, st, stream)
+    return st.read(stream)
+
+
+# ----------------------------------------------------------- projection
+class ProjectPlan:
+    """Compiled WHERE + SELECT list (FilterOperator + ProjectionOperator)."""
+
+    def __init__(self, col_types: list[int], col_widths: list[int], predicate: Expr | None, select: list):
+        self.pool = ConstPool()
+        self.pred = Compiled(compile_expr(predicate, self.pool, col_types) if predicate is not None else [])
+        self.select = select
+        self.progs = []
+        self.proj = (A.Projection * max(1, len(select)))()
+        self.out_types, self.out_widths = [], []
+        for i, s in enumerate(select):
+            if isinstance(s, int):
+                self.proj[i].column = s
+                self.proj[i].out_type = col_types[s]
+                self.out_types.append(col_types[s])
+                self.out_widths.append(col_widths[s])
+                self.progs.append(None)
+            else:
+                p = Compiled(compile_expr(s, self.pool, col_types))
+                self.progs.append(p)
+                self.proj[i].column = -1
+                self.proj[i].out_type = s.type
+                self.proj[i].program = p.prog
+                self.out_types.append(s.type)
+                self.out_widths.append({A.INT32: 4, A.FLOAT32: 4, A.INT64: 8, A.DATETIME: 8, A.FLOAT64: 8,
+                                        A.BOOL: 1}[s.type])
+        self.consts, self._keep = self.pool.to_c()
+
+    def run(self, batch: DeviceBatch, capacity: int | None = None, with_nulls: bool = True, stream=None):
+        cap = batch.rows if capacity is None else capacity
+        outs = [DeviceColumn.empty(t, max(cap, 1), w if t == A.TEXT else None, nulls=with_nulls)
+                for t, w in zip(self.out_types, self.out_widths)]
+        oc = (A.Column * max(1, len(outs)))(*[o.c() for o in outs])
+        b, keep = batch.c()
+        cnt = C.c_uint32(0)
+        st = lib().yq_filter_project(C.byref(b), C.byref(self.pred.prog), C.byref(self.consts), self.proj,
+                                     len(self.select), oc, cap, None, C.byref(cnt), None, 0, _stream(stream))
+        _check(st, "yq_filter_project")
+        n = cnt.value
+        return DeviceBatch([o.slice(0, n) for o in outs])
+
+
+def filter_project(batch: DeviceBatch, predicate: Expr | None, select: list, stream=None) -> DeviceBatch:
+    plan = ProjectPlan([c.type for c in batch.columns], [c.width for c in batch.columns], predicate, select)
+    return plan.run(batch, stream=stream)
+
+
+# ----------------------------------------------------------------- sort
+def sort_config(digit_bits=0, keep_trivial=False):
+    c = A.SortConfig()
+    c.digit_bits = digit_bits
+    c.keep_trivial = 1 if keep_trivial else 0
+    return c
+
+
+def sort_indices(col: DeviceColumn, descending=False, nulls_first=False, config=None, stream=None,
+                 out: torch.Tensor | None = None, workspace: torch.Tensor | None = None) -> torch.Tensor:
+    perm = out if out is not None else torch.empty(col.rows, dtype=torch.int32, device="cuda")
+    cc = col.c()
+    ws = workspace.data_ptr() if workspace is not None else None
+    wsb = workspace.numel() if workspace is not None else 0
+    _check(lib().yq_sort_indices(C.byref(cc), col.rows, int(descending), int(nulls_first), perm.data_ptr(),
+                                 C.byref(config) if config is not None else None, ws, wsb, _stream(stream)),
+           "yq_sort_indices")
+    return perm
+
+
+def sort_indices_multi(cols: list, descending: list, nulls_first: list | None = None, config=None, stream=None):
+    n = cols[0].rows
+    perm = torch.empty(n, dtype=torch.int32, device="cuda")
+    arr = (A.Column * len(cols))(*[c.c() for c in cols])
+    d = (C.c_int32 * len(cols))(*[int(x) for x in descending])
+    nf = (C.c_int32 * len(cols))(*[int(x) for x in (nulls_first or [0] * len(cols))])
+    _check(lib().yq_sort_indices_multi(arr, d, nf, len(cols), n, perm.data_ptr(),
+                                       C.byref(config) if config is not None else None, None, 0, _stream(stream)),
+           "yq_sort_indices_multi")
+    return perm
+
+
+def sort_segments(col: DeviceColumn, seg_offsets: list[int], descending=False, nulls_first=False, config=None,
+                  stream=None, out: torch.Tensor | None = None, workspace: torch.Tensor | None = None):
+    perm = out if out is not None else torch.empty(col.rows, dtype=torch.int32, device="cuda")
+    offs = (C.c_uint32 * len(seg_offsets))(*seg_offsets)
+    cc = col.c()
+    ws = workspace.data_ptr() if workspace is not None else None
+    wsb = workspace.numel() if workspace is not None else 0
+    _check(lib().yq_sort_segments(C.byref(cc), col.rows, offs, len(seg_offsets) - 1, int(descending),
+                                  int(nulls_first), perm.data_ptr(),
+                                  C.byref(config) if config is not None else None, ws, wsb, _stream(stream)),
+           "yq_sort_segments")
+    return perm
+
+
+def sort_workspace_bytes(col: DeviceColumn, seg_offsets: list[int] | None = None) -> int:
+    cc = col.c()
+    if seg_offsets is None:
+        return int(lib().yq_sort_workspace_size(C.byref(cc), col.rows))
+    offs = (C.c_uint32 * len(seg_offsets))(*seg_offsets)
+    return int(lib().yq_sort_segments_workspace_size(C.byref(cc), col.rows, offs, len(seg_offsets) - 1))
+
+
+def gather(batch: DeviceBatch, perm: torch.Tensor, stream=None, out: DeviceBatch | None = None) -> DeviceBatch:
+    n = int(perm.numel())
+    if out is None:
+        out = DeviceBatch([DeviceColumn.empty(c.type, n, c.width if c.type == A.TEXT else None,
+                                              nulls=c.nulls is not None) for c in batch.columns])
+    src = (A.Column * len(batch.columns))(*[c.c() for c in batch.columns])
+    dst = (A.Column * len(out.columns))(*[c.c() for c in out.columns])
+    _check(lib().yq_gather(src, len(batch.columns), perm.data_ptr(), n, dst, _stream(stream)), "yq_gather")
+    return out
+
+
+def sort_batch(batch: DeviceBatch, key: int, descending=False, nulls_first=False, config=None, stream=None):
+    """ORDER BY one key: argsort + gather every column (OrderOperator for one run)."""
+    perm = sort_indices(batch.columns[key], descending, nulls_first, config, stream)
+    return gather(batch, perm, stream)
