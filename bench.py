@@ -1,0 +1,365 @@
+#!/usr/bin/env python3
+"""Benchmark of the ORDER BY operator on the 64M-row table (B200).
+
+Workload (one step): over a 64,000,000-row table {key f32 uniform [-1e6, 1e6),
+id int64, txt 16-byte text, d date} (seed 1), run
+  ORDER BY key DESC   and then   ORDER BY d ASC,
+each producing the fully sorted table (all four columns). With --mode
+outofcore (default) each query is the reference's out-of-core plan: the
+table arrives as 4 MB batches (116,480 rows at 36 B/row), every batch is
+sorted into a run, and runs are merged pairwise by merge path until one run
+remains. --mode incore sorts the whole table at once. Metric: rows/s (rows
+sorted per second, both queries), plus the HBM roofline of the dominant kernel.
+
+`python bench.py --gpus N --steps K --warmup W [--impl reference]`; for N>1
+launch under torch.distributed.run: every rank sorts its own table (replicas,
+weak scaling), time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "operator rows/s & %HBM peak; query p50/p99 ms, batched vs plain, 1xB200"
+UNIT = "rows/s"
+ROW_BYTES = 4 + 8 + 16 + 8  # key, id, txt, d
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="yq", choices=["yq", "reference"])
+    p.add_argument("--rows", type=int, default=64_000_000)
+    p.add_argument("--dist", default="uniform", choices=["uniform", "zipf", "equal"])
+    p.add_argument("--mode", default="outofcore", choices=["outofcore", "incore"])
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def committed_traffic() -> dict:
+    """Per-launch DRAM bytes of the profiled kernels, from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+# ---------------------------------------------------------------- workload
+def make_table(rows: int, dist: str):
+    from yallasql_b200 import datagen
+    return datagen.order_table(rows, seed=1, dist=dist)
+
+
+class OrderByJob:
+    """Both ORDER BY queries over one device-resident table."""
+
+    def __init__(self, t: dict, mode: str):
+        import torch
+        from yallasql_b200 import _abi as A, datagen
+        from yallasql_b200.ops import DeviceBatch, DeviceColumn
+        self.torch = torch
+        self.A = A
+        self.rows = int(t["key"].shape[0])
+        self.mode = mode
+        dev = lambda a, ty: DeviceColumn(torch.from_numpy(a).cuda(), ty)
+        self.table = DeviceBatch([dev(t["key"], A.FLOAT32), dev(t["id"], A.INT64), dev(t["txt"], A.TEXT),
+                                  dev(t["d"], A.DATETIME)])
+        self.batch_rows = datagen.batch_row_counts(self.rows, ROW_BYTES)
+        self.offsets = [0]
+        for c in self.batch_rows:
+            self.offsets.append(self.offsets[-1] + c)
+        self.out = [DeviceBatch([DeviceColumn.empty(c.type, self.rows, c.width if c.type == A.TEXT else None)
+                                 for c in self.table.columns]) for _ in range(2)]
+        self.tmp = DeviceBatch([DeviceColumn.empty(c.type, self.rows, c.width if c.type == A.TEXT else None)
+                                for c in self.table.columns])
+        self.scratch = DeviceBatch([DeviceColumn.empty(c.type, self.rows, c.width if c.type == A.TEXT else None)
+                                    for c in self.table.columns])
+        self.perm = torch.empty(self.rows, dtype=torch.int32, device="cuda")
+        from yallasql_b200 import ops
+        self.ops = ops
+        ws = max(ops.sort_workspace_bytes(self.table.columns[0], self.offsets),
+                 ops.sort_workspace_bytes(self.table.columns[3], self.offsets),
+                 ops.sort_workspace_bytes(self.table.columns[0]), ops.sort_workspace_bytes(self.table.columns[3]))
+        self.ws = torch.empty(ws, dtype=torch.uint8, device="cuda")
+
+    def query(self, src, key: int, desc: bool, out):
+        ops = self.ops
+        if self.mode == "incore":
+            ops.sort_indices(src.columns[key], desc, out=self.perm, workspace=self.ws)
+            ops.gather(src, self.perm, out=out)
+            return out
+        # out-of-core: sort every 4 MB batch into a run, then merge runs pairwise
+        ops.sort_segments(src.columns[key], self.offsets, desc, out=self.perm, workspace=self.ws)
+        ops.gather(src, self.perm, out=self.tmp)
+        return ops.merge_runs(self.tmp, key, desc, self.offsets, out, scratch=self.scratch)
+
+    def step(self, src=None):
+        src = self.table if src is None else src
+        a = self.query(src, 0, True, self.out[0])
+        b = self.query(src, 3, False, self.out[1])
+        return a, b
+
+
+def run_reference(args, rank: int):
+    """Reference arm: the CPU port of the operator (oracle/ stable ORDER BY +
+    row gather), all host threads, a bounded sample per step."""
+    import oracle
+    threads = os.cpu_count() or 1
+    sample = min(args.rows, 8_000_000)
+    t = make_table(sample, args.dist)
+
+    def one():
+        for key, desc in (("key", True), ("d", False)):
+            perm = oracle.sort_perm(t[key], desc=desc, threads=threads,
+                                    type_=oracle.DATETIME if key == "d" else None)
+            for name in ("key", "id", "txt", "d"):
+                np.take(t[name], perm, axis=0)
+
+    for _ in range(args.warmup):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one()
+    dt = (time.perf_counter() - t0) / args.steps
+    value = 2 * sample / dt
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 keys, int64/text/date payload",
+            "data": "synthetic", "config": config(args),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"first {sample} rows of the table, both ORDER BY queries per step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def config(args) -> dict:
+    return {"workload": f"ORDER BY key DESC then ORDER BY d ASC on a {args.rows}-row table (key f32 {args.dist}, "
+                        f"id int64, txt 16-byte, d date; seed 1), {args.mode}"
+                        + (" as 4 MB batches sorted then merge-path merged" if args.mode == "outofcore" else ""),
+            "rows": args.rows, "row_bytes": ROW_BYTES, "key_distribution": args.dist, "mode": args.mode,
+            "l2": "inputs larger than L2 (64M rows x 36 B = 2.3 GB per table)", "parallelism": f"replicas x{args.gpus}"}
+
+
+def cpu_baseline(args, t: dict) -> dict:
+    import oracle
+    threads = os.cpu_count() or 1
+    sample = min(args.rows, 8_000_000)
+    sub = {k: v[:sample] for k, v in t.items()}
+    t0 = time.perf_counter()
+    for key, desc in (("key", True), ("d", False)):
+        perm = oracle.sort_perm(sub[key], desc=desc, threads=threads, type_=oracle.DATETIME if key == "d" else None)
+        for name in ("key", "id", "txt", "d"):
+            np.take(sub[name], perm, axis=0)
+    dt = time.perf_counter() - t0
+    return {"value": 2 * sample / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {sample} of {args.rows} rows, both ORDER BY queries (stable sort + gather of 4 columns)"}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from yallasql_b200 import _abi as A
+    lib = A.load()
+    t = make_table(args.rows, args.dist)
+    job = OrderByJob(t, args.mode)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        job.step()
+    barrier()
+    launches0 = lib.yq_launch_count()
+    lib.yq_profile_enable(1)
+    lib.yq_profile_read(None, 0, 1)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        s.record()
+        for _ in range(args.steps):
+            job.step()
+        e.record()
+        torch.cuda.synchronize()
+    lib.yq_profile_enable(0)
+    buf = C.create_string_buffer(1 << 16)
+    lib.yq_profile_read(buf, len(buf), 1)
+    prof = json.loads(buf.value.decode() or "{}")
+    launches = int(lib.yq_launch_count() - launches0)
+    ms = s.elapsed_time(e) / args.steps
+    if dist is not None:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    rows_per_step = 2 * args.rows
+    value = world * rows_per_step / (ms / 1e3)
+
+    # parity spot check of this run (cheap, on device): outputs ordered
+    a, b = job.step()
+    ok = bool((a.columns[0].data[:-1] >= a.columns[0].data[1:]).all()) and \
+        bool((b.columns[3].data[:-1] <= b.columns[3].data[1:]).all())
+
+    # end to end: pinned host table -> device -> both queries -> host (every step)
+    e2e = None
+    if not args.no_e2e:
+        pin = {k: torch.from_numpy(v).pin_memory() for k, v in t.items()}
+        outs = [{k: torch.empty_like(v).pin_memory() for k, v in pin.items()} for _ in range(2)]
+        names = ("key", "id", "txt", "d")
+        stage = job.table  # the device table is refilled from host memory every step
+        def e2e_step():
+            for c, n in zip(stage.columns, names):
+                c.data.copy_(pin[n], non_blocking=True)
+            ra, rb = job.step(stage)
+            for r, o in ((ra, outs[0]), (rb, outs[1])):
+                for c, n in zip(r.columns, names):
+                    o[n].copy_(c.data, non_blocking=True)
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_step()
+        barrier()
+        s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s2.record()
+        for _ in range(args.steps):
+            e2e_step()
+        e2.record()
+        torch.cuda.synchronize()
+        ms2 = s2.elapsed_time(e2) / args.steps
+        if dist is not None:
+            tt = torch.tensor([ms2], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms2 = float(tt.item())
+        tab_bytes = sum(v.nbytes for v in t.values())
+        e2e = {"value": world * rows_per_step / (ms2 / 1e3), "unit": UNIT, "h2d_bytes_per_step": tab_bytes,
+               "d2h_bytes_per_step": 2 * tab_bytes, "ms_per_step": ms2,
+               "path": "pinned host columns -> cudaMemcpyAsync -> C-ABI operators -> pinned host, every step"}
+
+    peak, peak_kind = peaks()
+    roof = None
+    if prof:
+        dom = max(prof.items(), key=lambda kv: kv[1]["ms"])
+        name, d = dom
+        per_launch_bytes = d["units"] / max(1, d["launches"])
+        per_launch_ms = d["ms"] / max(1, d["launches"])
+        achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
+        tr = committed_traffic().get(name, {})
+        traffic = None
+        if tr.get("dram_bytes_per_unit_row") is not None and tr.get("rows_per_launch_units"):
+            traffic = tr["dram_bytes_per_unit_row"] * per_launch_bytes / tr["rows_per_launch_units"]
+        roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback 6650 GB/s",
+                "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes,
+                "avg_launch_ms": round(per_launch_ms, 4)}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 keys, int64/text/date payload", "data": "synthetic",
+            "config": config(args), "roofline": roof, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk.summary(), "kernels": prof, "sorted_ok": ok}
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(args, t)
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -434,6 +434,13 @@ int yq_cross_product_col(const yq_column* col, uint32_t left_rows, uint32_t righ
 int yq_device_sm_count(void);
 /* Kernel launches issued by this library on this process (for accounting). */
 uint64_t yq_launch_count(void);
+/* Device timing of the library's own launches: when enabled, every kernel
+ * launch records a CUDA event pair on its stream, tagged with the kernel and
+ * its algorithmic bytes. yq_profile_read synchronises on the recorded events
+ * and writes a JSON object {tag: {launches, ms, units}} (units = bytes);
+ * returns the JSON length. */
+int yq_profile_enable(int32_t on);
+int yq_profile_read(char* out, size_t cap, int32_t reset);
 
 #ifdef __cplusplus
 }

@@ -136,6 +136,8 @@ PROTOTYPES = {
     "yq_cross_product_col": (C.c_int, [P(Column), u32, u32, i32, P(Column), vp]),
     "yq_device_sm_count": (C.c_int, []),
     "yq_launch_count": (u64, []),
+    "yq_profile_enable": (C.c_int, [i32]),
+    "yq_profile_read": (C.c_int, [C.c_char_p, sz, i32]),
 }
 
 

@@ -121,6 +121,26 @@ __global__ void __launch_bounds__(kRowBlock) k_filter_aggregate(const __grid_con
   if (threadIdx.x == 0) *ticket = 0u;
 }
 
+// Bytes per row of every input column a program references (plus null bytes).
+static double referenced_row_bytes(const VmProgram& P, int len) {
+  bool used[YQ_MAX_BATCH_COLUMNS] = {false};
+  for (int i = 0; i < len; ++i) {
+    const Insn& I = P.code[i];
+    switch (I.op & OP_MASK) {
+      case OP_COL: used[I.a] = true; break;
+      case OP_ARITH_COL:
+      case OP_CMP_COL_CONST:
+      case OP_AND_CMP_COL_CONST: used[I.b] = true; break;
+      case OP_CMP_COL_COL: used[I.b] = true; used[I.imm] = true; break;
+      default: break;
+    }
+  }
+  double b = 0;
+  for (int c = 0; c < P.ncols; ++c)
+    if (used[c]) b += P.cols[c].width + (P.cols[c].nulls ? 1 : 0);
+  return b;
+}
+
 static int occupancy_grid(const void* kernel, int block, size_t smem) {
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess || per_sm < 1)
@@ -176,6 +196,7 @@ static int build_agg_program(ProgramBuilder& B, const yq_program* predicate, con
 
 int launch_filter_aggregate(const FAParams& F, uint32_t rows, Acc* partials, uint32_t* ticket, Acc* state, int grid,
                             cudaStream_t s) {
+  ProfScope ps("filter_aggregate", s, (double)rows * referenced_row_bytes(F.P, F.pc_end));
   k_filter_aggregate<<<grid, kRowBlock, 0, s>>>(F, rows, partials, ticket, state);
   YQ_CHECK_LAUNCH();
   return YQ_OK;
@@ -471,8 +492,13 @@ int yq_filter_project(const yq_batch* batch, const yq_program* predicate, const 
   YQ_TRY_CUDA(cudaMemsetAsync(status, 0, ((size_t)ntiles + 1) * sizeof(unsigned long long), s));
   YQ_TRY_CUDA(cudaMemsetAsync(misc, 0, 4 * sizeof(uint32_t), s));
   uint32_t* cnt_dev = count_device ? count_device : misc + 2;
-  k_filter_project<<<ntiles, kRowBlock, 0, s>>>(F, rows, misc, status, cnt_dev, misc + 1);
-  YQ_CHECK_LAUNCH();
+  {
+    // algorithmic bytes: referenced input columns (outputs depend on selectivity)
+    const double in_b = referenced_row_bytes(F.P, F.proj_end);
+    ProfScope ps("filter_project", s, (double)rows * in_b);
+    k_filter_project<<<ntiles, kRowBlock, 0, s>>>(F, rows, misc, status, cnt_dev, misc + 1);
+    YQ_CHECK_LAUNCH();
+  }
   if (count_host) {
     uint32_t h[2];
     YQ_TRY_CUDA(cudaMemcpyAsync(&h[0], cnt_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));

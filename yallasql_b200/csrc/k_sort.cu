@@ -19,7 +19,7 @@
 // launches. A single global sort is the one-segment case.
 #include <string.h>
 #include <vector>
-#include "yq_common.cuh"
+#include "yq_keys.cuh"
 
 namespace yq {
 
@@ -29,88 +29,11 @@ constexpr uint32_t kStatIncl = 2u << 30;
 constexpr uint32_t kStatMask = (1u << 30) - 1u;
 constexpr uint32_t kMaxSortRows = (1u << 30) - 1u;
 
-// Where the first pass of a key reads its keys from.
-struct KeySrc {
-  const char* data;
-  const uint8_t* nulls;
-  const uint32_t* in_perm;  // multi-key: this key's row for element e is in_perm[e]
-  int32_t type;
-  int32_t width;
-  int32_t vwords;       // value words in the key (excluding the null word)
-  int32_t desc;
-  int32_t nulls_first;
-  int32_t null_word;    // 1: word `vwords` is the null flag
-};
-
 struct SegInfo {
   const uint32_t* seg_start;   // nseg + 1 row offsets
   const uint32_t* tile_start;  // nseg + 1 tile offsets
   int32_t nseg;
 };
-
-__device__ __forceinline__ uint32_t bswap(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
-
-// Order-preserving unsigned key words of one row (word 0 least significant).
-template <int KW>
-__device__ __forceinline__ void make_key(const KeySrc& s, uint32_t row, uint32_t (&k)[KW]) {
-#pragma unroll
-  for (int j = 0; j < KW; ++j) k[j] = 0u;
-  const bool is_null = s.nulls && s.nulls[row];
-  if (!is_null) {
-    switch (s.type) {
-      case YQ_INT32: {
-        k[0] = __ldg(reinterpret_cast<const uint32_t*>(s.data) + row) ^ 0x80000000u;
-        break;
-      }
-      case YQ_FLOAT32: {
-        uint32_t b = __ldg(reinterpret_cast<const uint32_t*>(s.data) + row);
-        if ((b & 0x7fffffffu) == 0u) b = 0u;                          // -0.0 ties with +0.0
-        else if ((b & 0x7f800000u) == 0x7f800000u && (b & 0x007fffffu)) b = 0x7fc00000u;  // NaN above +inf
-        k[0] = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-        break;
-      }
-      case YQ_INT64:
-      case YQ_DATETIME: {
-        unsigned long long v = __ldg(reinterpret_cast<const unsigned long long*>(s.data) + row);
-        k[0] = (uint32_t)v;
-        if (KW > 1) k[KW > 1 ? 1 : 0] = (uint32_t)(v >> 32) ^ 0x80000000u;
-        break;
-      }
-      case YQ_FLOAT64: {
-        unsigned long long b = __ldg(reinterpret_cast<const unsigned long long*>(s.data) + row);
-        if ((b & 0x7fffffffffffffffull) == 0ull) b = 0ull;
-        else if ((b & 0x7ff0000000000000ull) == 0x7ff0000000000000ull && (b & 0x000fffffffffffffull))
-          b = 0x7ff8000000000000ull;
-        b = (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
-        k[0] = (uint32_t)b;
-        if (KW > 1) k[KW > 1 ? 1 : 0] = (uint32_t)(b >> 32);
-        break;
-      }
-      case YQ_BOOL: {
-        k[0] = (uint32_t)(s.data[row] != 0);
-        break;
-      }
-      default: {  // TEXT: the first vwords words of the slot as a big-endian integer
-        const uint32_t* p = reinterpret_cast<const uint32_t*>(s.data + (size_t)row * s.width);
-#pragma unroll
-        for (int j = 0; j < KW; ++j)
-          if (j < s.vwords) k[j] = bswap(__ldg(p + (s.vwords - 1 - j)));
-        break;
-      }
-    }
-    if (s.desc) {
-#pragma unroll
-      for (int j = 0; j < KW; ++j)
-        if (j < s.vwords) k[j] = ~k[j];
-    }
-  }
-  if (s.null_word) {
-    const uint32_t nv = s.nulls_first ? (is_null ? 0u : 1u) : (is_null ? 1u : 0u);
-#pragma unroll
-    for (int j = 0; j < KW; ++j)
-      if (j == s.vwords) k[j] = nv;
-  }
-}
 
 template <int KW, int D>
 __device__ __forceinline__ uint32_t digit_of(const uint32_t (&k)[KW], int shift) {
@@ -736,7 +659,11 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
     seg.seg_start = d_seg;
     seg.tile_start = d_tiles;
     seg.nseg = nseg;
-    YQ_TRY(kp.K.hist(src, seg, kp.tile_rows, sp.ntiles, d_hist, s));
+    {
+      // algorithmic bytes: each key read once (+ the incoming permutation)
+      ProfScope ps("sort_histogram", s, (double)rows * (c.width + (perm_in ? 4 : 0)));
+      YQ_TRY(kp.K.hist(src, seg, kp.tile_rows, sp.ntiles, d_hist, s));
+    }
 
     std::vector<int> passes;
     if (keep_trivial) {
@@ -778,6 +705,12 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
       Sp.err = d_err;
       Sp.pass = passes[i];
       Sp.npass = kp.P;
+      // algorithmic bytes: keys + row ids in, keys + row ids out (the first
+      // pass reads the raw key (+ incoming permutation), the last writes ids only)
+      const double kb = 4.0 * kp.sh.kw;
+      const double in_b = first ? (double)c.width + (perm_in ? 4.0 : 0.0) : kb + 4.0;
+      const double out_b = last ? 4.0 : kb + 4.0;
+      ProfScope ps("sort_onesweep", s, (double)rows * (in_b + out_b));
       YQ_TRY(kp.K.sweep(Sp, sp.ntiles, s));
     }
     perm_in = dst_perm;
@@ -877,6 +810,9 @@ int yq_gather(const yq_column* in, int32_t ncols, const uint32_t* perm, uint32_t
   int grid = (int)ceil_div<uint32_t>(rows, 256);
   const int cap = sm_count() * 16;
   if (grid > cap) grid = cap;
+  double row_bytes = 4.0;  // permutation
+  for (int c = 0; c < ncols; ++c) row_bytes += 2.0 * in[c].width + (out[c].nulls ? 2.0 : 0.0);
+  ProfScope ps("gather", s, (double)rows * row_bytes);
   k_gather<<<grid, 256, 0, s>>>(G, perm, rows);
   YQ_CHECK_LAUNCH();
   return YQ_OK;

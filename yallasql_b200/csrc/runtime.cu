@@ -1,5 +1,11 @@
 // Library runtime: error bookkeeping, launch accounting, device queries.
 #include <atomic>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+#include <stdio.h>
+#include <string.h>
 #include "yq_common.cuh"
 
 namespace yq {
@@ -9,6 +15,52 @@ static std::atomic<unsigned long long> g_launches{0};
 
 void set_cuda_error(cudaError_t e) { g_last_cuda_error = (int)e; }
 void count_launch(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+
+// ---------------------------------------------------------------- profiler
+namespace {
+struct ProfRec {
+  std::string tag;
+  cudaEvent_t a, b;
+  double units;
+};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRec> g_prof;            // open and closed records, in launch order
+std::vector<size_t> g_prof_open;        // indices of records awaiting prof_end (nested scopes)
+std::vector<cudaEvent_t> g_event_pool;
+
+cudaEvent_t take_event() {
+  if (!g_event_pool.empty()) {
+    cudaEvent_t e = g_event_pool.back();
+    g_event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+}  // namespace
+
+void prof_begin(const char* tag, cudaStream_t s, double units) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  if (!g_prof_on) return;
+  ProfRec r;
+  r.tag = tag;
+  r.units = units;
+  r.a = take_event();
+  r.b = take_event();
+  cudaEventRecord(r.a, s);
+  g_prof_open.push_back(g_prof.size());
+  g_prof.push_back(r);
+}
+
+void prof_end(cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  if (!g_prof_on || g_prof_open.empty()) return;
+  ProfRec& r = g_prof[g_prof_open.back()];
+  g_prof_open.pop_back();
+  cudaEventRecord(r.b, s);
+}
 
 int sm_count() {
   static int cached[64] = {0};
@@ -43,5 +95,52 @@ int yq_last_cuda_error(void) { return yq::g_last_cuda_error; }
 int yq_abi_version(void) { return YQ_ABI_VERSION; }
 int yq_device_sm_count(void) { return yq::sm_count(); }
 uint64_t yq_launch_count(void) { return yq::g_launches.load(std::memory_order_relaxed); }
+
+int yq_profile_enable(int32_t on) {
+  std::lock_guard<std::mutex> lk(yq::g_prof_mu);
+  yq::g_prof_on = on != 0;
+  return YQ_OK;
+}
+
+int yq_profile_read(char* out, size_t cap, int32_t reset) {
+  // Synchronises on every recorded event, then reports per tag: launches,
+  // total device milliseconds and total work units (as tagged by the caller).
+  std::lock_guard<std::mutex> lk(yq::g_prof_mu);
+  struct Agg { long n = 0; double ms = 0, units = 0; };
+  std::map<std::string, Agg> agg;
+  for (auto& r : yq::g_prof) {
+    if (cudaEventSynchronize(r.b) != cudaSuccess) continue;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) continue;
+    Agg& a = agg[r.tag];
+    a.n += 1;
+    a.ms += ms;
+    a.units += r.units;
+  }
+  std::string js = "{";
+  bool first = true;
+  for (auto& kv : agg) {
+    char buf[512];
+    snprintf(buf, sizeof(buf), "%s\"%s\": {\"launches\": %ld, \"ms\": %.6f, \"units\": %.1f}", first ? "" : ", ",
+             kv.first.c_str(), kv.second.n, kv.second.ms, kv.second.units);
+    js += buf;
+    first = false;
+  }
+  js += "}";
+  if (reset) {
+    for (auto& r : yq::g_prof) {
+      yq::g_event_pool.push_back(r.a);
+      yq::g_event_pool.push_back(r.b);
+    }
+    yq::g_prof.clear();
+    yq::g_prof_open.clear();
+  }
+  if (out && cap > 0) {
+    size_t n = js.size() < cap - 1 ? js.size() : cap - 1;
+    memcpy(out, js.data(), n);
+    out[n] = 0;
+  }
+  return (int)js.size();
+}
 
 }  // extern "C"

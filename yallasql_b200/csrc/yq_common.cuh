@@ -13,6 +13,16 @@ namespace yq {
 void set_cuda_error(cudaError_t e);
 void count_launch(int n = 1);
 
+// Optional per-kernel device timing (yq_profile_enable): records a CUDA
+// event pair on the launch stream around each tagged launch.
+void prof_begin(const char* tag, cudaStream_t s, double units);
+void prof_end(cudaStream_t s);
+struct ProfScope {
+  cudaStream_t s;
+  ProfScope(const char* tag, cudaStream_t st, double units = 0.0) : s(st) { prof_begin(tag, st, units); }
+  ~ProfScope() { prof_end(s); }
+};
+
 #define YQ_TRY_CUDA(expr)                                   \
   do {                                                      \
     cudaError_t _e = (expr);                                \

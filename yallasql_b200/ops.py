@@ -269,3 +269,44 @@ def sort_batch(batch: DeviceBatch, key: int, descending=False, nulls_first=False
     """ORDER BY one key: argsort + gather every column (OrderOperator for one run)."""
     perm = sort_indices(batch.columns[key], descending, nulls_first, config, stream)
     return gather(batch, perm, stream)
+
+
+# ---------------------------------------------------------------- merge
+def merge_pass(src: DeviceBatch, key: int, descending: bool, offsets: list[int], dst: DeviceBatch,
+               nulls_first=False, stream=None) -> list[int]:
+    """Merge runs (0,1), (2,3), ... of `src` into `dst`; returns the new run offsets."""
+    offs = (C.c_uint32 * len(offsets))(*offsets)
+    sc = (A.Column * len(src.columns))(*[c.c() for c in src.columns])
+    dc = (A.Column * len(dst.columns))(*[c.c() for c in dst.columns])
+    _check(lib().yq_merge_pass(sc, len(src.columns), key, int(descending), int(nulls_first), offs,
+                               len(offsets) - 1, dc, None, 0, _stream(stream)), "yq_merge_pass")
+    return [offsets[i] for i in range(0, len(offsets) - 1, 2)] + [offsets[-1]]
+
+
+def merge_runs(runs: DeviceBatch, key: int, descending: bool, offsets: list[int], out: DeviceBatch,
+               scratch: DeviceBatch | None = None, nulls_first=False, stream=None) -> DeviceBatch:
+    """Merge sorted runs pairwise, level by level, until one run remains
+    (OrderOperator::merge_all_sorted, include/engine/operators/order_operator.hpp:160-193).
+    The final level writes into `out`; `runs` and `scratch` are clobbered."""
+    nruns = len(offsets) - 1
+    levels = 0
+    while (nruns + (1 << levels) - 1) >> levels > 1:
+        levels += 1
+    if levels == 0:
+        if runs is not out:
+            for a, b in zip(runs.columns, out.columns):
+                b.data.copy_(a.data)
+                if b.nulls is not None and a.nulls is not None:
+                    b.nulls.copy_(a.nulls)
+        return out
+    if scratch is None:
+        scratch = DeviceBatch([DeviceColumn.empty(c.type, c.rows, c.width if c.type == A.TEXT else None,
+                                                  nulls=c.nulls is not None) for c in runs.columns])
+    # alternate so that the last level lands in `out`
+    bufs = [out, scratch] if levels % 2 == 1 else [scratch, out]
+    src = runs
+    for lvl in range(levels):
+        dst = bufs[lvl % 2]
+        offsets = merge_pass(src, key, descending, offsets, dst, nulls_first, stream)
+        src = dst
+    return out
