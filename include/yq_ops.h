@@ -235,6 +235,27 @@ int yq_filter_project(const yq_batch* batch, const yq_program* predicate,
                       uint32_t* count_device, uint32_t* count_host, void* workspace,
                       size_t workspace_bytes, void* stream);
 
+/* ---- WHERE + projection that allocates nothing.
+ * No counterpart in the reference: it exists for hosts that must not allocate
+ * device memory inside the call — an engine that embeds this library and owns
+ * every byte of device memory through its own fixed arena, or a serving loop
+ * whose latency budget cannot absorb allocator calls and the synchronisation
+ * they may bring. Same contract as yq_filter_project, except that the
+ * look-back scratch is a static device array compiled into libyq_ops.so
+ * (about 512 KiB, held by every GPU that loads the library until the process
+ * exits), so batches are limited to YQ_FILTER_PROJECT_NOALLOC_MAX_ROWS rows;
+ * larger batches are rejected with YQ_ERR_INVALID_ARG before any device work.
+ * The first call on a device looks up that array's device address (once per
+ * device, under a lock); make that first call before any stream capture.
+ * Every call shares the one array and clears the part it uses on `stream`, so
+ * calls whose kernels overlap on the GPU (different streams, no ordering
+ * between them) race and must not be issued. */
+#define YQ_FILTER_PROJECT_NOALLOC_MAX_ROWS (1u << 26)
+int yq_filter_project_noalloc(const yq_batch* batch, const yq_program* predicate,
+                              const yq_constants* constants, const yq_projection* proj,
+                              int32_t nproj, yq_column* out, uint32_t capacity,
+                              uint32_t* count_device, uint32_t* count_host, void* stream);
+
 /* ---- ORDER BY: stable LSD radix argsort.
  * Replaces BoundRefSortExpression + launch_radix_sort + move_rows_batch
  * (include/engine/operators/expressions/bound_ref_sort.hpp:26-64,

@@ -105,6 +105,8 @@ PROTOTYPES = {
     "yq_filter_project_workspace_size": (sz, [u32]),
     "yq_filter_project": (C.c_int, [P(Batch), P(Program), P(Constants), P(Projection), i32, P(Column), u32,
                                     P(u32), P(u32), vp, sz, vp]),
+    "yq_filter_project_noalloc": (C.c_int, [P(Batch), P(Program), P(Constants), P(Projection), i32, P(Column), u32,
+                                            P(u32), P(u32), vp]),
     "yq_sort_workspace_size": (sz, [P(Column), u32]),
     "yq_sort_indices": (C.c_int, [P(Column), u32, i32, i32, vp, P(SortConfig), vp, sz, vp]),
     "yq_sort_indices_multi": (C.c_int, [P(Column), P(i32), P(i32), i32, u32, vp, P(SortConfig), vp, sz, vp]),

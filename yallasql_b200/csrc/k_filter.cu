@@ -512,3 +512,121 @@ int yq_filter_project(const yq_batch* batch, const yq_program* predicate, const 
 }
 
 }  // extern "C"
+
+// =================================================== allocation-free variant
+// yq_filter_project_noalloc runs the same kernel as yq_filter_project, but its
+// look-back scratch is this file-scope device array instead of a workspace
+// the caller passes or the library allocates. Layout: four 32-bit counters
+// (tile counter, error word, row count, spare), then one 64-bit look-back
+// status word per 1,024-row tile plus one.
+#include <mutex>
+
+namespace yq {
+
+constexpr uint32_t kNoAllocTiles = YQ_FILTER_PROJECT_NOALLOC_MAX_ROWS / kRowTile;
+constexpr size_t kNoAllocWords = 2 + (size_t)kNoAllocTiles + 1;  // 2 words hold the four counters
+
+static __device__ __align__(256) unsigned long long g_filter_project_scratch[kNoAllocWords];
+
+// Device address of the scratch array, looked up once per device with that
+// device current (host code only sees a host-side stand-in for the symbol).
+static int noalloc_scratch(unsigned long long** out) {
+  static std::mutex mu;
+  static void* addr[64] = {nullptr};
+  int dev = 0;
+  YQ_TRY_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return YQ_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_filter_project_scratch);
+    if (e != cudaSuccess || !p) {
+      set_cuda_error(e);
+      return YQ_ERR_CUDA;
+    }
+    addr[dev] = p;
+  }
+  *out = static_cast<unsigned long long*>(addr[dev]);
+  return YQ_OK;
+}
+
+// Same validation and program build as yq_filter_project.
+static int build_project_params(const yq_batch* batch, const yq_program* predicate, const yq_constants* constants,
+                                const yq_projection* proj, int32_t nproj, yq_column* out, uint32_t capacity,
+                                FPParams& F) {
+  if (!batch || nproj < 0 || nproj > YQ_MAX_PROJECTIONS || (nproj > 0 && (!proj || !out))) return YQ_ERR_INVALID_ARG;
+  ProgramBuilder B;
+  YQ_TRY(B.set_columns(batch->columns, batch->ncols));
+  YQ_TRY(B.set_constants(constants));
+  if (predicate && predicate->len > 0) {
+    int t = -1;
+    YQ_TRY(B.append(predicate, t));
+    if (t != YQ_BOOL) return YQ_ERR_INVALID_ARG;
+    YQ_TRY(B.emit(OP_EMIT_PRED, 0, 0, YQ_BOOL));
+  }
+  F.pred_end = B.len;
+  for (int p = 0; p < nproj; ++p) {
+    DevOut& o = F.out[p];
+    o.data = static_cast<char*>(out[p].data);
+    o.nulls = const_cast<uint8_t*>(out[p].nulls);
+    o.src_col = proj[p].column;
+    if (!o.data && capacity > 0) return YQ_ERR_INVALID_ARG;
+    if (proj[p].column >= 0) {
+      if (proj[p].column >= batch->ncols) return YQ_ERR_INVALID_ARG;
+      const yq_column& c = batch->columns[proj[p].column];
+      if (out[p].type != c.type || out[p].width != c.width) return YQ_ERR_INVALID_ARG;
+      o.width = c.width;
+    } else {
+      int t = -1;
+      YQ_TRY(B.append(&proj[p].program, t));
+      if (t != proj[p].out_type || t != out[p].type || !ProgramBuilder::valid_column(out[p])) return YQ_ERR_INVALID_ARG;
+      o.width = out[p].width;
+      YQ_TRY(B.emit(OP_EMIT_PROJ, (uint8_t)p, 0, (uint8_t)t));
+    }
+  }
+  B.finalize();
+  memcpy(&F.P, &B.P, sizeof(VmProgram));
+  F.proj_end = B.len;
+  F.nproj = nproj;
+  F.capacity = capacity;
+  return YQ_OK;
+}
+
+}  // namespace yq
+
+extern "C" int yq_filter_project_noalloc(const yq_batch* batch, const yq_program* predicate,
+                                         const yq_constants* constants, const yq_projection* proj, int32_t nproj,
+                                         yq_column* out, uint32_t capacity, uint32_t* count_device,
+                                         uint32_t* count_host, void* stream) {
+  if (!batch) return YQ_ERR_INVALID_ARG;
+  if (batch->rows > YQ_FILTER_PROJECT_NOALLOC_MAX_ROWS) return YQ_ERR_INVALID_ARG;  // scratch holds no more tiles
+  FPParams F;
+  YQ_TRY(build_project_params(batch, predicate, constants, proj, nproj, out, capacity, F));
+  cudaStream_t s = as_stream(stream);
+  const uint32_t rows = batch->rows;
+  if (rows == 0) {
+    if (count_device) YQ_TRY_CUDA(cudaMemsetAsync(count_device, 0, sizeof(uint32_t), s));
+    if (count_host) *count_host = 0;
+    return YQ_OK;
+  }
+  unsigned long long* scratch = nullptr;
+  YQ_TRY(noalloc_scratch(&scratch));
+  const uint32_t ntiles = ceil_div<uint32_t>(rows, kRowTile);
+  uint32_t* misc = reinterpret_cast<uint32_t*>(scratch);  // [0] tile counter, [1] error, [2] count
+  unsigned long long* status = scratch + 2;
+  // The previous call's values are still there: clear what this call reads.
+  YQ_TRY_CUDA(cudaMemsetAsync(scratch, 0, (2 + (size_t)ntiles + 1) * sizeof(unsigned long long), s));
+  uint32_t* cnt_dev = count_device ? count_device : misc + 2;
+  k_filter_project<<<ntiles, kRowBlock, 0, s>>>(F, rows, misc, status, cnt_dev, misc + 1);
+  YQ_CHECK_LAUNCH();
+  if (count_host) {
+    uint32_t h[2];
+    YQ_TRY_CUDA(cudaMemcpyAsync(&h[0], cnt_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    YQ_TRY_CUDA(cudaMemcpyAsync(&h[1], misc + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    YQ_TRY_CUDA(cudaStreamSynchronize(s));
+    *count_host = h[0];
+    if (h[1] & kErrTimeout) return YQ_ERR_TIMEOUT;
+    if (h[0] > capacity) return YQ_ERR_CAPACITY;
+  }
+  return YQ_OK;
+}
