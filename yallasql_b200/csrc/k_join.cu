@@ -1,0 +1,891 @@
+// Inner join (nested-loop semantics), cross product and the fused star-join
+// aggregate for sm_100a.
+//
+// Replaces ComparisonJoinExpression / ConjunctionJoinExpression with
+// outer_join_batches (one thread per (l, r) pair, one global atomic per match)
+// and and_join_batches (P1 x P2 intersection of pair lists), move_rows_join
+// per output column, and CrossProductOperator's per-column replication
+// (include/engine/operators/filters/comparison_join.hpp:70-236,
+//  src/kernels/comparison_operators_kernel.cu:6-54,136-167,
+//  src/kernels/move_rows_kernel.cu:8-30, include/engine/operators/join_operator.hpp:36-265,
+//  include/engine/operators/cross_product_operator.hpp:87-125, src/kernels/cross_product_kernel.cu:8-27).
+//
+// All conditions are evaluated in one kernel and pairs come out in a fixed
+// order (left row ascending, then right row ascending):
+//  - equality path: the right side's equality key is bucketed once into a
+//    stably ordered hash table that every block copies into shared memory;
+//    each left row probes its bucket, checks the remaining conditions, counts,
+//    and after a decoupled look-back over tiles writes its pairs;
+//  - nested-loop path: a warp per left row sweeps the right rows 32 at a time,
+//    ballots the matches and appends them with popc offsets (coalesced);
+//  - no condition: the cross product is written directly, left-major.
+#include <string.h>
+#include <vector>
+#include "vm_host.cuh"
+#include "yq_lookback.cuh"
+
+namespace yq {
+
+constexpr int kJoinBlock = 256;
+constexpr int kJoinItems = 4;
+constexpr uint32_t kJoinTile = kJoinBlock * kJoinItems;
+constexpr uint32_t kHashMaxRows = 8192;  // right rows that fit the shared-memory table
+constexpr int kMaxConds = 8;
+constexpr int kMaxJoinOut = YQ_MAX_PROJECTIONS;
+
+struct JCol {
+  const char* data;
+  const uint8_t* nulls;
+  int32_t type;
+  int32_t width;
+};
+
+struct JCond {
+  JCol l, r;
+  int32_t cmp;
+};
+
+struct JOut {
+  const char* src;
+  const uint8_t* src_nulls;
+  char* dst;
+  uint8_t* dst_nulls;
+  int32_t width;
+  int32_t side;  // 0 = left, 1 = right
+};
+
+struct JoinParams {
+  JCond cond[kMaxConds];
+  int32_t ncond;
+  int32_t eq;  // index of the equality condition used for hashing (-1: nested loop)
+  JOut out[kMaxJoinOut];
+  int32_t nout;          // 0: write pairs
+  uint32_t* out_left;    // pair output (nout == 0)
+  uint32_t* out_right;
+  unsigned long long capacity;
+  uint32_t L, R;
+  // hash table (equality path)
+  const uint32_t* bstart;  // nbuckets + 1
+  const unsigned long long* hkeys;
+  const uint32_t* hrows;
+  uint32_t nbuckets, hrows_n;
+  unsigned long long* status;
+  uint32_t* tile_counter;
+  unsigned long long* total;
+  uint32_t* err;
+};
+
+// ----------------------------------------------------------- cell access
+__device__ __forceinline__ uint64_t cell_u64(const JCol& c, uint32_t row) {
+  switch (c.width) {
+    case 4: {
+      const uint32_t v = __ldg(reinterpret_cast<const uint32_t*>(c.data) + row);
+      return c.type == YQ_INT32 ? (uint64_t)(int64_t)(int32_t)v : (uint64_t)v;
+    }
+    case 8: return (uint64_t)__ldg(reinterpret_cast<const unsigned long long*>(c.data) + row);
+    default: return (uint64_t)(uint8_t)c.data[row];
+  }
+}
+
+__device__ __forceinline__ bool cell_null(const JCol& c, uint32_t row) { return c.nulls && c.nulls[row]; }
+
+// Normalised equality/hash key: -0.0 folds into +0.0 so they join.
+__device__ __forceinline__ uint64_t hash_key(const JCol& c, uint32_t row) {
+  uint64_t v = cell_u64(c, row);
+  if (c.type == YQ_FLOAT32 && ((uint32_t)v & 0x7fffffffu) == 0u) v = 0;
+  if (c.type == YQ_FLOAT64 && (v & 0x7fffffffffffffffull) == 0ull) v = 0;
+  return v;
+}
+
+__device__ __forceinline__ uint32_t hash_bucket(uint64_t k, uint32_t nb) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdull;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ull;
+  k ^= k >> 33;
+  return (uint32_t)k & (nb - 1u);
+}
+
+__device__ __forceinline__ bool cmp_holds(int s, int op) {
+  switch (op) {
+    case YQ_LT: return s < 0;
+    case YQ_LE: return s <= 0;
+    case YQ_GT: return s > 0;
+    case YQ_GE: return s >= 0;
+    case YQ_EQ: return s == 0;
+    default: return s != 0;
+  }
+}
+
+// Three-way compare of left row l and right row r for one condition; false
+// when either side is NULL (an SQL comparison with NULL is not TRUE).
+__device__ __forceinline__ bool cond_holds(const JCond& c, uint32_t l, uint32_t r) {
+  if (cell_null(c.l, l) || cell_null(c.r, r)) return false;
+  int s;
+  if (c.l.type == YQ_TEXT) {
+    const uint32_t* p = reinterpret_cast<const uint32_t*>(c.l.data + (size_t)l * c.l.width);
+    const uint32_t* q = reinterpret_cast<const uint32_t*>(c.r.data + (size_t)r * c.r.width);
+    const int pw = c.l.width >> 2, qw = c.r.width >> 2, n = pw > qw ? pw : qw;
+    s = 0;
+    for (int i = 0; i < n && s == 0; ++i) {
+      const uint32_t a = i < pw ? __byte_perm(__ldg(p + i), 0, 0x0123) : 0u;
+      const uint32_t b = i < qw ? __byte_perm(__ldg(q + i), 0, 0x0123) : 0u;
+      s = (a > b) - (a < b);
+    }
+  } else {
+    const uint64_t a = cell_u64(c.l, l), b = cell_u64(c.r, r);
+    switch (c.l.type) {
+      case YQ_FLOAT32: {
+        const float x = __uint_as_float((uint32_t)a), y = __uint_as_float((uint32_t)b);
+        s = (x > y) - (x < y);
+        break;
+      }
+      case YQ_FLOAT64: {
+        const double x = __longlong_as_double((long long)a), y = __longlong_as_double((long long)b);
+        s = (x > y) - (x < y);
+        break;
+      }
+      default: {
+        const int64_t x = (int64_t)a, y = (int64_t)b;
+        s = (x > y) - (x < y);
+      }
+    }
+    if (c.l.type == YQ_FLOAT32 || c.l.type == YQ_FLOAT64) {
+      // NaN never satisfies a comparison
+      const bool nan_a = c.l.type == YQ_FLOAT32 ? isnan(__uint_as_float((uint32_t)a))
+                                                : isnan(__longlong_as_double((long long)a));
+      const bool nan_b = c.l.type == YQ_FLOAT32 ? isnan(__uint_as_float((uint32_t)b))
+                                                : isnan(__longlong_as_double((long long)b));
+      if (nan_a || nan_b) return c.cmp == YQ_NE;
+    }
+  }
+  return cmp_holds(s, c.cmp);
+}
+
+__device__ __forceinline__ bool all_conds(const JoinParams& J, uint32_t l, uint32_t r, int skip) {
+  for (int i = 0; i < J.ncond; ++i)
+    if (i != skip && !cond_holds(J.cond[i], l, r)) return false;
+  return true;
+}
+
+__device__ __forceinline__ void copy_cell_j(char* dst, const char* src, int width) {
+  if (width == 4) *reinterpret_cast<uint32_t*>(dst) = __ldg(reinterpret_cast<const uint32_t*>(src));
+  else if (width == 8)
+    *reinterpret_cast<unsigned long long*>(dst) = __ldg(reinterpret_cast<const unsigned long long*>(src));
+  else if (width == 1) *dst = *src;
+  else
+    for (int i = 0; i < width; i += 4)
+      *reinterpret_cast<uint32_t*>(dst + i) = __ldg(reinterpret_cast<const uint32_t*>(src + i));
+}
+
+__device__ __forceinline__ void emit_pair(const JoinParams& J, unsigned long long pos, uint32_t l, uint32_t r) {
+  if (pos >= J.capacity) return;
+  if (J.nout == 0) {
+    J.out_left[pos] = l;
+    J.out_right[pos] = r;
+    return;
+  }
+  for (int o = 0; o < J.nout; ++o) {
+    const JOut& w = J.out[o];
+    const uint32_t row = w.side ? r : l;
+    copy_cell_j(w.dst + (size_t)pos * w.width, w.src + (size_t)row * w.width, w.width);
+    if (w.dst_nulls) w.dst_nulls[pos] = w.src_nulls ? w.src_nulls[row] : 0;
+  }
+}
+
+// ------------------------------------------------------------ hash build
+// One block buckets the right rows (optionally only those passing a
+// predicate) by hash of the equality key; within a bucket rows stay in
+// ascending row order, so probing yields right rows in ascending order.
+struct BuildParams {
+  VmProgram P;        // predicate over the right batch (pred_len == 0: all rows)
+  int32_t pred_len;
+  JCol key;
+  uint32_t R;
+  uint32_t nbuckets;
+  uint32_t* bstart;   // [nbuckets + 1]
+  unsigned long long* hkeys;
+  uint32_t* hrows;
+  uint32_t* counts;   // [0] rows kept, [1] duplicate keys seen
+};
+
+struct SelEmit {
+  uint32_t sel;
+  __device__ __forceinline__ void pred(uint32_t bits) { sel &= bits; }
+  __device__ __forceinline__ void agg(int, int, int, const Val&) {}
+  __device__ __forceinline__ void proj(int, const Val&) {}
+};
+
+constexpr int kBuildBlock = 1024;
+
+__global__ void __launch_bounds__(kBuildBlock) k_hash_build(const __grid_constant__ BuildParams B) {
+  extern __shared__ uint32_t sb[];
+  uint32_t* s_cnt = sb;                        // [nbuckets] counts, then cursors
+  uint32_t* s_rows = s_cnt + B.nbuckets;       // [R] kept rows in order
+  uint32_t* s_warp = s_rows + kHashMaxRows;    // [33]
+  __shared__ uint32_t s_kept;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint32_t i = threadIdx.x; i < B.nbuckets; i += kBuildBlock) s_cnt[i] = 0;
+  if (threadIdx.x == 0) s_kept = 0;
+  __syncthreads();
+  // 1. stable compaction of the rows passing the predicate
+  for (uint32_t base = 0; base < B.R; base += kBuildBlock * ITEMS) {
+    const uint32_t row0 = base + threadIdx.x * ITEMS;
+    uint32_t inr = 0;
+    if (row0 < B.R) inr = (B.R - row0 >= (uint32_t)ITEMS) ? 0xfu : ((1u << (B.R - row0)) - 1u);
+    SelEmit E;
+    E.sel = inr;
+    if (B.pred_len > 0) {
+      Stack S;
+      run_vm(B.P, 0, B.pred_len, row0, inr, inr == 0xfu, S, E);
+    }
+    // key NULLs never join
+    for (int k = 0; k < ITEMS; ++k)
+      if ((E.sel >> k & 1u) && cell_null(B.key, row0 + k)) E.sel &= ~(1u << k);
+    uint32_t total;
+    const uint32_t excl = block_exclusive_sum<kBuildBlock>(__popc(E.sel), s_warp, total);
+    uint32_t pos = s_kept + excl;
+    for (int k = 0; k < ITEMS; ++k)
+      if (E.sel >> k & 1u) {
+        if (pos < kHashMaxRows) s_rows[pos] = row0 + k;
+        ++pos;
+      }
+    __syncthreads();
+    if (threadIdx.x == 0) s_kept += total;
+    __syncthreads();
+  }
+  const uint32_t kept = min(s_kept, kHashMaxRows);
+  // 2. bucket counts and starts
+  for (uint32_t i = threadIdx.x; i < kept; i += kBuildBlock)
+    atomicAdd(&s_cnt[hash_bucket(hash_key(B.key, s_rows[i]), B.nbuckets)], 1u);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (uint32_t b = 0; b < B.nbuckets; ++b) {
+      const uint32_t c = s_cnt[b];
+      B.bstart[b] = run;
+      s_cnt[b] = run;  // becomes the insertion cursor
+      run += c;
+    }
+    B.bstart[B.nbuckets] = run;
+    B.counts[0] = s_kept;
+  }
+  __syncthreads();
+  // 3. stable scatter: rows in ascending order, one warp at a time
+  for (uint32_t base = 0; base < kept; base += kBuildBlock) {
+    const uint32_t i = base + threadIdx.x;
+    const bool valid = i < kept;
+    const uint32_t row = valid ? s_rows[i] : 0u;
+    const uint64_t key = valid ? hash_key(B.key, row) : 0ull;
+    const uint32_t b = valid ? hash_bucket(key, B.nbuckets) : 0xffffffffu;
+    const uint32_t peers = __match_any_sync(0xffffffffu, b) & __ballot_sync(0xffffffffu, valid);
+    const uint32_t rank = __popc(peers & lanemask_lt());
+    for (int w = 0; w < kBuildBlock / 32; ++w) {
+      if (warp == w && valid) {
+        const uint32_t slot = s_cnt[b] + rank;
+        B.hkeys[slot] = key;
+        B.hrows[slot] = row;
+        __syncwarp(peers);
+        if (rank == 0) s_cnt[b] += __popc(peers);
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  // 4. duplicate keys (the fused aggregate needs unique dimension keys)
+  for (uint32_t b = threadIdx.x; b < B.nbuckets; b += kBuildBlock) {
+    const uint32_t s0 = B.bstart[b], s1 = B.bstart[b + 1];
+    for (uint32_t x = s0; x < s1; ++x)
+      for (uint32_t y = x + 1; y < s1; ++y)
+        if (B.hkeys[x] == B.hkeys[y]) atomicAdd(&B.counts[1], 1u);
+  }
+  (void)lane;
+}
+
+// ------------------------------------------------------ equality probing
+struct ProbeSmem {
+  uint32_t* bstart;
+  unsigned long long* keys;
+  uint32_t* rows;
+};
+
+__device__ __forceinline__ ProbeSmem load_table(const JoinParams& J, uint32_t* sm) {
+  ProbeSmem t;
+  t.bstart = sm;
+  t.keys = reinterpret_cast<unsigned long long*>(sm + ((J.nbuckets + 2) & ~1u));
+  t.rows = reinterpret_cast<uint32_t*>(t.keys + J.hrows_n);
+  for (uint32_t i = threadIdx.x; i <= J.nbuckets; i += blockDim.x) t.bstart[i] = __ldg(J.bstart + i);
+  for (uint32_t i = threadIdx.x; i < J.hrows_n; i += blockDim.x) {
+    t.keys[i] = __ldg(J.hkeys + i);
+    t.rows[i] = __ldg(J.hrows + i);
+  }
+  __syncthreads();
+  return t;
+}
+
+__global__ void __launch_bounds__(kJoinBlock) k_join_hash(const __grid_constant__ JoinParams J) {
+  extern __shared__ uint32_t sm[];
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_warp[kJoinBlock / 32 + 1];
+  __shared__ unsigned long long s_prefix;
+  if (threadIdx.x == 0) s_tile = atomicAdd(J.tile_counter, 1u);
+  const ProbeSmem T = load_table(J, sm);
+  const uint32_t tile = s_tile;
+  const uint32_t l0 = tile * kJoinTile + threadIdx.x * kJoinItems;
+  const JCond& ec = J.cond[J.eq];
+  // pass 1: count
+  uint32_t cnt = 0;
+  for (int k = 0; k < kJoinItems; ++k) {
+    const uint32_t l = l0 + k;
+    if (l >= J.L || cell_null(ec.l, l)) continue;
+    const uint64_t key = hash_key(ec.l, l);
+    const uint32_t b = hash_bucket(key, J.nbuckets);
+    for (uint32_t x = T.bstart[b]; x < T.bstart[b + 1]; ++x)
+      if (T.keys[x] == key && all_conds(J, l, T.rows[x], J.eq)) ++cnt;
+  }
+  uint32_t total;
+  const uint32_t excl = block_exclusive_sum<kJoinBlock>(cnt, s_warp, total);
+  if (threadIdx.x < 32) {
+    const unsigned long long p = tile_lookback(J.status, tile, total, J.err);
+    if (threadIdx.x == 0) s_prefix = p;
+  }
+  __syncthreads();
+  unsigned long long pos = s_prefix + excl;
+  // pass 2: write
+  if (cnt) {
+    for (int k = 0; k < kJoinItems; ++k) {
+      const uint32_t l = l0 + k;
+      if (l >= J.L || cell_null(ec.l, l)) continue;
+      const uint64_t key = hash_key(ec.l, l);
+      const uint32_t b = hash_bucket(key, J.nbuckets);
+      for (uint32_t x = T.bstart[b]; x < T.bstart[b + 1]; ++x)
+        if (T.keys[x] == key && all_conds(J, l, T.rows[x], J.eq)) emit_pair(J, pos++, l, T.rows[x]);
+    }
+  }
+  if (tile == gridDim.x - 1 && threadIdx.x == 0) *J.total = s_prefix + total;
+}
+
+// ------------------------------------------------------------ nested loop
+constexpr int kNlRowsPerWarp = 4;
+constexpr uint32_t kNlTile = (kJoinBlock / 32) * kNlRowsPerWarp;  // left rows per block
+
+__global__ void __launch_bounds__(kJoinBlock) k_join_nested(const __grid_constant__ JoinParams J) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_cnt[kNlTile];
+  __shared__ uint32_t s_warp[kJoinBlock / 32 + 1];
+  __shared__ unsigned long long s_prefix;
+  if (threadIdx.x == 0) s_tile = atomicAdd(J.tile_counter, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = lanemask_lt();
+  // pass 1: per left row, count the matching right rows (warp ballots)
+  for (int i = 0; i < kNlRowsPerWarp; ++i) {
+    const uint32_t slot = warp * kNlRowsPerWarp + i;
+    const uint32_t l = tile * kNlTile + slot;
+    uint32_t c = 0;
+    if (l < J.L)
+      for (uint32_t r0 = 0; r0 < J.R; r0 += 32) {
+        const uint32_t r = r0 + lane;
+        const bool m = r < J.R && all_conds(J, l, r, -1);
+        c += __popc(__ballot_sync(0xffffffffu, m));
+      }
+    if (lane == 0) s_cnt[slot] = c;
+  }
+  __syncthreads();
+  const uint32_t mine = threadIdx.x < kNlTile ? s_cnt[threadIdx.x] : 0u;
+  uint32_t total;
+  const uint32_t excl = block_exclusive_sum<kJoinBlock>(mine, s_warp, total);
+  if (threadIdx.x < kNlTile) s_cnt[threadIdx.x] = excl;  // row offset within the tile
+  if (threadIdx.x < 32) {
+    const unsigned long long p = tile_lookback(J.status, tile, total, J.err);
+    if (threadIdx.x == 0) s_prefix = p;
+  }
+  __syncthreads();
+  // pass 2: write matches, 32 right rows per ballot, consecutive positions
+  for (int i = 0; i < kNlRowsPerWarp; ++i) {
+    const uint32_t slot = warp * kNlRowsPerWarp + i;
+    const uint32_t l = tile * kNlTile + slot;
+    if (l >= J.L) continue;
+    unsigned long long pos = s_prefix + s_cnt[slot];
+    for (uint32_t r0 = 0; r0 < J.R; r0 += 32) {
+      const uint32_t r = r0 + lane;
+      const bool m = r < J.R && all_conds(J, l, r, -1);
+      const uint32_t bal = __ballot_sync(0xffffffffu, m);
+      if (m) emit_pair(J, pos + __popc(bal & lt), l, r);
+      pos += __popc(bal);
+    }
+  }
+  if (tile == gridDim.x - 1 && threadIdx.x == 0) *J.total = s_prefix + total;
+}
+
+// ------------------------------------------------------- cross product
+// Every (l, r), left-major: output row l*R + r.
+__global__ void __launch_bounds__(256) k_cross_fill(const __grid_constant__ JoinParams J) {
+  const unsigned long long n = (unsigned long long)J.L * J.R;
+  const unsigned long long lim = n < J.capacity ? n : J.capacity;
+  for (unsigned long long p = blockIdx.x * 256ull + threadIdx.x; p < lim; p += (unsigned long long)gridDim.x * 256ull) {
+    const uint32_t l = (uint32_t)(p / J.R), r = (uint32_t)(p % J.R);
+    emit_pair(J, p, l, r);
+  }
+}
+
+// ------------------------------------------------ fused star-join aggregate
+struct JAParams {
+  VmProgram P;           // fact predicate [0, pred_end) then aggregate inputs [pred_end, pc_end)
+  int32_t pred_end, pc_end;
+  int32_t nagg;
+  uint8_t upd[YQ_MAX_AGGREGATES];
+  JCol fkey;
+  uint32_t nbuckets, hrows_n;
+  const uint32_t* bstart;
+  const unsigned long long* hkeys;
+};
+
+struct JAggEmit {
+  uint32_t sel;
+  Acc acc[YQ_MAX_AGGREGATES];
+  __device__ __forceinline__ void pred(uint32_t bits) { sel &= bits; }
+  __device__ __forceinline__ void agg(int a, int upd, int t, const Val& x) {
+    switch (a) {
+#define YQ_JAGG_CASE(k) \
+  case k: acc_update(acc[k], upd, t, x, sel); break;
+      YQ_JAGG_CASE(0) YQ_JAGG_CASE(1) YQ_JAGG_CASE(2) YQ_JAGG_CASE(3)
+      YQ_JAGG_CASE(4) YQ_JAGG_CASE(5) YQ_JAGG_CASE(6) YQ_JAGG_CASE(7)
+#undef YQ_JAGG_CASE
+      default: break;
+    }
+  }
+  __device__ __forceinline__ void proj(int, const Val&) {}
+};
+
+__global__ void __launch_bounds__(kJoinBlock) k_join_aggregate(const __grid_constant__ JAParams F, uint32_t n,
+                                                               Acc* __restrict__ partials, uint32_t* ticket,
+                                                               Acc* __restrict__ state) {
+  extern __shared__ uint32_t sm[];
+  uint32_t* s_bstart = sm;
+  unsigned long long* s_keys = reinterpret_cast<unsigned long long*>(sm + ((F.nbuckets + 2) & ~1u));
+  for (uint32_t i = threadIdx.x; i <= F.nbuckets; i += kJoinBlock) s_bstart[i] = __ldg(F.bstart + i);
+  for (uint32_t i = threadIdx.x; i < F.hrows_n; i += kJoinBlock) s_keys[i] = __ldg(F.hkeys + i);
+  __syncthreads();
+
+  JAggEmit E;
+#pragma unroll
+  for (int a = 0; a < YQ_MAX_AGGREGATES; ++a) acc_init(E.acc[a], a < F.nagg ? F.upd[a] : UPD_COUNT);
+  const uint32_t tile_rows = kJoinBlock * ITEMS;
+  const uint32_t ntiles = ceil_div<uint32_t>(n, tile_rows);
+  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const uint32_t row0 = tile * tile_rows + threadIdx.x * ITEMS;
+    uint32_t inr = 0;
+    if (row0 < n) inr = (n - row0 >= (uint32_t)ITEMS) ? 0xfu : ((1u << (n - row0)) - 1u);
+    E.sel = inr;
+    Stack S;
+    if (F.pred_end > 0) run_vm(F.P, 0, F.pred_end, row0, inr, inr == 0xfu, S, E);
+    // probe: keep rows whose key is present among the (unique) dimension keys
+    for (int k = 0; k < ITEMS; ++k) {
+      if (!(E.sel >> k & 1u)) continue;
+      const uint32_t row = row0 + k;
+      bool hit = false;
+      if (!cell_null(F.fkey, row)) {
+        const uint64_t key = hash_key(F.fkey, row);
+        const uint32_t b = hash_bucket(key, F.nbuckets);
+        for (uint32_t x = s_bstart[b]; x < s_bstart[b + 1] && !hit; ++x) hit = (s_keys[x] == key);
+      }
+      if (!hit) E.sel &= ~(1u << k);
+    }
+    run_vm(F.P, F.pred_end, F.pc_end, row0, inr, inr == 0xfu, S, E);
+#pragma unroll
+    for (int a = 0; a < YQ_MAX_AGGREGATES; ++a)
+      if (a < F.nagg && F.upd[a] == UPD_COUNT_STAR) E.acc[a].cnt += __popc(E.sel);
+  }
+  __shared__ Acc s_acc[kJoinBlock / 32][YQ_MAX_AGGREGATES];
+  __shared__ bool s_last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < YQ_MAX_AGGREGATES; ++a) {
+    if (a < F.nagg) {
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) acc_shfl_down(E.acc[a], d, F.upd[a]);
+      if (lane == 0) s_acc[warp][a] = E.acc[a];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < F.nagg) {
+    const int a = threadIdx.x;
+    Acc t = s_acc[0][a];
+    for (int w = 1; w < kJoinBlock / 32; ++w) acc_combine(t, s_acc[w][a], F.upd[a]);
+    partials[blockIdx.x * YQ_MAX_AGGREGATES + a] = t;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x < F.nagg) {
+    const int a = threadIdx.x;
+    const int upd = F.upd[a];
+    Acc t;
+    acc_init(t, upd);
+    for (uint32_t b = 0; b < gridDim.x; ++b) {
+      const Acc* p = partials + b * YQ_MAX_AGGREGATES + a;
+      Acc q;
+      q.cnt = __ldcg(&p->cnt);
+      q.i = __ldcg(&p->i);
+      q.f = __ldcg(&p->f);
+      acc_combine(t, q, upd);
+    }
+    Acc s = state[a];
+    acc_combine(s, t, upd);
+    state[a] = s;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// ---------------------------------------------------------------- host
+static bool join_col_ok(const yq_column& c) {
+  if (!c.data) return false;
+  return ProgramBuilder::valid_column(c);
+}
+
+static JCol jcol(const yq_column& c) {
+  JCol j;
+  j.data = static_cast<const char*>(c.data);
+  j.nulls = c.nulls;
+  j.type = c.type;
+  j.width = c.width;
+  return j;
+}
+
+static bool hashable(int t) {
+  return t == YQ_INT32 || t == YQ_INT64 || t == YQ_DATETIME || t == YQ_FLOAT32 || t == YQ_FLOAT64 || t == YQ_BOOL;
+}
+
+static uint32_t pow2_at_least(uint32_t x) {
+  uint32_t p = 16;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+static size_t table_smem(uint32_t nbuckets, uint32_t nrows, bool with_rows) {
+  return sizeof(uint32_t) * ((nbuckets + 2) & ~1u) + sizeof(unsigned long long) * nrows +
+         (with_rows ? sizeof(uint32_t) * nrows : 0);
+}
+
+static int build_table(const yq_batch* right, const yq_program* pred, const yq_constants* consts, int key_col,
+                       uint32_t nbuckets, uint32_t* bstart, unsigned long long* hkeys, uint32_t* hrows,
+                       uint32_t* counts, cudaStream_t s) {
+  BuildParams B;
+  memset(&B, 0, sizeof(B));
+  ProgramBuilder PB;
+  YQ_TRY(PB.set_columns(right->columns, right->ncols));
+  YQ_TRY(PB.set_constants(consts));
+  if (pred && pred->len > 0) {
+    int t = -1;
+    YQ_TRY(PB.append(pred, t));
+    if (t != YQ_BOOL) return YQ_ERR_INVALID_ARG;
+    YQ_TRY(PB.emit(OP_EMIT_PRED, 0, 0, YQ_BOOL));
+  }
+  PB.finalize();
+  memcpy(&B.P, &PB.P, sizeof(VmProgram));
+  B.pred_len = PB.len;
+  B.key = jcol(right->columns[key_col]);
+  B.R = right->rows;
+  B.nbuckets = nbuckets;
+  B.bstart = bstart;
+  B.hkeys = hkeys;
+  B.hrows = hrows;
+  B.counts = counts;
+  const size_t smem = sizeof(uint32_t) * (nbuckets + kHashMaxRows + 40);
+  static size_t attr = 0;
+  if (smem > 48 * 1024 && smem > attr) {
+    YQ_TRY_CUDA(cudaFuncSetAttribute(k_hash_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = smem;
+  }
+  ProfScope ps("join_hash_build", s, (double)right->rows * right->columns[key_col].width);
+  k_hash_build<<<1, kBuildBlock, smem, s>>>(B);
+  YQ_CHECK_LAUNCH();
+  return YQ_OK;
+}
+
+// Shared by yq_join_pairs / yq_join_project.
+static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_cond* conds, int32_t ncond,
+                     const yq_join_output* outputs, int32_t nout, yq_column* out, uint32_t* out_left,
+                     uint32_t* out_right, uint64_t capacity, uint64_t* count_host, void* workspace,
+                     size_t workspace_bytes, cudaStream_t s) {
+  if (!left || !right || ncond < 0 || ncond > kMaxConds || (ncond > 0 && !conds) || nout < 0 || nout > kMaxJoinOut ||
+      (nout > 0 && (!outputs || !out)))
+    return YQ_ERR_INVALID_ARG;
+  JoinParams J;
+  memset(&J, 0, sizeof(J));
+  J.L = left->rows;
+  J.R = right->rows;
+  J.ncond = ncond;
+  J.eq = -1;
+  for (int i = 0; i < ncond; ++i) {
+    const yq_join_cond& c = conds[i];
+    if (c.left_col < 0 || c.left_col >= left->ncols || c.right_col < 0 || c.right_col >= right->ncols ||
+        c.cmp < YQ_LT || c.cmp > YQ_NE)
+      return YQ_ERR_INVALID_ARG;
+    const yq_column& a = left->columns[c.left_col];
+    const yq_column& b = right->columns[c.right_col];
+    if (!join_col_ok(a) || !join_col_ok(b) || a.type != b.type) return YQ_ERR_INVALID_ARG;
+    J.cond[i].l = jcol(a);
+    J.cond[i].r = jcol(b);
+    J.cond[i].cmp = c.cmp;
+    if (J.eq < 0 && c.cmp == YQ_EQ && hashable(a.type)) J.eq = i;
+  }
+  for (int o = 0; o < nout; ++o) {
+    const yq_join_output& w = outputs[o];
+    const yq_batch* side = w.side ? right : left;
+    if (w.column < 0 || w.column >= side->ncols) return YQ_ERR_INVALID_ARG;
+    const yq_column& c = side->columns[w.column];
+    if (!join_col_ok(c) || out[o].type != c.type || out[o].width != c.width || !out[o].data) return YQ_ERR_INVALID_ARG;
+    J.out[o].src = static_cast<const char*>(c.data);
+    J.out[o].src_nulls = c.nulls;
+    J.out[o].dst = static_cast<char*>(out[o].data);
+    J.out[o].dst_nulls = const_cast<uint8_t*>(out[o].nulls);
+    J.out[o].width = c.width;
+    J.out[o].side = w.side;
+  }
+  J.nout = nout;
+  if (nout == 0 && capacity > 0 && (!out_left || !out_right)) return YQ_ERR_INVALID_ARG;
+  J.out_left = out_left;
+  J.out_right = out_right;
+  J.capacity = capacity;
+
+  if (J.L == 0 || J.R == 0) {
+    if (count_host) *count_host = 0;
+    return YQ_OK;
+  }
+  if (ncond == 0) {  // cross product: size known up front
+    const unsigned long long n = (unsigned long long)J.L * J.R;
+    double row_bytes = nout == 0 ? 8.0 : 0.0;
+    for (int o = 0; o < nout; ++o) row_bytes += J.out[o].width + (J.out[o].dst_nulls ? 1 : 0);
+    ProfScope ps("cross_product", s, (double)(n < capacity ? n : capacity) * row_bytes);
+    const unsigned long long lim = n < capacity ? n : capacity;
+    int grid = (int)((lim + 255) / 256);
+    const int cap = sm_count() * 16;
+    if (grid > cap) grid = cap;
+    if (grid < 1) grid = 1;
+    k_cross_fill<<<grid, 256, 0, s>>>(J);
+    YQ_CHECK_LAUNCH();
+    if (count_host) *count_host = n;
+    return n > capacity ? YQ_ERR_CAPACITY : YQ_OK;
+  }
+
+  const bool use_hash = J.eq >= 0 && J.R <= kHashMaxRows;
+  const uint32_t nbuckets = use_hash ? pow2_at_least(J.R) : 0u;
+  const uint32_t ntiles = use_hash ? ceil_div<uint32_t>(J.L, kJoinTile) : ceil_div<uint32_t>(J.L, kNlTile);
+  WsSize w;
+  w.add<uint32_t>(nbuckets + 1);
+  w.add<unsigned long long>(use_hash ? J.R : 1);
+  w.add<uint32_t>(use_hash ? J.R : 1);
+  w.add<unsigned long long>((size_t)ntiles + 1);
+  w.add<uint32_t>(8);
+  w.add<unsigned long long>(2);
+  Workspace ws;
+  YQ_TRY(ws.acquire(workspace, workspace_bytes, w.total(), s));
+  uint32_t* d_bstart = ws.take<uint32_t>(nbuckets + 1);
+  unsigned long long* d_hkeys = ws.take<unsigned long long>(use_hash ? J.R : 1);
+  uint32_t* d_hrows = ws.take<uint32_t>(use_hash ? J.R : 1);
+  J.status = ws.take<unsigned long long>((size_t)ntiles + 1);
+  uint32_t* d_misc = ws.take<uint32_t>(8);  // [0] tile counter [1] err [2..3] build counts
+  J.total = ws.take<unsigned long long>(2);
+  J.tile_counter = d_misc;
+  J.err = d_misc + 1;
+  YQ_TRY_CUDA(cudaMemsetAsync(J.status, 0, ((size_t)ntiles + 1) * sizeof(unsigned long long), s));
+  YQ_TRY_CUDA(cudaMemsetAsync(d_misc, 0, 8 * sizeof(uint32_t), s));
+  YQ_TRY_CUDA(cudaMemsetAsync(J.total, 0, 2 * sizeof(unsigned long long), s));
+  double out_row_bytes = nout == 0 ? 8.0 : 0.0;
+  for (int o = 0; o < nout; ++o) out_row_bytes += J.out[o].width + (J.out[o].dst_nulls ? 1 : 0);
+  if (use_hash) {
+    YQ_TRY(build_table(right, nullptr, nullptr, conds[J.eq].right_col, nbuckets, d_bstart, d_hkeys, d_hrows,
+                       d_misc + 2, s));
+    J.bstart = d_bstart;
+    J.hkeys = d_hkeys;
+    J.hrows = d_hrows;
+    J.nbuckets = nbuckets;
+    J.hrows_n = J.R;
+    const size_t smem = table_smem(nbuckets, J.R, true);
+    static size_t attr = 0;
+    if (smem > 48 * 1024 && smem > attr) {
+      YQ_TRY_CUDA(cudaFuncSetAttribute(k_join_hash, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr = smem;
+    }
+    ProfScope ps("join_hash_probe", s, (double)J.L * left->columns[conds[J.eq].left_col].width);
+    k_join_hash<<<ntiles, kJoinBlock, smem, s>>>(J);
+    YQ_CHECK_LAUNCH();
+  } else {
+    ProfScope ps("join_nested_loop", s, (double)J.L * J.R * 0.0);
+    k_join_nested<<<ntiles, kJoinBlock, 0, s>>>(J);
+    YQ_CHECK_LAUNCH();
+  }
+  unsigned long long h_total = 0;
+  uint32_t h_err = 0;
+  YQ_TRY_CUDA(cudaMemcpyAsync(&h_total, J.total, sizeof(h_total), cudaMemcpyDeviceToHost, s));
+  YQ_TRY_CUDA(cudaMemcpyAsync(&h_err, J.err, sizeof(h_err), cudaMemcpyDeviceToHost, s));
+  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  if (count_host) *count_host = h_total;
+  if (h_err & kErrTimeout) return YQ_ERR_TIMEOUT;
+  return h_total > capacity ? YQ_ERR_CAPACITY : YQ_OK;
+}
+
+}  // namespace yq
+
+using namespace yq;
+
+extern "C" {
+
+size_t yq_join_workspace_size(uint32_t left_rows, uint32_t right_rows) {
+  const uint32_t nb = pow2_at_least(right_rows);
+  const uint32_t ntiles = ceil_div<uint32_t>(left_rows, kNlTile);
+  WsSize w;
+  w.add<uint32_t>(nb + 1);
+  w.add<unsigned long long>(right_rows ? right_rows : 1);
+  w.add<uint32_t>(right_rows ? right_rows : 1);
+  w.add<unsigned long long>((size_t)ntiles + 1);
+  w.add<uint32_t>(8);
+  w.add<unsigned long long>(2);
+  return w.total();
+}
+
+int yq_join_pairs(const yq_batch* left, const yq_batch* right, const yq_join_cond* conds, int32_t ncond,
+                  uint32_t* out_left, uint32_t* out_right, uint64_t capacity, uint64_t* count_host, void* workspace,
+                  size_t workspace_bytes, void* stream) {
+  return join_impl(left, right, conds, ncond, nullptr, 0, nullptr, out_left, out_right, capacity, count_host,
+                   workspace, workspace_bytes, as_stream(stream));
+}
+
+int yq_join_project(const yq_batch* left, const yq_batch* right, const yq_join_cond* conds, int32_t ncond,
+                    const yq_join_output* outputs, int32_t nout, yq_column* out, uint64_t capacity,
+                    uint64_t* count_host, void* workspace, size_t workspace_bytes, void* stream) {
+  if (nout <= 0) return YQ_ERR_INVALID_ARG;
+  return join_impl(left, right, conds, ncond, outputs, nout, out, nullptr, nullptr, capacity, count_host, workspace,
+                   workspace_bytes, as_stream(stream));
+}
+
+size_t yq_join_aggregate_workspace_size(uint32_t fact_rows, uint32_t dim_rows, int32_t nagg) {
+  (void)fact_rows;
+  (void)nagg;
+  const uint32_t nb = pow2_at_least(dim_rows);
+  WsSize w;
+  w.add<uint32_t>(nb + 1);
+  w.add<unsigned long long>(dim_rows ? dim_rows : 1);
+  w.add<uint32_t>(dim_rows ? dim_rows : 1);
+  w.add<uint32_t>(8);
+  w.add<Acc>((size_t)sm_count() * 8 * YQ_MAX_AGGREGATES);
+  return w.total();
+}
+
+int yq_join_aggregate(const yq_batch* fact, const yq_program* fact_predicate, int32_t fact_key, const yq_batch* dim,
+                      const yq_program* dim_predicate, int32_t dim_key, const yq_constants* constants,
+                      const yq_agg_spec* aggs, int32_t nagg, void* state, void* workspace, size_t workspace_bytes,
+                      void* stream) {
+  if (!fact || !dim || !state || fact_key < 0 || fact_key >= fact->ncols || dim_key < 0 || dim_key >= dim->ncols ||
+      nagg < 0 || nagg > YQ_MAX_AGGREGATES || (nagg > 0 && !aggs))
+    return YQ_ERR_INVALID_ARG;
+  const yq_column& fk = fact->columns[fact_key];
+  const yq_column& dk = dim->columns[dim_key];
+  if (!join_col_ok(fk) || !join_col_ok(dk) || fk.type != dk.type || !hashable(fk.type)) return YQ_ERR_INVALID_ARG;
+  if (dim->rows > kHashMaxRows) return YQ_ERR_UNSUPPORTED;
+  cudaStream_t s = as_stream(stream);
+  JAParams F;
+  memset(&F, 0, sizeof(F));
+  {
+    ProgramBuilder B;
+    YQ_TRY(B.set_columns(fact->columns, fact->ncols));
+    YQ_TRY(B.set_constants(constants));
+    if (fact_predicate && fact_predicate->len > 0) {
+      int t = -1;
+      YQ_TRY(B.append(fact_predicate, t));
+      if (t != YQ_BOOL) return YQ_ERR_INVALID_ARG;
+      YQ_TRY(B.emit(OP_EMIT_PRED, 0, 0, YQ_BOOL));
+    }
+    F.pred_end = B.len;
+    for (int a = 0; a < nagg; ++a) {
+      const yq_agg_spec& g = aggs[a];
+      if (g.kind < YQ_AGG_COUNT_STAR || g.kind > YQ_AGG_MAX) return YQ_ERR_INVALID_ARG;
+      const bool flt = (g.input_type == YQ_FLOAT32 || g.input_type == YQ_FLOAT64);
+      uint8_t upd;
+      switch (g.kind) {
+        case YQ_AGG_COUNT_STAR: upd = UPD_COUNT_STAR; break;
+        case YQ_AGG_COUNT: upd = UPD_COUNT; break;
+        case YQ_AGG_SUM:
+        case YQ_AGG_AVG: upd = flt ? UPD_SUM_F : UPD_SUM_I; break;
+        case YQ_AGG_MIN: upd = flt ? UPD_MIN_F : UPD_MIN_I; break;
+        default: upd = flt ? UPD_MAX_F : UPD_MAX_I; break;
+      }
+      F.upd[a] = upd;
+      if (g.kind == YQ_AGG_COUNT_STAR) continue;
+      int t = -1;
+      YQ_TRY(B.append(&g.input, t));
+      if (g.kind != YQ_AGG_COUNT && t != g.input_type) return YQ_ERR_INVALID_ARG;
+      YQ_TRY(B.emit(OP_EMIT_AGG, (uint8_t)a, upd, (uint8_t)t));
+    }
+    B.finalize();
+    memcpy(&F.P, &B.P, sizeof(VmProgram));
+    F.pc_end = B.len;
+    F.nagg = nagg;
+  }
+  if (fact->rows == 0 || nagg == 0) return YQ_OK;
+  const uint32_t nbuckets = pow2_at_least(dim->rows ? dim->rows : 1);
+  Workspace ws;
+  YQ_TRY(ws.acquire(workspace, workspace_bytes, yq_join_aggregate_workspace_size(fact->rows, dim->rows, nagg), s));
+  uint32_t* d_bstart = ws.take<uint32_t>(nbuckets + 1);
+  unsigned long long* d_hkeys = ws.take<unsigned long long>(dim->rows ? dim->rows : 1);
+  uint32_t* d_hrows = ws.take<uint32_t>(dim->rows ? dim->rows : 1);
+  uint32_t* d_misc = ws.take<uint32_t>(8);  // [0] ticket [2] kept rows [3] duplicate keys
+  const int grid_cap = sm_count() * 8;
+  Acc* partials = ws.take<Acc>((size_t)grid_cap * YQ_MAX_AGGREGATES);
+  YQ_TRY_CUDA(cudaMemsetAsync(d_misc, 0, 8 * sizeof(uint32_t), s));
+  YQ_TRY(build_table(dim, dim_predicate, constants, dim_key, nbuckets, d_bstart, d_hkeys, d_hrows, d_misc + 2, s));
+  uint32_t counts[2] = {0, 0};
+  YQ_TRY_CUDA(cudaMemcpyAsync(counts, d_misc + 2, sizeof(counts), cudaMemcpyDeviceToHost, s));
+  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  if (counts[1] != 0) return YQ_ERR_UNSUPPORTED;  // dimension keys repeat: use yq_join_pairs + an aggregate
+  F.fkey = jcol(fk);
+  F.nbuckets = nbuckets;
+  F.hrows_n = counts[0];
+  F.bstart = d_bstart;
+  F.hkeys = d_hkeys;
+  const size_t smem = table_smem(nbuckets, counts[0], false);
+  static size_t attr = 0;
+  if (smem > 48 * 1024 && smem > attr) {
+    YQ_TRY_CUDA(cudaFuncSetAttribute(k_join_aggregate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = smem;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_join_aggregate, kJoinBlock, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  if (per_sm > 8) per_sm = 8;
+  const uint32_t tiles = ceil_div<uint32_t>(fact->rows, kJoinBlock * ITEMS);
+  int grid = sm_count() * per_sm;
+  if ((uint32_t)grid > tiles) grid = (int)tiles;
+  double row_bytes = fk.width;
+  {
+    bool used[YQ_MAX_BATCH_COLUMNS] = {false};
+    used[fact_key] = true;
+    for (int i = 0; i < F.pc_end; ++i) {
+      const Insn& I = F.P.code[i];
+      switch (I.op & OP_MASK) {
+        case OP_COL: used[I.a] = true; break;
+        case OP_ARITH_COL:
+        case OP_CMP_COL_CONST:
+        case OP_AND_CMP_COL_CONST: used[I.b] = true; break;
+        case OP_CMP_COL_COL: used[I.b] = true; used[I.imm] = true; break;
+        default: break;
+      }
+    }
+    row_bytes = 0;
+    for (int c = 0; c < fact->ncols; ++c)
+      if (used[c]) row_bytes += fact->columns[c].width + (fact->columns[c].nulls ? 1 : 0);
+  }
+  ProfScope ps("join_aggregate", s, (double)fact->rows * row_bytes);
+  k_join_aggregate<<<grid, kJoinBlock, smem, s>>>(F, fact->rows, partials, d_misc, static_cast<Acc*>(state));
+  YQ_CHECK_LAUNCH();
+  return YQ_OK;
+}
+
+}  // extern "C"

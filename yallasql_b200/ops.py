@@ -310,3 +310,85 @@ def merge_runs(runs: DeviceBatch, key: int, descending: bool, offsets: list[int]
         offsets = merge_pass(src, key, descending, offsets, dst, nulls_first, stream)
         src = dst
     return out
+
+
+# ----------------------------------------------------------------- joins
+def _conds(conds):
+    arr = (A.JoinCond * max(1, len(conds)))(*[A.JoinCond(l, r, c) for l, r, c in conds])
+    return arr
+
+
+def join_pairs(left: DeviceBatch, right: DeviceBatch, conds: list, capacity: int | None = None, stream=None):
+    """Inner join pairs (left row, right row) in (left, right) order; conds =
+    [(left_col, right_col, yq_cmp)], all ANDed (JoinOperator + ComparisonJoinExpression)."""
+    lb, lk = left.c()
+    rb, rk = right.c()
+    cap = capacity if capacity is not None else max(1, left.rows * right.rows if len(conds) == 0 else left.rows * 4)
+    while True:
+        ol = torch.empty(max(1, cap), dtype=torch.int32, device="cuda")
+        orr = torch.empty(max(1, cap), dtype=torch.int32, device="cuda")
+        cnt = C.c_uint64(0)
+        st = lib().yq_join_pairs(C.byref(lb), C.byref(rb), _conds(conds), len(conds), ol.data_ptr(), orr.data_ptr(),
+                                 cap, C.byref(cnt), None, 0, _stream(stream))
+        if st == A.ERR_CAPACITY and capacity is None:
+            cap = int(cnt.value)  # count-then-retry with the exact size
+            continue
+        _check(st, "yq_join_pairs")
+        n = int(cnt.value)
+        return ol[:n], orr[:n]
+
+
+def join_project(left: DeviceBatch, right: DeviceBatch, conds: list, outputs: list, capacity: int | None = None,
+                 stream=None) -> DeviceBatch:
+    """Join and write the chosen columns [(side, column)] of every matching pair."""
+    lb, lk = left.c()
+    rb, rk = right.c()
+    srcs = [(right if s else left).columns[c] for s, c in outputs]
+    cap = capacity if capacity is not None else (left.rows * right.rows if not conds else max(1, left.rows * 4))
+    outs_c = (A.JoinOutput * len(outputs))(*[A.JoinOutput(s, c) for s, c in outputs])
+    while True:
+        outs = [DeviceColumn.empty(c.type, max(1, cap), c.width if c.type == A.TEXT else None,
+                                   nulls=c.nulls is not None) for c in srcs]
+        oc = (A.Column * len(outs))(*[o.c() for o in outs])
+        cnt = C.c_uint64(0)
+        st = lib().yq_join_project(C.byref(lb), C.byref(rb), _conds(conds), len(conds), outs_c, len(outputs), oc,
+                                   cap, C.byref(cnt), None, 0, _stream(stream))
+        if st == A.ERR_CAPACITY and capacity is None:
+            cap = int(cnt.value)
+            continue
+        _check(st, "yq_join_project")
+        n = int(cnt.value)
+        return DeviceBatch([o.slice(0, n) for o in outs])
+
+
+def cross_product(left: DeviceBatch, right: DeviceBatch, stream=None) -> DeviceBatch:
+    """Every (l, r) pair, left-major, all columns of both sides (CrossProductOperator)."""
+    outputs = [(0, i) for i in range(len(left.columns))] + [(1, i) for i in range(len(right.columns))]
+    return join_project(left, right, [], outputs, stream=stream)
+
+
+class JoinAggPlan:
+    """Fused star join + aggregate: fact rows passing `fact_pred` that find their
+    key among the dimension rows passing `dim_pred` feed the aggregates."""
+
+    def __init__(self, fact_types, dim_types, fact_pred, fact_key, dim_pred, dim_key, aggs):
+        self.pool = ConstPool()
+        self.fpred = Compiled(compile_expr(fact_pred, self.pool, fact_types) if fact_pred is not None else [])
+        self.dpred = Compiled(compile_expr(dim_pred, self.pool, dim_types) if dim_pred is not None else [])
+        self.inputs = [Compiled(compile_expr(a.arg, self.pool, fact_types) if a.arg is not None else []) for a in aggs]
+        self.aggs = aggs
+        self.fact_key, self.dim_key = fact_key, dim_key
+        self.specs = (A.AggSpec * max(1, len(aggs)))()
+        for i, (a, p) in enumerate(zip(aggs, self.inputs)):
+            self.specs[i].kind = a.kind
+            self.specs[i].input_type = a.input_type
+            self.specs[i].input = p.prog
+        self.consts, self._keep = self.pool.to_c()
+
+    def run(self, fact: DeviceBatch, dim: DeviceBatch, state: AggState, stream=None):
+        fb, fk = fact.c()
+        db, dk = dim.c()
+        _check(lib().yq_join_aggregate(C.byref(fb), C.byref(self.fpred.prog), self.fact_key, C.byref(db),
+                                       C.byref(self.dpred.prog), self.dim_key, C.byref(self.consts), self.specs,
+                                       len(self.aggs), state.buf.data_ptr(), None, 0, _stream(stream)),
+               "yq_join_aggregate")
