@@ -1,0 +1,92 @@
+/*
+ * yq_engine.h — C entry to the C++ operator layer (libyq_engine.so).
+ *
+ * The operator layer mirrors YallaSQL's pull-based physical operators
+ * (`YallaSQL::Operator::init()` / `BatchID next(CacheManager&)`,
+ * include/engine/operators/operator.hpp:12-60) over columnar batches with one
+ * null byte per row (include/batch.hpp:21-145) and a cache manager with a
+ * device-memory budget (include/engine/cache_manager.hpp:11-88). Operators call
+ * the kernels through include/yq_ops.h only. The reference builds the operator
+ * tree from DuckDB's logical plan (src/engine/operators/operator.cpp:14-44);
+ * DuckDB is not part of this path, so a host assembles the same tree here
+ * node by node, with expressions already compiled to yq_program form.
+ *
+ * Input columns live in HOST memory; the scan streams them to the device as
+ * 4 MB batches (include/config.hpp:28-36 sizing) through two pinned staging
+ * buffers and a copy stream, so the copy of batch k+1 overlaps the kernels of
+ * batch k (GetOperator::storeBuffer copies synchronously,
+ * src/engine/operators/get_operator.cpp:125-148). Results come back to host
+ * memory owned by the result object.
+ */
+#ifndef YQ_ENGINE_H
+#define YQ_ENGINE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "yq_ops.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct yq_plan yq_plan;
+typedef struct yq_result yq_result;
+
+/* A host column: `rows` values of `width` bytes at `data`, nulls one byte per
+ * row or NULL. Pinned host memory is copied directly; pageable memory is
+ * staged through the scan's pinned buffers. */
+typedef struct yq_host_column {
+  const void* data;
+  const uint8_t* nulls;
+  int32_t type;
+  int32_t width;
+} yq_host_column;
+
+/* A plan owns its operators, a compute stream, a copy stream and a cache
+ * manager whose device budget is `gpu_budget_bytes` (0 = 1 GiB, the
+ * reference's MAX_LIMIT_GPU_CACHE, include/config.hpp:19). Batches beyond the
+ * budget move to pinned host memory and come back on demand. */
+yq_plan* yq_plan_create(uint64_t gpu_budget_bytes);
+void yq_plan_destroy(yq_plan* plan);
+/* Node builders return the new node id (>= 0) or -yq_status. */
+int yq_plan_scan(yq_plan* plan, const yq_host_column* cols, int32_t ncols, uint64_t rows,
+                 uint32_t batch_rows /* 0 = 4 MB batches */);
+int yq_plan_filter(yq_plan* plan, int32_t child, const yq_program* predicate,
+                   const yq_constants* constants);
+int yq_plan_project(yq_plan* plan, int32_t child, const yq_projection* proj, int32_t nproj,
+                    const yq_constants* constants);
+int yq_plan_aggregate(yq_plan* plan, int32_t child, const yq_agg_spec* aggs, int32_t nagg,
+                      const yq_constants* constants);
+int yq_plan_order(yq_plan* plan, int32_t child, int32_t key_col, int32_t descending,
+                  int32_t nulls_first);
+int yq_plan_join(yq_plan* plan, int32_t left, int32_t right, const yq_join_cond* conds,
+                 int32_t ncond);
+int yq_plan_cross(yq_plan* plan, int32_t left, int32_t right);
+
+/* Pull every batch from `root` (ExecutorEngine::execute's loop,
+ * src/engine/executor_engine.cpp:28-38), copy the result to host memory and
+ * return it in *out (free with yq_result_destroy). */
+int yq_plan_execute(yq_plan* plan, int32_t root, yq_result** out);
+
+uint64_t yq_result_rows(const yq_result* r);
+int32_t yq_result_ncols(const yq_result* r);
+/* Host view of result column c (valid until yq_result_destroy). */
+int yq_result_column(const yq_result* r, int32_t c, yq_host_column* out);
+void yq_result_destroy(yq_result* r);
+
+/* Statistics of the last execute: batches pulled, bytes copied host->device
+ * and device->host, device milliseconds of the compute stream. */
+typedef struct yq_plan_stats {
+  uint64_t batches;
+  uint64_t h2d_bytes;
+  uint64_t d2h_bytes;
+  double compute_ms;
+  uint64_t spilled_batches;
+} yq_plan_stats;
+int yq_plan_stats_read(const yq_plan* plan, yq_plan_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* YQ_ENGINE_H */

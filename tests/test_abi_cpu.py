@@ -36,6 +36,18 @@ def test_every_declared_symbol_is_exported(yq):
     assert not missing, f"declared in yq_ops.h but not exported: {missing}"
 
 
+def test_engine_library_exports_its_header(yq):
+    from yallasql_b200 import build, plan
+    if not os.path.exists(plan.LIB_PATH):
+        build.build_engine()
+    names = declared_functions("yq_engine.h")
+    assert len(names) >= 14
+    missing = sorted(set(names) - exported(plan.LIB_PATH))
+    assert not missing, f"declared in yq_engine.h but not exported: {missing}"
+    assert set(names) <= set(plan.PROTOTYPES)
+    plan.lib()  # loads (with libyq_ops.so) without touching a GPU
+
+
 def test_prototypes_cover_header(yq):
     names = set(declared_functions("yq_ops.h"))
     assert names <= set(A.PROTOTYPES), sorted(names - set(A.PROTOTYPES))

@@ -1,0 +1,99 @@
+"""The C++ operator layer end to end from host columns: scan (pinned,
+double-buffered H2D) -> operators -> host result, against the oracle."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from oracle import expr_eval
+from yallasql_b200 import _abi as A
+from yallasql_b200 import datagen
+from yallasql_b200.expr import Aggregate, Arith, Cast, ColumnRef, Compare, Constant
+from yallasql_b200.plan import Plan
+
+from helpers import oracle_cols, rel_close
+from test_filter_gpu import sales_query_exprs
+
+pytestmark = pytest.mark.gpu
+
+
+def sales_cols(rows, seed=0):
+    t = datagen.sales_table(rows, seed=seed)
+    return t, [t["price"], t["qty"], t["discount"], t["category"]]
+
+
+@pytest.mark.parametrize("batch_rows", [0, 4096, 100_000])
+def test_filter_aggregate_query(cuda, batch_rows):
+    t, cols = sales_cols(500_000)
+    pred, aggs = sales_query_exprs()
+    p = Plan()
+    root = p.aggregate(p.filter(p.scan(cols, batch_rows=batch_rows), pred), aggs)
+    res = p.execute(root)
+    got = [v[0] if (n is None or not n[0]) else None for v, n in res]
+    want = expr_eval.aggregate(pred, aggs, oracle_cols(cols), len(cols[0]))
+    assert int(got[1]) == want[1]
+    assert float(got[2]) == want[2] and float(got[3]) == want[3]
+    assert rel_close(float(got[0]), want[0], 1e-6)
+    st = p.stats()
+    assert st.batches >= 1 and st.h2d_bytes == sum(c.nbytes for c in cols)
+
+
+def test_empty_aggregate_returns_one_row(cuda):
+    _, cols = sales_cols(1000)
+    p = Plan()
+    never = Compare(A.LT, ColumnRef(1, A.INT32), Constant(-1, A.INT32))
+    aggs = [Aggregate(A.AGG_COUNT_STAR), Aggregate(A.AGG_SUM, ColumnRef(0, A.FLOAT32)),
+            Aggregate(A.AGG_MIN, ColumnRef(1, A.INT32))]
+    res = p.execute(p.aggregate(p.filter(p.scan(cols), never), aggs))
+    assert res[0][0][0] == 0 and res[1][1][0] and res[2][1][0]
+
+
+def test_filter_project_query_pinned_and_pageable(cuda):
+    t, cols = sales_cols(300_000, seed=4)
+    pred, _ = sales_query_exprs()
+    select = [3, 0, Arith(A.MUL, ColumnRef(0, A.FLOAT32), Cast(ColumnRef(2, A.INT32), A.FLOAT32))]
+    want = expr_eval.project(pred, select, oracle_cols(cols), len(cols[0]))
+    for pinned in (False, True):
+        p = Plan()
+        if pinned:
+            src = [torch.from_numpy(c).pin_memory() for c in cols]
+            scan = p.scan(src, types=[A.FLOAT32, A.INT32, A.INT32, A.TEXT], batch_rows=50_000)
+        else:
+            scan = p.scan(cols, batch_rows=50_000)
+        res = p.execute(p.project(p.filter(scan, pred), select))
+        for (v, _), (wv, _) in zip(res, want):
+            np.testing.assert_array_equal(v, np.asarray(wv).astype(v.dtype))
+
+
+@pytest.mark.parametrize("budget", [0, 1 << 20])
+def test_order_by_query_with_spills(cuda, budget):
+    t = datagen.order_table(200_000, seed=1, dist="zipf")
+    cols = [t["key"], t["id"], t["txt"], t["d"]]
+    p = Plan(gpu_budget=budget)
+    root = p.order(p.scan(cols, types=[A.FLOAT32, A.INT64, A.TEXT, A.DATETIME], batch_rows=7000), 0, descending=True)
+    res = p.execute(root)
+    perm = oracle.sort_perm(t["key"], desc=True)
+    for (v, _), name in zip(res, ["key", "id", "txt", "d"]):
+        np.testing.assert_array_equal(v, t[name][perm])
+    if budget:
+        assert p.stats().spilled_batches > 0
+
+
+def test_join_and_cross_product_queries(cuda):
+    fact, dim = datagen.star_tables(50_000, seed=2)
+    p = Plan()
+    f = p.scan([fact["datekey"], fact["quantity"]], batch_rows=16_384)
+    d = p.filter(p.scan([dim["datekey"], dim["year"]]), Compare(A.EQ, ColumnRef(1, A.INT32), Constant(1993, A.INT32)))
+    res = p.execute(p.join(f, d, [(0, 0, A.EQ)]))
+    got = sorted(zip(res[0][0].tolist(), res[1][0].tolist(), res[2][0].tolist(), res[3][0].tolist()))
+    keep = dim["year"] == 1993
+    wl, wr = oracle.join_pairs([fact["datekey"]], [dim["datekey"][keep]], [(0, 0, A.EQ)])
+    want = sorted(zip(fact["datekey"][wl].tolist(), fact["quantity"][wl].tolist(),
+                      dim["datekey"][keep][wr].tolist(), dim["year"][keep][wr].tolist()))
+    assert got == want
+    x, y = datagen.cross_tables(300, seed=2)
+    p2 = Plan()
+    res2 = p2.execute(p2.cross(p2.scan([x]), p2.scan([y])))
+    assert len(res2[0][0]) == 300 * 300
+    np.testing.assert_array_equal(res2[0][0], np.repeat(x, 300))
+    np.testing.assert_array_equal(res2[1][0], np.tile(y, 300))

@@ -1,0 +1,854 @@
+// C++ operator layer over the yq kernels (see engine.hpp for the mapping to
+// the reference's classes) and its C entry points (include/yq_engine.h).
+#include "engine.hpp"
+
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+
+namespace yq::engine {
+
+static int32_t width_of(int32_t type, int32_t text_width = 16) {
+  switch (type) {
+    case YQ_INT32:
+    case YQ_FLOAT32: return 4;
+    case YQ_INT64:
+    case YQ_DATETIME:
+    case YQ_FLOAT64: return 8;
+    case YQ_BOOL: return 1;
+    default: return text_width;
+  }
+}
+
+// ------------------------------------------------------------------ Batch
+Batch::Batch(std::vector<ColumnPtr> cols, uint64_t n, cudaStream_t s, bool with_nulls)
+    : columns(std::move(cols)), rows(n), location(Device::GPU), stream(s) {
+  data.resize(columns.size(), nullptr);
+  nulls.resize(columns.size(), nullptr);
+  for (size_t c = 0; c < columns.size(); ++c) {
+    const size_t b = std::max<uint64_t>(1, n) * columns[c]->width;
+    check_cuda(cudaMallocAsync(&data[c], b, s), "Batch alloc");
+    if (with_nulls) check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&nulls[c]), std::max<uint64_t>(1, n), s),
+                               "Batch nulls alloc");
+  }
+}
+
+Batch::~Batch() {
+  for (size_t c = 0; c < columns.size(); ++c) {
+    if (location == Device::GPU) {
+      if (data[c]) cudaFreeAsync(data[c], stream);
+      if (nulls[c]) cudaFreeAsync(nulls[c], stream);
+    } else {
+      if (data[c]) cudaFreeHost(data[c]);
+      if (nulls[c]) cudaFreeHost(nulls[c]);
+    }
+  }
+}
+
+uint64_t Batch::bytes() const {
+  uint64_t b = 0;
+  for (size_t c = 0; c < columns.size(); ++c) b += rows * columns[c]->width + (nulls[c] ? rows : 0);
+  return b;
+}
+
+// GPU <-> pinned host (Batch::moveGpuToCpu / moveCpuToGpu, src/batch.cu:28-73).
+void Batch::moveTo(Device target) {
+  if (target == location) return;
+  for (size_t c = 0; c < columns.size(); ++c) {
+    const size_t b = std::max<uint64_t>(1, rows) * columns[c]->width;
+    const size_t nb = std::max<uint64_t>(1, rows);
+    void* p = nullptr;
+    void* q = nullptr;
+    if (target == Device::CPU) {
+      check_cuda(cudaMallocHost(&p, b), "spill alloc");
+      check_cuda(cudaMemcpyAsync(p, data[c], b, cudaMemcpyDeviceToHost, stream), "spill copy");
+      if (nulls[c]) {
+        check_cuda(cudaMallocHost(&q, nb), "spill alloc");
+        check_cuda(cudaMemcpyAsync(q, nulls[c], nb, cudaMemcpyDeviceToHost, stream), "spill copy");
+      }
+      check_cuda(cudaStreamSynchronize(stream), "spill sync");
+      cudaFreeAsync(data[c], stream);
+      if (nulls[c]) cudaFreeAsync(nulls[c], stream);
+    } else {
+      check_cuda(cudaMallocAsync(&p, b, stream), "reload alloc");
+      check_cuda(cudaMemcpyAsync(p, data[c], b, cudaMemcpyHostToDevice, stream), "reload copy");
+      if (nulls[c]) {
+        check_cuda(cudaMallocAsync(&q, nb, stream), "reload alloc");
+        check_cuda(cudaMemcpyAsync(q, nulls[c], nb, cudaMemcpyHostToDevice, stream), "reload copy");
+      }
+      check_cuda(cudaStreamSynchronize(stream), "reload sync");
+      cudaFreeHost(data[c]);
+      if (nulls[c]) cudaFreeHost(nulls[c]);
+    }
+    data[c] = p;
+    nulls[c] = static_cast<uint8_t*>(q);
+  }
+  location = target;
+}
+
+yq_column Batch::column(size_t c) const {
+  return yq_column{data[c], nulls[c], columns[c]->type, columns[c]->width};
+}
+
+yq_batch Batch::view(std::vector<yq_column>& storage) const {
+  storage.clear();
+  for (size_t c = 0; c < columns.size(); ++c) storage.push_back(column(c));
+  return yq_batch{storage.data(), (int32_t)storage.size(), (uint32_t)rows};
+}
+
+// ----------------------------------------------------------- CacheManager
+BatchID CacheManager::putBatch(std::unique_ptr<Batch> b) {
+  const BatchID id = next_++;
+  if (b->location == Device::GPU) gpu_bytes_ += b->bytes();
+  batches_[id] = std::move(b);
+  handleOverflow();
+  return id;
+}
+
+std::unique_ptr<Batch> CacheManager::getBatch(BatchID id) {
+  auto it = batches_.find(id);
+  if (it == batches_.end()) throw Error(YQ_ERR_INVALID_ARG, "getBatch: unknown batch");
+  std::unique_ptr<Batch> b = std::move(it->second);
+  batches_.erase(it);
+  if (b->location == Device::GPU) gpu_bytes_ -= std::min(gpu_bytes_, b->bytes());
+  else b->moveTo(Device::GPU);
+  return b;
+}
+
+Batch& CacheManager::refBatch(BatchID id) { return *batches_.at(id); }
+
+void CacheManager::handleOverflow() {
+  // Oldest device batches (lowest id) move to pinned host memory first.
+  for (auto& kv : batches_) {
+    if (gpu_bytes_ <= budget_) break;
+    Batch& b = *kv.second;
+    if (b.location != Device::GPU) continue;
+    const uint64_t bytes = b.bytes();
+    b.moveTo(Device::CPU);
+    gpu_bytes_ -= std::min(gpu_bytes_, bytes);
+    ++spilled_;
+  }
+}
+
+void ConstantsHolder::assign(const yq_constants* k) {
+  values.clear();
+  text.clear();
+  text_count = text_width = 0;
+  if (!k) return;
+  if (k->count > 0) values.assign(k->values, k->values + k->count);
+  if (k->text_count > 0) {
+    text.assign(k->text, k->text + (size_t)k->text_count * k->text_width);
+    text_count = k->text_count;
+    text_width = k->text_width;
+  }
+}
+
+static ProgramHolder hold(const yq_program* p) {
+  ProgramHolder h;
+  if (p && p->len > 0) h.code.assign(p->code, p->code + p->len);
+  return h;
+}
+
+// ------------------------------------------------------------ ScanOperator
+// Streams host columns to the device in batches. Pageable host memory is
+// first copied into one of two pinned staging sets; the H2D copy runs on the
+// copy stream and the compute stream waits on an event, so the copy of the
+// next batch overlaps the kernels of the current one.
+class ScanOperator final : public Operator {
+ public:
+  ScanOperator(const yq_host_column* cols, int ncols, uint64_t rows, uint32_t batch_rows)
+      : host_(cols, cols + ncols), rows_(rows) {
+    uint64_t row_bytes = 0;
+    for (auto& c : host_) {
+      columns.push_back(std::make_shared<Column>(Column{c.type, c.width}));
+      row_bytes += c.width;
+    }
+    if (batch_rows) {
+      batch_rows_ = batch_rows;
+    } else {  // calculateOptimalBatchSize (include/config.hpp:28-36)
+      const uint64_t per = (4ull << 20) / std::max<uint64_t>(1, row_bytes);
+      batch_rows_ = std::max<uint64_t>(256, per / 256 * 256);
+    }
+    pinned_ = true;
+    for (auto& c : host_) {
+      cudaPointerAttributes a{};
+      if (cudaPointerGetAttributes(&a, c.data) != cudaSuccess || a.type != cudaMemoryTypeHost) pinned_ = false;
+      if (c.nulls && (cudaPointerGetAttributes(&a, c.nulls) != cudaSuccess || a.type != cudaMemoryTypeHost))
+        pinned_ = false;
+    }
+    cudaGetLastError();
+  }
+  ~ScanOperator() override {
+    for (int s = 0; s < 2; ++s) {
+      for (auto* p : stage_[s]) cudaFreeHost(p);
+      if (done_[s]) cudaEventDestroy(done_[s]);
+    }
+  }
+  const char* kind() const override { return "scan"; }
+  void init() override {
+    if (isInitialized_) return;
+    for (int s = 0; s < 2; ++s) {
+      check_cuda(cudaEventCreateWithFlags(&done_[s], cudaEventDisableTiming), "scan event");
+      if (!pinned_) {
+        for (size_t c = 0; c < host_.size(); ++c) {
+          void* p = nullptr;
+          check_cuda(cudaMallocHost(&p, batch_rows_ * host_[c].width + (host_[c].nulls ? batch_rows_ : 0)), "stage");
+          stage_[s].push_back(static_cast<char*>(p));
+        }
+      }
+    }
+    isInitialized_ = true;
+  }
+  BatchID next(CacheManager& cache) override {
+    if (!isInitialized_) init();
+    if (issued_ == 0) {
+      issue();
+      issue();
+    }
+    if (taken_ == issued_) {
+      isFinished = true;
+      return 0;
+    }
+    const int slot = taken_ % 2;
+    std::unique_ptr<Batch> b = std::move(pending_[slot]);
+    check_cuda(cudaStreamWaitEvent(ctx_->compute, done_[slot], 0), "scan wait");
+    b->stream = ctx_->compute;
+    ++taken_;
+    ++ctx_->stats.batches;
+    const BatchID id = cache.putBatch(std::move(b));
+    issue();  // refill the freed slot: its copy overlaps the consumer's kernels
+    return id;
+  }
+
+ private:
+  void issue() {
+    if (pos_ >= rows_) return;
+    const int slot = issued_ % 2;
+    const uint64_t n = std::min<uint64_t>(batch_rows_, rows_ - pos_);
+    bool any_nulls = false;
+    for (auto& c : host_) any_nulls |= c.nulls != nullptr;
+    auto b = std::make_unique<Batch>(columns, n, ctx_->copy, any_nulls);
+    if (!pinned_) check_cuda(cudaEventSynchronize(done_[slot]), "stage reuse");  // staging set free again
+    for (size_t c = 0; c < host_.size(); ++c) {
+      const size_t w = host_[c].width;
+      const char* src = static_cast<const char*>(host_[c].data) + pos_ * w;
+      const uint8_t* nsrc = host_[c].nulls ? host_[c].nulls + pos_ : nullptr;
+      if (!pinned_) {
+        memcpy(stage_[slot][c], src, n * w);
+        if (nsrc) memcpy(stage_[slot][c] + batch_rows_ * w, nsrc, n);
+        src = stage_[slot][c];
+        if (nsrc) nsrc = reinterpret_cast<uint8_t*>(stage_[slot][c] + batch_rows_ * w);
+      }
+      check_cuda(cudaMemcpyAsync(b->data[c], src, n * w, cudaMemcpyHostToDevice, ctx_->copy), "scan H2D");
+      ctx_->stats.h2d_bytes += n * w;
+      if (b->nulls[c]) {
+        if (nsrc) {
+          check_cuda(cudaMemcpyAsync(b->nulls[c], nsrc, n, cudaMemcpyHostToDevice, ctx_->copy), "scan H2D");
+          ctx_->stats.h2d_bytes += n;
+        } else {
+          check_cuda(cudaMemsetAsync(b->nulls[c], 0, n, ctx_->copy), "scan nulls");
+        }
+      }
+    }
+    check_cuda(cudaEventRecord(done_[slot], ctx_->copy), "scan record");
+    pending_[slot] = std::move(b);
+    pos_ += n;
+    ++issued_;
+  }
+
+  std::vector<yq_host_column> host_;
+  uint64_t rows_, batch_rows_ = 0, pos_ = 0;
+  bool pinned_ = false;
+  std::vector<char*> stage_[2];
+  cudaEvent_t done_[2] = {nullptr, nullptr};
+  std::unique_ptr<Batch> pending_[2];
+  uint64_t issued_ = 0, taken_ = 0;
+};
+
+static bool has_nulls(const Batch& b) {
+  for (auto* n : b.nulls)
+    if (n) return true;
+  return false;
+}
+
+// ---------------------------------------------------------- FilterOperator
+class FilterOperator final : public Operator {
+ public:
+  FilterOperator(std::unique_ptr<Operator> child, const yq_program* pred, const yq_constants* k) : pred_(hold(pred)) {
+    children_.push_back(std::move(child));
+    consts_.assign(k);
+  }
+  const char* kind() const override { return "filter"; }
+  void init() override {
+    if (isInitialized_) return;
+    children_[0]->init();
+    columns = children_[0]->columns;
+    isInitialized_ = true;
+  }
+  BatchID next(CacheManager& cache) override {
+    if (!isInitialized_) init();
+    if (isFinished) return 0;
+    const BatchID id = children_[0]->next(cache);
+    if (!id) {
+      isFinished = true;
+      return 0;
+    }
+    auto in = cache.getBatch(id);
+    if (pred_.code.empty()) return cache.putBatch(std::move(in));
+    std::vector<yq_column> iv;
+    const yq_batch v = in->view(iv);
+    auto out = std::make_unique<Batch>(columns, in->rows, ctx_->compute, has_nulls(*in));
+    std::vector<yq_projection> proj(columns.size());
+    std::vector<yq_column> ov(columns.size());
+    for (size_t c = 0; c < columns.size(); ++c) {
+      proj[c].column = (int32_t)c;
+      ov[c] = out->column(c);
+    }
+    const yq_program p = pred_.prog();
+    const yq_constants k = consts_.get();
+    uint32_t count = 0;
+    check(yq_filter_project(&v, &p, &k, proj.data(), (int32_t)proj.size(), ov.data(), (uint32_t)in->rows, nullptr,
+                            &count, nullptr, 0, ctx_->compute),
+          "FilterOperator");
+    out->rows = count;
+    return cache.putBatch(std::move(out));
+  }
+  // AggregateOperator absorbs this node: its predicate is evaluated inside the
+  // aggregate kernel on the child's batches instead of compacting them first.
+  const ProgramHolder& predicate() const { return pred_; }
+  const ConstantsHolder& constants() const { return consts_; }
+
+ private:
+  ProgramHolder pred_;
+  ConstantsHolder consts_;
+};
+
+// ------------------------------------------------------ ProjectionOperator
+class ProjectionOperator final : public Operator {
+ public:
+  ProjectionOperator(std::unique_ptr<Operator> child, const yq_projection* proj, int nproj, const yq_constants* k) {
+    children_.push_back(std::move(child));
+    consts_.assign(k);
+    for (int i = 0; i < nproj; ++i) {
+      proj_.push_back(proj[i]);
+      progs_.push_back(hold(&proj[i].program));
+    }
+  }
+  const char* kind() const override { return "projection"; }
+  void init() override {
+    if (isInitialized_) return;
+    children_[0]->init();
+    for (auto& p : proj_) {
+      if (p.column >= 0) columns.push_back(children_[0]->columns.at(p.column));
+      else columns.push_back(std::make_shared<Column>(Column{p.out_type, width_of(p.out_type)}));
+    }
+    isInitialized_ = true;
+  }
+  BatchID next(CacheManager& cache) override {
+    if (!isInitialized_) init();
+    if (isFinished) return 0;
+    const BatchID id = children_[0]->next(cache);
+    if (!id) {
+      isFinished = true;
+      return 0;
+    }
+    auto in = cache.getBatch(id);
+    std::vector<yq_column> iv;
+    const yq_batch v = in->view(iv);
+    auto out = std::make_unique<Batch>(columns, in->rows, ctx_->compute, true);
+    std::vector<yq_projection> proj = proj_;
+    for (size_t i = 0; i < proj.size(); ++i) proj[i].program = progs_[i].prog();
+    std::vector<yq_column> ov;
+    for (size_t c = 0; c < columns.size(); ++c) ov.push_back(out->column(c));
+    const yq_program none{nullptr, 0};
+    const yq_constants k = consts_.get();
+    uint32_t count = 0;
+    check(yq_filter_project(&v, &none, &k, proj.data(), (int32_t)proj.size(), ov.data(), (uint32_t)in->rows, nullptr,
+                            &count, nullptr, 0, ctx_->compute),
+          "ProjectionOperator");
+    out->rows = count;
+    return cache.putBatch(std::move(out));
+  }
+
+ private:
+  std::vector<yq_projection> proj_;
+  std::vector<ProgramHolder> progs_;
+  ConstantsHolder consts_;
+};
+
+// ------------------------------------------------------- AggregateOperator
+class AggregateOperator final : public Operator {
+ public:
+  AggregateOperator(std::unique_ptr<Operator> child, const yq_agg_spec* aggs, int nagg, const yq_constants* k) {
+    children_.push_back(std::move(child));
+    consts_.assign(k);
+    for (int i = 0; i < nagg; ++i) {
+      aggs_.push_back(aggs[i]);
+      progs_.push_back(hold(&aggs[i].input));
+    }
+  }
+  const char* kind() const override { return "aggregate"; }
+  void init() override {
+    if (isInitialized_) return;
+    Operator* c = children_[0].get();
+    c->init();
+    source_ = c;
+    if (auto* f = dynamic_cast<FilterOperator*>(c)) {
+      // Fuse WHERE into the aggregate: merge the filter's constants in front
+      // of ours and shift our constant indices.
+      pred_ = f->predicate();
+      ConstantsHolder merged = f->constants();
+      const int shift = (int)merged.values.size();
+      const int tshift = merged.text_count;
+      if (!consts_.text.empty() && !merged.text.empty() && consts_.text_width != merged.text_width)
+        throw Error(YQ_ERR_UNSUPPORTED, "AggregateOperator: text constant widths differ");
+      merged.values.insert(merged.values.end(), consts_.values.begin(), consts_.values.end());
+      merged.text.insert(merged.text.end(), consts_.text.begin(), consts_.text.end());
+      merged.text_count += consts_.text_count;
+      if (!merged.text_width) merged.text_width = consts_.text_width;
+      for (auto& p : progs_)
+        for (auto& I : p.code) {
+          const bool num = I.op == YQ_OP_CONST || I.op == YQ_OP_ARITH_CONST ||
+                           ((I.op == YQ_OP_CMP_COL_CONST || I.op == YQ_OP_AND_CMP_COL_CONST) && I.type != YQ_TEXT);
+          const bool txt = (I.op == YQ_OP_CMP_COL_CONST || I.op == YQ_OP_AND_CMP_COL_CONST) && I.type == YQ_TEXT;
+          if (num) I.imm += shift;
+          if (txt) I.imm += tshift;
+        }
+      consts_ = merged;
+      source_ = f->child(0);
+    }
+    for (auto& a : aggs_) {
+      int32_t t;
+      switch (a.kind) {
+        case YQ_AGG_COUNT_STAR:
+        case YQ_AGG_COUNT: t = YQ_INT64; break;
+        case YQ_AGG_AVG: t = YQ_FLOAT64; break;
+        case YQ_AGG_SUM: t = (a.input_type == YQ_FLOAT32 || a.input_type == YQ_FLOAT64) ? YQ_FLOAT64 : YQ_INT64; break;
+        default: t = a.input_type;
+      }
+      columns.push_back(std::make_shared<Column>(Column{t, width_of(t)}));
+    }
+    isInitialized_ = true;
+  }
+  BatchID next(CacheManager& cache) override {
+    if (!isInitialized_) init();
+    if (isFinished) return 0;
+    isFinished = true;
+    const int nagg = (int)aggs_.size();
+    std::vector<yq_agg_spec> specs = aggs_;
+    for (int i = 0; i < nagg; ++i) specs[i].input = progs_[i].prog();
+    void* state = nullptr;
+    check_cuda(cudaMallocAsync(&state, std::max<size_t>(256, yq_agg_state_bytes(nagg)), ctx_->compute), "agg state");
+    check(yq_agg_state_init(state, specs.data(), nagg, ctx_->compute), "yq_agg_state_init");
+    const yq_program p = pred_.prog();
+    const yq_constants k = consts_.get();
+    for (BatchID id = source_->next(cache); id; id = source_->next(cache)) {
+      auto in = cache.getBatch(id);
+      std::vector<yq_column> iv;
+      const yq_batch v = in->view(iv);
+      check(yq_filter_aggregate(&v, &p, &k, specs.data(), nagg, state, nullptr, 0, ctx_->compute),
+            "AggregateOperator");
+    }
+    std::vector<yq_agg_result> res(nagg);
+    check(yq_agg_state_read(state, specs.data(), nagg, res.data(), ctx_->compute), "yq_agg_state_read");
+    cudaFreeAsync(state, ctx_->compute);
+    // One result row (SQL semantics over an empty input: counts 0, others NULL).
+    auto out = std::make_unique<Batch>(columns, 1, ctx_->compute, true);
+    for (int i = 0; i < nagg; ++i) {
+      unsigned char cell[8] = {0};
+      const int32_t t = columns[i]->type;
+      const yq_agg_result& r = res[i];
+      switch (t) {
+        case YQ_INT32: { int32_t v = (int32_t)r.i; memcpy(cell, &v, 4); break; }
+        case YQ_FLOAT32: { float v = (float)r.f; memcpy(cell, &v, 4); break; }
+        case YQ_FLOAT64: { double v = r.f; memcpy(cell, &v, 8); break; }
+        default: { int64_t v = r.i; memcpy(cell, &v, 8); break; }
+      }
+      uint8_t nul = (uint8_t)r.is_null;
+      check_cuda(cudaMemcpyAsync(out->data[i], cell, columns[i]->width, cudaMemcpyHostToDevice, ctx_->compute),
+                 "agg result");
+      check_cuda(cudaMemcpyAsync(out->nulls[i], &nul, 1, cudaMemcpyHostToDevice, ctx_->compute), "agg result");
+      check_cuda(cudaStreamSynchronize(ctx_->compute), "agg result");
+    }
+    return cache.putBatch(std::move(out));
+  }
+
+ private:
+  std::vector<yq_agg_spec> aggs_;
+  std::vector<ProgramHolder> progs_;
+  ProgramHolder pred_;
+  ConstantsHolder consts_;
+  Operator* source_ = nullptr;
+};
+
+// ----------------------------------------------------------- OrderOperator
+// Every child batch becomes a run (sorted by the segmented radix sort in one
+// set of launches), then runs merge pairwise by merge path until one remains
+// (OrderOperator::firstPass / merge_all_sorted, order_operator.hpp:89-193).
+class OrderOperator final : public Operator {
+ public:
+  OrderOperator(std::unique_ptr<Operator> child, int key, int desc, int nulls_first)
+      : key_(key), desc_(desc), nulls_first_(nulls_first) {
+    children_.push_back(std::move(child));
+  }
+  const char* kind() const override { return "order"; }
+  void init() override {
+    if (isInitialized_) return;
+    children_[0]->init();
+    columns = children_[0]->columns;
+    if (key_ < 0 || key_ >= (int)columns.size()) throw Error(YQ_ERR_INVALID_ARG, "OrderOperator key");
+    isInitialized_ = true;
+  }
+  BatchID next(CacheManager& cache) override {
+    if (!isInitialized_) init();
+    if (isFinished) return 0;
+    isFinished = true;
+    std::vector<std::unique_ptr<Batch>> runs;
+    uint64_t total = 0;
+    bool nullable = false;
+    for (BatchID id = children_[0]->next(cache); id; id = children_[0]->next(cache)) {
+      auto b = cache.getBatch(id);
+      if (b->rows == 0) continue;
+      total += b->rows;
+      nullable |= has_nulls(*b);
+      runs.push_back(std::move(b));
+    }
+    if (runs.empty()) return 0;
+    if (total > 0xffffffffull) throw Error(YQ_ERR_UNSUPPORTED, "OrderOperator: more than 2^32 rows");
+    cudaStream_t s = ctx_->compute;
+    // gather the runs back to back (the merge path reads contiguous runs)
+    auto all = std::make_unique<Batch>(columns, total, s, nullable);
+    std::vector<uint32_t> offs{0};
+    for (auto& r : runs) {
+      const uint64_t o = offs.back();
+      for (size_t c = 0; c < columns.size(); ++c) {
+        const size_t w = columns[c]->width;
+        check_cuda(cudaMemcpyAsync((char*)all->data[c] + o * w, r->data[c], r->rows * w, cudaMemcpyDeviceToDevice, s),
+                   "order concat");
+        if (all->nulls[c]) {
+          if (r->nulls[c])
+            check_cuda(cudaMemcpyAsync(all->nulls[c] + o, r->nulls[c], r->rows, cudaMemcpyDeviceToDevice, s), "concat");
+          else
+            check_cuda(cudaMemsetAsync(all->nulls[c] + o, 0, r->rows, s), "concat");
+        }
+      }
+      offs.push_back((uint32_t)(o + r->rows));
+    }
+    runs.clear();
+    std::vector<yq_column> av;
+    all->view(av);
+    uint32_t* perm = nullptr;
+    check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&perm), total * sizeof(uint32_t), s), "perm");
+    check(yq_sort_segments(&av[key_], (uint32_t)total, offs.data(), (int32_t)offs.size() - 1, desc_, nulls_first_,
+                           perm, nullptr, nullptr, 0, s),
+          "OrderOperator sort");
+    auto a = std::make_unique<Batch>(columns, total, s, nullable);
+    std::vector<yq_column> bv;
+    a->view(bv);
+    check(yq_gather(av.data(), (int32_t)av.size(), perm, (uint32_t)total, bv.data(), s), "OrderOperator gather");
+    cudaFreeAsync(perm, s);
+    // merge levels, ping-pong between `a` and `all`
+    Batch* src = a.get();
+    Batch* dst = all.get();
+    while (offs.size() > 2) {
+      std::vector<yq_column> sv, dv;
+      src->view(sv);
+      dst->view(dv);
+      check(yq_merge_pass(sv.data(), (int32_t)sv.size(), key_, desc_, nulls_first_, offs.data(),
+                          (int32_t)offs.size() - 1, dv.data(), nullptr, 0, s),
+            "OrderOperator merge");
+      std::vector<uint32_t> next_offs;
+      for (size_t i = 0; i + 1 < offs.size(); i += 2) next_offs.push_back(offs[i]);
+      next_offs.push_back(offs.back());
+      offs.swap(next_offs);
+      std::swap(src, dst);
+    }
+    std::unique_ptr<Batch> result = (src == a.get()) ? std::move(a) : std::move(all);
+    return cache.putBatch(std::move(result));
+  }
+
+ private:
+  int key_, desc_, nulls_first_;
+};
+
+// ---------------------------------------- JoinOperator / CrossProductOperator
+// All left batches are cached first; then every right batch meets every left
+// batch (JoinOperator::next, join_operator.hpp:36-100). Each pair of batches
+// yields one output batch with all left columns followed by all right columns.
+class JoinOperator final : public Operator {
+ public:
+  JoinOperator(std::unique_ptr<Operator> l, std::unique_ptr<Operator> r, const yq_join_cond* conds, int ncond)
+      : conds_(conds, conds + ncond) {
+    children_.push_back(std::move(l));
+    children_.push_back(std::move(r));
+  }
+  const char* kind() const override { return conds_.empty() ? "cross_product" : "join"; }
+  void init() override {
+    if (isInitialized_) return;
+    children_[0]->init();
+    children_[1]->init();
+    columns = children_[0]->columns;
+    columns.insert(columns.end(), children_[1]->columns.begin(), children_[1]->columns.end());
+    isInitialized_ = true;
+  }
+  BatchID next(CacheManager& cache) override {
+    if (!isInitialized_) init();
+    if (isFinished) return 0;
+    if (!cached_) {
+      for (BatchID id = children_[0]->next(cache); id; id = children_[0]->next(cache)) left_.push_back(id);
+      cached_ = true;
+    }
+    for (;;) {
+      if (!right_ || li_ >= left_.size()) {
+        if (right_) right_.reset();
+        const BatchID rid = children_[1]->next(cache);
+        if (!rid || left_.empty()) {
+          isFinished = true;
+          return 0;
+        }
+        right_ = cache.getBatch(rid);
+        li_ = 0;
+      }
+      auto lb = cache.getBatch(left_[li_]);
+      BatchID out = join_pair(*lb, *right_, cache);
+      left_[li_] = cache.putBatch(std::move(lb));
+      ++li_;
+      if (out) return out;
+    }
+  }
+
+ private:
+  BatchID join_pair(const Batch& l, const Batch& r, CacheManager& cache) {
+    std::vector<yq_column> lv, rv;
+    const yq_batch L = l.view(lv), R = r.view(rv);
+    std::vector<yq_join_output> outs;
+    for (size_t c = 0; c < l.columns.size(); ++c) outs.push_back({0, (int32_t)c});
+    for (size_t c = 0; c < r.columns.size(); ++c) outs.push_back({1, (int32_t)c});
+    const bool nullable = has_nulls(l) || has_nulls(r);
+    uint64_t cap = conds_.empty() ? l.rows * r.rows : std::max<uint64_t>(1, l.rows * 2);
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      auto out = std::make_unique<Batch>(columns, cap, ctx_->compute, nullable);
+      std::vector<yq_column> ov;
+      out->view(ov);
+      uint64_t count = 0;
+      const int st = yq_join_project(&L, &R, conds_.data(), (int32_t)conds_.size(), outs.data(), (int32_t)outs.size(),
+                                     ov.data(), cap, &count, nullptr, 0, ctx_->compute);
+      if (st == YQ_ERR_CAPACITY) {
+        cap = count;
+        continue;
+      }
+      check(st, "JoinOperator");
+      if (count == 0) return 0;
+      out->rows = count;
+      return cache.putBatch(std::move(out));
+    }
+    throw Error(YQ_ERR_CAPACITY, "JoinOperator");
+  }
+
+  std::vector<yq_join_cond> conds_;
+  std::vector<BatchID> left_;
+  bool cached_ = false;
+  std::unique_ptr<Batch> right_;
+  size_t li_ = 0;
+};
+
+}  // namespace yq::engine
+
+// ================================================================== C API
+using namespace yq::engine;
+
+struct yq_plan {
+  std::vector<std::unique_ptr<Operator>> owned;  // nodes not yet attached to a parent
+  std::vector<Operator*> nodes;
+  ExecContext ctx;
+  uint64_t budget;
+};
+
+struct yq_result {
+  uint64_t rows = 0;
+  std::vector<yq_host_column> cols;
+  std::vector<void*> bufs;
+  ~yq_result() {
+    for (void* p : bufs) cudaFreeHost(p);
+  }
+};
+
+namespace {
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const Error& e) {
+    return -e.status;
+  } catch (const std::exception&) {
+    return -YQ_ERR_INVALID_ARG;
+  }
+}
+
+std::unique_ptr<Operator> take(yq_plan* p, int id) {
+  if (id < 0 || id >= (int)p->nodes.size()) throw Error(YQ_ERR_INVALID_ARG, "unknown node");
+  for (auto& o : p->owned)
+    if (o.get() == p->nodes[id]) {
+      std::unique_ptr<Operator> r = std::move(o);
+      p->owned.erase(std::remove(p->owned.begin(), p->owned.end(), nullptr), p->owned.end());
+      return r;
+    }
+  throw Error(YQ_ERR_INVALID_ARG, "node already has a parent");
+}
+
+int add(yq_plan* p, std::unique_ptr<Operator> op) {
+  p->nodes.push_back(op.get());
+  p->owned.push_back(std::move(op));
+  return (int)p->nodes.size() - 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+yq_plan* yq_plan_create(uint64_t gpu_budget_bytes) {
+  auto* p = new yq_plan();
+  p->budget = gpu_budget_bytes ? gpu_budget_bytes : (1ull << 30);
+  if (cudaStreamCreateWithFlags(&p->ctx.compute, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&p->ctx.copy, cudaStreamNonBlocking) != cudaSuccess) {
+    delete p;
+    return nullptr;
+  }
+  return p;
+}
+
+void yq_plan_destroy(yq_plan* p) {
+  if (!p) return;
+  cudaStreamSynchronize(p->ctx.compute);
+  cudaStreamSynchronize(p->ctx.copy);
+  p->owned.clear();
+  cudaStreamDestroy(p->ctx.compute);
+  cudaStreamDestroy(p->ctx.copy);
+  delete p;
+}
+
+int yq_plan_scan(yq_plan* p, const yq_host_column* cols, int32_t ncols, uint64_t rows, uint32_t batch_rows) {
+  if (!p || !cols || ncols <= 0 || ncols > YQ_MAX_BATCH_COLUMNS) return -YQ_ERR_INVALID_ARG;
+  return guarded([&] { return add(p, std::make_unique<ScanOperator>(cols, ncols, rows, batch_rows)); });
+}
+
+int yq_plan_filter(yq_plan* p, int32_t child, const yq_program* pred, const yq_constants* k) {
+  if (!p) return -YQ_ERR_INVALID_ARG;
+  return guarded([&] { return add(p, std::make_unique<FilterOperator>(take(p, child), pred, k)); });
+}
+
+int yq_plan_project(yq_plan* p, int32_t child, const yq_projection* proj, int32_t nproj, const yq_constants* k) {
+  if (!p || !proj || nproj <= 0) return -YQ_ERR_INVALID_ARG;
+  return guarded([&] { return add(p, std::make_unique<ProjectionOperator>(take(p, child), proj, nproj, k)); });
+}
+
+int yq_plan_aggregate(yq_plan* p, int32_t child, const yq_agg_spec* aggs, int32_t nagg, const yq_constants* k) {
+  if (!p || !aggs || nagg <= 0 || nagg > YQ_MAX_AGGREGATES) return -YQ_ERR_INVALID_ARG;
+  return guarded([&] { return add(p, std::make_unique<AggregateOperator>(take(p, child), aggs, nagg, k)); });
+}
+
+int yq_plan_order(yq_plan* p, int32_t child, int32_t key, int32_t desc, int32_t nulls_first) {
+  if (!p) return -YQ_ERR_INVALID_ARG;
+  return guarded([&] { return add(p, std::make_unique<OrderOperator>(take(p, child), key, desc, nulls_first)); });
+}
+
+int yq_plan_join(yq_plan* p, int32_t left, int32_t right, const yq_join_cond* conds, int32_t ncond) {
+  if (!p || ncond <= 0 || !conds) return -YQ_ERR_INVALID_ARG;
+  return guarded([&] {
+    auto l = take(p, left);
+    auto r = take(p, right);
+    return add(p, std::make_unique<JoinOperator>(std::move(l), std::move(r), conds, ncond));
+  });
+}
+
+int yq_plan_cross(yq_plan* p, int32_t left, int32_t right) {
+  if (!p) return -YQ_ERR_INVALID_ARG;
+  return guarded([&] {
+    auto l = take(p, left);
+    auto r = take(p, right);
+    return add(p, std::make_unique<JoinOperator>(std::move(l), std::move(r), nullptr, 0));
+  });
+}
+
+int yq_plan_execute(yq_plan* p, int32_t root, yq_result** out) {
+  if (!p || !out || root < 0 || root >= (int)p->nodes.size()) return YQ_ERR_INVALID_ARG;
+  const int st = guarded([&]() -> int {
+    Operator* op = p->nodes[root];
+    p->ctx.stats = yq_plan_stats{};
+    op->setContext(&p->ctx);
+    CacheManager cache(p->budget);
+    cudaEvent_t e0, e1;
+    check_cuda(cudaEventCreate(&e0), "event");
+    check_cuda(cudaEventCreate(&e1), "event");
+    check_cuda(cudaEventRecord(e0, p->ctx.compute), "event");
+    op->init();
+    std::vector<std::unique_ptr<Batch>> batches;
+    uint64_t rows = 0;
+    for (BatchID id = op->next(cache); id; id = op->next(cache)) {
+      auto b = cache.getBatch(id);
+      rows += b->rows;
+      batches.push_back(std::move(b));
+    }
+    auto res = std::make_unique<yq_result>();
+    res->rows = rows;
+    for (size_t c = 0; c < op->columns.size(); ++c) {
+      const size_t w = op->columns[c]->width;
+      void* buf = nullptr;
+      void* nbuf = nullptr;
+      check_cuda(cudaMallocHost(&buf, std::max<uint64_t>(1, rows) * w), "result");
+      res->bufs.push_back(buf);
+      bool nullable = false;
+      for (auto& b : batches) nullable |= b->nulls[c] != nullptr;
+      if (nullable) {
+        check_cuda(cudaMallocHost(&nbuf, std::max<uint64_t>(1, rows)), "result");
+        res->bufs.push_back(nbuf);
+      }
+      uint64_t o = 0;
+      for (auto& b : batches) {
+        check_cuda(cudaMemcpyAsync((char*)buf + o * w, b->data[c], b->rows * w, cudaMemcpyDeviceToHost, p->ctx.compute),
+                   "result D2H");
+        p->ctx.stats.d2h_bytes += b->rows * w;
+        if (nbuf) {
+          if (b->nulls[c])
+            check_cuda(cudaMemcpyAsync((char*)nbuf + o, b->nulls[c], b->rows, cudaMemcpyDeviceToHost, p->ctx.compute),
+                       "result D2H");
+          else
+            memset((char*)nbuf + o, 0, b->rows);  // host memory: no device work
+        }
+        o += b->rows;
+      }
+      res->cols.push_back(yq_host_column{buf, static_cast<uint8_t*>(nbuf), op->columns[c]->type, (int32_t)w});
+    }
+    check_cuda(cudaEventRecord(e1, p->ctx.compute), "event");
+    check_cuda(cudaStreamSynchronize(p->ctx.compute), "execute");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    p->ctx.stats.compute_ms = ms;
+    p->ctx.stats.spilled_batches = cache.spilled();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    batches.clear();
+    *out = res.release();
+    return YQ_OK;
+  });
+  return st < 0 ? -st : st;
+}
+
+uint64_t yq_result_rows(const yq_result* r) { return r ? r->rows : 0; }
+int32_t yq_result_ncols(const yq_result* r) { return r ? (int32_t)r->cols.size() : 0; }
+int yq_result_column(const yq_result* r, int32_t c, yq_host_column* out) {
+  if (!r || !out || c < 0 || c >= (int32_t)r->cols.size()) return YQ_ERR_INVALID_ARG;
+  *out = r->cols[c];
+  return YQ_OK;
+}
+void yq_result_destroy(yq_result* r) { delete r; }
+
+int yq_plan_stats_read(const yq_plan* p, yq_plan_stats* out) {
+  if (!p || !out) return YQ_ERR_INVALID_ARG;
+  *out = p->ctx.stats;
+  return YQ_OK;
+}
+
+}  // extern "C"
