@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--mode", default="outofcore", choices=["outofcore", "incore"])
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-ops", action="store_true", help="skip the other operators' workloads")
     return p.parse_args()
 
 
@@ -151,10 +152,9 @@ class OrderByJob:
             self.offsets.append(self.offsets[-1] + c)
         self.out = [DeviceBatch([DeviceColumn.empty(c.type, self.rows, c.width if c.type == A.TEXT else None)
                                  for c in self.table.columns]) for _ in range(2)]
-        self.tmp = DeviceBatch([DeviceColumn.empty(c.type, self.rows, c.width if c.type == A.TEXT else None)
-                                for c in self.table.columns])
-        self.scratch = DeviceBatch([DeviceColumn.empty(c.type, self.rows, c.width if c.type == A.TEXT else None)
-                                    for c in self.table.columns])
+        if mode == "outofcore":
+            from yallasql_b200.ops import OrderByRuns
+            self.runs = {k: OrderByRuns(self.table, k, self.offsets) for k in (0, 3)}
         self.perm = torch.empty(self.rows, dtype=torch.int32, device="cuda")
         from yallasql_b200 import ops
         self.ops = ops
@@ -169,16 +169,116 @@ class OrderByJob:
             ops.sort_indices(src.columns[key], desc, out=self.perm, workspace=self.ws)
             ops.gather(src, self.perm, out=out)
             return out
-        # out-of-core: sort every 4 MB batch into a run, then merge runs pairwise
-        ops.sort_segments(src.columns[key], self.offsets, desc, out=self.perm, workspace=self.ws)
-        ops.gather(src, self.perm, out=self.tmp)
-        return ops.merge_runs(self.tmp, key, desc, self.offsets, out, scratch=self.scratch)
+        # out-of-core: sort every 4 MB batch into a run, merge (key, row id)
+        # runs pairwise by merge path, gather the payload once at the end
+        return self.runs[key].run(src, desc, out)
 
     def step(self, src=None):
         src = self.table if src is None else src
         a = self.query(src, 0, True, self.out[0])
         b = self.query(src, 3, False, self.out[1])
         return a, b
+
+
+def _timed(fn, reps: int):
+    """Device ms per call of fn() (CUDA events on the current stream), after one warm call."""
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        fn()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps
+
+
+def operator_suite(lib, peak: float) -> dict:
+    """The other operators of the metric on their config workloads: rows/s and
+    the HBM roofline of each operator's kernel (algorithmic bytes from the
+    library's per-launch accounting / device time)."""
+    import torch
+    from yallasql_b200 import _abi as A, datagen, ops
+    from yallasql_b200.expr import Aggregate, And, Arith, Cast, ColumnRef, Compare, Constant, between
+    dev = lambda a, t: ops.DeviceColumn(torch.from_numpy(np.ascontiguousarray(a)).cuda(), t)
+    out = {}
+
+    def profiled(name, fn, rows, reps, tag):
+        lib.yq_profile_enable(1)
+        lib.yq_profile_read(None, 0, 1)
+        ms = _timed(fn, reps)
+        buf = C.create_string_buffer(1 << 14)
+        lib.yq_profile_read(buf, len(buf), 1)
+        lib.yq_profile_enable(0)
+        prof = json.loads(buf.value.decode() or "{}")
+        k = prof.get(tag, {})
+        entry = {"rows": rows, "ms": round(ms, 4), "rows_per_s": rows / (ms / 1e3)}
+        if k.get("launches"):
+            per_ms = k["ms"] / k["launches"]
+            gbs = k["units"] / k["launches"] / (per_ms / 1e3) / 1e9
+            entry.update({"kernel": tag, "kernel_ms": round(per_ms, 4), "achieved_gbs": round(gbs, 1),
+                          "frac_of_measured_hbm": round(gbs / peak, 4),
+                          "algorithmic_bytes_per_launch": k["units"] / k["launches"]})
+        out[name] = entry
+
+    price, qty, disc, cat = (ColumnRef(0, A.FLOAT32), ColumnRef(1, A.INT32), ColumnRef(2, A.INT32),
+                             ColumnRef(3, A.TEXT))
+    pred = And(between(disc, Constant(1, A.INT32), Constant(3, A.INT32)), Compare(A.LT, qty, Constant(25, A.INT32)),
+               Compare(A.NE, cat, Constant(datagen.EXCLUDED_CATEGORY, A.TEXT)))
+    aggs = [Aggregate(A.AGG_SUM, Arith(A.MUL, price, Cast(disc, A.FLOAT32))), Aggregate(A.AGG_COUNT_STAR),
+            Aggregate(A.AGG_MIN, price), Aggregate(A.AGG_MAX, price)]
+    for rows, name in ((1_000_000, "filter_aggregate_1M"), (64_000_000, "filter_aggregate_64M")):
+        t = datagen.sales_table(rows, seed=0)
+        b = ops.DeviceBatch([dev(t["price"], A.FLOAT32), dev(t["qty"], A.INT32), dev(t["discount"], A.INT32),
+                             dev(t["category"], A.TEXT)])
+        plan = ops.AggPlan([A.FLOAT32, A.INT32, A.INT32, A.TEXT], pred, aggs)
+        st = ops.AggState(aggs)
+        ws = torch.empty(lib.yq_filter_aggregate_workspace_size(rows, len(aggs)), dtype=torch.uint8, device="cuda")
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if rows <= 4_000_000 else None
+
+        def fa():
+            if flush is not None:
+                flush.zero_()  # 256 MB write evicts the 28 MB table from L2 between reps
+            plan.run(b, st, workspace=ws)
+        profiled(name, fa, rows, 10, "filter_aggregate")
+        if rows == 64_000_000:
+            sel = [3, 0, Arith(A.MUL, price, Cast(disc, A.FLOAT32))]
+            pplan = ops.ProjectPlan([A.FLOAT32, A.INT32, A.INT32, A.TEXT], [4, 4, 4, 16], pred, sel)
+            profiled("filter_project_64M", lambda: pplan.run(b, with_nulls=False), rows, 5, "filter_project")
+        del b, t
+    fact, dim = datagen.star_tables(60_000_000, seed=2)
+    fb = ops.DeviceBatch([dev(fact["datekey"], A.INT32), dev(fact["quantity"], A.INT32),
+                          dev(fact["discount"], A.INT32), dev(fact["extendedprice"], A.FLOAT32)])
+    db = ops.DeviceBatch([dev(dim["datekey"], A.INT32), dev(dim["year"], A.INT32), dev(dim["month"], A.INT32)])
+    jp = ops.JoinAggPlan([A.INT32] * 3 + [A.FLOAT32], [A.INT32] * 3,
+                         And(between(ColumnRef(2, A.INT32), Constant(1, A.INT32), Constant(3, A.INT32)),
+                             Compare(A.LT, ColumnRef(1, A.INT32), Constant(25, A.INT32))), 0,
+                         Compare(A.EQ, ColumnRef(1, A.INT32), Constant(1993, A.INT32)), 0,
+                         [Aggregate(A.AGG_SUM, Arith(A.MUL, ColumnRef(3, A.FLOAT32),
+                                                     Cast(ColumnRef(2, A.INT32), A.FLOAT32)))])
+    jst = ops.AggState(jp.aggs)
+    profiled("star_join_aggregate_60M", lambda: jp.run(fb, db, jst), 60_000_000, 5, "join_aggregate")
+    del fb, fact
+    x, y = datagen.cross_tables(20_000, seed=2)
+    xb, yb = ops.DeviceBatch([dev(x, A.INT32)]), ops.DeviceBatch([dev(y, A.INT32)])
+    res = ops.join_project(xb, yb, [(0, 0, A.LT)], [(0, 0), (1, 0)])
+    pairs = res.rows
+    outs_c = (A.JoinOutput * 2)(A.JoinOutput(0, 0), A.JoinOutput(1, 0))
+    oc = (A.Column * 2)(*[c.c() for c in res.columns])
+    lbc, lk = xb.c()
+    rbc, rk = yb.c()
+    conds = (A.JoinCond * 1)(A.JoinCond(0, 0, A.LT))
+    n64 = C.c_uint64()
+    profiled("cross_product_lt_20Kx20K",
+             lambda: lib.yq_join_project(C.byref(lbc), C.byref(rbc), conds, 1, outs_c, 2, oc, pairs, C.byref(n64),
+                                         None, 0, torch.cuda.current_stream().cuda_stream),
+             pairs, 5, "join_nested_loop")
+    out["cross_product_lt_20Kx20K"]["output_pairs"] = pairs
+    out["cross_product_lt_20Kx20K"]["output_bytes_per_s"] = pairs * 8 / (out["cross_product_lt_20Kx20K"]["ms"] / 1e3)
+    out["cross_product_lt_20Kx20K"]["frac_of_measured_hbm_output"] = round(
+        pairs * 8 / (out["cross_product_lt_20Kx20K"]["ms"] / 1e3) / 1e9 / peak, 4)
+    return out
 
 
 def run_reference(args, rank: int):
@@ -352,6 +452,10 @@ def main():
             "vs_baseline": None, "dtype": "f32 keys, int64/text/date payload", "data": "synthetic",
             "config": config(args), "roofline": roof, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk.summary(), "kernels": prof, "sorted_ok": ok}
+    if rank == 0 and not args.no_ops:
+        del job
+        torch.cuda.empty_cache()
+        line["operators"] = operator_suite(lib, peak)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args, t)
     if rank == 0:

@@ -46,6 +46,25 @@ def test_outofcore_order_by_equals_stable_sort(cuda, dist, batch):
             np.testing.assert_array_equal(col.data.cpu().numpy(), t[n][perm])
 
 
+@pytest.mark.parametrize("dist", ["uniform", "zipf", "equal"])
+@pytest.mark.parametrize("batch", [116_480, 3_001, 300_000])
+def test_order_by_runs_key_id_path(cuda, dist, batch):
+    """Runs sorted, (key, row id) merged, payload gathered once: same table as one stable sort."""
+    rows = 250_000
+    t = datagen.order_table(rows, seed=2, dist=dist)
+    b = table_batch(t)
+    counts = [batch] * (rows // batch) + ([rows % batch] if rows % batch else [])
+    offs = list(np.concatenate([[0], np.cumsum(counts)]).astype(int))
+    for key, name, desc, ty in ((0, "key", True, None), (3, "d", False, oracle.DATETIME)):
+        job = ops.OrderByRuns(b, key, offs)
+        out = out_like(b)
+        for _ in range(2):  # buffers are reused across calls
+            job.run(b, desc, out)
+            perm = oracle.sort_perm(t[name], desc=desc, type_=ty)
+            for col, n in zip(out.columns, ["key", "id", "txt", "d"]):
+                np.testing.assert_array_equal(col.data.cpu().numpy(), t[n][perm])
+
+
 @pytest.mark.parametrize("nruns", [1, 2, 3, 8, 13])
 @pytest.mark.parametrize("kind", ["i32", "i64", "text16", "f32_nulls"])
 def test_merge_pass_types(cuda, nruns, kind):

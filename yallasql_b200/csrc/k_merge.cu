@@ -36,6 +36,7 @@ struct MergeCol {
   char* dst;
   uint8_t* dst_nulls;
   int32_t width;
+  int32_t vec;  // src and dst aligned to `width`: cells move as one 4/8/16-byte word
 };
 
 struct MergeParams {
@@ -160,6 +161,20 @@ __device__ __forceinline__ void copy_cell(char* dst, const char* src, int width)
       *reinterpret_cast<uint32_t*>(dst + i) = __ldg(reinterpret_cast<const uint32_t*>(src + i));
 }
 
+// Move kMergeItems cells of one column (value type V, widths 4/8/16).
+template <typename V>
+__device__ __forceinline__ void move_items(const MergeCol& mc, const uint32_t (&rows)[kMergeItems], uint32_t out_base) {
+  const V* src = reinterpret_cast<const V*>(mc.src);
+  V* dst = reinterpret_cast<V*>(mc.dst);
+  V v[kMergeItems];
+#pragma unroll
+  for (int i = 0; i < kMergeItems; ++i)
+    if (rows[i] != 0xffffffffu) v[i] = __ldg(src + rows[i]);
+#pragma unroll
+  for (int i = 0; i < kMergeItems; ++i)
+    if (rows[i] != 0xffffffffu) dst[out_base + threadIdx.x + i * kMergeBlock] = v[i];
+}
+
 template <int KW>
 __global__ void __launch_bounds__(kMergeBlock) k_merge_tiles(const __grid_constant__ MergeParams M) {
   extern __shared__ __align__(128) char smem[];
@@ -271,15 +286,38 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_tiles(const __grid_consta
   }
   __syncthreads();
 
-  // Move every column (key included) for the tile's outputs.
+  // Move every column (key included) for the tile's outputs: the source row
+  // of each output is resolved once, then per column all kMergeItems loads
+  // are issued before the (coalesced) stores.
   const uint32_t out_base = p.out0 + k0;
+  uint32_t rows[kMergeItems];
+#pragma unroll
+  for (int i = 0; i < kMergeItems; ++i) {
+    const uint32_t x = threadIdx.x + i * kMergeBlock;
+    rows[i] = 0xffffffffu;
+    if (x < cnt) {
+      const uint32_t s = s_src[x];
+      rows[i] = (s & kFromB) ? p.b0 + j0 + (s & ~kFromB) : p.a0 + i0 + s;
+    }
+  }
   for (int c = 0; c < M.ncols; ++c) {
     const MergeCol& mc = M.c[c];
-    for (uint32_t x = threadIdx.x; x < cnt; x += kMergeBlock) {
-      const uint32_t s = s_src[x];
-      const uint32_t row = (s & kFromB) ? p.b0 + j0 + (s & ~kFromB) : p.a0 + i0 + s;
-      copy_cell(mc.dst + (size_t)(out_base + x) * mc.width, mc.src + (size_t)row * mc.width, mc.width);
-      if (mc.dst_nulls) mc.dst_nulls[out_base + x] = mc.src_nulls ? mc.src_nulls[row] : 0;
+    switch (mc.vec ? mc.width : 0) {
+      case 4: move_items<uint32_t>(mc, rows, out_base); break;
+      case 8: move_items<unsigned long long>(mc, rows, out_base); break;
+      case 16: move_items<uint4>(mc, rows, out_base); break;
+      default:
+#pragma unroll
+        for (int i = 0; i < kMergeItems; ++i)
+          if (rows[i] != 0xffffffffu)
+            copy_cell(mc.dst + (size_t)(out_base + threadIdx.x + i * kMergeBlock) * mc.width,
+                      mc.src + (size_t)rows[i] * mc.width, mc.width);
+    }
+    if (mc.dst_nulls) {
+#pragma unroll
+      for (int i = 0; i < kMergeItems; ++i)
+        if (rows[i] != 0xffffffffu)
+          mc.dst_nulls[out_base + threadIdx.x + i * kMergeBlock] = mc.src_nulls ? mc.src_nulls[rows[i]] : 0;
     }
   }
 }
@@ -361,6 +399,11 @@ int yq_merge_pass(const yq_column* cols, int32_t ncols, int32_t key_col, int32_t
     M.c[c].dst = static_cast<char*>(out[c].data);
     M.c[c].dst_nulls = const_cast<uint8_t*>(out[c].nulls);
     M.c[c].width = cols[c].width;
+    {
+      const int w = cols[c].width;
+      const uintptr_t a = reinterpret_cast<uintptr_t>(cols[c].data) | reinterpret_cast<uintptr_t>(out[c].data);
+      M.c[c].vec = (w == 4 || w == 8 || w == 16) && (a % (uintptr_t)w) == 0;
+    }
     row_bytes += 2.0 * cols[c].width + (out[c].nulls ? 2.0 : 0.0);
   }
   M.ncols = ncols;

@@ -103,15 +103,23 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_histogram(const KeySrc src,
       }
       const uint32_t vb = __ballot_sync(0xffffffffu, valid);
       const int first = __ffs(vb) - 1;
+      // One vote per key: when every valid lane of the warp holds the same key
+      // (all-equal columns, heavy Zipf heads) lane `first` counts them all.
+      // Every lane executes the shuffle (full mask), valid or not.
+      bool same = true;
 #pragma unroll
-      for (int p = 0; p < P; ++p) {
-        const uint32_t d = digit_of<KW, D>(k, p * D);
-        const uint32_t d0 = __shfl_sync(0xffffffffu, d, first);
-        if (__all_sync(0xffffffffu, !valid || d == d0)) {
-          if (lane == first) atomicAdd(&s_hist[p * RADIX + d0], (uint32_t)__popc(vb));
-        } else if (valid) {
-          atomicAdd(&s_hist[p * RADIX + d], 1u);
+      for (int j = 0; j < KW; ++j) {
+        const uint32_t kf = __shfl_sync(0xffffffffu, k[j], first < 0 ? 0 : first);
+        same &= (!valid || k[j] == kf);
+      }
+      if (__all_sync(0xffffffffu, same)) {
+        if (lane == first) {
+#pragma unroll
+          for (int p = 0; p < P; ++p) atomicAdd(&s_hist[p * RADIX + digit_of<KW, D>(k, p * D)], (uint32_t)__popc(vb));
         }
+      } else if (valid) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) atomicAdd(&s_hist[p * RADIX + digit_of<KW, D>(k, p * D)], 1u);
       }
     }
   }
@@ -140,7 +148,7 @@ struct SweepParams {
 };
 
 template <int KW, int D, int ITEMS>
-__global__ void __launch_bounds__(kSortBlock) k_sort_onesweep(const __grid_constant__ SweepParams S) {
+__global__ void __launch_bounds__(kSortBlock, 3) k_sort_onesweep(const __grid_constant__ SweepParams S) {
   constexpr int RADIX = 1 << D;
   constexpr int NW = kSortBlock / 32;
   constexpr uint32_t TILE = kSortBlock * ITEMS;
@@ -173,7 +181,6 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_onesweep(const __grid_const
   // 1. load (warp-striped: element = r0 + warp*ITEMS*32 + k*32 + lane)
   uint32_t key[ITEMS][KW];
   uint32_t val[ITEMS];
-  uint32_t dig[ITEMS];
   uint32_t rank[ITEMS];
 #pragma unroll
   for (int k = 0; k < ITEMS; ++k) {
@@ -204,12 +211,10 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_onesweep(const __grid_const
         make_key<KW>(S.src, row, key[k]);
         val[k] = row;
       }
-      dig[k] = digit_of<KW, D>(key[k], shift);
     } else {
 #pragma unroll
       for (int j = 0; j < KW; ++j) key[k][j] = 0u;
       val[k] = 0u;
-      dig[k] = 0u;
     }
   }
 
@@ -220,17 +225,18 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_onesweep(const __grid_const
     const uint32_t off = (uint32_t)(warp * ITEMS * 32 + k * 32 + lane);
     const bool valid = off < tile_n;
     uint32_t peers = __ballot_sync(0xffffffffu, valid);
+    const uint32_t dk = digit_of<KW, D>(key[k], shift);
 #pragma unroll
     for (int b = 0; b < D; ++b) {
-      const bool bit = (dig[k] >> b) & 1u;
+      const bool bit = (dk >> b) & 1u;
       const uint32_t bb = __ballot_sync(0xffffffffu, bit);
       peers &= bit ? bb : ~bb;
     }
     const int leader = __ffs(peers) - 1;
     uint32_t old = 0u;
     if (valid && lane == leader) {
-      old = s_whist[warp * RADIX + dig[k]];
-      s_whist[warp * RADIX + dig[k]] = old + __popc(peers);
+      old = s_whist[warp * RADIX + dk];
+      s_whist[warp * RADIX + dk] = old + __popc(peers);
     }
     old = __shfl_sync(0xffffffffu, old, leader < 0 ? 0 : leader);
     rank[k] = old + __popc(peers & lt_mask);
@@ -292,7 +298,8 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_onesweep(const __grid_const
   for (int k = 0; k < ITEMS; ++k) {
     const uint32_t off = (uint32_t)(warp * ITEMS * 32 + k * 32 + lane);
     if (off < tile_n) {
-      const uint32_t lp = s_tile_base[dig[k]] + s_whist[warp * RADIX + dig[k]] + rank[k];
+      const uint32_t dk = digit_of<KW, D>(key[k], shift);
+      const uint32_t lp = s_tile_base[dk] + s_whist[warp * RADIX + dk] + rank[k];
       if (lp >= tile_n) {
         atomicOr(S.err, kErrBounds);
         continue;
@@ -378,6 +385,67 @@ __device__ __forceinline__ void copy_bytes(char* dst, const char* src, int width
   else
     for (int i = 0; i < width; i += 4)
       *reinterpret_cast<uint32_t*>(dst + i) = __ldg(reinterpret_cast<const uint32_t*>(src + i));
+}
+
+// Column-parallel gather: blockIdx.y picks the column, each thread moves
+// kGatherItems rows of it with all random loads issued before any store, so
+// a warp keeps 8 x 32 independent sector reads in flight.
+constexpr int kGatherItems = 8;
+
+template <typename V>
+__device__ __forceinline__ void gather_rows(const V* __restrict__ src, V* __restrict__ dst,
+                                            const uint32_t* __restrict__ perm, uint32_t i0, uint32_t n) {
+  uint32_t r[kGatherItems];
+  V v[kGatherItems];
+#pragma unroll
+  for (int k = 0; k < kGatherItems; ++k) {
+    const uint32_t i = i0 + k * 256;
+    r[k] = i < n ? __ldg(perm + i) : 0xffffffffu;
+  }
+#pragma unroll
+  for (int k = 0; k < kGatherItems; ++k)
+    if (r[k] < n) v[k] = __ldg(src + r[k]);
+#pragma unroll
+  for (int k = 0; k < kGatherItems; ++k)
+    if (r[k] < n) dst[i0 + k * 256] = v[k];
+}
+
+__global__ void __launch_bounds__(256) k_gather_cols(const __grid_constant__ GatherParams G,
+                                                     const uint32_t* __restrict__ perm, uint32_t n) {
+  const GatherCol& g = G.c[blockIdx.y];
+  for (uint32_t base = blockIdx.x * (256u * kGatherItems); base < n; base += gridDim.x * (256u * kGatherItems)) {
+    const uint32_t i0 = base + threadIdx.x;
+    switch (g.width) {
+      case 4:
+        gather_rows<uint32_t>(reinterpret_cast<const uint32_t*>(g.src), reinterpret_cast<uint32_t*>(g.dst), perm, i0, n);
+        break;
+      case 8:
+        gather_rows<unsigned long long>(reinterpret_cast<const unsigned long long*>(g.src),
+                                        reinterpret_cast<unsigned long long*>(g.dst), perm, i0, n);
+        break;
+      case 16:
+        gather_rows<uint4>(reinterpret_cast<const uint4*>(g.src), reinterpret_cast<uint4*>(g.dst), perm, i0, n);
+        break;
+      case 1:
+        gather_rows<uint8_t>(reinterpret_cast<const uint8_t*>(g.src), reinterpret_cast<uint8_t*>(g.dst), perm, i0, n);
+        break;
+      default:
+        for (int k = 0; k < kGatherItems; ++k) {
+          const uint32_t i = i0 + k * 256;
+          if (i >= n) break;
+          const uint32_t r = __ldg(perm + i);
+          if (r < n) copy_bytes(g.dst + (size_t)i * g.width, g.src + (size_t)r * g.width, g.width);
+        }
+    }
+    if (g.dst_nulls) {
+      for (int k = 0; k < kGatherItems; ++k) {
+        const uint32_t i = i0 + k * 256;
+        if (i >= n) break;
+        const uint32_t r = __ldg(perm + i);
+        if (r < n) g.dst_nulls[i] = g.src_nulls ? g.src_nulls[r] : 0;
+      }
+    }
+  }
 }
 
 __global__ void __launch_bounds__(256) k_gather(const __grid_constant__ GatherParams G, const uint32_t* __restrict__ perm,
@@ -807,13 +875,26 @@ int yq_gather(const yq_column* in, int32_t ncols, const uint32_t* perm, uint32_t
     G.c[c].width = in[c].width;
   }
   cudaStream_t s = as_stream(stream);
-  int grid = (int)ceil_div<uint32_t>(rows, 256);
-  const int cap = sm_count() * 16;
-  if (grid > cap) grid = cap;
+  // Aligned columns (16-byte text slots, 4/8-byte values) take the
+  // column-parallel kernel; others the row-parallel one.
+  bool aligned = true;
+  for (int c = 0; c < ncols; ++c)
+    aligned &= ((reinterpret_cast<uintptr_t>(G.c[c].src) | reinterpret_cast<uintptr_t>(G.c[c].dst)) &
+                (uintptr_t)(G.c[c].width >= 16 ? 15 : (G.c[c].width >= 8 ? 7 : (G.c[c].width >= 4 ? 3 : 0)))) == 0;
   double row_bytes = 4.0;  // permutation
   for (int c = 0; c < ncols; ++c) row_bytes += 2.0 * in[c].width + (out[c].nulls ? 2.0 : 0.0);
   ProfScope ps("gather", s, (double)rows * row_bytes);
-  k_gather<<<grid, 256, 0, s>>>(G, perm, rows);
+  if (aligned) {
+    const uint32_t tiles = ceil_div<uint32_t>(rows, 256u * kGatherItems);
+    const uint32_t cap = (uint32_t)sm_count() * 8;
+    dim3 grid(tiles < cap ? tiles : cap, (unsigned)ncols);
+    k_gather_cols<<<grid, 256, 0, s>>>(G, perm, rows);
+  } else {
+    int grid = (int)ceil_div<uint32_t>(rows, 256);
+    const int cap = sm_count() * 16;
+    if (grid > cap) grid = cap;
+    k_gather<<<grid, 256, 0, s>>>(G, perm, rows);
+  }
   YQ_CHECK_LAUNCH();
   return YQ_OK;
 }

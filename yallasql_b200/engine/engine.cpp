@@ -538,33 +538,58 @@ class OrderOperator final : public Operator {
     runs.clear();
     std::vector<yq_column> av;
     all->view(av);
-    uint32_t* perm = nullptr;
-    check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&perm), total * sizeof(uint32_t), s), "perm");
+    // 1. sort every run (segmented radix sort: one set of launches for all runs)
+    uint32_t* ids[2] = {nullptr, nullptr};
+    for (auto*& p : ids) check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&p), total * 4, s), "ids");
     check(yq_sort_segments(&av[key_], (uint32_t)total, offs.data(), (int32_t)offs.size() - 1, desc_, nulls_first_,
-                           perm, nullptr, nullptr, 0, s),
+                           ids[0], nullptr, nullptr, 0, s),
           "OrderOperator sort");
-    auto a = std::make_unique<Batch>(columns, total, s, nullable);
-    std::vector<yq_column> bv;
-    a->view(bv);
-    check(yq_gather(av.data(), (int32_t)av.size(), perm, (uint32_t)total, bv.data(), s), "OrderOperator gather");
-    cudaFreeAsync(perm, s);
-    // merge levels, ping-pong between `a` and `all`
-    Batch* src = a.get();
-    Batch* dst = all.get();
+    // 2. runs of (key, row id): only these 8 bytes per row go through the
+    //    merge levels; the payload is gathered once at the end
+    std::vector<ColumnPtr> kcols{columns[key_]};
+    const bool knull = all->nulls[key_] != nullptr;
+    auto result = std::make_unique<Batch>(columns, total, s, nullable);
+    auto k0 = std::make_unique<Batch>(kcols, total, s, knull);
+    auto k1 = std::make_unique<Batch>(kcols, total, s, knull);
+    yq_column kc0 = k0->column(0);
+    check(yq_gather(&av[key_], 1, ids[0], (uint32_t)total, &kc0, s), "OrderOperator key runs");
+    int cur = 0;
+    bool merged = false;
+    Batch* kb[2] = {k0.get(), k1.get()};
     while (offs.size() > 2) {
-      std::vector<yq_column> sv, dv;
-      src->view(sv);
-      dst->view(dv);
-      check(yq_merge_pass(sv.data(), (int32_t)sv.size(), key_, desc_, nulls_first_, offs.data(),
-                          (int32_t)offs.size() - 1, dv.data(), nullptr, 0, s),
+      const bool last = offs.size() - 1 <= 2;  // two runs left: this level writes the result's key column
+      merged = true;
+      yq_column sv[2] = {kb[cur]->column(0), yq_column{ids[cur], nullptr, YQ_INT32, 4}};
+      yq_column dv[2] = {last ? result->column(key_) : kb[cur ^ 1]->column(0),
+                         yq_column{ids[cur ^ 1], nullptr, YQ_INT32, 4}};
+      check(yq_merge_pass(sv, 2, 0, desc_, nulls_first_, offs.data(), (int32_t)offs.size() - 1, dv, nullptr, 0, s),
             "OrderOperator merge");
       std::vector<uint32_t> next_offs;
       for (size_t i = 0; i + 1 < offs.size(); i += 2) next_offs.push_back(offs[i]);
       next_offs.push_back(offs.back());
       offs.swap(next_offs);
-      std::swap(src, dst);
+      cur ^= 1;
+      if (last) break;
     }
-    std::unique_ptr<Batch> result = (src == a.get()) ? std::move(a) : std::move(all);
+    if (!merged) {
+      // a single run: its sorted keys are the result's key column
+      yq_column kr = result->column(key_), ks = kb[0]->column(0);
+      check_cuda(cudaMemcpyAsync(kr.data, ks.data, total * kr.width, cudaMemcpyDeviceToDevice, s), "key copy");
+      if (kr.nulls && ks.nulls)
+        check_cuda(cudaMemcpyAsync(const_cast<uint8_t*>(kr.nulls), ks.nulls, total, cudaMemcpyDeviceToDevice, s),
+                   "key copy");
+    }
+    // 3. payload columns by the final row ids
+    std::vector<yq_column> src_rest, dst_rest;
+    for (size_t c = 0; c < columns.size(); ++c) {
+      if ((int)c == key_) continue;
+      src_rest.push_back(av[c]);
+      dst_rest.push_back(result->column(c));
+    }
+    if (!src_rest.empty())
+      check(yq_gather(src_rest.data(), (int32_t)src_rest.size(), ids[cur], (uint32_t)total, dst_rest.data(), s),
+            "OrderOperator gather");
+    for (auto* p : ids) cudaFreeAsync(p, s);
     return cache.putBatch(std::move(result));
   }
 
