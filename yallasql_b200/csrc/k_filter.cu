@@ -4,148 +4,112 @@
 // prefix_sum_mask -> move_rows_filter per column, then cast -> mul ->
 // reduction per aggregate; include/engine/operators/filter_operator.hpp:31-98,
 // include/engine/operators/expressions/aggregate.hpp:55-284,
-// src/kernels/reduction_kernel.cu:79-185) with one kernel per operator that
-// keeps every intermediate in registers.
+// src/kernels/reduction_kernel.cu:79-185) with one persistent kernel per
+// operator that keeps every intermediate in registers. The columns a program
+// reads are staged in shared memory a few steps ahead by bulk copies
+// (yq_stage.cuh) when they are 16-byte aligned and fit; otherwise the kernel
+// reads them from global memory directly.
 #include "vm_host.cuh"
+#include "yq_agg.cuh"
 #include "yq_lookback.cuh"
+#include "yq_stage.cuh"
 
 namespace yq {
-
-constexpr int kRowBlock = 256;
-constexpr uint32_t kRowTile = kRowBlock * ITEMS;  // 1024 rows per tile
-
-// ================================================================ aggregate
-struct FAParams {
-  VmProgram P;
-  int32_t pc_end;
-  int32_t nagg;
-  uint8_t upd[YQ_MAX_AGGREGATES];
-};
-
-struct AggEmit {
-  uint32_t sel;
-  Acc acc[YQ_MAX_AGGREGATES];
-  __device__ __forceinline__ void pred(uint32_t bits) { sel &= bits; }
-  __device__ __forceinline__ void agg(int a, int upd, int t, const Val& x) {
-    switch (a) {
-#define YQ_AGG_CASE(k) \
-  case k: acc_update(acc[k], upd, t, x, sel); break;
-      YQ_AGG_CASE(0) YQ_AGG_CASE(1) YQ_AGG_CASE(2) YQ_AGG_CASE(3)
-      YQ_AGG_CASE(4) YQ_AGG_CASE(5) YQ_AGG_CASE(6) YQ_AGG_CASE(7)
-#undef YQ_AGG_CASE
-      default: break;
-    }
-  }
-  __device__ __forceinline__ void proj(int, const Val&) {}
-};
-
-__device__ __forceinline__ uint32_t in_range_bits(uint32_t row0, uint32_t n) {
-  if (row0 >= n) return 0u;
-  const uint32_t left = n - row0;
-  return left >= (uint32_t)ITEMS ? ((1u << ITEMS) - 1u) : ((1u << left) - 1u);
-}
-
-struct AggInitParams {
-  int32_t nagg;
-  uint8_t upd[YQ_MAX_AGGREGATES];
-};
-
-__global__ void k_agg_state_init(Acc* state, const AggInitParams p) {
-  const int a = threadIdx.x;
-  if (a < p.nagg) acc_init(state[a], p.upd[a]);
-}
-
-__global__ void __launch_bounds__(kRowBlock) k_filter_aggregate(const __grid_constant__ FAParams F, uint32_t n,
-                                                                Acc* __restrict__ partials, uint32_t* ticket,
-                                                                Acc* __restrict__ state) {
-  AggEmit E;
-#pragma unroll
-  for (int a = 0; a < YQ_MAX_AGGREGATES; ++a) acc_init(E.acc[a], a < F.nagg ? F.upd[a] : UPD_COUNT);
-
-  const uint32_t ntiles = ceil_div<uint32_t>(n, kRowTile);
-  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const uint32_t row0 = tile * kRowTile + threadIdx.x * ITEMS;
-    const uint32_t inr = in_range_bits(row0, n);
-    E.sel = inr;
-    Stack S;
-    run_vm(F.P, 0, F.pc_end, row0, inr, inr == 0xfu, S, E);
-#pragma unroll
-    for (int a = 0; a < YQ_MAX_AGGREGATES; ++a)
-      if (a < F.nagg && F.upd[a] == UPD_COUNT_STAR) E.acc[a].cnt += __popc(E.sel);
-  }
-
-  // Block reduction: warp shuffles, then warps in order.
-  __shared__ Acc s_acc[kRowBlock / 32][YQ_MAX_AGGREGATES];
-  __shared__ bool s_last;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int a = 0; a < YQ_MAX_AGGREGATES; ++a) {
-    if (a < F.nagg) {
-#pragma unroll
-      for (int d = 16; d > 0; d >>= 1) acc_shfl_down(E.acc[a], d, F.upd[a]);
-      if (lane == 0) s_acc[warp][a] = E.acc[a];
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < F.nagg) {
-    const int a = threadIdx.x;
-    Acc t = s_acc[0][a];
-    for (int w = 1; w < kRowBlock / 32; ++w) acc_combine(t, s_acc[w][a], F.upd[a]);
-    partials[blockIdx.x * YQ_MAX_AGGREGATES + a] = t;
-  }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  if (threadIdx.x < F.nagg) {
-    // Fold the per-block partials in block order: the result does not depend
-    // on which block finished last.
-    const int a = threadIdx.x;
-    const int upd = F.upd[a];
-    Acc t;
-    acc_init(t, upd);
-    for (uint32_t b = 0; b < gridDim.x; ++b) {
-      const Acc* p = partials + b * YQ_MAX_AGGREGATES + a;
-      Acc q;
-      q.cnt = __ldcg(&p->cnt);
-      q.i = __ldcg(&p->i);
-      q.f = __ldcg(&p->f);
-      acc_combine(t, q, upd);
-    }
-    Acc s = state[a];
-    acc_combine(s, t, upd);
-    state[a] = s;
-  }
-  if (threadIdx.x == 0) *ticket = 0u;
-}
-
-// Bytes per row of every input column a program references (plus null bytes).
-static double referenced_row_bytes(const VmProgram& P, int len) {
-  bool used[YQ_MAX_BATCH_COLUMNS] = {false};
-  for (int i = 0; i < len; ++i) {
-    const Insn& I = P.code[i];
-    switch (I.op & OP_MASK) {
-      case OP_COL: used[I.a] = true; break;
-      case OP_ARITH_COL:
-      case OP_CMP_COL_CONST:
-      case OP_AND_CMP_COL_CONST: used[I.b] = true; break;
-      case OP_CMP_COL_COL: used[I.b] = true; used[I.imm] = true; break;
-      default: break;
-    }
-  }
-  double b = 0;
-  for (int c = 0; c < P.ncols; ++c)
-    if (used[c]) b += P.cols[c].width + (P.cols[c].nulls ? 1 : 0);
-  return b;
-}
 
 static int occupancy_grid(const void* kernel, int block, size_t smem) {
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess || per_sm < 1)
     per_sm = 1;
   return per_sm * sm_count();
+}
+
+// Raise a kernel's dynamic shared memory limit (once per size) to `smem`.
+static int allow_smem(const void* kernel, size_t smem, size_t& done) {
+  if (smem > 48 * 1024 && smem > done) {
+    YQ_TRY_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    done = smem;
+  }
+  return YQ_OK;
+}
+
+// Persistent grid of a row kernel: resident blocks, no more than the steps.
+struct GridCache {
+  int cap = 0;
+  size_t smem = (size_t)-1;
+  int grid(const void* kernel, size_t dyn_smem, uint32_t steps) {
+    if (smem != dyn_smem) {
+      cap = occupancy_grid(kernel, kRowBlock, dyn_smem);
+      smem = dyn_smem;
+    }
+    int g = (int)(steps < (uint32_t)cap ? steps : (uint32_t)cap);
+    return g < 1 ? 1 : g;
+  }
+};
+
+static size_t max_row_grid() { return (size_t)sm_count() * 8; }
+
+// ================================================================ aggregate
+struct FAParams {
+  VmProgram P;
+  StagePlan SP;
+  int32_t pc_end;
+  AggParams A;
+};
+
+__global__ void k_agg_state_init(Acc* state, const AggParams p) {
+  const int a = threadIdx.x;
+  if (a < YQ_MAX_AGGREGATES) state[a] = Acc{0, acc_identity(a < p.nagg ? p.upd[a] : UPD_COUNT)};
+  if (a == 0) *agg_state_err(state) = 0u;
+}
+
+template <bool STAGED>
+__global__ void __launch_bounds__(kRowBlock, 2) k_filter_aggregate(const __grid_constant__ FAParams F, uint32_t n,
+                                                                   Acc* __restrict__ partials, uint32_t* ticket,
+                                                                   Acc* state) {
+  uint32_t* err = agg_state_err(state);
+  AggEmit E;
+  agg_thread_init(E, F.A);
+  uint32_t nsel = 0;
+  const uint32_t ntiles = ceil_div<uint32_t>(n, kStepRows);
+  const uint32_t G = gridDim.x;
+  int S = 1;
+  if constexpr (STAGED) {
+    S = F.SP.nstages;
+    stage_init(F.SP);
+    if (threadIdx.x == 0)
+      for (int j = 0; j < S - 1; ++j) {
+        const uint32_t t = blockIdx.x + (uint32_t)j * G;
+        if (t < ntiles && full_step(t, n)) stage_issue(F.SP, j, t * kStepRows);
+      }
+  }
+  int slot = 0;
+  uint32_t parity = 0;
+  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += G) {
+    Ctx X;
+    X.tile0 = tile * kStepRows;
+    X.lr = threadIdx.x * ITEMS;
+    X.inr = in_range_bits(X.tile0 + X.lr, n);
+    X.stage = 0;
+    if constexpr (STAGED) {
+      __syncthreads();  // every thread is done with the previous step: its slot is free
+      if (threadIdx.x == 0) {
+        const uint32_t t = tile + (uint32_t)(S - 1) * G;
+        const int ns = slot == 0 ? S - 1 : slot - 1;
+        if (t < ntiles && full_step(t, n)) stage_issue(F.SP, ns, t * kStepRows);
+      }
+      stage_step(F.SP, slot, parity, tile, n, err);
+      X.stage = (uint32_t)slot * F.SP.stage_bytes;
+    }
+    E.sel = X.inr;
+    Stack St;
+    run_vm<STAGED>(F.P, 0, F.pc_end, X, St, E);
+    nsel += __popc(E.sel);
+    if (++slot == S) {
+      slot = 0;
+      parity ^= 1u;
+    }
+  }
+  agg_block_finish<kRowBlock>(E, nsel, F.A, partials, ticket, state);
 }
 
 static uint8_t agg_update_code(int kind, int t) {
@@ -190,27 +154,11 @@ static int build_agg_program(ProgramBuilder& B, const yq_program* predicate, con
     if (aggs[a].kind != YQ_AGG_COUNT && t != aggs[a].input_type) return YQ_ERR_INVALID_ARG;
     YQ_TRY(B.emit(OP_EMIT_AGG, (uint8_t)a, upd[a], (uint8_t)t));
   }
-  B.finalize();
-  return YQ_OK;
+  return B.finalize();
 }
 
-int launch_filter_aggregate(const FAParams& F, uint32_t rows, Acc* partials, uint32_t* ticket, Acc* state, int grid,
-                            cudaStream_t s) {
-  ProfScope ps("filter_aggregate", s, (double)rows * referenced_row_bytes(F.P, F.pc_end));
-  k_filter_aggregate<<<grid, kRowBlock, 0, s>>>(F, rows, partials, ticket, state);
-  YQ_CHECK_LAUNCH();
-  return YQ_OK;
-}
-
-int filter_aggregate_grid(uint32_t rows) {
-  static int cap = 0;
-  if (!cap) cap = occupancy_grid((const void*)k_filter_aggregate, kRowBlock, 0);
-  const int tiles = (int)ceil_div<uint32_t>(rows, kRowTile);
-  return tiles < cap ? (tiles > 0 ? tiles : 1) : cap;
-}
-
-int prepare_filter_aggregate(const yq_batch* batch, const yq_program* predicate, const yq_constants* constants,
-                             const yq_agg_spec* aggs, int32_t nagg, FAParams* F) {
+static int prepare_filter_aggregate(const yq_batch* batch, const yq_program* predicate, const yq_constants* constants,
+                                    const yq_agg_spec* aggs, int32_t nagg, FAParams* F) {
   if (!batch || !F) return YQ_ERR_INVALID_ARG;
   YQ_TRY(check_aggs(aggs, nagg));
   ProgramBuilder B;
@@ -218,10 +166,30 @@ int prepare_filter_aggregate(const yq_batch* batch, const yq_program* predicate,
   YQ_TRY(B.set_constants(constants));
   uint8_t upd[YQ_MAX_AGGREGATES] = {0};
   YQ_TRY(build_agg_program(B, predicate, aggs, nagg, upd));
+  if (!plan_stages(B.P, B.used_cols, F->SP)) F->SP.nstages = 0;
   memcpy(&F->P, &B.P, sizeof(VmProgram));
   F->pc_end = B.len;
-  F->nagg = nagg;
-  for (int a = 0; a < YQ_MAX_AGGREGATES; ++a) F->upd[a] = a < nagg ? upd[a] : UPD_COUNT;
+  F->A.nagg = nagg;
+  for (int a = 0; a < YQ_MAX_AGGREGATES; ++a) F->A.upd[a] = a < nagg ? upd[a] : UPD_COUNT;
+  return YQ_OK;
+}
+
+static int launch_filter_aggregate(const FAParams& F, uint32_t rows, Acc* partials, uint32_t* ticket, Acc* state,
+                                   cudaStream_t s) {
+  const bool staged = F.SP.nstages > 0;
+  const void* kern = staged ? (const void*)k_filter_aggregate<true> : (const void*)k_filter_aggregate<false>;
+  const size_t smem = stage_smem_bytes(F.SP);
+  static size_t done_smem = 0;
+  YQ_TRY(allow_smem(kern, smem, done_smem));
+  static GridCache gc[2];
+  int grid = gc[staged ? 1 : 0].grid(kern, smem, ceil_div<uint32_t>(rows, kStepRows));
+  if ((size_t)grid > max_row_grid()) grid = (int)max_row_grid();
+  ProfScope ps("filter_aggregate", s, (double)rows * row_bytes_of(F.P, program_columns(F.P, F.pc_end, 0)));
+  if (staged)
+    k_filter_aggregate<true><<<grid, kRowBlock, smem, s>>>(F, rows, partials, ticket, state);
+  else
+    k_filter_aggregate<false><<<grid, kRowBlock, 0, s>>>(F, rows, partials, ticket, state);
+  YQ_CHECK_LAUNCH();
   return YQ_OK;
 }
 
@@ -235,6 +203,7 @@ struct DevOut {
 
 struct FPParams {
   VmProgram P;
+  StagePlan SP;
   int32_t pred_end;
   int32_t proj_end;
   int32_t nproj;
@@ -242,26 +211,24 @@ struct FPParams {
   DevOut out[YQ_MAX_PROJECTIONS];
 };
 
-__device__ __forceinline__ void store_slot(char* base, uint32_t pos, int width, uint64_t v) {
-  if (width == 4) reinterpret_cast<uint32_t*>(base)[pos] = (uint32_t)v;
-  else if (width == 8) reinterpret_cast<unsigned long long*>(base)[pos] = v;
-  else reinterpret_cast<uint8_t*>(base)[pos] = (uint8_t)v;
-}
-
 struct ProjEmit {
   uint32_t sel;
   uint32_t pos;
   const FPParams* F;
   __device__ __forceinline__ void pred(uint32_t bits) { sel &= bits; }
-  __device__ __forceinline__ void agg(int, int, int, const Val&) {}
+  template <int K>
+  __device__ __forceinline__ void agg(int, const Val&) {}
+  template <int W>
   __device__ __forceinline__ void proj(int p, const Val& x) {
     const DevOut& o = F->out[p];
     uint32_t q = pos;
 #pragma unroll
     for (int k = 0; k < ITEMS; ++k) {
-      if (sel & (1u << k)) {
+      if (sel >> k & 1u) {
         if (q < F->capacity) {
-          store_slot(o.data, q, o.width, x.v[k]);
+          if constexpr (W == 0) reinterpret_cast<uint8_t*>(o.data)[q] = (uint8_t)((x.v[0] >> k) & 1u);
+          else if constexpr (W == 1) reinterpret_cast<uint32_t*>(o.data)[q] = (uint32_t)x.v[k];
+          else reinterpret_cast<unsigned long long*>(o.data)[q] = x.v[k];
           if (o.nulls) o.nulls[q] = (x.valid >> k & 1u) ? 0 : 1;
         }
         ++q;
@@ -270,74 +237,199 @@ struct ProjEmit {
   }
 };
 
-__device__ __forceinline__ void copy_value(char* dst, const char* src, int width) {
+// One cell of `width` bytes; `src` is shared or global memory (generic).
+__device__ __forceinline__ void copy_cell_any(char* dst, const char* src, int width) {
   if (width == 4) {
-    *reinterpret_cast<uint32_t*>(dst) = __ldg(reinterpret_cast<const uint32_t*>(src));
+    *reinterpret_cast<uint32_t*>(dst) = *reinterpret_cast<const uint32_t*>(src);
   } else if (width == 8) {
-    *reinterpret_cast<unsigned long long*>(dst) = __ldg(reinterpret_cast<const unsigned long long*>(src));
+    *reinterpret_cast<unsigned long long*>(dst) = *reinterpret_cast<const unsigned long long*>(src);
   } else if (width == 1) {
     *dst = *src;
   } else if ((width & 15) == 0 && ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0) {
     for (int i = 0; i < width; i += 16)
-      *reinterpret_cast<uint4*>(dst + i) = ldg_nc_v4(src + i);
+      *reinterpret_cast<uint4*>(dst + i) = *reinterpret_cast<const uint4*>(src + i);
   } else {
     for (int i = 0; i < width; i += 4)
-      *reinterpret_cast<uint32_t*>(dst + i) = __ldg(reinterpret_cast<const uint32_t*>(src + i));
+      *reinterpret_cast<uint32_t*>(dst + i) = *reinterpret_cast<const uint32_t*>(src + i);
   }
 }
 
-__global__ void __launch_bounds__(kRowBlock) k_filter_project(const __grid_constant__ FPParams F, uint32_t n,
-                                                              uint32_t* tile_counter,
-                                                              unsigned long long* __restrict__ status,
-                                                              uint32_t* out_count, uint32_t* err) {
-  __shared__ uint32_t s_tile;
-  __shared__ uint32_t s_warp[kRowBlock / 32 + 1];
-  __shared__ unsigned long long s_prefix;
-  if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
-  __syncthreads();
-  const uint32_t tile = s_tile;
-  const uint32_t row0 = tile * kRowTile + threadIdx.x * ITEMS;
-  const uint32_t inr = in_range_bits(row0, n);
-  const bool full = (inr == 0xfu);
-
-  ProjEmit E;
-  E.sel = inr;
-  E.pos = 0;
-  E.F = &F;
-  Stack S;
-  if (F.pred_end > 0) run_vm(F.P, 0, F.pred_end, row0, inr, full, S, E);
-
-  uint32_t total;
-  const uint32_t excl = block_exclusive_sum<kRowBlock>(__popc(E.sel), s_warp, total);
-  if (threadIdx.x < 32) {
-    unsigned long long p = tile_lookback(status, tile, total, err);
-    if (threadIdx.x == 0) s_prefix = p;
-  }
-  __syncthreads();
-  const unsigned long long base = s_prefix;
-  E.pos = (uint32_t)(base + excl);
-
-  if (F.proj_end > F.pred_end) run_vm(F.P, F.pred_end, F.proj_end, row0, inr, full, S, E);
+// Projections that copy an input column: selected rows to positions pos, pos+1, ...
+template <bool STAGED>
+__device__ __forceinline__ void copy_source_columns(const FPParams& F, const Ctx& X, uint32_t sel, uint32_t pos) {
   for (int p = 0; p < F.nproj; ++p) {
     const DevOut& o = F.out[p];
     if (o.src_col < 0) continue;
     const DevCol& c = F.P.cols[o.src_col];
-    uint32_t q = E.pos;
+    uint32_t q = pos;
 #pragma unroll
     for (int k = 0; k < ITEMS; ++k) {
-      if (E.sel & (1u << k)) {
+      if (sel >> k & 1u) {
         if (q < F.capacity) {
-          copy_value(o.data + (size_t)q * o.width, c.data + (size_t)(row0 + k) * c.width, c.width);
-          if (o.nulls) o.nulls[q] = c.nulls ? c.nulls[row0 + k] : 0;
+          const uint32_t lr = X.lr + k;
+          const char* src;
+          uint8_t nul = 0;
+          if constexpr (STAGED) {
+            src = reinterpret_cast<const char*>(yq_dyn_smem + X.stage + c.soff + lr * (uint32_t)c.width);
+            if (c.nulls) nul = yq_dyn_smem[X.stage + c.snoff + lr];
+          } else {
+            src = c.data + (size_t)(X.tile0 + lr) * c.width;
+            if (c.nulls) nul = c.nulls[X.tile0 + lr];
+          }
+          copy_cell_any(o.data + (size_t)q * o.width, src, c.width);
+          if (o.nulls) o.nulls[q] = nul;
         }
         ++q;
       }
     }
   }
-  if (tile == gridDim.x - 1 && threadIdx.x == 0) {
-    const unsigned long long cnt = base + total;
-    *out_count = cnt > 0xffffffffull ? 0xffffffffu : (uint32_t)cnt;
+}
+
+// Tiles are claimed in order from a counter (a few steps ahead when staged),
+// every block processes its claims in order, so each tile's predecessors are
+// held by running blocks and the decoupled look-back always completes.
+template <bool STAGED>
+__global__ void __launch_bounds__(kRowBlock, 2) k_filter_project(const __grid_constant__ FPParams F, uint32_t n,
+                                                                 uint32_t* tile_counter,
+                                                                 unsigned long long* __restrict__ status,
+                                                                 uint32_t* out_count, uint32_t* err) {
+  __shared__ uint32_t s_tiles[kStageMax];
+  __shared__ uint32_t s_warp[kRowBlock / 32 + 1];
+  __shared__ unsigned long long s_prefix;
+  const uint32_t ntiles = ceil_div<uint32_t>(n, kStepRows);
+  int S = 1;
+  if constexpr (STAGED) {
+    S = F.SP.nstages;
+    stage_init(F.SP);
   }
+  if (threadIdx.x == 0)
+    for (int j = 0; j < S - 1; ++j) {
+      const uint32_t t = atomicAdd(tile_counter, 1u);
+      s_tiles[j] = t;
+      if constexpr (STAGED)
+        if (t < ntiles && full_step(t, n)) stage_issue(F.SP, j, t * kStepRows);
+    }
+  int slot = 0;
+  uint32_t parity = 0;
+  for (;;) {
+    __syncthreads();  // every thread is done with the previous step
+    if (threadIdx.x == 0) {
+      const int ns = slot == 0 ? S - 1 : slot - 1;
+      const uint32_t t = atomicAdd(tile_counter, 1u);
+      s_tiles[ns] = t;
+      if constexpr (STAGED)
+        if (t < ntiles && full_step(t, n)) stage_issue(F.SP, ns, t * kStepRows);
+    }
+    __syncthreads();
+    const uint32_t tile = s_tiles[slot];
+    if (tile >= ntiles) break;  // later claims are larger: no copy is in flight
+    Ctx X;
+    X.tile0 = tile * kStepRows;
+    X.lr = threadIdx.x * ITEMS;
+    X.inr = in_range_bits(X.tile0 + X.lr, n);
+    X.stage = 0;
+    if constexpr (STAGED) {
+      stage_step(F.SP, slot, parity, tile, n, err);
+      X.stage = (uint32_t)slot * F.SP.stage_bytes;
+    }
+    ProjEmit E;
+    E.sel = X.inr;
+    E.pos = 0;
+    E.F = &F;
+    Stack St;
+    if (F.pred_end > 0) run_vm<STAGED>(F.P, 0, F.pred_end, X, St, E);
+
+    uint32_t total;
+    const uint32_t excl = block_exclusive_sum<kRowBlock>(__popc(E.sel), s_warp, total);
+    if (threadIdx.x < 32) {
+      const unsigned long long p = tile_lookback(status, tile, total, err);
+      if (threadIdx.x == 0) s_prefix = p;
+    }
+    __syncthreads();
+    const unsigned long long base = s_prefix;
+    E.pos = (uint32_t)(base + excl);
+    if (F.proj_end > F.pred_end) run_vm<STAGED>(F.P, F.pred_end, F.proj_end, X, St, E);
+    copy_source_columns<STAGED>(F, X, E.sel, E.pos);
+    if (tile == ntiles - 1 && threadIdx.x == 0) {
+      const unsigned long long cnt = base + total;
+      *out_count = cnt > 0xffffffffull ? 0xffffffffu : (uint32_t)cnt;
+    }
+    if (++slot == S) {
+      slot = 0;
+      parity ^= 1u;
+    }
+  }
+}
+
+// Validation and program build shared by yq_filter_project and its
+// allocation-free variant.
+static int build_project_params(const yq_batch* batch, const yq_program* predicate, const yq_constants* constants,
+                                const yq_projection* proj, int32_t nproj, yq_column* out, uint32_t capacity,
+                                FPParams& F) {
+  if (!batch || nproj < 0 || nproj > YQ_MAX_PROJECTIONS || (nproj > 0 && (!proj || !out))) return YQ_ERR_INVALID_ARG;
+  ProgramBuilder B;
+  YQ_TRY(B.set_columns(batch->columns, batch->ncols));
+  YQ_TRY(B.set_constants(constants));
+  if (predicate && predicate->len > 0) {
+    int t = -1;
+    YQ_TRY(B.append(predicate, t));
+    if (t != YQ_BOOL) return YQ_ERR_INVALID_ARG;
+    YQ_TRY(B.emit(OP_EMIT_PRED, 0, 0, YQ_BOOL));
+  }
+  const int pred_end = B.len;
+  uint32_t copy_mask = 0;
+  for (int p = 0; p < nproj; ++p) {
+    DevOut& o = F.out[p];
+    o.data = static_cast<char*>(out[p].data);
+    o.nulls = const_cast<uint8_t*>(out[p].nulls);
+    o.src_col = proj[p].column;
+    if (!o.data && capacity > 0) return YQ_ERR_INVALID_ARG;
+    if (proj[p].column >= 0) {
+      if (proj[p].column >= batch->ncols) return YQ_ERR_INVALID_ARG;
+      const yq_column& c = batch->columns[proj[p].column];
+      if (out[p].type != c.type || out[p].width != c.width) return YQ_ERR_INVALID_ARG;
+      o.width = c.width;
+      copy_mask |= 1u << proj[p].column;
+    } else {
+      int t = -1;
+      YQ_TRY(B.append(&proj[p].program, t));
+      if (t != proj[p].out_type || t != out[p].type || !ProgramBuilder::valid_column(out[p])) return YQ_ERR_INVALID_ARG;
+      o.width = out[p].width;
+      YQ_TRY(B.emit(OP_EMIT_PROJ, (uint8_t)p, 0, (uint8_t)t));
+    }
+  }
+  YQ_TRY(B.finalize());
+  if (!plan_stages(B.P, B.used_cols | copy_mask, F.SP)) F.SP.nstages = 0;
+  memcpy(&F.P, &B.P, sizeof(VmProgram));
+  F.pred_end = B.remap[pred_end];
+  F.proj_end = B.len;
+  F.nproj = nproj;
+  F.capacity = capacity;
+  return YQ_OK;
+}
+
+// Launch over `rows` rows with look-back scratch `status` (one word per tile
+// plus one) and `misc` = {tile counter, error word} (both zeroed).
+static int launch_filter_project(const FPParams& F, uint32_t rows, uint32_t* misc, unsigned long long* status,
+                                 uint32_t* cnt_dev, cudaStream_t s) {
+  const bool staged = F.SP.nstages > 0;
+  const void* kern = staged ? (const void*)k_filter_project<true> : (const void*)k_filter_project<false>;
+  const size_t smem = stage_smem_bytes(F.SP);
+  static size_t done_smem = 0;
+  YQ_TRY(allow_smem(kern, smem, done_smem));
+  static GridCache gc[2];
+  const int grid = gc[staged ? 1 : 0].grid(kern, smem, ceil_div<uint32_t>(rows, kStepRows));
+  uint32_t mask = program_columns(F.P, F.proj_end, 0);
+  for (int p = 0; p < F.nproj; ++p)
+    if (F.out[p].src_col >= 0) mask |= 1u << F.out[p].src_col;
+  // algorithmic bytes: referenced input columns (outputs depend on selectivity)
+  ProfScope ps("filter_project", s, (double)rows * row_bytes_of(F.P, mask));
+  if (staged)
+    k_filter_project<true><<<grid, kRowBlock, smem, s>>>(F, rows, misc, status, cnt_dev, misc + 1);
+  else
+    k_filter_project<false><<<grid, kRowBlock, 0, s>>>(F, rows, misc, status, cnt_dev, misc + 1);
+  YQ_CHECK_LAUNCH();
+  return YQ_OK;
 }
 
 }  // namespace yq
@@ -347,15 +439,15 @@ using namespace yq;
 extern "C" {
 
 size_t yq_agg_state_bytes(int32_t nagg) {
-  if (nagg < 0) nagg = 0;
-  return align_up((size_t)nagg * sizeof(Acc), 256);
+  (void)nagg;
+  return kAggStateBytes;
 }
 
 int yq_agg_state_init(void* state, const yq_agg_spec* aggs, int32_t nagg, void* stream) {
   if (!state) return YQ_ERR_INVALID_ARG;
   YQ_TRY(check_aggs(aggs, nagg));
-  if (nagg == 0) return YQ_OK;
-  AggInitParams p;
+  AggParams p;
+  memset(&p, 0, sizeof(p));
   p.nagg = nagg;
   for (int a = 0; a < YQ_MAX_AGGREGATES; ++a) p.upd[a] = a < nagg ? agg_update_code(aggs[a].kind, aggs[a].input_type) : 0;
   k_agg_state_init<<<1, 32, 0, as_stream(stream)>>>(static_cast<Acc*>(state), p);
@@ -365,8 +457,9 @@ int yq_agg_state_init(void* state, const yq_agg_spec* aggs, int32_t nagg, void* 
 
 size_t yq_filter_aggregate_workspace_size(uint32_t rows, int32_t nagg) {
   (void)nagg;
+  (void)rows;
   WsSize w;
-  w.add<Acc>((size_t)filter_aggregate_grid(rows) * YQ_MAX_AGGREGATES);
+  w.add<Acc>(max_row_grid() * YQ_MAX_AGGREGATES);
   w.add<uint32_t>(4);
   return w.total();
 }
@@ -379,28 +472,32 @@ int yq_filter_aggregate(const yq_batch* batch, const yq_program* predicate, cons
   YQ_TRY(prepare_filter_aggregate(batch, predicate, constants, aggs, nagg, &F));
   if (batch->rows == 0 || nagg == 0) return YQ_OK;
   cudaStream_t s = as_stream(stream);
-  const int grid = filter_aggregate_grid(batch->rows);
   Workspace ws;
   YQ_TRY(ws.acquire(workspace, workspace_bytes, yq_filter_aggregate_workspace_size(batch->rows, nagg), s));
-  Acc* partials = ws.take<Acc>((size_t)grid * YQ_MAX_AGGREGATES);
+  Acc* partials = ws.take<Acc>(max_row_grid() * YQ_MAX_AGGREGATES);
   uint32_t* ticket = ws.take<uint32_t>(4);
   YQ_TRY_CUDA(cudaMemsetAsync(ticket, 0, sizeof(uint32_t), s));
-  return launch_filter_aggregate(F, batch->rows, partials, ticket, static_cast<Acc*>(state), grid, s);
+  return launch_filter_aggregate(F, batch->rows, partials, ticket, static_cast<Acc*>(state), s);
 }
 
 int yq_agg_state_read(const void* state, const yq_agg_spec* aggs, int32_t nagg, yq_agg_result* out, void* stream) {
   if (!state || !out) return YQ_ERR_INVALID_ARG;
   YQ_TRY(check_aggs(aggs, nagg));
-  Acc host[YQ_MAX_AGGREGATES];
+  Acc host[YQ_MAX_AGGREGATES + 1];
   cudaStream_t s = as_stream(stream);
-  YQ_TRY_CUDA(cudaMemcpyAsync(host, state, (size_t)nagg * sizeof(Acc), cudaMemcpyDeviceToHost, s));
+  YQ_TRY_CUDA(
+      cudaMemcpyAsync(host, state, sizeof(Acc) * YQ_MAX_AGGREGATES + sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  if (*agg_state_err(host)) return YQ_ERR_TIMEOUT;
   for (int a = 0; a < nagg; ++a) {
     const Acc& h = host[a];
     yq_agg_result& r = out[a];
     const int kind = aggs[a].kind;
     const int t = aggs[a].input_type;
     const bool flt = (t == YQ_FLOAT32 || t == YQ_FLOAT64);
+    double hf;
+    memcpy(&hf, &h.bits, sizeof(hf));
+    const long long hi = (long long)h.bits;
     r.kind = kind;
     r.count = h.cnt;
     r.i = 0;
@@ -409,19 +506,14 @@ int yq_agg_state_read(const void* state, const yq_agg_spec* aggs, int32_t nagg, 
     switch (kind) {
       case YQ_AGG_COUNT_STAR:
       case YQ_AGG_COUNT: r.i = h.cnt; break;
-      case YQ_AGG_SUM:
-        r.is_null = h.cnt == 0;
-        if (flt) r.f = h.f;
-        else r.i = h.i;
-        break;
       case YQ_AGG_AVG:
         r.is_null = h.cnt == 0;
-        if (h.cnt) r.f = flt ? h.f / (double)h.cnt : (double)h.i / (double)h.cnt;
+        if (h.cnt) r.f = flt ? hf / (double)h.cnt : (double)hi / (double)h.cnt;
         break;
-      default:
+      default:  // SUM, MIN, MAX
         r.is_null = h.cnt == 0;
-        if (flt) r.f = h.f;
-        else r.i = h.i;
+        if (flt) r.f = hf;
+        else r.i = hi;
         break;
     }
   }
@@ -430,7 +522,7 @@ int yq_agg_state_read(const void* state, const yq_agg_spec* aggs, int32_t nagg, 
 
 size_t yq_filter_project_workspace_size(uint32_t rows) {
   WsSize w;
-  w.add<unsigned long long>((size_t)ceil_div<uint32_t>(rows, kRowTile) + 1);
+  w.add<unsigned long long>((size_t)ceil_div<uint32_t>(rows, kStepRows) + 1);
   w.add<uint32_t>(4);
   return w.total();
 }
@@ -439,52 +531,16 @@ int yq_filter_project(const yq_batch* batch, const yq_program* predicate, const 
                       const yq_projection* proj, int32_t nproj, yq_column* out, uint32_t capacity,
                       uint32_t* count_device, uint32_t* count_host, void* workspace, size_t workspace_bytes,
                       void* stream) {
-  if (!batch || nproj < 0 || nproj > YQ_MAX_PROJECTIONS || (nproj > 0 && (!proj || !out))) return YQ_ERR_INVALID_ARG;
   cudaStream_t s = as_stream(stream);
   FPParams F;
-  {
-    ProgramBuilder B;
-    YQ_TRY(B.set_columns(batch->columns, batch->ncols));
-    YQ_TRY(B.set_constants(constants));
-    if (predicate && predicate->len > 0) {
-      int t = -1;
-      YQ_TRY(B.append(predicate, t));
-      if (t != YQ_BOOL) return YQ_ERR_INVALID_ARG;
-      YQ_TRY(B.emit(OP_EMIT_PRED, 0, 0, YQ_BOOL));
-    }
-    F.pred_end = B.len;
-    for (int p = 0; p < nproj; ++p) {
-      DevOut& o = F.out[p];
-      o.data = static_cast<char*>(out[p].data);
-      o.nulls = const_cast<uint8_t*>(out[p].nulls);
-      o.src_col = proj[p].column;
-      if (!o.data && capacity > 0) return YQ_ERR_INVALID_ARG;
-      if (proj[p].column >= 0) {
-        if (proj[p].column >= batch->ncols) return YQ_ERR_INVALID_ARG;
-        const yq_column& c = batch->columns[proj[p].column];
-        if (out[p].type != c.type || out[p].width != c.width) return YQ_ERR_INVALID_ARG;
-        o.width = c.width;
-      } else {
-        int t = -1;
-        YQ_TRY(B.append(&proj[p].program, t));
-        if (t != proj[p].out_type || t != out[p].type || !ProgramBuilder::valid_column(out[p])) return YQ_ERR_INVALID_ARG;
-        o.width = out[p].width;
-        YQ_TRY(B.emit(OP_EMIT_PROJ, (uint8_t)p, 0, (uint8_t)t));
-      }
-    }
-    B.finalize();
-    memcpy(&F.P, &B.P, sizeof(VmProgram));
-    F.proj_end = B.len;
-    F.nproj = nproj;
-    F.capacity = capacity;
-  }
+  YQ_TRY(build_project_params(batch, predicate, constants, proj, nproj, out, capacity, F));
   const uint32_t rows = batch->rows;
   if (rows == 0) {
     if (count_device) YQ_TRY_CUDA(cudaMemsetAsync(count_device, 0, sizeof(uint32_t), s));
     if (count_host) *count_host = 0;
     return YQ_OK;
   }
-  const uint32_t ntiles = ceil_div<uint32_t>(rows, kRowTile);
+  const uint32_t ntiles = ceil_div<uint32_t>(rows, kStepRows);
   Workspace ws;
   YQ_TRY(ws.acquire(workspace, workspace_bytes, yq_filter_project_workspace_size(rows), s));
   unsigned long long* status = ws.take<unsigned long long>((size_t)ntiles + 1);
@@ -492,13 +548,7 @@ int yq_filter_project(const yq_batch* batch, const yq_program* predicate, const 
   YQ_TRY_CUDA(cudaMemsetAsync(status, 0, ((size_t)ntiles + 1) * sizeof(unsigned long long), s));
   YQ_TRY_CUDA(cudaMemsetAsync(misc, 0, 4 * sizeof(uint32_t), s));
   uint32_t* cnt_dev = count_device ? count_device : misc + 2;
-  {
-    // algorithmic bytes: referenced input columns (outputs depend on selectivity)
-    const double in_b = referenced_row_bytes(F.P, F.proj_end);
-    ProfScope ps("filter_project", s, (double)rows * in_b);
-    k_filter_project<<<ntiles, kRowBlock, 0, s>>>(F, rows, misc, status, cnt_dev, misc + 1);
-    YQ_CHECK_LAUNCH();
-  }
+  YQ_TRY(launch_filter_project(F, rows, misc, status, cnt_dev, s));
   if (count_host) {
     uint32_t h[2];
     YQ_TRY_CUDA(cudaMemcpyAsync(&h[0], cnt_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
@@ -523,7 +573,7 @@ int yq_filter_project(const yq_batch* batch, const yq_program* predicate, const 
 
 namespace yq {
 
-constexpr uint32_t kNoAllocTiles = YQ_FILTER_PROJECT_NOALLOC_MAX_ROWS / kRowTile;
+constexpr uint32_t kNoAllocTiles = YQ_FILTER_PROJECT_NOALLOC_MAX_ROWS / kStepRows;
 constexpr size_t kNoAllocWords = 2 + (size_t)kNoAllocTiles + 1;  // 2 words hold the four counters
 
 static __device__ __align__(256) unsigned long long g_filter_project_scratch[kNoAllocWords];
@@ -550,48 +600,6 @@ static int noalloc_scratch(unsigned long long** out) {
   return YQ_OK;
 }
 
-// Same validation and program build as yq_filter_project.
-static int build_project_params(const yq_batch* batch, const yq_program* predicate, const yq_constants* constants,
-                                const yq_projection* proj, int32_t nproj, yq_column* out, uint32_t capacity,
-                                FPParams& F) {
-  if (!batch || nproj < 0 || nproj > YQ_MAX_PROJECTIONS || (nproj > 0 && (!proj || !out))) return YQ_ERR_INVALID_ARG;
-  ProgramBuilder B;
-  YQ_TRY(B.set_columns(batch->columns, batch->ncols));
-  YQ_TRY(B.set_constants(constants));
-  if (predicate && predicate->len > 0) {
-    int t = -1;
-    YQ_TRY(B.append(predicate, t));
-    if (t != YQ_BOOL) return YQ_ERR_INVALID_ARG;
-    YQ_TRY(B.emit(OP_EMIT_PRED, 0, 0, YQ_BOOL));
-  }
-  F.pred_end = B.len;
-  for (int p = 0; p < nproj; ++p) {
-    DevOut& o = F.out[p];
-    o.data = static_cast<char*>(out[p].data);
-    o.nulls = const_cast<uint8_t*>(out[p].nulls);
-    o.src_col = proj[p].column;
-    if (!o.data && capacity > 0) return YQ_ERR_INVALID_ARG;
-    if (proj[p].column >= 0) {
-      if (proj[p].column >= batch->ncols) return YQ_ERR_INVALID_ARG;
-      const yq_column& c = batch->columns[proj[p].column];
-      if (out[p].type != c.type || out[p].width != c.width) return YQ_ERR_INVALID_ARG;
-      o.width = c.width;
-    } else {
-      int t = -1;
-      YQ_TRY(B.append(&proj[p].program, t));
-      if (t != proj[p].out_type || t != out[p].type || !ProgramBuilder::valid_column(out[p])) return YQ_ERR_INVALID_ARG;
-      o.width = out[p].width;
-      YQ_TRY(B.emit(OP_EMIT_PROJ, (uint8_t)p, 0, (uint8_t)t));
-    }
-  }
-  B.finalize();
-  memcpy(&F.P, &B.P, sizeof(VmProgram));
-  F.proj_end = B.len;
-  F.nproj = nproj;
-  F.capacity = capacity;
-  return YQ_OK;
-}
-
 }  // namespace yq
 
 extern "C" int yq_filter_project_noalloc(const yq_batch* batch, const yq_program* predicate,
@@ -611,14 +619,13 @@ extern "C" int yq_filter_project_noalloc(const yq_batch* batch, const yq_program
   }
   unsigned long long* scratch = nullptr;
   YQ_TRY(noalloc_scratch(&scratch));
-  const uint32_t ntiles = ceil_div<uint32_t>(rows, kRowTile);
+  const uint32_t ntiles = ceil_div<uint32_t>(rows, kStepRows);
   uint32_t* misc = reinterpret_cast<uint32_t*>(scratch);  // [0] tile counter, [1] error, [2] count
   unsigned long long* status = scratch + 2;
   // The previous call's values are still there: clear what this call reads.
   YQ_TRY_CUDA(cudaMemsetAsync(scratch, 0, (2 + (size_t)ntiles + 1) * sizeof(unsigned long long), s));
   uint32_t* cnt_dev = count_device ? count_device : misc + 2;
-  k_filter_project<<<ntiles, kRowBlock, 0, s>>>(F, rows, misc, status, cnt_dev, misc + 1);
-  YQ_CHECK_LAUNCH();
+  YQ_TRY(launch_filter_project(F, rows, misc, status, cnt_dev, s));
   if (count_host) {
     uint32_t h[2];
     YQ_TRY_CUDA(cudaMemcpyAsync(&h[0], cnt_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));

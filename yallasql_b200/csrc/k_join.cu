@@ -22,7 +22,9 @@
 #include <string.h>
 #include <vector>
 #include "vm_host.cuh"
+#include "yq_agg.cuh"
 #include "yq_lookback.cuh"
+#include "yq_stage.cuh"
 
 namespace yq {
 
@@ -209,12 +211,6 @@ struct BuildParams {
   uint32_t* counts;   // [0] rows kept, [1] duplicate keys seen
 };
 
-struct SelEmit {
-  uint32_t sel;
-  __device__ __forceinline__ void pred(uint32_t bits) { sel &= bits; }
-  __device__ __forceinline__ void agg(int, int, int, const Val&) {}
-  __device__ __forceinline__ void proj(int, const Val&) {}
-};
 
 constexpr int kBuildBlock = 1024;
 
@@ -236,8 +232,13 @@ __global__ void __launch_bounds__(kBuildBlock) k_hash_build(const __grid_constan
     SelEmit E;
     E.sel = inr;
     if (B.pred_len > 0) {
+      Ctx X;
+      X.tile0 = base;
+      X.lr = threadIdx.x * ITEMS;
+      X.inr = inr;
+      X.stage = 0;
       Stack S;
-      run_vm(B.P, 0, B.pred_len, row0, inr, inr == 0xfu, S, E);
+      run_vm<false>(B.P, 0, B.pred_len, X, S, E);
     }
     // key NULLs never join
     for (int k = 0; k < ITEMS; ++k)
@@ -432,114 +433,106 @@ __global__ void __launch_bounds__(256) k_cross_fill(const __grid_constant__ Join
 
 // ------------------------------------------------ fused star-join aggregate
 struct JAParams {
-  VmProgram P;           // fact predicate [0, pred_end) then aggregate inputs [pred_end, pc_end)
+  VmProgram P;  // fact predicate [0, pred_end) then aggregate inputs [pred_end, pc_end)
+  StagePlan SP;
   int32_t pred_end, pc_end;
-  int32_t nagg;
-  uint8_t upd[YQ_MAX_AGGREGATES];
+  AggParams A;
+  int32_t fkey_col;  // fact key column (staged with the others when the ring is used)
   JCol fkey;
   uint32_t nbuckets, hrows_n;
+  uint32_t table_off;  // byte offset of the dimension table in dynamic shared memory
   const uint32_t* bstart;
   const unsigned long long* hkeys;
 };
 
-struct JAggEmit {
-  uint32_t sel;
-  Acc acc[YQ_MAX_AGGREGATES];
-  __device__ __forceinline__ void pred(uint32_t bits) { sel &= bits; }
-  __device__ __forceinline__ void agg(int a, int upd, int t, const Val& x) {
-    switch (a) {
-#define YQ_JAGG_CASE(k) \
-  case k: acc_update(acc[k], upd, t, x, sel); break;
-      YQ_JAGG_CASE(0) YQ_JAGG_CASE(1) YQ_JAGG_CASE(2) YQ_JAGG_CASE(3)
-      YQ_JAGG_CASE(4) YQ_JAGG_CASE(5) YQ_JAGG_CASE(6) YQ_JAGG_CASE(7)
-#undef YQ_JAGG_CASE
-      default: break;
-    }
-  }
-  __device__ __forceinline__ void proj(int, const Val&) {}
-};
+// Normalised key from the raw bits of a cell (as hash_key).
+__device__ __forceinline__ uint64_t norm_key(int type, uint64_t raw) {
+  uint64_t v = raw;
+  if (type == YQ_INT32) v = (uint64_t)(int64_t)(int32_t)(uint32_t)raw;
+  if (type == YQ_FLOAT32 && ((uint32_t)v & 0x7fffffffu) == 0u) v = 0;
+  if (type == YQ_FLOAT64 && (v & 0x7fffffffffffffffull) == 0ull) v = 0;
+  return v;
+}
 
-__global__ void __launch_bounds__(kJoinBlock) k_join_aggregate(const __grid_constant__ JAParams F, uint32_t n,
-                                                               Acc* __restrict__ partials, uint32_t* ticket,
-                                                               Acc* __restrict__ state) {
-  extern __shared__ uint32_t sm[];
-  uint32_t* s_bstart = sm;
-  unsigned long long* s_keys = reinterpret_cast<unsigned long long*>(sm + ((F.nbuckets + 2) & ~1u));
-  for (uint32_t i = threadIdx.x; i <= F.nbuckets; i += kJoinBlock) s_bstart[i] = __ldg(F.bstart + i);
-  for (uint32_t i = threadIdx.x; i < F.hrows_n; i += kJoinBlock) s_keys[i] = __ldg(F.hkeys + i);
+template <bool STAGED>
+__global__ void __launch_bounds__(kRowBlock, 2) k_join_aggregate(const __grid_constant__ JAParams F, uint32_t n,
+                                                                 Acc* __restrict__ partials, uint32_t* ticket,
+                                                                 Acc* state) {
+  uint32_t* s_bstart = reinterpret_cast<uint32_t*>(yq_dyn_smem + F.table_off);
+  unsigned long long* s_keys =
+      reinterpret_cast<unsigned long long*>(yq_dyn_smem + F.table_off + 4 * ((F.nbuckets + 2) & ~1u));
+  for (uint32_t i = threadIdx.x; i <= F.nbuckets; i += kRowBlock) s_bstart[i] = __ldg(F.bstart + i);
+  for (uint32_t i = threadIdx.x; i < F.hrows_n; i += kRowBlock) s_keys[i] = __ldg(F.hkeys + i);
   __syncthreads();
 
-  JAggEmit E;
-#pragma unroll
-  for (int a = 0; a < YQ_MAX_AGGREGATES; ++a) acc_init(E.acc[a], a < F.nagg ? F.upd[a] : UPD_COUNT);
-  const uint32_t tile_rows = kJoinBlock * ITEMS;
-  const uint32_t ntiles = ceil_div<uint32_t>(n, tile_rows);
-  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const uint32_t row0 = tile * tile_rows + threadIdx.x * ITEMS;
-    uint32_t inr = 0;
-    if (row0 < n) inr = (n - row0 >= (uint32_t)ITEMS) ? 0xfu : ((1u << (n - row0)) - 1u);
-    E.sel = inr;
-    Stack S;
-    if (F.pred_end > 0) run_vm(F.P, 0, F.pred_end, row0, inr, inr == 0xfu, S, E);
+  uint32_t* err = agg_state_err(state);
+  AggEmit E;
+  agg_thread_init(E, F.A);
+  uint32_t nsel = 0;
+  const uint32_t ntiles = ceil_div<uint32_t>(n, kStepRows);
+  const uint32_t G = gridDim.x;
+  int S = 1;
+  if constexpr (STAGED) {
+    S = F.SP.nstages;
+    stage_init(F.SP);
+    if (threadIdx.x == 0)
+      for (int j = 0; j < S - 1; ++j) {
+        const uint32_t t = blockIdx.x + (uint32_t)j * G;
+        if (t < ntiles && full_step(t, n)) stage_issue(F.SP, j, t * kStepRows);
+      }
+  }
+  const DevCol& kc = F.P.cols[F.fkey_col];
+  int slot = 0;
+  uint32_t parity = 0;
+  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += G) {
+    Ctx X;
+    X.tile0 = tile * kStepRows;
+    X.lr = threadIdx.x * ITEMS;
+    X.inr = in_range_bits(X.tile0 + X.lr, n);
+    X.stage = 0;
+    if constexpr (STAGED) {
+      __syncthreads();  // every thread is done with the previous step: its slot is free
+      if (threadIdx.x == 0) {
+        const uint32_t t = tile + (uint32_t)(S - 1) * G;
+        const int ns = slot == 0 ? S - 1 : slot - 1;
+        if (t < ntiles && full_step(t, n)) stage_issue(F.SP, ns, t * kStepRows);
+      }
+      stage_step(F.SP, slot, parity, tile, n, err);
+      X.stage = (uint32_t)slot * F.SP.stage_bytes;
+    }
+    E.sel = X.inr;
+    Stack St;
+    if (F.pred_end > 0) run_vm<STAGED>(F.P, 0, F.pred_end, X, St, E);
     // probe: keep rows whose key is present among the (unique) dimension keys
+    const uint32_t knull = null_bits<STAGED>(kc, X);
+#pragma unroll
     for (int k = 0; k < ITEMS; ++k) {
       if (!(E.sel >> k & 1u)) continue;
-      const uint32_t row = row0 + k;
       bool hit = false;
-      if (!cell_null(F.fkey, row)) {
-        const uint64_t key = hash_key(F.fkey, row);
+      if (!(knull >> k & 1u)) {
+        uint64_t key;
+        if constexpr (STAGED) {
+          const unsigned char* p = yq_dyn_smem + X.stage + kc.soff + (X.lr + k) * (uint32_t)kc.width;
+          const uint64_t raw = kc.width == 8   ? *reinterpret_cast<const unsigned long long*>(p)
+                               : kc.width == 4 ? (uint64_t)*reinterpret_cast<const uint32_t*>(p)
+                                               : (uint64_t)*p;
+          key = norm_key(kc.type, raw);
+        } else {
+          key = hash_key(F.fkey, X.tile0 + X.lr + k);
+        }
         const uint32_t b = hash_bucket(key, F.nbuckets);
         for (uint32_t x = s_bstart[b]; x < s_bstart[b + 1] && !hit; ++x) hit = (s_keys[x] == key);
       }
       if (!hit) E.sel &= ~(1u << k);
     }
-    run_vm(F.P, F.pred_end, F.pc_end, row0, inr, inr == 0xfu, S, E);
-#pragma unroll
-    for (int a = 0; a < YQ_MAX_AGGREGATES; ++a)
-      if (a < F.nagg && F.upd[a] == UPD_COUNT_STAR) E.acc[a].cnt += __popc(E.sel);
-  }
-  __shared__ Acc s_acc[kJoinBlock / 32][YQ_MAX_AGGREGATES];
-  __shared__ bool s_last;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int a = 0; a < YQ_MAX_AGGREGATES; ++a) {
-    if (a < F.nagg) {
-#pragma unroll
-      for (int d = 16; d > 0; d >>= 1) acc_shfl_down(E.acc[a], d, F.upd[a]);
-      if (lane == 0) s_acc[warp][a] = E.acc[a];
+    run_vm<STAGED>(F.P, F.pred_end, F.pc_end, X, St, E);
+    nsel += __popc(E.sel);
+    if (++slot == S) {
+      slot = 0;
+      parity ^= 1u;
     }
   }
-  __syncthreads();
-  if (threadIdx.x < F.nagg) {
-    const int a = threadIdx.x;
-    Acc t = s_acc[0][a];
-    for (int w = 1; w < kJoinBlock / 32; ++w) acc_combine(t, s_acc[w][a], F.upd[a]);
-    partials[blockIdx.x * YQ_MAX_AGGREGATES + a] = t;
-  }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  if (threadIdx.x < F.nagg) {
-    const int a = threadIdx.x;
-    const int upd = F.upd[a];
-    Acc t;
-    acc_init(t, upd);
-    for (uint32_t b = 0; b < gridDim.x; ++b) {
-      const Acc* p = partials + b * YQ_MAX_AGGREGATES + a;
-      Acc q;
-      q.cnt = __ldcg(&p->cnt);
-      q.i = __ldcg(&p->i);
-      q.f = __ldcg(&p->f);
-      acc_combine(t, q, upd);
-    }
-    Acc s = state[a];
-    acc_combine(s, t, upd);
-    state[a] = s;
-  }
-  if (threadIdx.x == 0) *ticket = 0u;
+  agg_block_finish<kRowBlock>(E, nsel, F.A, partials, ticket, state);
 }
 
 // ---------------------------------------------------------------- host
@@ -586,7 +579,7 @@ static int build_table(const yq_batch* right, const yq_program* pred, const yq_c
     if (t != YQ_BOOL) return YQ_ERR_INVALID_ARG;
     YQ_TRY(PB.emit(OP_EMIT_PRED, 0, 0, YQ_BOOL));
   }
-  PB.finalize();
+  YQ_TRY(PB.finalize());
   memcpy(&B.P, &PB.P, sizeof(VmProgram));
   B.pred_len = PB.len;
   B.key = jcol(right->columns[key_col]);
@@ -802,7 +795,7 @@ int yq_join_aggregate(const yq_batch* fact, const yq_program* fact_predicate, in
       if (t != YQ_BOOL) return YQ_ERR_INVALID_ARG;
       YQ_TRY(B.emit(OP_EMIT_PRED, 0, 0, YQ_BOOL));
     }
-    F.pred_end = B.len;
+    const int pred_end = B.len;
     for (int a = 0; a < nagg; ++a) {
       const yq_agg_spec& g = aggs[a];
       if (g.kind < YQ_AGG_COUNT_STAR || g.kind > YQ_AGG_MAX) return YQ_ERR_INVALID_ARG;
@@ -816,17 +809,20 @@ int yq_join_aggregate(const yq_batch* fact, const yq_program* fact_predicate, in
         case YQ_AGG_MIN: upd = flt ? UPD_MIN_F : UPD_MIN_I; break;
         default: upd = flt ? UPD_MAX_F : UPD_MAX_I; break;
       }
-      F.upd[a] = upd;
+      F.A.upd[a] = upd;
       if (g.kind == YQ_AGG_COUNT_STAR) continue;
       int t = -1;
       YQ_TRY(B.append(&g.input, t));
       if (g.kind != YQ_AGG_COUNT && t != g.input_type) return YQ_ERR_INVALID_ARG;
       YQ_TRY(B.emit(OP_EMIT_AGG, (uint8_t)a, upd, (uint8_t)t));
     }
-    B.finalize();
+    YQ_TRY(B.finalize());
+    F.fkey_col = fact_key;
+    if (!plan_stages(B.P, B.used_cols | (1u << fact_key), F.SP)) F.SP.nstages = 0;
     memcpy(&F.P, &B.P, sizeof(VmProgram));
+    F.pred_end = B.remap[pred_end];
     F.pc_end = B.len;
-    F.nagg = nagg;
+    F.A.nagg = nagg;
   }
   if (fact->rows == 0 || nagg == 0) return YQ_OK;
   const uint32_t nbuckets = pow2_at_least(dim->rows ? dim->rows : 1);
@@ -849,41 +845,36 @@ int yq_join_aggregate(const yq_batch* fact, const yq_program* fact_predicate, in
   F.hrows_n = counts[0];
   F.bstart = d_bstart;
   F.hkeys = d_hkeys;
-  const size_t smem = table_smem(nbuckets, counts[0], false);
-  static size_t attr = 0;
-  if (smem > 48 * 1024 && smem > attr) {
-    YQ_TRY_CUDA(cudaFuncSetAttribute(k_join_aggregate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = smem;
+  const size_t table = table_smem(nbuckets, counts[0], false);
+  // The ring leaves room for the table; with too few stages left the kernel
+  // reads the fact columns from global memory.
+  const size_t budget = kStageBudget + 8 * 1024;
+  if (F.SP.nstages && stage_smem_bytes(F.SP) + table > budget) {
+    const int fit = (int)((budget > table ? budget - table : 0) / (F.SP.stage_bytes + 8));
+    F.SP.nstages = fit >= 2 ? (fit > kStageMax ? kStageMax : fit) : 0;
+  }
+  const bool staged = F.SP.nstages > 0;
+  F.table_off = (uint32_t)align_up(stage_smem_bytes(F.SP), 16);
+  const size_t smem = F.table_off + table;
+  const void* kern = staged ? (const void*)k_join_aggregate<true> : (const void*)k_join_aggregate<false>;
+  static size_t attr[2] = {0, 0};
+  if (smem > 48 * 1024 && smem > attr[staged]) {
+    YQ_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr[staged] = smem;
   }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_join_aggregate, kJoinBlock, smem) != cudaSuccess ||
-      per_sm < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kRowBlock, smem) != cudaSuccess || per_sm < 1)
     per_sm = 1;
   if (per_sm > 8) per_sm = 8;
-  const uint32_t tiles = ceil_div<uint32_t>(fact->rows, kJoinBlock * ITEMS);
+  const uint32_t tiles = ceil_div<uint32_t>(fact->rows, kStepRows);
   int grid = sm_count() * per_sm;
   if ((uint32_t)grid > tiles) grid = (int)tiles;
-  double row_bytes = fk.width;
-  {
-    bool used[YQ_MAX_BATCH_COLUMNS] = {false};
-    used[fact_key] = true;
-    for (int i = 0; i < F.pc_end; ++i) {
-      const Insn& I = F.P.code[i];
-      switch (I.op & OP_MASK) {
-        case OP_COL: used[I.a] = true; break;
-        case OP_ARITH_COL:
-        case OP_CMP_COL_CONST:
-        case OP_AND_CMP_COL_CONST: used[I.b] = true; break;
-        case OP_CMP_COL_COL: used[I.b] = true; used[I.imm] = true; break;
-        default: break;
-      }
-    }
-    row_bytes = 0;
-    for (int c = 0; c < fact->ncols; ++c)
-      if (used[c]) row_bytes += fact->columns[c].width + (fact->columns[c].nulls ? 1 : 0);
-  }
+  const double row_bytes = row_bytes_of(F.P, program_columns(F.P, F.pc_end, 1u << fact_key));
   ProfScope ps("join_aggregate", s, (double)fact->rows * row_bytes);
-  k_join_aggregate<<<grid, kJoinBlock, smem, s>>>(F, fact->rows, partials, d_misc, static_cast<Acc*>(state));
+  if (staged)
+    k_join_aggregate<true><<<grid, kRowBlock, smem, s>>>(F, fact->rows, partials, d_misc, static_cast<Acc*>(state));
+  else
+    k_join_aggregate<false><<<grid, kRowBlock, smem, s>>>(F, fact->rows, partials, d_misc, static_cast<Acc*>(state));
   YQ_CHECK_LAUNCH();
   return YQ_OK;
 }

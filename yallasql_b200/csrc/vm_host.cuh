@@ -1,6 +1,7 @@
 // Host-side loader for expression programs: validates a client's postfix
-// program against the batch schema, applies peephole fusions, and annotates
-// each instruction with the stack moves it needs (see yq_vm.cuh).
+// program against the batch schema, applies peephole fusions, and resolves
+// each instruction into the kernels' opcode for its operation, value class and
+// operator, with the stack moves it needs (see yq_vm.cuh).
 #pragma once
 
 #include <string.h>
@@ -10,11 +11,17 @@ namespace yq {
 
 struct ProgramBuilder {
   VmProgram P;
+  Insn code[kMaxInsns];  // loader form; resolved into P.code by finalize()
   int len = 0;
   int nconsts = 0;
   int ntext = 0;
+  uint32_t used_cols = 0;    // bit c: column c is read by the program (after finalize)
+  int remap[kMaxInsns + 1];  // after finalize: loader index -> resolved index
 
-  ProgramBuilder() { memset(&P, 0, sizeof(P)); }
+  ProgramBuilder() {
+    memset(&P, 0, sizeof(P));
+    memset(code, 0, sizeof(code));
+  }
 
   int set_columns(const yq_column* cols, int ncols) {
     if (ncols < 0 || ncols > YQ_MAX_BATCH_COLUMNS || (ncols > 0 && !cols)) return YQ_ERR_INVALID_ARG;
@@ -26,9 +33,11 @@ struct ProgramBuilder {
       d.data = static_cast<const char*>(c.data);
       d.nulls = c.nulls;
       d.type = c.type;
+      d.tc = type_class(c.type);
       d.width = c.width;
       d.vec = ((reinterpret_cast<uintptr_t>(c.data) & 15u) == 0);
       d.nvec = ((reinterpret_cast<uintptr_t>(c.nulls) & 3u) == 0);
+      d.soff = d.snoff = 0;
     }
     return YQ_OK;
   }
@@ -182,7 +191,7 @@ struct ProgramBuilder {
       if (depth + pushes > 4) return YQ_ERR_UNSUPPORTED;  // deeper than the register stack
       for (int p = 0; p < pushes; ++p) types[depth++] = out_t;
       if (len >= kMaxInsns - 1) return YQ_ERR_UNSUPPORTED;
-      P.code[len++] = I;
+      code[len++] = I;
       peephole(start);
     }
     if (depth != 1) return YQ_ERR_INVALID_ARG;
@@ -194,8 +203,8 @@ struct ProgramBuilder {
   void peephole(int start) {
     for (;;) {
       if (len - start >= 2) {
-        Insn& x = P.code[len - 2];
-        Insn& y = P.code[len - 1];
+        Insn& x = code[len - 2];
+        Insn& y = code[len - 1];
         // COL c ; CAST c.type->t   =>  COL c as t (only from the column's own type)
         if (x.op == OP_COL && y.op == OP_CAST && x.type == y.type && x.type == col_type(x.a)) {
           x.type = y.a;
@@ -204,9 +213,9 @@ struct ProgramBuilder {
         }
       }
       if (len - start >= 3) {
-        Insn& x = P.code[len - 3];
-        Insn& y = P.code[len - 2];
-        Insn& z = P.code[len - 1];
+        Insn& x = code[len - 3];
+        Insn& y = code[len - 2];
+        Insn& z = code[len - 1];
         // <bool> ; CMP_COL_CONST ; AND  =>  <bool> ; AND_CMP_COL_CONST
         if (y.op == OP_CMP_COL_CONST && z.op == OP_AND && produces_value(x)) {
           y.op = OP_AND_CMP_COL_CONST;
@@ -244,50 +253,165 @@ struct ProgramBuilder {
   // True when x leaves a value on the stack that the next instruction's
   // fused form may consume (any non-emit instruction).
   static bool produces_value(const Insn& x) {
-    uint8_t op = x.op & OP_MASK;
-    return op != OP_EMIT_PRED && op != OP_EMIT_AGG && op != OP_EMIT_PROJ && op != OP_END;
+    return x.op != OP_EMIT_PRED && x.op != OP_EMIT_AGG && x.op != OP_EMIT_PROJ;
   }
 
   int emit(uint8_t op, uint8_t a, uint8_t b, uint8_t type) {
     if (len >= kMaxInsns) return YQ_ERR_UNSUPPORTED;
     Insn I;
     I.op = op; I.a = a; I.b = b; I.type = type; I.imm = 0;
-    P.code[len++] = I;
+    code[len++] = I;
     return YQ_OK;
   }
 
-  // Set the stack-move flags from the depth before each instruction.
-  void finalize() {
-    int depth = 0;
+  static int agg_kind(int upd, int cls) {
+    switch (upd) {
+      case UPD_SUM_I: return cls == TC_I32 ? AK_SUM_I32 : AK_SUM_I64;
+      case UPD_SUM_F: return cls == TC_F32 ? AK_SUM_F32 : AK_SUM_F64;
+      case UPD_MIN_I: return cls == TC_I32 ? AK_MIN_I32 : AK_MIN_I64;
+      case UPD_MAX_I: return cls == TC_I32 ? AK_MAX_I32 : AK_MAX_I64;
+      case UPD_MIN_F: return cls == TC_F32 ? AK_MIN_F32 : AK_MIN_F64;
+      case UPD_MAX_F: return cls == TC_F32 ? AK_MAX_F32 : AK_MAX_F64;
+      default: return AK_COUNT;
+    }
+  }
+
+  static Insn mk(uint8_t op, uint8_t type, uint8_t a, uint8_t b, int32_t imm) {
+    Insn I;
+    I.op = op; I.type = type; I.a = a; I.b = b; I.imm = imm;
+    return I;
+  }
+
+  // Resolve the loader form into P.code. A fused comparison whose column is
+  // not already of the comparison's class runs as its plain sequence, and a
+  // BOOL aggregate input is widened to INT64 first. Resolved programs end up
+  // in P.code[0, len); `remap` maps loader positions (such as the end of a
+  // predicate) to resolved ones and `used_cols` lists the columns read.
+  int finalize() {
+    Insn x[kMaxInsns];
+    int m = 0;
+    auto put = [&](const Insn& I) {
+      if (m >= kMaxInsns) return false;
+      x[m++] = I;
+      return true;
+    };
     for (int i = 0; i < len; ++i) {
-      Insn& I = P.code[i];
-      const uint8_t op = I.op & OP_MASK;
-      I.op = op;
-      switch (op) {
+      const Insn& I = code[i];
+      remap[i] = m;
+      bool ok = true;
+      if ((I.op == OP_CMP_COL_CONST || I.op == OP_AND_CMP_COL_CONST) && I.type != YQ_TEXT &&
+          P.cols[I.b].tc != type_class(I.type)) {
+        ok = put(mk(OP_COL, I.type, I.b, 0, 0)) && put(mk(OP_CONST, I.type, 0, 0, I.imm)) &&
+             put(mk(OP_CMP, I.type, I.a, 0, 0)) && (I.op == OP_CMP_COL_CONST || put(mk(OP_AND, YQ_BOOL, 0, 0, 0)));
+      } else if (I.op == OP_CMP_COL_COL && I.type != YQ_TEXT &&
+                 (P.cols[I.b].tc != type_class(I.type) || P.cols[I.imm].tc != type_class(I.type))) {
+        ok = put(mk(OP_COL, I.type, I.b, 0, 0)) && put(mk(OP_COL, I.type, (uint8_t)I.imm, 0, 0)) &&
+             put(mk(OP_CMP, I.type, I.a, 0, 0));
+      } else if (I.op == OP_EMIT_AGG && I.type == YQ_BOOL && I.b != UPD_COUNT && I.b != UPD_COUNT_STAR) {
+        ok = put(mk(OP_CAST, YQ_BOOL, YQ_INT64, 0, 0)) && put(mk(OP_EMIT_AGG, YQ_INT64, I.a, I.b, 0));
+      } else {
+        ok = put(I);
+      }
+      if (!ok) return YQ_ERR_UNSUPPORTED;
+    }
+    remap[len] = m;
+    int depth = 0;
+    used_cols = 0;
+    for (int i = 0; i < m; ++i) {
+      const Insn& I = x[i];
+      RInsn R;
+      memset(&R, 0, sizeof(R));
+      int pushes = 0, pops = 0;
+      const int tc = type_class(I.type);
+      switch (I.op) {
         case OP_COL:
+          R.opc = (uint16_t)(R_COL + tc);
+          R.a = I.a;
+          used_cols |= 1u << I.a;
+          pushes = 1;
+          break;
         case OP_CONST:
+          R.opc = (uint16_t)(R_CONST + tc);
+          R.imm = (uint16_t)I.imm;
+          pushes = 1;
+          break;
         case OP_NULL:
-        case OP_CMP_COL_CONST:
-        case OP_CMP_COL_COL:
-          if (depth >= 1) I.op |= OPF_PUSH;
-          ++depth;
+          R.opc = R_NULL;
+          pushes = 1;
+          break;
+        case OP_CAST:
+          R.opc = (uint16_t)(R_CAST + tc * 5 + type_class(I.a));
           break;
         case OP_ARITH:
+          R.opc = (uint16_t)(R_ARITH + tc * 5 + I.a);
+          pops = 2;
+          break;
+        case OP_ARITH_COL:
+          R.opc = (uint16_t)(R_ARITH_COL + tc * 5 + I.a);
+          R.b = I.b;
+          used_cols |= 1u << I.b;
+          break;
+        case OP_ARITH_CONST:
+          R.opc = (uint16_t)(R_ARITH_CONST + tc * 5 + I.a);
+          R.imm = (uint16_t)I.imm;
+          break;
         case OP_CMP:
-        case OP_AND:
-        case OP_OR:
-          if (depth >= 3) I.op |= OPF_POPSHIFT;
-          --depth;
+          R.opc = (uint16_t)(R_CMP + tc * 6 + I.a);
+          pops = 2;
           break;
-        case OP_EMIT_PRED:
+        case OP_CMP_COL_CONST:
+        case OP_AND_CMP_COL_CONST:
+          R.opc = (uint16_t)(R_CMP_CC + tc * 6 + I.a);
+          R.b = I.b;
+          R.imm = (uint16_t)I.imm;
+          used_cols |= 1u << I.b;
+          if (I.op == OP_AND_CMP_COL_CONST) R.flags |= RF_AND;
+          else pushes = 1;
+          break;
+        case OP_CMP_COL_COL:
+          R.opc = (uint16_t)(R_CMP_CCOL + tc * 6 + I.a);
+          R.b = I.b;
+          R.c = (uint8_t)I.imm;
+          used_cols |= (1u << I.b) | (1u << I.imm);
+          pushes = 1;
+          break;
+        case OP_AND: R.opc = R_AND; pops = 2; break;
+        case OP_OR: R.opc = R_OR; pops = 2; break;
+        case OP_NOT: R.opc = R_NOT; break;
+        case OP_IS_NULL: R.opc = R_IS_NULL; break;
+        case OP_IS_NOT_NULL: R.opc = R_IS_NOT_NULL; break;
+        case OP_EMIT_PRED: R.opc = R_EMIT_PRED; pops = 1; break;
         case OP_EMIT_AGG:
-        case OP_EMIT_PROJ:
-          if (depth >= 2) I.op |= OPF_POPSHIFT;
-          --depth;
+          R.opc = (uint16_t)(R_EMIT_AGG + agg_kind(I.b, tc));
+          R.a = I.a;
+          pops = 1;
           break;
-        default: break;  // in-place ops keep the depth
+        case OP_EMIT_PROJ: {
+          const int w = tc == TC_BOOL ? 0 : ((tc == TC_I32 || tc == TC_F32) ? 1 : 2);
+          R.opc = (uint16_t)(R_EMIT_PROJ + w);
+          R.a = I.a;
+          pops = 1;
+          break;
+        }
+        default: return YQ_ERR_INVALID_ARG;
       }
+      if (pushes) {
+        if (depth >= 4) return YQ_ERR_UNSUPPORTED;
+        R.flags |= (uint8_t)(depth < 3 ? depth : 3);
+        ++depth;
+      } else if (pops == 2) {
+        if (depth < 2) return YQ_ERR_INVALID_ARG;
+        R.flags |= (uint8_t)(depth - 2);
+        --depth;
+      } else if (pops == 1) {
+        if (depth < 1) return YQ_ERR_INVALID_ARG;
+        R.flags |= (uint8_t)(depth - 1 < 3 ? depth - 1 : 3);
+        --depth;
+      }
+      P.code[i] = R;
     }
+    len = m;
+    return YQ_OK;
   }
 };
 

@@ -180,4 +180,49 @@ __device__ __forceinline__ uint32_t block_exclusive_sum(uint32_t x, uint32_t* s_
   return excl;
 }
 
+// ---------------------------------------------- mbarrier + 1-D bulk copies
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+// 1-D bulk copy global -> shared (both 16-byte aligned, bytes % 16 == 0).
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Bounded wait for phase `parity` of `bar`. When the bound runs out, thread 0
+// sets kErrTimeout in *err and the copies still in flight get one more
+// bounded wait before the caller goes on (its data is then not used as valid:
+// the error word fails the call).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t* err) {
+  uint32_t spins = 0;
+  bool done = mbar_try_wait(bar, parity);
+  while (!done && ++spins < kSpinLimit) done = mbar_try_wait(bar, parity);
+  if (done) return true;
+  if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
+  for (uint32_t s2 = 0; s2 < kSpinLimit && !mbar_try_wait(bar, parity); ++s2) {
+  }
+  return false;
+}
+
 }  // namespace yq

@@ -1,0 +1,164 @@
+// Shared-memory staging of column tiles for the row kernels (sm_100a).
+//
+// A block processes steps of kStepRows consecutive rows. The columns a
+// program reads are laid out back to back in one stage (each column's
+// kStepRows values, then its null bytes when it has them); a ring of 2-4
+// stages in dynamic shared memory is filled by 1-D bulk copies
+// (cp.async.bulk global -> shared, no multicast) that complete on one
+// mbarrier per stage, so the copies of the next steps are in flight while the
+// expression machine works on the current one. A step that is not full (the
+// last rows of the batch) is copied with plain loads and zero padded.
+#pragma once
+
+#include <string.h>
+#include "yq_vm.cuh"
+
+namespace yq {
+
+constexpr int kRowBlock = 256;
+constexpr uint32_t kStepRows = kRowBlock * ITEMS;  // 1024 rows per step
+constexpr int kStageMax = 4;
+// Dynamic shared memory one block may use for its ring (two blocks per SM).
+constexpr size_t kStageBudget = 110 * 1024;
+
+struct StageCopy {
+  const char* src;     // first row of the column (16-byte aligned)
+  uint32_t row_bytes;  // bytes per row
+  uint32_t soff;       // offset in the stage
+};
+
+struct StagePlan {
+  int32_t ncopy;
+  int32_t nstages;       // 0 = columns are read from global memory
+  uint32_t stage_bytes;  // bytes of one stage (multiple of 128)
+  uint32_t tx_bytes;     // bytes a full step copies
+  StageCopy c[2 * YQ_MAX_BATCH_COLUMNS];
+};
+
+// Lays the columns of `mask` out in one stage and sizes the ring. Returns
+// false (nstages = 0) when a column or null array is not 16-byte aligned,
+// when there is nothing to stage, or when fewer than two stages fit.
+inline bool plan_stages(VmProgram& P, uint32_t mask, StagePlan& SP) {
+  memset(&SP, 0, sizeof(SP));
+  uint32_t off = 0;
+  int n = 0;
+  for (int c = 0; c < P.ncols; ++c) {
+    if (!(mask >> c & 1u)) continue;
+    DevCol& d = P.cols[c];
+    if (reinterpret_cast<uintptr_t>(d.data) & 15u) return false;
+    d.soff = off;
+    SP.c[n++] = StageCopy{d.data, (uint32_t)d.width, off};
+    off += kStepRows * (uint32_t)d.width;
+    if (d.nulls) {
+      if (reinterpret_cast<uintptr_t>(d.nulls) & 15u) return false;
+      d.snoff = off;
+      SP.c[n++] = StageCopy{reinterpret_cast<const char*>(d.nulls), 1u, off};
+      off += kStepRows;
+    }
+  }
+  if (n == 0) return false;
+  const uint32_t stage = (uint32_t)align_up(off, 128);
+  int ns = (int)(kStageBudget / stage);
+  if (ns > kStageMax) ns = kStageMax;
+  if (ns < 2) return false;
+  SP.ncopy = n;
+  SP.nstages = ns;
+  SP.stage_bytes = stage;
+  SP.tx_bytes = off;
+  return true;
+}
+
+inline size_t stage_smem_bytes(const StagePlan& SP) {
+  return SP.nstages ? (size_t)SP.nstages * SP.stage_bytes + (size_t)SP.nstages * 8 : 0;
+}
+
+__device__ __forceinline__ uint64_t* stage_bar(const StagePlan& SP, int slot) {
+  return reinterpret_cast<uint64_t*>(yq_dyn_smem + (size_t)SP.nstages * SP.stage_bytes) + slot;
+}
+
+__device__ __forceinline__ void stage_init(const StagePlan& SP) {
+  if (threadIdx.x == 0)
+    for (int s = 0; s < SP.nstages; ++s) mbar_init(stage_bar(SP, s), 1);
+  __syncthreads();
+}
+
+// Thread 0: start the copies of the full step at row `row0` into `slot`.
+__device__ __forceinline__ void stage_issue(const StagePlan& SP, int slot, uint32_t row0) {
+  uint64_t* bar = stage_bar(SP, slot);
+  mbar_arrive_expect_tx(bar, SP.tx_bytes);
+  unsigned char* dst = yq_dyn_smem + (size_t)slot * SP.stage_bytes;
+  for (int i = 0; i < SP.ncopy; ++i) {
+    const StageCopy& c = SP.c[i];
+    tma_load_1d(dst + c.soff, c.src + (size_t)row0 * c.row_bytes, kStepRows * c.row_bytes, bar);
+  }
+}
+
+// All threads: copy a partial step of `rows` rows with plain loads, zero the rest.
+__device__ __forceinline__ void stage_fill(const StagePlan& SP, int slot, uint32_t row0, uint32_t rows) {
+  unsigned char* dst = yq_dyn_smem + (size_t)slot * SP.stage_bytes;
+  for (int i = 0; i < SP.ncopy; ++i) {
+    const StageCopy& c = SP.c[i];
+    const uint32_t valid = rows * c.row_bytes, total = kStepRows * c.row_bytes;
+    const unsigned char* src = reinterpret_cast<const unsigned char*>(c.src) + (size_t)row0 * c.row_bytes;
+    for (uint32_t b = threadIdx.x * 4; b < total; b += blockDim.x * 4) {
+      uint32_t w = 0;
+      if (b + 4 <= valid) {
+        w = *reinterpret_cast<const uint32_t*>(src + b);
+      } else {
+        for (uint32_t j = 0; j < 4; ++j)
+          if (b + j < valid) w |= (uint32_t)src[b + j] << (8 * j);
+      }
+      *reinterpret_cast<uint32_t*>(dst + c.soff + b) = w;
+    }
+  }
+}
+
+// Make the step of `tile` readable in `slot` (ring pass parity `parity`):
+// a partial last step is filled by every thread, a full one was started by
+// stage_issue and is waited for.
+__device__ __forceinline__ void stage_step(const StagePlan& SP, int slot, uint32_t parity, uint32_t tile, uint32_t n,
+                                           uint32_t* err) {
+  const uint32_t row0 = tile * kStepRows;
+  const uint32_t rows = min(kStepRows, n - row0);
+  if (rows < kStepRows) {
+    stage_fill(SP, slot, row0, rows);
+    __syncthreads();
+  } else {
+    mbar_wait_bounded(stage_bar(SP, slot), parity, err);
+  }
+}
+
+__device__ __forceinline__ bool full_step(uint32_t tile, uint32_t n) {
+  return (uint64_t)(tile + 1) * kStepRows <= n;
+}
+
+__device__ __forceinline__ uint32_t in_range_bits(uint32_t row0, uint32_t n) {
+  if (row0 >= n) return 0u;
+  const uint32_t left = n - row0;
+  return left >= (uint32_t)ITEMS ? kItemsMask : ((1u << left) - 1u);
+}
+
+// Columns an expression program reads (plus `extra`).
+inline uint32_t program_columns(const VmProgram& P, int end, uint32_t extra) {
+  uint32_t mask = extra;
+  for (int i = 0; i < end; ++i) {
+    const RInsn& I = P.code[i];
+    if (I.opc < R_CONST) {
+      mask |= 1u << I.a;
+    } else if ((I.opc >= R_ARITH_COL && I.opc < R_ARITH_CONST) || (I.opc >= R_CMP_CC && I.opc < R_AND)) {
+      mask |= 1u << I.b;
+      if (I.opc >= R_CMP_CCOL) mask |= 1u << I.c;
+    }
+  }
+  return mask;
+}
+
+// Bytes per row of the columns in `mask` (plus null bytes).
+inline double row_bytes_of(const VmProgram& P, uint32_t mask) {
+  double b = 0;
+  for (int c = 0; c < P.ncols; ++c)
+    if (mask >> c & 1u) b += P.cols[c].width + (P.cols[c].nulls ? 1 : 0);
+  return b;
+}
+
+}  // namespace yq
