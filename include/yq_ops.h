@@ -323,6 +323,25 @@ int yq_merge_pass(const yq_column* cols, int32_t ncols, int32_t key_col,
                   int32_t nruns, yq_column* out, void* workspace,
                   size_t workspace_bytes, void* stream);
 
+/* ---- Out-of-core ORDER BY of one key: the whole operator in one call.
+ * Replaces OrderOperator::firstPass + merge_all_sorted
+ * (include/engine/operators/order_operator.hpp:89-193,
+ *  src/engine/operators/order_operator.cpp:14-220): the rows of `in` arrive as
+ * nruns sorted-on-arrival batches (run r = rows [run_offsets[r],
+ * run_offsets[r+1]), host array). Every run is sorted by the segmented radix
+ * sort, whose last pass also leaves each row's order-preserving key words;
+ * the runs are then merged pairwise, level by level, as (key words, row id)
+ * pairs by a persistent merge-path kernel that stages both windows of the
+ * tiles ahead with 1-D bulk copies; finally every column is gathered once by
+ * the merged row ids into `out` (same schema, at least in->rows rows).
+ * Stable: equal keys keep their input order. The call waits for the device
+ * once, at the end, to report errors. */
+size_t yq_order_by_workspace_size(const yq_column* key, uint32_t rows, const uint32_t* run_offsets,
+                                  int32_t nruns);
+int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
+                const uint32_t* run_offsets, int32_t nruns, yq_batch* out, void* workspace,
+                size_t workspace_bytes, void* stream);
+
 /* ---- Inner join (nested loop semantics) and cross product.
  * Replaces ComparisonJoinExpression/ConjunctionJoinExpression +
  * outer_join_batches/and_join_batches + move_rows_join_kernel and

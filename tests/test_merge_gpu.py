@@ -89,3 +89,54 @@ def test_merge_pass_types(cuda, nruns, kind):
         out = run_outofcore(b, 0, desc, offs)
         perm = oracle.sort_perm(k, desc=desc, nulls=nulls)
         np.testing.assert_array_equal(out.columns[1].data.cpu().numpy(), payload[perm])
+
+
+@pytest.mark.parametrize("nruns", [1, 2, 5, 16])
+@pytest.mark.parametrize("kind", ["f32", "i32", "i64", "date", "f64", "text16", "text32", "f32_nulls", "bool",
+                                  "equal"])
+@pytest.mark.parametrize("desc,nulls_first", [(False, False), (True, False), (True, True)])
+def test_order_by_entry_matches_stable_sort(cuda, nruns, kind, desc, nulls_first):
+    """yq_order_by over runs of random sizes (empty runs included): every column
+    equals the rows of one stable sort of the whole table."""
+    rng = np.random.default_rng(nruns * 31 + len(kind) + 7 * desc + nulls_first)
+    sizes = rng.integers(0, 6000, nruns)
+    if nruns > 2:
+        sizes[1] = 0
+    n = int(sizes.sum())
+    offs = [0] + list(np.cumsum(sizes).astype(int))
+    nulls = None
+    ty = None
+    if kind == "f32":
+        k, t = rng.uniform(-1e6, 1e6, n).astype(np.float32), A.FLOAT32
+    elif kind == "i32":
+        k, t = rng.integers(-50, 50, n).astype(np.int32), A.INT32
+    elif kind == "i64":
+        k, t = rng.integers(-(1 << 40), 1 << 40, n).astype(np.int64), A.INT64
+    elif kind == "date":
+        k, t, ty = rng.integers(1420070400, 1640995199, n).astype(np.int64), A.DATETIME, oracle.DATETIME
+    elif kind == "f64":
+        k, t = rng.normal(0, 1e3, n).astype(np.float64), A.FLOAT64
+    elif kind == "text16":
+        k, t = datagen.text_slots([["", "a", "ab", "b", "zz", "hello", "category_007"][j]
+                                   for j in rng.integers(0, 7, n)]), A.TEXT
+    elif kind == "text32":
+        k = np.zeros((n, 32), np.uint8)
+        k[:, :20] = rng.integers(97, 100, (n, 20))
+        t = A.TEXT
+    elif kind == "f32_nulls":
+        k, t = rng.normal(0, 10, n).astype(np.float32), A.FLOAT32
+        nulls = rng.random(n) < 0.2
+    elif kind == "bool":
+        k, t = (rng.random(n) < 0.5).astype(np.uint8), A.BOOL
+    else:
+        k, t = np.full(n, 3.5, np.float32), A.FLOAT32
+    payload = np.arange(n, dtype=np.int64)
+    txt = datagen.text_slots([f"r{i % 97}" for i in range(n)])
+    b = ops.DeviceBatch([dev_col(k, t, nulls), dev_col(payload), dev_col(txt, A.TEXT)])
+    out = ops.order_by(b, 0, desc, offs, nulls_first=nulls_first)
+    perm = oracle.sort_perm(k, desc=desc, nulls=nulls, nulls_first=nulls_first, type_=ty)
+    np.testing.assert_array_equal(out.columns[1].data.cpu().numpy(), payload[perm])
+    np.testing.assert_array_equal(out.columns[0].data.cpu().numpy(), k[perm])
+    np.testing.assert_array_equal(out.columns[2].data.cpu().numpy(), txt[perm])
+    if nulls is not None:
+        np.testing.assert_array_equal(out.columns[0].nulls.cpu().numpy().astype(bool), nulls[perm])

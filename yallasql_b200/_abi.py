@@ -115,6 +115,8 @@ PROTOTYPES = {
     "yq_gather": (C.c_int, [P(Column), i32, vp, u32, P(Column), vp]),
     "yq_merge_workspace_size": (sz, [u32, i32]),
     "yq_merge_pass": (C.c_int, [P(Column), i32, i32, i32, i32, P(u32), i32, P(Column), vp, sz, vp]),
+    "yq_order_by_workspace_size": (sz, [P(Column), u32, P(u32), i32]),
+    "yq_order_by": (C.c_int, [P(Batch), i32, i32, i32, P(u32), i32, P(Batch), vp, sz, vp]),
     "yq_join_workspace_size": (sz, [u32, u32]),
     "yq_join_pairs": (C.c_int, [P(Batch), P(Batch), P(JoinCond), i32, vp, vp, u64, P(u64), vp, sz, vp]),
     "yq_join_project": (C.c_int, [P(Batch), P(Batch), P(JoinCond), i32, P(JoinOutput), i32, P(Column), u64,

@@ -14,7 +14,7 @@
 //      and moves every payload column with coalesced writes.
 #include <string.h>
 #include <vector>
-#include "yq_keys.cuh"
+#include "yq_sort.cuh"
 
 namespace yq {
 
@@ -328,6 +328,471 @@ static int launch_merge(const MergeParams& M, cudaStream_t s, double bytes) {
   return YQ_OK;
 }
 
+
+// ===================================================== merges of key words
+// ORDER BY over sorted runs as the radix sort leaves them: each row is its
+// order-preserving key words (yq_keys.cuh) plus its row id, so the merge
+// compares unsigned words only. A level is two launches: the partition kernel
+// gives every output tile its A and B windows (merge-path co-ranks at both
+// ends of the tile); the tile kernel is persistent, and thread 0 of a block
+// starts the bulk copies of the key and id windows of the tiles kRawStages - 1
+// ahead of the one the block merges, so the copies overlap the merging.
+// Windows are copied from their 16-byte aligned hull (buffers are padded).
+constexpr int kRawStages = 3;
+
+struct RawPair {
+  uint32_t a0, m, b0, n, tile0;
+};
+
+struct RawTile {
+  uint32_t a_row, na, b_row, nb, out0, cnt, pad0, pad1;
+};
+
+struct RawLevel {
+  const uint32_t* keys_in;  // [rows][KW] words
+  const uint32_t* ids_in;   // [rows]
+  uint32_t* keys_out;       // null: the level writes row ids only
+  uint32_t* ids_out;
+  const RawPair* pairs;
+  int32_t npairs;
+  uint32_t ntiles;
+  RawTile* tiles;  // [ntiles], written by the partition kernel
+  uint32_t* err;
+};
+
+__device__ __forceinline__ int raw_pair_of_tile(const RawPair* pairs, int npairs, uint32_t tile) {
+  int lo = 0, hi = npairs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&pairs[mid].tile0) <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int KW>
+__device__ __forceinline__ void raw_key_g(const uint32_t* keys, uint32_t row, uint32_t (&k)[KW]) {
+#pragma unroll
+  for (int j = 0; j < KW; ++j) k[j] = __ldg(keys + (size_t)row * KW + j);
+}
+
+// Number of A rows among the first k outputs of pair p (ties from A).
+template <int KW>
+__device__ __forceinline__ uint32_t raw_corank(const uint32_t* keys, const RawPair& p, uint32_t k) {
+  uint32_t lo = k > p.n ? k - p.n : 0u, hi = k < p.m ? k : p.m;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    uint32_t ka[KW], kb[KW];
+    raw_key_g<KW>(keys, p.a0 + mid, ka);
+    raw_key_g<KW>(keys, p.b0 + (k - mid - 1), kb);
+    if (key_le<KW>(ka, kb)) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <int KW>
+__global__ void k_merge_raw_partition(const __grid_constant__ RawLevel L) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= L.ntiles) return;
+  const RawPair p = L.pairs[raw_pair_of_tile(L.pairs, L.npairs, t)];
+  const uint32_t total = p.m + p.n;
+  const uint32_t k0 = (t - p.tile0) * kMergeTile;
+  const uint32_t k1 = min(k0 + kMergeTile, total);
+  if (k0 >= total) {  // a descriptor with no work (never produced by the host plan)
+    L.tiles[t] = RawTile{0, 0, 0, 0, 0, 0, 0, 0};
+    atomicOr(L.err, kErrBounds);
+    return;
+  }
+  const uint32_t i0 = raw_corank<KW>(L.keys_in, p, k0);
+  const uint32_t i1 = (k1 == total) ? p.m : raw_corank<KW>(L.keys_in, p, k1);
+  RawTile d;
+  d.a_row = p.a0 + i0;
+  d.na = i1 - i0;
+  d.b_row = p.b0 + (k0 - i0);
+  d.nb = (k1 - i1) - (k0 - i0);
+  d.out0 = p.a0 + k0;
+  d.cnt = k1 - k0;
+  d.pad0 = d.pad1 = 0;
+  L.tiles[t] = d;
+}
+
+// Where a tile's windows sit inside its stage slot.
+struct RawSlot {
+  uint32_t na, nb, cnt, out0;
+  uint32_t ka, kb, ia, ib;  // byte offsets of the first A / B key and id in the slot
+};
+
+template <int KW>
+struct RawGeom {
+  static constexpr uint32_t W = 4u * KW;
+  static constexpr uint32_t kreg = kMergeTile * W + 64;  // keys of both windows + alignment slack
+  static constexpr uint32_t ireg = kMergeTile * 4 + 64;  // ids of both windows + alignment slack
+  static constexpr uint32_t slot = kreg + ireg;
+  static constexpr size_t smem = (size_t)kRawStages * slot + (size_t)kMergeTile * 4 + kRawStages * 8;
+};
+
+// Copy rows [r0, r0 + n) (w bytes each) from their 16-byte hull; returns the
+// byte offset of row r0 inside the copy and advances `off` / `bytes`.
+__device__ __forceinline__ uint32_t raw_window(unsigned char* region, uint32_t& off, const void* base, uint32_t r0,
+                                               uint32_t n, uint32_t w, uint64_t* bar, uint32_t& bytes, bool issue) {
+  if (n == 0) return off;
+  const uintptr_t g0 = reinterpret_cast<uintptr_t>(base) + (uintptr_t)r0 * w;
+  const uintptr_t g1 = g0 + (uintptr_t)n * w;
+  const uintptr_t h0 = g0 & ~(uintptr_t)15, h1 = (g1 + 15) & ~(uintptr_t)15;
+  const uint32_t at = off + (uint32_t)(g0 - h0);
+  if (issue) tma_load_1d(region + off, reinterpret_cast<const void*>(h0), (uint32_t)(h1 - h0), bar);
+  bytes += (uint32_t)(h1 - h0);
+  off += (uint32_t)(h1 - h0);
+  return at;
+}
+
+// Thread 0: start the copies of tile descriptor d into `slot`.
+template <int KW>
+__device__ __forceinline__ void raw_issue(const RawLevel& L, const RawTile& d, int slot, unsigned char* smem,
+                                          RawSlot* s_slot) {
+  using G = RawGeom<KW>;
+  unsigned char* kreg = smem + (size_t)slot * G::slot;
+  unsigned char* ireg = kreg + G::kreg;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + (size_t)kRawStages * G::slot + (size_t)kMergeTile * 4) + slot;
+  uint32_t bytes = 0, ko = 0, io = 0;
+  // sizes first (expect_tx before the copies)
+  RawSlot r;
+  r.na = d.na;
+  r.nb = d.nb;
+  r.cnt = d.cnt;
+  r.out0 = d.out0;
+  {
+    uint32_t k2 = 0, i2 = 0, b2 = 0;
+    r.ka = raw_window(kreg, k2, L.keys_in, d.a_row, d.na, G::W, bar, b2, false);
+    r.kb = raw_window(kreg, k2, L.keys_in, d.b_row, d.nb, G::W, bar, b2, false);
+    r.ia = raw_window(ireg, i2, L.ids_in, d.a_row, d.na, 4u, bar, b2, false);
+    r.ib = raw_window(ireg, i2, L.ids_in, d.b_row, d.nb, 4u, bar, b2, false);
+    mbar_arrive_expect_tx(bar, b2);
+  }
+  s_slot[slot] = r;
+  raw_window(kreg, ko, L.keys_in, d.a_row, d.na, G::W, bar, bytes, true);
+  raw_window(kreg, ko, L.keys_in, d.b_row, d.nb, G::W, bar, bytes, true);
+  raw_window(ireg, io, L.ids_in, d.a_row, d.na, 4u, bar, bytes, true);
+  raw_window(ireg, io, L.ids_in, d.b_row, d.nb, 4u, bar, bytes, true);
+}
+
+template <int KW>
+__device__ __forceinline__ void raw_key_s(const unsigned char* p, uint32_t (&k)[KW]) {
+  if constexpr (KW == 1) {
+    k[0] = *reinterpret_cast<const uint32_t*>(p);
+  } else if constexpr (KW == 2) {
+    const uint2 v = *reinterpret_cast<const uint2*>(p);
+    k[0] = v.x;
+    k[1] = v.y;
+  } else {
+#pragma unroll
+    for (int j = 0; j < KW; j += 4) {
+      const uint4 v = *reinterpret_cast<const uint4*>(p + 4 * j);
+      k[j] = v.x;
+      k[j + 1] = v.y;
+      k[j + 2] = v.z;
+      k[j + 3] = v.w;
+    }
+  }
+}
+
+template <int KW>
+__device__ __forceinline__ void raw_key_store(uint32_t* out, size_t row, const uint32_t (&k)[KW]) {
+  if constexpr (KW == 1) {
+    out[row] = k[0];
+  } else if constexpr (KW == 2) {
+    reinterpret_cast<uint2*>(out)[row] = make_uint2(k[0], k[1]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < KW; j += 4)
+      *reinterpret_cast<uint4*>(out + row * KW + j) = make_uint4(k[j], k[j + 1], k[j + 2], k[j + 3]);
+  }
+}
+
+template <int KW>
+__global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_constant__ RawLevel L) {
+  using G = RawGeom<KW>;
+  extern __shared__ __align__(128) unsigned char raw_smem[];
+  __shared__ RawSlot s_slot[kRawStages];
+  uint32_t* s_src = reinterpret_cast<uint32_t*>(raw_smem + (size_t)kRawStages * G::slot);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(raw_smem + (size_t)kRawStages * G::slot + (size_t)kMergeTile * 4);
+  const uint32_t NT = L.ntiles, GR = gridDim.x;
+  if (threadIdx.x == 0)
+    for (int s = 0; s < kRawStages; ++s) mbar_init(bars + s, 1);
+  __syncthreads();
+  RawTile next{};
+  if (threadIdx.x == 0) {
+    for (int j = 0; j < kRawStages - 1; ++j) {
+      const uint32_t t = blockIdx.x + (uint32_t)j * GR;
+      if (t < NT) raw_issue<KW>(L, L.tiles[t], j, raw_smem, s_slot);
+    }
+    const uint32_t t = blockIdx.x + (uint32_t)(kRawStages - 1) * GR;
+    if (t < NT) next = L.tiles[t];
+  }
+  int slot = 0;
+  uint32_t parity = 0;
+  for (uint32_t t = blockIdx.x; t < NT; t += GR) {
+    __syncthreads();  // every thread is done with the previous tile: its slot and s_src are free
+    if (threadIdx.x == 0) {
+      const uint32_t tn = t + (uint32_t)(kRawStages - 1) * GR;
+      const int ns = slot == 0 ? kRawStages - 1 : slot - 1;
+      if (tn < NT) {
+        raw_issue<KW>(L, next, ns, raw_smem, s_slot);
+        const uint32_t tf = tn + GR;  // descriptor for the next issue, loaded a tile ahead
+        if (tf < NT) next = L.tiles[tf];
+      }
+    }
+    mbar_wait_bounded(bars + slot, parity, L.err);
+    const RawSlot r = s_slot[slot];
+    const unsigned char* kreg = raw_smem + (size_t)slot * G::slot;
+    const unsigned char* ireg = kreg + G::kreg;
+    const unsigned char* kA = kreg + r.ka;
+    const unsigned char* kB = kreg + r.kb;
+
+    // Each thread merges kMergeItems consecutive outputs of the tile.
+    const uint32_t kk = threadIdx.x * kMergeItems;
+    if (kk < r.cnt) {
+      uint32_t lo = kk > r.nb ? kk - r.nb : 0u, hi = kk < r.na ? kk : r.na;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        uint32_t ka[KW], kb[KW];
+        raw_key_s<KW>(kA + (size_t)mid * G::W, ka);
+        raw_key_s<KW>(kB + (size_t)(kk - mid - 1) * G::W, kb);
+        if (key_le<KW>(ka, kb)) lo = mid + 1;
+        else hi = mid;
+      }
+      uint32_t ia = lo, jb = kk - lo;
+      uint32_t ka[KW], kb[KW];
+#pragma unroll
+      for (int j = 0; j < KW; ++j) ka[j] = kb[j] = 0u;
+      if (ia < r.na) raw_key_s<KW>(kA + (size_t)ia * G::W, ka);
+      if (jb < r.nb) raw_key_s<KW>(kB + (size_t)jb * G::W, kb);
+#pragma unroll
+      for (int x = 0; x < kMergeItems; ++x) {
+        if (kk + x >= r.cnt) break;
+        const bool takeA = ia < r.na && (jb >= r.nb || key_le<KW>(ka, kb));
+        if (takeA) {
+          s_src[kk + x] = ia++;
+          if (ia < r.na) raw_key_s<KW>(kA + (size_t)ia * G::W, ka);
+        } else {
+          s_src[kk + x] = kFromB | jb++;
+          if (jb < r.nb) raw_key_s<KW>(kB + (size_t)jb * G::W, kb);
+        }
+      }
+    }
+    __syncthreads();
+    // Coalesced writes of the merged keys and ids.
+    for (uint32_t x = threadIdx.x; x < r.cnt; x += kMergeBlock) {
+      const uint32_t v = s_src[x];
+      const bool fromB = (v & kFromB) != 0u;
+      const uint32_t j = v & ~kFromB;
+      const uint32_t id = *reinterpret_cast<const uint32_t*>(ireg + (fromB ? r.ib : r.ia) + 4u * j);
+      L.ids_out[r.out0 + x] = id;
+      if (L.keys_out) {
+        uint32_t k[KW];
+        raw_key_s<KW>((fromB ? kB : kA) + (size_t)j * G::W, k);
+        raw_key_store<KW>(L.keys_out, (size_t)r.out0 + x, k);
+      }
+    }
+    if (++slot == kRawStages) {
+      slot = 0;
+      parity ^= 1u;
+    }
+  }
+}
+
+template <int KW>
+static int launch_raw_level(const RawLevel& L, cudaStream_t s, double bytes) {
+  using G = RawGeom<KW>;
+  static bool attr = false;
+  if (!attr) {
+    YQ_TRY_CUDA(cudaFuncSetAttribute(k_merge_raw_tiles<KW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem));
+    attr = true;
+  }
+  static int cap = 0;
+  if (!cap) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_merge_raw_tiles<KW>, kMergeBlock, G::smem) !=
+            cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    cap = per_sm * sm_count();
+  }
+  {
+    ProfScope ps("merge_partition", s, 0.0);
+    k_merge_raw_partition<KW><<<ceil_div<uint32_t>(L.ntiles, 128), 128, 0, s>>>(L);
+    YQ_CHECK_LAUNCH();
+  }
+  const int grid = (int)(L.ntiles < (uint32_t)cap ? L.ntiles : (uint32_t)cap);
+  ProfScope ps("merge_tiles", s, bytes);
+  k_merge_raw_tiles<KW><<<grid, kMergeBlock, G::smem, s>>>(L);
+  YQ_CHECK_LAUNCH();
+  return YQ_OK;
+}
+
+// Merge levels of one ORDER BY: host plan of every level's pairs.
+struct OrderPlan {
+  std::vector<RawPair> pairs;         // all levels, back to back
+  std::vector<int> level_first;       // first pair of each level (+ end)
+  std::vector<uint32_t> level_tiles;  // tiles per level
+};
+
+static void plan_order_levels(const uint32_t* offsets, int nruns, OrderPlan& P) {
+  std::vector<uint32_t> offs(offsets, offsets + nruns + 1);
+  P.pairs.clear();
+  P.level_first.clear();
+  P.level_tiles.clear();
+  while (offs.size() > 2) {
+    P.level_first.push_back((int)P.pairs.size());
+    uint32_t tiles = 0;
+    std::vector<uint32_t> next;
+    const int runs = (int)offs.size() - 1;
+    for (int r = 0; r < runs; r += 2) {
+      RawPair p;
+      p.a0 = offs[r];
+      p.m = offs[r + 1] - offs[r];
+      p.b0 = offs[r + 1];
+      p.n = (r + 1 < runs) ? offs[r + 2] - offs[r + 1] : 0u;
+      p.tile0 = tiles;
+      next.push_back(offs[r]);
+      const uint32_t t = ceil_div<uint32_t>(p.m + p.n, kMergeTile);
+      if (t == 0) continue;  // empty pair
+      tiles += t;
+      P.pairs.push_back(p);
+    }
+    next.push_back(offs.back());
+    offs.swap(next);
+    P.level_tiles.push_back(tiles);
+  }
+  P.level_first.push_back((int)P.pairs.size());
+}
+
+struct OrderWs {
+  size_t sort_bytes = 0;
+  int kw_max = 0;
+  uint32_t max_tiles = 0;
+  size_t npairs = 0;
+};
+
+static int order_ws_layout(const yq_column& key, uint32_t rows, const uint32_t* offsets, int nruns, OrderWs& o,
+                           WsSize& w) {
+  o.kw_max = sort_key_words_max(key);
+  if (o.kw_max < 0) return YQ_ERR_INVALID_ARG;
+  KeyJob j{key, 0, 0};
+  YQ_TRY(sort_segments_impl(&j, 1, rows, offsets, nruns, nullptr, nullptr, nullptr, 0, nullptr, &o.sort_bytes));
+  o.max_tiles = ceil_div<uint32_t>(rows, kMergeTile) + (uint32_t)nruns + 1;
+  o.npairs = (size_t)nruns + 64;
+  w.add<char>(o.sort_bytes);
+  w.add<uint32_t>((size_t)rows * o.kw_max + 16);  // keys, two buffers
+  w.add<uint32_t>((size_t)rows * o.kw_max + 16);
+  w.add<uint32_t>((size_t)rows + 16);  // row ids, two buffers
+  w.add<uint32_t>((size_t)rows + 16);
+  w.add<RawPair>(o.npairs);
+  w.add<RawTile>(o.max_tiles);
+  w.add<uint32_t>(4);
+  return YQ_OK;
+}
+
+}  // namespace yq
+
+using namespace yq;
+
+extern "C" size_t yq_order_by_workspace_size(const yq_column* key, uint32_t rows, const uint32_t* run_offsets,
+                                             int32_t nruns) {
+  if (!key || !run_offsets || nruns <= 0) return 0;
+  OrderWs o;
+  WsSize w;
+  if (order_ws_layout(*key, rows, run_offsets, nruns, o, w) != YQ_OK) return 0;
+  return w.total();
+}
+
+extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
+                           const uint32_t* run_offsets, int32_t nruns, yq_batch* out, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+  if (!in || !out || !run_offsets || nruns <= 0 || key_col < 0 || key_col >= in->ncols || out->ncols != in->ncols ||
+      in->ncols > YQ_MAX_BATCH_COLUMNS)
+    return YQ_ERR_INVALID_ARG;
+  const uint32_t rows = in->rows;
+  if (run_offsets[0] != 0 || run_offsets[nruns] != rows) return YQ_ERR_INVALID_ARG;
+  for (int r = 0; r < nruns; ++r)
+    if (run_offsets[r + 1] < run_offsets[r]) return YQ_ERR_INVALID_ARG;
+  for (int c = 0; c < in->ncols; ++c) {
+    const yq_column& a = in->columns[c];
+    const yq_column& b = out->columns[c];
+    if (a.type != b.type || a.width != b.width || (rows > 0 && (!a.data || !b.data))) return YQ_ERR_INVALID_ARG;
+  }
+  if (rows == 0) return YQ_OK;
+  cudaStream_t s = as_stream(stream);
+  const yq_column& key = in->columns[key_col];
+  OrderWs o;
+  WsSize wsz;
+  YQ_TRY(order_ws_layout(key, rows, run_offsets, nruns, o, wsz));
+  Workspace ws;
+  YQ_TRY(ws.acquire(workspace, workspace_bytes, wsz.total(), s));
+  char* sort_ws = ws.take<char>(o.sort_bytes);
+  uint32_t* keys[2] = {ws.take<uint32_t>((size_t)rows * o.kw_max + 16), ws.take<uint32_t>((size_t)rows * o.kw_max + 16)};
+  uint32_t* ids[2] = {ws.take<uint32_t>((size_t)rows + 16), ws.take<uint32_t>((size_t)rows + 16)};
+  RawPair* d_pairs = ws.take<RawPair>(o.npairs);
+  RawTile* d_tiles = ws.take<RawTile>(o.max_tiles);
+  uint32_t* d_err = ws.take<uint32_t>(4);
+  YQ_TRY_CUDA(cudaMemsetAsync(d_err, 0, 4 * sizeof(uint32_t), s));
+
+  // 1. every run sorted; the sort hands over its key words and row ids
+  KeyJob job{key, descending != 0, nulls_first != 0};
+  int kw = 0;
+  uint32_t* sort_err = nullptr;
+  YQ_TRY(sort_segments_impl(&job, 1, rows, run_offsets, nruns, ids[0], nullptr, sort_ws, o.sort_bytes, s, nullptr,
+                            keys[0], &kw, true, &sort_err));
+  // 2. merge levels over (key words, row id)
+  int cur = 0;
+  if (kw > 0 && nruns > 1) {
+    OrderPlan P;
+    plan_order_levels(run_offsets, nruns, P);
+    if (P.pairs.size() > o.npairs) return YQ_ERR_UNSUPPORTED;
+    YQ_TRY(h2d_async(d_pairs, P.pairs.data(), P.pairs.size() * sizeof(RawPair), s));
+    const int levels = (int)P.level_tiles.size();
+    for (int l = 0; l < levels; ++l) {
+      const bool last = l + 1 == levels;
+      RawLevel L;
+      L.keys_in = keys[cur];
+      L.ids_in = ids[cur];
+      L.keys_out = last ? nullptr : keys[cur ^ 1];
+      L.ids_out = ids[cur ^ 1];
+      L.pairs = d_pairs + P.level_first[l];
+      L.npairs = P.level_first[l + 1] - P.level_first[l];
+      L.ntiles = P.level_tiles[l];
+      L.tiles = d_tiles;
+      L.err = d_err;
+      if (L.ntiles > o.max_tiles) return YQ_ERR_UNSUPPORTED;
+      if (L.ntiles == 0) continue;
+      // algorithmic bytes: key words + id in and out (ids only out on the last level)
+      const double bytes = (double)rows * (4.0 * kw + 4.0 + (last ? 4.0 : 4.0 * kw + 4.0));
+      switch (kw) {
+        case 1: YQ_TRY(launch_raw_level<1>(L, s, bytes)); break;
+        case 2: YQ_TRY(launch_raw_level<2>(L, s, bytes)); break;
+        case 4: YQ_TRY(launch_raw_level<4>(L, s, bytes)); break;
+        case 8: YQ_TRY(launch_raw_level<8>(L, s, bytes)); break;
+        default: return YQ_ERR_UNSUPPORTED;
+      }
+      cur ^= 1;
+    }
+  }
+  // 3. every column (the key included) gathered once by the final row ids
+  yq_column outs[YQ_MAX_BATCH_COLUMNS];
+  for (int c = 0; c < in->ncols; ++c) outs[c] = out->columns[c];
+  YQ_TRY(yq_gather(in->columns, in->ncols, ids[cur], rows, outs, s));
+  uint32_t err[2] = {0, 0};
+  YQ_TRY_CUDA(cudaMemcpyAsync(&err[0], sort_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  YQ_TRY_CUDA(cudaMemcpyAsync(&err[1], d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  const uint32_t e = err[0] | err[1];
+  if (e & kErrTimeout) return YQ_ERR_TIMEOUT;
+  if (e & kErrBounds) return YQ_ERR_INVALID_ARG;
+  return YQ_OK;
+}
+
+namespace yq {
 }  // namespace yq
 
 using namespace yq;

@@ -19,7 +19,7 @@
 // launches. A single global sort is the one-segment case.
 #include <string.h>
 #include <vector>
-#include "yq_keys.cuh"
+#include "yq_sort.cuh"
 
 namespace yq {
 
@@ -588,10 +588,6 @@ static void plan_segments(const uint32_t* offsets, int nseg, uint32_t tile_rows,
 }
 
 // One key of a (possibly multi-key) segmented sort: perm_in (null = identity) -> perm_out.
-struct KeyJob {
-  yq_column key;
-  int desc, nulls_first;
-};
 
 // Resolved plan for one key: words, digit width, tiling.
 struct KeyPlan {
@@ -622,9 +618,44 @@ static int plan_key(const yq_column& c, int vwords_override, int want_d, const u
 
 // Workspace: [seg offsets][tile offsets][histograms][look-back status per pass]
 //            [counters][keys A/B][vals A/B][perm between keys]
+int sort_key_words_max(const yq_column& c) {
+  int vw = key_value_words(c);
+  if (vw < 0) return -1;
+  if (c.type == YQ_TEXT && vw > 8 - (c.nulls ? 1 : 0)) vw = 8 - (c.nulls ? 1 : 0);
+  return round_kw(vw + (c.nulls ? 1 : 0));
+}
+
+// Key words of every row in row order (a key whose passes all fall out: its
+// sorted order is the row order).
+template <int KW>
+__global__ void k_make_keys(const KeySrc src, uint32_t* __restrict__ out, uint32_t rows) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    uint32_t k[KW];
+    make_key<KW>(src, src.in_perm ? __ldg(src.in_perm + r) : r, k);
+#pragma unroll
+    for (int j = 0; j < KW; ++j) out[(size_t)r * KW + j] = k[j];
+  }
+}
+
+static int launch_make_keys(int kw, const KeySrc& src, uint32_t* out, uint32_t rows, cudaStream_t s) {
+  const int grid = sm_count() * 8;
+  switch (kw) {
+    case 1: k_make_keys<1><<<grid, 256, 0, s>>>(src, out, rows); break;
+    case 2: k_make_keys<2><<<grid, 256, 0, s>>>(src, out, rows); break;
+    case 4: k_make_keys<4><<<grid, 256, 0, s>>>(src, out, rows); break;
+    case 8: k_make_keys<8><<<grid, 256, 0, s>>>(src, out, rows); break;
+    default: return YQ_ERR_UNSUPPORTED;
+  }
+  YQ_CHECK_LAUNCH();
+  return YQ_OK;
+}
+
 int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint32_t* seg_offsets_host, int nseg,
                        uint32_t* out_perm, const yq_sort_config* cfg, void* workspace, size_t workspace_bytes,
-                       cudaStream_t s, size_t* size_only) {
+                       cudaStream_t s, size_t* size_only, uint32_t* keys_out, int* kw_out, bool defer_err,
+                       uint32_t** err_out) {
+  if (keys_out && (njobs != 1 || !kw_out)) return YQ_ERR_INVALID_ARG;
+  if (kw_out) *kw_out = 0;
   if (njobs <= 0 || nseg <= 0 || !seg_offsets_host) return YQ_ERR_INVALID_ARG;
   if (rows > kMaxSortRows) return YQ_ERR_UNSUPPORTED;
   if (seg_offsets_host[0] != 0 || seg_offsets_host[nseg] != rows) return YQ_ERR_INVALID_ARG;
@@ -707,8 +738,8 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
     YQ_TRY(plan_key(c, vw, want_d, seg_offsets_host, nseg, kp));
     SegPlan sp;
     plan_segments(seg_offsets_host, nseg, kp.tile_rows, sp);
-    YQ_TRY_CUDA(cudaMemcpyAsync(d_seg, sp.seg.data(), (nseg + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-    YQ_TRY_CUDA(cudaMemcpyAsync(d_tiles, sp.tiles.data(), (nseg + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    YQ_TRY(h2d_async(d_seg, sp.seg.data(), (nseg + 1) * sizeof(uint32_t), s));
+    YQ_TRY(h2d_async(d_tiles, sp.tiles.data(), (nseg + 1) * sizeof(uint32_t), s));
     YQ_TRY_CUDA(cudaMemsetAsync(d_hist, 0, (size_t)nseg * kp.P * kp.R * sizeof(uint32_t), s));
     YQ_TRY_CUDA(cudaMemsetAsync(d_status, 0, (size_t)kp.P * sp.ntiles * kp.R * sizeof(uint32_t), s));
     YQ_TRY_CUDA(cudaMemsetAsync(d_misc, 0, 64 * sizeof(uint32_t), s));
@@ -755,7 +786,11 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
         if (!trivial) passes.push_back(p);
       }
     }
-    if (passes.empty()) continue;  // order unchanged by this key
+    if (keys_out) *kw_out = kp.sh.kw;
+    if (passes.empty()) {  // order unchanged by this key
+      if (keys_out) YQ_TRY(launch_make_keys(kp.sh.kw, src, keys_out, rows, s));
+      continue;
+    }
     if (passes.size() > 64) return YQ_ERR_UNSUPPORTED;
     uint32_t* dst_perm = (perm_in == out_perm) ? d_perm_tmp : out_perm;
     for (size_t i = 0; i < passes.size(); ++i) {
@@ -763,7 +798,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
       SweepParams Sp;
       Sp.keys_in = first ? nullptr : d_keys[(i - 1) & 1];
       Sp.vals_in = first ? nullptr : d_vals[(i - 1) & 1];
-      Sp.keys_out = last ? nullptr : d_keys[i & 1];
+      Sp.keys_out = last ? keys_out : d_keys[i & 1];
       Sp.vals_out = last ? dst_perm : d_vals[i & 1];
       Sp.src = src;
       Sp.seg = seg;
@@ -777,7 +812,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
       // pass reads the raw key (+ incoming permutation), the last writes ids only)
       const double kb = 4.0 * kp.sh.kw;
       const double in_b = first ? (double)c.width + (perm_in ? 4.0 : 0.0) : kb + 4.0;
-      const double out_b = last ? 4.0 : kb + 4.0;
+      const double out_b = (last && !keys_out) ? 4.0 : kb + 4.0;
       ProfScope ps("sort_onesweep", s, (double)rows * (in_b + out_b));
       YQ_TRY(kp.K.sweep(Sp, sp.ntiles, s));
     }
@@ -791,7 +826,8 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
       YQ_CHECK_LAUNCH();
     }
   }
-  if (!keep_trivial) {
+  if (err_out) *err_out = d_err;
+  if (!keep_trivial && !defer_err) {
     uint32_t err = 0;
     YQ_TRY_CUDA(cudaMemcpyAsync(&err, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     YQ_TRY_CUDA(cudaStreamSynchronize(s));

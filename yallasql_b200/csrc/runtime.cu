@@ -16,6 +16,47 @@ static std::atomic<unsigned long long> g_launches{0};
 void set_cuda_error(cudaError_t e) { g_last_cuda_error = (int)e; }
 void count_launch(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 
+// ------------------------------------------------------ small host uploads
+// A copy from pageable host memory may make the host wait for the stream;
+// small descriptor arrays (segment offsets, merge pairs) go through a ring of
+// pinned slots instead, so the call that issues them does not block. A slot
+// is reused only after the event recorded behind its previous copy fired.
+namespace {
+constexpr int kStageSlots = 16;
+constexpr size_t kStageSlotBytes = 64 * 1024;
+std::mutex g_stage_mu;
+char* g_stage_host = nullptr;
+cudaEvent_t g_stage_ev[kStageSlots] = {};
+int g_stage_next = 0;
+int g_stage_dev = -1;
+}  // namespace
+
+int h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return YQ_OK;
+  int dev = 0;
+  YQ_TRY_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_stage_mu);
+  if (bytes > kStageSlotBytes || (g_stage_dev >= 0 && g_stage_dev != dev)) {
+    YQ_TRY_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    return YQ_OK;
+  }
+  if (!g_stage_host) {
+    void* h = nullptr;
+    YQ_TRY_CUDA(cudaMallocHost(&h, kStageSlots * kStageSlotBytes));
+    for (int i = 0; i < kStageSlots; ++i) YQ_TRY_CUDA(cudaEventCreateWithFlags(&g_stage_ev[i], cudaEventDisableTiming));
+    g_stage_host = static_cast<char*>(h);
+    g_stage_dev = dev;
+  }
+  const int slot = g_stage_next;
+  g_stage_next = (g_stage_next + 1) % kStageSlots;
+  YQ_TRY_CUDA(cudaEventSynchronize(g_stage_ev[slot]));  // the slot's previous copy has been read
+  char* h = g_stage_host + (size_t)slot * kStageSlotBytes;
+  memcpy(h, src, bytes);
+  YQ_TRY_CUDA(cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, s));
+  YQ_TRY_CUDA(cudaEventRecord(g_stage_ev[slot], s));
+  return YQ_OK;
+}
+
 // ---------------------------------------------------------------- profiler
 namespace {
 struct ProfRec {

@@ -51,6 +51,10 @@ struct ProfScope {
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Host -> device copy of a small host array that returns without waiting for
+// the stream (staged through pinned memory; runtime.cu).
+int h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
 int sm_count();
 
 template <typename T>

@@ -1,0 +1,29 @@
+// Internal interface of the segmented radix sort (k_sort.cu) for the other
+// operator files.
+#pragma once
+
+#include "yq_keys.cuh"
+
+namespace yq {
+
+// One key of a (possibly multi-key) sort.
+struct KeyJob {
+  yq_column key;
+  int desc, nulls_first;
+};
+
+// Words of the order-preserving key the sort builds for column `c` at most
+// (text keys use fewer when their slots end in zero words); -1 = unsupported.
+int sort_key_words_max(const yq_column& c);
+
+// Segmented stable sort of `rows` rows by `jobs` (most significant first) into
+// `out_perm`. With `keys_out` (single key only) the last pass also writes the
+// transformed key words of the sorted rows ([rows][*kw_out] words; *kw_out = 0
+// when every key is equal). With `defer_err` the call does not wait for the
+// device to report errors: *err_out points at the workspace's error word.
+int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint32_t* seg_offsets_host, int nseg,
+                       uint32_t* out_perm, const yq_sort_config* cfg, void* workspace, size_t workspace_bytes,
+                       cudaStream_t s, size_t* size_only, uint32_t* keys_out = nullptr, int* kw_out = nullptr,
+                       bool defer_err = false, uint32_t** err_out = nullptr);
+
+}  // namespace yq

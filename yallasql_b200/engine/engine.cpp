@@ -483,9 +483,9 @@ class AggregateOperator final : public Operator {
 };
 
 // ----------------------------------------------------------- OrderOperator
-// Every child batch becomes a run (sorted by the segmented radix sort in one
-// set of launches), then runs merge pairwise by merge path until one remains
-// (OrderOperator::firstPass / merge_all_sorted, order_operator.hpp:89-193).
+// Every child batch becomes a run; yq_order_by sorts the runs (segmented radix
+// sort), merges them pairwise by merge path until one remains and gathers the
+// rows (OrderOperator::firstPass / merge_all_sorted, order_operator.hpp:89-193).
 class OrderOperator final : public Operator {
  public:
   OrderOperator(std::unique_ptr<Operator> child, int key, int desc, int nulls_first)
@@ -536,60 +536,16 @@ class OrderOperator final : public Operator {
       offs.push_back((uint32_t)(o + r->rows));
     }
     runs.clear();
-    std::vector<yq_column> av;
+    // Sort every run, merge the runs level by level as (key words, row id)
+    // pairs and gather every column once (yq_order_by).
+    std::vector<yq_column> av, rv;
     all->view(av);
-    // 1. sort every run (segmented radix sort: one set of launches for all runs)
-    uint32_t* ids[2] = {nullptr, nullptr};
-    for (auto*& p : ids) check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&p), total * 4, s), "ids");
-    check(yq_sort_segments(&av[key_], (uint32_t)total, offs.data(), (int32_t)offs.size() - 1, desc_, nulls_first_,
-                           ids[0], nullptr, nullptr, 0, s),
-          "OrderOperator sort");
-    // 2. runs of (key, row id): only these 8 bytes per row go through the
-    //    merge levels; the payload is gathered once at the end
-    std::vector<ColumnPtr> kcols{columns[key_]};
-    const bool knull = all->nulls[key_] != nullptr;
     auto result = std::make_unique<Batch>(columns, total, s, nullable);
-    auto k0 = std::make_unique<Batch>(kcols, total, s, knull);
-    auto k1 = std::make_unique<Batch>(kcols, total, s, knull);
-    yq_column kc0 = k0->column(0);
-    check(yq_gather(&av[key_], 1, ids[0], (uint32_t)total, &kc0, s), "OrderOperator key runs");
-    int cur = 0;
-    bool merged = false;
-    Batch* kb[2] = {k0.get(), k1.get()};
-    while (offs.size() > 2) {
-      const bool last = offs.size() - 1 <= 2;  // two runs left: this level writes the result's key column
-      merged = true;
-      yq_column sv[2] = {kb[cur]->column(0), yq_column{ids[cur], nullptr, YQ_INT32, 4}};
-      yq_column dv[2] = {last ? result->column(key_) : kb[cur ^ 1]->column(0),
-                         yq_column{ids[cur ^ 1], nullptr, YQ_INT32, 4}};
-      check(yq_merge_pass(sv, 2, 0, desc_, nulls_first_, offs.data(), (int32_t)offs.size() - 1, dv, nullptr, 0, s),
-            "OrderOperator merge");
-      std::vector<uint32_t> next_offs;
-      for (size_t i = 0; i + 1 < offs.size(); i += 2) next_offs.push_back(offs[i]);
-      next_offs.push_back(offs.back());
-      offs.swap(next_offs);
-      cur ^= 1;
-      if (last) break;
-    }
-    if (!merged) {
-      // a single run: its sorted keys are the result's key column
-      yq_column kr = result->column(key_), ks = kb[0]->column(0);
-      check_cuda(cudaMemcpyAsync(kr.data, ks.data, total * kr.width, cudaMemcpyDeviceToDevice, s), "key copy");
-      if (kr.nulls && ks.nulls)
-        check_cuda(cudaMemcpyAsync(const_cast<uint8_t*>(kr.nulls), ks.nulls, total, cudaMemcpyDeviceToDevice, s),
-                   "key copy");
-    }
-    // 3. payload columns by the final row ids
-    std::vector<yq_column> src_rest, dst_rest;
-    for (size_t c = 0; c < columns.size(); ++c) {
-      if ((int)c == key_) continue;
-      src_rest.push_back(av[c]);
-      dst_rest.push_back(result->column(c));
-    }
-    if (!src_rest.empty())
-      check(yq_gather(src_rest.data(), (int32_t)src_rest.size(), ids[cur], (uint32_t)total, dst_rest.data(), s),
-            "OrderOperator gather");
-    for (auto* p : ids) cudaFreeAsync(p, s);
+    result->view(rv);
+    yq_batch ib{av.data(), (int32_t)av.size(), (uint32_t)total};
+    yq_batch ob{rv.data(), (int32_t)rv.size(), (uint32_t)total};
+    check(yq_order_by(&ib, key_, desc_, nulls_first_, offs.data(), (int32_t)offs.size() - 1, &ob, nullptr, 0, s),
+          "OrderOperator");
     return cache.putBatch(std::move(result));
   }
 

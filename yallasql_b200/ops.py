@@ -394,53 +394,43 @@ class JoinAggPlan:
                "yq_join_aggregate")
 
 
+def order_by_workspace_bytes(col: DeviceColumn, offsets: list[int]) -> int:
+    offs = (C.c_uint32 * len(offsets))(*offsets)
+    cc = col.c()
+    return int(lib().yq_order_by_workspace_size(C.byref(cc), col.rows, offs, len(offsets) - 1))
+
+
 class OrderByRuns:
-    """Out-of-core ORDER BY of one key over a batch made of runs (4 MB batches):
-    every run is sorted by the segmented radix sort, then only (key, row id)
-    pairs go through the merge-path levels, and the payload columns are
-    gathered once by the final row ids. The reference moves whole rows through
-    every merge window (OrderOperator::merge_two_runs, order_operator.cpp:117-220);
-    carrying 8 bytes per row instead of the full row cuts each level's traffic
-    to 16 bytes per row. Buffers are allocated once and reused across calls."""
+    """Out-of-core ORDER BY of one key over a batch made of runs (4 MB
+    batches), through yq_order_by: the runs are sorted by the segmented radix
+    sort, merged level by level as (key words, row id) pairs, and every column
+    is gathered once by the merged row ids (OrderOperator::firstPass +
+    merge_all_sorted, order_operator.hpp:89-193 / order_operator.cpp:14-220).
+    The workspace is allocated once and reused across calls."""
 
     def __init__(self, batch: DeviceBatch, key: int, offsets: list[int]):
-        kc = batch.columns[key]
-        n = batch.rows
-        self.key, self.offsets, self.n = key, list(offsets), n
-        w = kc.width if kc.type == A.TEXT else None
-        nl = kc.nulls is not None
-        self.k = [DeviceColumn.empty(kc.type, n, w, nulls=nl) for _ in range(2)]
-        self.ids = [torch.empty(n, dtype=torch.int32, device="cuda") for _ in range(3)]
-        self.ws = torch.empty(max(sort_workspace_bytes(kc, self.offsets), 256), dtype=torch.uint8, device="cuda")
+        self.key, self.offsets, self.n = key, list(offsets), batch.rows
+        self._offs = (C.c_uint32 * len(self.offsets))(*self.offsets)
+        self.ws = torch.empty(max(order_by_workspace_bytes(batch.columns[key], self.offsets), 256),
+                              dtype=torch.uint8, device="cuda")
 
     def run(self, batch: DeviceBatch, descending: bool, out: DeviceBatch, nulls_first=False, stream=None):
-        kc = batch.columns[self.key]
-        perm = sort_segments(kc, self.offsets, descending, nulls_first, stream=stream, out=self.ids[0],
-                             workspace=self.ws)
-        gather(DeviceBatch([kc]), perm, stream, out=DeviceBatch([self.k[0]]))
-        nruns = len(self.offsets) - 1
-        levels = 0
-        while (nruns + (1 << levels) - 1) >> levels > 1:
-            levels += 1
-        okey = out.columns[self.key]
-        src = DeviceBatch([self.k[0], DeviceColumn(self.ids[0], A.INT32)])
-        offs = self.offsets
-        for lvl in range(levels):
-            last = lvl == levels - 1
-            if last:
-                dst = DeviceBatch([okey, DeviceColumn(self.ids[2], A.INT32)])
-            else:
-                j = (lvl + 1) % 2
-                dst = DeviceBatch([self.k[j], DeviceColumn(self.ids[j], A.INT32)])
-            offs = merge_pass(src, 0, descending, offs, dst, nulls_first, stream)
-            src = dst
-        if levels == 0:
-            okey.data.copy_(self.k[0].data)
-            if okey.nulls is not None and self.k[0].nulls is not None:
-                okey.nulls.copy_(self.k[0].nulls)
-        final_ids = src.columns[1].data
-        rest = [i for i in range(len(batch.columns)) if i != self.key]
-        if rest:
-            gather(DeviceBatch([batch.columns[i] for i in rest]), final_ids, stream,
-                   out=DeviceBatch([out.columns[i] for i in rest]))
+        ib, _ia = batch.c()
+        ob, _oa = out.c()
+        _check(lib().yq_order_by(C.byref(ib), self.key, int(descending), int(nulls_first), self._offs,
+                                 len(self.offsets) - 1, C.byref(ob), self.ws.data_ptr(), self.ws.numel(),
+                                 _stream(stream)), "yq_order_by")
         return out
+
+
+def order_by(batch: DeviceBatch, key: int, descending: bool, offsets: list[int], nulls_first=False,
+             stream=None) -> DeviceBatch:
+    """One-shot yq_order_by into a new batch (workspace from the library)."""
+    out = DeviceBatch([DeviceColumn.empty(c.type, c.rows, c.width if c.type == A.TEXT else None,
+                                          nulls=c.nulls is not None) for c in batch.columns])
+    offs = (C.c_uint32 * len(offsets))(*offsets)
+    ib, _ia = batch.c()
+    ob, _oa = out.c()
+    _check(lib().yq_order_by(C.byref(ib), key, int(descending), int(nulls_first), offs, len(offsets) - 1,
+                             C.byref(ob), None, 0, _stream(stream)), "yq_order_by")
+    return out
