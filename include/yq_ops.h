@@ -270,9 +270,9 @@ int yq_filter_project_noalloc(const yq_batch* batch, const yq_program* predicate
  * for every key are skipped (this reads the histogram back: the call
  * synchronises `stream` once). NULL keys sort last unless nulls_first. */
 typedef struct yq_sort_config {
-  int32_t digit_bits;        /* 4, 6 or 8; 0 = autotuned                       */
-  int32_t items_per_thread;  /* 0 = autotuned                                  */
-  int32_t block_threads;     /* 0 = autotuned                                  */
+  int32_t digit_bits;        /* 4, 6 or 8; 0 = autotuned (yq_sort_autotune), else 8 */
+  int32_t items_per_thread;  /* 0 = autotuned / the variant's default          */
+  int32_t block_threads;     /* fixed at 256 (kept for layout)                 */
   int32_t keep_trivial;      /* 1 = never skip passes (no host read-back)      */
 } yq_sort_config;
 
@@ -341,6 +341,41 @@ size_t yq_order_by_workspace_size(const yq_column* key, uint32_t rows, const uin
 int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
                 const uint32_t* run_offsets, int32_t nruns, yq_batch* out, void* workspace,
                 size_t workspace_bytes, void* stream);
+
+/* ---- Batched forms: many independent tasks in one set of launches.
+ * The tasks' rows sit back to back in one batch (task g = rows
+ * [seg_offsets[g], seg_offsets[g+1]), host array); every launch walks the
+ * steps of all tasks as one device-side queue, so hundreds of small tasks
+ * cost a handful of launches instead of hundreds (the reference runs each
+ * batch through its own launch sequence, operator.hpp:45-47).
+ *
+ * yq_filter_aggregate_segments: WHERE + aggregates per task into
+ * states[g] = (char*)states + g * yq_agg_state_bytes(nagg), each initialised
+ * by yq_agg_states_init. Task starts must be multiples of 16 rows. Results
+ * equal running each task alone (partials fold in a fixed order).
+ * yq_order_by_segments: ORDER BY per task (segmented radix sort + one gather).
+ * With config->keep_trivial set it enqueues device work only and never waits
+ * (it can be captured in a CUDA graph); an error is then left as a non-zero
+ * 32-bit word at offset 0 of `workspace` (required in that mode).
+ * yq_sort_autotune: times every instantiated (digit bits, items per thread)
+ * variant on the given key and segments, remembers the fastest for this key
+ * width and segment size (used whenever a sort's config leaves those fields 0)
+ * and returns it. */
+int yq_agg_states_init(void* states, int32_t count, const yq_agg_spec* aggs, int32_t nagg, void* stream);
+int yq_agg_states_read(const void* states, int32_t count, const yq_agg_spec* aggs, int32_t nagg,
+                       yq_agg_result* out, void* stream);
+size_t yq_filter_aggregate_segments_workspace_size(uint32_t rows, int32_t nseg);
+int yq_filter_aggregate_segments(const yq_batch* batch, const uint32_t* seg_offsets, int32_t nseg,
+                                 const yq_program* predicate, const yq_constants* constants,
+                                 const yq_agg_spec* aggs, int32_t nagg, void* states, void* workspace,
+                                 size_t workspace_bytes, void* stream);
+size_t yq_order_by_segments_workspace_size(const yq_column* key, uint32_t rows, const uint32_t* seg_offsets,
+                                           int32_t nseg);
+int yq_order_by_segments(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
+                         const uint32_t* seg_offsets, int32_t nseg, yq_batch* out, const yq_sort_config* config,
+                         void* workspace, size_t workspace_bytes, void* stream);
+int yq_sort_autotune(const yq_column* key, uint32_t rows, const uint32_t* seg_offsets, int32_t nseg,
+                     int32_t descending, yq_sort_config* best, void* stream);
 
 /* ---- Inner join (nested loop semantics) and cross product.
  * Replaces ComparisonJoinExpression/ConjunctionJoinExpression +

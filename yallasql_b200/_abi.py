@@ -116,6 +116,14 @@ PROTOTYPES = {
     "yq_merge_workspace_size": (sz, [u32, i32]),
     "yq_merge_pass": (C.c_int, [P(Column), i32, i32, i32, i32, P(u32), i32, P(Column), vp, sz, vp]),
     "yq_order_by_workspace_size": (sz, [P(Column), u32, P(u32), i32]),
+    "yq_agg_states_init": (C.c_int, [vp, i32, P(AggSpec), i32, vp]),
+    "yq_agg_states_read": (C.c_int, [vp, i32, P(AggSpec), i32, P(AggResult), vp]),
+    "yq_filter_aggregate_segments_workspace_size": (sz, [u32, i32]),
+    "yq_filter_aggregate_segments": (C.c_int, [P(Batch), P(u32), i32, P(Program), P(Constants), P(AggSpec), i32,
+                                                vp, vp, sz, vp]),
+    "yq_order_by_segments_workspace_size": (sz, [P(Column), u32, P(u32), i32]),
+    "yq_order_by_segments": (C.c_int, [P(Batch), i32, i32, i32, P(u32), i32, P(Batch), P(SortConfig), vp, sz, vp]),
+    "yq_sort_autotune": (C.c_int, [P(Column), u32, P(u32), i32, i32, P(SortConfig), vp]),
     "yq_order_by": (C.c_int, [P(Batch), i32, i32, i32, P(u32), i32, P(Batch), vp, sz, vp]),
     "yq_join_workspace_size": (sz, [u32, u32]),
     "yq_join_pairs": (C.c_int, [P(Batch), P(Batch), P(JoinCond), i32, vp, vp, u64, P(u64), vp, sz, vp]),

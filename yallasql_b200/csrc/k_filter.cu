@@ -9,6 +9,7 @@
 // reads are staged in shared memory a few steps ahead by bulk copies
 // (yq_stage.cuh) when they are 16-byte aligned and fit; otherwise the kernel
 // reads them from global memory directly.
+#include <vector>
 #include "vm_host.cuh"
 #include "yq_agg.cuh"
 #include "yq_lookback.cuh"
@@ -79,7 +80,7 @@ __global__ void __launch_bounds__(kRowBlock, 2) k_filter_aggregate(const __grid_
     if (threadIdx.x == 0)
       for (int j = 0; j < S - 1; ++j) {
         const uint32_t t = blockIdx.x + (uint32_t)j * G;
-        if (t < ntiles && full_step(t, n)) stage_issue(F.SP, j, t * kStepRows);
+        if (t < ntiles) stage_start(F.SP, j, t * kStepRows, step_rows(t, n));
       }
   }
   int slot = 0;
@@ -95,9 +96,9 @@ __global__ void __launch_bounds__(kRowBlock, 2) k_filter_aggregate(const __grid_
       if (threadIdx.x == 0) {
         const uint32_t t = tile + (uint32_t)(S - 1) * G;
         const int ns = slot == 0 ? S - 1 : slot - 1;
-        if (t < ntiles && full_step(t, n)) stage_issue(F.SP, ns, t * kStepRows);
+        if (t < ntiles) stage_start(F.SP, ns, t * kStepRows, step_rows(t, n));
       }
-      stage_step(F.SP, slot, parity, tile, n, err);
+      stage_finish(F.SP, slot, parity, X.tile0, step_rows(tile, n), err);
       X.stage = (uint32_t)slot * F.SP.stage_bytes;
     }
     E.sel = X.inr;
@@ -191,6 +192,129 @@ static int launch_filter_aggregate(const FAParams& F, uint32_t rows, Acc* partia
     k_filter_aggregate<false><<<grid, kRowBlock, 0, s>>>(F, rows, partials, ticket, state);
   YQ_CHECK_LAUNCH();
   return YQ_OK;
+}
+
+// ======================================================= segmented aggregate
+// Many independent filter+aggregate tasks in one launch: task g owns rows
+// [seg[g], seg[g+1]) of the batch and its own aggregate state. Steps never
+// straddle tasks; the persistent blocks walk the steps of all tasks as one
+// queue (step -> task by binary search over the tasks' first steps), write
+// one partial per step, and k_agg_seg_fold folds each task's partials in step
+// order, so every task's result is deterministic and equal to the result of
+// running it alone.
+struct FASegParams {
+  FAParams F;
+  const uint32_t* seg;    // [nseg + 1] row offsets
+  const uint32_t* step0;  // [nseg + 1] first step of each task
+  int32_t nseg;
+  uint32_t nsteps;
+  Acc* partials;          // [nsteps][YQ_MAX_AGGREGATES]
+  uint32_t* err;
+};
+
+__device__ __forceinline__ int seg_of_step(const uint32_t* step0, int nseg, uint32_t t) {
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(step0 + mid) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void seg_step(const FASegParams& Q, uint32_t t, uint32_t& row0, uint32_t& rows) {
+  const int g = seg_of_step(Q.step0, Q.nseg, t);
+  row0 = __ldg(Q.seg + g) + (t - __ldg(Q.step0 + g)) * kStepRows;
+  const uint32_t end = __ldg(Q.seg + g + 1);
+  rows = end - row0 < kStepRows ? end - row0 : kStepRows;
+}
+
+template <bool STAGED>
+__global__ void __launch_bounds__(kRowBlock, 2) k_filter_aggregate_seg(const __grid_constant__ FASegParams Q) {
+  const FAParams& F = Q.F;
+  const uint32_t G = gridDim.x;
+  int S = 1;
+  if constexpr (STAGED) {
+    S = F.SP.nstages;
+    stage_init(F.SP);
+    if (threadIdx.x == 0)
+      for (int j = 0; j < S - 1; ++j) {
+        const uint32_t t = blockIdx.x + (uint32_t)j * G;
+        if (t < Q.nsteps) {
+          uint32_t r0, nr;
+          seg_step(Q, t, r0, nr);
+          stage_start(F.SP, j, r0, nr);
+        }
+      }
+  }
+  int slot = 0;
+  uint32_t parity = 0;
+  for (uint32_t t = blockIdx.x; t < Q.nsteps; t += G) {
+    uint32_t row0, rows;
+    seg_step(Q, t, row0, rows);
+    Ctx X;
+    X.tile0 = row0;
+    X.lr = threadIdx.x * ITEMS;
+    X.inr = in_range_bits(X.lr, rows);
+    X.stage = 0;
+    if constexpr (STAGED) {
+      __syncthreads();  // every thread is done with the previous step: its slot is free
+      if (threadIdx.x == 0) {
+        const uint32_t tn = t + (uint32_t)(S - 1) * G;
+        const int ns = slot == 0 ? S - 1 : slot - 1;
+        if (tn < Q.nsteps) {
+          uint32_t r0, nr;
+          seg_step(Q, tn, r0, nr);
+          stage_start(F.SP, ns, r0, nr);
+        }
+      }
+      stage_finish(F.SP, slot, parity, row0, rows, Q.err);
+      X.stage = (uint32_t)slot * F.SP.stage_bytes;
+    }
+    AggEmit E;
+    agg_thread_init(E, F.A);
+    E.sel = X.inr;
+    Stack St;
+    run_vm<STAGED>(F.P, 0, F.pc_end, X, St, E);
+    agg_block_partial<kRowBlock>(E, __popc(E.sel), F.A, Q.partials + (size_t)t * YQ_MAX_AGGREGATES);
+    if (++slot == S) {
+      slot = 0;
+      parity ^= 1u;
+    }
+  }
+}
+
+// One warp per task: aggregate a < nagg folds the task's step partials in order.
+__global__ void k_agg_seg_fold(const Acc* __restrict__ partials, const uint32_t* __restrict__ step0, int nseg,
+                               const AggParams A, Acc* states, const uint32_t* err) {
+  const int g = blockIdx.x;
+  const int a = threadIdx.x;
+  if (g >= nseg) return;
+  Acc* st = reinterpret_cast<Acc*>(reinterpret_cast<char*>(states) + (size_t)g * kAggStateBytes);
+  if (a == 0 && *err) *agg_state_err(st) |= *err;
+  if (a >= A.nagg) return;
+  const int upd = A.upd[a];
+  Acc t{0, acc_identity(upd)};
+  for (uint32_t s = step0[g]; s < step0[g + 1]; ++s) {
+    const Acc p = partials[(size_t)s * YQ_MAX_AGGREGATES + a];
+    t.cnt += p.cnt;
+    t.bits = acc_merge(upd, t.bits, p.bits);
+  }
+  Acc cur = st[a];
+  cur.cnt += t.cnt;
+  cur.bits = acc_merge(upd, cur.bits, t.bits);
+  st[a] = cur;
+}
+
+static uint32_t seg_steps(const uint32_t* seg, int nseg, std::vector<uint32_t>& step0) {
+  step0.resize((size_t)nseg + 1);
+  uint32_t t = 0;
+  for (int g = 0; g < nseg; ++g) {
+    step0[g] = t;
+    t += ceil_div<uint32_t>(seg[g + 1] - seg[g], kStepRows);
+  }
+  step0[nseg] = t;
+  return t;
 }
 
 // ================================================================ project
@@ -307,7 +431,7 @@ __global__ void __launch_bounds__(kRowBlock, 2) k_filter_project(const __grid_co
       const uint32_t t = atomicAdd(tile_counter, 1u);
       s_tiles[j] = t;
       if constexpr (STAGED)
-        if (t < ntiles && full_step(t, n)) stage_issue(F.SP, j, t * kStepRows);
+        if (t < ntiles) stage_start(F.SP, j, t * kStepRows, step_rows(t, n));
     }
   int slot = 0;
   uint32_t parity = 0;
@@ -318,7 +442,7 @@ __global__ void __launch_bounds__(kRowBlock, 2) k_filter_project(const __grid_co
       const uint32_t t = atomicAdd(tile_counter, 1u);
       s_tiles[ns] = t;
       if constexpr (STAGED)
-        if (t < ntiles && full_step(t, n)) stage_issue(F.SP, ns, t * kStepRows);
+        if (t < ntiles) stage_start(F.SP, ns, t * kStepRows, step_rows(t, n));
     }
     __syncthreads();
     const uint32_t tile = s_tiles[slot];
@@ -329,7 +453,7 @@ __global__ void __launch_bounds__(kRowBlock, 2) k_filter_project(const __grid_co
     X.inr = in_range_bits(X.tile0 + X.lr, n);
     X.stage = 0;
     if constexpr (STAGED) {
-      stage_step(F.SP, slot, parity, tile, n, err);
+      stage_finish(F.SP, slot, parity, X.tile0, step_rows(tile, n), err);
       X.stage = (uint32_t)slot * F.SP.stage_bytes;
     }
     ProjEmit E;
@@ -517,6 +641,119 @@ int yq_agg_state_read(const void* state, const yq_agg_spec* aggs, int32_t nagg, 
         break;
     }
   }
+  return YQ_OK;
+}
+
+int yq_agg_states_init(void* states, int32_t count, const yq_agg_spec* aggs, int32_t nagg, void* stream) {
+  if (!states || count < 0) return YQ_ERR_INVALID_ARG;
+  for (int g = 0; g < count; ++g)
+    YQ_TRY(yq_agg_state_init(static_cast<char*>(states) + (size_t)g * kAggStateBytes, aggs, nagg, stream));
+  return YQ_OK;
+}
+
+int yq_agg_states_read(const void* states, int32_t count, const yq_agg_spec* aggs, int32_t nagg, yq_agg_result* out,
+                       void* stream) {
+  if (!states || !out || count < 0) return YQ_ERR_INVALID_ARG;
+  YQ_TRY(check_aggs(aggs, nagg));
+  if (count == 0) return YQ_OK;
+  std::vector<char> host((size_t)count * kAggStateBytes);
+  cudaStream_t s = as_stream(stream);
+  YQ_TRY_CUDA(cudaMemcpyAsync(host.data(), states, host.size(), cudaMemcpyDeviceToHost, s));
+  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  int status = YQ_OK;
+  for (int g = 0; g < count; ++g) {
+    Acc* st = reinterpret_cast<Acc*>(host.data() + (size_t)g * kAggStateBytes);
+    if (*agg_state_err(st)) status = YQ_ERR_TIMEOUT;
+    for (int a = 0; a < nagg; ++a) {
+      const Acc& h = st[a];
+      yq_agg_result& r = out[(size_t)g * nagg + a];
+      const int kind = aggs[a].kind, t = aggs[a].input_type;
+      const bool flt = (t == YQ_FLOAT32 || t == YQ_FLOAT64);
+      double hf;
+      memcpy(&hf, &h.bits, sizeof(hf));
+      const long long hi = (long long)h.bits;
+      r.kind = kind;
+      r.count = h.cnt;
+      r.i = 0;
+      r.f = 0.0;
+      r.is_null = 0;
+      if (kind == YQ_AGG_COUNT_STAR || kind == YQ_AGG_COUNT) {
+        r.i = h.cnt;
+      } else if (kind == YQ_AGG_AVG) {
+        r.is_null = h.cnt == 0;
+        if (h.cnt) r.f = flt ? hf / (double)h.cnt : (double)hi / (double)h.cnt;
+      } else {
+        r.is_null = h.cnt == 0;
+        if (flt) r.f = hf;
+        else r.i = hi;
+      }
+    }
+  }
+  return status;
+}
+
+size_t yq_filter_aggregate_segments_workspace_size(uint32_t rows, int32_t nseg) {
+  if (nseg < 0) return 0;
+  WsSize w;
+  const size_t steps = (size_t)ceil_div<uint32_t>(rows, kStepRows) + (size_t)nseg;
+  w.add<uint32_t>((size_t)nseg + 1);
+  w.add<uint32_t>((size_t)nseg + 1);
+  w.add<Acc>(steps * YQ_MAX_AGGREGATES);
+  w.add<uint32_t>(4);
+  return w.total();
+}
+
+int yq_filter_aggregate_segments(const yq_batch* batch, const uint32_t* seg_offsets, int32_t nseg,
+                                 const yq_program* predicate, const yq_constants* constants, const yq_agg_spec* aggs,
+                                 int32_t nagg, void* states, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!batch || !states || nseg < 0 || (nseg > 0 && !seg_offsets)) return YQ_ERR_INVALID_ARG;
+  if (nseg == 0) return YQ_OK;
+  if (seg_offsets[0] != 0 || seg_offsets[nseg] > batch->rows) return YQ_ERR_INVALID_ARG;
+  for (int g = 0; g < nseg; ++g) {
+    if (seg_offsets[g + 1] < seg_offsets[g]) return YQ_ERR_INVALID_ARG;
+    if (seg_offsets[g] % 16u) return YQ_ERR_INVALID_ARG;  // task starts on a 16-row boundary
+  }
+  FASegParams Q;
+  memset(&Q, 0, sizeof(Q));
+  YQ_TRY(prepare_filter_aggregate(batch, predicate, constants, aggs, nagg, &Q.F));
+  if (nagg == 0) return YQ_OK;
+  std::vector<uint32_t> step0;
+  const uint32_t nsteps = seg_steps(seg_offsets, nseg, step0);
+  cudaStream_t s = as_stream(stream);
+  Workspace ws;
+  YQ_TRY(ws.acquire(workspace, workspace_bytes, yq_filter_aggregate_segments_workspace_size(batch->rows, nseg), s));
+  uint32_t* d_seg = ws.take<uint32_t>((size_t)nseg + 1);
+  uint32_t* d_step0 = ws.take<uint32_t>((size_t)nseg + 1);
+  Acc* partials = ws.take<Acc>(((size_t)ceil_div<uint32_t>(batch->rows, kStepRows) + nseg) * YQ_MAX_AGGREGATES);
+  uint32_t* d_err = ws.take<uint32_t>(4);
+  YQ_TRY(h2d_async(d_seg, seg_offsets, ((size_t)nseg + 1) * sizeof(uint32_t), s));
+  YQ_TRY(h2d_async(d_step0, step0.data(), ((size_t)nseg + 1) * sizeof(uint32_t), s));
+  YQ_TRY_CUDA(cudaMemsetAsync(d_err, 0, 4 * sizeof(uint32_t), s));
+  Q.seg = d_seg;
+  Q.step0 = d_step0;
+  Q.nseg = nseg;
+  Q.nsteps = nsteps;
+  Q.partials = partials;
+  Q.err = d_err;
+  if (nsteps > 0) {
+    const bool staged = Q.F.SP.nstages > 0;
+    const void* kern =
+        staged ? (const void*)k_filter_aggregate_seg<true> : (const void*)k_filter_aggregate_seg<false>;
+    const size_t smem = stage_smem_bytes(Q.F.SP);
+    static size_t done_smem = 0;
+    YQ_TRY(allow_smem(kern, smem, done_smem));
+    static GridCache gc[2];
+    const int grid = gc[staged ? 1 : 0].grid(kern, smem, nsteps);
+    ProfScope ps("filter_aggregate_seg", s,
+                 (double)seg_offsets[nseg] * row_bytes_of(Q.F.P, program_columns(Q.F.P, Q.F.pc_end, 0)));
+    if (staged)
+      k_filter_aggregate_seg<true><<<grid, kRowBlock, smem, s>>>(Q);
+    else
+      k_filter_aggregate_seg<false><<<grid, kRowBlock, 0, s>>>(Q);
+    YQ_CHECK_LAUNCH();
+  }
+  k_agg_seg_fold<<<nseg, 32, 0, s>>>(partials, d_step0, nseg, Q.F.A, static_cast<Acc*>(states), d_err);
+  YQ_CHECK_LAUNCH();
   return YQ_OK;
 }
 

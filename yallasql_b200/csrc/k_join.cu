@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(kRowBlock, 2) k_join_aggregate(const __grid_co
     if (threadIdx.x == 0)
       for (int j = 0; j < S - 1; ++j) {
         const uint32_t t = blockIdx.x + (uint32_t)j * G;
-        if (t < ntiles && full_step(t, n)) stage_issue(F.SP, j, t * kStepRows);
+        if (t < ntiles) stage_start(F.SP, j, t * kStepRows, step_rows(t, n));
       }
   }
   const DevCol& kc = F.P.cols[F.fkey_col];
@@ -495,9 +495,9 @@ __global__ void __launch_bounds__(kRowBlock, 2) k_join_aggregate(const __grid_co
       if (threadIdx.x == 0) {
         const uint32_t t = tile + (uint32_t)(S - 1) * G;
         const int ns = slot == 0 ? S - 1 : slot - 1;
-        if (t < ntiles && full_step(t, n)) stage_issue(F.SP, ns, t * kStepRows);
+        if (t < ntiles) stage_start(F.SP, ns, t * kStepRows, step_rows(t, n));
       }
-      stage_step(F.SP, slot, parity, tile, n, err);
+      stage_finish(F.SP, slot, parity, X.tile0, step_rows(tile, n), err);
       X.stage = (uint32_t)slot * F.SP.stage_bytes;
     }
     E.sel = X.inr;

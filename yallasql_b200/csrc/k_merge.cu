@@ -707,6 +707,64 @@ extern "C" size_t yq_order_by_workspace_size(const yq_column* key, uint32_t rows
   return w.total();
 }
 
+// Many independent ORDER BY tasks: task g owns rows [seg[g], seg[g+1]);
+// one segmented sort orders every task and one gather moves every column.
+extern "C" size_t yq_order_by_segments_workspace_size(const yq_column* key, uint32_t rows, const uint32_t* seg_offsets,
+                                                      int32_t nseg) {
+  if (!key || !seg_offsets || nseg <= 0) return 0;
+  KeyJob j{*key, 0, 0};
+  size_t sort_bytes = 0;
+  if (sort_segments_impl(&j, 1, rows, seg_offsets, nseg, nullptr, nullptr, nullptr, 0, nullptr, &sort_bytes) != YQ_OK)
+    return 0;
+  WsSize w;
+  w.add<uint32_t>(4);
+  w.add<char>(sort_bytes);
+  w.add<uint32_t>((size_t)rows + 16);
+  return w.total();
+}
+
+extern "C" int yq_order_by_segments(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
+                                    const uint32_t* seg_offsets, int32_t nseg, yq_batch* out,
+                                    const yq_sort_config* config, void* workspace, size_t workspace_bytes,
+                                    void* stream) {
+  if (!in || !out || !seg_offsets || nseg <= 0 || key_col < 0 || key_col >= in->ncols || out->ncols != in->ncols ||
+      in->ncols > YQ_MAX_BATCH_COLUMNS)
+    return YQ_ERR_INVALID_ARG;
+  const uint32_t rows = in->rows;
+  if (seg_offsets[0] != 0 || seg_offsets[nseg] != rows) return YQ_ERR_INVALID_ARG;
+  for (int c = 0; c < in->ncols; ++c)
+    if (in->columns[c].type != out->columns[c].type || in->columns[c].width != out->columns[c].width)
+      return YQ_ERR_INVALID_ARG;
+  const bool no_wait = config && config->keep_trivial;
+  if (no_wait && !workspace) return YQ_ERR_INVALID_ARG;  // the error word lives in the caller's workspace
+  cudaStream_t s = as_stream(stream);
+  const size_t need = yq_order_by_segments_workspace_size(&in->columns[key_col], rows, seg_offsets, nseg);
+  if (need == 0) return YQ_ERR_INVALID_ARG;
+  Workspace ws;
+  YQ_TRY(ws.acquire(workspace, workspace_bytes, need, s));
+  uint32_t* d_err = ws.take<uint32_t>(4);
+  KeyJob j{in->columns[key_col], descending != 0, nulls_first != 0};
+  size_t sort_bytes = 0;
+  YQ_TRY(sort_segments_impl(&j, 1, rows, seg_offsets, nseg, nullptr, nullptr, nullptr, 0, nullptr, &sort_bytes));
+  char* sort_ws = ws.take<char>(sort_bytes);
+  uint32_t* perm = ws.take<uint32_t>((size_t)rows + 16);
+  if (rows == 0) return YQ_OK;
+  uint32_t* sort_err = nullptr;
+  YQ_TRY(sort_segments_impl(&j, 1, rows, seg_offsets, nseg, perm, config, sort_ws, sort_bytes, s, nullptr, nullptr,
+                            nullptr, true, &sort_err));
+  yq_column outs[YQ_MAX_BATCH_COLUMNS];
+  for (int c = 0; c < in->ncols; ++c) outs[c] = out->columns[c];
+  YQ_TRY(yq_gather(in->columns, in->ncols, perm, rows, outs, s));
+  YQ_TRY_CUDA(cudaMemcpyAsync(d_err, sort_err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+  if (no_wait) return YQ_OK;
+  uint32_t e = 0;
+  YQ_TRY_CUDA(cudaMemcpyAsync(&e, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  if (e & kErrTimeout) return YQ_ERR_TIMEOUT;
+  if (e & kErrBounds) return YQ_ERR_INVALID_ARG;
+  return YQ_OK;
+}
+
 extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
                            const uint32_t* run_offsets, int32_t nruns, yq_batch* out, void* workspace,
                            size_t workspace_bytes, void* stream) {

@@ -18,6 +18,8 @@
 // so all 4 MB batches of a table (or all tasks of a batch) sort in one set of
 // launches. A single global sort is the one-segment case.
 #include <string.h>
+#include <map>
+#include <mutex>
 #include <vector>
 #include "yq_sort.cuh"
 
@@ -554,18 +556,48 @@ static SortKernels make_kernels() {
   return k;
 }
 
-static bool pick_kernels(int kw, int d, SortKernels& k) {
-  switch (kw * 100 + d) {
-    case 108: k = make_kernels<1, 8, 16>(); return true;
-    case 106: k = make_kernels<1, 6, 16>(); return true;
-    case 104: k = make_kernels<1, 4, 16>(); return true;
-    case 208: k = make_kernels<2, 8, 12>(); return true;
-    case 206: k = make_kernels<2, 6, 12>(); return true;
-    case 204: k = make_kernels<2, 4, 12>(); return true;
-    case 408: k = make_kernels<4, 8, 8>(); return true;
-    case 808: k = make_kernels<8, 8, 4>(); return true;
+// Instantiated (key words, digit bits, items per thread) variants; items = 0
+// picks the first listed for (kw, d).
+static bool pick_kernels(int kw, int d, int items, SortKernels& k) {
+  switch (kw * 10000 + d * 100 + items) {
+    case 10816: case 10800: k = make_kernels<1, 8, 16>(); return true;
+    case 10812: k = make_kernels<1, 8, 12>(); return true;
+    case 10808: k = make_kernels<1, 8, 8>(); return true;
+    case 10616: case 10600: k = make_kernels<1, 6, 16>(); return true;
+    case 10416: case 10400: k = make_kernels<1, 4, 16>(); return true;
+    case 20812: case 20800: k = make_kernels<2, 8, 12>(); return true;
+    case 20808: k = make_kernels<2, 8, 8>(); return true;
+    case 20612: case 20600: k = make_kernels<2, 6, 12>(); return true;
+    case 20412: case 20400: k = make_kernels<2, 4, 12>(); return true;
+    case 40808: case 40800: k = make_kernels<4, 8, 8>(); return true;
+    case 80804: case 80800: k = make_kernels<8, 8, 4>(); return true;
     default: return false;
   }
+}
+
+// Fewest items per thread any variant of key width kw uses (sizes the
+// look-back status of the most tiles a tuned choice can make).
+static int min_items(int kw) { return kw == 1 ? 8 : (kw == 2 ? 8 : (kw == 4 ? 8 : 4)); }
+
+// Autotuned (digit bits, items) per (key words, log2 of rows per segment).
+static std::mutex g_tune_mu;
+static std::map<std::pair<int, int>, std::pair<int, int>> g_tuned;
+
+static int rows_bucket(uint32_t rows, int nseg) {
+  uint32_t avg = nseg > 0 ? rows / (uint32_t)nseg : rows;
+  int b = 0;
+  while (avg > 1) {
+    avg >>= 1;
+    ++b;
+  }
+  return b;
+}
+
+static std::pair<int, int> tuned_choice(int kw, uint32_t rows, int nseg) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tuned.find({kw, rows_bucket(rows, nseg)});
+  if (it == g_tuned.end()) return {8, 0};
+  return it->second;
 }
 
 struct SegPlan {
@@ -597,20 +629,29 @@ struct KeyPlan {
   uint32_t tile_rows, ntiles;
 };
 
-static int plan_key(const yq_column& c, int vwords_override, int want_d, const uint32_t* seg_offsets, int nseg,
-                    KeyPlan& kp) {
+// want_d / want_items = 0: the autotuned choice for this key width and
+// segment size (yq_sort_autotune), else 8-bit digits with the default items.
+// `sizing`: tile count for the variant with the fewest items (workspace bound).
+static int plan_key(const yq_column& c, int vwords_override, int want_d, int want_items, const uint32_t* seg_offsets,
+                    int nseg, KeyPlan& kp, bool sizing = false) {
   kp.sh.vwords = vwords_override >= 0 ? vwords_override : key_value_words(c);
   kp.sh.null_word = c.nulls != nullptr;
   kp.sh.kw = round_kw(kp.sh.vwords + kp.sh.null_word);
   if (kp.sh.kw < 0) return YQ_ERR_UNSUPPORTED;
   kp.D = want_d;
-  if (!pick_kernels(kp.sh.kw, kp.D, kp.K)) {
+  int items = want_items;
+  if (kp.D == 0) {
+    const std::pair<int, int> t = tuned_choice(kp.sh.kw, seg_offsets[nseg] - seg_offsets[0], nseg);
+    kp.D = t.first;
+    if (items == 0) items = t.second;
+  }
+  if (!pick_kernels(kp.sh.kw, kp.D, items, kp.K)) {
     kp.D = 8;
-    if (!pick_kernels(kp.sh.kw, 8, kp.K)) return YQ_ERR_UNSUPPORTED;
+    if (!pick_kernels(kp.sh.kw, 8, 0, kp.K)) return YQ_ERR_UNSUPPORTED;
   }
   kp.P = (kp.sh.kw * 32 + kp.D - 1) / kp.D;
   kp.R = 1 << kp.D;
-  kp.tile_rows = (uint32_t)kSortBlock * kp.K.items;
+  kp.tile_rows = (uint32_t)kSortBlock * (sizing ? min_items(kp.sh.kw) : kp.K.items);
   kp.ntiles = 0;
   for (int i = 0; i < nseg; ++i) kp.ntiles += ceil_div<uint32_t>(seg_offsets[i + 1] - seg_offsets[i], kp.tile_rows);
   return YQ_OK;
@@ -661,8 +702,10 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
   if (seg_offsets_host[0] != 0 || seg_offsets_host[nseg] != rows) return YQ_ERR_INVALID_ARG;
   for (int i = 0; i < nseg; ++i)
     if (seg_offsets_host[i + 1] < seg_offsets_host[i]) return YQ_ERR_INVALID_ARG;
-  const int want_d = (cfg && cfg->digit_bits) ? cfg->digit_bits : 8;
-  if (want_d != 4 && want_d != 6 && want_d != 8) return YQ_ERR_INVALID_ARG;
+  const int want_d = cfg ? cfg->digit_bits : 0;
+  const int want_items = cfg ? cfg->items_per_thread : 0;
+  if (want_d != 0 && want_d != 4 && want_d != 6 && want_d != 8) return YQ_ERR_INVALID_ARG;
+  if (want_items < 0 || want_items > 16) return YQ_ERR_INVALID_ARG;
   const bool keep_trivial = cfg && cfg->keep_trivial;
 
   // Size buffers for the widest plan any key can take (text keys are sized
@@ -675,7 +718,9 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
     KeyPlan kp;
     int vw = key_value_words(c);
     if (c.type == YQ_TEXT && vw > 8 - (c.nulls ? 1 : 0)) vw = 8 - (c.nulls ? 1 : 0);
-    int st = plan_key(c, vw, want_d, seg_offsets_host, nseg, kp);
+    // Sized for 8-bit digits (the largest passes x bins) and the fewest items
+    // per thread (the most tiles), which bound every variant's buffers.
+    int st = plan_key(c, vw, 8, 0, seg_offsets_host, nseg, kp, true);
     if (st != YQ_OK) return st;
     // For a text key this is the plan at its full (clamped) width, which
     // bounds every narrower plan: fewer words mean fewer passes and larger tiles.
@@ -735,7 +780,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
       if (vw == 0 && !c.nulls) continue;  // every key equal: order unchanged
     }
     KeyPlan kp;
-    YQ_TRY(plan_key(c, vw, want_d, seg_offsets_host, nseg, kp));
+    YQ_TRY(plan_key(c, vw, want_d, want_items, seg_offsets_host, nseg, kp));
     SegPlan sp;
     plan_segments(seg_offsets_host, nseg, kp.tile_rows, sp);
     YQ_TRY(h2d_async(d_seg, sp.seg.data(), (nseg + 1) * sizeof(uint32_t), s));
@@ -892,6 +937,65 @@ int yq_sort_segments(const yq_column* key, uint32_t rows, const uint32_t* seg_of
   KeyJob j{*key, descending != 0, nulls_first != 0};
   return sort_segments_impl(&j, 1, rows, seg_offsets, nseg, out_perm, config, workspace, workspace_bytes,
                             as_stream(stream), nullptr);
+}
+
+int yq_sort_autotune(const yq_column* key, uint32_t rows, const uint32_t* seg_offsets, int32_t nseg,
+                     int32_t descending, yq_sort_config* best, void* stream) {
+  if (!key || !seg_offsets || nseg <= 0 || !best || !valid_key_column(*key)) return YQ_ERR_INVALID_ARG;
+  const int kw = round_kw(key_value_words(*key) + (key->nulls ? 1 : 0));
+  if (kw < 0) return YQ_ERR_UNSUPPORTED;
+  // Every instantiated (digit bits, items per thread) variant of this key width.
+  std::vector<std::pair<int, int>> cand;
+  for (int d : {8, 6, 4})
+    for (int it : {16, 12, 8, 4}) {
+      SortKernels k;
+      if (pick_kernels(kw, d, it, k) && k.items == it) cand.push_back({d, it});
+    }
+  if (cand.empty()) return YQ_ERR_UNSUPPORTED;
+  cudaStream_t s = as_stream(stream);
+  KeyJob j{*key, descending != 0, 0};
+  size_t wsb = 0;
+  YQ_TRY(sort_segments_impl(&j, 1, rows, seg_offsets, nseg, nullptr, nullptr, nullptr, 0, nullptr, &wsb));
+  void* ws = nullptr;
+  uint32_t* perm = nullptr;
+  YQ_TRY_CUDA(cudaMallocAsync(&ws, wsb, s));
+  YQ_TRY_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&perm), (size_t)(rows ? rows : 1) * 4, s));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  YQ_TRY_CUDA(cudaEventCreate(&e0));
+  YQ_TRY_CUDA(cudaEventCreate(&e1));
+  float best_ms = 1e30f;
+  std::pair<int, int> pick = cand[0];
+  int status = YQ_OK;
+  for (const auto& c : cand) {
+    yq_sort_config cfg{c.first, c.second, 0, 1};
+    status = sort_segments_impl(&j, 1, rows, seg_offsets, nseg, perm, &cfg, ws, wsb, s, nullptr);  // warm-up
+    if (status != YQ_OK) break;
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 3 && status == YQ_OK; ++r)
+      status = sort_segments_impl(&j, 1, rows, seg_offsets, nseg, perm, &cfg, ws, wsb, s, nullptr);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (status == YQ_OK && ms < best_ms) {
+      best_ms = ms;
+      pick = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(ws, s);
+  cudaFreeAsync(perm, s);
+  if (status != YQ_OK) return status;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[{kw, rows_bucket(rows, nseg)}] = pick;
+  }
+  best->digit_bits = pick.first;
+  best->items_per_thread = pick.second;
+  best->block_threads = kSortBlock;
+  best->keep_trivial = 0;
+  return YQ_OK;
 }
 
 int yq_gather(const yq_column* in, int32_t ncols, const uint32_t* perm, uint32_t rows, yq_column* out, void* stream) {

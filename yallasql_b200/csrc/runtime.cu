@@ -31,8 +31,34 @@ int g_stage_next = 0;
 int g_stage_dev = -1;
 }  // namespace
 
+// Under stream capture a copy from a reused pinned slot would be replayed
+// from whatever the slot holds then; the bytes go as kernel parameters
+// instead, which the graph keeps with the node.
+struct ParamChunk {
+  uint32_t words[1024];
+};
+
+__global__ void k_param_copy(uint32_t* __restrict__ dst, const __grid_constant__ ParamChunk c, uint32_t nwords) {
+  for (uint32_t i = threadIdx.x; i < nwords; i += blockDim.x) dst[i] = c.words[i];
+}
+
 int h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   if (bytes == 0) return YQ_OK;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  YQ_TRY_CUDA(cudaStreamIsCapturing(s, &cap));
+  if (cap != cudaStreamCaptureStatusNone) {
+    if ((bytes & 3u) || (reinterpret_cast<uintptr_t>(dst) & 3u)) return YQ_ERR_UNSUPPORTED;
+    const uint32_t* w = static_cast<const uint32_t*>(src);
+    const size_t nw = bytes / 4;
+    for (size_t o = 0; o < nw; o += 1024) {
+      ParamChunk c;
+      const uint32_t n = (uint32_t)((nw - o) < 1024 ? (nw - o) : 1024);
+      memcpy(c.words, w + o, (size_t)n * 4);
+      k_param_copy<<<1, 256, 0, s>>>(static_cast<uint32_t*>(dst) + o, c, n);
+      YQ_CHECK_LAUNCH();
+    }
+    return YQ_OK;
+  }
   int dev = 0;
   YQ_TRY_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(g_stage_mu);

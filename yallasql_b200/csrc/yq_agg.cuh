@@ -61,6 +61,39 @@ __device__ __forceinline__ void agg_thread_init(AggEmit& E, const AggParams& A) 
   }
 }
 
+// Block reduction of every thread's accumulators into out[0, nagg) (one
+// partial per block and step); ends with the block synchronised.
+template <int BLOCK>
+__device__ __forceinline__ void agg_block_partial(const AggEmit& E, uint32_t nsel, const AggParams& A, Acc* out) {
+  __shared__ Acc s_part[BLOCK / 32][YQ_MAX_AGGREGATES];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < YQ_MAX_AGGREGATES; ++a) {
+    if (a < A.nagg) {
+      const int upd = A.upd[a];
+      long long c = (upd == UPD_COUNT_STAR) ? (long long)nsel : (long long)E.cnt[a];
+      unsigned long long v = E.acc[a];
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) {
+        c += __shfl_down_sync(0xffffffffu, c, d);
+        v = acc_merge(upd, v, __shfl_down_sync(0xffffffffu, v, d));
+      }
+      if (lane == 0) s_part[warp][a] = Acc{c, v};
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < A.nagg) {
+    const int a = threadIdx.x, upd = A.upd[a];
+    Acc t = s_part[0][a];
+    for (int w = 1; w < BLOCK / 32; ++w) {
+      t.cnt += s_part[w][a].cnt;
+      t.bits = acc_merge(upd, t.bits, s_part[w][a].bits);
+    }
+    out[a] = t;
+  }
+  __syncthreads();
+}
+
 // `nsel` = rows this thread selected (COUNT(*)).
 template <int BLOCK>
 __device__ __forceinline__ void agg_block_finish(const AggEmit& E, uint32_t nsel, const AggParams& A,

@@ -113,23 +113,29 @@ __device__ __forceinline__ void stage_fill(const StagePlan& SP, int slot, uint32
   }
 }
 
-// Make the step of `tile` readable in `slot` (ring pass parity `parity`):
-// a partial last step is filled by every thread, a full one was started by
-// stage_issue and is waited for.
-__device__ __forceinline__ void stage_step(const StagePlan& SP, int slot, uint32_t parity, uint32_t tile, uint32_t n,
-                                           uint32_t* err) {
-  const uint32_t row0 = tile * kStepRows;
-  const uint32_t rows = min(kStepRows, n - row0);
+// Thread 0: start the step of `rows` rows at `row0` in `slot`. A full step is
+// copied by bulk copies; a partial one (the last rows of a batch or of a
+// segment) only completes the slot's barrier phase, and every thread fills
+// it at stage_finish. Either way each use of a slot completes one phase.
+__device__ __forceinline__ void stage_start(const StagePlan& SP, int slot, uint32_t row0, uint32_t rows) {
+  if (rows == kStepRows) stage_issue(SP, slot, row0);
+  else mbar_arrive(stage_bar(SP, slot));
+}
+
+// All threads: make the step in `slot` (ring pass parity `parity`) readable.
+__device__ __forceinline__ void stage_finish(const StagePlan& SP, int slot, uint32_t parity, uint32_t row0,
+                                             uint32_t rows, uint32_t* err) {
+  mbar_wait_bounded(stage_bar(SP, slot), parity, err);
   if (rows < kStepRows) {
     stage_fill(SP, slot, row0, rows);
     __syncthreads();
-  } else {
-    mbar_wait_bounded(stage_bar(SP, slot), parity, err);
   }
 }
 
-__device__ __forceinline__ bool full_step(uint32_t tile, uint32_t n) {
-  return (uint64_t)(tile + 1) * kStepRows <= n;
+// Rows of step `tile` of a batch of n rows.
+__device__ __forceinline__ uint32_t step_rows(uint32_t tile, uint32_t n) {
+  const uint32_t row0 = tile * kStepRows;
+  return n - row0 < kStepRows ? n - row0 : kStepRows;
 }
 
 __device__ __forceinline__ uint32_t in_range_bits(uint32_t row0, uint32_t n) {
