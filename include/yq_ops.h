@@ -351,8 +351,9 @@ int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descending, int32_t
  *
  * yq_filter_aggregate_segments: WHERE + aggregates per task into
  * states[g] = (char*)states + g * yq_agg_state_bytes(nagg), each initialised
- * by yq_agg_states_init. Task starts must be multiples of 16 rows. Results
- * equal running each task alone (partials fold in a fixed order).
+ * by yq_agg_states_init. Results equal running each task alone up to the
+ * summation order of float SUM/AVG (partials fold in a fixed order, so a
+ * task's result is the same on every run).
  * yq_order_by_segments: ORDER BY per task (segmented radix sort + one gather).
  * With config->keep_trivial set it enqueues device work only and never waits
  * (it can be captured in a CUDA graph); an error is then left as a non-zero

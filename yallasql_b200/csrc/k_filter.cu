@@ -63,6 +63,14 @@ __global__ void k_agg_state_init(Acc* state, const AggParams p) {
   if (a == 0) *agg_state_err(state) = 0u;
 }
 
+// One block per state of a back-to-back array of states.
+__global__ void k_agg_states_init(char* states, const AggParams p) {
+  Acc* st = reinterpret_cast<Acc*>(states + (size_t)blockIdx.x * kAggStateBytes);
+  const int a = threadIdx.x;
+  if (a < YQ_MAX_AGGREGATES) st[a] = Acc{0, acc_identity(a < p.nagg ? p.upd[a] : UPD_COUNT)};
+  if (a == 0) *agg_state_err(st) = 0u;
+}
+
 template <bool STAGED>
 __global__ void __launch_bounds__(kRowBlock, 2) k_filter_aggregate(const __grid_constant__ FAParams F, uint32_t n,
                                                                    Acc* __restrict__ partials, uint32_t* ticket,
@@ -91,6 +99,7 @@ __global__ void __launch_bounds__(kRowBlock, 2) k_filter_aggregate(const __grid_
     X.lr = threadIdx.x * ITEMS;
     X.inr = in_range_bits(X.tile0 + X.lr, n);
     X.stage = 0;
+    X.vec_ok = (X.tile0 & 15u) == 0u;
     if constexpr (STAGED) {
       __syncthreads();  // every thread is done with the previous step: its slot is free
       if (threadIdx.x == 0) {
@@ -222,11 +231,16 @@ __device__ __forceinline__ int seg_of_step(const uint32_t* step0, int nseg, uint
   return lo;
 }
 
+// Step t: task g's rows within the absolute step window of t (windows are
+// kStepRows-aligned, so only a task's first and last steps are partial).
 __device__ __forceinline__ void seg_step(const FASegParams& Q, uint32_t t, uint32_t& row0, uint32_t& rows) {
   const int g = seg_of_step(Q.step0, Q.nseg, t);
-  row0 = __ldg(Q.seg + g) + (t - __ldg(Q.step0 + g)) * kStepRows;
-  const uint32_t end = __ldg(Q.seg + g + 1);
-  rows = end - row0 < kStepRows ? end - row0 : kStepRows;
+  const uint32_t s = __ldg(Q.seg + g), e = __ldg(Q.seg + g + 1);
+  const uint64_t base = ((uint64_t)(s / kStepRows) + (t - __ldg(Q.step0 + g))) * kStepRows;
+  const uint64_t lo = base > s ? base : s;
+  const uint64_t hi = base + kStepRows < e ? base + kStepRows : e;
+  row0 = (uint32_t)lo;
+  rows = (uint32_t)(hi - lo);
 }
 
 template <bool STAGED>
@@ -257,6 +271,7 @@ __global__ void __launch_bounds__(kRowBlock, 2) k_filter_aggregate_seg(const __g
     X.lr = threadIdx.x * ITEMS;
     X.inr = in_range_bits(X.lr, rows);
     X.stage = 0;
+    X.vec_ok = (X.tile0 & 15u) == 0u;
     if constexpr (STAGED) {
       __syncthreads();  // every thread is done with the previous step: its slot is free
       if (threadIdx.x == 0) {
@@ -311,7 +326,7 @@ static uint32_t seg_steps(const uint32_t* seg, int nseg, std::vector<uint32_t>& 
   uint32_t t = 0;
   for (int g = 0; g < nseg; ++g) {
     step0[g] = t;
-    t += ceil_div<uint32_t>(seg[g + 1] - seg[g], kStepRows);
+    if (seg[g + 1] > seg[g]) t += ceil_div<uint32_t>(seg[g + 1], kStepRows) - seg[g] / kStepRows;
   }
   step0[nseg] = t;
   return t;
@@ -452,6 +467,7 @@ __global__ void __launch_bounds__(kRowBlock, 2) k_filter_project(const __grid_co
     X.lr = threadIdx.x * ITEMS;
     X.inr = in_range_bits(X.tile0 + X.lr, n);
     X.stage = 0;
+    X.vec_ok = (X.tile0 & 15u) == 0u;
     if constexpr (STAGED) {
       stage_finish(F.SP, slot, parity, X.tile0, step_rows(tile, n), err);
       X.stage = (uint32_t)slot * F.SP.stage_bytes;
@@ -646,8 +662,14 @@ int yq_agg_state_read(const void* state, const yq_agg_spec* aggs, int32_t nagg, 
 
 int yq_agg_states_init(void* states, int32_t count, const yq_agg_spec* aggs, int32_t nagg, void* stream) {
   if (!states || count < 0) return YQ_ERR_INVALID_ARG;
-  for (int g = 0; g < count; ++g)
-    YQ_TRY(yq_agg_state_init(static_cast<char*>(states) + (size_t)g * kAggStateBytes, aggs, nagg, stream));
+  YQ_TRY(check_aggs(aggs, nagg));
+  if (count == 0) return YQ_OK;
+  AggParams p;
+  memset(&p, 0, sizeof(p));
+  p.nagg = nagg;
+  for (int a = 0; a < YQ_MAX_AGGREGATES; ++a) p.upd[a] = a < nagg ? agg_update_code(aggs[a].kind, aggs[a].input_type) : 0;
+  k_agg_states_init<<<count, 32, 0, as_stream(stream)>>>(static_cast<char*>(states), p);
+  YQ_CHECK_LAUNCH();
   return YQ_OK;
 }
 
@@ -695,7 +717,7 @@ int yq_agg_states_read(const void* states, int32_t count, const yq_agg_spec* agg
 size_t yq_filter_aggregate_segments_workspace_size(uint32_t rows, int32_t nseg) {
   if (nseg < 0) return 0;
   WsSize w;
-  const size_t steps = (size_t)ceil_div<uint32_t>(rows, kStepRows) + (size_t)nseg;
+  const size_t steps = (size_t)ceil_div<uint32_t>(rows, kStepRows) + 2 * (size_t)nseg;
   w.add<uint32_t>((size_t)nseg + 1);
   w.add<uint32_t>((size_t)nseg + 1);
   w.add<Acc>(steps * YQ_MAX_AGGREGATES);
@@ -709,10 +731,8 @@ int yq_filter_aggregate_segments(const yq_batch* batch, const uint32_t* seg_offs
   if (!batch || !states || nseg < 0 || (nseg > 0 && !seg_offsets)) return YQ_ERR_INVALID_ARG;
   if (nseg == 0) return YQ_OK;
   if (seg_offsets[0] != 0 || seg_offsets[nseg] > batch->rows) return YQ_ERR_INVALID_ARG;
-  for (int g = 0; g < nseg; ++g) {
+  for (int g = 0; g < nseg; ++g)
     if (seg_offsets[g + 1] < seg_offsets[g]) return YQ_ERR_INVALID_ARG;
-    if (seg_offsets[g] % 16u) return YQ_ERR_INVALID_ARG;  // task starts on a 16-row boundary
-  }
   FASegParams Q;
   memset(&Q, 0, sizeof(Q));
   YQ_TRY(prepare_filter_aggregate(batch, predicate, constants, aggs, nagg, &Q.F));
@@ -724,7 +744,7 @@ int yq_filter_aggregate_segments(const yq_batch* batch, const uint32_t* seg_offs
   YQ_TRY(ws.acquire(workspace, workspace_bytes, yq_filter_aggregate_segments_workspace_size(batch->rows, nseg), s));
   uint32_t* d_seg = ws.take<uint32_t>((size_t)nseg + 1);
   uint32_t* d_step0 = ws.take<uint32_t>((size_t)nseg + 1);
-  Acc* partials = ws.take<Acc>(((size_t)ceil_div<uint32_t>(batch->rows, kStepRows) + nseg) * YQ_MAX_AGGREGATES);
+  Acc* partials = ws.take<Acc>(((size_t)ceil_div<uint32_t>(batch->rows, kStepRows) + 2 * (size_t)nseg) * YQ_MAX_AGGREGATES);
   uint32_t* d_err = ws.take<uint32_t>(4);
   YQ_TRY(h2d_async(d_seg, seg_offsets, ((size_t)nseg + 1) * sizeof(uint32_t), s));
   YQ_TRY(h2d_async(d_step0, step0.data(), ((size_t)nseg + 1) * sizeof(uint32_t), s));

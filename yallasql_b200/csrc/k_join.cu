@@ -237,6 +237,7 @@ __global__ void __launch_bounds__(kBuildBlock) k_hash_build(const __grid_constan
       X.lr = threadIdx.x * ITEMS;
       X.inr = inr;
       X.stage = 0;
+      X.vec_ok = (base & 15u) == 0u;
       Stack S;
       run_vm<false>(B.P, 0, B.pred_len, X, S, E);
     }
@@ -490,6 +491,7 @@ __global__ void __launch_bounds__(kRowBlock, 2) k_join_aggregate(const __grid_co
     X.lr = threadIdx.x * ITEMS;
     X.inr = in_range_bits(X.tile0 + X.lr, n);
     X.stage = 0;
+    X.vec_ok = (X.tile0 & 15u) == 0u;
     if constexpr (STAGED) {
       __syncthreads();  // every thread is done with the previous step: its slot is free
       if (threadIdx.x == 0) {

@@ -100,9 +100,10 @@ __device__ __forceinline__ void stage_fill(const StagePlan& SP, int slot, uint32
     const StageCopy& c = SP.c[i];
     const uint32_t valid = rows * c.row_bytes, total = kStepRows * c.row_bytes;
     const unsigned char* src = reinterpret_cast<const unsigned char*>(c.src) + (size_t)row0 * c.row_bytes;
+    const bool words = (reinterpret_cast<uintptr_t>(src) & 3u) == 0u;
     for (uint32_t b = threadIdx.x * 4; b < total; b += blockDim.x * 4) {
       uint32_t w = 0;
-      if (b + 4 <= valid) {
+      if (words && b + 4 <= valid) {
         w = *reinterpret_cast<const uint32_t*>(src + b);
       } else {
         for (uint32_t j = 0; j < 4; ++j)
@@ -113,12 +114,18 @@ __device__ __forceinline__ void stage_fill(const StagePlan& SP, int slot, uint32
   }
 }
 
-// Thread 0: start the step of `rows` rows at `row0` in `slot`. A full step is
-// copied by bulk copies; a partial one (the last rows of a batch or of a
-// segment) only completes the slot's barrier phase, and every thread fills
-// it at stage_finish. Either way each use of a slot completes one phase.
+// A step goes through bulk copies when it is full and starts on a 16-row
+// boundary (every column's slice is then 16-byte aligned).
+__device__ __forceinline__ bool step_bulk(uint32_t row0, uint32_t rows) {
+  return rows == kStepRows && (row0 & 15u) == 0u;
+}
+
+// Thread 0: start the step of `rows` rows at `row0` in `slot`. A bulk step is
+// copied by bulk copies; any other (the first or last rows of a batch or of a
+// task) only completes the slot's barrier phase, and every thread fills it at
+// stage_finish. Either way each use of a slot completes one phase.
 __device__ __forceinline__ void stage_start(const StagePlan& SP, int slot, uint32_t row0, uint32_t rows) {
-  if (rows == kStepRows) stage_issue(SP, slot, row0);
+  if (step_bulk(row0, rows)) stage_issue(SP, slot, row0);
   else mbar_arrive(stage_bar(SP, slot));
 }
 
@@ -126,7 +133,7 @@ __device__ __forceinline__ void stage_start(const StagePlan& SP, int slot, uint3
 __device__ __forceinline__ void stage_finish(const StagePlan& SP, int slot, uint32_t parity, uint32_t row0,
                                              uint32_t rows, uint32_t* err) {
   mbar_wait_bounded(stage_bar(SP, slot), parity, err);
-  if (rows < kStepRows) {
+  if (!step_bulk(row0, rows)) {
     stage_fill(SP, slot, row0, rows);
     __syncthreads();
   }

@@ -171,8 +171,9 @@ struct Stack {
 struct Ctx {
   uint32_t tile0;
   uint32_t lr;
-  uint32_t inr;    // rows in range
-  uint32_t stage;  // shared-memory offset of the step's stage (staged kernels)
+  uint32_t inr;     // rows in range
+  uint32_t stage;   // shared-memory offset of the step's stage (staged kernels)
+  uint32_t vec_ok;  // tile0 is a multiple of 16 rows (vector loads of aligned columns allowed)
 };
 
 // ----------------------------------------------------------- stack moves
@@ -224,7 +225,7 @@ __device__ __forceinline__ uint32_t null_bits(const DevCol& c, const Ctx& X) {
     return nonzero_bytes(w) & X.inr;
   } else {
     const uint8_t* p = c.nulls + X.tile0 + X.lr;
-    if (X.inr == kItemsMask && c.nvec) return nonzero_bytes(__ldg(reinterpret_cast<const uint32_t*>(p)));
+    if (X.inr == kItemsMask && c.nvec && X.vec_ok) return nonzero_bytes(__ldg(reinterpret_cast<const uint32_t*>(p)));
     uint32_t nb = 0;
 #pragma unroll
     for (int k = 0; k < ITEMS; ++k)
@@ -242,7 +243,7 @@ __device__ __forceinline__ void load_raw(const DevCol& c, const Ctx& X, uint64_t
       v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
     } else {
       const char* p = c.data + (size_t)(X.tile0 + X.lr) * 4;
-      if (X.inr == kItemsMask && c.vec) {
+      if (X.inr == kItemsMask && c.vec && X.vec_ok) {
         const uint4 q = ldg_nc_v4(p);
         v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
       } else {
@@ -259,7 +260,7 @@ __device__ __forceinline__ void load_raw(const DevCol& c, const Ctx& X, uint64_t
       q1 = *reinterpret_cast<const uint4*>(p + 16);
     } else {
       const char* p = c.data + (size_t)(X.tile0 + X.lr) * 8;
-      if (X.inr == kItemsMask && c.vec) {
+      if (X.inr == kItemsMask && c.vec && X.vec_ok) {
         q0 = ldg_nc_v4(p);
         q1 = ldg_nc_v4(p + 16);
       } else {
@@ -279,7 +280,7 @@ __device__ __forceinline__ void load_raw(const DevCol& c, const Ctx& X, uint64_t
       w = *reinterpret_cast<const uint32_t*>(yq_dyn_smem + X.stage + c.soff + X.lr);
     } else {
       const uint8_t* p = reinterpret_cast<const uint8_t*>(c.data) + X.tile0 + X.lr;
-      if (X.inr == kItemsMask && c.vec) {
+      if (X.inr == kItemsMask && c.vec && X.vec_ok) {
         w = __ldg(reinterpret_cast<const uint32_t*>(p));
       } else {
 #pragma unroll
@@ -599,7 +600,7 @@ __device__ __forceinline__ void text_cmp_cc(const VmProgram& P, const DevCol& c,
       const uint32_t* p = text_slot<STAGED>(c, X, k);
       uint4 q;
       if constexpr (STAGED) q = *reinterpret_cast<const uint4*>(p);
-      else if (c.vec) q = ldg_nc_v4(p);
+      else if (c.vec && X.vec_ok) q = ldg_nc_v4(p);
       else q = make_uint4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3));
       const bool eq = ((q.x ^ r0) | (q.y ^ r1) | (q.z ^ r2) | (q.w ^ r3)) == 0u;
       m |= (uint32_t)(R == YQ_EQ ? eq : !eq) << k;

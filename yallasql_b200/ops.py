@@ -145,6 +145,55 @@ class AggPlan:
                "yq_filter_aggregate")
 
 
+    def run_segments(self, batch: DeviceBatch, seg_offsets, states: "AggStates", stream=None,
+                     workspace: torch.Tensor | None = None):
+        """One launch for many tasks: task g = rows [seg_offsets[g], seg_offsets[g+1])."""
+        b, keep = batch.c()
+        offs = seg_offsets if isinstance(seg_offsets, C.Array) else (C.c_uint32 * len(seg_offsets))(*seg_offsets)
+        ws = workspace.data_ptr() if workspace is not None else None
+        wsb = workspace.numel() if workspace is not None else 0
+        _check(lib().yq_filter_aggregate_segments(C.byref(b), offs, len(offs) - 1, C.byref(self.pred.prog),
+                                                  C.byref(self.consts), self.specs, len(self.aggs),
+                                                  states.buf.data_ptr(), ws, wsb, _stream(stream)),
+               "yq_filter_aggregate_segments")
+
+
+class AggStates:
+    """`count` aggregate states back to back (one per task of a batched call)."""
+
+    def __init__(self, aggs: list[Aggregate], count: int, stream=None):
+        self.aggs, self.count = aggs, count
+        self.step = int(lib().yq_agg_state_bytes(len(aggs)))
+        self.buf = torch.empty(max(1, count) * self.step, dtype=torch.uint8, device="cuda")
+        self._specs = _agg_specs_stub(aggs)
+        self.reset(stream)
+
+    def reset(self, stream=None):
+        _check(lib().yq_agg_states_init(self.buf.data_ptr(), self.count, self._specs, len(self.aggs),
+                                        _stream(stream)), "yq_agg_states_init")
+
+    def read(self, stream=None) -> list:
+        n = len(self.aggs)
+        out = (A.AggResult * max(1, self.count * n))()
+        _check(lib().yq_agg_states_read(self.buf.data_ptr(), self.count, self._specs, n, out, _stream(stream)),
+               "yq_agg_states_read")
+        res = []
+        for g in range(self.count):
+            vals = []
+            for i, a in enumerate(self.aggs):
+                r = out[g * n + i]
+                if r.is_null:
+                    vals.append(None)
+                elif a.kind in (A.AGG_COUNT, A.AGG_COUNT_STAR):
+                    vals.append(int(r.i))
+                elif a.kind == A.AGG_AVG or a.input_type in (A.FLOAT32, A.FLOAT64):
+                    vals.append(float(r.f))
+                else:
+                    vals.append(int(r.i))
+            res.append(vals)
+        return res
+
+
 def filter_aggregate(batch: DeviceBatch, predicate: Expr | None, aggs: list[Aggregate], stream=None) -> list:
     plan = AggPlan([c.type for c in batch.columns], predicate, aggs)
     st = AggState(aggs, stream)
@@ -434,3 +483,34 @@ def order_by(batch: DeviceBatch, key: int, descending: bool, offsets: list[int],
     _check(lib().yq_order_by(C.byref(ib), key, int(descending), int(nulls_first), offs, len(offsets) - 1,
                              C.byref(ob), None, 0, _stream(stream)), "yq_order_by")
     return out
+
+
+def order_by_segments_workspace_bytes(col: DeviceColumn, offsets) -> int:
+    offs = (C.c_uint32 * len(offsets))(*offsets)
+    cc = col.c()
+    return int(lib().yq_order_by_segments_workspace_size(C.byref(cc), col.rows, offs, len(offsets) - 1))
+
+
+def order_by_segments(batch: DeviceBatch, key: int, descending: bool, offsets, out: DeviceBatch, config=None,
+                      workspace: torch.Tensor | None = None, nulls_first=False, stream=None) -> DeviceBatch:
+    """ORDER BY per task: task g = rows [offsets[g], offsets[g+1]) (yq_order_by_segments)."""
+    offs = offsets if isinstance(offsets, C.Array) else (C.c_uint32 * len(offsets))(*offsets)
+    ib, _ia = batch.c()
+    ob, _oa = out.c()
+    ws = workspace.data_ptr() if workspace is not None else None
+    wsb = workspace.numel() if workspace is not None else 0
+    _check(lib().yq_order_by_segments(C.byref(ib), key, int(descending), int(nulls_first), offs, len(offs) - 1,
+                                      C.byref(ob), C.byref(config) if config is not None else None, ws, wsb,
+                                      _stream(stream)), "yq_order_by_segments")
+    return out
+
+
+def sort_autotune(col: DeviceColumn, offsets, descending=False, stream=None) -> "A.SortConfig":
+    """Time every sort variant on this key and segments; the winner is remembered
+    for this key width and segment size and returned."""
+    offs = (C.c_uint32 * len(offsets))(*offsets)
+    cc = col.c()
+    best = A.SortConfig()
+    _check(lib().yq_sort_autotune(C.byref(cc), col.rows, offs, len(offsets) - 1, int(descending), C.byref(best),
+                                  _stream(stream)), "yq_sort_autotune")
+    return best
