@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-ops", action="store_true", help="skip the other operators' workloads")
+    p.add_argument("--no-batched", action="store_true", help="skip the batched-form comparison")
+    p.add_argument("--batched-tasks", type=int, default=512)
     return p.parse_args()
 
 
@@ -281,6 +283,38 @@ def operator_suite(lib, peak: float) -> dict:
     return out
 
 
+def batched_form(args) -> dict:
+    """Batched form (512 tasks, row counts log-uniform in [1K, 4M], seed 3):
+    the plain per-task form against the segmented launches replayed as one CUDA
+    graph, on the same GPU and data; tasks/s from device time around each form."""
+    import torch
+    from yallasql_b200 import batched
+    ntasks = args.batched_tasks
+    rows = batched.task_rows(ntasks, seed=3)
+    ts = batched.TaskSet(rows, seed=3, on_device=True)
+    plain = batched.PlainRunner(ts)
+    t0 = time.perf_counter()
+    pipe = batched.BatchedPipeline(ts, graph=True)
+    setup_s = time.perf_counter() - t0
+    plain_ms = _timed(plain.run, 2)
+    batched_ms = _timed(pipe.run, 3)
+    torch.cuda.synchronize()
+    same_sorted = all(torch.equal(ts.sout.columns[c].data[a:b], ts.souts[g].columns[c].data)
+                      for g, (a, b) in enumerate(zip(ts.soffs[:-1], ts.soffs[1:])) for c in range(6))
+    pres, bres = plain.results(), pipe.results()
+    same_aggs = all(p[1:] == q[1:] and abs(p[0] - q[0]) <= 1e-6 * max(1.0, abs(p[0])) if p[1] else p == q
+                    for p, q in zip(pres, bres))
+    total_rows = int(sum(rows))
+    return {"tasks": ntasks, "rows": total_rows, "filter_tasks": len(ts.frows), "order_by_tasks": len(ts.srows),
+            "plain_ms": round(plain_ms, 3), "batched_ms": round(batched_ms, 3),
+            "plain_tasks_per_s": ntasks / (plain_ms / 1e3), "batched_tasks_per_s": ntasks / (batched_ms / 1e3),
+            "speedup": round(plain_ms / batched_ms, 3),
+            "batched_algorithmic_gbs": round(ts.algorithmic_bytes / (batched_ms / 1e3) / 1e9, 1),
+            "sort_autotuned": {"digit_bits": pipe.tuned[0], "items_per_thread": pipe.tuned[1]},
+            "graph": True, "setup_s": round(setup_s, 2), "results_equal_plain": bool(same_sorted and same_aggs),
+            "error_word": pipe.error_word()}
+
+
 def run_reference(args, rank: int):
     """Reference arm: the CPU port of the operator (oracle/ stable ORDER BY +
     row gather), all host threads, a bounded sample per step."""
@@ -456,6 +490,9 @@ def main():
         del job
         torch.cuda.empty_cache()
         line["operators"] = operator_suite(lib, peak)
+    if rank == 0 and not args.no_batched:
+        torch.cuda.empty_cache()
+        line["batched"] = batched_form(args)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args, t)
     if rank == 0:
