@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--no-ops", action="store_true", help="skip the other operators' workloads")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-form comparison")
     p.add_argument("--batched-tasks", type=int, default=512)
+    p.add_argument("--no-serving", action="store_true", help="skip the serving-form comparison")
+    p.add_argument("--serving-requests", type=int, default=400)
     return p.parse_args()
 
 
@@ -315,6 +317,37 @@ def batched_form(args) -> dict:
             "error_word": pipe.error_word()}
 
 
+def serving_form(args) -> dict:
+    """Serving form (seed 4): 40/30/20/10 filter / ORDER BY / join / scalar
+    subquery mix over resident tables of 10K-60M rows. Saturation throughput of
+    the plain form (one request at a time) and the continuous form (streams,
+    budgeted admission, co-launched filters), then both at the same Poisson
+    arrival rate (70% of the plain form's saturation) with p50/p99 latency."""
+    import copy
+    import torch
+    from yallasql_b200 import serving
+    cat = serving.Catalog(ntables=8, lo=10_000, hi=60_000_000, seed=4)
+    plans = serving.Plans()
+    n = args.serving_requests
+    warm = serving.make_trace(40, 0.0, cat, seed=5)
+    serving.serve_plain(copy.deepcopy(warm), cat, plans)
+    serving.serve_continuous(copy.deepcopy(warm), cat, plans)
+    burst = serving.make_trace(n, 0.0, cat, seed=4)
+    plain_sat = serving.serve_plain(copy.deepcopy(burst), cat, plans)
+    cont_sat = serving.serve_continuous(copy.deepcopy(burst), cat, plans, slots=8, budget=40e9)
+    rate = 0.7 * plain_sat["queries_per_s"]
+    trace = serving.make_trace(n, rate, cat, seed=4)
+    plain_open = serving.serve_plain(copy.deepcopy(trace), cat, plans)
+    cont_open = serving.serve_continuous(copy.deepcopy(trace), cat, plans, slots=8, budget=40e9)
+    torch.cuda.synchronize()
+    r = lambda d: {k: (round(v, 3) if isinstance(v, float) else v) for k, v in d.items()}
+    return {"requests": n, "mix": dict(zip(serving.CLASSES, serving.MIX)), "table_rows": "log-uniform 10K-60M",
+            "budget_gb": 40, "slots": 8,
+            "saturation": {"plain": r(plain_sat), "continuous": r(cont_sat),
+                           "throughput_ratio": round(cont_sat["queries_per_s"] / plain_sat["queries_per_s"], 3)},
+            "open_loop": {"arrival_rate_per_s": round(rate, 1), "plain": r(plain_open), "continuous": r(cont_open)}}
+
+
 def run_reference(args, rank: int):
     """Reference arm: the CPU port of the operator (oracle/ stable ORDER BY +
     row gather), all host threads, a bounded sample per step."""
@@ -493,6 +526,9 @@ def main():
     if rank == 0 and not args.no_batched:
         torch.cuda.empty_cache()
         line["batched"] = batched_form(args)
+    if rank == 0 and not args.no_serving:
+        torch.cuda.empty_cache()
+        line["serving"] = serving_form(args)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args, t)
     if rank == 0:

@@ -370,6 +370,14 @@ int yq_filter_aggregate_segments(const yq_batch* batch, const uint32_t* seg_offs
                                  const yq_program* predicate, const yq_constants* constants,
                                  const yq_agg_spec* aggs, int32_t nagg, void* states, void* workspace,
                                  size_t workspace_bytes, void* stream);
+/* Same as yq_filter_aggregate_segments for tasks given as row ranges
+ * [begin[g], end[g]) of the batch: ranges may leave gaps, repeat or overlap
+ * (a serving loop co-launches pending queries over resident tables). */
+size_t yq_filter_aggregate_ranges_workspace_size(const uint32_t* begin, const uint32_t* end, int32_t nseg);
+int yq_filter_aggregate_ranges(const yq_batch* batch, const uint32_t* begin, const uint32_t* end, int32_t nseg,
+                               const yq_program* predicate, const yq_constants* constants,
+                               const yq_agg_spec* aggs, int32_t nagg, void* states, void* workspace,
+                               size_t workspace_bytes, void* stream);
 size_t yq_order_by_segments_workspace_size(const yq_column* key, uint32_t rows, const uint32_t* seg_offsets,
                                            int32_t nseg);
 int yq_order_by_segments(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,

@@ -121,6 +121,9 @@ PROTOTYPES = {
     "yq_filter_aggregate_segments_workspace_size": (sz, [u32, i32]),
     "yq_filter_aggregate_segments": (C.c_int, [P(Batch), P(u32), i32, P(Program), P(Constants), P(AggSpec), i32,
                                                 vp, vp, sz, vp]),
+    "yq_filter_aggregate_ranges_workspace_size": (sz, [P(u32), P(u32), i32]),
+    "yq_filter_aggregate_ranges": (C.c_int, [P(Batch), P(u32), P(u32), i32, P(Program), P(Constants), P(AggSpec),
+                                              i32, vp, vp, sz, vp]),
     "yq_order_by_segments_workspace_size": (sz, [P(Column), u32, P(u32), i32]),
     "yq_order_by_segments": (C.c_int, [P(Batch), i32, i32, i32, P(u32), i32, P(Batch), P(SortConfig), vp, sz, vp]),
     "yq_sort_autotune": (C.c_int, [P(Column), u32, P(u32), i32, i32, P(SortConfig), vp]),

@@ -213,7 +213,8 @@ static int launch_filter_aggregate(const FAParams& F, uint32_t rows, Acc* partia
 // running it alone.
 struct FASegParams {
   FAParams F;
-  const uint32_t* seg;    // [nseg + 1] row offsets
+  const uint32_t* seg;    // [nseg] first row of each task
+  const uint32_t* seg_end;  // [nseg] end row of each task
   const uint32_t* step0;  // [nseg + 1] first step of each task
   int32_t nseg;
   uint32_t nsteps;
@@ -235,7 +236,7 @@ __device__ __forceinline__ int seg_of_step(const uint32_t* step0, int nseg, uint
 // kStepRows-aligned, so only a task's first and last steps are partial).
 __device__ __forceinline__ void seg_step(const FASegParams& Q, uint32_t t, uint32_t& row0, uint32_t& rows) {
   const int g = seg_of_step(Q.step0, Q.nseg, t);
-  const uint32_t s = __ldg(Q.seg + g), e = __ldg(Q.seg + g + 1);
+  const uint32_t s = __ldg(Q.seg + g), e = __ldg(Q.seg_end + g);
   const uint64_t base = ((uint64_t)(s / kStepRows) + (t - __ldg(Q.step0 + g))) * kStepRows;
   const uint64_t lo = base > s ? base : s;
   const uint64_t hi = base + kStepRows < e ? base + kStepRows : e;
@@ -321,12 +322,12 @@ __global__ void k_agg_seg_fold(const Acc* __restrict__ partials, const uint32_t*
   st[a] = cur;
 }
 
-static uint32_t seg_steps(const uint32_t* seg, int nseg, std::vector<uint32_t>& step0) {
+static uint32_t seg_steps(const uint32_t* begin, const uint32_t* end, int nseg, std::vector<uint32_t>& step0) {
   step0.resize((size_t)nseg + 1);
   uint32_t t = 0;
   for (int g = 0; g < nseg; ++g) {
     step0[g] = t;
-    if (seg[g + 1] > seg[g]) t += ceil_div<uint32_t>(seg[g + 1], kStepRows) - seg[g] / kStepRows;
+    if (end[g] > begin[g]) t += ceil_div<uint32_t>(end[g], kStepRows) - begin[g] / kStepRows;
   }
   step0[nseg] = t;
   return t;
@@ -714,42 +715,51 @@ int yq_agg_states_read(const void* states, int32_t count, const yq_agg_spec* agg
   return status;
 }
 
-size_t yq_filter_aggregate_segments_workspace_size(uint32_t rows, int32_t nseg) {
-  if (nseg < 0) return 0;
+// Steps of nseg ranges: at most one per kStepRows window a range touches.
+static size_t ranges_steps_bound(const uint32_t* begin, const uint32_t* end, int nseg) {
+  size_t t = 0;
+  for (int g = 0; g < nseg; ++g)
+    if (end[g] > begin[g]) t += ceil_div<uint32_t>(end[g], kStepRows) - begin[g] / kStepRows;
+  return t;
+}
+
+static size_t ranges_ws(size_t steps, int nseg) {
   WsSize w;
-  const size_t steps = (size_t)ceil_div<uint32_t>(rows, kStepRows) + 2 * (size_t)nseg;
   w.add<uint32_t>((size_t)nseg + 1);
   w.add<uint32_t>((size_t)nseg + 1);
-  w.add<Acc>(steps * YQ_MAX_AGGREGATES);
+  w.add<uint32_t>((size_t)nseg + 1);
+  w.add<Acc>((steps ? steps : 1) * YQ_MAX_AGGREGATES);
   w.add<uint32_t>(4);
   return w.total();
 }
 
-int yq_filter_aggregate_segments(const yq_batch* batch, const uint32_t* seg_offsets, int32_t nseg,
-                                 const yq_program* predicate, const yq_constants* constants, const yq_agg_spec* aggs,
-                                 int32_t nagg, void* states, void* workspace, size_t workspace_bytes, void* stream) {
-  if (!batch || !states || nseg < 0 || (nseg > 0 && !seg_offsets)) return YQ_ERR_INVALID_ARG;
+static int filter_aggregate_ranges(const yq_batch* batch, const uint32_t* begin, const uint32_t* end, int32_t nseg,
+                                   const yq_program* predicate, const yq_constants* constants,
+                                   const yq_agg_spec* aggs, int32_t nagg, void* states, void* workspace,
+                                   size_t workspace_bytes, cudaStream_t s) {
+  if (!batch || !states || nseg < 0 || (nseg > 0 && (!begin || !end))) return YQ_ERR_INVALID_ARG;
   if (nseg == 0) return YQ_OK;
-  if (seg_offsets[0] != 0 || seg_offsets[nseg] > batch->rows) return YQ_ERR_INVALID_ARG;
   for (int g = 0; g < nseg; ++g)
-    if (seg_offsets[g + 1] < seg_offsets[g]) return YQ_ERR_INVALID_ARG;
+    if (end[g] < begin[g] || end[g] > batch->rows) return YQ_ERR_INVALID_ARG;
   FASegParams Q;
   memset(&Q, 0, sizeof(Q));
   YQ_TRY(prepare_filter_aggregate(batch, predicate, constants, aggs, nagg, &Q.F));
   if (nagg == 0) return YQ_OK;
   std::vector<uint32_t> step0;
-  const uint32_t nsteps = seg_steps(seg_offsets, nseg, step0);
-  cudaStream_t s = as_stream(stream);
+  const uint32_t nsteps = seg_steps(begin, end, nseg, step0);
   Workspace ws;
-  YQ_TRY(ws.acquire(workspace, workspace_bytes, yq_filter_aggregate_segments_workspace_size(batch->rows, nseg), s));
-  uint32_t* d_seg = ws.take<uint32_t>((size_t)nseg + 1);
+  YQ_TRY(ws.acquire(workspace, workspace_bytes, ranges_ws(nsteps, nseg), s));
+  uint32_t* d_begin = ws.take<uint32_t>((size_t)nseg + 1);
+  uint32_t* d_end = ws.take<uint32_t>((size_t)nseg + 1);
   uint32_t* d_step0 = ws.take<uint32_t>((size_t)nseg + 1);
-  Acc* partials = ws.take<Acc>(((size_t)ceil_div<uint32_t>(batch->rows, kStepRows) + 2 * (size_t)nseg) * YQ_MAX_AGGREGATES);
+  Acc* partials = ws.take<Acc>((nsteps ? nsteps : 1) * (size_t)YQ_MAX_AGGREGATES);
   uint32_t* d_err = ws.take<uint32_t>(4);
-  YQ_TRY(h2d_async(d_seg, seg_offsets, ((size_t)nseg + 1) * sizeof(uint32_t), s));
+  YQ_TRY(h2d_async(d_begin, begin, (size_t)nseg * sizeof(uint32_t), s));
+  YQ_TRY(h2d_async(d_end, end, (size_t)nseg * sizeof(uint32_t), s));
   YQ_TRY(h2d_async(d_step0, step0.data(), ((size_t)nseg + 1) * sizeof(uint32_t), s));
   YQ_TRY_CUDA(cudaMemsetAsync(d_err, 0, 4 * sizeof(uint32_t), s));
-  Q.seg = d_seg;
+  Q.seg = d_begin;
+  Q.seg_end = d_end;
   Q.step0 = d_step0;
   Q.nseg = nseg;
   Q.nsteps = nsteps;
@@ -764,8 +774,9 @@ int yq_filter_aggregate_segments(const yq_batch* batch, const uint32_t* seg_offs
     YQ_TRY(allow_smem(kern, smem, done_smem));
     static GridCache gc[2];
     const int grid = gc[staged ? 1 : 0].grid(kern, smem, nsteps);
-    ProfScope ps("filter_aggregate_seg", s,
-                 (double)seg_offsets[nseg] * row_bytes_of(Q.F.P, program_columns(Q.F.P, Q.F.pc_end, 0)));
+    double rows = 0;
+    for (int g = 0; g < nseg; ++g) rows += end[g] - begin[g];
+    ProfScope ps("filter_aggregate_seg", s, rows * row_bytes_of(Q.F.P, program_columns(Q.F.P, Q.F.pc_end, 0)));
     if (staged)
       k_filter_aggregate_seg<true><<<grid, kRowBlock, smem, s>>>(Q);
     else
@@ -775,6 +786,34 @@ int yq_filter_aggregate_segments(const yq_batch* batch, const uint32_t* seg_offs
   k_agg_seg_fold<<<nseg, 32, 0, s>>>(partials, d_step0, nseg, Q.F.A, static_cast<Acc*>(states), d_err);
   YQ_CHECK_LAUNCH();
   return YQ_OK;
+}
+
+size_t yq_filter_aggregate_segments_workspace_size(uint32_t rows, int32_t nseg) {
+  if (nseg < 0) return 0;
+  // every range touches at most one window more than its rows fill
+  return ranges_ws((size_t)ceil_div<uint32_t>(rows, kStepRows) + (size_t)nseg, nseg);
+}
+
+int yq_filter_aggregate_segments(const yq_batch* batch, const uint32_t* seg_offsets, int32_t nseg,
+                                 const yq_program* predicate, const yq_constants* constants, const yq_agg_spec* aggs,
+                                 int32_t nagg, void* states, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!batch || nseg < 0 || (nseg > 0 && !seg_offsets)) return YQ_ERR_INVALID_ARG;
+  if (nseg == 0) return YQ_OK;
+  if (seg_offsets[0] != 0) return YQ_ERR_INVALID_ARG;
+  return filter_aggregate_ranges(batch, seg_offsets, seg_offsets + 1, nseg, predicate, constants, aggs, nagg, states,
+                                 workspace, workspace_bytes, as_stream(stream));
+}
+
+size_t yq_filter_aggregate_ranges_workspace_size(const uint32_t* begin, const uint32_t* end, int32_t nseg) {
+  if (nseg < 0 || (nseg > 0 && (!begin || !end))) return 0;
+  return ranges_ws(ranges_steps_bound(begin, end, nseg), nseg);
+}
+
+int yq_filter_aggregate_ranges(const yq_batch* batch, const uint32_t* begin, const uint32_t* end, int32_t nseg,
+                               const yq_program* predicate, const yq_constants* constants, const yq_agg_spec* aggs,
+                               int32_t nagg, void* states, void* workspace, size_t workspace_bytes, void* stream) {
+  return filter_aggregate_ranges(batch, begin, end, nseg, predicate, constants, aggs, nagg, states, workspace,
+                                 workspace_bytes, as_stream(stream));
 }
 
 size_t yq_filter_project_workspace_size(uint32_t rows) {

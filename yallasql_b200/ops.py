@@ -23,6 +23,9 @@ def lib():
 
 
 def _stream(stream=None) -> int:
+    """Raw cudaStream_t of a torch stream, a raw handle, or the current stream."""
+    if isinstance(stream, int):
+        return stream
     s = stream if stream is not None else torch.cuda.current_stream()
     return int(s.cuda_stream)
 
@@ -156,6 +159,19 @@ class AggPlan:
                                                   C.byref(self.consts), self.specs, len(self.aggs),
                                                   states.buf.data_ptr(), ws, wsb, _stream(stream)),
                "yq_filter_aggregate_segments")
+
+
+    def run_ranges(self, batch: DeviceBatch, begin: list, end: list, states: "AggStates", stream=None,
+                   workspace: torch.Tensor | None = None):
+        """One launch for tasks given as row ranges [begin[g], end[g]) of the batch."""
+        b, keep = batch.c()
+        n = len(begin)
+        cb, ce = (C.c_uint32 * n)(*begin), (C.c_uint32 * n)(*end)
+        ws = workspace.data_ptr() if workspace is not None else None
+        wsb = workspace.numel() if workspace is not None else 0
+        _check(lib().yq_filter_aggregate_ranges(C.byref(b), cb, ce, n, C.byref(self.pred.prog), C.byref(self.consts),
+                                                self.specs, len(self.aggs), states.buf.data_ptr(), ws, wsb,
+                                                _stream(stream)), "yq_filter_aggregate_ranges")
 
 
 class AggStates:
