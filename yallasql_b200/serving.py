@@ -190,6 +190,7 @@ class OrderJob(Job):
 
     def launch(self, stream):
         n = self.tbl.rows
+        self.stream = stream
         with torch.cuda.stream(stream):
             self.out = ops.DeviceBatch([ops.DeviceColumn.empty(t, n, w if t == A.TEXT else None)
                                         for t, w in zip(ORDER_TYPES, ORDER_WIDTHS)])
@@ -200,7 +201,8 @@ class OrderJob(Job):
             self.event.record(stream)
 
     def finish(self):
-        err = int(self.ws[:4].view(torch.int32)[0].item())
+        with torch.cuda.stream(self.stream):
+            err = int(self.ws[:4].view(torch.int32)[0].item())
         if err:
             raise RuntimeError(f"ORDER BY request {self.reqs[0].rid}: device error word {err}")
         self.reqs[0].result = self.out if self.keep else ("ok", self.tbl.rows)
@@ -267,25 +269,27 @@ class SubqueryRows(Job):
             And(eq, Compare(A.NE, ColumnRef(1, A.INT32), ColumnRef(1, A.INT32)))
         self.plan = ops.ProjectPlan(SALES_TYPES, [4, 4, 4, 16], pred, [p.revenue, 1])
         n = max(1, self.tbl.rows)
+        self.stream = stream
         with torch.cuda.stream(stream):
             self.outs = [ops.DeviceColumn.empty(A.FLOAT32, n), ops.DeviceColumn.empty(A.INT32, n)]
             self.cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
             oc = (A.Column * 2)(*[o.c() for o in self.outs])
             b, keep = self.tbl.c()
             self._keep = (oc, b, keep)
+            cnt_ptr = C.cast(C.c_void_p(self.cnt.data_ptr()), C.POINTER(C.c_uint32))
             st = ops.lib().yq_filter_project(C.byref(b), C.byref(self.plan.pred.prog), C.byref(self.plan.consts),
-                                             self.plan.proj, 2, oc, n, self.cnt.data_ptr(), None, None, 0,
-                                             stream.cuda_stream)
+                                             self.plan.proj, 2, oc, n, cnt_ptr, None, None, 0, stream.cuda_stream)
             ops._check(st, "yq_filter_project")
             self.event = torch.cuda.Event()
             self.event.record(stream)
 
     def finish(self):
-        n = int(self.cnt.item())
-        if self.first.keep:
-            self.reqs[0].result = (n, self.outs[0].data[:n].clone(), self.outs[1].data[:n].clone())
-        else:
-            self.reqs[0].result = (n,)
+        with torch.cuda.stream(self.stream):
+            n = int(self.cnt.item())
+            if self.first.keep:
+                self.reqs[0].result = (n, self.outs[0].data[:n].clone(), self.outs[1].data[:n].clone())
+            else:
+                self.reqs[0].result = (n,)
         self.outs = None
 
 
