@@ -121,7 +121,8 @@ def peaks() -> tuple[float, str]:
 
 
 def committed_traffic() -> dict:
-    """Per-launch DRAM bytes of the profiled kernels, from the committed ncu summary."""
+    """DRAM bytes and algorithmic bytes of one ncu-captured launch per kernel tag
+    (profiles/traffic.json, written from the committed ncu summaries)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(p) as f:
@@ -507,8 +508,9 @@ def main():
         achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
         tr = committed_traffic().get(name, {})
         traffic = None
-        if tr.get("dram_bytes_per_unit_row") is not None and tr.get("rows_per_launch_units"):
-            traffic = tr["dram_bytes_per_unit_row"] * per_launch_bytes / tr["rows_per_launch_units"]
+        if tr.get("dram_bytes") and tr.get("algorithmic_bytes"):
+            # ncu capture of a smaller case of the same kernel, scaled by the units this launch processes
+            traffic = round(tr["dram_bytes"] / tr["algorithmic_bytes"] * per_launch_bytes)
         roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6650 GB/s",
