@@ -93,7 +93,7 @@ def test_merge_pass_types(cuda, nruns, kind):
 
 @pytest.mark.parametrize("nruns", [1, 2, 5, 16])
 @pytest.mark.parametrize("kind", ["f32", "i32", "i64", "date", "f64", "text16", "text32", "f32_nulls", "bool",
-                                  "equal"])
+                                  "equal", "f32_special", "bool_bytes"])
 @pytest.mark.parametrize("desc,nulls_first", [(False, False), (True, False), (True, True)])
 def test_order_by_entry_matches_stable_sort(cuda, nruns, kind, desc, nulls_first):
     """yq_order_by over runs of random sizes (empty runs included): every column
@@ -128,6 +128,16 @@ def test_order_by_entry_matches_stable_sort(cuda, nruns, kind, desc, nulls_first
         nulls = rng.random(n) < 0.2
     elif kind == "bool":
         k, t = (rng.random(n) < 0.5).astype(np.uint8), A.BOOL
+    elif kind == "f32_special":
+        # -0.0 ties +0.0 and NaNs sort last: the key column must still come out bit for bit
+        k = rng.choice(np.array([0.0, -0.0, 1.5, -2.5], np.float32), n)
+        bits = k.view(np.uint32)
+        bits[rng.random(n) < 0.05] = 0x7fc00000
+        bits[rng.random(n) < 0.05] = 0x7f800001
+        bits[rng.random(n) < 0.05] = 0xffc00000
+        t = A.FLOAT32
+    elif kind == "bool_bytes":
+        k, t = rng.integers(0, 4, n).astype(np.uint8), A.BOOL
     else:
         k, t = np.full(n, 3.5, np.float32), A.FLOAT32
     payload = np.arange(n, dtype=np.int64)
@@ -136,7 +146,8 @@ def test_order_by_entry_matches_stable_sort(cuda, nruns, kind, desc, nulls_first
     out = ops.order_by(b, 0, desc, offs, nulls_first=nulls_first)
     perm = oracle.sort_perm(k, desc=desc, nulls=nulls, nulls_first=nulls_first, type_=ty)
     np.testing.assert_array_equal(out.columns[1].data.cpu().numpy(), payload[perm])
-    np.testing.assert_array_equal(out.columns[0].data.cpu().numpy(), k[perm])
+    got = out.columns[0].data.cpu().numpy()
+    np.testing.assert_array_equal(got.view(np.uint8), k[perm].view(np.uint8))  # bit for bit
     np.testing.assert_array_equal(out.columns[2].data.cpu().numpy(), txt[perm])
     if nulls is not None:
         np.testing.assert_array_equal(out.columns[0].nulls.cpu().numpy().astype(bool), nulls[perm])

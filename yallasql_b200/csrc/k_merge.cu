@@ -348,10 +348,21 @@ struct RawTile {
   uint32_t a_row, na, b_row, nb, out0, cnt, pad0, pad1;
 };
 
+// Decoding of key words back into the key column's values (the last level
+// writes the sorted key column itself instead of its words).
+struct KeyDecode {
+  char* out;        // null: no decode
+  int32_t type;
+  int32_t vwords;   // value words (text: significant slot words)
+  int32_t width;    // slot width (text)
+  int32_t desc;
+};
+
 struct RawLevel {
   const uint32_t* keys_in;  // [rows][KW] words
   const uint32_t* ids_in;   // [rows]
   uint32_t* keys_out;       // null: the level writes row ids only
+  KeyDecode dec;
   uint32_t* ids_out;
   const RawPair* pairs;
   int32_t npairs;
@@ -510,6 +521,42 @@ __device__ __forceinline__ void raw_key_store(uint32_t* out, size_t row, const u
   }
 }
 
+// Inverse of make_key_ptr for a key without nulls (exact when the column holds
+// no -0.0, non-canonical NaN or bool byte other than 0/1: see k_key_lossy).
+template <int KW>
+__device__ __forceinline__ void decode_store(const KeyDecode& d, size_t row, const uint32_t (&k0)[KW]) {
+  uint32_t k[KW];
+#pragma unroll
+  for (int j = 0; j < KW; ++j) k[j] = (d.desc && j < d.vwords) ? ~k0[j] : k0[j];
+  switch (d.type) {
+    case YQ_INT32: reinterpret_cast<uint32_t*>(d.out)[row] = k[0] ^ 0x80000000u; break;
+    case YQ_FLOAT32: reinterpret_cast<uint32_t*>(d.out)[row] = (k[0] & 0x80000000u) ? (k[0] & 0x7fffffffu) : ~k[0]; break;
+    case YQ_BOOL: reinterpret_cast<uint8_t*>(d.out)[row] = (uint8_t)(k[0] & 1u); break;
+    case YQ_INT64:
+    case YQ_DATETIME:
+      if constexpr (KW >= 2)
+        reinterpret_cast<uint2*>(d.out)[row] = make_uint2(k[0], k[1] ^ 0x80000000u);
+      break;
+    case YQ_FLOAT64:
+      if constexpr (KW >= 2) {
+        unsigned long long b = ((unsigned long long)k[1] << 32) | k[0];
+        b = (b & 0x8000000000000000ull) ? (b & 0x7fffffffffffffffull) : ~b;
+        reinterpret_cast<unsigned long long*>(d.out)[row] = b;
+      }
+      break;
+    default: {  // TEXT: word i of the slot = bswap(k[vwords - 1 - i]); later words are zero
+      uint32_t* w = reinterpret_cast<uint32_t*>(d.out + row * (size_t)d.width);
+      for (int i = 0; i < (d.width >> 2); ++i) {
+        uint32_t v = 0u;
+#pragma unroll
+        for (int j = 0; j < KW; ++j)
+          if (i < d.vwords && j == d.vwords - 1 - i) v = bswap(k[j]);
+        w[i] = v;
+      }
+    }
+  }
+}
+
 template <int KW>
 __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_constant__ RawLevel L) {
   using G = RawGeom<KW>;
@@ -589,10 +636,11 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
       const uint32_t j = v & ~kFromB;
       const uint32_t id = *reinterpret_cast<const uint32_t*>(ireg + (fromB ? r.ib : r.ia) + 4u * j);
       L.ids_out[r.out0 + x] = id;
-      if (L.keys_out) {
+      if (L.keys_out || L.dec.out) {
         uint32_t k[KW];
         raw_key_s<KW>((fromB ? kB : kA) + (size_t)j * G::W, k);
-        raw_key_store<KW>(L.keys_out, (size_t)r.out0 + x, k);
+        if (L.keys_out) raw_key_store<KW>(L.keys_out, (size_t)r.out0 + x, k);
+        else decode_store<KW>(L.dec, (size_t)r.out0 + x, k);
       }
     }
     if (++slot == kRawStages) {
@@ -629,6 +677,25 @@ static int launch_raw_level(const RawLevel& L, cudaStream_t s, double bytes) {
   k_merge_raw_tiles<KW><<<grid, kMergeBlock, G::smem, s>>>(L);
   YQ_CHECK_LAUNCH();
   return YQ_OK;
+}
+
+// *flag |= 1 when a key value would not survive the key-word round trip
+// (-0.0, a NaN other than the canonical one, a bool byte other than 0/1).
+__global__ void k_key_lossy(const char* __restrict__ data, int type, uint32_t rows, uint32_t* flag) {
+  bool lossy = false;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    if (type == YQ_FLOAT32) {
+      const uint32_t b = __ldg(reinterpret_cast<const uint32_t*>(data) + r);
+      lossy |= b == 0x80000000u || (((b & 0x7f800000u) == 0x7f800000u) && (b & 0x007fffffu) && b != 0x7fc00000u);
+    } else if (type == YQ_FLOAT64) {
+      const unsigned long long b = __ldg(reinterpret_cast<const unsigned long long*>(data) + r);
+      lossy |= b == 0x8000000000000000ull || (((b & 0x7ff0000000000000ull) == 0x7ff0000000000000ull) &&
+                                              (b & 0x000fffffffffffffull) && b != 0x7ff8000000000000ull);
+    } else if (type == YQ_BOOL) {
+      lossy |= (uint8_t)data[r] > 1u;
+    }
+  }
+  if (__any_sync(0xffffffffu, lossy) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
 }
 
 // Merge levels of one ORDER BY: host plan of every level's pairs.
@@ -802,6 +869,15 @@ extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descendi
   uint32_t* sort_err = nullptr;
   YQ_TRY(sort_segments_impl(&job, 1, rows, run_offsets, nruns, ids[0], nullptr, sort_ws, o.sort_bytes, s, nullptr,
                             keys[0], &kw, true, &sort_err));
+  // The last merge level writes the key column itself when the key has no
+  // nulls; the gather then moves the key column only if some value would not
+  // round-trip through its key words (flag set on the device).
+  const bool decode = kw > 0 && nruns > 1 && !key.nulls && key.type != YQ_TEXT;
+  uint32_t* d_lossy = d_err + 1;
+  if (decode && (key.type == YQ_FLOAT32 || key.type == YQ_FLOAT64 || key.type == YQ_BOOL)) {
+    k_key_lossy<<<sm_count() * 4, 256, 0, s>>>(static_cast<const char*>(key.data), key.type, rows, d_lossy);
+    YQ_CHECK_LAUNCH();
+  }
   // 2. merge levels over (key words, row id)
   int cur = 0;
   if (kw > 0 && nruns > 1) {
@@ -816,6 +892,14 @@ extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descendi
       L.keys_in = keys[cur];
       L.ids_in = ids[cur];
       L.keys_out = last ? nullptr : keys[cur ^ 1];
+      memset(&L.dec, 0, sizeof(L.dec));
+      if (last && decode) {
+        L.dec.out = static_cast<char*>(out->columns[key_col].data);
+        L.dec.type = key.type;
+        L.dec.vwords = key.type == YQ_INT32 || key.type == YQ_FLOAT32 || key.type == YQ_BOOL ? 1 : 2;
+        L.dec.width = key.width;
+        L.dec.desc = descending != 0;
+      }
       L.ids_out = ids[cur ^ 1];
       L.pairs = d_pairs + P.level_first[l];
       L.npairs = P.level_first[l + 1] - P.level_first[l];
@@ -837,9 +921,9 @@ extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descendi
     }
   }
   // 3. every column (the key included) gathered once by the final row ids
-  yq_column outs[YQ_MAX_BATCH_COLUMNS];
-  for (int c = 0; c < in->ncols; ++c) outs[c] = out->columns[c];
-  YQ_TRY(yq_gather(in->columns, in->ncols, ids[cur], rows, outs, s));
+  const uint32_t* only_if[YQ_MAX_BATCH_COLUMNS] = {nullptr};
+  if (decode) only_if[key_col] = d_lossy;  // zero unless a value would not round-trip
+  YQ_TRY(gather_impl(in->columns, in->ncols, ids[cur], rows, out->columns, only_if, s));
   uint32_t err[2] = {0, 0};
   YQ_TRY_CUDA(cudaMemcpyAsync(&err[0], sort_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   YQ_TRY_CUDA(cudaMemcpyAsync(&err[1], d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));

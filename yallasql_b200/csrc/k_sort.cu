@@ -370,6 +370,7 @@ struct GatherCol {
   const uint8_t* src_nulls;
   char* dst;
   uint8_t* dst_nulls;
+  const uint32_t* only_if;  // non-null: the column moves only when *only_if != 0
   int32_t width;
 };
 struct GatherParams {
@@ -415,6 +416,7 @@ __device__ __forceinline__ void gather_rows(const V* __restrict__ src, V* __rest
 __global__ void __launch_bounds__(256) k_gather_cols(const __grid_constant__ GatherParams G,
                                                      const uint32_t* __restrict__ perm, uint32_t n) {
   const GatherCol& g = G.c[blockIdx.y];
+  if (g.only_if && *g.only_if == 0u) return;
   for (uint32_t base = blockIdx.x * (256u * kGatherItems); base < n; base += gridDim.x * (256u * kGatherItems)) {
     const uint32_t i0 = base + threadIdx.x;
     switch (g.width) {
@@ -457,6 +459,7 @@ __global__ void __launch_bounds__(256) k_gather(const __grid_constant__ GatherPa
     if (r >= n) continue;  // perm must be a permutation of [0, n): skip anything else
     for (int c = 0; c < G.ncols; ++c) {
       const GatherCol& g = G.c[c];
+      if (g.only_if && *g.only_if == 0u) continue;
       copy_bytes(g.dst + (size_t)i * g.width, g.src + (size_t)r * g.width, g.width);
       if (g.dst_nulls) g.dst_nulls[i] = g.src_nulls ? g.src_nulls[r] : 0;
     }
@@ -882,6 +885,50 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
   return YQ_OK;
 }
 
+// Gather used by yq_gather and yq_order_by (see yq_sort.cuh).
+int gather_impl(const yq_column* in, int32_t ncols, const uint32_t* perm, uint32_t rows, const yq_column* out,
+                const uint32_t* const* only_if, cudaStream_t s) {
+  if (ncols < 0 || ncols > YQ_MAX_BATCH_COLUMNS || (ncols > 0 && (!in || !out)) || (rows > 0 && !perm))
+    return YQ_ERR_INVALID_ARG;
+  if (rows == 0 || ncols == 0) return YQ_OK;
+  GatherParams G;
+  memset(&G, 0, sizeof(G));
+  G.ncols = ncols;
+  for (int c = 0; c < ncols; ++c) {
+    if (!in[c].data || !out[c].data || in[c].width != out[c].width || in[c].width <= 0) return YQ_ERR_INVALID_ARG;
+    if (in[c].width != 1 && in[c].width % 4 != 0) return YQ_ERR_INVALID_ARG;
+    G.c[c].src = static_cast<const char*>(in[c].data);
+    G.c[c].src_nulls = in[c].nulls;
+    G.c[c].dst = static_cast<char*>(out[c].data);
+    G.c[c].dst_nulls = const_cast<uint8_t*>(out[c].nulls);
+    G.c[c].width = in[c].width;
+    G.c[c].only_if = only_if ? only_if[c] : nullptr;
+  }
+  // Aligned columns (16-byte text slots, 4/8-byte values) take the
+  // column-parallel kernel; others the row-parallel one.
+  bool aligned = true;
+  for (int c = 0; c < ncols; ++c)
+    aligned &= ((reinterpret_cast<uintptr_t>(G.c[c].src) | reinterpret_cast<uintptr_t>(G.c[c].dst)) &
+                (uintptr_t)(G.c[c].width >= 16 ? 15 : (G.c[c].width >= 8 ? 7 : (G.c[c].width >= 4 ? 3 : 0)))) == 0;
+  double row_bytes = 4.0;  // permutation
+  for (int c = 0; c < ncols; ++c)
+    if (!only_if || !only_if[c]) row_bytes += 2.0 * in[c].width + (out[c].nulls ? 2.0 : 0.0);
+  ProfScope ps("gather", s, (double)rows * row_bytes);
+  if (aligned) {
+    const uint32_t tiles = ceil_div<uint32_t>(rows, 256u * kGatherItems);
+    const uint32_t cap = (uint32_t)sm_count() * 8;
+    dim3 grid(tiles < cap ? tiles : cap, (unsigned)ncols);
+    k_gather_cols<<<grid, 256, 0, s>>>(G, perm, rows);
+  } else {
+    int grid = (int)ceil_div<uint32_t>(rows, 256);
+    const int cap = sm_count() * 16;
+    if (grid > cap) grid = cap;
+    k_gather<<<grid, 256, 0, s>>>(G, perm, rows);
+  }
+  YQ_CHECK_LAUNCH();
+  return YQ_OK;
+}
+
 }  // namespace yq
 
 using namespace yq;
@@ -999,44 +1046,7 @@ int yq_sort_autotune(const yq_column* key, uint32_t rows, const uint32_t* seg_of
 }
 
 int yq_gather(const yq_column* in, int32_t ncols, const uint32_t* perm, uint32_t rows, yq_column* out, void* stream) {
-  if (ncols < 0 || ncols > YQ_MAX_BATCH_COLUMNS || (ncols > 0 && (!in || !out)) || (rows > 0 && !perm))
-    return YQ_ERR_INVALID_ARG;
-  if (rows == 0 || ncols == 0) return YQ_OK;
-  GatherParams G;
-  memset(&G, 0, sizeof(G));
-  G.ncols = ncols;
-  for (int c = 0; c < ncols; ++c) {
-    if (!in[c].data || !out[c].data || in[c].width != out[c].width || in[c].width <= 0) return YQ_ERR_INVALID_ARG;
-    if (in[c].width != 1 && in[c].width % 4 != 0) return YQ_ERR_INVALID_ARG;
-    G.c[c].src = static_cast<const char*>(in[c].data);
-    G.c[c].src_nulls = in[c].nulls;
-    G.c[c].dst = static_cast<char*>(out[c].data);
-    G.c[c].dst_nulls = const_cast<uint8_t*>(out[c].nulls);
-    G.c[c].width = in[c].width;
-  }
-  cudaStream_t s = as_stream(stream);
-  // Aligned columns (16-byte text slots, 4/8-byte values) take the
-  // column-parallel kernel; others the row-parallel one.
-  bool aligned = true;
-  for (int c = 0; c < ncols; ++c)
-    aligned &= ((reinterpret_cast<uintptr_t>(G.c[c].src) | reinterpret_cast<uintptr_t>(G.c[c].dst)) &
-                (uintptr_t)(G.c[c].width >= 16 ? 15 : (G.c[c].width >= 8 ? 7 : (G.c[c].width >= 4 ? 3 : 0)))) == 0;
-  double row_bytes = 4.0;  // permutation
-  for (int c = 0; c < ncols; ++c) row_bytes += 2.0 * in[c].width + (out[c].nulls ? 2.0 : 0.0);
-  ProfScope ps("gather", s, (double)rows * row_bytes);
-  if (aligned) {
-    const uint32_t tiles = ceil_div<uint32_t>(rows, 256u * kGatherItems);
-    const uint32_t cap = (uint32_t)sm_count() * 8;
-    dim3 grid(tiles < cap ? tiles : cap, (unsigned)ncols);
-    k_gather_cols<<<grid, 256, 0, s>>>(G, perm, rows);
-  } else {
-    int grid = (int)ceil_div<uint32_t>(rows, 256);
-    const int cap = sm_count() * 16;
-    if (grid > cap) grid = cap;
-    k_gather<<<grid, 256, 0, s>>>(G, perm, rows);
-  }
-  YQ_CHECK_LAUNCH();
-  return YQ_OK;
+  return gather_impl(in, ncols, perm, rows, out, nullptr, as_stream(stream));
 }
 
 }  // extern "C"

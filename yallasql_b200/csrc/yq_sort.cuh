@@ -26,4 +26,9 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
                        cudaStream_t s, size_t* size_only, uint32_t* keys_out = nullptr, int* kw_out = nullptr,
                        bool defer_err = false, uint32_t** err_out = nullptr);
 
+// out[c][i] = in[c][perm[i]] for every column (yq_gather); with `only_if`,
+// column c moves only when only_if[c] is null or *only_if[c] != 0 on the device.
+int gather_impl(const yq_column* in, int32_t ncols, const uint32_t* perm, uint32_t rows, const yq_column* out,
+                const uint32_t* const* only_if, cudaStream_t s);
+
 }  // namespace yq
