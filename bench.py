@@ -405,6 +405,21 @@ def cpu_baseline(args, t: dict) -> dict:
             "sample": f"first {sample} of {args.rows} rows, both ORDER BY queries (stable sort + gather of 4 columns)"}
 
 
+def max_over_ranks(ms: float, dist, device="cuda") -> float:
+    """Step time of the whole job: the slowest rank's (every rank calls this)."""
+    if dist is None:
+        return ms
+    import torch
+    tt = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def whole_job_rows_per_s(world: int, rows_per_step: int, ms: float) -> float:
+    """Units all ranks processed (weak scaling: each rank runs the full workload) / the slowest rank's time."""
+    return world * rows_per_step / (ms / 1e3)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -452,13 +467,9 @@ def main():
     lib.yq_profile_read(buf, len(buf), 1)
     prof = json.loads(buf.value.decode() or "{}")
     launches = int(lib.yq_launch_count() - launches0)
-    ms = s.elapsed_time(e) / args.steps
-    if dist is not None:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(s.elapsed_time(e) / args.steps, dist)
     rows_per_step = 2 * args.rows
-    value = world * rows_per_step / (ms / 1e3)
+    value = whole_job_rows_per_s(world, rows_per_step, ms)
 
     # parity spot check of this run (cheap, on device): outputs ordered
     a, b = job.step()
@@ -488,13 +499,9 @@ def main():
             e2e_step()
         e2.record()
         torch.cuda.synchronize()
-        ms2 = s2.elapsed_time(e2) / args.steps
-        if dist is not None:
-            tt = torch.tensor([ms2], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms2 = float(tt.item())
+        ms2 = max_over_ranks(s2.elapsed_time(e2) / args.steps, dist)
         tab_bytes = sum(v.nbytes for v in t.values())
-        e2e = {"value": world * rows_per_step / (ms2 / 1e3), "unit": UNIT, "h2d_bytes_per_step": tab_bytes,
+        e2e = {"value": whole_job_rows_per_s(world, rows_per_step, ms2), "unit": UNIT, "h2d_bytes_per_step": tab_bytes,
                "d2h_bytes_per_step": 2 * tab_bytes, "ms_per_step": ms2,
                "path": "pinned host columns -> cudaMemcpyAsync -> C-ABI operators -> pinned host, every step"}
 
