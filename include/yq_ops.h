@@ -28,8 +28,10 @@
 #ifndef YQ_OPS_H
 #define YQ_OPS_H
 
+#ifndef __CUDACC_RTC__ /* runtime-compiled kernels get these types from yq_common.cuh */
 #include <stddef.h>
 #include <stdint.h>
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -518,6 +520,21 @@ int yq_cross_product_col(const yq_column* col, uint32_t left_rows, uint32_t righ
 int yq_device_sm_count(void);
 /* Kernel launches issued by this library on this process (for accounting). */
 uint64_t yq_launch_count(void);
+/* ---- Program-specialised row kernels.
+ * The fused row operators (filter + aggregate / projection, their segmented
+ * forms, the star-join aggregate) run an expression program. By default the
+ * library compiles, once per distinct program (its instruction words; the
+ * constants stay parameters), a kernel whose program is compile-time constant
+ * (NVRTC, opened at run time, sm_100a) and launches it instead of the
+ * interpreting kernel; the results are the same. yq_jit_enable(0) (or
+ * YQ_JIT=0 in the environment) keeps the interpreting kernels; it returns the
+ * previous setting. yq_jit_stats reports kernels compiled, compilations that
+ * failed (their programs use the interpreting kernel), cache hits, total
+ * compile time and the last compiler log. */
+int yq_jit_enable(int32_t on);
+int yq_jit_stats(int32_t* compiled, int32_t* failed, int32_t* hits, double* compile_ms, char* log,
+                 size_t log_bytes);
+
 /* Device timing of the library's own launches: when enabled, every kernel
  * launch records a CUDA event pair on its stream, tagged with the kernel and
  * its algorithmic bytes. yq_profile_read synchronises on the recorded events

@@ -152,6 +152,8 @@ PROTOTYPES = {
     "yq_device_sm_count": (C.c_int, []),
     "yq_launch_count": (u64, []),
     "yq_profile_enable": (C.c_int, [i32]),
+    "yq_jit_enable": (C.c_int, [i32]),
+    "yq_jit_stats": (C.c_int, [P(i32), P(i32), P(i32), P(C.c_double), C.c_char_p, sz]),
     "yq_profile_read": (C.c_int, [C.c_char_p, sz, i32]),
 }
 

@@ -72,12 +72,49 @@ def _compile_all(srcs: list[str], extra: list[str], headers: list[str]) -> list[
     return objs
 
 
+# Device headers the runtime-compiled kernels include (jit.cu), by the name
+# each is #included under.
+JIT_HEADERS = [("row_kernels.cuh", os.path.join(CSRC, "row_kernels.cuh")),
+               ("yq_agg.cuh", os.path.join(CSRC, "yq_agg.cuh")),
+               ("yq_hash.cuh", os.path.join(CSRC, "yq_hash.cuh")),
+               ("yq_lookback.cuh", os.path.join(CSRC, "yq_lookback.cuh")),
+               ("yq_stage.cuh", os.path.join(CSRC, "yq_stage.cuh")),
+               ("yq_vm.cuh", os.path.join(CSRC, "yq_vm.cuh")),
+               ("yq_common.cuh", os.path.join(CSRC, "yq_common.cuh")),
+               ("../../include/yq_ops.h", os.path.join(INCLUDE, "yq_ops.h"))]
+
+
+def _jit_headers_source() -> str:
+    """A C++ file holding the JIT device headers as string literals."""
+    os.makedirs(BUILD, exist_ok=True)
+    out = os.path.join(BUILD, "jit_headers.gen.cpp")
+    if not _stale(out, [p for _, p in JIT_HEADERS] + [os.path.abspath(__file__)]):
+        return out
+    parts = ["// Generated by yallasql_b200/build.py: device headers for runtime compilation.\n"]
+    names, texts = [], []
+    for i, (name, path) in enumerate(JIT_HEADERS):
+        with open(path) as f:
+            text = f.read()
+        if ")YQJIT\"" in text:
+            raise RuntimeError(f"{path} contains the raw-string delimiter")
+        parts.append(f'static const char h{i}[] = R"YQJIT({text})YQJIT";\n')
+        names.append(f'"{name}"')
+        texts.append(f"h{i}")
+    parts.append(f"extern const int yq_jit_header_count = {len(JIT_HEADERS)};\n")
+    parts.append("extern const char* const yq_jit_header_names[] = {" + ", ".join(names) + "};\n")
+    parts.append("extern const char* const yq_jit_header_texts[] = {" + ", ".join(texts) + "};\n")
+    with open(out, "w") as f:
+        f.write("".join(parts))
+    return out
+
+
 def build_ops(verbose: bool = False) -> str:
     srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    srcs.append(_jit_headers_source())
     headers = _headers(CSRC)
     objs = _compile_all(srcs, [], headers)
     if _stale(OPS_LIB, objs):
-        _run([nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", OPS_LIB] + objs)
+        _run([nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", OPS_LIB] + objs + ["-ldl"])
         if verbose:
             print("built", OPS_LIB)
     return OPS_LIB

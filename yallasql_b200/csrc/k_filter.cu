@@ -11,9 +11,8 @@
 // reads them from global memory directly.
 #include <vector>
 #include "vm_host.cuh"
-#include "yq_agg.cuh"
-#include "yq_lookback.cuh"
-#include "yq_stage.cuh"
+#include "row_kernels.cuh"
+#include "yq_jit.cuh"
 
 namespace yq {
 
@@ -50,12 +49,6 @@ struct GridCache {
 static size_t max_row_grid() { return (size_t)sm_count() * 8; }
 
 // ================================================================ aggregate
-struct FAParams {
-  VmProgram P;
-  StagePlan SP;
-  int32_t pc_end;
-  AggParams A;
-};
 
 __global__ void k_agg_state_init(Acc* state, const AggParams p) {
   const int a = threadIdx.x;
@@ -75,51 +68,7 @@ template <bool STAGED>
 __global__ void __launch_bounds__(kRowBlock, 2) k_filter_aggregate(const __grid_constant__ FAParams F, uint32_t n,
                                                                    Acc* __restrict__ partials, uint32_t* ticket,
                                                                    Acc* state) {
-  uint32_t* err = agg_state_err(state);
-  AggEmit E;
-  agg_thread_init(E, F.A);
-  uint32_t nsel = 0;
-  const uint32_t ntiles = ceil_div<uint32_t>(n, kStepRows);
-  const uint32_t G = gridDim.x;
-  int S = 1;
-  if constexpr (STAGED) {
-    S = F.SP.nstages;
-    stage_init(F.SP);
-    if (threadIdx.x == 0)
-      for (int j = 0; j < S - 1; ++j) {
-        const uint32_t t = blockIdx.x + (uint32_t)j * G;
-        if (t < ntiles) stage_start(F.SP, j, t * kStepRows, step_rows(t, n));
-      }
-  }
-  int slot = 0;
-  uint32_t parity = 0;
-  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += G) {
-    Ctx X;
-    X.tile0 = tile * kStepRows;
-    X.lr = threadIdx.x * ITEMS;
-    X.inr = in_range_bits(X.tile0 + X.lr, n);
-    X.stage = 0;
-    X.vec_ok = (X.tile0 & 15u) == 0u;
-    if constexpr (STAGED) {
-      __syncthreads();  // every thread is done with the previous step: its slot is free
-      if (threadIdx.x == 0) {
-        const uint32_t t = tile + (uint32_t)(S - 1) * G;
-        const int ns = slot == 0 ? S - 1 : slot - 1;
-        if (t < ntiles) stage_start(F.SP, ns, t * kStepRows, step_rows(t, n));
-      }
-      stage_finish(F.SP, slot, parity, X.tile0, step_rows(tile, n), err);
-      X.stage = (uint32_t)slot * F.SP.stage_bytes;
-    }
-    E.sel = X.inr;
-    Stack St;
-    run_vm<STAGED>(F.P, 0, F.pc_end, X, St, E);
-    nsel += __popc(E.sel);
-    if (++slot == S) {
-      slot = 0;
-      parity ^= 1u;
-    }
-  }
-  agg_block_finish<kRowBlock>(E, nsel, F.A, partials, ticket, state);
+  filter_aggregate_body<STAGED, InterpRunner>(F, n, partials, ticket, state);
 }
 
 static uint8_t agg_update_code(int kind, int t) {
@@ -195,6 +144,10 @@ static int launch_filter_aggregate(const FAParams& F, uint32_t rows, Acc* partia
   int grid = gc[staged ? 1 : 0].grid(kern, smem, ceil_div<uint32_t>(rows, kStepRows));
   if ((size_t)grid > max_row_grid()) grid = (int)max_row_grid();
   ProfScope ps("filter_aggregate", s, (double)rows * row_bytes_of(F.P, program_columns(F.P, F.pc_end, 0)));
+  if (const void* jk = jit_kernel(JIT_FILTER_AGG, staged, F.P, F.pc_end, F.pc_end)) {
+    void* args[] = {const_cast<FAParams*>(&F), &rows, &partials, &ticket, &state};
+    return jit_launch(jk, (int)max_row_grid(), ceil_div<uint32_t>(rows, kStepRows), smem, args, s);
+  }
   if (staged)
     k_filter_aggregate<true><<<grid, kRowBlock, smem, s>>>(F, rows, partials, ticket, state);
   else
@@ -204,100 +157,10 @@ static int launch_filter_aggregate(const FAParams& F, uint32_t rows, Acc* partia
 }
 
 // ======================================================= segmented aggregate
-// Many independent filter+aggregate tasks in one launch: task g owns rows
-// [seg[g], seg[g+1]) of the batch and its own aggregate state. Steps never
-// straddle tasks; the persistent blocks walk the steps of all tasks as one
-// queue (step -> task by binary search over the tasks' first steps), write
-// one partial per step, and k_agg_seg_fold folds each task's partials in step
-// order, so every task's result is deterministic and equal to the result of
-// running it alone.
-struct FASegParams {
-  FAParams F;
-  const uint32_t* seg;    // [nseg] first row of each task
-  const uint32_t* seg_end;  // [nseg] end row of each task
-  const uint32_t* step0;  // [nseg + 1] first step of each task
-  int32_t nseg;
-  uint32_t nsteps;
-  Acc* partials;          // [nsteps][YQ_MAX_AGGREGATES]
-  uint32_t* err;
-};
-
-__device__ __forceinline__ int seg_of_step(const uint32_t* step0, int nseg, uint32_t t) {
-  int lo = 0, hi = nseg - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(step0 + mid) <= t) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
-// Step t: task g's rows within the absolute step window of t (windows are
-// kStepRows-aligned, so only a task's first and last steps are partial).
-__device__ __forceinline__ void seg_step(const FASegParams& Q, uint32_t t, uint32_t& row0, uint32_t& rows) {
-  const int g = seg_of_step(Q.step0, Q.nseg, t);
-  const uint32_t s = __ldg(Q.seg + g), e = __ldg(Q.seg_end + g);
-  const uint64_t base = ((uint64_t)(s / kStepRows) + (t - __ldg(Q.step0 + g))) * kStepRows;
-  const uint64_t lo = base > s ? base : s;
-  const uint64_t hi = base + kStepRows < e ? base + kStepRows : e;
-  row0 = (uint32_t)lo;
-  rows = (uint32_t)(hi - lo);
-}
 
 template <bool STAGED>
 __global__ void __launch_bounds__(kRowBlock, 2) k_filter_aggregate_seg(const __grid_constant__ FASegParams Q) {
-  const FAParams& F = Q.F;
-  const uint32_t G = gridDim.x;
-  int S = 1;
-  if constexpr (STAGED) {
-    S = F.SP.nstages;
-    stage_init(F.SP);
-    if (threadIdx.x == 0)
-      for (int j = 0; j < S - 1; ++j) {
-        const uint32_t t = blockIdx.x + (uint32_t)j * G;
-        if (t < Q.nsteps) {
-          uint32_t r0, nr;
-          seg_step(Q, t, r0, nr);
-          stage_start(F.SP, j, r0, nr);
-        }
-      }
-  }
-  int slot = 0;
-  uint32_t parity = 0;
-  for (uint32_t t = blockIdx.x; t < Q.nsteps; t += G) {
-    uint32_t row0, rows;
-    seg_step(Q, t, row0, rows);
-    Ctx X;
-    X.tile0 = row0;
-    X.lr = threadIdx.x * ITEMS;
-    X.inr = in_range_bits(X.lr, rows);
-    X.stage = 0;
-    X.vec_ok = (X.tile0 & 15u) == 0u;
-    if constexpr (STAGED) {
-      __syncthreads();  // every thread is done with the previous step: its slot is free
-      if (threadIdx.x == 0) {
-        const uint32_t tn = t + (uint32_t)(S - 1) * G;
-        const int ns = slot == 0 ? S - 1 : slot - 1;
-        if (tn < Q.nsteps) {
-          uint32_t r0, nr;
-          seg_step(Q, tn, r0, nr);
-          stage_start(F.SP, ns, r0, nr);
-        }
-      }
-      stage_finish(F.SP, slot, parity, row0, rows, Q.err);
-      X.stage = (uint32_t)slot * F.SP.stage_bytes;
-    }
-    AggEmit E;
-    agg_thread_init(E, F.A);
-    E.sel = X.inr;
-    Stack St;
-    run_vm<STAGED>(F.P, 0, F.pc_end, X, St, E);
-    agg_block_partial<kRowBlock>(E, __popc(E.sel), F.A, Q.partials + (size_t)t * YQ_MAX_AGGREGATES);
-    if (++slot == S) {
-      slot = 0;
-      parity ^= 1u;
-    }
-  }
+  filter_aggregate_seg_body<STAGED, InterpRunner>(Q);
 }
 
 // One warp per task: aggregate a < nagg folds the task's step partials in order.
@@ -334,172 +197,12 @@ static uint32_t seg_steps(const uint32_t* begin, const uint32_t* end, int nseg, 
 }
 
 // ================================================================ project
-struct DevOut {
-  char* data;
-  uint8_t* nulls;
-  int32_t width;
-  int32_t src_col;  // >= 0: copy of this input column
-};
-
-struct FPParams {
-  VmProgram P;
-  StagePlan SP;
-  int32_t pred_end;
-  int32_t proj_end;
-  int32_t nproj;
-  uint32_t capacity;
-  DevOut out[YQ_MAX_PROJECTIONS];
-};
-
-struct ProjEmit {
-  uint32_t sel;
-  uint32_t pos;
-  const FPParams* F;
-  __device__ __forceinline__ void pred(uint32_t bits) { sel &= bits; }
-  template <int K>
-  __device__ __forceinline__ void agg(int, const Val&) {}
-  template <int W>
-  __device__ __forceinline__ void proj(int p, const Val& x) {
-    const DevOut& o = F->out[p];
-    uint32_t q = pos;
-#pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
-      if (sel >> k & 1u) {
-        if (q < F->capacity) {
-          if constexpr (W == 0) reinterpret_cast<uint8_t*>(o.data)[q] = (uint8_t)((x.v[0] >> k) & 1u);
-          else if constexpr (W == 1) reinterpret_cast<uint32_t*>(o.data)[q] = (uint32_t)x.v[k];
-          else reinterpret_cast<unsigned long long*>(o.data)[q] = x.v[k];
-          if (o.nulls) o.nulls[q] = (x.valid >> k & 1u) ? 0 : 1;
-        }
-        ++q;
-      }
-    }
-  }
-};
-
-// One cell of `width` bytes; `src` is shared or global memory (generic).
-__device__ __forceinline__ void copy_cell_any(char* dst, const char* src, int width) {
-  if (width == 4) {
-    *reinterpret_cast<uint32_t*>(dst) = *reinterpret_cast<const uint32_t*>(src);
-  } else if (width == 8) {
-    *reinterpret_cast<unsigned long long*>(dst) = *reinterpret_cast<const unsigned long long*>(src);
-  } else if (width == 1) {
-    *dst = *src;
-  } else if ((width & 15) == 0 && ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0) {
-    for (int i = 0; i < width; i += 16)
-      *reinterpret_cast<uint4*>(dst + i) = *reinterpret_cast<const uint4*>(src + i);
-  } else {
-    for (int i = 0; i < width; i += 4)
-      *reinterpret_cast<uint32_t*>(dst + i) = *reinterpret_cast<const uint32_t*>(src + i);
-  }
-}
-
-// Projections that copy an input column: selected rows to positions pos, pos+1, ...
-template <bool STAGED>
-__device__ __forceinline__ void copy_source_columns(const FPParams& F, const Ctx& X, uint32_t sel, uint32_t pos) {
-  for (int p = 0; p < F.nproj; ++p) {
-    const DevOut& o = F.out[p];
-    if (o.src_col < 0) continue;
-    const DevCol& c = F.P.cols[o.src_col];
-    uint32_t q = pos;
-#pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
-      if (sel >> k & 1u) {
-        if (q < F.capacity) {
-          const uint32_t lr = X.lr + k;
-          const char* src;
-          uint8_t nul = 0;
-          if constexpr (STAGED) {
-            src = reinterpret_cast<const char*>(yq_dyn_smem + X.stage + c.soff + lr * (uint32_t)c.width);
-            if (c.nulls) nul = yq_dyn_smem[X.stage + c.snoff + lr];
-          } else {
-            src = c.data + (size_t)(X.tile0 + lr) * c.width;
-            if (c.nulls) nul = c.nulls[X.tile0 + lr];
-          }
-          copy_cell_any(o.data + (size_t)q * o.width, src, c.width);
-          if (o.nulls) o.nulls[q] = nul;
-        }
-        ++q;
-      }
-    }
-  }
-}
-
-// Tiles are claimed in order from a counter (a few steps ahead when staged),
-// every block processes its claims in order, so each tile's predecessors are
-// held by running blocks and the decoupled look-back always completes.
 template <bool STAGED>
 __global__ void __launch_bounds__(kRowBlock, 2) k_filter_project(const __grid_constant__ FPParams F, uint32_t n,
                                                                  uint32_t* tile_counter,
                                                                  unsigned long long* __restrict__ status,
                                                                  uint32_t* out_count, uint32_t* err) {
-  __shared__ uint32_t s_tiles[kStageMax];
-  __shared__ uint32_t s_warp[kRowBlock / 32 + 1];
-  __shared__ unsigned long long s_prefix;
-  const uint32_t ntiles = ceil_div<uint32_t>(n, kStepRows);
-  int S = 1;
-  if constexpr (STAGED) {
-    S = F.SP.nstages;
-    stage_init(F.SP);
-  }
-  if (threadIdx.x == 0)
-    for (int j = 0; j < S - 1; ++j) {
-      const uint32_t t = atomicAdd(tile_counter, 1u);
-      s_tiles[j] = t;
-      if constexpr (STAGED)
-        if (t < ntiles) stage_start(F.SP, j, t * kStepRows, step_rows(t, n));
-    }
-  int slot = 0;
-  uint32_t parity = 0;
-  for (;;) {
-    __syncthreads();  // every thread is done with the previous step
-    if (threadIdx.x == 0) {
-      const int ns = slot == 0 ? S - 1 : slot - 1;
-      const uint32_t t = atomicAdd(tile_counter, 1u);
-      s_tiles[ns] = t;
-      if constexpr (STAGED)
-        if (t < ntiles) stage_start(F.SP, ns, t * kStepRows, step_rows(t, n));
-    }
-    __syncthreads();
-    const uint32_t tile = s_tiles[slot];
-    if (tile >= ntiles) break;  // later claims are larger: no copy is in flight
-    Ctx X;
-    X.tile0 = tile * kStepRows;
-    X.lr = threadIdx.x * ITEMS;
-    X.inr = in_range_bits(X.tile0 + X.lr, n);
-    X.stage = 0;
-    X.vec_ok = (X.tile0 & 15u) == 0u;
-    if constexpr (STAGED) {
-      stage_finish(F.SP, slot, parity, X.tile0, step_rows(tile, n), err);
-      X.stage = (uint32_t)slot * F.SP.stage_bytes;
-    }
-    ProjEmit E;
-    E.sel = X.inr;
-    E.pos = 0;
-    E.F = &F;
-    Stack St;
-    if (F.pred_end > 0) run_vm<STAGED>(F.P, 0, F.pred_end, X, St, E);
-
-    uint32_t total;
-    const uint32_t excl = block_exclusive_sum<kRowBlock>(__popc(E.sel), s_warp, total);
-    if (threadIdx.x < 32) {
-      const unsigned long long p = tile_lookback(status, tile, total, err);
-      if (threadIdx.x == 0) s_prefix = p;
-    }
-    __syncthreads();
-    const unsigned long long base = s_prefix;
-    E.pos = (uint32_t)(base + excl);
-    if (F.proj_end > F.pred_end) run_vm<STAGED>(F.P, F.pred_end, F.proj_end, X, St, E);
-    copy_source_columns<STAGED>(F, X, E.sel, E.pos);
-    if (tile == ntiles - 1 && threadIdx.x == 0) {
-      const unsigned long long cnt = base + total;
-      *out_count = cnt > 0xffffffffull ? 0xffffffffu : (uint32_t)cnt;
-    }
-    if (++slot == S) {
-      slot = 0;
-      parity ^= 1u;
-    }
-  }
+  filter_project_body<STAGED, InterpRunner>(F, n, tile_counter, status, out_count, err);
 }
 
 // Validation and program build shared by yq_filter_project and its
@@ -552,7 +255,7 @@ static int build_project_params(const yq_batch* batch, const yq_program* predica
 // Launch over `rows` rows with look-back scratch `status` (one word per tile
 // plus one) and `misc` = {tile counter, error word} (both zeroed).
 static int launch_filter_project(const FPParams& F, uint32_t rows, uint32_t* misc, unsigned long long* status,
-                                 uint32_t* cnt_dev, cudaStream_t s) {
+                                 uint32_t* cnt_dev, cudaStream_t s, bool allow_jit = true) {
   const bool staged = F.SP.nstages > 0;
   const void* kern = staged ? (const void*)k_filter_project<true> : (const void*)k_filter_project<false>;
   const size_t smem = stage_smem_bytes(F.SP);
@@ -565,6 +268,11 @@ static int launch_filter_project(const FPParams& F, uint32_t rows, uint32_t* mis
     if (F.out[p].src_col >= 0) mask |= 1u << F.out[p].src_col;
   // algorithmic bytes: referenced input columns (outputs depend on selectivity)
   ProfScope ps("filter_project", s, (double)rows * row_bytes_of(F.P, mask));
+  if (const void* jk = allow_jit ? jit_kernel(JIT_FILTER_PROJECT, staged, F.P, F.pred_end, F.proj_end) : nullptr) {
+    uint32_t* err = misc + 1;
+    void* args[] = {const_cast<FPParams*>(&F), &rows, &misc, &status, &cnt_dev, &err};
+    return jit_launch(jk, 1 << 30, ceil_div<uint32_t>(rows, kStepRows), smem, args, s);
+  }
   if (staged)
     k_filter_project<true><<<grid, kRowBlock, smem, s>>>(F, rows, misc, status, cnt_dev, misc + 1);
   else
@@ -777,7 +485,10 @@ static int filter_aggregate_ranges(const yq_batch* batch, const uint32_t* begin,
     double rows = 0;
     for (int g = 0; g < nseg; ++g) rows += end[g] - begin[g];
     ProfScope ps("filter_aggregate_seg", s, rows * row_bytes_of(Q.F.P, program_columns(Q.F.P, Q.F.pc_end, 0)));
-    if (staged)
+    if (const void* jk = jit_kernel(JIT_FILTER_AGG_SEG, staged, Q.F.P, Q.F.pc_end, Q.F.pc_end)) {
+      void* args[] = {&Q};
+      YQ_TRY(jit_launch(jk, (int)max_row_grid(), nsteps, smem, args, s));
+    } else if (staged)
       k_filter_aggregate_seg<true><<<grid, kRowBlock, smem, s>>>(Q);
     else
       k_filter_aggregate_seg<false><<<grid, kRowBlock, 0, s>>>(Q);
@@ -921,7 +632,8 @@ extern "C" int yq_filter_project_noalloc(const yq_batch* batch, const yq_program
   // The previous call's values are still there: clear what this call reads.
   YQ_TRY_CUDA(cudaMemsetAsync(scratch, 0, (2 + (size_t)ntiles + 1) * sizeof(unsigned long long), s));
   uint32_t* cnt_dev = count_device ? count_device : misc + 2;
-  YQ_TRY(launch_filter_project(F, rows, misc, status, cnt_dev, s));
+  // the library's own kernel: loading a program-specialised one would allocate
+  YQ_TRY(launch_filter_project(F, rows, misc, status, cnt_dev, s, false));
   if (count_host) {
     uint32_t h[2];
     YQ_TRY_CUDA(cudaMemcpyAsync(&h[0], cnt_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));

@@ -22,9 +22,8 @@
 #include <string.h>
 #include <vector>
 #include "vm_host.cuh"
-#include "yq_agg.cuh"
-#include "yq_lookback.cuh"
-#include "yq_stage.cuh"
+#include "row_kernels.cuh"
+#include "yq_jit.cuh"
 
 namespace yq {
 
@@ -34,13 +33,6 @@ constexpr uint32_t kJoinTile = kJoinBlock * kJoinItems;
 constexpr uint32_t kHashMaxRows = 8192;  // right rows that fit the shared-memory table
 constexpr int kMaxConds = 8;
 constexpr int kMaxJoinOut = YQ_MAX_PROJECTIONS;
-
-struct JCol {
-  const char* data;
-  const uint8_t* nulls;
-  int32_t type;
-  int32_t width;
-};
 
 struct JCond {
   JCol l, r;
@@ -77,36 +69,6 @@ struct JoinParams {
   uint32_t* err;
 };
 
-// ----------------------------------------------------------- cell access
-__device__ __forceinline__ uint64_t cell_u64(const JCol& c, uint32_t row) {
-  switch (c.width) {
-    case 4: {
-      const uint32_t v = __ldg(reinterpret_cast<const uint32_t*>(c.data) + row);
-      return c.type == YQ_INT32 ? (uint64_t)(int64_t)(int32_t)v : (uint64_t)v;
-    }
-    case 8: return (uint64_t)__ldg(reinterpret_cast<const unsigned long long*>(c.data) + row);
-    default: return (uint64_t)(uint8_t)c.data[row];
-  }
-}
-
-__device__ __forceinline__ bool cell_null(const JCol& c, uint32_t row) { return c.nulls && c.nulls[row]; }
-
-// Normalised equality/hash key: -0.0 folds into +0.0 so they join.
-__device__ __forceinline__ uint64_t hash_key(const JCol& c, uint32_t row) {
-  uint64_t v = cell_u64(c, row);
-  if (c.type == YQ_FLOAT32 && ((uint32_t)v & 0x7fffffffu) == 0u) v = 0;
-  if (c.type == YQ_FLOAT64 && (v & 0x7fffffffffffffffull) == 0ull) v = 0;
-  return v;
-}
-
-__device__ __forceinline__ uint32_t hash_bucket(uint64_t k, uint32_t nb) {
-  k ^= k >> 33;
-  k *= 0xff51afd7ed558ccdull;
-  k ^= k >> 33;
-  k *= 0xc4ceb9fe1a85ec53ull;
-  k ^= k >> 33;
-  return (uint32_t)k & (nb - 1u);
-}
 
 __device__ __forceinline__ bool cmp_holds(int s, int op) {
   switch (op) {
@@ -432,109 +394,11 @@ __global__ void __launch_bounds__(256) k_cross_fill(const __grid_constant__ Join
   }
 }
 
-// ------------------------------------------------ fused star-join aggregate
-struct JAParams {
-  VmProgram P;  // fact predicate [0, pred_end) then aggregate inputs [pred_end, pc_end)
-  StagePlan SP;
-  int32_t pred_end, pc_end;
-  AggParams A;
-  int32_t fkey_col;  // fact key column (staged with the others when the ring is used)
-  JCol fkey;
-  uint32_t nbuckets, hrows_n;
-  uint32_t table_off;  // byte offset of the dimension table in dynamic shared memory
-  const uint32_t* bstart;
-  const unsigned long long* hkeys;
-};
-
-// Normalised key from the raw bits of a cell (as hash_key).
-__device__ __forceinline__ uint64_t norm_key(int type, uint64_t raw) {
-  uint64_t v = raw;
-  if (type == YQ_INT32) v = (uint64_t)(int64_t)(int32_t)(uint32_t)raw;
-  if (type == YQ_FLOAT32 && ((uint32_t)v & 0x7fffffffu) == 0u) v = 0;
-  if (type == YQ_FLOAT64 && (v & 0x7fffffffffffffffull) == 0ull) v = 0;
-  return v;
-}
-
 template <bool STAGED>
 __global__ void __launch_bounds__(kRowBlock, 2) k_join_aggregate(const __grid_constant__ JAParams F, uint32_t n,
                                                                  Acc* __restrict__ partials, uint32_t* ticket,
                                                                  Acc* state) {
-  uint32_t* s_bstart = reinterpret_cast<uint32_t*>(yq_dyn_smem + F.table_off);
-  unsigned long long* s_keys =
-      reinterpret_cast<unsigned long long*>(yq_dyn_smem + F.table_off + 4 * ((F.nbuckets + 2) & ~1u));
-  for (uint32_t i = threadIdx.x; i <= F.nbuckets; i += kRowBlock) s_bstart[i] = __ldg(F.bstart + i);
-  for (uint32_t i = threadIdx.x; i < F.hrows_n; i += kRowBlock) s_keys[i] = __ldg(F.hkeys + i);
-  __syncthreads();
-
-  uint32_t* err = agg_state_err(state);
-  AggEmit E;
-  agg_thread_init(E, F.A);
-  uint32_t nsel = 0;
-  const uint32_t ntiles = ceil_div<uint32_t>(n, kStepRows);
-  const uint32_t G = gridDim.x;
-  int S = 1;
-  if constexpr (STAGED) {
-    S = F.SP.nstages;
-    stage_init(F.SP);
-    if (threadIdx.x == 0)
-      for (int j = 0; j < S - 1; ++j) {
-        const uint32_t t = blockIdx.x + (uint32_t)j * G;
-        if (t < ntiles) stage_start(F.SP, j, t * kStepRows, step_rows(t, n));
-      }
-  }
-  const DevCol& kc = F.P.cols[F.fkey_col];
-  int slot = 0;
-  uint32_t parity = 0;
-  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += G) {
-    Ctx X;
-    X.tile0 = tile * kStepRows;
-    X.lr = threadIdx.x * ITEMS;
-    X.inr = in_range_bits(X.tile0 + X.lr, n);
-    X.stage = 0;
-    X.vec_ok = (X.tile0 & 15u) == 0u;
-    if constexpr (STAGED) {
-      __syncthreads();  // every thread is done with the previous step: its slot is free
-      if (threadIdx.x == 0) {
-        const uint32_t t = tile + (uint32_t)(S - 1) * G;
-        const int ns = slot == 0 ? S - 1 : slot - 1;
-        if (t < ntiles) stage_start(F.SP, ns, t * kStepRows, step_rows(t, n));
-      }
-      stage_finish(F.SP, slot, parity, X.tile0, step_rows(tile, n), err);
-      X.stage = (uint32_t)slot * F.SP.stage_bytes;
-    }
-    E.sel = X.inr;
-    Stack St;
-    if (F.pred_end > 0) run_vm<STAGED>(F.P, 0, F.pred_end, X, St, E);
-    // probe: keep rows whose key is present among the (unique) dimension keys
-    const uint32_t knull = null_bits<STAGED>(kc, X);
-#pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
-      if (!(E.sel >> k & 1u)) continue;
-      bool hit = false;
-      if (!(knull >> k & 1u)) {
-        uint64_t key;
-        if constexpr (STAGED) {
-          const unsigned char* p = yq_dyn_smem + X.stage + kc.soff + (X.lr + k) * (uint32_t)kc.width;
-          const uint64_t raw = kc.width == 8   ? *reinterpret_cast<const unsigned long long*>(p)
-                               : kc.width == 4 ? (uint64_t)*reinterpret_cast<const uint32_t*>(p)
-                                               : (uint64_t)*p;
-          key = norm_key(kc.type, raw);
-        } else {
-          key = hash_key(F.fkey, X.tile0 + X.lr + k);
-        }
-        const uint32_t b = hash_bucket(key, F.nbuckets);
-        for (uint32_t x = s_bstart[b]; x < s_bstart[b + 1] && !hit; ++x) hit = (s_keys[x] == key);
-      }
-      if (!hit) E.sel &= ~(1u << k);
-    }
-    run_vm<STAGED>(F.P, F.pred_end, F.pc_end, X, St, E);
-    nsel += __popc(E.sel);
-    if (++slot == S) {
-      slot = 0;
-      parity ^= 1u;
-    }
-  }
-  agg_block_finish<kRowBlock>(E, nsel, F.A, partials, ticket, state);
+  join_aggregate_body<STAGED, InterpRunner>(F, n, partials, ticket, state);
 }
 
 // ---------------------------------------------------------------- host
@@ -873,6 +737,12 @@ int yq_join_aggregate(const yq_batch* fact, const yq_program* fact_predicate, in
   if ((uint32_t)grid > tiles) grid = (int)tiles;
   const double row_bytes = row_bytes_of(F.P, program_columns(F.P, F.pc_end, 1u << fact_key));
   ProfScope ps("join_aggregate", s, (double)fact->rows * row_bytes);
+  if (const void* jk = jit_kernel(JIT_JOIN_AGG, staged, F.P, F.pred_end, F.pc_end)) {
+    uint32_t n = fact->rows;
+    Acc* st = static_cast<Acc*>(state);
+    void* args[] = {&F, &n, &partials, &d_misc, &st};
+    return jit_launch(jk, grid_cap, tiles, smem, args, s);
+  }
   if (staged)
     k_join_aggregate<true><<<grid, kRowBlock, smem, s>>>(F, fact->rows, partials, d_misc, static_cast<Acc*>(state));
   else

@@ -8,7 +8,9 @@
 // depend on which block finished last.
 #pragma once
 
+#ifndef __CUDACC_RTC__
 #include <limits.h>
+#endif
 #include "yq_vm.cuh"
 
 namespace yq {

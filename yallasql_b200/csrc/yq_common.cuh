@@ -1,13 +1,34 @@
 // Shared device/host plumbing for the yq kernels (sm_100a).
 #pragma once
 
+#ifdef __CUDACC_RTC__
+// Program-specialised kernels are compiled at run time (jit.cu) without the
+// system headers: the fixed-width types and limits device code uses are here.
+typedef signed char int8_t;
+typedef unsigned char uint8_t;
+typedef short int16_t;
+typedef unsigned short uint16_t;
+typedef int int32_t;
+typedef unsigned int uint32_t;
+typedef long long int64_t;
+typedef unsigned long long uint64_t;
+typedef unsigned long uintptr_t;
+typedef decltype(sizeof(0)) size_t;
+#define INT32_MIN (-2147483647 - 1)
+#define INT32_MAX 2147483647
+#define LLONG_MAX 9223372036854775807LL
+#define LLONG_MIN (-LLONG_MAX - 1LL)
+#else
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stddef.h>
+#endif
 
 #include "../../include/yq_ops.h"
 
 namespace yq {
+
+#ifndef __CUDACC_RTC__
 
 // ------------------------------------------------------------------ errors
 void set_cuda_error(cudaError_t e);
@@ -57,8 +78,12 @@ int h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s);
 
 int sm_count();
 
+#endif  // !__CUDACC_RTC__
+
 template <typename T>
 __host__ __device__ inline T ceil_div(T a, T b) { return (a + b - 1) / b; }
+
+#ifndef __CUDACC_RTC__
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -111,6 +136,8 @@ struct WsSize {
   void add(size_t count) { used = align_up(used, 256) + count * sizeof(T); }
   size_t total() const { return align_up(used, 256) + 256; }
 };
+
+#endif  // !__CUDACC_RTC__
 
 // ---------------------------------------------------------- device helpers
 // Bound on every spin wait: ~2^22 polls with a 64-256 ns back-off is well

@@ -1,0 +1,21 @@
+// Program-specialised row kernels (jit.cu): host interface.
+#pragma once
+
+#include "yq_vm.cuh"
+
+namespace yq {
+
+enum JitKind { JIT_FILTER_AGG = 0, JIT_FILTER_AGG_SEG = 1, JIT_FILTER_PROJECT = 2, JIT_JOIN_AGG = 3 };
+
+// Kernel for `kind` (staged or not) that runs P's resolved instructions
+// [0, seg0_end) as segment 0 and [seg0_end, end) as segment 1, compiled for
+// this program (cached by its instruction words; constants stay parameters).
+// Null when runtime compilation is switched off or unavailable, or failed:
+// the caller then launches the interpreter kernel, which computes the same.
+const void* jit_kernel(JitKind kind, bool staged, const VmProgram& P, int seg0_end, int end);
+
+// Launch helper for a kernel jit_kernel returned: raises its dynamic shared
+// memory limit when needed and sizes a persistent grid (at most `steps`).
+int jit_launch(const void* kernel, int max_grid, uint32_t steps, size_t smem, void** args, cudaStream_t s);
+
+}  // namespace yq

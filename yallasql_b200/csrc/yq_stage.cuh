@@ -10,7 +10,9 @@
 // last rows of the batch) is copied with plain loads and zero padded.
 #pragma once
 
+#ifndef __CUDACC_RTC__
 #include <string.h>
+#endif
 #include "yq_vm.cuh"
 
 namespace yq {
@@ -35,6 +37,7 @@ struct StagePlan {
   StageCopy c[2 * YQ_MAX_BATCH_COLUMNS];
 };
 
+#ifndef __CUDACC_RTC__
 // Lays the columns of `mask` out in one stage and sizes the ring. Returns
 // false (nstages = 0) when a column or null array is not 16-byte aligned,
 // when there is nothing to stage, or when fewer than two stages fit.
@@ -67,10 +70,13 @@ inline bool plan_stages(VmProgram& P, uint32_t mask, StagePlan& SP) {
   SP.tx_bytes = off;
   return true;
 }
+#endif
 
+#ifndef __CUDACC_RTC__
 inline size_t stage_smem_bytes(const StagePlan& SP) {
   return SP.nstages ? (size_t)SP.nstages * SP.stage_bytes + (size_t)SP.nstages * 8 : 0;
 }
+#endif
 
 __device__ __forceinline__ uint64_t* stage_bar(const StagePlan& SP, int slot) {
   return reinterpret_cast<uint64_t*>(yq_dyn_smem + (size_t)SP.nstages * SP.stage_bytes) + slot;
@@ -151,6 +157,7 @@ __device__ __forceinline__ uint32_t in_range_bits(uint32_t row0, uint32_t n) {
   return left >= (uint32_t)ITEMS ? kItemsMask : ((1u << left) - 1u);
 }
 
+#ifndef __CUDACC_RTC__
 // Columns an expression program reads (plus `extra`).
 inline uint32_t program_columns(const VmProgram& P, int end, uint32_t extra) {
   uint32_t mask = extra;
@@ -165,7 +172,9 @@ inline uint32_t program_columns(const VmProgram& P, int end, uint32_t extra) {
   }
   return mask;
 }
+#endif
 
+#ifndef __CUDACC_RTC__
 // Bytes per row of the columns in `mask` (plus null bytes).
 inline double row_bytes_of(const VmProgram& P, uint32_t mask) {
   double b = 0;
@@ -173,5 +182,6 @@ inline double row_bytes_of(const VmProgram& P, uint32_t mask) {
     if (mask >> c & 1u) b += P.cols[c].width + (P.cols[c].nulls ? 1 : 0);
   return b;
 }
+#endif
 
 }  // namespace yq
