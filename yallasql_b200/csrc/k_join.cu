@@ -736,8 +736,9 @@ int yq_join_aggregate(const yq_batch* fact, const yq_program* fact_predicate, in
   int grid = sm_count() * per_sm;
   if ((uint32_t)grid > tiles) grid = (int)tiles;
   const double row_bytes = row_bytes_of(F.P, program_columns(F.P, F.pc_end, 1u << fact_key));
+  const void* jk = jit_kernel(JIT_JOIN_AGG, staged, F.P, F.pred_end, F.pc_end);
   ProfScope ps("join_aggregate", s, (double)fact->rows * row_bytes);
-  if (const void* jk = jit_kernel(JIT_JOIN_AGG, staged, F.P, F.pred_end, F.pc_end)) {
+  if (jk) {
     uint32_t n = fact->rows;
     Acc* st = static_cast<Acc*>(state);
     void* args[] = {&F, &n, &partials, &d_misc, &st};
