@@ -121,6 +121,33 @@ def test_where_projection_matches_oracle(cuda, rows):
         np.testing.assert_array_equal(v[valid], np.asarray(wv)[wvalid].astype(v.dtype))
 
 
+# Batches long enough that one claimed chunk spans several 1,024-row steps,
+# with a last chunk that ends early (its missing steps sit between the
+# predicate pass and the output pass of the ring).
+@pytest.mark.parametrize("jit", [True, False])
+@pytest.mark.parametrize("rows", [2_500_001, 5_000_000, 9_437_185])
+def test_sales_projection_multi_step_chunks(cuda, rows, jit):
+    t = datagen.sales_table(rows, seed=11)
+    cols = [t["price"], t["qty"], t["discount"], t["category"]]
+    price, disc = ColumnRef(0, A.FLOAT32), ColumnRef(2, A.INT32)
+    pred, _ = sales_query_exprs()
+    select = [3, 0, Arith(A.MUL, price, Cast(disc, A.FLOAT32)), 1]
+    lib = ops.lib()
+    prev = lib.yq_jit_enable(1 if jit else 0)
+    try:
+        out = ops.filter_project(dev_batch(cols), pred, select)
+    finally:
+        lib.yq_jit_enable(prev)
+    keep = ((t["discount"] >= 1) & (t["discount"] <= 3) & (t["qty"] < 25) &
+            np.any(t["category"] != datagen.text_slots([datagen.EXCLUDED_CATEGORY])[0], axis=1))
+    assert out.rows == int(keep.sum())
+    np.testing.assert_array_equal(host(out.columns[0])[0], t["category"][keep])
+    np.testing.assert_array_equal(host(out.columns[1])[0], t["price"][keep])
+    np.testing.assert_array_equal(host(out.columns[2])[0],
+                                  (t["price"] * t["discount"].astype(np.float32))[keep])
+    np.testing.assert_array_equal(host(out.columns[3])[0], t["qty"][keep])
+
+
 def test_projection_capacity_reported(cuda):
     rng = np.random.default_rng(3)
     x = rng.integers(0, 100, 10_000).astype(np.int32)

@@ -27,6 +27,7 @@
 #include <vector>
 #include <nvrtc.h>  // types and prototypes only
 #include "yq_jit.cuh"
+#include "yq_stage.cuh"
 
 // Device headers embedded by the build (yallasql_b200/build.py).
 extern const int yq_jit_header_count;
@@ -107,7 +108,7 @@ const char* kernel_decl(JitKind kind) {
   }
 }
 
-std::string make_source(JitKind kind, bool staged, const VmProgram& P, int seg0_end, int end) {
+std::string make_source(JitKind kind, bool staged, const VmProgram& P, int seg0_end, int end, int min_blocks) {
   std::string s;
   s += "#include \"row_kernels.cuh\"\n#define STAGED_ ";
   s += staged ? "true" : "false";
@@ -128,7 +129,7 @@ std::string make_source(JitKind kind, bool staged, const VmProgram& P, int seg0_
     }
   }
   s += "    }\n  }\n};\n}  // namespace yq\n";
-  s += "extern \"C\" __global__ void __launch_bounds__(256, 2) yq_jit_kernel";
+  s += "extern \"C\" __global__ void __launch_bounds__(256, " + std::to_string(min_blocks) + ") yq_jit_kernel";
   s += kernel_decl(kind);
   s += "\n";
   return s;
@@ -145,7 +146,20 @@ std::string cache_key(JitKind kind, bool staged, const VmProgram& P, int seg0_en
   return k;
 }
 
-const void* compile_locked(const std::string& src) {
+// Spill stores ptxas reported for the kernel entry (-1 when not found).
+long entry_spills(const std::string& log) {
+  const size_t at = log.find("Function properties for yq_jit_kernel");
+  if (at == std::string::npos) return -1;
+  const size_t sp = log.find("bytes spill stores", at);
+  if (sp == std::string::npos) return -1;
+  const size_t b = log.rfind(',', sp);  // "N bytes stack frame, N bytes spill stores"
+  if (b == std::string::npos || b < at) return -1;
+  return strtol(log.c_str() + b + 1, nullptr, 10);
+}
+
+// Compiles and loads one kernel source. `spills` receives the entry's spill
+// stores as ptxas reported them.
+const void* compile_locked(const std::string& src, long* spills) {
   nvrtcProgram prog = nullptr;
   if (g_nvrtc.create(&prog, src.c_str(), "yq_jit.cu", yq_jit_header_count, yq_jit_header_texts,
                      yq_jit_header_names) != NVRTC_SUCCESS) {
@@ -154,13 +168,15 @@ const void* compile_locked(const std::string& src) {
   }
   // -default-device: the C declarations of the public header are never defined
   // or called here; 9 = nested comment in the header's prose.
-  const char* opts[] = {"-arch=sm_100a", "-std=c++17", "-DNDEBUG", "-default-device", "-diag-suppress=9"};
-  const nvrtcResult r = g_nvrtc.compile(prog, 5, opts);
+  const char* opts[] = {"-arch=sm_100a", "-std=c++17", "-DNDEBUG", "-default-device", "-diag-suppress=9",
+                        "--ptxas-options=-v"};
+  const nvrtcResult r = g_nvrtc.compile(prog, 6, opts);
   size_t ls = 0;
   g_nvrtc.log_size(prog, &ls);
   std::string log(ls, '\0');
   if (ls) g_nvrtc.log(prog, &log[0]);
   g_last_log = log;
+  *spills = entry_spills(log);
   const void* kernel = nullptr;
   if (r == NVRTC_SUCCESS) {
     size_t n = 0;
@@ -197,7 +213,13 @@ const void* jit_kernel(JitKind kind, bool staged, const VmProgram& P, int seg0_e
   const void* k = nullptr;
   if (open_nvrtc()) {
     const auto t0 = std::chrono::steady_clock::now();
-    k = compile_locked(make_source(kind, staged, P, seg0_end, end));
+    // Registers for four blocks of 256 threads per SM (64 a thread) when the
+    // kernel fits them without spilling, else for three, else for two.
+    long spills = 0;
+    for (int blocks = 4; blocks >= 2; --blocks) {
+      k = compile_locked(make_source(kind, staged, P, seg0_end, end, blocks), &spills);
+      if (!k || spills == 0) break;
+    }
     g_compile_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
   if (k) ++g_compiled;
@@ -206,16 +228,90 @@ const void* jit_kernel(JitKind kind, bool staged, const VmProgram& P, int seg0_e
   return k;
 }
 
+namespace {
+
+std::mutex g_launch_mu;
+std::unordered_map<std::string, size_t> g_smem_cap;  // dynamic shared memory a kernel allows, per device
+std::unordered_map<std::string, int> g_resident;     // blocks per SM per (kernel, shared memory, device)
+std::unordered_map<std::string, int> g_depth;        // ring depth per (kernel, stage bytes, device)
+
+std::string launch_key(const void* kernel, size_t extra, int dev) {
+  std::string k(reinterpret_cast<const char*>(&kernel), sizeof(kernel));
+  k.append(reinterpret_cast<const char*>(&extra), sizeof(extra));
+  k.append(reinterpret_cast<const char*>(&dev), sizeof(dev));
+  return k;
+}
+
+// Lets `kernel` take `smem` bytes of dynamic shared memory on `dev`. The cap
+// only ever rises, so a launch with less never lowers what another needs.
+cudaError_t allow_smem_locked(const void* kernel, size_t smem, int dev) {
+  if (smem <= 48 * 1024) return cudaSuccess;
+  size_t& cap = g_smem_cap[launch_key(kernel, 0, dev)];
+  if (smem <= cap) return cudaSuccess;
+  cudaKernel_t k = reinterpret_cast<cudaKernel_t>(const_cast<void*>(kernel));
+  const cudaError_t e = cudaKernelSetAttributeForDevice(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem, dev);
+  if (e == cudaSuccess) cap = smem;
+  return e;
+}
+
+// Blocks of 256 threads per SM (0 when the shared memory cannot be allowed).
+int resident_locked(const void* kernel, size_t smem, int dev) {
+  const std::string key = launch_key(kernel, smem, dev);
+  auto it = g_resident.find(key);
+  if (it != g_resident.end()) return it->second;
+  int per_sm = 0;
+  if (allow_smem_locked(kernel, smem, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem) != cudaSuccess)
+    per_sm = 0;
+  cudaGetLastError();
+  g_resident.emplace(key, per_sm);
+  return per_sm;
+}
+
+}  // namespace
+
+int jit_stages(const void* kernel, uint32_t stage_bytes, int nstages) {
+  if (!kernel || nstages < 2 || stage_bytes == 0) return nstages;
+  static int fit = -1;
+  std::lock_guard<std::mutex> lk(g_launch_mu);
+  if (fit < 0) {
+    const char* e = getenv("YQ_STAGE_FIT");
+    fit = (e && e[0] == '0') ? 0 : 1;
+  }
+  if (!fit) return nstages;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return nstages;
+  }
+  const std::string key = launch_key(kernel, stage_bytes, dev);
+  auto it = g_depth.find(key);
+  if (it != g_depth.end()) return it->second;
+  int best = nstages, best_blocks = 0;
+  for (int ns = 2; ns <= kStageMax; ++ns) {  // deeper on a tie
+    const int per_sm = resident_locked(kernel, (size_t)ns * stage_bytes + (size_t)ns * 8, dev);
+    if (per_sm == 0) break;
+    if (per_sm >= best_blocks) {
+      best_blocks = per_sm;
+      best = ns;
+    }
+  }
+  g_depth.emplace(key, best);
+  return best;
+}
+
 int jit_launch(const void* kernel, int max_grid, uint32_t steps, size_t smem, void** args, cudaStream_t s) {
   int dev = 0;
   YQ_TRY_CUDA(cudaGetDevice(&dev));
-  cudaKernel_t k = reinterpret_cast<cudaKernel_t>(const_cast<void*>(kernel));
-  if (smem > 48 * 1024)
-    YQ_TRY_CUDA(cudaKernelSetAttributeForDevice(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem, dev));
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem) != cudaSuccess || per_sm < 1) {
-    cudaGetLastError();
-    per_sm = 2;
+  {
+    std::lock_guard<std::mutex> lk(g_launch_mu);
+    per_sm = resident_locked(kernel, smem, dev);
+    if (per_sm == 0) {  // shared memory not allowed: report it
+      const cudaError_t e = allow_smem_locked(kernel, smem, dev);
+      set_cuda_error(e == cudaSuccess ? cudaErrorInvalidConfiguration : e);
+      return YQ_ERR_CUDA;
+    }
   }
   int grid = per_sm * sm_count();
   if (grid > max_grid) grid = max_grid;

@@ -9,6 +9,7 @@
 // reads are staged in shared memory a few steps ahead by bulk copies
 // (yq_stage.cuh) when they are 16-byte aligned and fit; otherwise the kernel
 // reads them from global memory directly.
+#include <algorithm>
 #include <vector>
 #include "vm_host.cuh"
 #include "row_kernels.cuh"
@@ -146,8 +147,10 @@ static int launch_filter_aggregate(const FAParams& F, uint32_t rows, Acc* partia
   const void* jk = jit_kernel(JIT_FILTER_AGG, staged, F.P, F.pc_end, F.pc_end);  // compiles once, outside the timing
   ProfScope ps("filter_aggregate", s, (double)rows * row_bytes_of(F.P, program_columns(F.P, F.pc_end, 0)));
   if (jk) {
-    void* args[] = {const_cast<FAParams*>(&F), &rows, &partials, &ticket, &state};
-    return jit_launch(jk, (int)max_row_grid(), ceil_div<uint32_t>(rows, kStepRows), smem, args, s);
+    FAParams G = F;
+    if (staged) G.SP.nstages = jit_stages(jk, G.SP.stage_bytes, G.SP.nstages);
+    void* args[] = {&G, &rows, &partials, &ticket, &state};
+    return jit_launch(jk, (int)max_row_grid(), ceil_div<uint32_t>(rows, kStepRows), stage_smem_bytes(G.SP), args, s);
   }
   if (staged)
     k_filter_aggregate<true><<<grid, kRowBlock, smem, s>>>(F, rows, partials, ticket, state);
@@ -164,21 +167,48 @@ __global__ void __launch_bounds__(kRowBlock, 2) k_filter_aggregate_seg(const __g
   filter_aggregate_seg_body<STAGED, InterpRunner>(Q);
 }
 
-// One warp per task: aggregate a < nagg folds the task's step partials in order.
-__global__ void k_agg_seg_fold(const Acc* __restrict__ partials, const uint32_t* __restrict__ step0, int nseg,
-                               const AggParams A, Acc* states, const uint32_t* err) {
+// One block per task folds the task's step partials: thread t takes steps
+// t, t + kFoldBlock, ... of the task, then the warps and the block combine
+// them in a fixed order, so the result is deterministic.
+constexpr int kFoldBlock = 256;
+
+__global__ void __launch_bounds__(kFoldBlock) k_agg_seg_fold(const Acc* __restrict__ partials,
+                                                             const uint32_t* __restrict__ step0, int nseg,
+                                                             const AggParams A, Acc* states, const uint32_t* err) {
+  __shared__ Acc s_acc[kFoldBlock / 32][YQ_MAX_AGGREGATES];
   const int g = blockIdx.x;
-  const int a = threadIdx.x;
   if (g >= nseg) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   Acc* st = reinterpret_cast<Acc*>(reinterpret_cast<char*>(states) + (size_t)g * kAggStateBytes);
-  if (a == 0 && *err) *agg_state_err(st) |= *err;
+  if (threadIdx.x == 0 && *err) *agg_state_err(st) |= *err;
+  const uint32_t s0 = step0[g], s1 = step0[g + 1];
+#pragma unroll
+  for (int a = 0; a < YQ_MAX_AGGREGATES; ++a) {
+    if (a < A.nagg) {
+      const int upd = A.upd[a];
+      long long c = 0;
+      unsigned long long v = acc_identity(upd);
+      for (uint32_t s = s0 + threadIdx.x; s < s1; s += kFoldBlock) {
+        const Acc p = partials[(size_t)s * YQ_MAX_AGGREGATES + a];
+        c += p.cnt;
+        v = acc_merge(upd, v, p.bits);
+      }
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) {
+        c += __shfl_down_sync(0xffffffffu, c, d);
+        v = acc_merge(upd, v, __shfl_down_sync(0xffffffffu, v, d));
+      }
+      if (lane == 0) s_acc[warp][a] = Acc{c, v};
+    }
+  }
+  __syncthreads();
+  const int a = threadIdx.x;
   if (a >= A.nagg) return;
   const int upd = A.upd[a];
-  Acc t{0, acc_identity(upd)};
-  for (uint32_t s = step0[g]; s < step0[g + 1]; ++s) {
-    const Acc p = partials[(size_t)s * YQ_MAX_AGGREGATES + a];
-    t.cnt += p.cnt;
-    t.bits = acc_merge(upd, t.bits, p.bits);
+  Acc t = s_acc[0][a];
+  for (int w = 1; w < kFoldBlock / 32; ++w) {
+    t.cnt += s_acc[w][a].cnt;
+    t.bits = acc_merge(upd, t.bits, s_acc[w][a].bits);
   }
   Acc cur = st[a];
   cur.cnt += t.cnt;
@@ -200,10 +230,10 @@ static uint32_t seg_steps(const uint32_t* begin, const uint32_t* end, int nseg, 
 // ================================================================ project
 template <bool STAGED>
 __global__ void __launch_bounds__(kRowBlock, 2) k_filter_project(const __grid_constant__ FPParams F, uint32_t n,
-                                                                 uint32_t* tile_counter,
+                                                                 uint32_t* chunk_counter,
                                                                  unsigned long long* __restrict__ status,
                                                                  uint32_t* out_count, uint32_t* err) {
-  filter_project_body<STAGED, InterpRunner>(F, n, tile_counter, status, out_count, err);
+  filter_project_body<STAGED, InterpRunner>(F, n, chunk_counter, status, out_count, err);
 }
 
 // Validation and program build shared by yq_filter_project and its
@@ -244,7 +274,10 @@ static int build_project_params(const yq_batch* batch, const yq_program* predica
     }
   }
   YQ_TRY(B.finalize());
-  if (!plan_stages(B.P, B.used_cols | copy_mask, F.SP)) F.SP.nstages = 0;
+  // Pass 0 stages what the predicate reads, pass 1 what the output reads.
+  const int pe = B.remap[pred_end];
+  if (!plan_stages2(B.P, program_columns_in(B.P, 0, pe, 0), program_columns_in(B.P, pe, B.len, copy_mask), F.SP))
+    F.SP.nstages = 0;
   memcpy(&F.P, &B.P, sizeof(VmProgram));
   F.pred_end = B.remap[pred_end];
   F.proj_end = B.len;
@@ -253,11 +286,14 @@ static int build_project_params(const yq_batch* batch, const yq_program* predica
   return YQ_OK;
 }
 
-// Launch over `rows` rows with look-back scratch `status` (one word per tile
-// plus one) and `misc` = {tile counter, error word} (both zeroed).
-static int launch_filter_project(const FPParams& F, uint32_t rows, uint32_t* misc, unsigned long long* status,
+// Launch over `rows` rows with look-back scratch `status` (one word per
+// 1,024-row step plus one; a chunk of steps uses one) and `misc` = {chunk
+// counter, error word} (both zeroed). Chunks are as long as keeps about eight
+// of them per SM (at most 8 steps), so a batch still spreads over every SM.
+static int launch_filter_project(FPParams& F, uint32_t rows, uint32_t* misc, unsigned long long* status,
                                  uint32_t* cnt_dev, cudaStream_t s, bool allow_jit = true) {
   const bool staged = F.SP.nstages > 0;
+  F.csteps = std::max<uint32_t>(1u, std::min<uint32_t>(8u, ceil_div<uint32_t>(rows, kStepRows) / (8u * sm_count())));
   const void* kern = staged ? (const void*)k_filter_project<true> : (const void*)k_filter_project<false>;
   const size_t smem = stage_smem_bytes(F.SP);
   static size_t done_smem = 0;
@@ -272,8 +308,9 @@ static int launch_filter_project(const FPParams& F, uint32_t rows, uint32_t* mis
   ProfScope ps("filter_project", s, (double)rows * row_bytes_of(F.P, mask));
   if (jk) {
     uint32_t* err = misc + 1;
-    void* args[] = {const_cast<FPParams*>(&F), &rows, &misc, &status, &cnt_dev, &err};
-    return jit_launch(jk, 1 << 30, ceil_div<uint32_t>(rows, kStepRows), smem, args, s);
+    if (staged) F.SP.nstages = jit_stages(jk, F.SP.stage_bytes, F.SP.nstages);
+    void* args[] = {&F, &rows, &misc, &status, &cnt_dev, &err};
+    return jit_launch(jk, 1 << 30, ceil_div<uint32_t>(rows, kStepRows), stage_smem_bytes(F.SP), args, s);
   }
   if (staged)
     k_filter_project<true><<<grid, kRowBlock, smem, s>>>(F, rows, misc, status, cnt_dev, misc + 1);
@@ -489,15 +526,16 @@ static int filter_aggregate_ranges(const yq_batch* batch, const uint32_t* begin,
     const void* jk = jit_kernel(JIT_FILTER_AGG_SEG, staged, Q.F.P, Q.F.pc_end, Q.F.pc_end);
     ProfScope ps("filter_aggregate_seg", s, rows * row_bytes_of(Q.F.P, program_columns(Q.F.P, Q.F.pc_end, 0)));
     if (jk) {
+      if (staged) Q.F.SP.nstages = jit_stages(jk, Q.F.SP.stage_bytes, Q.F.SP.nstages);
       void* args[] = {&Q};
-      YQ_TRY(jit_launch(jk, (int)max_row_grid(), nsteps, smem, args, s));
+      YQ_TRY(jit_launch(jk, (int)max_row_grid(), nsteps, stage_smem_bytes(Q.F.SP), args, s));
     } else if (staged)
       k_filter_aggregate_seg<true><<<grid, kRowBlock, smem, s>>>(Q);
     else
       k_filter_aggregate_seg<false><<<grid, kRowBlock, 0, s>>>(Q);
     YQ_CHECK_LAUNCH();
   }
-  k_agg_seg_fold<<<nseg, 32, 0, s>>>(partials, d_step0, nseg, Q.F.A, static_cast<Acc*>(states), d_err);
+  k_agg_seg_fold<<<nseg, kFoldBlock, 0, s>>>(partials, d_step0, nseg, Q.F.A, static_cast<Acc*>(states), d_err);
   YQ_CHECK_LAUNCH();
   return YQ_OK;
 }
@@ -554,7 +592,7 @@ int yq_filter_project(const yq_batch* batch, const yq_program* predicate, const 
   Workspace ws;
   YQ_TRY(ws.acquire(workspace, workspace_bytes, yq_filter_project_workspace_size(rows), s));
   unsigned long long* status = ws.take<unsigned long long>((size_t)ntiles + 1);
-  uint32_t* misc = ws.take<uint32_t>(4);  // [0] tile counter, [1] error, [2] count
+  uint32_t* misc = ws.take<uint32_t>(4);  // [0] chunk counter, [1] error, [2] count
   YQ_TRY_CUDA(cudaMemsetAsync(status, 0, ((size_t)ntiles + 1) * sizeof(unsigned long long), s));
   YQ_TRY_CUDA(cudaMemsetAsync(misc, 0, 4 * sizeof(uint32_t), s));
   uint32_t* cnt_dev = count_device ? count_device : misc + 2;
@@ -577,8 +615,8 @@ int yq_filter_project(const yq_batch* batch, const yq_program* predicate, const 
 // yq_filter_project_noalloc runs the same kernel as yq_filter_project, but its
 // look-back scratch is this file-scope device array instead of a workspace
 // the caller passes or the library allocates. Layout: four 32-bit counters
-// (tile counter, error word, row count, spare), then one 64-bit look-back
-// status word per 1,024-row tile plus one.
+// (chunk counter, error word, row count, spare), then one 64-bit look-back
+// status word per 1,024-row step plus one (a chunk of steps uses one).
 #include <mutex>
 
 namespace yq {
@@ -630,7 +668,7 @@ extern "C" int yq_filter_project_noalloc(const yq_batch* batch, const yq_program
   unsigned long long* scratch = nullptr;
   YQ_TRY(noalloc_scratch(&scratch));
   const uint32_t ntiles = ceil_div<uint32_t>(rows, kStepRows);
-  uint32_t* misc = reinterpret_cast<uint32_t*>(scratch);  // [0] tile counter, [1] error, [2] count
+  uint32_t* misc = reinterpret_cast<uint32_t*>(scratch);  // [0] chunk counter, [1] error, [2] count
   unsigned long long* status = scratch + 2;
   // The previous call's values are still there: clear what this call reads.
   YQ_TRY_CUDA(cudaMemsetAsync(scratch, 0, (2 + (size_t)ntiles + 1) * sizeof(unsigned long long), s));

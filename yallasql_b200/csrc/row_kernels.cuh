@@ -199,32 +199,54 @@ struct FPParams {
   int32_t proj_end;
   int32_t nproj;
   uint32_t capacity;
+  uint32_t csteps;  // 1,024-row steps per claimed chunk (1..8)
   DevOut out[YQ_MAX_PROJECTIONS];
 };
 
+// One warp's lists in the output pass: its selected rows in input order (row
+// within the step) and, for the projection program being emitted, their values.
+struct WarpOut {
+  uint16_t rows[ITEMS * 32];
+  unsigned long long vals[ITEMS * 32];
+  uint8_t ok[ITEMS * 32];
+};
+
+// Output rows of a warp are consecutive: entry i of its lists goes to output
+// row wbase + i, written by lane i % 32, so a warp's stores are coalesced
+// whatever rows were selected.
 struct ProjEmit {
   uint32_t sel;
-  uint32_t pos;
+  uint32_t pos;  // this thread's first output row
   const FPParams* F;
+  WarpOut* W;             // this warp's lists (output pass only)
+  uint32_t wbase, wcount;  // the warp's first output row and its selected rows
+  uint32_t first;         // this thread's first entry in the lists
   __device__ __forceinline__ void pred(uint32_t bits) { sel &= bits; }
   template <int K>
   __device__ __forceinline__ void agg(int, const Val&) {}
-  template <int W>
+  template <int WD>
   __device__ __forceinline__ void proj(int p, const Val& x) {
     const DevOut& o = F->out[p];
-    uint32_t q = pos;
+    uint32_t e = first;
 #pragma unroll
     for (int k = 0; k < ITEMS; ++k) {
       if (sel >> k & 1u) {
-        if (q < F->capacity) {
-          if constexpr (W == 0) reinterpret_cast<uint8_t*>(o.data)[q] = (uint8_t)((x.v[0] >> k) & 1u);
-          else if constexpr (W == 1) reinterpret_cast<uint32_t*>(o.data)[q] = (uint32_t)x.v[k];
-          else reinterpret_cast<unsigned long long*>(o.data)[q] = x.v[k];
-          if (o.nulls) o.nulls[q] = (x.valid >> k & 1u) ? 0 : 1;
-        }
-        ++q;
+        W->vals[e] = WD == 0 ? ((x.v[0] >> k) & 1u) : x.v[k];
+        W->ok[e] = (uint8_t)((x.valid >> k) & 1u);
+        ++e;
       }
     }
+    __syncwarp();
+    const uint32_t cap = F->capacity;
+    for (uint32_t i = threadIdx.x & 31u; i < wcount; i += 32) {
+      const uint32_t q = wbase + i;
+      if (q >= cap) break;
+      if constexpr (WD == 0) reinterpret_cast<uint8_t*>(o.data)[q] = (uint8_t)W->vals[i];
+      else if constexpr (WD == 1) reinterpret_cast<uint32_t*>(o.data)[q] = (uint32_t)W->vals[i];
+      else reinterpret_cast<unsigned long long*>(o.data)[q] = W->vals[i];
+      if (o.nulls) o.nulls[q] = W->ok[i] ? 0 : 1;
+    }
+    __syncwarp();
   }
 };
 
@@ -245,111 +267,162 @@ __device__ __forceinline__ void copy_cell_any(char* dst, const char* src, int wi
   }
 }
 
-// Projections that copy an input column: selected rows to positions pos, pos+1, ...
+// Projections that copy an input column: the warp's selected rows (listed in
+// E.W->rows) to output rows E.wbase, E.wbase + 1, ..., lane i % 32 copying
+// entry i.
 template <bool STAGED>
-__device__ __forceinline__ void copy_source_columns(const FPParams& F, const Ctx& X, uint32_t sel, uint32_t pos) {
+__device__ __forceinline__ void copy_source_columns(const FPParams& F, const Ctx& X, const ProjEmit& E) {
   for (int p = 0; p < F.nproj; ++p) {
     const DevOut& o = F.out[p];
     if (o.src_col < 0) continue;
     const DevCol& c = F.P.cols[o.src_col];
-    uint32_t q = pos;
-#pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
-      if (sel >> k & 1u) {
-        if (q < F.capacity) {
-          const uint32_t lr = X.lr + k;
-          const char* src;
-          uint8_t nul = 0;
-          if constexpr (STAGED) {
-            src = reinterpret_cast<const char*>(yq_dyn_smem + X.stage + c.soff + lr * (uint32_t)c.width);
-            if (c.nulls) nul = yq_dyn_smem[X.stage + c.snoff + lr];
-          } else {
-            src = c.data + (size_t)(X.tile0 + lr) * c.width;
-            if (c.nulls) nul = c.nulls[X.tile0 + lr];
-          }
-          copy_cell_any(o.data + (size_t)q * o.width, src, c.width);
-          if (o.nulls) o.nulls[q] = nul;
-        }
-        ++q;
+    const uint32_t w = (uint32_t)c.width;
+    for (uint32_t i = threadIdx.x & 31u; i < E.wcount; i += 32) {
+      const uint32_t q = E.wbase + i;
+      if (q >= F.capacity) break;
+      const uint32_t lr = E.W->rows[i];
+      const char* src;
+      uint8_t nul = 0;
+      if constexpr (STAGED) {
+        src = reinterpret_cast<const char*>(yq_dyn_smem + X.stage + c.soff + lr * w);
+        if (c.nulls) nul = yq_dyn_smem[X.stage + c.snoff + lr];
+      } else {
+        src = c.data + (size_t)(X.tile0 + lr) * w;
+        if (c.nulls) nul = c.nulls[X.tile0 + lr];
       }
+      copy_cell_any(o.data + (size_t)q * w, src, (int)w);
+      if (o.nulls) o.nulls[q] = nul;
     }
   }
 }
 
-// Tiles are claimed in order from a counter (a few steps ahead when staged),
-// every block processes its claims in order, so each tile's predecessors are
-// held by running blocks and the decoupled look-back always completes.
+// Rows are cut into chunks of F.csteps 1,024-row steps. Chunks are claimed in
+// order from a counter (when the staging ring reaches the next one), and every
+// block processes its claims in order, so each chunk's predecessors are held
+// by running blocks and the decoupled look-back always completes.
+//
+// A chunk is 2 * csteps ring steps. The first csteps run the predicate over
+// the staged predicate columns and keep each thread's 4 selection bits per
+// step (at most 8 steps: one word). Then one block scan turns the per-step
+// counts into output positions and one look-back gives the chunk's first
+// output row, while the ring is already loading the same steps again with the
+// columns the output reads (pass 1 of the stage plan; the chunk was just
+// streamed, so these copies mostly hit L2). The last csteps run the
+// projection programs and copy the source columns for the selected rows.
+// Output rows keep input order.
 template <bool STAGED, typename R>
-__device__ __forceinline__ void filter_project_body(const FPParams& F, uint32_t n,
-                                                                 uint32_t* tile_counter,
-                                                                 unsigned long long* __restrict__ status,
-                                                                 uint32_t* out_count, uint32_t* err) {
-  __shared__ uint32_t s_tiles[kStageMax];
-  __shared__ uint32_t s_warp[kRowBlock / 32 + 1];
+__device__ __forceinline__ void filter_project_body(const FPParams& F, uint32_t n, uint32_t* chunk_counter,
+                                                    unsigned long long* __restrict__ status, uint32_t* out_count,
+                                                    uint32_t* err) {
+  constexpr uint32_t Q = 8;  // claimed chunk ids kept: the current one through the one being prefetched
+  __shared__ uint32_t s_claims[Q];
+  __shared__ unsigned long long s_scan[2 * (kRowBlock / 32 + 1)];
   __shared__ unsigned long long s_prefix;
-  const uint32_t ntiles = ceil_div<uint32_t>(n, kStepRows);
-  int S = 1;
+  __shared__ WarpOut s_out[kRowBlock / 32];
+  const uint32_t nsteps = ceil_div<uint32_t>(n, kStepRows);
+  const uint32_t C = F.csteps;  // 1..8
+  const uint32_t V = 2 * C;     // ring steps per chunk
+  const uint32_t nchunks = ceil_div<uint32_t>(nsteps, C);
+  uint32_t S = 1;
   if constexpr (STAGED) {
-    S = F.SP.nstages;
+    S = (uint32_t)F.SP.nstages;
     stage_init(F.SP);
   }
-  if (threadIdx.x == 0)
-    for (int j = 0; j < S - 1; ++j) {
-      const uint32_t t = atomicAdd(tile_counter, 1u);
-      s_tiles[j] = t;
-      if constexpr (STAGED)
-        if (t < ntiles) stage_start(F.SP, j, t * kStepRows, step_rows(t, n));
-    }
-  int slot = 0;
-  uint32_t parity = 0;
-  for (;;) {
-    __syncthreads();  // every thread is done with the previous step
-    if (threadIdx.x == 0) {
-      const int ns = slot == 0 ? S - 1 : slot - 1;
-      const uint32_t t = atomicAdd(tile_counter, 1u);
-      s_tiles[ns] = t;
-      if constexpr (STAGED)
-        if (t < ntiles) stage_start(F.SP, ns, t * kStepRows, step_rows(t, n));
-    }
-    __syncthreads();
-    const uint32_t tile = s_tiles[slot];
-    if (tile >= ntiles) break;  // later claims are larger: no copy is in flight
-    Ctx X;
-    X.tile0 = tile * kStepRows;
-    X.lr = threadIdx.x * ITEMS;
-    X.inr = in_range_bits(X.tile0 + X.lr, n);
-    X.stage = 0;
-    X.vec_ok = (X.tile0 & 15u) == 0u;
+  // Thread 0: claim (at a chunk's first ring step) and start the copies of
+  // the block's ring step pv: chunk number pv / V of this block, step
+  // (pv % V) % C of it, pass (pv % V) / C.
+  // The last chunk can end before its csteps: its missing steps of pass 0
+  // come before its steps of pass 1, so each still completes its slot's
+  // barrier phase (an arrive, no copy) and every slot keeps one phase per use.
+  auto ahead = [&](uint32_t pv) {
+    if (pv % V == 0) s_claims[(pv / V) % Q] = atomicAdd(chunk_counter, 1u);
     if constexpr (STAGED) {
-      stage_finish(F.SP, slot, parity, X.tile0, step_rows(tile, n), err);
-      X.stage = (uint32_t)slot * F.SP.stage_bytes;
+      const uint32_t c = s_claims[(pv / V) % Q], r = pv % V, step = c * C + (r < C ? r : r - C);
+      if (c < nchunks) {
+        if (step < nsteps) stage_start(F.SP, (int)(pv % S), step * kStepRows, step_rows(step, n), r < C ? 0 : 1);
+        else mbar_arrive(stage_bar(F.SP, (int)(pv % S)));
+      }
     }
-    ProjEmit E;
-    E.sel = X.inr;
-    E.pos = 0;
-    E.F = &F;
-    Stack St;
-    if (F.pred_end > 0) R::template run<STAGED>(F.P, 0, 0, F.pred_end, X, St, E);
-
-    uint32_t total;
-    const uint32_t excl = block_exclusive_sum<kRowBlock>(__popc(E.sel), s_warp, total);
-    if (threadIdx.x < 32) {
-      const unsigned long long p = tile_lookback(status, tile, total, err);
-      if (threadIdx.x == 0) s_prefix = p;
+  };
+  if (threadIdx.x == 0)
+    for (uint32_t j = 0; j + 1 < S; ++j) ahead(j);
+  uint32_t selmask = 0;
+  unsigned long long ex_lo = 0, ex_hi = 0, tot_lo = 0, tot_hi = 0, run = 0;
+  for (uint32_t v = 0;; ++v) {
+    __syncthreads();  // every thread is done with the previous step: its slot is free
+    if (threadIdx.x == 0) ahead(v + S - 1);
+    if (S == 1) __syncthreads();  // the current chunk may have been claimed just now
+    const uint32_t chunk = s_claims[(v / V) % Q];
+    if (chunk >= nchunks) break;  // later claims are larger: no copy is in flight
+    const uint32_t r = v % V, j = r < C ? r : r - C, step = chunk * C + j;
+    const int pass = r < C ? 0 : 1;
+    if (step < nsteps) {
+      Ctx X;
+      X.tile0 = step * kStepRows;
+      X.lr = threadIdx.x * ITEMS;
+      X.inr = in_range_bits(X.tile0 + X.lr, n);
+      X.stage = 0;
+      X.vec_ok = (X.tile0 & 15u) == 0u;
+      if constexpr (STAGED) {
+        const uint32_t slot = v % S;
+        stage_finish(F.SP, (int)slot, (v / S) & 1u, X.tile0, step_rows(step, n), err, pass);
+        X.stage = slot * F.SP.stage_bytes;
+      }
+      ProjEmit E;
+      E.F = &F;
+      E.W = nullptr;
+      E.wbase = E.wcount = E.first = 0;
+      Stack St;
+      if (pass == 0) {
+        E.sel = X.inr;
+        E.pos = 0;
+        if (F.pred_end > 0) R::template run<STAGED>(F.P, 0, 0, F.pred_end, X, St, E);
+        selmask |= E.sel << (4 * j);
+      } else {
+        const uint32_t sh = 16u * (j & 3u);
+        E.sel = (selmask >> (4 * j)) & 15u;
+        E.pos = (uint32_t)(run + (((j < 4 ? ex_lo : ex_hi) >> sh) & 0xffffu));
+        if (__any_sync(0xffffffffu, E.sel != 0u)) {
+          E.W = &s_out[threadIdx.x >> 5];
+          E.wbase = __shfl_sync(0xffffffffu, E.pos, 0);
+          E.first = E.pos - E.wbase;
+          E.wcount = __shfl_sync(0xffffffffu, E.first + (uint32_t)__popc(E.sel), 31);
+          uint32_t e = E.first;
+#pragma unroll
+          for (int k = 0; k < ITEMS; ++k)
+            if (E.sel >> k & 1u) E.W->rows[e++] = (uint16_t)(X.lr + k);
+          __syncwarp();
+          if (F.proj_end > F.pred_end) R::template run<STAGED>(F.P, 1, F.pred_end, F.proj_end, X, St, E);
+          copy_source_columns<STAGED>(F, X, E);
+        }
+        run += ((j < 4 ? tot_lo : tot_hi) >> sh) & 0xffffu;
+      }
     }
-    __syncthreads();
-    const unsigned long long base = s_prefix;
-    E.pos = (uint32_t)(base + excl);
-    if (F.proj_end > F.pred_end) R::template run<STAGED>(F.P, 1, F.pred_end, F.proj_end, X, St, E);
-    copy_source_columns<STAGED>(F, X, E.sel, E.pos);
-    if (tile == ntiles - 1 && threadIdx.x == 0) {
-      const unsigned long long cnt = base + total;
-      *out_count = cnt > 0xffffffffull ? 0xffffffffu : (uint32_t)cnt;
+    if (r == C - 1) {
+      // Predicate done for the chunk: per-step counts as 16-bit fields (steps
+      // 0-3 in ex_lo, 4-7 in ex_hi), positions, look-back.
+      ex_lo = ex_hi = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        ex_lo |= (unsigned long long)__popc((selmask >> (4 * k)) & 15u) << (16 * k);
+        ex_hi |= (unsigned long long)__popc((selmask >> (4 * k + 16)) & 15u) << (16 * k);
+      }
+      block_exclusive_sum2<kRowBlock>(ex_lo, ex_hi, s_scan, tot_lo, tot_hi);
+      unsigned long long total = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) total += ((tot_lo >> (16 * k)) & 0xffffu) + ((tot_hi >> (16 * k)) & 0xffffu);
+      if (threadIdx.x < 32) {
+        const unsigned long long p = tile_lookback(status, chunk, total, err);
+        if (threadIdx.x == 0) s_prefix = p;
+      }
+      __syncthreads();
+      run = s_prefix;
+      if (chunk == nchunks - 1 && threadIdx.x == 0) {
+        const unsigned long long cnt = run + total;
+        *out_count = cnt > 0xffffffffull ? 0xffffffffu : (uint32_t)cnt;
+      }
     }
-    if (++slot == S) {
-      slot = 0;
-      parity ^= 1u;
-    }
+    if (r == V - 1) selmask = 0;
   }
 }
 

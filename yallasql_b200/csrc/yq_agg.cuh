@@ -133,13 +133,35 @@ __device__ __forceinline__ void agg_block_finish(const AggEmit& E, uint32_t nsel
   __syncthreads();
   if (!s_last) return;
   __threadfence();
+  // The last block folds the partials with every thread (blocks t, t + BLOCK,
+  // ... per thread, then the warps, then across warps): independent loads
+  // instead of one chain of gridDim.x dependent ones.
+#pragma unroll
+  for (int a = 0; a < YQ_MAX_AGGREGATES; ++a) {
+    if (a < A.nagg) {
+      const int upd = A.upd[a];
+      long long c = 0;
+      unsigned long long v = acc_identity(upd);
+      for (uint32_t b = threadIdx.x; b < gridDim.x; b += BLOCK) {
+        const Acc* p = partials + b * YQ_MAX_AGGREGATES + a;
+        c += __ldcg(&p->cnt);
+        v = acc_merge(upd, v, __ldcg(&p->bits));
+      }
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) {
+        c += __shfl_down_sync(0xffffffffu, c, d);
+        v = acc_merge(upd, v, __shfl_down_sync(0xffffffffu, v, d));
+      }
+      if (lane == 0) s_acc[warp][a] = Acc{c, v};
+    }
+  }
+  __syncthreads();
   if (threadIdx.x < A.nagg) {
     const int a = threadIdx.x, upd = A.upd[a];
-    Acc t{0, acc_identity(upd)};
-    for (uint32_t b = 0; b < gridDim.x; ++b) {
-      const Acc* p = partials + b * YQ_MAX_AGGREGATES + a;
-      t.cnt += __ldcg(&p->cnt);
-      t.bits = acc_merge(upd, t.bits, __ldcg(&p->bits));
+    Acc t = s_acc[0][a];
+    for (int w = 1; w < BLOCK / 32; ++w) {
+      t.cnt += s_acc[w][a].cnt;
+      t.bits = acc_merge(upd, t.bits, s_acc[w][a].bits);
     }
     Acc s = state[a];
     s.cnt += t.cnt;

@@ -211,6 +211,61 @@ __device__ __forceinline__ uint32_t block_exclusive_sum(uint32_t x, uint32_t* s_
   return excl;
 }
 
+// Block-wide exclusive sum of two 64-bit words per thread in one pass (each
+// word holds independent fields that never carry into one another).
+// `s_warp` holds 2 * (BLOCK / 32 + 1) words; a and b become the exclusive sums.
+template <int BLOCK>
+__device__ __forceinline__ void block_exclusive_sum2(unsigned long long& a, unsigned long long& b,
+                                                     unsigned long long* s_warp, unsigned long long& ta,
+                                                     unsigned long long& tb) {
+  constexpr int NW = BLOCK / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long ia = a, ib = b;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned long long ya = __shfl_up_sync(0xffffffffu, ia, d);
+    const unsigned long long yb = __shfl_up_sync(0xffffffffu, ib, d);
+    if (lane >= d) {
+      ia += ya;
+      ib += yb;
+    }
+  }
+  if (lane == 31) {
+    s_warp[2 * warp] = ia;
+    s_warp[2 * warp + 1] = ib;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const unsigned long long wa = lane < NW ? s_warp[2 * lane] : 0ull;
+    const unsigned long long wb = lane < NW ? s_warp[2 * lane + 1] : 0ull;
+    unsigned long long sa = wa, sb = wb;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const unsigned long long ya = __shfl_up_sync(0xffffffffu, sa, d);
+      const unsigned long long yb = __shfl_up_sync(0xffffffffu, sb, d);
+      if (lane >= d) {
+        sa += ya;
+        sb += yb;
+      }
+    }
+    if (lane < NW) {
+      s_warp[2 * lane] = sa - wa;
+      s_warp[2 * lane + 1] = sb - wb;
+    }
+    if (lane == NW - 1) {
+      s_warp[2 * NW] = sa;
+      s_warp[2 * NW + 1] = sb;
+    }
+  }
+  __syncthreads();
+  const unsigned long long ea = s_warp[2 * warp] + ia - a, eb = s_warp[2 * warp + 1] + ib - b;
+  ta = s_warp[2 * NW];
+  tb = s_warp[2 * NW + 1];
+  __syncthreads();
+  a = ea;
+  b = eb;
+}
+
 // ---------------------------------------------- mbarrier + 1-D bulk copies
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));

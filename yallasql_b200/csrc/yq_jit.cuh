@@ -14,6 +14,13 @@ enum JitKind { JIT_FILTER_AGG = 0, JIT_FILTER_AGG_SEG = 1, JIT_FILTER_PROJECT = 
 // the caller then launches the interpreter kernel, which computes the same.
 const void* jit_kernel(JitKind kind, bool staged, const VmProgram& P, int seg0_end, int end);
 
+// Ring depth for `kernel` with stages of `stage_bytes`: of 2..kStageMax stages,
+// the count that lets the most blocks share an SM, the deeper ring on a tie
+// (a kernel with few registers then runs more blocks, each with a shallower
+// ring). `nstages` (the plan made for the interpreter) when the occupancy
+// cannot be queried or YQ_STAGE_FIT=0 is set in the environment.
+int jit_stages(const void* kernel, uint32_t stage_bytes, int nstages);
+
 // Launch helper for a kernel jit_kernel returned: raises its dynamic shared
 // memory limit when needed and sizes a persistent grid (at most `steps`).
 int jit_launch(const void* kernel, int max_grid, uint32_t steps, size_t smem, void** args, cudaStream_t s);

@@ -19,8 +19,20 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
   return v;
 }
 
+// Predecessor words read per lane and round: a warp looks at a window of 128
+// predecessors per memory round trip. Many tiles finish together, so the
+// nearest inclusive value can lie a whole wave of tiles back; a wide window
+// reaches it in one or two round trips.
+constexpr int kLookbackPerLane = 4;
+constexpr int kLookbackWindow = 32 * kLookbackPerLane;
+
 // Called by all 32 lanes of one warp. Publishes `agg` for `tile`, walks back
 // over predecessors and returns the exclusive prefix of this tile (all lanes).
+// Window position p (0 = nearest predecessor) is word base - p, read by lane
+// p / kLookbackPerLane. The walk waits while a word nearer than the nearest
+// inclusive one is unpublished; otherwise it adds the window's values up to
+// and including that inclusive word and stops, or adds the whole window and
+// moves it back.
 __device__ __forceinline__ unsigned long long tile_lookback(unsigned long long* status, uint32_t tile,
                                                             unsigned long long agg, uint32_t* err) {
   const int lane = threadIdx.x & 31;
@@ -34,10 +46,26 @@ __device__ __forceinline__ unsigned long long tile_lookback(unsigned long long* 
   uint32_t spins = 0;
   bool timed_out = false;
   for (;;) {
-    const long long j = base - lane;
-    unsigned long long s = (j >= 0) ? ld_relaxed_u64(status + j) : kFlagIncl;
-    const unsigned long long flag = s & ~kValMask;
-    if (__any_sync(0xffffffffu, flag == 0ull)) {
+    unsigned long long w[kLookbackPerLane];
+#pragma unroll
+    for (int i = 0; i < kLookbackPerLane; ++i) {
+      const long long j = base - (long long)(lane * kLookbackPerLane + i);
+      w[i] = (j >= 0) ? ld_relaxed_u64(status + j) : kFlagIncl;  // before tile 0: inclusive 0
+    }
+    int fz = kLookbackPerLane, fi = kLookbackPerLane;  // this lane's first unpublished / inclusive word
+#pragma unroll
+    for (int i = kLookbackPerLane - 1; i >= 0; --i) {
+      const unsigned long long flag = w[i] & ~kValMask;
+      if (flag == 0ull) fz = i;
+      if (flag == kFlagIncl) fi = i;
+    }
+    const uint32_t zl = __ballot_sync(0xffffffffu, fz < kLookbackPerLane);
+    const uint32_t il = __ballot_sync(0xffffffffu, fi < kLookbackPerLane);
+    const int lz = zl ? __ffs(zl) - 1 : 0, li = il ? __ffs(il) - 1 : 0;
+    const int fz_at = __shfl_sync(0xffffffffu, fz, lz), fi_at = __shfl_sync(0xffffffffu, fi, li);
+    const int gz = zl ? lz * kLookbackPerLane + fz_at : kLookbackWindow;
+    const int gi = il ? li * kLookbackPerLane + fi_at : kLookbackWindow;
+    if (gz < gi) {
       // Give up at the bound, or early once another tile has already failed.
       if (++spins > kSpinLimit || ((spins & 63u) == 0u && ld_relaxed_u32(err) != 0u)) {
         timed_out = true;
@@ -46,14 +74,13 @@ __device__ __forceinline__ unsigned long long tile_lookback(unsigned long long* 
       __nanosleep(spins < 64 ? 32 : 256);
       continue;
     }
-    const uint32_t incl = __ballot_sync(0xffffffffu, flag == kFlagIncl);
-    if (incl) {
-      const int first = __ffs(incl) - 1;  // nearest predecessor with an inclusive value
-      excl += warp_sum_u64(lane <= first ? (s & kValMask) : 0ull);
-      break;
-    }
-    excl += warp_sum_u64(s & kValMask);
-    base -= 32;
+    unsigned long long part = 0;
+#pragma unroll
+    for (int i = 0; i < kLookbackPerLane; ++i)
+      if (lane * kLookbackPerLane + i <= gi) part += w[i] & kValMask;
+    excl += warp_sum_u64(part);
+    if (gi < kLookbackWindow) break;
+    base -= kLookbackWindow;
   }
   if (timed_out) {
     if (lane == 0) atomicOr(err, kErrTimeout);
