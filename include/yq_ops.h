@@ -337,9 +337,18 @@ int yq_merge_pass(const yq_column* cols, int32_t ncols, int32_t key_col,
  * tiles ahead with 1-D bulk copies; finally every column is gathered once by
  * the merged row ids into `out` (same schema, at least in->rows rows).
  * Stable: equal keys keep their input order. The call waits for the device
- * once, at the end, to report errors. */
+ * once, at the end, to report errors.
+ *
+ * With many runs over a table larger than L2 the gather goes in two levels
+ * when the workspace allows (or the library allocates it): the columns are
+ * first gathered run by run into sorted-run order, and the final gather then
+ * reads every run's rows in increasing order. yq_order_by_workspace_size is
+ * the least workspace (one-level gather); yq_order_by_batch_workspace_size
+ * includes the sorted-run copy of the batch's columns. */
 size_t yq_order_by_workspace_size(const yq_column* key, uint32_t rows, const uint32_t* run_offsets,
                                   int32_t nruns);
+size_t yq_order_by_batch_workspace_size(const yq_batch* in, int32_t key_col, const uint32_t* run_offsets,
+                                        int32_t nruns);
 int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
                 const uint32_t* run_offsets, int32_t nruns, yq_batch* out, void* workspace,
                 size_t workspace_bytes, void* stream);

@@ -65,6 +65,28 @@ def test_order_by_runs_key_id_path(cuda, dist, batch):
                 np.testing.assert_array_equal(col.data.cpu().numpy(), t[n][perm])
 
 
+@pytest.mark.parametrize("dist", ["uniform", "zipf", "equal"])
+@pytest.mark.parametrize("two_level", [True, False])
+def test_order_by_runs_two_level_gather(cuda, dist, two_level):
+    """A table above the two-level threshold (2.1M rows x 36 bytes): the
+    columns go through the sorted-run copy, or not when the workspace only
+    holds the one-level minimum; both equal one stable sort."""
+    rows = 2_100_003
+    t = datagen.order_table(rows, seed=4, dist=dist)
+    b = table_batch(t)
+    batch = 116_480
+    counts = [batch] * (rows // batch) + ([rows % batch] if rows % batch else [])
+    offs = list(np.concatenate([[0], np.cumsum(counts)]).astype(int))
+    assert (ops.order_by_batch_workspace_bytes(b, 0, offs) > ops.order_by_workspace_bytes(b.columns[0], offs))
+    for key, name, desc, ty in ((0, "key", True, None), (3, "d", False, oracle.DATETIME)):
+        job = ops.OrderByRuns(b, key, offs, two_level=two_level)
+        out = out_like(b)
+        job.run(b, desc, out)
+        perm = oracle.sort_perm(t[name], desc=desc, type_=ty)
+        for col, n in zip(out.columns, ["key", "id", "txt", "d"]):
+            np.testing.assert_array_equal(col.data.cpu().numpy(), t[n][perm])
+
+
 @pytest.mark.parametrize("nruns", [1, 2, 3, 8, 13])
 @pytest.mark.parametrize("kind", ["i32", "i64", "text16", "f32_nulls"])
 def test_merge_pass_types(cuda, nruns, kind):

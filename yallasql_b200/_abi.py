@@ -116,6 +116,7 @@ PROTOTYPES = {
     "yq_merge_workspace_size": (sz, [u32, i32]),
     "yq_merge_pass": (C.c_int, [P(Column), i32, i32, i32, i32, P(u32), i32, P(Column), vp, sz, vp]),
     "yq_order_by_workspace_size": (sz, [P(Column), u32, P(u32), i32]),
+    "yq_order_by_batch_workspace_size": (sz, [P(Batch), i32, P(u32), i32]),
     "yq_agg_states_init": (C.c_int, [vp, i32, P(AggSpec), i32, vp]),
     "yq_agg_states_read": (C.c_int, [vp, i32, P(AggSpec), i32, P(AggResult), vp]),
     "yq_filter_aggregate_segments_workspace_size": (sz, [u32, i32]),

@@ -742,6 +742,35 @@ struct OrderWs {
   size_t npairs = 0;
 };
 
+// Two-level gather: with many runs over a table larger than L2, one gather by
+// the merged row ids reads every cell at a random row of the whole table
+// (each 4-16-byte cell costs a DRAM sector or more). Instead every column is
+// first gathered run by run into sorted-run order (the rows a run reads lie
+// within that run, so the in-flight window stays in L2), the row ids become
+// positions in that layout, and after the merges the final gather reads each
+// run's rows in increasing order: hundreds of sequential streams whose
+// sectors L2 serves until every cell of them is used.
+constexpr double kTwoLevelGatherBytes = 64.0 * 1024 * 1024;
+
+static bool two_level_gather(const yq_batch& in, int nruns) {
+  if (nruns < 2) return false;
+  double b = 0;
+  for (int c = 0; c < in.ncols; ++c) b += (double)in.rows * (in.columns[c].width + (in.columns[c].nulls ? 1 : 0));
+  return b >= kTwoLevelGatherBytes;
+}
+
+// The sorted-run copy of every column (same widths, nulls where the input has them).
+static void stage_ws_layout(const yq_batch& in, WsSize& w) {
+  for (int c = 0; c < in.ncols; ++c) {
+    w.add<char>((size_t)in.rows * in.columns[c].width + 16);
+    if (in.columns[c].nulls) w.add<uint8_t>((size_t)in.rows + 16);
+  }
+}
+
+__global__ void k_iota(uint32_t* __restrict__ ids, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) ids[i] = i;
+}
+
 static int order_ws_layout(const yq_column& key, uint32_t rows, const uint32_t* offsets, int nruns, OrderWs& o,
                            WsSize& w) {
   o.kw_max = sort_key_words_max(key);
@@ -771,6 +800,16 @@ extern "C" size_t yq_order_by_workspace_size(const yq_column* key, uint32_t rows
   OrderWs o;
   WsSize w;
   if (order_ws_layout(*key, rows, run_offsets, nruns, o, w) != YQ_OK) return 0;
+  return w.total();
+}
+
+extern "C" size_t yq_order_by_batch_workspace_size(const yq_batch* in, int32_t key_col, const uint32_t* run_offsets,
+                                                   int32_t nruns) {
+  if (!in || !run_offsets || nruns <= 0 || key_col < 0 || key_col >= in->ncols) return 0;
+  OrderWs o;
+  WsSize w;
+  if (order_ws_layout(in->columns[key_col], in->rows, run_offsets, nruns, o, w) != YQ_OK) return 0;
+  if (two_level_gather(*in, nruns)) stage_ws_layout(*in, w);
   return w.total();
 }
 
@@ -853,14 +892,29 @@ extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descendi
   OrderWs o;
   WsSize wsz;
   YQ_TRY(order_ws_layout(key, rows, run_offsets, nruns, o, wsz));
+  const size_t base_bytes = wsz.total();
+  // The sorted-run copy needs more workspace: used when the caller's holds it
+  // (yq_order_by_batch_workspace_size) or the library allocates.
+  bool staged = two_level_gather(*in, nruns);
+  if (staged) {
+    stage_ws_layout(*in, wsz);
+    if (workspace && workspace_bytes < wsz.total()) staged = false;
+  }
   Workspace ws;
-  YQ_TRY(ws.acquire(workspace, workspace_bytes, wsz.total(), s));
+  YQ_TRY(ws.acquire(workspace, workspace_bytes, staged ? wsz.total() : base_bytes, s));
   char* sort_ws = ws.take<char>(o.sort_bytes);
   uint32_t* keys[2] = {ws.take<uint32_t>((size_t)rows * o.kw_max + 16), ws.take<uint32_t>((size_t)rows * o.kw_max + 16)};
   uint32_t* ids[2] = {ws.take<uint32_t>((size_t)rows + 16), ws.take<uint32_t>((size_t)rows + 16)};
   RawPair* d_pairs = ws.take<RawPair>(o.npairs);
   RawTile* d_tiles = ws.take<RawTile>(o.max_tiles);
   uint32_t* d_err = ws.take<uint32_t>(4);
+  yq_column stage[YQ_MAX_BATCH_COLUMNS];
+  if (staged)
+    for (int c = 0; c < in->ncols; ++c) {
+      stage[c] = in->columns[c];
+      stage[c].data = ws.take<char>((size_t)rows * in->columns[c].width + 16);
+      stage[c].nulls = in->columns[c].nulls ? ws.take<uint8_t>((size_t)rows + 16) : nullptr;
+    }
   YQ_TRY_CUDA(cudaMemsetAsync(d_err, 0, 4 * sizeof(uint32_t), s));
 
   // 1. every run sorted; the sort hands over its key words and row ids
@@ -878,9 +932,20 @@ extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descendi
     k_key_lossy<<<sm_count() * 4, 256, 0, s>>>(static_cast<const char*>(key.data), key.type, rows, d_lossy);
     YQ_CHECK_LAUNCH();
   }
+  const uint32_t* only_if[YQ_MAX_BATCH_COLUMNS] = {nullptr};
+  if (decode) only_if[key_col] = d_lossy;  // zero unless a value would not round-trip
+  // 1b. two-level gather, first level: every column into sorted-run order;
+  // the row ids become positions in that copy
+  const bool merged = kw > 0 && nruns > 1;
+  staged = staged && merged;
+  if (staged) {
+    YQ_TRY(gather_impl(in->columns, in->ncols, ids[0], rows, stage, only_if, s));
+    k_iota<<<sm_count() * 4, 256, 0, s>>>(ids[0], rows);
+    YQ_CHECK_LAUNCH();
+  }
   // 2. merge levels over (key words, row id)
   int cur = 0;
-  if (kw > 0 && nruns > 1) {
+  if (merged) {
     OrderPlan P;
     plan_order_levels(run_offsets, nruns, P);
     if (P.pairs.size() > o.npairs) return YQ_ERR_UNSUPPORTED;
@@ -921,9 +986,7 @@ extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descendi
     }
   }
   // 3. every column (the key included) gathered once by the final row ids
-  const uint32_t* only_if[YQ_MAX_BATCH_COLUMNS] = {nullptr};
-  if (decode) only_if[key_col] = d_lossy;  // zero unless a value would not round-trip
-  YQ_TRY(gather_impl(in->columns, in->ncols, ids[cur], rows, out->columns, only_if, s));
+  YQ_TRY(gather_impl(staged ? stage : in->columns, in->ncols, ids[cur], rows, out->columns, only_if, s));
   uint32_t err[2] = {0, 0};
   YQ_TRY_CUDA(cudaMemcpyAsync(&err[0], sort_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   YQ_TRY_CUDA(cudaMemcpyAsync(&err[1], d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));

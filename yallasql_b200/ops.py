@@ -460,9 +460,17 @@ class JoinAggPlan:
 
 
 def order_by_workspace_bytes(col: DeviceColumn, offsets: list[int]) -> int:
+    """Least workspace of yq_order_by (one-level gather)."""
     offs = (C.c_uint32 * len(offsets))(*offsets)
     cc = col.c()
     return int(lib().yq_order_by_workspace_size(C.byref(cc), col.rows, offs, len(offsets) - 1))
+
+
+def order_by_batch_workspace_bytes(batch: DeviceBatch, key: int, offsets: list[int]) -> int:
+    """Workspace of yq_order_by including the sorted-run copy of the columns."""
+    offs = (C.c_uint32 * len(offsets))(*offsets)
+    b, _keep = batch.c()
+    return int(lib().yq_order_by_batch_workspace_size(C.byref(b), key, offs, len(offsets) - 1))
 
 
 class OrderByRuns:
@@ -471,13 +479,16 @@ class OrderByRuns:
     sort, merged level by level as (key words, row id) pairs, and every column
     is gathered once by the merged row ids (OrderOperator::firstPass +
     merge_all_sorted, order_operator.hpp:89-193 / order_operator.cpp:14-220).
-    The workspace is allocated once and reused across calls."""
+    The workspace is allocated once and reused across calls; `two_level`
+    sizes it for the sorted-run copy that the two-level gather uses on large
+    tables."""
 
-    def __init__(self, batch: DeviceBatch, key: int, offsets: list[int]):
+    def __init__(self, batch: DeviceBatch, key: int, offsets: list[int], two_level: bool = True):
         self.key, self.offsets, self.n = key, list(offsets), batch.rows
         self._offs = (C.c_uint32 * len(self.offsets))(*self.offsets)
-        self.ws = torch.empty(max(order_by_workspace_bytes(batch.columns[key], self.offsets), 256),
-                              dtype=torch.uint8, device="cuda")
+        need = (order_by_batch_workspace_bytes(batch, key, self.offsets) if two_level
+                else order_by_workspace_bytes(batch.columns[key], self.offsets))
+        self.ws = torch.empty(max(need, 256), dtype=torch.uint8, device="cuda")
 
     def run(self, batch: DeviceBatch, descending: bool, out: DeviceBatch, nulls_first=False, stream=None):
         ib, _ia = batch.c()
