@@ -356,6 +356,7 @@ struct KeyDecode {
   int32_t vwords;   // value words (text: significant slot words)
   int32_t width;    // slot width (text)
   int32_t desc;
+  uint32_t high[8];  // key words above the merged ones, shared by every row (key form)
 };
 
 struct RawLevel {
@@ -525,31 +526,31 @@ __device__ __forceinline__ void raw_key_store(uint32_t* out, size_t row, const u
 // no -0.0, non-canonical NaN or bool byte other than 0/1: see k_key_lossy).
 template <int KW>
 __device__ __forceinline__ void decode_store(const KeyDecode& d, size_t row, const uint32_t (&k0)[KW]) {
-  uint32_t k[KW];
+  // the whole key: the merged words, then the words every row shares
+  uint32_t k[8];
 #pragma unroll
-  for (int j = 0; j < KW; ++j) k[j] = (d.desc && j < d.vwords) ? ~k0[j] : k0[j];
+  for (int j = 0; j < 8; ++j) {
+    const uint32_t w = j < KW ? k0[j < KW ? j : 0] : d.high[j >= KW ? j - KW : 0];
+    k[j] = (d.desc && j < d.vwords) ? ~w : w;
+  }
   switch (d.type) {
     case YQ_INT32: reinterpret_cast<uint32_t*>(d.out)[row] = k[0] ^ 0x80000000u; break;
     case YQ_FLOAT32: reinterpret_cast<uint32_t*>(d.out)[row] = (k[0] & 0x80000000u) ? (k[0] & 0x7fffffffu) : ~k[0]; break;
     case YQ_BOOL: reinterpret_cast<uint8_t*>(d.out)[row] = (uint8_t)(k[0] & 1u); break;
     case YQ_INT64:
-    case YQ_DATETIME:
-      if constexpr (KW >= 2)
-        reinterpret_cast<uint2*>(d.out)[row] = make_uint2(k[0], k[1] ^ 0x80000000u);
+    case YQ_DATETIME: reinterpret_cast<uint2*>(d.out)[row] = make_uint2(k[0], k[1] ^ 0x80000000u); break;
+    case YQ_FLOAT64: {
+      unsigned long long b = ((unsigned long long)k[1] << 32) | k[0];
+      b = (b & 0x8000000000000000ull) ? (b & 0x7fffffffffffffffull) : ~b;
+      reinterpret_cast<unsigned long long*>(d.out)[row] = b;
       break;
-    case YQ_FLOAT64:
-      if constexpr (KW >= 2) {
-        unsigned long long b = ((unsigned long long)k[1] << 32) | k[0];
-        b = (b & 0x8000000000000000ull) ? (b & 0x7fffffffffffffffull) : ~b;
-        reinterpret_cast<unsigned long long*>(d.out)[row] = b;
-      }
-      break;
+    }
     default: {  // TEXT: word i of the slot = bswap(k[vwords - 1 - i]); later words are zero
       uint32_t* w = reinterpret_cast<uint32_t*>(d.out + row * (size_t)d.width);
       for (int i = 0; i < (d.width >> 2); ++i) {
         uint32_t v = 0u;
 #pragma unroll
-        for (int j = 0; j < KW; ++j)
+        for (int j = 0; j < 8; ++j)
           if (i < d.vwords && j == d.vwords - 1 - i) v = bswap(k[j]);
         w[i] = v;
       }
@@ -921,8 +922,9 @@ extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descendi
   KeyJob job{key, descending != 0, nulls_first != 0};
   int kw = 0;
   uint32_t* sort_err = nullptr;
+  uint32_t high[8];
   YQ_TRY(sort_segments_impl(&job, 1, rows, run_offsets, nruns, ids[0], nullptr, sort_ws, o.sort_bytes, s, nullptr,
-                            keys[0], &kw, true, &sort_err));
+                            keys[0], &kw, true, &sort_err, high));
   // The last merge level writes the key column itself when the key has no
   // nulls; the gather then moves the key column only if some value would not
   // round-trip through its key words (flag set on the device).
@@ -964,6 +966,7 @@ extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descendi
         L.dec.vwords = key.type == YQ_INT32 || key.type == YQ_FLOAT32 || key.type == YQ_BOOL ? 1 : 2;
         L.dec.width = key.width;
         L.dec.desc = descending != 0;
+        memcpy(L.dec.high, high, sizeof(high));
       }
       L.ids_out = ids[cur ^ 1];
       L.pairs = d_pairs + P.level_first[l];

@@ -697,9 +697,10 @@ static int launch_make_keys(int kw, const KeySrc& src, uint32_t* out, uint32_t r
 int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint32_t* seg_offsets_host, int nseg,
                        uint32_t* out_perm, const yq_sort_config* cfg, void* workspace, size_t workspace_bytes,
                        cudaStream_t s, size_t* size_only, uint32_t* keys_out, int* kw_out, bool defer_err,
-                       uint32_t** err_out) {
+                       uint32_t** err_out, uint32_t* high_out) {
   if (keys_out && (njobs != 1 || !kw_out)) return YQ_ERR_INVALID_ARG;
   if (kw_out) *kw_out = 0;
+  if (high_out) memset(high_out, 0, 8 * sizeof(uint32_t));
   if (njobs <= 0 || nseg <= 0 || !seg_offsets_host) return YQ_ERR_INVALID_ARG;
   if (rows > kMaxSortRows) return YQ_ERR_UNSUPPORTED;
   if (seg_offsets_host[0] != 0 || seg_offsets_host[nseg] != rows) return YQ_ERR_INVALID_ARG;
@@ -813,31 +814,71 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
     }
 
     std::vector<int> passes;
+    KeyPlan kq = kp;  // the passes' plan: kp, or fewer key words when the leading ones are shared
+    uint32_t high[8] = {0};
     if (keep_trivial) {
       for (int p = 0; p < kp.P; ++p) passes.push_back(p);
     } else {
       // A pass whose digit is the same for every key of every segment leaves
-      // the order unchanged and is skipped.
+      // the order unchanged and is skipped. common[p] = that digit when it is
+      // also the same across segments, else -1.
       std::vector<uint32_t> h((size_t)nseg * kp.P * kp.R);
       YQ_TRY_CUDA(cudaMemcpyAsync(h.data(), d_hist, h.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
       YQ_TRY_CUDA(cudaStreamSynchronize(s));
+      std::vector<int> common(kp.P, -1);
       for (int p = 0; p < kp.P; ++p) {
         bool trivial = true;
+        int digit = -2;  // -2: no non-empty segment seen yet
         for (int g = 0; g < nseg && trivial; ++g) {
           const uint32_t len = seg_offsets_host[g + 1] - seg_offsets_host[g];
           if (len == 0) continue;
           const uint32_t* hp = h.data() + ((size_t)g * kp.P + p) * kp.R;
-          bool one = false;
-          for (int d = 0; d < kp.R && !one; ++d) one = (hp[d] == len);
-          trivial = one;
+          int one = -1;
+          for (int d = 0; d < kp.R && one < 0; ++d)
+            if (hp[d] == len) one = d;
+          trivial = one >= 0;
+          digit = (digit == -2 || digit == one) ? one : -1;
         }
         if (!trivial) passes.push_back(p);
+        else common[p] = digit;
+      }
+      // Leading words whose every digit is common to all rows: the passes
+      // keep the words below them (a kernel width of 1, 2 or 4 words).
+      if (32 % kp.D == 0 && !passes.empty()) {
+        const int ppw = 32 / kp.D;
+        int shared = 0;
+        for (int w = kp.sh.kw - 1; w >= 1; --w) {
+          bool all = true;
+          for (int q = 0; q < ppw && all; ++q) all = common[w * ppw + q] >= 0;
+          if (!all) break;
+          ++shared;
+        }
+        const int kw_eff = round_kw(kp.sh.kw - shared);
+        if (kw_eff > 0 && kw_eff < kp.sh.kw && pick_kernels(kw_eff, kp.D, 0, kq.K)) {
+          kq.sh.kw = kw_eff;
+          kq.P = kw_eff * ppw;
+          kq.tile_rows = (uint32_t)kSortBlock * kq.K.items;
+          for (int w = kw_eff; w < kp.sh.kw; ++w)
+            for (int q = 0; q < ppw; ++q) high[w - kw_eff] |= (uint32_t)common[w * ppw + q] << (q * kp.D);
+          std::vector<int> kept;
+          for (int p : passes)
+            if (p < kq.P) kept.push_back(p);
+          passes.swap(kept);
+        } else {
+          kq = kp;
+        }
       }
     }
-    if (keys_out) *kw_out = kp.sh.kw;
+    if (keys_out) *kw_out = kq.sh.kw;
+    if (high_out) memcpy(high_out, high, sizeof(high));
     if (passes.empty()) {  // order unchanged by this key
-      if (keys_out) YQ_TRY(launch_make_keys(kp.sh.kw, src, keys_out, rows, s));
+      if (keys_out) YQ_TRY(launch_make_keys(kq.sh.kw, src, keys_out, rows, s));
       continue;
+    }
+    if (kq.sh.kw != kp.sh.kw) {  // tiles of the narrower kernels
+      plan_segments(seg_offsets_host, nseg, kq.tile_rows, sp);
+      YQ_TRY(h2d_async(d_tiles, sp.tiles.data(), (nseg + 1) * sizeof(uint32_t), s));
+      YQ_TRY_CUDA(cudaMemsetAsync(d_status, 0, passes.size() * sp.ntiles * kq.R * sizeof(uint32_t), s));
     }
     if (passes.size() > 64) return YQ_ERR_UNSUPPORTED;
     uint32_t* dst_perm = (perm_in == out_perm) ? d_perm_tmp : out_perm;
@@ -851,18 +892,18 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
       Sp.src = src;
       Sp.seg = seg;
       Sp.hist = d_hist;
-      Sp.status = d_status + (size_t)i * sp.ntiles * kp.R;
+      Sp.status = d_status + (size_t)i * sp.ntiles * kq.R;
       Sp.tile_counter = d_misc + i;
       Sp.err = d_err;
       Sp.pass = passes[i];
       Sp.npass = kp.P;
       // algorithmic bytes: keys + row ids in, keys + row ids out (the first
       // pass reads the raw key (+ incoming permutation), the last writes ids only)
-      const double kb = 4.0 * kp.sh.kw;
+      const double kb = 4.0 * kq.sh.kw;
       const double in_b = first ? (double)c.width + (perm_in ? 4.0 : 0.0) : kb + 4.0;
       const double out_b = (last && !keys_out) ? 4.0 : kb + 4.0;
       ProfScope ps("sort_onesweep", s, (double)rows * (in_b + out_b));
-      YQ_TRY(kp.K.sweep(Sp, sp.ntiles, s));
+      YQ_TRY(kq.K.sweep(Sp, sp.ntiles, s));
     }
     perm_in = dst_perm;
   }

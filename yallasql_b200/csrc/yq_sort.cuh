@@ -21,10 +21,16 @@ int sort_key_words_max(const yq_column& c);
 // transformed key words of the sorted rows ([rows][*kw_out] words; *kw_out = 0
 // when every key is equal). With `defer_err` the call does not wait for the
 // device to report errors: *err_out points at the workspace's error word.
+//
+// Leading key words that every row shares (found from the digit histogram:
+// one bucket, the same in every segment) take no part in the passes: the
+// passes, and `keys_out`, carry only the words below them. With `high_out`
+// (8 words) the call reports the words it left out, least significant first:
+// high_out[i] is key word *kw_out + i, in key form (after the DESC inversion).
 int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint32_t* seg_offsets_host, int nseg,
                        uint32_t* out_perm, const yq_sort_config* cfg, void* workspace, size_t workspace_bytes,
                        cudaStream_t s, size_t* size_only, uint32_t* keys_out = nullptr, int* kw_out = nullptr,
-                       bool defer_err = false, uint32_t** err_out = nullptr);
+                       bool defer_err = false, uint32_t** err_out = nullptr, uint32_t* high_out = nullptr);
 
 // out[c][i] = in[c][perm[i]] for every column (yq_gather); with `only_if`,
 // column c moves only when only_if[c] is null or *only_if[c] != 0 on the device.
