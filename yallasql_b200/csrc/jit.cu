@@ -270,7 +270,7 @@ int resident_locked(const void* kernel, size_t smem, int dev) {
 
 }  // namespace
 
-int jit_stages(const void* kernel, uint32_t stage_bytes, int nstages) {
+int jit_stages(const void* kernel, uint32_t stage_bytes, int nstages, size_t extra) {
   if (!kernel || nstages < 2 || stage_bytes == 0) return nstages;
   static int fit = -1;
   std::lock_guard<std::mutex> lk(g_launch_mu);
@@ -284,12 +284,14 @@ int jit_stages(const void* kernel, uint32_t stage_bytes, int nstages) {
     cudaGetLastError();
     return nstages;
   }
-  const std::string key = launch_key(kernel, stage_bytes, dev);
+  const std::string key = launch_key(kernel, stage_bytes, dev) + std::string(reinterpret_cast<const char*>(&extra),
+                                                                          sizeof(extra));
   auto it = g_depth.find(key);
   if (it != g_depth.end()) return it->second;
   int best = nstages, best_blocks = 0;
   for (int ns = 2; ns <= kStageMax; ++ns) {  // deeper on a tie
-    const int per_sm = resident_locked(kernel, (size_t)ns * stage_bytes + (size_t)ns * 8, dev);
+    const size_t ring = (size_t)ns * stage_bytes + (size_t)ns * 8;
+    const int per_sm = resident_locked(kernel, extra ? align_up(ring, 16) + extra : ring, dev);
     if (per_sm == 0) break;
     if (per_sm >= best_blocks) {
       best_blocks = per_sm;

@@ -739,10 +739,16 @@ int yq_join_aggregate(const yq_batch* fact, const yq_program* fact_predicate, in
   const void* jk = jit_kernel(JIT_JOIN_AGG, staged, F.P, F.pred_end, F.pc_end);
   ProfScope ps("join_aggregate", s, (double)fact->rows * row_bytes);
   if (jk) {
+    size_t jsmem = smem;
+    if (staged) {  // ring depth for the specialised kernel's occupancy, table after it
+      F.SP.nstages = jit_stages(jk, F.SP.stage_bytes, F.SP.nstages, table);
+      F.table_off = (uint32_t)align_up(stage_smem_bytes(F.SP), 16);
+      jsmem = F.table_off + table;
+    }
     uint32_t n = fact->rows;
     Acc* st = static_cast<Acc*>(state);
     void* args[] = {&F, &n, &partials, &d_misc, &st};
-    return jit_launch(jk, grid_cap, tiles, smem, args, s);
+    return jit_launch(jk, grid_cap, tiles, jsmem, args, s);
   }
   if (staged)
     k_join_aggregate<true><<<grid, kRowBlock, smem, s>>>(F, fact->rows, partials, d_misc, static_cast<Acc*>(state));

@@ -18,8 +18,9 @@ const void* jit_kernel(JitKind kind, bool staged, const VmProgram& P, int seg0_e
 // the count that lets the most blocks share an SM, the deeper ring on a tie
 // (a kernel with few registers then runs more blocks, each with a shallower
 // ring). `nstages` (the plan made for the interpreter) when the occupancy
-// cannot be queried or YQ_STAGE_FIT=0 is set in the environment.
-int jit_stages(const void* kernel, uint32_t stage_bytes, int nstages);
+// cannot be queried or YQ_STAGE_FIT=0 is set in the environment. `extra`:
+// dynamic shared memory the kernel keeps after the ring (16-byte aligned).
+int jit_stages(const void* kernel, uint32_t stage_bytes, int nstages, size_t extra = 0);
 
 // Launch helper for a kernel jit_kernel returned: raises its dynamic shared
 // memory limit when needed and sizes a persistent grid (at most `steps`).
