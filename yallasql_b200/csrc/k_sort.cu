@@ -149,8 +149,13 @@ struct SweepParams {
   int32_t npass;         // P
 };
 
+// Blocks per SM the registers are sized for: four for the variants whose
+// keys, values and ranks fit 64 registers without spilling (one key word, up
+// to 12 items per thread, or 8 items of two words), three otherwise.
+constexpr int sweep_min_blocks(int kw, int d, int items) { return (kw * items <= 12 && d == 8) || (kw == 2 && items <= 8 && d == 8) ? 4 : 3; }
+
 template <int KW, int D, int ITEMS>
-__global__ void __launch_bounds__(kSortBlock, 3) k_sort_onesweep(const __grid_constant__ SweepParams S) {
+__global__ void __launch_bounds__(kSortBlock, sweep_min_blocks(KW, D, ITEMS)) k_sort_onesweep(const __grid_constant__ SweepParams S) {
   constexpr int RADIX = 1 << D;
   constexpr int NW = kSortBlock / 32;
   constexpr uint32_t TILE = kSortBlock * ITEMS;
@@ -502,8 +507,6 @@ static bool valid_key_column(const yq_column& c) {
 
 static int round_kw(int w) { return w <= 1 ? 1 : (w <= 2 ? 2 : (w <= 4 ? 4 : (w <= 8 ? 8 : -1))); }
 
-static int items_for(int kw) { return kw == 1 ? 16 : (kw == 2 ? 12 : (kw == 4 ? 8 : 4)); }
-
 template <int KW, int D, int ITEMS>
 static size_t sweep_smem() {
   constexpr int RADIX = 1 << D;
@@ -560,11 +563,11 @@ static SortKernels make_kernels() {
 }
 
 // Instantiated (key words, digit bits, items per thread) variants; items = 0
-// picks the first listed for (kw, d).
+// picks the default for (kw, d), the case that lists digit bits x 100 + 0.
 static bool pick_kernels(int kw, int d, int items, SortKernels& k) {
   switch (kw * 10000 + d * 100 + items) {
-    case 10816: case 10800: k = make_kernels<1, 8, 16>(); return true;
-    case 10812: k = make_kernels<1, 8, 12>(); return true;
+    case 10816: k = make_kernels<1, 8, 16>(); return true;
+    case 10812: case 10800: k = make_kernels<1, 8, 12>(); return true;  // 12 items: four blocks per SM
     case 10808: k = make_kernels<1, 8, 8>(); return true;
     case 10616: case 10600: k = make_kernels<1, 6, 16>(); return true;
     case 10416: case 10400: k = make_kernels<1, 4, 16>(); return true;
