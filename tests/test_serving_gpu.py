@@ -48,3 +48,21 @@ def test_results_same_alone_and_in_mix(cuda, rate):
             assert torch.equal(a.result[1], m.result[1]) and torch.equal(a.result[2], m.result[2])
         assert m.done >= m.arrival
     assert seen == set(serving.CLASSES)
+
+
+def test_slot_buffers_reused_across_requests(cuda):
+    """Without keep, ORDER BY and subquery requests write into their slot's
+    reused buffers; the counts and aggregates still match the plain form."""
+    cat = serving.Catalog(ntables=4, lo=1_000, hi=200_000, seed=6)
+    plans = serving.Plans()
+    trace = serving.make_trace(80, 0.0, cat, seed=6)
+    alone = copy.deepcopy(trace)
+    serving.serve_plain(alone, cat, plans)
+    mixed = copy.deepcopy(trace)
+    serving.serve_continuous(mixed, cat, plans, slots=4)
+    for a, m in zip(alone, mixed):
+        if a.klass in ("filter", "join"):
+            assert all(close(x, y) for x, y in zip(a.result, m.result)), (a.rid, a.result, m.result)
+        else:
+            assert a.result == m.result, (a.rid, a.result, m.result)
+    assert len(cat._slots) == 4 and any(b._order is not None for b in cat._slots.values())

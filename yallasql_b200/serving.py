@@ -86,6 +86,14 @@ class Catalog:
                                     for k in ("datekey", "year", "month")])
         self.ntables = ntables
 
+    def slot_buffers(self, slot: int) -> SlotBuffers:
+        """The reusable buffers of serving slot `slot` (created on first use)."""
+        if not hasattr(self, "_slots"):
+            self._slots = {}
+        if slot not in self._slots:
+            self._slots[slot] = SlotBuffers(self)
+        return self._slots[slot]
+
     def sales_view(self, i: int) -> ops.DeviceBatch:
         return self.arena.slice(self.sales_begin[i], self.sales_end[i])
 
@@ -144,12 +152,54 @@ class Plans:
 
 
 # ------------------------------------------------------------------- jobs
+class SlotBuffers:
+    """Outputs and workspaces one slot (stream) reuses from request to request:
+    an ORDER BY result and workspace sized for the largest order table and a
+    subquery's projected columns sized for the largest sales table, allocated
+    before the slot serves its first request. Requests then allocate nothing large on the
+    request path (no allocator calls, no device-wide synchronisation from
+    them); results that must outlive the request (keep=True) are allocated
+    per request instead."""
+
+    def __init__(self, cat: "Catalog"):
+        self.cat = cat
+        self._order = None
+        self._sub = None
+
+    def ensure(self):
+        """Allocate both buffers now (before a timed run)."""
+        self.order(0, 0)
+        self.subquery(0)
+        return self
+
+    def order(self, n: int, ws_bytes: int):
+        if self._order is None:
+            nmax = max(t.rows for t in self.cat.order)
+            out = ops.DeviceBatch([ops.DeviceColumn.empty(t, nmax, w if t == A.TEXT else None)
+                                   for t, w in zip(ORDER_TYPES, ORDER_WIDTHS)])
+            big = max(self.cat.order, key=lambda t: t.rows)
+            wsb = max(256, ops.order_by_segments_workspace_bytes(big.columns[0], [0, big.rows]))
+            self._order = (out, torch.empty(wsb, dtype=torch.uint8, device="cuda"))
+        out, ws = self._order
+        if n > out.rows or ws_bytes > ws.numel():
+            raise ValueError("ORDER BY request larger than the slot's buffers")
+        return out.slice(0, n), ws[:ws_bytes]
+
+    def subquery(self, n: int):
+        if self._sub is None:
+            nmax = max(1, max(e - b for b, e in zip(self.cat.sales_begin, self.cat.sales_end)))
+            self._sub = [ops.DeviceColumn.empty(A.FLOAT32, nmax), ops.DeviceColumn.empty(A.INT32, nmax)]
+        if n > self._sub[0].rows:
+            raise ValueError("subquery larger than the slot's buffers")
+        return [c.slice(0, n) for c in self._sub]
+
+
 class Job:
     """Device work of one dispatch on one stream; `event` fires when it is done."""
     mem = 0
     reqs: list = []
 
-    def launch(self, stream: torch.cuda.Stream): ...
+    def launch(self, stream: torch.cuda.Stream, bufs: "SlotBuffers | None" = None): ...
 
     def finish(self): ...
 
@@ -164,7 +214,7 @@ class FilterGroup(Job):
         self.end = [cat.sales_end[r.table] for r in reqs]
         self.mem = 256 * len(reqs) + 8 * sum(e - b for b, e in zip(self.begin, self.end)) // 1024 + (1 << 16)
 
-    def launch(self, stream):
+    def launch(self, stream, bufs=None):
         self.stream = stream
         with torch.cuda.stream(stream):
             self.states = ops.AggStates(self.plans.aggs, len(self.reqs), stream=stream.cuda_stream)
@@ -188,13 +238,16 @@ class OrderJob(Job):
         self.ws_bytes = max(256, ops.order_by_segments_workspace_bytes(self.tbl.columns[0], [0, n]))
         self.mem = 36 * n + self.ws_bytes
 
-    def launch(self, stream):
+    def launch(self, stream, bufs: SlotBuffers | None = None):
         n = self.tbl.rows
         self.stream = stream
         with torch.cuda.stream(stream):
-            self.out = ops.DeviceBatch([ops.DeviceColumn.empty(t, n, w if t == A.TEXT else None)
-                                        for t, w in zip(ORDER_TYPES, ORDER_WIDTHS)])
-            self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device="cuda")
+            if bufs is not None and not self.keep:
+                self.out, self.ws = bufs.order(n, self.ws_bytes)
+            else:
+                self.out = ops.DeviceBatch([ops.DeviceColumn.empty(t, n, w if t == A.TEXT else None)
+                                            for t, w in zip(ORDER_TYPES, ORDER_WIDTHS)])
+                self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device="cuda")
             ops.order_by_segments(self.tbl, 0, True, self.offs, self.out, config=self.plans.order_cfg,
                                   workspace=self.ws, stream=stream.cuda_stream)
             self.event = torch.cuda.Event()
@@ -214,7 +267,7 @@ class JoinJob(Job):
         self.cat, self.plans, self.reqs = cat, plans, [req]
         self.mem = 1 << 20
 
-    def launch(self, stream):
+    def launch(self, stream, bufs=None):
         self.stream = stream
         with torch.cuda.stream(stream):
             self.state = ops.AggState(self.plans.join.aggs, stream=stream.cuda_stream)
@@ -236,7 +289,7 @@ class SubqueryJob(Job):
         self.tbl = cat.sales_view(cat.ntables + req.table)
         self.mem = (1 << 20) + 8 * self.tbl.rows
 
-    def launch(self, stream):
+    def launch(self, stream, bufs=None):
         self.stream = stream
         with torch.cuda.stream(stream):
             plan = self.plans.avg[self.reqs[0].param]
@@ -259,7 +312,7 @@ class SubqueryRows(Job):
         self.tbl = first.tbl
         self.mem = 8 * self.tbl.rows + (1 << 20)
 
-    def launch(self, stream):
+    def launch(self, stream, bufs=None):
         p = self.first.plans
         c = self.reqs[0].param
         eq = Compare(A.EQ, ColumnRef(3, A.TEXT), Constant(datagen.CATEGORIES[c], A.TEXT))
@@ -271,7 +324,10 @@ class SubqueryRows(Job):
         n = max(1, self.tbl.rows)
         self.stream = stream
         with torch.cuda.stream(stream):
-            self.outs = [ops.DeviceColumn.empty(A.FLOAT32, n), ops.DeviceColumn.empty(A.INT32, n)]
+            if bufs is not None and not self.first.keep:
+                self.outs = bufs.subquery(n)
+            else:
+                self.outs = [ops.DeviceColumn.empty(A.FLOAT32, n), ops.DeviceColumn.empty(A.INT32, n)]
             self.cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
             oc = (A.Column * 2)(*[o.c() for o in self.outs])
             b, keep = self.tbl.c()
@@ -312,13 +368,14 @@ def _wait_until(t0: float, at: float):
 def serve_plain(trace: list[Request], cat: Catalog, plans: Plans, keep: bool = False) -> dict:
     """One request at a time, in arrival order, on one stream."""
     stream = torch.cuda.Stream()
+    bufs = cat.slot_buffers(0).ensure()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for r in trace:
         _wait_until(t0, r.arrival)
         job = make_job(cat, plans, r, keep)
         while job is not None:
-            job.launch(stream)
+            job.launch(stream, bufs)
             job.event.synchronize()
             job.finish()
             job = job.next_stage()
@@ -331,6 +388,8 @@ def serve_continuous(trace: list[Request], cat: Catalog, plans: Plans, slots: in
     """Admit requests as streams and budget free up; overlap their work on the
     device; co-launch pending filter requests as one segmented launch."""
     streams = [torch.cuda.Stream() for _ in range(slots)]
+    for sl in range(slots):
+        cat.slot_buffers(sl).ensure()
     free = list(range(slots))
     pending: deque[Request] = deque()
     ready: deque[Job] = deque()  # later stages of admitted requests (go first)
@@ -386,7 +445,7 @@ def serve_continuous(trace: list[Request], cat: Catalog, plans: Plans, slots: in
             else:
                 pending.popleft()
             sl = free.pop()
-            job.launch(streams[sl])
+            job.launch(streams[sl], cat.slot_buffers(sl))
             used += job.mem
             inflight.append((job, sl))
             peak_inflight = max(peak_inflight, len(inflight))
