@@ -21,13 +21,14 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <array>
 #include <mutex>
 #include <string>
 #include <unordered_map>
 #include <vector>
 #include <nvrtc.h>  // types and prototypes only
 #include "yq_jit.cuh"
-#include "yq_stage.cuh"
+#include "row_kernels.cuh"
 
 // Device headers embedded by the build (yallasql_b200/build.py).
 extern const int yq_jit_header_count;
@@ -108,7 +109,21 @@ const char* kernel_decl(JitKind kind) {
   }
 }
 
-std::string make_source(JitKind kind, bool staged, const VmProgram& P, int seg0_end, int end, int min_blocks) {
+// The source-column copies of a WHERE + projection: (output, column, width,
+// output nulls, source nulls) for each projection that copies a column.
+std::vector<std::array<int, 5>> copy_list(const FPParams* fp) {
+  std::vector<std::array<int, 5>> v;
+  if (!fp) return v;
+  for (int p = 0; p < fp->nproj; ++p) {
+    const DevOut& o = fp->out[p];
+    if (o.src_col < 0) continue;
+    v.push_back({p, o.src_col, o.width, o.nulls ? 1 : 0, fp->P.cols[o.src_col].nulls ? 1 : 0});
+  }
+  return v;
+}
+
+std::string make_source(JitKind kind, bool staged, const VmProgram& P, int seg0_end, int end, int min_blocks,
+                        const FPParams* fp) {
   std::string s;
   s += "#include \"row_kernels.cuh\"\n#define STAGED_ ";
   s += staged ? "true" : "false";
@@ -128,14 +143,25 @@ std::string make_source(JitKind kind, bool staged, const VmProgram& P, int seg0_
       s += line;
     }
   }
-  s += "    }\n  }\n};\n}  // namespace yq\n";
+  s += "    }\n  }\n";
+  if (kind == JIT_FILTER_PROJECT) {
+    s += "  template <bool STAGED>\n  __device__ __forceinline__ static void copies(const FPParams& F, const Ctx& X,"
+         " const ProjEmit& E) {\n";
+    for (const auto& c : copy_list(fp)) {
+      snprintf(line, sizeof(line), "    copy_column<STAGED, %d, %d, %d, %s, %s>(F, X, E);\n", c[0], c[1], c[2],
+               c[3] ? "true" : "false", c[4] ? "true" : "false");
+      s += line;
+    }
+    s += "  }\n";
+  }
+  s += "};\n}  // namespace yq\n";
   s += "extern \"C\" __global__ void __launch_bounds__(256, " + std::to_string(min_blocks) + ") yq_jit_kernel";
   s += kernel_decl(kind);
   s += "\n";
   return s;
 }
 
-std::string cache_key(JitKind kind, bool staged, const VmProgram& P, int seg0_end, int end) {
+std::string cache_key(JitKind kind, bool staged, const VmProgram& P, int seg0_end, int end, const FPParams* fp) {
   std::string k;
   k.reserve(16 + (size_t)end * sizeof(RInsn));
   k += (char)('0' + (int)kind);
@@ -143,6 +169,8 @@ std::string cache_key(JitKind kind, bool staged, const VmProgram& P, int seg0_en
   k.append(reinterpret_cast<const char*>(&seg0_end), sizeof(int));
   k.append(reinterpret_cast<const char*>(&end), sizeof(int));
   k.append(reinterpret_cast<const char*>(P.code), (size_t)end * sizeof(RInsn));
+  if (kind == JIT_FILTER_PROJECT)
+    for (const auto& c : copy_list(fp)) k.append(reinterpret_cast<const char*>(c.data()), sizeof(int) * 5);
   return k;
 }
 
@@ -200,11 +228,11 @@ const void* compile_locked(const std::string& src, long* spills) {
 
 }  // namespace
 
-const void* jit_kernel(JitKind kind, bool staged, const VmProgram& P, int seg0_end, int end) {
+const void* jit_kernel(JitKind kind, bool staged, const VmProgram& P, int seg0_end, int end, const FPParams* fp) {
   if (end < 0 || end > kMaxInsns || seg0_end < 0 || seg0_end > end) return nullptr;
   std::lock_guard<std::mutex> lk(g_mu);
   if (!enabled_locked()) return nullptr;
-  const std::string key = cache_key(kind, staged, P, seg0_end, end);
+  const std::string key = cache_key(kind, staged, P, seg0_end, end, fp);
   auto it = g_cache.find(key);
   if (it != g_cache.end()) {
     ++g_hits;
@@ -217,7 +245,7 @@ const void* jit_kernel(JitKind kind, bool staged, const VmProgram& P, int seg0_e
     // kernel fits them without spilling, else for three, else for two.
     long spills = 0;
     for (int blocks = 4; blocks >= 2; --blocks) {
-      k = compile_locked(make_source(kind, staged, P, seg0_end, end, blocks), &spills);
+      k = compile_locked(make_source(kind, staged, P, seg0_end, end, blocks, fp), &spills);
       if (!k || spills == 0) break;
     }
     g_compile_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

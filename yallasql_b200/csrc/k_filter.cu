@@ -304,7 +304,7 @@ static int launch_filter_project(FPParams& F, uint32_t rows, uint32_t* misc, uns
   for (int p = 0; p < F.nproj; ++p)
     if (F.out[p].src_col >= 0) mask |= 1u << F.out[p].src_col;
   // algorithmic bytes: referenced input columns (outputs depend on selectivity)
-  const void* jk = allow_jit ? jit_kernel(JIT_FILTER_PROJECT, staged, F.P, F.pred_end, F.proj_end) : nullptr;
+  const void* jk = allow_jit ? jit_kernel(JIT_FILTER_PROJECT, staged, F.P, F.pred_end, F.proj_end, &F) : nullptr;
   ProfScope ps("filter_project", s, (double)rows * row_bytes_of(F.P, mask));
   if (jk) {
     uint32_t* err = misc + 1;

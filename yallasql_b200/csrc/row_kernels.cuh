@@ -19,12 +19,22 @@ namespace yq {
 
 // Runs instructions [begin, end) of segment `seg` (0 = the predicate or the
 // whole program, 1 = what follows the predicate) through the opcode switch.
+struct FPParams;
+struct ProjEmit;
+template <bool STAGED>
+__device__ __forceinline__ void copy_source_columns(const FPParams& F, const Ctx& X, const ProjEmit& E);
+
 struct InterpRunner {
   template <bool STAGED, typename Emit>
   __device__ __forceinline__ static void run(const VmProgram& P, int seg, int begin, int end, const Ctx& X, Stack& S,
                                              Emit& E) {
     (void)seg;
     run_vm<STAGED>(P, begin, end, X, S, E);
+  }
+  // WHERE + projection: the projections that copy a source column.
+  template <bool STAGED>
+  __device__ __forceinline__ static void copies(const FPParams& F, const Ctx& X, const ProjEmit& E) {
+    copy_source_columns<STAGED>(F, X, E);
   }
 };
 
@@ -296,6 +306,30 @@ __device__ __forceinline__ void copy_source_columns(const FPParams& F, const Ctx
   }
 }
 
+// One projection that copies source column C (W-byte cells) to output P, as
+// copy_source_columns does for all of them; ON / SN: the output / the source
+// has null bytes. The program-specialised kernels list their copies with
+// these as compile-time constants.
+template <bool STAGED, int P, int C, int W, bool ON, bool SN>
+__device__ __forceinline__ void copy_column(const FPParams& F, const Ctx& X, const ProjEmit& E) {
+  const DevOut& o = F.out[P];
+  const DevCol& c = F.P.cols[C];
+  for (uint32_t i = threadIdx.x & 31u; i < E.wcount; i += 32) {
+    const uint32_t q = E.wbase + i;
+    if (q >= F.capacity) break;
+    const uint32_t lr = E.W->rows[i];
+    const char* src;
+    if constexpr (STAGED) src = reinterpret_cast<const char*>(yq_dyn_smem + X.stage + c.soff + lr * (uint32_t)W);
+    else src = c.data + (size_t)(X.tile0 + lr) * W;
+    copy_cell_any(o.data + (size_t)q * W, src, W);
+    if constexpr (ON) {
+      uint8_t nul = 0;
+      if constexpr (SN) nul = STAGED ? yq_dyn_smem[X.stage + c.snoff + lr] : c.nulls[X.tile0 + lr];
+      o.nulls[q] = nul;
+    }
+  }
+}
+
 // Rows are cut into chunks of F.csteps 1,024-row steps. Chunks are claimed in
 // order from a counter (when the staging ring reaches the next one), and every
 // block processes its claims in order, so each chunk's predecessors are held
@@ -393,7 +427,7 @@ __device__ __forceinline__ void filter_project_body(const FPParams& F, uint32_t 
             if (E.sel >> k & 1u) E.W->rows[e++] = (uint16_t)(X.lr + k);
           __syncwarp();
           if (F.proj_end > F.pred_end) R::template run<STAGED>(F.P, 1, F.pred_end, F.proj_end, X, St, E);
-          copy_source_columns<STAGED>(F, X, E);
+          R::template copies<STAGED>(F, X, E);
         }
         run += ((j < 4 ? tot_lo : tot_hi) >> sh) & 0xffffu;
       }

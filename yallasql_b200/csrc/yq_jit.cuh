@@ -12,7 +12,12 @@ enum JitKind { JIT_FILTER_AGG = 0, JIT_FILTER_AGG_SEG = 1, JIT_FILTER_PROJECT = 
 // this program (cached by its instruction words; constants stay parameters).
 // Null when runtime compilation is switched off or unavailable, or failed:
 // the caller then launches the interpreter kernel, which computes the same.
-const void* jit_kernel(JitKind kind, bool staged, const VmProgram& P, int seg0_end, int end);
+// For JIT_FILTER_PROJECT, `fp` lists the projections that copy a source
+// column; the kernel copies them with their columns and widths as constants
+// (they are part of the cache key).
+struct FPParams;
+const void* jit_kernel(JitKind kind, bool staged, const VmProgram& P, int seg0_end, int end,
+                       const FPParams* fp = nullptr);
 
 // Ring depth for `kernel` with stages of `stage_bytes`: of 2..kStageMax stages,
 // the count that lets the most blocks share an SM, the deeper ring on a tie
