@@ -49,6 +49,40 @@ def test_join_pairs_match_oracle(cuda, L, R, conds):
     np.testing.assert_array_equal(gr, wr)
 
 
+_NP_CMP = {A.LT: np.less, A.LE: np.less_equal, A.GT: np.greater, A.GE: np.greater_equal, A.EQ: np.equal,
+           A.NE: np.not_equal}
+
+
+@pytest.mark.parametrize("kind", ["i32", "i64", "f32", "f64", "date"])
+@pytest.mark.parametrize("cmp", [A.LT, A.LE, A.GT, A.GE, A.EQ, A.NE])
+def test_single_inequality_nested_loop_types(cuda, kind, cmp):
+    """One comparison of two null-free columns of the same type (the typed
+    nested-loop kernel): right side longer than one shared-memory chunk,
+    floats with NaN and signed zeros. IEEE comparisons are the SQL results
+    (NaN satisfies only <>, -0.0 equals +0.0)."""
+    rng = np.random.default_rng(len(kind) * 7 + cmp)
+    L, R = 131, 9_001
+
+    def side(n):
+        if kind == "i32":
+            return rng.integers(-30, 30, n).astype(np.int32), A.INT32
+        if kind in ("i64", "date"):
+            return rng.integers(-(1 << 35), 1 << 35, n).astype(np.int64) // (1 << 30), \
+                (A.INT64 if kind == "i64" else A.DATETIME)
+        dt = np.float32 if kind == "f32" else np.float64
+        v = rng.choice(np.array([0.0, -0.0, 1.5, -2.5, np.nan, 3.0], dt), n)
+        return v, (A.FLOAT32 if kind == "f32" else A.FLOAT64)
+
+    (x, tx), (y, ty) = side(L), side(R)
+    gl, gr = pairs_np(*ops.join_pairs(ops.DeviceBatch([dev_col(x, tx)]), ops.DeviceBatch([dev_col(y, ty)]),
+                                      [(0, 0, cmp)]))
+    with np.errstate(invalid="ignore"):
+        m = _NP_CMP[cmp](x[:, None], y[None, :])
+    wl, wr = np.nonzero(m)  # row-major: left ascending, then right ascending
+    np.testing.assert_array_equal(gl, wl.astype(np.uint32))
+    np.testing.assert_array_equal(gr, wr.astype(np.uint32))
+
+
 def test_join_project_writes_pair_columns(cuda):
     rng = np.random.default_rng(5)
     lc, _ = random_side(rng, 4000)

@@ -383,6 +383,114 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_nested(const __grid_constan
   if (tile == gridDim.x - 1 && threadIdx.x == 0) *J.total = s_prefix + total;
 }
 
+// Nested loop for one comparison of two columns of the same fixed-width
+// numeric type without nulls (the common inequality join): the right column
+// is staged in shared memory kNlChunk rows at a time, each warp holds its
+// kNlRowsPerWarp left values in registers, and every right value a lane
+// loads is compared with all of them, so a comparison costs a compare, a
+// ballot and a popc. IEEE comparisons give the SQL results for NaN (only <>
+// holds) and for -0.0 = +0.0. Same tiles, look-back and output order (left
+// row major, right rows ascending) as k_join_nested.
+constexpr uint32_t kNlChunk = 4096;
+
+template <typename T, int OP>
+__device__ __forceinline__ bool nl_cmp(T a, T b) {
+  if constexpr (OP == YQ_LT) return a < b;
+  else if constexpr (OP == YQ_LE) return a <= b;
+  else if constexpr (OP == YQ_GT) return a > b;
+  else if constexpr (OP == YQ_GE) return a >= b;
+  else if constexpr (OP == YQ_EQ) return a == b;
+  else return a != b;
+}
+
+template <typename T, int OP>
+__global__ void __launch_bounds__(kJoinBlock) k_join_nested_typed(const __grid_constant__ JoinParams J) {
+  __shared__ T s_r[kNlChunk];
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_cnt[kNlTile];
+  __shared__ uint32_t s_warp[kJoinBlock / 32 + 1];
+  __shared__ unsigned long long s_prefix;
+  if (threadIdx.x == 0) s_tile = atomicAdd(J.tile_counter, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = lanemask_lt();
+  const JCond& c = J.cond[0];
+  const T* lcol = reinterpret_cast<const T*>(c.l.data);
+  const T* rcol = reinterpret_cast<const T*>(c.r.data);
+  T lv[kNlRowsPerWarp];
+  bool lok[kNlRowsPerWarp];
+#pragma unroll
+  for (int i = 0; i < kNlRowsPerWarp; ++i) {
+    const uint32_t l = tile * kNlTile + warp * kNlRowsPerWarp + i;
+    lok[i] = l < J.L;
+    lv[i] = lok[i] ? __ldg(lcol + l) : T(0);
+  }
+  // pass 1: matches per left row
+  uint32_t cnt[kNlRowsPerWarp];
+#pragma unroll
+  for (int i = 0; i < kNlRowsPerWarp; ++i) cnt[i] = 0;
+  for (uint32_t r0 = 0; r0 < J.R; r0 += kNlChunk) {
+    const uint32_t n = min(kNlChunk, J.R - r0);
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < n; x += kJoinBlock) s_r[x] = __ldg(rcol + r0 + x);
+    __syncthreads();
+    for (uint32_t x = lane; x < ((n + 31) & ~31u); x += 32) {
+      const bool ok = x < n;
+      const T rv = ok ? s_r[x] : T(0);
+#pragma unroll
+      for (int i = 0; i < kNlRowsPerWarp; ++i) cnt[i] += __popc(__ballot_sync(0xffffffffu, ok && lok[i] && nl_cmp<T, OP>(lv[i], rv)));
+    }
+  }
+  if (lane == 0)
+#pragma unroll
+    for (int i = 0; i < kNlRowsPerWarp; ++i) s_cnt[warp * kNlRowsPerWarp + i] = cnt[i];
+  __syncthreads();
+  const uint32_t mine = threadIdx.x < kNlTile ? s_cnt[threadIdx.x] : 0u;
+  uint32_t total;
+  const uint32_t excl = block_exclusive_sum<kJoinBlock>(mine, s_warp, total);
+  if (threadIdx.x < kNlTile) s_cnt[threadIdx.x] = excl;  // row offset within the tile
+  if (threadIdx.x < 32) {
+    const unsigned long long p = tile_lookback(J.status, tile, total, J.err);
+    if (threadIdx.x == 0) s_prefix = p;
+  }
+  __syncthreads();
+  // pass 2: write the matches, consecutive positions per left row
+  unsigned long long pos[kNlRowsPerWarp];
+#pragma unroll
+  for (int i = 0; i < kNlRowsPerWarp; ++i) pos[i] = s_prefix + s_cnt[warp * kNlRowsPerWarp + i];
+  for (uint32_t r0 = 0; r0 < J.R; r0 += kNlChunk) {
+    const uint32_t n = min(kNlChunk, J.R - r0);
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < n; x += kJoinBlock) s_r[x] = __ldg(rcol + r0 + x);
+    __syncthreads();
+    for (uint32_t x = lane; x < ((n + 31) & ~31u); x += 32) {
+      const bool ok = x < n;
+      const T rv = ok ? s_r[x] : T(0);
+#pragma unroll
+      for (int i = 0; i < kNlRowsPerWarp; ++i) {
+        const bool m = ok && lok[i] && nl_cmp<T, OP>(lv[i], rv);
+        const uint32_t bal = __ballot_sync(0xffffffffu, m);
+        if (m) emit_pair(J, pos[i] + __popc(bal & lt), tile * kNlTile + warp * kNlRowsPerWarp + i, r0 + x);
+        pos[i] += __popc(bal);
+      }
+    }
+  }
+  if (tile == gridDim.x - 1 && threadIdx.x == 0) *J.total = s_prefix + total;
+}
+
+template <typename T>
+static void launch_nested_typed(int op, unsigned grid, const JoinParams& J, cudaStream_t s) {
+  switch (op) {
+    case YQ_LT: k_join_nested_typed<T, YQ_LT><<<grid, kJoinBlock, 0, s>>>(J); break;
+    case YQ_LE: k_join_nested_typed<T, YQ_LE><<<grid, kJoinBlock, 0, s>>>(J); break;
+    case YQ_GT: k_join_nested_typed<T, YQ_GT><<<grid, kJoinBlock, 0, s>>>(J); break;
+    case YQ_GE: k_join_nested_typed<T, YQ_GE><<<grid, kJoinBlock, 0, s>>>(J); break;
+    case YQ_EQ: k_join_nested_typed<T, YQ_EQ><<<grid, kJoinBlock, 0, s>>>(J); break;
+    default: k_join_nested_typed<T, YQ_NE><<<grid, kJoinBlock, 0, s>>>(J); break;
+  }
+}
+
 // ------------------------------------------------------- cross product
 // Every (l, r), left-major: output row l*R + r.
 __global__ void __launch_bounds__(256) k_cross_fill(const __grid_constant__ JoinParams J) {
@@ -577,7 +685,21 @@ static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_
     YQ_CHECK_LAUNCH();
   } else {
     ProfScope ps("join_nested_loop", s, (double)J.L * J.R * 0.0);
-    k_join_nested<<<ntiles, kJoinBlock, 0, s>>>(J);
+    const JCond& c0 = J.cond[0];
+    const bool typed = J.ncond == 1 && c0.l.type == c0.r.type && !c0.l.nulls && !c0.r.nulls &&
+                       c0.l.width == c0.r.width && (c0.l.type == YQ_INT32 || c0.l.type == YQ_FLOAT32 ||
+                                                     c0.l.type == YQ_INT64 || c0.l.type == YQ_DATETIME ||
+                                                     c0.l.type == YQ_FLOAT64);
+    if (typed) {
+      switch (c0.l.type) {
+        case YQ_INT32: launch_nested_typed<int32_t>(c0.cmp, ntiles, J, s); break;
+        case YQ_FLOAT32: launch_nested_typed<float>(c0.cmp, ntiles, J, s); break;
+        case YQ_FLOAT64: launch_nested_typed<double>(c0.cmp, ntiles, J, s); break;
+        default: launch_nested_typed<long long>(c0.cmp, ntiles, J, s); break;  // INT64, DATETIME
+      }
+    } else {
+      k_join_nested<<<ntiles, kJoinBlock, 0, s>>>(J);
+    }
     YQ_CHECK_LAUNCH();
   }
   unsigned long long h_total = 0;
