@@ -38,7 +38,9 @@ def check_aggs(got, want):
             assert g == w, (got, want)
 
 
-@pytest.mark.parametrize("rows", [1_000_000, 0, 1, 5, 1023, 1024, 1025, 77_777])
+# 3,000,017 rows: enough steps per block for the staged (shared-memory ring)
+# kernel; the smaller batches take the unstaged one.
+@pytest.mark.parametrize("rows", [1_000_000, 0, 1, 5, 1023, 1024, 1025, 77_777, 3_000_017])
 def test_sales_query_matches_oracle(cuda, orc, rows):
     t = datagen.sales_table(max(rows, 1), seed=0)
     cols = [t["price"][:rows], t["qty"][:rows], t["discount"][:rows], t["category"][:rows]]

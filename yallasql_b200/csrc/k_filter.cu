@@ -134,8 +134,15 @@ static int prepare_filter_aggregate(const yq_batch* batch, const yq_program* pre
   return YQ_OK;
 }
 
-static int launch_filter_aggregate(const FAParams& F, uint32_t rows, Acc* partials, uint32_t* ticket, Acc* state,
+// Batches with fewer steps than about four per resident block (1M rows and
+// less) skip the staging ring: every block then handles one or two steps, and
+// setting up a ring (barriers, copies issued ahead) costs more than it hides.
+static bool few_steps(uint32_t rows) { return ceil_div<uint32_t>(rows, kStepRows) < 12u * (uint32_t)sm_count(); }
+
+static int launch_filter_aggregate(const FAParams& F0, uint32_t rows, Acc* partials, uint32_t* ticket, Acc* state,
                                    cudaStream_t s) {
+  FAParams F = F0;
+  if (few_steps(rows)) F.SP.nstages = 0;
   const bool staged = F.SP.nstages > 0;
   const void* kern = staged ? (const void*)k_filter_aggregate<true> : (const void*)k_filter_aggregate<false>;
   const size_t smem = stage_smem_bytes(F.SP);

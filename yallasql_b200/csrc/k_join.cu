@@ -435,13 +435,17 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_nested_typed(const __grid_c
     __syncthreads();
     for (uint32_t x = threadIdx.x; x < n; x += kJoinBlock) s_r[x] = __ldg(rcol + r0 + x);
     __syncthreads();
-    for (uint32_t x = lane; x < ((n + 31) & ~31u); x += 32) {
-      const bool ok = x < n;
-      const T rv = ok ? s_r[x] : T(0);
+    // per-lane counts (one predicated add a comparison), summed over the warp below
+    for (uint32_t x = lane; x < n; x += 32) {
+      const T rv = s_r[x];
 #pragma unroll
-      for (int i = 0; i < kNlRowsPerWarp; ++i) cnt[i] += __popc(__ballot_sync(0xffffffffu, ok && lok[i] && nl_cmp<T, OP>(lv[i], rv)));
+      for (int i = 0; i < kNlRowsPerWarp; ++i) cnt[i] += (lok[i] && nl_cmp<T, OP>(lv[i], rv)) ? 1u : 0u;
     }
   }
+#pragma unroll
+  for (int i = 0; i < kNlRowsPerWarp; ++i)
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) cnt[i] += __shfl_xor_sync(0xffffffffu, cnt[i], d);
   if (lane == 0)
 #pragma unroll
     for (int i = 0; i < kNlRowsPerWarp; ++i) s_cnt[warp * kNlRowsPerWarp + i] = cnt[i];

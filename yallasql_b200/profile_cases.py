@@ -3,6 +3,9 @@
     python -m yallasql_b200.profile_cases filter   # 32M-row sales table: WHERE + aggregate, then WHERE + projection
     python -m yallasql_b200.profile_cases join     # 30M-row fact table joined to the 2,556-row date table + SUM
     python -m yallasql_b200.profile_cases order    # 16M rows (key f32, id, 16-byte txt, date), 116,480-row runs
+    python -m yallasql_b200.profile_cases cross    # 20K x 20K cross product with < (198M output pairs)
+
+An optional second argument sets the row count (rows per side for cross).
 
 The inputs are larger than L2 (so DRAM counters mean something) and hold a few
 GB of device memory at most; every case runs its operators once and exits.
@@ -66,11 +69,21 @@ def order_case(rows: int = 16_000_000, run_rows: int = 116_480) -> None:
     torch.cuda.synchronize()
 
 
-CASES = {"filter": filter_case, "join": join_case, "order": order_case}
+def cross_case(rows: int = 20_000) -> None:
+    x, y = datagen.cross_tables(rows, seed=2)
+    ops.join_project(ops.DeviceBatch([_dev(x, A.INT32)]), ops.DeviceBatch([_dev(y, A.INT32)]), [(0, 0, A.LT)],
+                     [(0, 0), (1, 0)])
+    torch.cuda.synchronize()
+
+
+CASES = {"filter": filter_case, "join": join_case, "order": order_case, "cross": cross_case}
 
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "filter"
     if which not in CASES:
         raise SystemExit(f"unknown case {which!r}; one of {sorted(CASES)}")
-    CASES[which]()
+    if len(sys.argv) > 2:
+        CASES[which](int(sys.argv[2]))
+    else:
+        CASES[which]()
     print("ok")
