@@ -403,7 +403,16 @@ __device__ __forceinline__ bool nl_cmp(T a, T b) {
   else return a != b;
 }
 
-template <typename T, int OP>
+// Outputs of a join that are all 4- or 8-byte cells without null bytes (at
+// most kSimpleOut of them, e.g. one column of each side): the typed kernel
+// writes them directly, reading each left row's cells once.
+constexpr int kSimpleOut = 2;
+
+__device__ __forceinline__ unsigned long long cell_bits(const char* p, int w) {
+  return w == 8 ? __ldg(reinterpret_cast<const unsigned long long*>(p)) : (unsigned long long)__ldg(reinterpret_cast<const uint32_t*>(p));
+}
+
+template <typename T, int OP, bool SIMPLE>
 __global__ void __launch_bounds__(kJoinBlock) k_join_nested_typed(const __grid_constant__ JoinParams J) {
   __shared__ T s_r[kNlChunk];
   __shared__ uint32_t s_tile;
@@ -463,6 +472,17 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_nested_typed(const __grid_c
   unsigned long long pos[kNlRowsPerWarp];
 #pragma unroll
   for (int i = 0; i < kNlRowsPerWarp; ++i) pos[i] = s_prefix + s_cnt[warp * kNlRowsPerWarp + i];
+  unsigned long long lcell[kNlRowsPerWarp][SIMPLE ? kSimpleOut : 1];  // left-side output cells of each row
+  if constexpr (SIMPLE) {
+#pragma unroll
+    for (int i = 0; i < kNlRowsPerWarp; ++i)
+#pragma unroll
+      for (int o = 0; o < kSimpleOut; ++o) {
+        const uint32_t l = tile * kNlTile + warp * kNlRowsPerWarp + i;
+        lcell[i][o] = (o < J.nout && J.out[o].side == 0 && lok[i])
+                          ? cell_bits(J.out[o].src + (size_t)l * J.out[o].width, J.out[o].width) : 0ull;
+      }
+  }
   for (uint32_t r0 = 0; r0 < J.R; r0 += kNlChunk) {
     const uint32_t n = min(kNlChunk, J.R - r0);
     __syncthreads();
@@ -475,7 +495,24 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_nested_typed(const __grid_c
       for (int i = 0; i < kNlRowsPerWarp; ++i) {
         const bool m = ok && lok[i] && nl_cmp<T, OP>(lv[i], rv);
         const uint32_t bal = __ballot_sync(0xffffffffu, m);
-        if (m) emit_pair(J, pos[i] + __popc(bal & lt), tile * kNlTile + warp * kNlRowsPerWarp + i, r0 + x);
+        if (m) {
+          const unsigned long long at = pos[i] + __popc(bal & lt);
+          if constexpr (SIMPLE) {
+            if (at < J.capacity) {
+#pragma unroll
+              for (int o = 0; o < kSimpleOut; ++o) {
+                if (o >= J.nout) break;
+                const JOut& w = J.out[o];
+                const unsigned long long v =
+                    w.side ? cell_bits(w.src + (size_t)(r0 + x) * w.width, w.width) : lcell[i][o];
+                if (w.width == 8) reinterpret_cast<unsigned long long*>(w.dst)[at] = v;
+                else reinterpret_cast<uint32_t*>(w.dst)[at] = (uint32_t)v;
+              }
+            }
+          } else {
+            emit_pair(J, at, tile * kNlTile + warp * kNlRowsPerWarp + i, r0 + x);
+          }
+        }
         pos[i] += __popc(bal);
       }
     }
@@ -483,16 +520,24 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_nested_typed(const __grid_c
   if (tile == gridDim.x - 1 && threadIdx.x == 0) *J.total = s_prefix + total;
 }
 
+template <typename T, bool SIMPLE>
+static void launch_nested_typed_op(int op, unsigned grid, const JoinParams& J, cudaStream_t s) {
+  switch (op) {
+    case YQ_LT: k_join_nested_typed<T, YQ_LT, SIMPLE><<<grid, kJoinBlock, 0, s>>>(J); break;
+    case YQ_LE: k_join_nested_typed<T, YQ_LE, SIMPLE><<<grid, kJoinBlock, 0, s>>>(J); break;
+    case YQ_GT: k_join_nested_typed<T, YQ_GT, SIMPLE><<<grid, kJoinBlock, 0, s>>>(J); break;
+    case YQ_GE: k_join_nested_typed<T, YQ_GE, SIMPLE><<<grid, kJoinBlock, 0, s>>>(J); break;
+    case YQ_EQ: k_join_nested_typed<T, YQ_EQ, SIMPLE><<<grid, kJoinBlock, 0, s>>>(J); break;
+    default: k_join_nested_typed<T, YQ_NE, SIMPLE><<<grid, kJoinBlock, 0, s>>>(J); break;
+  }
+}
+
 template <typename T>
 static void launch_nested_typed(int op, unsigned grid, const JoinParams& J, cudaStream_t s) {
-  switch (op) {
-    case YQ_LT: k_join_nested_typed<T, YQ_LT><<<grid, kJoinBlock, 0, s>>>(J); break;
-    case YQ_LE: k_join_nested_typed<T, YQ_LE><<<grid, kJoinBlock, 0, s>>>(J); break;
-    case YQ_GT: k_join_nested_typed<T, YQ_GT><<<grid, kJoinBlock, 0, s>>>(J); break;
-    case YQ_GE: k_join_nested_typed<T, YQ_GE><<<grid, kJoinBlock, 0, s>>>(J); break;
-    case YQ_EQ: k_join_nested_typed<T, YQ_EQ><<<grid, kJoinBlock, 0, s>>>(J); break;
-    default: k_join_nested_typed<T, YQ_NE><<<grid, kJoinBlock, 0, s>>>(J); break;
-  }
+  bool simple = J.nout >= 1 && J.nout <= kSimpleOut;
+  for (int o = 0; o < J.nout && simple; ++o) simple = (J.out[o].width == 4 || J.out[o].width == 8) && !J.out[o].dst_nulls;
+  if (simple) launch_nested_typed_op<T, true>(op, grid, J, s);
+  else launch_nested_typed_op<T, false>(op, grid, J, s);
 }
 
 // ------------------------------------------------------- cross product
