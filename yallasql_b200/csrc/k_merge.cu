@@ -441,7 +441,7 @@ struct RawGeom {
   static constexpr uint32_t kreg = kMergeTile * W + 64;  // keys of both windows + alignment slack
   static constexpr uint32_t ireg = kMergeTile * 4 + 64;  // ids of both windows + alignment slack
   static constexpr uint32_t slot = kreg + ireg;
-  static constexpr size_t smem = (size_t)kRawStages * slot + (size_t)kMergeTile * 4 + kRawStages * 8;
+  static constexpr size_t smem = (size_t)kRawStages * slot + kRawStages * 8;
 };
 
 // Copy rows [r0, r0 + n) (w bytes each) from their 16-byte hull; returns the
@@ -466,7 +466,7 @@ __device__ __forceinline__ void raw_issue(const RawLevel& L, const RawTile& d, i
   using G = RawGeom<KW>;
   unsigned char* kreg = smem + (size_t)slot * G::slot;
   unsigned char* ireg = kreg + G::kreg;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + (size_t)kRawStages * G::slot + (size_t)kMergeTile * 4) + slot;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + (size_t)kRawStages * G::slot) + slot;
   uint32_t bytes = 0, ko = 0, io = 0;
   // sizes first (expect_tx before the copies)
   RawSlot r;
@@ -563,8 +563,7 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
   using G = RawGeom<KW>;
   extern __shared__ __align__(128) unsigned char raw_smem[];
   __shared__ RawSlot s_slot[kRawStages];
-  uint32_t* s_src = reinterpret_cast<uint32_t*>(raw_smem + (size_t)kRawStages * G::slot);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(raw_smem + (size_t)kRawStages * G::slot + (size_t)kMergeTile * 4);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(raw_smem + (size_t)kRawStages * G::slot);
   const uint32_t NT = L.ntiles, GR = gridDim.x;
   if (threadIdx.x == 0)
     for (int s = 0; s < kRawStages; ++s) mbar_init(bars + s, 1);
@@ -581,7 +580,7 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
   int slot = 0;
   uint32_t parity = 0;
   for (uint32_t t = blockIdx.x; t < NT; t += GR) {
-    __syncthreads();  // every thread is done with the previous tile: its slot and s_src are free
+    __syncthreads();  // every thread is done with the previous tile: its slot is free
     if (threadIdx.x == 0) {
       const uint32_t tn = t + (uint32_t)(kRawStages - 1) * GR;
       const int ns = slot == 0 ? kRawStages - 1 : slot - 1;
@@ -598,7 +597,9 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
     const unsigned char* kA = kreg + r.ka;
     const unsigned char* kB = kreg + r.kb;
 
-    // Each thread merges kMergeItems consecutive outputs of the tile.
+    // Each thread merges kMergeItems consecutive outputs of the tile in
+    // registers and stores them itself: a warp's stores cover one contiguous
+    // run of 32 x kMergeItems outputs (16-byte stores when aligned).
     const uint32_t kk = threadIdx.x * kMergeItems;
     if (kk < r.cnt) {
       uint32_t lo = kk > r.nb ? kk - r.nb : 0u, hi = kk < r.na ? kk : r.na;
@@ -616,32 +617,51 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
       for (int j = 0; j < KW; ++j) ka[j] = kb[j] = 0u;
       if (ia < r.na) raw_key_s<KW>(kA + (size_t)ia * G::W, ka);
       if (jb < r.nb) raw_key_s<KW>(kB + (size_t)jb * G::W, kb);
+      const uint32_t* idA = reinterpret_cast<const uint32_t*>(ireg + r.ia);
+      const uint32_t* idB = reinterpret_cast<const uint32_t*>(ireg + r.ib);
+      uint32_t okey[kMergeItems][KW], oid[kMergeItems];
+      const uint32_t m = r.cnt - kk < (uint32_t)kMergeItems ? r.cnt - kk : (uint32_t)kMergeItems;
 #pragma unroll
       for (int x = 0; x < kMergeItems; ++x) {
-        if (kk + x >= r.cnt) break;
+        if ((uint32_t)x >= m) break;
         const bool takeA = ia < r.na && (jb >= r.nb || key_le<KW>(ka, kb));
         if (takeA) {
-          s_src[kk + x] = ia++;
+#pragma unroll
+          for (int j = 0; j < KW; ++j) okey[x][j] = ka[j];
+          oid[x] = idA[ia++];
           if (ia < r.na) raw_key_s<KW>(kA + (size_t)ia * G::W, ka);
         } else {
-          s_src[kk + x] = kFromB | jb++;
+#pragma unroll
+          for (int j = 0; j < KW; ++j) okey[x][j] = kb[j];
+          oid[x] = idB[jb++];
           if (jb < r.nb) raw_key_s<KW>(kB + (size_t)jb * G::W, kb);
         }
       }
-    }
-    __syncthreads();
-    // Coalesced writes of the merged keys and ids.
-    for (uint32_t x = threadIdx.x; x < r.cnt; x += kMergeBlock) {
-      const uint32_t v = s_src[x];
-      const bool fromB = (v & kFromB) != 0u;
-      const uint32_t j = v & ~kFromB;
-      const uint32_t id = *reinterpret_cast<const uint32_t*>(ireg + (fromB ? r.ib : r.ia) + 4u * j);
-      L.ids_out[r.out0 + x] = id;
-      if (L.keys_out || L.dec.out) {
-        uint32_t k[KW];
-        raw_key_s<KW>((fromB ? kB : kA) + (size_t)j * G::W, k);
-        if (L.keys_out) raw_key_store<KW>(L.keys_out, (size_t)r.out0 + x, k);
-        else decode_store<KW>(L.dec, (size_t)r.out0 + x, k);
+      const size_t o0 = (size_t)r.out0 + kk;
+      if (m == (uint32_t)kMergeItems && (o0 & 3u) == 0u) {
+#pragma unroll
+        for (int x = 0; x < kMergeItems; x += 4)
+          *reinterpret_cast<uint4*>(L.ids_out + o0 + x) = make_uint4(oid[x], oid[x + 1], oid[x + 2], oid[x + 3]);
+      } else {
+#pragma unroll
+        for (int x = 0; x < kMergeItems; ++x)
+          if ((uint32_t)x < m) L.ids_out[o0 + x] = oid[x];
+      }
+      if (L.keys_out) {
+        if (KW == 1 && m == (uint32_t)kMergeItems && (o0 & 3u) == 0u) {
+#pragma unroll
+          for (int x = 0; x < kMergeItems; x += 4)
+            *reinterpret_cast<uint4*>(L.keys_out + o0 + x) =
+                make_uint4(okey[x][0], okey[x + 1][0], okey[x + 2][0], okey[x + 3][0]);
+        } else {
+#pragma unroll
+          for (int x = 0; x < kMergeItems; ++x)
+            if ((uint32_t)x < m) raw_key_store<KW>(L.keys_out, o0 + x, okey[x]);
+        }
+      } else if (L.dec.out) {
+#pragma unroll
+        for (int x = 0; x < kMergeItems; ++x)
+          if ((uint32_t)x < m) decode_store<KW>(L.dec, o0 + x, okey[x]);
       }
     }
     if (++slot == kRawStages) {
