@@ -288,6 +288,99 @@ def operator_suite(lib, peak: float) -> dict:
     return out
 
 
+def csv_suite(lib, peak: float, rows: int = 8_000_000) -> dict:
+    """CSV scan (the device-side GetOperator::next) over the filter+aggregate
+    table written as CSV text: device-resident text (larger than L2) -> typed
+    columns; per-kernel HBM roofline; the same from pinned host bytes with the
+    host->device copy inside (ingress reported against the measured pinned copy
+    rate); the reference's own reader (csv-parser + std::stoi/stof/strptime) on
+    a bounded sample on the host."""
+    import torch
+    import oracle
+    from yallasql_b200 import _abi as A, datagen, ops
+    header, body = datagen.sales_csv(rows, seed=0)
+    nbytes = int(body.size)
+    types = [A.INT32, A.FLOAT32, A.INT32, A.INT32, A.TEXT, A.DATETIME]
+    host = torch.from_numpy(body).pin_memory()
+    text = host.cuda()
+    s = torch.cuda.current_stream().cuda_stream
+    n = C.c_uint64(0)
+    lib.yq_csv_index(text.data_ptr(), nbytes, None, 0, C.byref(n), None, 0, s)
+    nrec = int(n.value)
+    starts = torch.empty(nrec + 1, dtype=torch.int32, device="cuda")
+    iws = torch.empty(lib.yq_csv_index_workspace_size(nbytes), dtype=torch.uint8, device="cuda")
+    pws = torch.empty(lib.yq_csv_parse_workspace_size(nrec), dtype=torch.uint8, device="cuda")
+    cols = [ops.DeviceColumn.empty(t, nrec, 16 if t == A.TEXT else None, nulls=True) for t in types]
+    ccols = (A.Column * len(cols))(*[c.c() for c in cols])
+    fc = (C.c_int32 * len(types))(*range(len(types)))
+    out_rows = C.c_uint32(0)
+    err = A.CsvError()
+
+    def scan(src):
+        A.check(lib.yq_csv_index(src.data_ptr(), nbytes, starts.data_ptr(), nrec + 1, C.byref(n), iws.data_ptr(),
+                                 iws.numel(), s), "yq_csv_index")
+        A.check(lib.yq_csv_parse(src.data_ptr(), nbytes, starts.data_ptr(), nrec, fc, len(types), ccols, len(cols),
+                                 C.byref(out_rows), C.byref(err), pws.data_ptr(), pws.numel(), s), "yq_csv_parse")
+
+    scan(text)
+    assert out_rows.value == rows
+    torch.cuda.synchronize()
+    lib.yq_profile_enable(1)
+    lib.yq_profile_read(None, 0, 1)
+    reps = 5
+    ms = _timed(lambda: scan(text), reps)
+    buf = C.create_string_buffer(1 << 14)
+    lib.yq_profile_read(buf, len(buf), 1)
+    lib.yq_profile_enable(0)
+    prof = json.loads(buf.value.decode() or "{}")
+    kernels = {}
+    for tag in ("csv_tiles", "csv_tile_scan", "csv_emit", "csv_parse"):
+        k = prof.get(tag, {})
+        if k.get("launches"):
+            per_ms = k["ms"] / k["launches"]
+            gbs = k["units"] / k["launches"] / (per_ms / 1e3) / 1e9
+            kernels[tag] = {"kernel_ms": round(per_ms, 4), "achieved_gbs": round(gbs, 1),
+                            "frac_of_measured_hbm": round(gbs / peak, 4),
+                            "algorithmic_bytes_per_launch": k["units"] / k["launches"]}
+    # from pinned host bytes: the copy in, then the scan (what GetOperator::next + storeBuffer do)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    staging = torch.empty_like(text)
+
+    def e2e():
+        staging.copy_(host, non_blocking=True)
+        scan(staging)
+    e2e()
+    torch.cuda.synchronize()
+    e2e_ms = _timed(e2e, 3)
+    ev0.record()
+    for _ in range(3):
+        staging.copy_(host, non_blocking=True)
+    ev1.record()
+    torch.cuda.synchronize()
+    h2d_gbs = 3 * nbytes / (ev0.elapsed_time(ev1) / 1e3) / 1e9
+    out = {"rows": rows, "csv_bytes": nbytes, "ms": round(ms, 4), "rows_per_s": rows / (ms / 1e3),
+           "text_gbs": round(nbytes / (ms / 1e3) / 1e9, 1), "kernels": kernels,
+           "e2e_from_pinned_host": {"ms": round(e2e_ms, 4), "rows_per_s": rows / (e2e_ms / 1e3),
+                                    "h2d_bytes": nbytes, "ingress_pinned_h2d_gbs": round(h2d_gbs, 1)}}
+    # the reference's reader on the host: bounded sample, one thread of conversions (+ csv-parser's reader thread)
+    sample = min(rows, 1_000_000)
+    cut = int(np.flatnonzero(body == ord("\n"))[sample - 1]) + 1
+    sub = body[:cut].tobytes()
+    t0 = time.perf_counter()
+    if oracle.ref_csv_available():
+        oracle.ref_csv_scan(header, sub, [0, 1, 0, 0, 3, 2], width=16, guess=True)
+        kind = "reference"
+    else:
+        oracle.csv_scan(sub, [0, 1, 0, 0, 3, 2], width=16)
+        kind = "port"
+    dt = time.perf_counter() - t0
+    out["cpu_baseline"] = {"value": sample / dt, "unit": "rows/s", "cores": 1, "kind": kind,
+                           "sample": f"first {sample} of {rows} rows ({cut} bytes): csv-parser read_row + "
+                                     "std::stoi/std::stof/strptime+timegm per field, as GetOperator::next"}
+    del text, staging, cols
+    return out
+
+
 def batched_form(args) -> dict:
     """Batched form (512 tasks, row counts log-uniform in [1K, 4M], seed 3):
     the plain per-task form against the segmented launches replayed as one CUDA
@@ -574,6 +667,7 @@ def main():
         del job
         torch.cuda.empty_cache()
         line["operators"] = operator_suite(lib, peak)
+        line["operators"]["csv_scan_8M"] = csv_suite(lib, peak)
     if rank == 0 and not args.no_batched:
         torch.cuda.empty_cache()
         line["batched"] = batched_form(args)

@@ -524,6 +524,51 @@ int yq_merge_path(const void* a, const void* b, int32_t type, int32_t width,
 int yq_cross_product_col(const yq_column* col, uint32_t left_rows, uint32_t right_rows,
                          int32_t is_left, yq_column* out, void* stream);
 
+/* ---------------------------------------------------------------- CSV scan
+ * Device-side replacement of GetOperator::next's per-row loop
+ * (src/engine/operators/get_operator.cpp:56-109): csv-parser's tokenizer
+ * (vendor/csv-parser/csv.hpp:7063-7140, default format: ',' delimiter, '"'
+ * quote, CR/LF newlines, blank lines skipped) and the per-field conversions
+ * std::stoi / std::stof / getDateTime (strptime "%Y-%m-%d %H:%M:%S" + timegm,
+ * include/enums/data_type_utils.hpp:24-44) / String::set
+ * (include/kernels/string_kernel.hpp:16-31). `data` is the CSV text after the
+ * header line, resident on the device; offsets are 32-bit, so one call takes
+ * less than 4 GiB (the reference reads 4 MiB batches). */
+#define YQ_CSV_MAX_FIELDS 64
+
+/* A cell whose conversion throws in the reference (std::invalid_argument or
+ * std::out_of_range from stoi/stof). The reference's process exits there; this
+ * library writes 0 into the cell, finishes the batch and reports the first one. */
+typedef struct yq_csv_error {
+  uint64_t bad_cells;     /* cells that failed to convert                       */
+  uint32_t first_row;     /* output row of the first                            */
+  int32_t first_field;    /* its CSV field index, -1 when there is none         */
+  int32_t kind;           /* 1: nothing converts (invalid_argument), 2: out of range */
+} yq_csv_error;
+
+size_t yq_csv_index_workspace_size(uint64_t nbytes);
+/* Splits the text into records: the byte offset of each record's first byte
+ * goes to record_starts[0..*records). Synchronises `stream` to read the count;
+ * when it exceeds `capacity`, returns YQ_ERR_CAPACITY with *records = the count
+ * and writes nothing (record_starts may be NULL to only count). */
+int yq_csv_index(const uint8_t* data, uint64_t nbytes, uint32_t* record_starts, uint64_t capacity,
+                 uint64_t* records, void* workspace, size_t workspace_bytes, void* stream);
+size_t yq_csv_parse_workspace_size(uint32_t records);
+/* Converts the records into typed columns. field_column[f] is the output
+ * column of CSV field f (0 <= f < nfields, nfields = the header's field count)
+ * or -1 when the field is not projected. Each output column has type INT32,
+ * FLOAT32, DATETIME or TEXT (slot width multiple of 4, <= 256), room for
+ * `records` rows, and a writable null-byte array: an empty field is NULL
+ * (null byte 1, value INT_MIN / FLT_MIN / 0 / empty text, the sentinels of
+ * get_operator.cpp:80-86). Records whose field count differs from nfields are
+ * dropped, order kept (csv-parser's IGNORE_ROW policy); *rows = rows kept.
+ * Synchronises `stream`. Cells that fail to convert: YQ_ERR_INVALID_ARG with
+ * *error filled, every other cell still converted. Dropping rows allocates
+ * stream-ordered temporaries (cudaMallocAsync) even with a workspace. */
+int yq_csv_parse(const uint8_t* data, uint64_t nbytes, const uint32_t* record_starts, uint32_t records,
+                 const int32_t* field_column, int32_t nfields, yq_column* out, int32_t ncols, uint32_t* rows,
+                 yq_csv_error* error, void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------- device */
 /* Number of SMs of the current device (cached per device). */
 int yq_device_sm_count(void);

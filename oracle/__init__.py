@@ -154,3 +154,98 @@ def cross_lt(x: np.ndarray, y: np.ndarray, cap=None):
     oy = np.empty(max(1, cap), dtype=np.int32)
     n = lib().orc_cross_lt(_ptr(x), len(x), _ptr(y), len(y), _ptr(ox), _ptr(oy), cap)
     return ox[: min(n, cap)], oy[: min(n, cap)], n
+
+
+# ------------------------------------------------------------------ CSV scan
+REF_CSV_LIB = os.path.join(HERE, "_ref", "libcsvref.so")
+CSV_WIDTH = {0: 4, 1: 4, 2: 8}
+CSV_DTYPE = {0: np.int32, 1: np.float32, 2: np.int64}
+
+
+def _csv_outputs(types, width, cap):
+    datas, nulls = [], []
+    for t in types:
+        if t < 0:
+            datas.append(np.zeros(1, np.uint8))
+            nulls.append(np.zeros(1, np.uint8))
+            continue
+        w = width if t == 3 else CSV_WIDTH[t]
+        datas.append(np.zeros(cap * w + 1, np.uint8))
+        nulls.append(np.zeros(cap + 1, np.uint8))
+    return datas, nulls
+
+
+def _csv_result(rows, bad, fr, ff, fk, types, width, datas, nulls):
+    cols = []
+    for t, d, n in zip(types, datas, nulls):
+        if t < 0:
+            cols.append(None)
+            continue
+        w = width if t == 3 else CSV_WIDTH[t]
+        raw = d[: rows * w]
+        vals = raw.reshape(rows, w).copy() if t == 3 else raw.view(CSV_DTYPE[t]).copy()
+        cols.append((vals, n[:rows].copy()))
+    return {"rows": rows, "bad": bad, "first_row": fr, "first_field": ff, "first_kind": fk, "cols": cols}
+
+
+def csv_scan(body: bytes, types: list, width: int = 16) -> dict:
+    """The oracle's CSV scan of `body` (text after the header line): rows kept,
+    conversion failures, and per field (values, null bytes) or None when skipped."""
+    L = lib()
+    L.orc_csv_scan.restype = C.c_int64
+    n = len(types)
+    cap = body.count(b"\n") + body.count(b"\r") + 2
+    datas, nulls = _csv_outputs(types, width, cap)
+    dp = (C.c_void_p * n)(*[d.ctypes.data for d in datas])
+    npp = (C.c_void_p * n)(*[x.ctypes.data for x in nulls])
+    ty = (C.c_int * n)(*types)
+    wd = (C.c_int * n)(*[width if t == 3 else 0 for t in types])
+    bad, fr, ff, fk = C.c_uint64(), C.c_int64(), C.c_int(), C.c_int()
+    rows = L.orc_csv_scan(C.c_char_p(body), C.c_uint64(len(body)), n, ty, wd, dp, npp, C.c_uint64(cap),
+                          C.byref(bad), C.byref(fr), C.byref(ff), C.byref(fk))
+    assert rows >= 0
+    return _csv_result(rows, bad.value, fr.value, ff.value, fk.value, types, width, datas, nulls)
+
+
+def ref_csv_available() -> bool:
+    return os.path.exists(REF_CSV_LIB)
+
+
+def ref_csv_scan(header: bytes, body: bytes, types: list, width: int = 16, guess: bool = False) -> dict:
+    """The reference's own reader (csv-parser + std::stoi/stof + strptime), from
+    oracle/_ref/libcsvref.so, on header + body written to a temporary file."""
+    import tempfile
+    L = C.CDLL(REF_CSV_LIB)
+    n = len(types)
+    cap = body.count(b"\n") + body.count(b"\r") + 2
+    datas, nulls = _csv_outputs(types, width, cap)
+    dp = (C.c_void_p * n)(*[d.ctypes.data for d in datas])
+    npp = (C.c_void_p * n)(*[x.ctypes.data for x in nulls])
+    ty = (C.c_int * n)(*types)
+    wd = (C.c_int * n)(*[width if t == 3 else 0 for t in types])
+    rows, bad, fr, ff, fk = C.c_uint64(), C.c_uint64(), C.c_int64(), C.c_int(), C.c_int()
+    with tempfile.NamedTemporaryFile("wb", suffix=".csv", delete=False) as fh:
+        fh.write(header + body)
+        path = fh.name
+    try:
+        rc = L.ref_csv_scan(C.c_char_p(path.encode()), C.c_int(1 if guess else 0), n, ty, wd, dp, npp,
+                            C.c_uint64(cap), C.byref(rows), C.byref(bad), C.byref(fr), C.byref(ff), C.byref(fk))
+    finally:
+        os.unlink(path)
+    if rc != 0:
+        raise RuntimeError(f"reference CSV reader returned {rc}")
+    return _csv_result(rows.value, bad.value, fr.value, ff.value, fk.value, types, width, datas, nulls)
+
+
+def convert_batch(kind: int, strings: list) -> tuple:
+    """glibc conversions as the reference calls them: kind 0 std::stoi, 1 std::stof
+    (float bits), 2 strptime+timegm. Returns (values int64, status int32)."""
+    L = lib()
+    buf = b"".join(strings)
+    offs = np.zeros(len(strings) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(s) for s in strings])
+    out = np.zeros(len(strings), np.int64)
+    st = np.zeros(len(strings), np.int32)
+    L.orc_convert_batch(C.c_int(kind), C.c_char_p(buf), offs.ctypes.data_as(C.c_void_p), C.c_uint64(len(strings)),
+                        out.ctypes.data_as(C.c_void_p), st.ctypes.data_as(C.c_void_p))
+    return out, st

@@ -23,6 +23,7 @@
  *  - aggregates: FP64 accumulation of float sums (reduction_kernel.cu:79-121
  *    accumulates SUM(float) in double), exact int64 integer sums.
  */
+#define _GNU_SOURCE  /* strptime, timegm (the CSV scan restatement) */
 #include <math.h>
 #include <pthread.h>
 #include <stdint.h>
@@ -399,4 +400,221 @@ void orc_gather(const void* src, void* dst, int width, const uint32_t* perm, uin
   const char* s = (const char*)src;
   char* d = (char*)dst;
   for (uint32_t i = 0; i < n; ++i) memcpy(d + (size_t)i * width, s + (size_t)perm[i] * width, (size_t)width);
+}
+
+/* ------------------------------------------------------------------ CSV scan
+ * Restates the reference's CSV path for the device CSV scan's parity tests:
+ * csv-parser's default parse loop (vendor/csv-parser/csv.hpp:7063-7140 and
+ * end_feed, :6985-7003) over the text after the header line, rows whose field
+ * count differs from the header's dropped (VariableColumnPolicy::IGNORE_ROW,
+ * csv.hpp CSVReader::read_row), then GetOperator::next's conversions
+ * (src/engine/operators/get_operator.cpp:66-101): strtol + int range check
+ * (std::stoi), strtof + ERANGE check (std::stof), strptime("%Y-%m-%d
+ * %H:%M:%S") + timegm (include/enums/data_type_utils.hpp:24-44), and a
+ * NUL-padded copy of at most width-1 bytes (string_kernel.hpp:16-31). */
+#include <errno.h>
+#include <limits.h>
+#include <float.h>
+#include <time.h>
+
+typedef struct {
+  const int* type;
+  const int* width;
+  void** data;
+  unsigned char** nulls;
+  int nfields;
+  uint64_t capacity;
+  uint64_t rows;
+  uint64_t bad;
+  int64_t bad_row;
+  int bad_field, bad_kind;
+  int overflow;
+  int has_dq; /* the current field held an escaped "" */
+  /* fields of the current row: contents back to back in buf */
+  char* buf;
+  size_t len, cap;
+  size_t* fstart;
+  int nf, fcap;
+} csv_state;
+
+static void csv_append(csv_state* S, char c) {
+  if (S->len + 1 >= S->cap) {
+    S->cap = S->cap ? 2 * S->cap : 4096;
+    S->buf = (char*)realloc(S->buf, S->cap);
+  }
+  S->buf[S->len++] = c;
+}
+
+static void csv_push_field(csv_state* S, size_t* field_start) {
+  if (S->has_dq) {
+    /* csv-parser's un-escaping (csv.hpp:7775-7792): of the field's quotes,
+     * keep the 1st, 3rd, ... and drop the others */
+    size_t o = *field_start;
+    int prev = 0;
+    for (size_t i = *field_start; i < S->len; ++i) {
+      if (S->buf[i] == '"') {
+        if (prev) { prev = 0; continue; }
+        prev = 1;
+      }
+      S->buf[o++] = S->buf[i];
+    }
+    S->len = o;
+    S->has_dq = 0;
+  }
+  if (S->nf + 2 > S->fcap) {
+    S->fcap = S->fcap ? 2 * S->fcap : 64;
+    S->fstart = (size_t*)realloc(S->fstart, sizeof(size_t) * (S->fcap + 1));
+  }
+  S->fstart[S->nf++] = *field_start;
+  csv_append(S, 0); /* each field NUL terminated in buf, like c_str() */
+  *field_start = S->len;
+}
+
+static void csv_convert_row(csv_state* S) {
+  const uint64_t r = S->rows;
+  if (S->nf != S->nfields) return; /* IGNORE_ROW */
+  if (r >= S->capacity) { S->overflow = 1; return; }
+  for (int f = 0; f < S->nfields; ++f) {
+    const int ty = S->type[f];
+    if (ty < 0) continue;
+    const char* v = S->buf + S->fstart[f];
+    /* the field's std::string length: up to the next field (embedded NULs count) */
+    size_t vlen = (f + 1 < S->nf ? S->fstart[f + 1] : S->len) - S->fstart[f] - 1;
+    S->nulls[f][r] = vlen == 0;
+    int kind = 0;
+    if (ty == 0) {
+      int32_t x = INT_MIN;
+      if (vlen) {
+        char* end;
+        errno = 0;
+        long l = strtol(v, &end, 10);
+        if (end == v) { x = 0; kind = 1; }
+        else if (errno == ERANGE || l < INT_MIN || l > INT_MAX) { x = 0; kind = 2; }
+        else x = (int32_t)l;
+      }
+      ((int32_t*)S->data[f])[r] = x;
+    } else if (ty == 1) {
+      float x = FLT_MIN;
+      if (vlen) {
+        char* end;
+        errno = 0;
+        x = strtof(v, &end);
+        if (end == v) { x = 0; kind = 1; }
+        else if (errno == ERANGE) { x = 0; kind = 2; }
+      }
+      ((float*)S->data[f])[r] = x;
+    } else if (ty == 2) {
+      int64_t x = 0;
+      if (vlen) {
+        struct tm t;
+        memset(&t, 0, sizeof t);
+        if (strptime(v, "%Y-%m-%d %H:%M:%S", &t) != NULL) x = (int64_t)timegm(&t);
+      }
+      ((int64_t*)S->data[f])[r] = x;
+    } else {
+      const int w = S->width[f];
+      char* slot = (char*)S->data[f] + r * (uint64_t)w;
+      memset(slot, 0, w);
+      for (int i = 0; i < w - 1 && v[i]; ++i) slot[i] = v[i];
+    }
+    if (kind) {
+      if (S->bad == 0) { S->bad_row = (int64_t)r; S->bad_field = f; S->bad_kind = kind; }
+      ++S->bad;
+    }
+  }
+  ++S->rows;
+}
+
+static void csv_push_row(csv_state* S) {
+  csv_convert_row(S);
+  S->nf = 0;
+  S->len = 0;
+}
+
+/* text: the CSV body (after the header line). Returns rows kept; -1 on overflow. */
+int64_t orc_csv_scan(const char* text, uint64_t n, int nfields, const int* field_type, const int* field_width,
+                     void** out_data, unsigned char** out_nulls, uint64_t capacity, uint64_t* bad_cells,
+                     int64_t* first_bad_row, int* first_bad_field, int* first_bad_kind) {
+  csv_state S;
+  memset(&S, 0, sizeof S);
+  S.type = field_type;
+  S.width = field_width;
+  S.data = out_data;
+  S.nulls = out_nulls;
+  S.nfields = nfields;
+  S.capacity = capacity;
+  S.bad_row = -1;
+  S.bad_field = -1;
+  size_t field_start = 0;
+  int quoted = 0;
+  uint64_t pos = 0;
+  /* newlines at the start belong to the header line's newline run */
+  while (pos < n && (text[pos] == '\r' || text[pos] == '\n')) ++pos;
+  while (pos < n) {
+    const char c = text[pos];
+    if (!quoted) {
+      if (c == ',') { csv_push_field(&S, &field_start); ++pos; }
+      else if (c == '\r' || c == '\n') {
+        ++pos;
+        while (pos < n && (text[pos] == '\r' || text[pos] == '\n')) ++pos;
+        csv_push_field(&S, &field_start);
+        csv_push_row(&S);
+        field_start = 0;
+      } else if (c == '"' && S.len == field_start) { quoted = 1; ++pos; }  /* opens only an empty field */
+      else { csv_append(&S, c); ++pos; }
+    } else if (c == '"') {
+      if (pos + 1 == n) { quoted = 0; ++pos; }                        /* closing quote at the end */
+      else {
+        const char d = text[pos + 1];
+        if (d == ',' || d == '\r' || d == '\n') { quoted = 0; ++pos; } /* closes the field */
+        else if (d == '"') { csv_append(&S, '"'); csv_append(&S, '"'); S.has_dq = 1; pos += 2; } /* "" */
+        else { csv_append(&S, '"'); ++pos; }                           /* a lone quote stays */
+      }
+    } else { csv_append(&S, c); ++pos; }
+  }
+  /* end of data: the last field is pushed when it has bytes or the text ends
+   * in a delimiter or a quote; the row when it has fields */
+  if (S.len > field_start || (n && (text[n - 1] == ',' || text[n - 1] == '"'))) csv_push_field(&S, &field_start);
+  if (S.nf) csv_push_row(&S);
+  free(S.buf);
+  free(S.fstart);
+  *bad_cells = S.bad;
+  *first_bad_row = S.bad_row;
+  *first_bad_field = S.bad_field;
+  *first_bad_kind = S.bad_kind;
+  return S.overflow ? -1 : (int64_t)S.rows;
+}
+
+/* glibc conversions, one per string (strings back to back, offs[n+1]):
+ * kind 0 std::stoi, 1 std::stof (out = float bits), 2 strptime + timegm.
+ * status: 0 ok, 1 nothing converts, 2 out of range (where the std:: calls throw). */
+void orc_convert_batch(int kind, const char* buf, const uint64_t* offs, uint64_t n, int64_t* out, int32_t* status) {
+  char tmp[4096];
+  for (uint64_t i = 0; i < n; ++i) {
+    size_t len = offs[i + 1] - offs[i];
+    if (len >= sizeof tmp) len = sizeof tmp - 1;
+    memcpy(tmp, buf + offs[i], len);
+    tmp[len] = 0;
+    status[i] = 0;
+    char* end;
+    if (kind == 0) {
+      errno = 0;
+      long l = strtol(tmp, &end, 10);
+      if (end == tmp) { status[i] = 1; out[i] = 0; }
+      else if (errno == ERANGE || l < INT_MIN || l > INT_MAX) { status[i] = 2; out[i] = 0; }
+      else out[i] = l;
+    } else if (kind == 1) {
+      errno = 0;
+      float f = strtof(tmp, &end);
+      uint32_t b;
+      memcpy(&b, &f, 4);
+      out[i] = b;
+      if (end == tmp) status[i] = 1;
+      else if (errno == ERANGE) status[i] = 2;
+    } else {
+      struct tm t;
+      memset(&t, 0, sizeof t);
+      out[i] = strptime(tmp, "%Y-%m-%d %H:%M:%S", &t) != NULL ? (int64_t)timegm(&t) : 0;
+    }
+  }
 }

@@ -1,0 +1,163 @@
+// Test infrastructure: the device CSV scan's tokenizer and field conversions
+// (yallasql_b200/csrc/yq_csv.cuh) compiled for the host with g++, so the CPU
+// suite checks them against glibc and the reference's csv-parser without a GPU.
+// hs_csv_scan follows the kernels' structure: record starts from 64-byte chunk
+// summaries composed in order (the state-map tables, with the same
+// four-ordinary-bytes shortcut), then one walk per record.
+#include "../yallasql_b200/csrc/yq_csv.cuh"
+
+#include <cfloat>
+#include <climits>
+#include <cstring>
+#include <vector>
+
+using namespace yq::csv;
+
+namespace {
+
+constexpr Tables kT = make_tables();
+static_assert(kT.count == NMAPS, "tables");
+
+uint32_t classes4_host(uint32_t w) {
+  uint32_t r = 0;
+  for (int b = 0; b < 4; ++b) r |= char_class((w >> (8 * b)) & 0xff) << (8 * b);
+  return r;
+}
+
+struct Summ {
+  uint32_t map;
+  uint64_t c[NSTATES];
+};
+
+Summ chunk_summary(const uint8_t* p, uint64_t n) {
+  uint32_t id = 0;
+  uint64_t cnt = 0;
+  uint64_t i = 0;
+  auto byte = [&](uint32_t cls) {
+    uint64_t e = kT.step[id * 4 + cls];
+    id = (uint32_t)(e & 63);
+    cnt += e >> 8;
+  };
+  for (; i + 4 <= n; i += 4) {
+    uint32_t w;
+    std::memcpy(&w, p + i, 4);
+    uint32_t c4 = classes4_host(w);
+    if (c4 == 0) byte(C_OTHER);
+    else
+      for (int b = 0; b < 4; ++b) byte((c4 >> (8 * b)) & 3);
+  }
+  for (; i < n; ++i) byte(char_class(p[i]));
+  Summ s;
+  s.map = kT.map_word[id];
+  for (int k = 0; k < NSTATES; ++k) s.c[k] = (cnt >> (8 * k)) & 0xff;
+  return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+// kind 0: stoi -> out (int32), 1: stof -> out (float bits), 2: datetime -> out.
+void hs_convert(int kind, const uint8_t* buf, const uint64_t* offs, uint64_t n, int64_t* out, int32_t* status) {
+  for (uint64_t i = 0; i < n; ++i) {
+    View v{buf + offs[i], (uint32_t)(offs[i + 1] - offs[i])};
+    if (kind == 0) {
+      int32_t x;
+      status[i] = parse_int32(v, &x);
+      out[i] = x;
+    } else if (kind == 1) {
+      float x;
+      status[i] = parse_float32(v, &x);
+      out[i] = float_bits(x);
+    } else {
+      status[i] = 0;
+      out[i] = parse_datetime(v);
+    }
+  }
+}
+
+// Record starts two ways: the plain state machine, and chunk summaries
+// composed in order. Returns the count, or -1 when the two disagree.
+int64_t hs_record_starts(const uint8_t* text, uint64_t n, uint32_t* starts, uint64_t cap) {
+  std::vector<uint32_t> a;
+  uint32_t st = S_REC;
+  for (uint64_t i = 0; i < n; ++i) {
+    uint32_t cls = char_class(text[i]);
+    if (starts_record(cls, st)) a.push_back((uint32_t)i);
+    st = step(cls, st);
+  }
+  uint64_t total = 0;
+  uint32_t state = S_REC;
+  for (uint64_t lo = 0; lo < n; lo += 64) {
+    uint64_t len = n - lo < 64 ? n - lo : 64;
+    Summ s = chunk_summary(text + lo, len);
+    total += s.c[state];
+    state = (s.map >> (3 * state)) & 7;
+  }
+  if (total != a.size()) return -1;
+  for (uint64_t k = 0; k < a.size() && k < cap; ++k) starts[k] = a[k];
+  return (int64_t)a.size();
+}
+
+// The device scan's semantics on the host (the same walk and conversions).
+int64_t hs_csv_scan(const uint8_t* text, uint64_t n, int nfields, const int* field_type, const int* field_width,
+                    void** out_data, unsigned char** out_nulls, uint64_t capacity, uint64_t* bad,
+                    int64_t* first_bad_row, int* first_bad_field, int* first_bad_kind) {
+  std::vector<uint32_t> starts(n + 1);
+  int64_t nrec = hs_record_starts(text, n, starts.data(), n + 1);
+  if (nrec < 0) return -2;
+  *bad = 0;
+  *first_bad_row = -1;
+  *first_bad_field = -1;
+  *first_bad_kind = 0;
+  uint64_t rows = 0;
+  std::vector<std::vector<uint8_t>> tmp(nfields);
+  for (int64_t r = 0; r < nrec; ++r) {
+    const uint64_t st = starts[r], en = r + 1 < nrec ? starts[r + 1] : n;
+    if (rows >= capacity) return -1;
+    struct Cell { int type, width; int kind; } cells[64];
+    int64_t vals[64];
+    unsigned char nul[64];
+    std::vector<uint32_t> text_words[64];
+    auto sink = [&](uint32_t f, View v, bool, bool escapes) {
+      if ((int)f >= nfields || field_type[f] < 0) return;
+      const int ty = field_type[f];
+      cells[f].kind = 0;
+      nul[f] = v.len == 0;
+      if (ty == 0) {
+        int32_t x = INT_MIN;
+        if (v.len) cells[f].kind = parse_int32(v, &x);
+        vals[f] = cells[f].kind ? 0 : x;
+      } else if (ty == 1) {
+        float x = FLT_MIN;
+        if (v.len) cells[f].kind = parse_float32(v, &x);
+        vals[f] = cells[f].kind ? 0 : float_bits(x);
+      } else if (ty == 2) {
+        vals[f] = v.len ? parse_datetime(v) : 0;
+      } else {
+        text_words[f].assign(field_width[f] / 4, 0xdeadbeefu);
+        auto store = [&](uint32_t k, uint32_t w) { text_words[f][k] = w; };
+        copy_text(v, escapes, (uint32_t)field_width[f], store);
+      }
+    };
+    uint32_t nf = walk_record(text + st, (uint32_t)(en - st), sink);
+    if ((int)nf != nfields) continue;
+    for (int f = 0; f < nfields; ++f) {
+      const int ty = field_type[f];
+      if (ty < 0) continue;
+      out_nulls[f][rows] = nul[f];
+      if (ty == 0) static_cast<int32_t*>(out_data[f])[rows] = (int32_t)vals[f];
+      else if (ty == 1) static_cast<uint32_t*>(out_data[f])[rows] = (uint32_t)vals[f];
+      else if (ty == 2) static_cast<int64_t*>(out_data[f])[rows] = vals[f];
+      else std::memcpy(static_cast<char*>(out_data[f]) + rows * field_width[f], text_words[f].data(), field_width[f]);
+      if (ty <= 1 && cells[f].kind) {
+        if (*bad == 0) { *first_bad_row = (int64_t)rows; *first_bad_field = f; *first_bad_kind = cells[f].kind; }
+        ++*bad;
+      }
+    }
+    ++rows;
+  }
+  return (int64_t)rows;
+}
+
+}  // extern "C"

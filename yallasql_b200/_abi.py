@@ -89,6 +89,13 @@ class Operand(C.Structure):
     _fields_ = [("data", C.c_void_p), ("type", C.c_int32), ("width", C.c_int32), ("is_scalar", C.c_int32)]
 
 
+class CsvError(C.Structure):
+    _fields_ = [("bad_cells", C.c_uint64), ("first_row", C.c_uint32), ("first_field", C.c_int32),
+                ("kind", C.c_int32)]
+
+
+CSV_MAX_FIELDS = 64
+
 P = C.POINTER
 vp, sz, u32, i32, u64 = C.c_void_p, C.c_size_t, C.c_uint32, C.c_int32, C.c_uint64
 
@@ -150,6 +157,10 @@ PROTOTYPES = {
     "yq_key_transform": (C.c_int, [vp, i32, vp, u32, i32, vp]),
     "yq_merge_path": (C.c_int, [vp, vp, i32, i32, i32, u32, u32, u32, vp, vp, vp, vp, vp]),
     "yq_cross_product_col": (C.c_int, [P(Column), u32, u32, i32, P(Column), vp]),
+    "yq_csv_index_workspace_size": (sz, [u64]),
+    "yq_csv_index": (C.c_int, [vp, u64, vp, u64, P(u64), vp, sz, vp]),
+    "yq_csv_parse_workspace_size": (sz, [u32]),
+    "yq_csv_parse": (C.c_int, [vp, u64, vp, u32, P(i32), i32, P(Column), i32, P(u32), P(CsvError), vp, sz, vp]),
     "yq_device_sm_count": (C.c_int, []),
     "yq_launch_count": (u64, []),
     "yq_profile_enable": (C.c_int, [i32]),

@@ -58,13 +58,36 @@ def _run(cmd: list[str]) -> None:
         raise RuntimeError("build failed:\n" + " ".join(cmd) + "\n" + r.stdout)
 
 
+_INCLUDE_RE = None
+
+
+def _includes(path: str, seen: set[str]) -> set[str]:
+    """Local headers `path` includes, transitively (quoted #include lines)."""
+    global _INCLUDE_RE
+    import re
+    if _INCLUDE_RE is None:
+        _INCLUDE_RE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+    try:
+        with open(path) as f:
+            text = f.read()
+    except OSError:
+        return seen
+    for name in _INCLUDE_RE.findall(text):
+        dep = os.path.normpath(os.path.join(os.path.dirname(path), name))
+        if dep not in seen and os.path.exists(dep):
+            seen.add(dep)
+            _includes(dep, seen)
+    return seen
+
+
 def _compile_all(srcs: list[str], extra: list[str], headers: list[str]) -> list[str]:
     os.makedirs(BUILD, exist_ok=True)
     objs, jobs = [], []
     for s in srcs:
         o = os.path.join(BUILD, os.path.basename(s) + ".o")
         objs.append(o)
-        if _stale(o, [s] + headers):
+        deps = sorted(_includes(s, set())) if s.endswith((".cu", ".cpp")) else headers
+        if _stale(o, [s] + deps):
             jobs.append([nvcc()] + ARCH + NVCC_FLAGS + extra + ["-c", s, "-o", o])
     if jobs:
         with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:

@@ -112,3 +112,92 @@ def batch_row_counts(total_rows: int, row_bytes: int, batch_bytes: int = 4 << 20
     if total_rows % per:
         counts.append(total_rows % per)
     return counts
+
+
+# ---------------------------------------------------------------- CSV text
+def _digits(x: np.ndarray, width: int) -> tuple[np.ndarray, np.ndarray]:
+    """Right-aligned decimal digits of non-negative integers in a (rows, width)
+    byte array, and a mask of the significant ones (no leading zeros; 0 is "0")."""
+    x = x.astype(np.int64)
+    pw = 10 ** np.arange(width - 1, -1, -1, dtype=np.int64)
+    d = (x[:, None] // pw[None, :]) % 10
+    ndig = np.maximum(1, np.floor(np.log10(np.maximum(x, 1))).astype(np.int64) + 1)
+    mask = np.arange(width)[None, :] >= (width - ndig)[:, None]
+    return (d + 48).astype(np.uint8), mask
+
+
+def _fixed(rows: int, text: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    return text, np.ones(text.shape, dtype=bool)
+
+
+def csv_text(columns: list[tuple[np.ndarray, np.ndarray]]) -> np.ndarray:
+    """Rows of comma-separated fields, each line ending in '\n', from per-field
+    (bytes [rows, w], mask [rows, w]) pieces: a field is its masked bytes."""
+    rows = columns[0][0].shape[0]
+    parts, masks = [], []
+    for i, (b, m) in enumerate(columns):
+        parts.append(b)
+        masks.append(m)
+        sep = np.full((rows, 1), ord(",") if i + 1 < len(columns) else ord("\n"), dtype=np.uint8)
+        parts.append(sep)
+        masks.append(np.ones((rows, 1), dtype=bool))
+    full = np.concatenate(parts, axis=1)
+    mask = np.concatenate(masks, axis=1)
+    return full[mask]
+
+
+SALES_CSV_HEADER = "id (N) (P),price (N),qty (N),discount (N),category (T),updated_at (D)\n"
+
+
+def sales_csv(rows: int = 1_000_000, seed: int = 0) -> tuple[bytes, np.ndarray]:
+    """The filter+aggregate table as a CSV file in the reference's header-tag
+    convention: (header line, body bytes). Prices are written with two
+    decimals (cents uniform over [1.00, 999.99]), dates as
+    "YYYY-MM-DD HH:MM:SS" (UTC), categories as their 12-character names."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    cents = rng.integers(100, 100_000, rows)
+    qty = rng.integers(1, 51, rows)
+    disc = rng.integers(0, 11, rows)
+    cat = rng.integers(0, len(CATEGORIES), rows)
+    secs = rng.integers(DATE_LO, DATE_HI + 86400, rows)
+    chunks = []
+    step = 1 << 21
+    for lo in range(0, rows, step):
+        hi = min(rows, lo + step)
+        n = hi - lo
+        ident = _digits(np.arange(lo, hi), 10)
+        pint = _digits(cents[lo:hi] // 100, 3)
+        frac = (_digits(cents[lo:hi] % 100 + 100, 3)[0][:, 1:], np.ones((n, 2), dtype=bool))
+        dot = np.full((n, 1), ord("."), dtype=np.uint8)
+        price = (np.concatenate([pint[0], dot, frac[0]], axis=1),
+                 np.concatenate([pint[1], np.ones((n, 1), dtype=bool), frac[1]], axis=1))
+        catb = np.frombuffer("".join(CATEGORIES).encode(), dtype=np.uint8).reshape(len(CATEGORIES), 12)[cat[lo:hi]]
+        chunks.append(csv_text([ident, price, _digits(qty[lo:hi], 2), _digits(disc[lo:hi], 2),
+                                _fixed(n, catb), _fixed(n, _date_text(secs[lo:hi]))]))
+    return SALES_CSV_HEADER.encode(), np.concatenate(chunks)
+
+
+def _date_text(secs: np.ndarray) -> np.ndarray:
+    """"YYYY-MM-DD HH:MM:SS" bytes [rows, 19] of epoch seconds (UTC)."""
+    days, rem = np.divmod(secs.astype(np.int64), 86400)
+    # civil date from days since 1970-01-01 (proleptic Gregorian)
+    z = days + 719468
+    era = np.floor_divide(z, 146097)
+    doe = z - era * 146097
+    yoe = (doe - doe // 1460 + doe // 36524 - doe // 146096) // 365
+    y = yoe + era * 400
+    doy = doe - (365 * yoe + yoe // 4 - yoe // 100)
+    mp = (5 * doy + 2) // 153
+    d = doy - (153 * mp + 2) // 5 + 1
+    m = np.where(mp < 10, mp + 3, mp - 9)
+    y = y + (m <= 2)
+    hh, rem = np.divmod(rem, 3600)
+    mi, ss = np.divmod(rem, 60)
+    out = np.empty((secs.shape[0], 19), dtype=np.uint8)
+    for col, (v, w) in zip([0, 5, 8, 11, 14, 17], [(y, 4), (m, 2), (d, 2), (hh, 2), (mi, 2), (ss, 2)]):
+        pw = 10 ** np.arange(w - 1, -1, -1)
+        out[:, col:col + w] = ((v[:, None] // pw[None, :]) % 10 + 48).astype(np.uint8)
+    out[:, 4] = out[:, 7] = ord("-")
+    out[:, 10] = ord(" ")
+    out[:, 13] = out[:, 16] = ord(":")
+    return out

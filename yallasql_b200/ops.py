@@ -541,3 +541,119 @@ def sort_autotune(col: DeviceColumn, offsets, descending=False, stream=None) -> 
     _check(lib().yq_sort_autotune(C.byref(cc), col.rows, offs, len(offsets) - 1, int(descending), C.byref(best),
                                   _stream(stream)), "yq_sort_autotune")
     return best
+
+
+# ------------------------------------------------------------------ CSV scan
+@dataclass
+class CsvColumn:
+    """One column of a CSV table: name without its tags, type, primary-key tag."""
+    name: str
+    type: int
+    pk: bool = False
+
+
+def csv_schema(header: str, first_line: str = "") -> list[CsvColumn]:
+    """Column names and types from a header line in the reference's tag
+    convention (Table::inferDBSchema, src/db/table.cpp:43-150): the header and
+    the first data line are split at every ',' (pairwise, stopping at the
+    shorter), quotes/CR/LF removed; "(P)" marks a primary key; "(N)" is FLOAT
+    when the first data line's value contains '.', else INT; "(D)" DATETIME;
+    "(T)" or no tag STRING."""
+    names = header.split(",")
+    values = first_line.split(",")
+    out = []
+    for name, value in zip(names, values):
+        for ch in '"\r\n':
+            name = name.replace(ch, "")
+            value = value.replace(ch, "")
+        base = name.strip(" \t")
+        pk = base.endswith("(P)")
+        if pk:
+            base = base[:-3].rstrip(" \t")
+        if base.endswith("(N)"):
+            type_ = A.FLOAT32 if "." in value.strip(" \t") else A.INT32
+            base = base[:-3]
+        elif base.endswith("(D)"):
+            type_, base = A.DATETIME, base[:-3]
+        elif base.endswith("(T)"):
+            type_, base = A.TEXT, base[:-3]
+        else:
+            type_ = A.TEXT
+        base = base.rstrip(" \t")
+        if not base:
+            raise ValueError(f"invalid column name in CSV header: {name!r}")
+        out.append(CsvColumn(base, type_, pk))
+    return out
+
+
+class CsvScanError(ValueError):
+    """A cell that std::stoi / std::stof would reject (the reference exits there)."""
+
+    def __init__(self, err: "A.CsvError", batch: "DeviceBatch"):
+        kind = {1: "no conversion (invalid_argument)", 2: "out of range"}.get(err.kind, str(err.kind))
+        super().__init__(f"{err.bad_cells} bad cell(s); first at row {err.first_row}, field {err.first_field}: {kind}")
+        self.error = err
+        self.batch = batch
+
+
+def csv_scan(text: torch.Tensor, types: list[int], project: list[int] | None = None, text_width: int = 256,
+             stream=None) -> DeviceBatch:
+    """Parse CSV text resident on the device (uint8 tensor, the header line
+    removed) into a DeviceBatch: the device-side GetOperator::next
+    (src/engine/operators/get_operator.cpp:56-109). `types[f]` is the type of
+    CSV field f (from csv_schema); `project` lists the fields to keep, in output
+    order (default: all). Text columns get slots of `text_width` bytes (the
+    reference's slot is 256). Raises CsvScanError (batch attached) when a cell
+    fails to convert."""
+    L = lib()
+    s = _stream(stream)
+    nbytes = int(text.numel())
+    project = list(range(len(types))) if project is None else list(project)
+    if text.dtype != torch.uint8 or not text.is_cuda or not text.is_contiguous():
+        raise ValueError("text must be a contiguous uint8 CUDA tensor")
+    records = C.c_uint64(0)
+    ptr = text.data_ptr() if nbytes else None
+    st = L.yq_csv_index(ptr, nbytes, None, 0, C.byref(records), None, 0, s)
+    if st not in (A.OK, A.ERR_CAPACITY):
+        _check(st, "yq_csv_index")
+    n = int(records.value)
+    starts = torch.empty(max(n, 1), dtype=torch.int32, device=text.device)
+    _check(L.yq_csv_index(ptr, nbytes, starts.data_ptr(), n, C.byref(records), None, 0, s), "yq_csv_index")
+    cols = []
+    field_col = [-1] * len(types)
+    for i, f in enumerate(project):
+        field_col[f] = i
+        cols.append(DeviceColumn.empty(types[f], n, text_width if types[f] == A.TEXT else None, nulls=True,
+                                       device=text.device))
+    ccols = (A.Column * max(1, len(cols)))(*[c.c() for c in cols])
+    fc = (C.c_int32 * len(types))(*field_col)
+    rows = C.c_uint32(0)
+    err = A.CsvError()
+    st = L.yq_csv_parse(ptr, nbytes, starts.data_ptr(), n, fc, len(types), ccols, len(cols), C.byref(rows),
+                        C.byref(err), None, 0, s)
+    if st not in (A.OK, A.ERR_INVALID_ARG) or (st == A.ERR_INVALID_ARG and err.bad_cells == 0):
+        _check(st, "yq_csv_parse")
+    r = int(rows.value)
+    batch = DeviceBatch([DeviceColumn(c.data[:r], c.type, c.nulls[:r]) for c in cols])
+    if st == A.ERR_INVALID_ARG:
+        raise CsvScanError(err, batch)
+    return batch
+
+
+def read_csv(data: bytes, project: list[str] | None = None, text_width: int = 256, device="cuda",
+             stream=None) -> tuple[list[CsvColumn], DeviceBatch]:
+    """A whole CSV file (header line included): schema from the header on the
+    host, the body copied to the device and scanned there."""
+    if data.startswith(b"\xef\xbb\xbf"):
+        data = data[3:]  # csv-parser drops a UTF-8 byte-order mark
+    nl = data.find(b"\n")
+    header = data[: nl if nl >= 0 else len(data)].decode("utf-8", "replace")
+    body = data[nl + 1:] if nl >= 0 else b""
+    nl2 = body.find(b"\n")
+    first = body[: nl2 if nl2 >= 0 else len(body)].decode("utf-8", "replace")
+    schema = csv_schema(header, first)
+    fields = list(range(len(schema))) if project is None else [[c.name for c in schema].index(p) for p in project]
+    host = torch.frombuffer(bytearray(body), dtype=torch.uint8) if body else torch.empty(0, dtype=torch.uint8)
+    text = host.to(device, non_blocking=False)
+    batch = csv_scan(text, [c.type for c in schema], fields, text_width, stream)
+    return [schema[f] for f in fields], batch

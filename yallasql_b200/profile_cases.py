@@ -4,6 +4,7 @@
     python -m yallasql_b200.profile_cases join     # 30M-row fact table joined to the 2,556-row date table + SUM
     python -m yallasql_b200.profile_cases order    # 16M rows (key f32, id, 16-byte txt, date), 116,480-row runs
     python -m yallasql_b200.profile_cases cross    # 20K x 20K cross product with < (198M output pairs)
+    python -m yallasql_b200.profile_cases csv      # 4M-row sales table as CSV text (~205 MB): index + parse
 
 An optional second argument sets the row count (rows per side for cross).
 
@@ -76,7 +77,14 @@ def cross_case(rows: int = 20_000) -> None:
     torch.cuda.synchronize()
 
 
-CASES = {"filter": filter_case, "join": join_case, "order": order_case, "cross": cross_case}
+def csv_case(rows: int = 4_000_000) -> None:
+    _, body = datagen.sales_csv(rows, seed=0)
+    text = torch.from_numpy(body).cuda()
+    ops.csv_scan(text, [A.INT32, A.FLOAT32, A.INT32, A.INT32, A.TEXT, A.DATETIME], text_width=16)
+    torch.cuda.synchronize()
+
+
+CASES = {"filter": filter_case, "join": join_case, "order": order_case, "cross": cross_case, "csv": csv_case}
 
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "filter"
