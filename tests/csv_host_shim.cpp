@@ -18,36 +18,24 @@ namespace {
 constexpr Tables kT = make_tables();
 static_assert(kT.count == NMAPS, "tables");
 
-uint32_t classes4_host(uint32_t w) {
-  uint32_t r = 0;
-  for (int b = 0; b < 4; ++b) r |= char_class((w >> (8 * b)) & 0xff) << (8 * b);
-  return r;
-}
-
-struct Summ {
-  uint32_t map;
-  uint64_t c[NSTATES];
-};
-
-Summ chunk_summary(const uint8_t* p, uint64_t n) {
+// Summary of a chunk as the kernels make it: full 64-byte chunks through the
+// quote-free shortcut or the map table, shorter ones byte by byte.
+Summary chunk_summary(const uint8_t* p, uint64_t n) {
+  if (n == 64) {
+    uint32_t w[16];
+    std::memcpy(w, p, 64);
+    const Chunk64 k = scan64(w);
+    if (!k.quotes) return summary_quote_free(k);
+    return summary_by_table(w, kT.step, kT.map_word);
+  }
   uint32_t id = 0;
   uint64_t cnt = 0;
-  uint64_t i = 0;
-  auto byte = [&](uint32_t cls) {
-    uint64_t e = kT.step[id * 4 + cls];
+  for (uint64_t i = 0; i < n; ++i) {
+    uint64_t e = kT.step[id * 4 + char_class(p[i])];
     id = (uint32_t)(e & 63);
     cnt += e >> 8;
-  };
-  for (; i + 4 <= n; i += 4) {
-    uint32_t w;
-    std::memcpy(&w, p + i, 4);
-    uint32_t c4 = classes4_host(w);
-    if (c4 == 0) byte(C_OTHER);
-    else
-      for (int b = 0; b < 4; ++b) byte((c4 >> (8 * b)) & 3);
   }
-  for (; i < n; ++i) byte(char_class(p[i]));
-  Summ s;
+  Summary s;
   s.map = kT.map_word[id];
   for (int k = 0; k < NSTATES; ++k) s.c[k] = (cnt >> (8 * k)) & 0xff;
   return s;
@@ -88,12 +76,36 @@ int64_t hs_record_starts(const uint8_t* text, uint64_t n, uint32_t* starts, uint
   }
   uint64_t total = 0;
   uint32_t state = S_REC;
+  std::vector<uint32_t> b;  // record starts as the emit kernel finds them, chunk by chunk
   for (uint64_t lo = 0; lo < n; lo += 64) {
     uint64_t len = n - lo < 64 ? n - lo : 64;
-    Summ s = chunk_summary(text + lo, len);
+    Summary s = chunk_summary(text + lo, len);
+    if (len == 64) {
+      uint32_t w[16];
+      std::memcpy(w, text + lo, 64);
+      const Chunk64 k = scan64(w);
+      if (!k.quotes) {
+        for (uint64_t m = starts_quote_free(k, state); m; m &= m - 1) b.push_back((uint32_t)(lo + __builtin_ctzll(m)));
+      } else {
+        uint32_t st2 = state;
+        for (uint64_t i = 0; i < 64; ++i) {
+          uint32_t cls = char_class(text[lo + i]);
+          if (starts_record(cls, st2)) b.push_back((uint32_t)(lo + i));
+          st2 = step(cls, st2);
+        }
+      }
+    } else {
+      uint32_t st2 = state;
+      for (uint64_t i = 0; i < len; ++i) {
+        uint32_t cls = char_class(text[lo + i]);
+        if (starts_record(cls, st2)) b.push_back((uint32_t)(lo + i));
+        st2 = step(cls, st2);
+      }
+    }
     total += s.c[state];
     state = (s.map >> (3 * state)) & 7;
   }
+  if (b != a) return -1;
   if (total != a.size()) return -1;
   for (uint64_t k = 0; k < a.size() && k < cap; ++k) starts[k] = a[k];
   return (int64_t)a.size();
@@ -119,7 +131,7 @@ int64_t hs_csv_scan(const uint8_t* text, uint64_t n, int nfields, const int* fie
     int64_t vals[64];
     unsigned char nul[64];
     std::vector<uint32_t> text_words[64];
-    auto sink = [&](uint32_t f, View v, bool, bool escapes) {
+    auto sink = [&](uint32_t f, View v, bool escapes) {
       if ((int)f >= nfields || field_type[f] < 0) return;
       const int ty = field_type[f];
       cells[f].kind = 0;

@@ -129,9 +129,25 @@ def test_datetime_conversion_matches_strptime_timegm(shim):
     assert np.array_equal(a, b)
 
 
+def quote_free_cases(rng):
+    """Long quote-free texts (most 64-byte chunks take the kernels' newline-
+    bitmask shortcut): the sales table, and CR/LF runs of every length at
+    every offset across chunk boundaries."""
+    from yallasql_b200 import datagen
+    _, sales = datagen.sales_csv(3000, seed=3)
+    out = [([0, 1, 0, 0, 3, 2], b"", sales.tobytes())]
+    for _ in range(20):
+        parts = []
+        for _ in range(int(rng.integers(20, 200))):
+            parts.append(",".join(str(int(x)) for x in rng.integers(0, 10**int(rng.integers(1, 9)), 2)))
+            parts.append("".join(rng.choice(["\n", "\r", "\r\n", "\n\n"], int(rng.integers(1, 4)))))
+        out.append(([0, 0], b"", "".join(parts).encode()))
+    return out
+
+
 def test_device_scan_semantics_match_oracle(shim):
     rng = np.random.default_rng(14)
-    cases = csv_cases.edge_cases() + [csv_cases.random_csv(rng) for _ in range(300)]
+    cases = csv_cases.edge_cases() + [csv_cases.random_csv(rng) for _ in range(300)] + quote_free_cases(rng)
     for types, header, body in cases:
         same_scan(shim_scan(shim, body, types), oracle.csv_scan(body, types))
 

@@ -15,8 +15,9 @@
 //   k_csv_emit      each tile again, now from its known state: byte offset of
 //                   every record start
 //   k_csv_parse     128 records a block: their bytes staged into shared memory
-//                   with 16-byte loads, one thread per record walks its fields
-//                   and converts the projected ones into the output columns
+//                   with 16-byte loads; one thread per record, the lanes of a
+//                   warp on the same field at a time, so each conversion runs
+//                   converged
 // Rows whose field count differs from the header's are dropped afterwards
 // (csv-parser's default VariableColumnPolicy::IGNORE_ROW), by a stable
 // compaction that only runs when there are such rows.
@@ -37,15 +38,10 @@ constexpr int kBytesPerThread = 64;
 constexpr uint64_t kTileBytes = (uint64_t)kTileThreads * kBytesPerThread;  // 16 KiB
 constexpr int kScanThreads = 1024;
 constexpr int kParseThreads = 128;
-constexpr uint32_t kSpanCap = 48 * 1024;  // staged bytes per parse block
+constexpr uint32_t kSpanCap = 16 * 1024;  // staged bytes per parse block (128 B a record on average)
 constexpr uint32_t kIdentityMap = 0u | 1u << 3 | 2u << 6 | 3u << 9 | 4u << 12;
 
-// Tokenizer summary of a byte range: the state map and, per start state, the
-// number of records that start inside the range.
-struct Summ {
-  uint32_t map;
-  uint32_t c[NSTATES];
-};
+using Summ = Summary;
 
 __device__ __forceinline__ uint32_t map_at(uint32_t map, uint32_t s) { return (map >> (3 * s)) & 7u; }
 
@@ -115,61 +111,46 @@ __device__ Summ block_exclusive(const Summ& mine, Summ* warp_tot, Summ* total) {
   return r;
 }
 
-// Class of each byte of a 32-bit word, 2 bits at the bottom of each byte.
-__device__ __forceinline__ uint32_t classes4(uint32_t w) {
-  uint32_t q = __vcmpeq4(w, 0x22222222u);
-  uint32_t d = __vcmpeq4(w, 0x2c2c2c2cu);
-  uint32_t n = __vcmpeq4(w, 0x0a0a0a0au) | __vcmpeq4(w, 0x0d0d0d0du);
-  return (q & 0x01010101u) | (d & 0x02020202u) | (n & 0x03030303u);
+__device__ __forceinline__ void load_tables(uint64_t* s_step, uint32_t* s_mapw) {
+  for (int i = threadIdx.x; i < NMAPS * 4; i += blockDim.x) s_step[i] = kTab.step[i];
+  for (int i = threadIdx.x; i < NMAPS; i += blockDim.x) s_mapw[i] = kTab.map_word[i];
+  __syncthreads();
 }
 
-struct Walker {
-  const uint64_t* tab;  // shared-memory copy of kTab.step
-  uint32_t id = 0;
-  uint64_t cnt = 0;
-  __device__ __forceinline__ void byte_cls(uint32_t cls) {
-    uint64_t e = tab[id * 4 + cls];
-    id = (uint32_t)e & 63u;
-    cnt += e >> 8;
-  }
-  __device__ __forceinline__ void word(uint32_t w) {
-    uint32_t c4 = classes4(w);
-    if (c4 == 0) {
-      byte_cls(C_OTHER);  // ordinary bytes: the class map is idempotent and starts at most one record
-    } else {
+__device__ __forceinline__ void load64(const uint8_t* p, uint32_t* w) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
 #pragma unroll
-      for (int b = 0; b < 4; ++b) byte_cls((c4 >> (8 * b)) & 3u);
-    }
+  for (int v = 0; v < 4; ++v) {
+    const uint4 x = __ldg(q + v);
+    w[4 * v] = x.x;
+    w[4 * v + 1] = x.y;
+    w[4 * v + 2] = x.z;
+    w[4 * v + 3] = x.w;
   }
-};
-
-__device__ __forceinline__ void load_tables(uint64_t* s_step) {
-  for (int i = threadIdx.x; i < NMAPS * 4; i += blockDim.x) s_step[i] = kTab.step[i];
-  __syncthreads();
 }
 
 // Summary of this thread's 64 bytes of the tile.
 __device__ Summ thread_summary(const uint8_t* data, uint64_t nbytes, uint64_t lo, bool aligned,
-                               const uint64_t* s_step) {
-  Walker w{s_step};
+                               const uint64_t* s_step, const uint32_t* s_mapw) {
   if (aligned && lo + kBytesPerThread <= nbytes) {
-    const uint4* p = reinterpret_cast<const uint4*>(data + lo);
-#pragma unroll
-    for (int v = 0; v < kBytesPerThread / 16; ++v) {
-      uint4 q = __ldg(p + v);
-      w.word(q.x);
-      w.word(q.y);
-      w.word(q.z);
-      w.word(q.w);
-    }
-  } else {
-    uint64_t hi = lo + kBytesPerThread < nbytes ? lo + kBytesPerThread : nbytes;
-    for (uint64_t i = lo; i < hi; ++i) w.byte_cls(char_class(data[i]));
+    uint32_t w[16];
+    load64(data + lo, w);
+    const Chunk64 k = scan64(w);
+    if (!k.quotes) return summary_quote_free(k);
+    return summary_by_table(w, s_step, s_mapw);
+  }
+  const uint64_t hi = lo + kBytesPerThread < nbytes ? lo + kBytesPerThread : nbytes;
+  uint32_t id = 0;
+  uint64_t cnt = 0;
+  for (uint64_t i = lo; i < hi; ++i) {
+    const uint64_t e = s_step[id * 4 + char_class(data[i])];
+    id = (uint32_t)e & 63u;
+    cnt += e >> 8;
   }
   Summ r;
-  r.map = kTab.map_word[w.id];
+  r.map = s_mapw[id];
 #pragma unroll
-  for (int s = 0; s < NSTATES; ++s) r.c[s] = (uint32_t)(w.cnt >> (8 * s)) & 0xffu;
+  for (int st = 0; st < NSTATES; ++st) r.c[st] = (uint32_t)(cnt >> (8 * st)) & 0xffu;
   return r;
 }
 
@@ -177,12 +158,13 @@ __global__ void __launch_bounds__(kTileThreads) k_csv_tiles(const uint8_t* __res
                                                             int aligned, uint32_t* __restrict__ tile_map,
                                                             uint32_t* __restrict__ tile_cnt) {
   __shared__ uint64_t s_step[NMAPS * 4];
+  __shared__ uint32_t s_mapw[NMAPS];
   __shared__ Summ s_warp[kTileThreads / 32];
   __shared__ Summ s_total;
-  load_tables(s_step);
+  load_tables(s_step, s_mapw);
   const uint64_t tile = blockIdx.x;
   const uint64_t lo = tile * kTileBytes + (uint64_t)threadIdx.x * kBytesPerThread;
-  Summ mine = lo < nbytes ? thread_summary(data, nbytes, lo, aligned != 0, s_step) : identity_summ();
+  Summ mine = lo < nbytes ? thread_summary(data, nbytes, lo, aligned != 0, s_step, s_mapw) : identity_summ();
   block_exclusive<kTileThreads>(mine, s_warp, &s_total);
   // the total is written by warp 0 before the scan's second barrier
   if (threadIdx.x == 0) {
@@ -228,11 +210,12 @@ __global__ void __launch_bounds__(kTileThreads) k_csv_emit(const uint8_t* __rest
                                                            const unsigned long long* __restrict__ tile_start,
                                                            uint32_t* __restrict__ starts) {
   __shared__ uint64_t s_step[NMAPS * 4];
+  __shared__ uint32_t s_mapw[NMAPS];
   __shared__ Summ s_warp[kTileThreads / 32];
-  load_tables(s_step);
+  load_tables(s_step, s_mapw);
   const uint64_t tile = blockIdx.x;
   const uint64_t lo = tile * kTileBytes + (uint64_t)threadIdx.x * kBytesPerThread;
-  Summ mine = lo < nbytes ? thread_summary(data, nbytes, lo, aligned != 0, s_step) : identity_summ();
+  Summ mine = lo < nbytes ? thread_summary(data, nbytes, lo, aligned != 0, s_step, s_mapw) : identity_summ();
   Summ excl = block_exclusive<kTileThreads>(mine, s_warp, nullptr);
   if (lo >= nbytes) return;
   const unsigned long long ts = tile_start[tile];
@@ -241,31 +224,32 @@ __global__ void __launch_bounds__(kTileThreads) k_csv_emit(const uint8_t* __rest
   uint32_t idx = (uint32_t)ts + excl.c[tstate];
   const uint64_t hi = lo + kBytesPerThread < nbytes ? lo + kBytesPerThread : nbytes;
   if (aligned && hi - lo == kBytesPerThread) {
-    const uint4* p = reinterpret_cast<const uint4*>(data + lo);
+    uint32_t w[16];
+    load64(data + lo, w);  // a second read of the same 64 bytes: an L1 hit
+    const Chunk64 k = scan64(w);
+    if (!k.quotes) {
+      for (uint64_t m = starts_quote_free(k, state); m; m &= m - 1) starts[idx++] = (uint32_t)(lo + __ffsll(m) - 1);
+      return;
+    }
 #pragma unroll
-    for (int v = 0; v < kBytesPerThread / 16; ++v) {
-      uint4 q = __ldg(p + v);
-      uint32_t ws[4] = {q.x, q.y, q.z, q.w};
+    for (int j = 0; j < 16; ++j) {
+      const uint32_t c4 = classes4(w[j]);
+      const uint32_t off = (uint32_t)(lo + 4 * j);
+      if (c4 == 0) {
+        if (state == S_REC) starts[idx++] = off;
+        state = step(C_OTHER, state);
+      } else {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        uint32_t c4 = classes4(ws[k]);
-        uint32_t off = (uint32_t)(lo + v * 16 + k * 4);
-        if (c4 == 0) {
-          if (state == S_REC) starts[idx++] = off;
-          state = step(C_OTHER, state);
-        } else {
-#pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            uint32_t cls = (c4 >> (8 * b)) & 3u;
-            if (starts_record(cls, state)) starts[idx++] = off + b;
-            state = step(cls, state);
-          }
+        for (int b = 0; b < 4; ++b) {
+          const uint32_t cls = (c4 >> (8 * b)) & 3u;
+          if (starts_record(cls, state)) starts[idx++] = off + b;
+          state = step(cls, state);
         }
       }
     }
   } else {
     for (uint64_t i = lo; i < hi; ++i) {
-      uint32_t cls = char_class(data[i]);
+      const uint32_t cls = char_class(data[i]);
       if (starts_record(cls, state)) starts[idx++] = (uint32_t)i;
       state = step(cls, state);
     }
@@ -292,51 +276,40 @@ struct ParseParams {
   FieldDesc f[YQ_CSV_MAX_FIELDS];
 };
 
-struct CellSink {
-  const ParseParams* P;
-  uint32_t row;
-  uint32_t bad;
-  unsigned long long first_bad;
-  __device__ void operator()(uint32_t field, View v, bool quoted, bool escapes) {
-    if (field >= (uint32_t)P->nfields) return;
-    const FieldDesc& fd = P->f[field];
-    if (!fd.data) return;
-    const bool empty = v.len == 0;
-    fd.nulls[row] = empty ? 1 : 0;
-    int32_t st = CONV_OK;
-    switch (fd.type) {
-      case YQ_INT32: {
-        int32_t x = INT32_MIN;
-        if (!empty) st = parse_int32(v, &x);
-        static_cast<int32_t*>(fd.data)[row] = st == CONV_OK ? x : 0;
-        break;
-      }
-      case YQ_FLOAT32: {
-        float x = bits_float(0x00800000u);  // FLT_MIN, the reference's NULL sentinel
-        if (!empty) st = parse_float32(v, &x);
-        static_cast<float*>(fd.data)[row] = st == CONV_OK ? x : 0.0f;
-        break;
-      }
-      case YQ_DATETIME: {
-        static_cast<long long*>(fd.data)[row] = empty ? 0 : parse_datetime(v);
-        break;
-      }
-      default: {  // YQ_TEXT
-        uint32_t* slot = reinterpret_cast<uint32_t*>(static_cast<char*>(fd.data) + (size_t)row * fd.width);
-        auto store = [slot](uint32_t k, uint32_t w) { slot[k] = w; };
-        copy_text(v, escapes, (uint32_t)fd.width, store);
-        break;
-      }
+// Converts one field into row `row` of its output column; returns CONV_*.
+__device__ __forceinline__ int32_t convert_cell(const FieldDesc& fd, uint32_t row, View v, bool escapes) {
+  const bool empty = v.len == 0;
+  fd.nulls[row] = empty ? 1 : 0;
+  int32_t st = CONV_OK;
+  switch (fd.type) {
+    case YQ_INT32: {
+      int32_t x = INT32_MIN;
+      if (!empty) st = parse_int32(v, &x);
+      static_cast<int32_t*>(fd.data)[row] = st == CONV_OK ? x : 0;
+      break;
     }
-    (void)quoted;
-    if (st != CONV_OK) {
-      ++bad;
-      unsigned long long key = (unsigned long long)row << 12 | (unsigned long long)field << 2 | (unsigned)st;
-      if (key < first_bad) first_bad = key;
+    case YQ_FLOAT32: {
+      float x = bits_float(0x00800000u);  // FLT_MIN, the reference's NULL sentinel
+      if (!empty) st = parse_float32(v, &x);
+      static_cast<float*>(fd.data)[row] = st == CONV_OK ? x : 0.0f;
+      break;
+    }
+    case YQ_DATETIME:
+      static_cast<long long*>(fd.data)[row] = empty ? 0 : parse_datetime(v);
+      break;
+    default: {  // YQ_TEXT
+      uint32_t* slot = reinterpret_cast<uint32_t*>(static_cast<char*>(fd.data) + (size_t)row * fd.width);
+      auto store = [slot](uint32_t k, uint32_t w) { slot[k] = w; };
+      copy_text(v, escapes, (uint32_t)fd.width, store);
+      break;
     }
   }
-};
+  return st;
+}
 
+// One thread per record, fields in lockstep: every lane of a warp walks to the
+// end of field f of its own record and then converts it with the same
+// field type, so the conversions run converged.
 __global__ void __launch_bounds__(kParseThreads) k_csv_parse(const __grid_constant__ ParseParams P) {
   extern __shared__ __align__(16) uint8_t s_span[];
   const uint32_t r0 = blockIdx.x * kParseThreads;
@@ -361,16 +334,31 @@ __global__ void __launch_bounds__(kParseThreads) k_csv_parse(const __grid_consta
   if (r >= rend) return;
   const uint64_t st = P.starts[r];
   const uint64_t en = r + 1 < P.nrec ? P.starts[r + 1] : P.nbytes;
-  const uint8_t* rec = staged ? s_span + (st - a0) : P.data + st;
-  CellSink sink{&P, r, 0u, ~0ull};
-  const uint32_t nf = walk_record(rec, (uint32_t)(en - st), sink);
-  const bool ok = nf == (uint32_t)P.nfields;
+  FieldCursor cur;
+  cur.init(staged ? s_span + (st - a0) : P.data + st, (uint32_t)(en - st));
+  uint32_t bad = 0;
+  unsigned long long first_bad = ~0ull;
+  bool ok = true;
+  for (int f = 0; f < P.nfields; ++f) {
+    View v;
+    bool esc;
+    if (!cur.next(&v, &esc)) { ok = false; break; }  // fewer fields than the header
+    const FieldDesc& fd = P.f[f];
+    if (!fd.data) continue;
+    const int32_t cs = convert_cell(fd, r, v, esc);
+    if (cs != CONV_OK) {
+      ++bad;
+      const unsigned long long key = (unsigned long long)r << 12 | (unsigned long long)f << 2 | (unsigned)cs;
+      if (key < first_bad) first_bad = key;
+    }
+  }
+  if (cur.more()) ok = false;  // more fields than the header
   P.valid[r] = ok ? 1 : 0;
   if (!ok) {
     atomicAdd(&P.counters[0], 1ull);
-  } else if (sink.bad) {
-    atomicAdd(&P.counters[1], (unsigned long long)sink.bad);
-    atomicMin(&P.counters[2], sink.first_bad);
+  } else if (bad) {
+    atomicAdd(&P.counters[1], (unsigned long long)bad);
+    atomicMin(&P.counters[2], first_bad);
   }
 }
 
@@ -482,7 +470,7 @@ int yq_csv_parse(const uint8_t* data, uint64_t nbytes, const uint32_t* record_st
     if (c >= ncols || c >= (int)sizeof(seen) || seen[c]) return YQ_ERR_INVALID_ARG;
     seen[c] = 1;
     const yq_column& oc = out[c];
-    if (!oc.data || !oc.nulls) return YQ_ERR_INVALID_ARG;
+    if (records && (!oc.data || !oc.nulls)) return YQ_ERR_INVALID_ARG;  // nothing is written for 0 records
     if (oc.type == YQ_TEXT) {
       if (oc.width < 4 || oc.width > YQ_MAX_TEXT_WIDTH || oc.width % 4) return YQ_ERR_INVALID_ARG;
     } else if (value_width(oc.type) == 0 || oc.width != value_width(oc.type)) {

@@ -20,8 +20,10 @@
 
 #if defined(__CUDACC__)
 #define YQ_CSV_HD __host__ __device__ inline
+#define YQ_CSV_COLD __host__ __device__ __noinline__  // rare paths stay out of the hot loops
 #else
 #define YQ_CSV_HD inline
+#define YQ_CSV_COLD inline __attribute__((noinline))
 #endif
 
 #include <stdint.h>
@@ -100,6 +102,117 @@ constexpr Tables make_tables() {
   }
   t.count = n;
   return t;
+}
+
+// ------------------------------------------------------- chunk summaries
+// A byte range's effect on the tokenizer: the state map and, per start state,
+// how many records start inside the range.
+struct Summary {
+  uint32_t map;
+  uint32_t c[NSTATES];
+};
+
+// 0xff in each byte of w equal to the same byte of pat.
+YQ_CSV_HD uint32_t eq4(uint32_t w, uint32_t pat) {
+#if defined(__CUDA_ARCH__)
+  return __vcmpeq4(w, pat);
+#else
+  uint32_t r = 0;
+  for (int b = 0; b < 4; ++b)
+    if (((w >> (8 * b)) & 0xffu) == ((pat >> (8 * b)) & 0xffu)) r |= 0xffu << (8 * b);
+  return r;
+#endif
+}
+
+// One bit per byte (bit b = byte b) of a 0x00/0xff byte mask.
+YQ_CSV_HD uint32_t byte_bits(uint32_t m) { return ((((m >> 7) & 0x01010101u) * 0x01020408u) >> 24) & 0xfu; }
+
+YQ_CSV_HD int popc64(uint64_t x) {
+#if defined(__CUDA_ARCH__)
+  return __popcll(x);
+#else
+  return __builtin_popcountll(x);
+#endif
+}
+
+// Class of each byte of a word, 2 bits at the bottom of each byte.
+YQ_CSV_HD uint32_t classes4(uint32_t w) {
+  const uint32_t q = eq4(w, 0x22222222u), d = eq4(w, 0x2c2c2c2cu);
+  const uint32_t n = eq4(w, 0x0a0a0a0au) | eq4(w, 0x0d0d0d0du);
+  return (q & 0x01010101u) | (d & 0x02020202u) | (n & 0x03030303u);
+}
+
+// Quote-free 64-byte chunks (most chunks of numeric text): newline bitmask
+// and the first and last byte classes decide everything. With no quote, a
+// start state outside quotes ends in the state the last byte sets, QUO stays
+// QUO, and QQ leaves quotes unless its first byte is ordinary; records start
+// at the non-newline bytes that follow a newline, plus byte 0 from REC.
+struct Chunk64 {
+  uint64_t nl;      // bit b: byte b is '\n' or '\r'
+  bool quotes;      // any '"' in the chunk
+  uint32_t c0, cl;  // classes of the first and last byte
+};
+
+YQ_CSV_HD Chunk64 scan64(const uint32_t* w) {
+  Chunk64 k;
+  uint32_t anyq = 0;
+  k.nl = 0;
+  for (int i = 0; i < 16; ++i) {
+    anyq |= eq4(w[i], 0x22222222u);
+    k.nl |= (uint64_t)byte_bits(eq4(w[i], 0x0a0a0a0au) | eq4(w[i], 0x0d0d0d0du)) << (4 * i);
+  }
+  k.quotes = anyq != 0;
+  k.c0 = char_class(w[0] & 0xffu);
+  k.cl = char_class(w[15] >> 24);
+  return k;
+}
+
+YQ_CSV_HD Summary summary_quote_free(const Chunk64& k) {
+  const uint32_t e = k.cl == C_NL ? S_REC : k.cl == C_DELIM ? S_FIELD : S_UNQ;
+  const uint32_t cnt = (uint32_t)popc64(~k.nl & (k.nl << 1));
+  const bool qq_stays = k.c0 == C_OTHER;
+  Summary s;
+  s.map = e | e << 3 | S_QUO << 6 | (qq_stays ? S_QUO : e) << 9 | e << 12;
+  s.c[S_FIELD] = cnt;
+  s.c[S_UNQ] = cnt;
+  s.c[S_QUO] = 0;
+  s.c[S_QQ] = qq_stays ? 0 : cnt;
+  s.c[S_REC] = cnt + (k.c0 != C_NL ? 1u : 0u);
+  return s;
+}
+
+// Record starts of a quote-free chunk entered in `state`, as a bitmask.
+YQ_CSV_HD uint64_t starts_quote_free(const Chunk64& k, uint32_t state) {
+  if (state == S_QUO || (state == S_QQ && k.c0 == C_OTHER)) return 0;
+  uint64_t m = ~k.nl & (k.nl << 1);
+  if (state == S_REC && k.c0 != C_NL) m |= 1;
+  return m;
+}
+
+// Summary of 64 bytes (16 little-endian words) by the map table: one lookup
+// per byte, one per word of four ordinary bytes (the "other" class map is
+// idempotent and starts at most one record).
+YQ_CSV_HD Summary summary_by_table(const uint32_t* w, const uint64_t* step_tab, const uint32_t* map_word) {
+  uint32_t id = 0;
+  uint64_t cnt = 0;
+  for (int i = 0; i < 16; ++i) {
+    const uint32_t c4 = classes4(w[i]);
+    if (c4 == 0) {
+      const uint64_t e = step_tab[id * 4 + C_OTHER];
+      id = (uint32_t)e & 63u;
+      cnt += e >> 8;
+    } else {
+      for (int b = 0; b < 4; ++b) {
+        const uint64_t e = step_tab[id * 4 + ((c4 >> (8 * b)) & 3u)];
+        id = (uint32_t)e & 63u;
+        cnt += e >> 8;
+      }
+    }
+  }
+  Summary s;
+  s.map = map_word[id];
+  for (int k = 0; k < NSTATES; ++k) s.c[k] = (uint32_t)(cnt >> (8 * k)) & 0xffu;
+  return s;
 }
 
 // ------------------------------------------------------------ field views
@@ -272,7 +385,7 @@ YQ_CSV_HD double pow10_exact(int k) {
 // even) and report ERANGE as glibc's strtof does: overflow, or a result that
 // is tiny (below 2^-126 after rounding to 24 bits) and inexact.
 // `approx` is a double within a relative 1e-12 of the value (or a clamp).
-YQ_CSV_HD int32_t round_decimal(const Decimal& d, double approx, uint32_t* out_bits) {
+YQ_CSV_COLD int32_t round_decimal(const Decimal& d, double approx, uint32_t* out_bits) {
   const uint32_t FMAX = 0x7f7fffffu;
   uint32_t f;
   if (!(approx < 3.4028234663852886e38)) f = FMAX;
@@ -313,7 +426,7 @@ YQ_CSV_HD int32_t round_decimal(const Decimal& d, double approx, uint32_t* out_b
 }
 
 // Round m * 2^e (m > 0, exact) to float32 bits; sticky = nonzero bits below m.
-YQ_CSV_HD int32_t round_binary(uint64_t m, int64_t e, bool sticky, uint32_t* out_bits) {
+YQ_CSV_COLD int32_t round_binary(uint64_t m, int64_t e, bool sticky, uint32_t* out_bits) {
   // normalise m to have bit 63 set
   int lz = 0;
   while (!(m >> 63)) { m <<= 1; ++lz; }
@@ -604,35 +717,86 @@ struct FieldOut {
   int32_t width;  // bytes per value in the output column
 };
 
-// Walks one record starting at rec[0] (state S_REC) and calls
-// sink(field_index, content_view, quoted, has_escapes) for every field; stops
-// at the newline that ends the record or at `len`. Returns the field count.
+// Walks one record field by field, from its first byte (a record start) to
+// the newline that ends it or to `len`: the state machine above, taken one
+// field at a time. A field that opens with '"' is quoted: inside it, "" is an
+// escaped quote, a quote before ',' or a newline (or the end) closes it, and a
+// quote before anything else is kept. An unquoted field runs to the first ','
+// or newline (a quote in it is an ordinary byte).
+struct FieldCursor {
+  const uint8_t* rec;
+  uint32_t len;
+  uint32_t i;
+  bool done;
+
+  YQ_CSV_HD void init(const uint8_t* r, uint32_t l) {
+    rec = r;
+    len = l;
+    i = 0;
+    done = false;
+  }
+  // The next field's content (without its quotes); false once the record has
+  // no more fields.
+  YQ_CSV_HD bool next(View* v, bool* escapes) {
+    if (done) return false;
+    *escapes = false;
+    if (i < len && rec[i] == '"') {
+      const uint32_t begin = ++i;
+      for (;;) {
+        if (i >= len) {  // the text ends inside the quotes
+          *v = View{rec + begin, i - begin};
+          done = true;
+          return true;
+        }
+        if (rec[i] != '"') { ++i; continue; }
+        if (i + 1 >= len) {  // closing quote at the end of the text
+          *v = View{rec + begin, i - begin};
+          done = true;
+          return true;
+        }
+        const uint32_t d = rec[i + 1];
+        if (d == ',') {
+          *v = View{rec + begin, i - begin};
+          i += 2;
+          return true;
+        }
+        if (d == '\n' || d == '\r') {
+          *v = View{rec + begin, i - begin};
+          done = true;
+          return true;
+        }
+        if (d == '"') { *escapes = true; i += 2; continue; }
+        ++i;  // a lone quote stays in the field
+      }
+    }
+    const uint32_t begin = i;
+    for (; i < len; ++i) {
+      const uint32_t c = rec[i];
+      if (c == ',') {
+        *v = View{rec + begin, i - begin};
+        ++i;
+        return true;
+      }
+      if (c == '\n' || c == '\r') break;
+    }
+    *v = View{rec + begin, i - begin};
+    done = true;
+    return true;
+  }
+  YQ_CSV_HD bool more() const { return !done; }
+};
+
+// Calls sink(field_index, content_view, has_escapes) for every field of the
+// record; returns the field count.
 template <class Sink>
 YQ_CSV_HD uint32_t walk_record(const uint8_t* rec, uint32_t len, Sink& sink) {
-  uint32_t state = S_REC, field = 0, begin = 0;
-  bool quoted = false, escapes = false;
-  uint32_t i = 0;
-  for (; i < len; ++i) {
-    uint32_t c = rec[i], cls = char_class(c);
-    uint32_t ns = step(cls, state);
-    if ((state == S_REC || state == S_FIELD) && cls == C_QUOTE) { quoted = true; begin = i + 1; }
-    if (state == S_QQ && cls == C_QUOTE) escapes = true;
-    bool ends_field = (cls == C_DELIM || cls == C_NL) && state != S_QUO;
-    if (ends_field) {
-      uint32_t end = (quoted && state == S_QQ) ? i - 1 : i;
-      sink(field, View{rec + begin, end - begin}, quoted, escapes);
-      ++field;
-      quoted = false;
-      escapes = false;
-      begin = i + 1;
-      if (cls == C_NL) return field;
-    }
-    state = ns;
-  }
-  // end of data: the last field closes here
-  uint32_t end = (quoted && state == S_QQ) ? i - 1 : i;
-  sink(field, View{rec + begin, end - begin}, quoted, escapes);
-  return field + 1;
+  FieldCursor cur;
+  cur.init(rec, len);
+  View v;
+  bool esc;
+  uint32_t n = 0;
+  while (cur.next(&v, &esc)) sink(n++, v, esc);
+  return n;
 }
 
 // Copies a field's text into a slot of `width` bytes as String::set does:

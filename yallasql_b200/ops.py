@@ -613,12 +613,16 @@ def csv_scan(text: torch.Tensor, types: list[int], project: list[int] | None = N
         raise ValueError("text must be a contiguous uint8 CUDA tensor")
     records = C.c_uint64(0)
     ptr = text.data_ptr() if nbytes else None
-    st = L.yq_csv_index(ptr, nbytes, None, 0, C.byref(records), None, 0, s)
-    if st not in (A.OK, A.ERR_CAPACITY):
-        _check(st, "yq_csv_index")
+    # one index call with room for records of 16 bytes on average; a second
+    # one, with the exact count, only for text of shorter records
+    cap = nbytes // 16 + 1024
+    starts = torch.empty(cap, dtype=torch.int32, device=text.device)
+    st = L.yq_csv_index(ptr, nbytes, starts.data_ptr(), cap, C.byref(records), None, 0, s)
+    if st == A.ERR_CAPACITY:
+        starts = torch.empty(int(records.value), dtype=torch.int32, device=text.device)
+        st = L.yq_csv_index(ptr, nbytes, starts.data_ptr(), int(records.value), C.byref(records), None, 0, s)
+    _check(st, "yq_csv_index")
     n = int(records.value)
-    starts = torch.empty(max(n, 1), dtype=torch.int32, device=text.device)
-    _check(L.yq_csv_index(ptr, nbytes, starts.data_ptr(), n, C.byref(records), None, 0, s), "yq_csv_index")
     cols = []
     field_col = [-1] * len(types)
     for i, f in enumerate(project):
