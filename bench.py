@@ -377,7 +377,49 @@ def csv_suite(lib, peak: float, rows: int = 8_000_000) -> dict:
     out["cpu_baseline"] = {"value": sample / dt, "unit": "rows/s", "cores": 1, "kind": kind,
                            "sample": f"first {sample} of {rows} rows ({cut} bytes): csv-parser read_row + "
                                      "std::stoi/std::stof/strptime+timegm per field, as GetOperator::next"}
-    del text, staging, cols
+    # the writer (CsvWriter::batchToCsv on the device) over the scanned columns
+    batch = ops.DeviceBatch(cols)
+    bc, keep = batch.c()
+    nout = C.c_uint64(0)
+    lib.yq_csv_format(C.byref(bc), None, 0, C.byref(nout), None, 0, s)
+    text_out = torch.empty(int(nout.value), dtype=torch.uint8, device="cuda")
+    fws = torch.empty(lib.yq_csv_format_workspace_size(rows), dtype=torch.uint8, device="cuda")
+
+    def fmt():
+        A.check(lib.yq_csv_format(C.byref(bc), text_out.data_ptr(), text_out.numel(), C.byref(nout), fws.data_ptr(),
+                                  fws.numel(), s), "yq_csv_format")
+    fmt()
+    torch.cuda.synchronize()
+    lib.yq_profile_enable(1)
+    lib.yq_profile_read(None, 0, 1)
+    fms = _timed(fmt, reps)
+    buf = C.create_string_buffer(1 << 14)
+    lib.yq_profile_read(buf, len(buf), 1)
+    lib.yq_profile_enable(0)
+    prof = json.loads(buf.value.decode() or "{}")
+    fk = {}
+    for tag in ("csv_format_len", "csv_format_write"):
+        k = prof.get(tag, {})
+        if k.get("launches"):
+            per_ms = k["ms"] / k["launches"]
+            entry = {"kernel_ms": round(per_ms, 4)}
+            if k["units"]:
+                gbs = k["units"] / k["launches"] / (per_ms / 1e3) / 1e9
+                entry.update({"achieved_gbs": round(gbs, 1), "frac_of_measured_hbm": round(gbs / peak, 4),
+                              "algorithmic_bytes_per_launch": k["units"] / k["launches"]})
+            fk[tag] = entry
+    w_sample = min(rows, 1_000_000)
+    host_cols = [(t, c.width if t == A.TEXT else 0, c.data[:w_sample].cpu().numpy(), c.nulls[:w_sample].cpu().numpy())
+                 for t, c in zip([0, 1, 0, 0, 3, 2], cols)]
+    t0 = time.perf_counter()
+    oracle.csv_format(host_cols, w_sample)
+    wdt = time.perf_counter() - t0
+    out["write"] = {"rows": rows, "text_bytes": int(nout.value), "ms": round(fms, 4), "rows_per_s": rows / (fms / 1e3),
+                    "text_gbs": round(int(nout.value) / (fms / 1e3) / 1e9, 1), "kernels": fk,
+                    "cpu_baseline": {"value": w_sample / wdt, "unit": "rows/s", "cores": 1, "kind": "port",
+                                     "sample": f"first {w_sample} rows: snprintf / gmtime_r + strftime per cell, "
+                                               "as CsvWriter::batchToCsv (std::to_chars) formats them"}}
+    del text, staging, cols, batch, keep, text_out
     return out
 
 

@@ -569,6 +569,20 @@ int yq_csv_parse(const uint8_t* data, uint64_t nbytes, const uint32_t* record_st
                  const int32_t* field_column, int32_t nfields, yq_column* out, int32_t ncols, uint32_t* rows,
                  yq_csv_error* error, void* workspace, size_t workspace_bytes, void* stream);
 
+size_t yq_csv_format_workspace_size(uint32_t rows);
+/* CsvWriter::batchToCsv (include/engine/operators/csv_writer.hpp:24-76) on the
+ * device, without the header line: each row's cells joined by ',' and ended
+ * by '\n'; NULL -> ""; INT32/INT64 -> std::to_chars; FLOAT32 -> std::to_chars
+ * (fixed, 4 decimals; inf, -inf, nan, -nan); DATETIME -> quoted gmtime_r +
+ * strftime("%Y-%m-%d %H:%M:%S") (data_type_utils.hpp:46-57); TEXT -> quoted
+ * bytes up to the slot's first NUL, not escaped. Writes the text to `out`
+ * (device) and its length to *bytes; synchronises `stream` to read the
+ * length, and returns YQ_ERR_CAPACITY (nothing written, *bytes = the length)
+ * when it exceeds `capacity`. Line offsets are 32-bit: YQ_ERR_UNSUPPORTED when
+ * rows x the widest possible line reaches 4 GiB. */
+int yq_csv_format(const yq_batch* batch, uint8_t* out, uint64_t capacity, uint64_t* bytes, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------- device */
 /* Number of SMs of the current device (cached per device). */
 int yq_device_sm_count(void);

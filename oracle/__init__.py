@@ -249,3 +249,22 @@ def convert_batch(kind: int, strings: list) -> tuple:
     L.orc_convert_batch(C.c_int(kind), C.c_char_p(buf), offs.ctypes.data_as(C.c_void_p), C.c_uint64(len(strings)),
                         out.ctypes.data_as(C.c_void_p), st.ctypes.data_as(C.c_void_p))
     return out, st
+
+
+def csv_format(cols: list, rows: int) -> bytes:
+    """The reference writer's rows (CsvWriter::batchToCsv without the header)
+    for columns given as (type, width, values ndarray, nulls ndarray or None);
+    type 0 INT32, 1 FLOAT32, 2 DATETIME, 3 TEXT (values uint8 [rows, width]), 4 INT64."""
+    L = lib()
+    L.orc_csv_format.restype = C.c_uint64
+    n = len(cols)
+    keep = [np.ascontiguousarray(v) for _, _, v, _ in cols]
+    nul = [None if x is None else np.ascontiguousarray(x, dtype=np.uint8) for _, _, _, x in cols]
+    ty = (C.c_int * n)(*[c[0] for c in cols])
+    wd = (C.c_int * n)(*[c[1] for c in cols])
+    dp = (C.c_void_p * n)(*[k.ctypes.data for k in keep])
+    npp = (C.c_void_p * n)(*[None if x is None else x.ctypes.data for x in nul])
+    need = L.orc_csv_format(n, ty, wd, dp, npp, C.c_uint64(rows), None, C.c_uint64(0))
+    buf = C.create_string_buffer(int(need) + 1)
+    L.orc_csv_format(n, ty, wd, dp, npp, C.c_uint64(rows), buf, C.c_uint64(need))
+    return buf.raw[: int(need)]

@@ -415,6 +415,7 @@ void orc_gather(const void* src, void* dst, int width, const uint32_t* perm, uin
 #include <errno.h>
 #include <limits.h>
 #include <float.h>
+#include <stdio.h>
 #include <time.h>
 
 typedef struct {
@@ -617,4 +618,56 @@ void orc_convert_batch(int kind, const char* buf, const uint64_t* offs, uint64_t
       out[i] = strptime(tmp, "%Y-%m-%d %H:%M:%S", &t) != NULL ? (int64_t)timegm(&t) : 0;
     }
   }
+}
+
+/* ---------------------------------------------------------------- CSV writer
+ * Restates CsvWriter::batchToCsv's row loop (include/engine/operators/
+ * csv_writer.hpp:42-76) without the header line: cells joined by ',', rows
+ * ended by '\n'; NULL -> ""; STRING -> "value" (up to its NUL, no escaping);
+ * INT -> decimal (std::to_chars); FLOAT -> std::to_chars(fixed, 4), which
+ * formats like printf("%.4f") of the exact value; DATETIME -> "..." from
+ * gmtime_r + strftime("%Y-%m-%d %H:%M:%S") into 26 bytes (data_type_utils.hpp:46-57).
+ * type: 0 INT32, 1 FLOAT32, 2 DATETIME, 3 TEXT (slot `width`), 4 INT64.
+ * Returns the bytes written, or the bytes needed when above `cap`. */
+static size_t orc_cell(char* o, int type, const void* data, const unsigned char* nulls, int width, uint64_t r) {
+  if (nulls && nulls[r]) { memcpy(o, "\"\"", 2); return 2; }
+  if (type == 0) return (size_t)sprintf(o, "%d", ((const int32_t*)data)[r]);
+  if (type == 4) return (size_t)sprintf(o, "%lld", (long long)((const int64_t*)data)[r]);
+  if (type == 1) return (size_t)sprintf(o, "%.4f", (double)((const float*)data)[r]);
+  if (type == 2) {
+    time_t t = (time_t)((const int64_t*)data)[r];
+    struct tm tm;
+    char buf[26];
+    size_t n = 0;
+    o[n++] = '"';
+    if (gmtime_r(&t, &tm)) {
+      size_t k = strftime(buf, 26, "%Y-%m-%d %H:%M:%S", &tm);
+      memcpy(o + n, buf, k);
+      n += k;
+    }
+    o[n++] = '"';
+    return n;
+  }
+  const char* s = (const char*)data + r * (uint64_t)width;
+  size_t n = 0;
+  o[n++] = '"';
+  for (int i = 0; i < width && s[i]; ++i) o[n++] = s[i];
+  o[n++] = '"';
+  return n;
+}
+
+uint64_t orc_csv_format(int ncols, const int* types, const int* widths, const void** data,
+                        const unsigned char** nulls, uint64_t rows, char* out, uint64_t cap) {
+  char cell[512];
+  uint64_t n = 0;
+  for (uint64_t r = 0; r < rows; ++r) {
+    for (int c = 0; c < ncols; ++c) {
+      size_t k = orc_cell(cell, types[c], data[c], nulls ? nulls[c] : NULL, widths[c], r);
+      if (c + 1 < ncols) cell[k++] = ',';
+      else cell[k++] = '\n';
+      if (n + k <= cap) memcpy(out + n, cell, k);
+      n += k;
+    }
+  }
+  return n;
 }

@@ -173,3 +173,34 @@ int64_t hs_csv_scan(const uint8_t* text, uint64_t n, int nfields, const int* fie
 }
 
 }  // extern "C"
+
+extern "C" {
+// The writer's cell formatting on the host: kind 0 int32, 1 float32 (bits),
+// 2 datetime, 4 int64. Each cell's text goes to out[i*64 ...], its length to len[i].
+void hs_format(int kind, const int64_t* vals, uint64_t n, char* out, int32_t* len) {
+  for (uint64_t i = 0; i < n; ++i) {
+    int32_t i32 = (int32_t)vals[i];
+    uint32_t fb = (uint32_t)vals[i];
+    float f;
+    std::memcpy(&f, &fb, 4);
+    const void* data = kind == 0 ? (const void*)&i32 : kind == 1 ? (const void*)&f : (const void*)&vals[i];
+    BufOut o{reinterpret_cast<uint8_t*>(out + i * 64)};
+    put_cell(o, data, nullptr, kind, 0, 0);
+    CountOut c;
+    put_cell(c, data, nullptr, kind, 0, 0);
+    len[i] = (int32_t)(o.p - reinterpret_cast<uint8_t*>(out + i * 64));
+    if ((uint32_t)len[i] != c.n) len[i] = -1;  // the counting pass must agree with the writing pass
+  }
+}
+}
+
+#include <charconv>
+extern "C" {
+// std::to_chars(float, fixed, 4): the reference writer's own float routine.
+int32_t hs_to_chars_fixed4(uint32_t bits, char* out) {
+  float f;
+  std::memcpy(&f, &bits, 4);
+  auto r = std::to_chars(out, out + 64, f, std::chars_format::fixed, 4);
+  return (int32_t)(r.ptr - out);
+}
+}

@@ -192,3 +192,43 @@ def test_schema_follows_header_tags():
                                                    ("t", A.TEXT, False), ("plain", A.TEXT, False)]
     with pytest.raises(ValueError):
         ops.csv_schema(" (N)", "1")
+
+
+def test_writer_cells_match_the_reference_routines(shim):
+    """Cell text of the device writer (host build) against the oracle's
+    snprintf / gmtime_r + strftime, and the oracle's "%.4f" against
+    std::to_chars(fixed, 4), the reference writer's own float routine."""
+    rng = np.random.default_rng(16)
+
+    def shim_cells(kind, vals):
+        vals = np.asarray(vals, dtype=np.int64)
+        out = C.create_string_buffer(64 * len(vals))
+        ln = np.zeros(len(vals), np.int32)
+        shim.hs_format(C.c_int(kind), vals.ctypes.data_as(C.c_void_p), C.c_uint64(len(vals)), out,
+                       ln.ctypes.data_as(C.c_void_p))
+        assert (ln >= 0).all(), "counting and writing passes disagree"
+        return [out.raw[i * 64:i * 64 + ln[i]] for i in range(len(vals))]
+
+    def oracle_cells(kind, vals, dtype):
+        arr = np.asarray(vals).astype(dtype)
+        text = oracle.csv_format([(kind, 0, arr, None)], len(arr))
+        return text.split(b"\n")[:-1]
+
+    bits = [int(b) for b in rng.integers(0, 2**32, 20000, dtype=np.uint64)]
+    bits += [int(x) for x in (rng.integers(100, 100000, 5000) / 100.0).astype(np.float32).view(np.uint32)]
+    bits += [int(np.float32(m / 2.0**k).view(np.uint32)) for k in range(1, 40) for m in (1, 3, 5, 7)]  # ties
+    bits += [0, 0x80000000, 1, 0x7f7fffff, 0xff7fffff, 0x7f800000, 0xff800000, 0x7fc00000, 0xffc00000]
+    assert shim_cells(1, bits) == oracle_cells(1, bits, np.uint32)
+    shim.hs_to_chars_fixed4.restype = C.c_int32
+    buf = C.create_string_buffer(64)
+    want = oracle_cells(1, bits[:3000], np.uint32)
+    for b, w in zip(bits[:3000], want):
+        n = shim.hs_to_chars_fixed4(C.c_uint32(b), buf)
+        assert buf.raw[:n] == w
+    ints = [int(x) for x in rng.integers(-2**31, 2**31, 5000)] + [-2**31, 2**31 - 1, 0]
+    assert shim_cells(0, ints) == oracle_cells(0, ints, np.int32)
+    big = [int(x) for x in rng.integers(-2**63, 2**63 - 1, 5000, dtype=np.int64)] + [-2**63, 2**63 - 1]
+    assert shim_cells(4, big) == oracle_cells(4, big, np.int64)
+    secs = [int(x) for x in rng.integers(-62167219200 - 86400 * 366 * 50, 253402300800 + 86400 * 366 * 50, 5000)]
+    secs += [int(x) for x in rng.integers(-2**40, 2**40, 2000)] + [0, -1, -62167219200, -62167219201, 253402300800]
+    assert shim_cells(2, secs) == oracle_cells(2, secs, np.int64)

@@ -161,6 +161,8 @@ PROTOTYPES = {
     "yq_csv_index": (C.c_int, [vp, u64, vp, u64, P(u64), vp, sz, vp]),
     "yq_csv_parse_workspace_size": (sz, [u32]),
     "yq_csv_parse": (C.c_int, [vp, u64, vp, u32, P(i32), i32, P(Column), i32, P(u32), P(CsvError), vp, sz, vp]),
+    "yq_csv_format_workspace_size": (sz, [u32]),
+    "yq_csv_format": (C.c_int, [P(Batch), vp, u64, P(u64), vp, sz, vp]),
     "yq_device_sm_count": (C.c_int, []),
     "yq_launch_count": (u64, []),
     "yq_profile_enable": (C.c_int, [i32]),

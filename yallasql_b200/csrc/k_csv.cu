@@ -376,6 +376,86 @@ __global__ void k_csv_compact(const uint8_t* __restrict__ src, const uint8_t* __
   }
 }
 
+// ------------------------------------------------------------------ writer
+constexpr int kFmtThreads = 128;
+constexpr uint32_t kFmtSpan = 24 * 1024;  // staged output bytes per write block
+
+struct FmtCol {
+  const void* data;
+  const uint8_t* nulls;
+  int32_t type;
+  int32_t width;
+};
+
+struct FmtParams {
+  FmtCol c[YQ_CSV_MAX_FIELDS];
+  int32_t ncols;
+  uint32_t rows;
+  uint32_t* len;        // bytes of each row's line
+  const uint32_t* end;  // inclusive scan of len: where each line ends
+  uint8_t* out;
+  int32_t out_aligned4;  // `out` is 4-byte aligned: the copy-out may use word stores
+};
+
+// One row's line, columns in lockstep across the warp (one cell type at a time).
+template <class Out>
+__device__ __forceinline__ void format_row(const FmtParams& P, uint32_t r, Out& o) {
+  for (int c = 0; c < P.ncols; ++c) {
+    if (c) o.put(',');
+    const FmtCol& fc = P.c[c];
+    put_cell(o, fc.data, fc.nulls, fc.type, fc.width, r);
+  }
+  o.put('\n');
+}
+
+__global__ void __launch_bounds__(256) k_csv_format_len(const __grid_constant__ FmtParams P) {
+  const uint32_t r = blockIdx.x * 256 + threadIdx.x;
+  if (r >= P.rows) return;
+  CountOut o;
+  format_row(P, r, o);
+  P.len[r] = o.n;
+}
+
+// 128 lines a block, written into shared memory and copied out with 4-byte
+// stores (the block's first and last partial words byte by byte: they share
+// a word with the neighbouring blocks' lines).
+__global__ void __launch_bounds__(kFmtThreads) k_csv_format_write(const __grid_constant__ FmtParams P) {
+  extern __shared__ __align__(16) uint8_t s_out[];
+  const uint32_t r0 = blockIdx.x * kFmtThreads;
+  const uint32_t rend = r0 + kFmtThreads < P.rows ? r0 + kFmtThreads : P.rows;
+  const uint32_t base = r0 ? P.end[r0 - 1] : 0u, stop = P.end[rend - 1];
+  const uint32_t abase = base & ~3u;  // s_out[i] holds output byte abase + i
+  const bool staged = stop - abase <= kFmtSpan;
+  const uint32_t r = r0 + threadIdx.x;
+  if (r < rend) {
+    const uint32_t off = P.end[r] - P.len[r];
+    BufOut o{staged ? s_out + (off - abase) : P.out + off};
+    format_row(P, r, o);
+  }
+  if (!staged) return;
+  __syncthreads();
+  const uint32_t w0 = (base + 3) & ~3u, w1 = stop & ~3u;  // whole words inside [base, stop)
+  if (w0 >= w1 || !P.out_aligned4) {
+    for (uint32_t i = base + threadIdx.x; i < stop; i += kFmtThreads) P.out[i] = s_out[i - abase];
+    return;
+  }
+  for (uint32_t i = base + threadIdx.x; i < w0; i += kFmtThreads) P.out[i] = s_out[i - abase];
+  for (uint32_t i = w1 + threadIdx.x; i < stop; i += kFmtThreads) P.out[i] = s_out[i - abase];
+  for (uint32_t i = w0 + 4 * threadIdx.x; i < w1; i += 4 * kFmtThreads)
+    *reinterpret_cast<uint32_t*>(P.out + i) = *reinterpret_cast<const uint32_t*>(s_out + (i - abase));
+}
+
+int fmt_max_cell(int32_t type, int32_t width) {
+  switch (type) {
+    case YQ_INT32: return 11;
+    case YQ_INT64: return 20;
+    case YQ_FLOAT32: return 46;   // sign, 39 integer digits, '.', 4 decimals
+    case YQ_DATETIME: return 29;  // quotes, signed 11-digit year, "-MM-DD HH:MM:SS"
+    case YQ_TEXT: return width + 2;
+    default: return -1;
+  }
+}
+
 uint32_t csv_tiles(uint64_t nbytes) { return (uint32_t)((nbytes + kTileBytes - 1) / kTileBytes); }
 
 int value_width(int32_t type) {
@@ -543,6 +623,76 @@ int yq_csv_parse(const uint8_t* data, uint64_t nbytes, const uint32_t* record_st
       *error = yq_csv_error{h[1], first, (int32_t)((h[2] >> 2) & 1023), (int32_t)(h[2] & 3)};
     }
     return YQ_ERR_INVALID_ARG;
+  }
+  return YQ_OK;
+}
+
+size_t yq_csv_format_workspace_size(uint32_t rows) {
+  WsSize w;
+  w.add<uint32_t>((size_t)rows + 1);
+  w.add<uint32_t>((size_t)rows + 1);
+  w.used += yq_prefix_sum_workspace_size(rows);
+  return w.total();
+}
+
+int yq_csv_format(const yq_batch* batch, uint8_t* out, uint64_t capacity, uint64_t* bytes, void* workspace,
+                  size_t workspace_bytes, void* stream) {
+  if (!batch || !bytes || batch->ncols <= 0 || batch->ncols > YQ_CSV_MAX_FIELDS || !batch->columns)
+    return YQ_ERR_INVALID_ARG;
+  *bytes = 0;
+  const uint32_t rows = batch->rows;
+  FmtParams P;
+  uint64_t max_line = 0;
+  for (int c = 0; c < batch->ncols; ++c) {
+    const yq_column& col = batch->columns[c];
+    const int mc = fmt_max_cell(col.type, col.width);
+    if (mc < 0) return YQ_ERR_UNSUPPORTED;
+    if ((col.type == YQ_TEXT && (col.width < 1 || col.width > YQ_MAX_TEXT_WIDTH)) ||
+        (col.type != YQ_TEXT && col.width != (col.type == YQ_INT32 || col.type == YQ_FLOAT32 ? 4 : 8)))
+      return YQ_ERR_INVALID_ARG;
+    if (rows && !col.data) return YQ_ERR_INVALID_ARG;
+    P.c[c] = FmtCol{col.data, col.nulls, col.type, col.width};
+    max_line += (uint64_t)mc + 1;
+  }
+  if (rows == 0) return YQ_OK;
+  if ((uint64_t)rows * max_line >= (1ull << 32)) return YQ_ERR_UNSUPPORTED;  // 32-bit line offsets
+  cudaStream_t s = as_stream(stream);
+  Workspace ws;
+  YQ_TRY(ws.acquire(workspace, workspace_bytes, yq_csv_format_workspace_size(rows), s));
+  P.ncols = batch->ncols;
+  P.rows = rows;
+  P.len = ws.take<uint32_t>((size_t)rows + 1);
+  uint32_t* end = ws.take<uint32_t>((size_t)rows + 1);
+  void* scan_ws = ws.take<uint8_t>(yq_prefix_sum_workspace_size(rows));
+  P.end = end;
+  P.out = out;
+  P.out_aligned4 = (reinterpret_cast<uintptr_t>(out) & 3) == 0;
+  {
+    ProfScope ps("csv_format_len", s, 0.0);
+    k_csv_format_len<<<ceil_div<uint32_t>(rows, 256), 256, 0, s>>>(P);
+    YQ_CHECK_LAUNCH();
+  }
+  YQ_TRY(yq_prefix_sum_u32(P.len, end, rows, scan_ws, yq_prefix_sum_workspace_size(rows), stream));
+  uint32_t total = 0;
+  YQ_TRY_CUDA(cudaMemcpyAsync(&total, end + rows - 1, sizeof(total), cudaMemcpyDeviceToHost, s));
+  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  *bytes = total;
+  if (total > capacity) return YQ_ERR_CAPACITY;
+  if (!out) return YQ_ERR_INVALID_ARG;
+  int dev = 0;
+  YQ_TRY_CUDA(cudaGetDevice(&dev));
+  static unsigned long long smem_set = 0;  // one bit per device
+  if (dev < 64 && !((smem_set >> dev) & 1)) {
+    YQ_TRY_CUDA(cudaFuncSetAttribute(k_csv_format_write, cudaFuncAttributeMaxDynamicSharedMemorySize, kFmtSpan + 16));
+    smem_set |= 1ull << dev;
+  }
+  double in_bytes = 0;
+  for (int c = 0; c < batch->ncols; ++c)
+    in_bytes += (double)rows * (batch->columns[c].width + (batch->columns[c].nulls ? 1 : 0));
+  {
+    ProfScope ps("csv_format_write", s, in_bytes + (double)total);
+    k_csv_format_write<<<ceil_div<uint32_t>(rows, kFmtThreads), kFmtThreads, kFmtSpan + 16, s>>>(P);
+    YQ_CHECK_LAUNCH();
   }
   return YQ_OK;
 }

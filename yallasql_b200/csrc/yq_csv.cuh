@@ -825,5 +825,180 @@ YQ_CSV_HD void copy_text(View v, bool escapes, uint32_t width, Store& store) {
   }
 }
 
+// ---------------------------------------------------------------- writer
+// Cell text as CsvWriter::batchToCsv writes it
+// (include/engine/operators/csv_writer.hpp:42-73): INT by std::to_chars,
+// FLOAT by std::to_chars(..., chars_format::fixed, 4), DATETIME quoted as
+// gmtime_r + strftime("%Y-%m-%d %H:%M:%S") (data_type_utils.hpp:46-57), STRING
+// quoted as stored (up to its NUL, no escaping), NULL as "". `Out` provides
+// put(c) (append a byte), put_at(k, c) (the byte k places after the current
+// end, before a skip(n) that moves the end past it) and skip(n).
+
+template <class Out>
+YQ_CSV_HD void put_u64(Out& o, uint64_t v) {
+  uint32_t n = 1;
+  for (uint64_t t = v; t >= 10; t /= 10) ++n;
+  for (uint32_t k = n; k-- > 0; v /= 10) o.put_at(k, (uint32_t)('0' + v % 10));
+  o.skip(n);
+}
+
+template <class Out>
+YQ_CSV_HD void put_i64(Out& o, int64_t v) {
+  if (v < 0) {
+    o.put('-');
+    put_u64(o, 0ull - (uint64_t)v);
+  } else {
+    put_u64(o, (uint64_t)v);
+  }
+}
+
+template <class Out>
+YQ_CSV_HD void put_2(Out& o, uint32_t v) {
+  o.put('0' + v / 10);
+  o.put('0' + v % 10);
+}
+
+// Decimal digits of a value below 2^128 held as four 32-bit limbs.
+template <class Out>
+YQ_CSV_COLD void put_u128(Out& o, uint32_t l0, uint32_t l1, uint32_t l2, uint32_t l3) {
+  uint32_t lim[4] = {l0, l1, l2, l3};
+  uint32_t chunk[5];  // base 10^9, least significant first
+  int nc = 0;
+  do {
+    uint64_t rem = 0;
+    for (int i = 3; i >= 0; --i) {
+      const uint64_t cur = rem << 32 | lim[i];
+      lim[i] = (uint32_t)(cur / 1000000000u);
+      rem = cur % 1000000000u;
+    }
+    chunk[nc++] = (uint32_t)rem;
+  } while ((lim[0] | lim[1] | lim[2] | lim[3]) && nc < 5);
+  put_u64(o, chunk[nc - 1]);
+  for (int c = nc - 2; c >= 0; --c) {
+    uint32_t v = chunk[c];
+    for (int k = 8; k >= 0; --k, v /= 10) o.put_at((uint32_t)k, '0' + v % 10);
+    o.skip(9);
+  }
+}
+
+// std::to_chars(float, fixed, 4): the exact binary value rounded to four
+// decimals, ties to even; "inf", "-inf", "nan", "-nan".
+template <class Out>
+YQ_CSV_HD void put_fixed4(Out& o, float x) {
+  const uint32_t b = float_bits(x);
+  const uint32_t ex = (b >> 23) & 0xffu, man = b & 0x7fffffu;
+  if (b >> 31) o.put('-');
+  if (ex == 0xff) {
+    if (man) { o.put('n'); o.put('a'); o.put('n'); }
+    else { o.put('i'); o.put('n'); o.put('f'); }
+    return;
+  }
+  const uint64_t m = ex ? (man | 0x800000u) : man;
+  const int e = ex ? (int)ex - 150 : -149;
+  if (e >= 0) {  // an integer m * 2^e < 2^128
+    const int w = e >> 5, sh = e & 31;
+    uint32_t lim[5] = {0, 0, 0, 0, 0};
+    const uint64_t v = m << sh;  // < 2^56
+    lim[w] = (uint32_t)v;
+    lim[w + 1] = (uint32_t)(v >> 32);
+    put_u128(o, lim[0], lim[1], lim[2], lim[3]);
+    o.put('.'); o.put('0'); o.put('0'); o.put('0'); o.put('0');
+    return;
+  }
+  const int k = -e;                  // 1..149
+  const uint64_t t = m * 10000u;     // < 2^38
+  uint64_t q = 0;
+  if (k < 64) {
+    q = t >> k;
+    const uint64_t r = t & ((1ull << k) - 1), half = 1ull << (k - 1);
+    if (r > half || (r == half && (q & 1))) ++q;
+  }
+  put_u64(o, q / 10000);
+  uint32_t f = (uint32_t)(q % 10000);
+  o.put('.');
+  o.put('0' + f / 1000);
+  o.put('0' + f / 100 % 10);
+  o.put('0' + f / 10 % 10);
+  o.put('0' + f % 10);
+}
+
+// y-m-d from days since 1970-01-01 (proleptic Gregorian; the inverse of
+// days_from_civil, H. Hinnant's civil_from_days).
+YQ_CSV_HD void civil_from_days(int64_t z, int64_t* y, uint32_t* m, uint32_t* d) {
+  z += 719468;
+  const int64_t era = (z >= 0 ? z : z - 146096) / 146097;
+  const uint64_t doe = (uint64_t)(z - era * 146097);
+  const uint64_t yoe = (doe - doe / 1460 + doe / 36524 - doe / 146096) / 365;
+  const uint64_t doy = doe - (365 * yoe + yoe / 4 - yoe / 100);
+  const uint64_t mp = (5 * doy + 2) / 153;
+  *d = (uint32_t)(doy - (153 * mp + 2) / 5 + 1);
+  *m = (uint32_t)(mp < 10 ? mp + 3 : mp - 9);
+  *y = (int64_t)yoe + era * 400 + (*m <= 2);
+}
+
+// gmtime_r + strftime("%Y-%m-%d %H:%M:%S"): the year unpadded, with its sign.
+template <class Out>
+YQ_CSV_HD void put_datetime(Out& o, int64_t secs) {
+  int64_t days = secs / 86400, rem = secs % 86400;
+  if (rem < 0) { rem += 86400; --days; }
+  int64_t y;
+  uint32_t mo, d;
+  civil_from_days(days, &y, &mo, &d);
+  put_i64(o, y);
+  o.put('-');
+  put_2(o, mo);
+  o.put('-');
+  put_2(o, d);
+  o.put(' ');
+  put_2(o, (uint32_t)(rem / 3600));
+  o.put(':');
+  put_2(o, (uint32_t)(rem / 60 % 60));
+  o.put(':');
+  put_2(o, (uint32_t)(rem % 60));
+}
+
+// One cell. type: YQ_INT32 0, YQ_FLOAT32 1, YQ_DATETIME 2, YQ_TEXT 3, YQ_INT64 4.
+template <class Out>
+YQ_CSV_HD void put_cell(Out& o, const void* data, const uint8_t* nulls, int32_t type, int32_t width, uint64_t row) {
+  if (nulls && nulls[row]) {
+    o.put('"');
+    o.put('"');
+    return;
+  }
+  switch (type) {
+    case 0: put_i64(o, static_cast<const int32_t*>(data)[row]); break;
+    case 1: put_fixed4(o, static_cast<const float*>(data)[row]); break;
+    case 2:
+      o.put('"');
+      put_datetime(o, static_cast<const int64_t*>(data)[row]);
+      o.put('"');
+      break;
+    case 4: put_i64(o, static_cast<const int64_t*>(data)[row]); break;
+    default: {
+      const uint8_t* t = static_cast<const uint8_t*>(data) + row * (uint64_t)width;
+      o.put('"');
+      for (int32_t i = 0; i < width && t[i]; ++i) o.put(t[i]);
+      o.put('"');
+      break;
+    }
+  }
+}
+
+// Output that only counts bytes.
+struct CountOut {
+  uint32_t n = 0;
+  YQ_CSV_HD void put(uint32_t) { ++n; }
+  YQ_CSV_HD void put_at(uint32_t, uint32_t) {}
+  YQ_CSV_HD void skip(uint32_t k) { n += k; }
+};
+
+// Output into a byte buffer.
+struct BufOut {
+  uint8_t* p;
+  YQ_CSV_HD void put(uint32_t c) { *p++ = (uint8_t)c; }
+  YQ_CSV_HD void put_at(uint32_t k, uint32_t c) { p[k] = (uint8_t)c; }
+  YQ_CSV_HD void skip(uint32_t k) { p += k; }
+};
+
 }  // namespace csv
 }  // namespace yq

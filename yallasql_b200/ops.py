@@ -661,3 +661,28 @@ def read_csv(data: bytes, project: list[str] | None = None, text_width: int = 25
     text = host.to(device, non_blocking=False)
     batch = csv_scan(text, [c.type for c in schema], fields, text_width, stream)
     return [schema[f] for f in fields], batch
+
+
+def csv_format(batch: DeviceBatch, stream=None) -> torch.Tensor:
+    """The rows of a device batch as CSV text on the device (uint8 tensor),
+    formatted as the reference's CsvWriter::batchToCsv formats them
+    (include/engine/operators/csv_writer.hpp:24-76), without the header line."""
+    L = lib()
+    s = _stream(stream)
+    cols, keep = batch.c()
+    n = C.c_uint64(0)
+    st = L.yq_csv_format(C.byref(cols), None, 0, C.byref(n), None, 0, s)
+    if st not in (A.OK, A.ERR_CAPACITY):
+        _check(st, "yq_csv_format")
+    out = torch.empty(max(int(n.value), 1), dtype=torch.uint8, device="cuda")
+    if n.value:
+        _check(L.yq_csv_format(C.byref(cols), out.data_ptr(), int(n.value), C.byref(n), None, 0, s), "yq_csv_format")
+    del keep
+    return out[: int(n.value)]
+
+
+def write_csv(names: list[str], batch: DeviceBatch, stream=None) -> bytes:
+    """A whole CSV file as the reference writes it: the header line (column
+    names joined by ',') and the formatted rows, copied to the host."""
+    text = csv_format(batch, stream)
+    return (",".join(names) + "\n").encode() + bytes(text.cpu().numpy().tobytes())

@@ -4,7 +4,7 @@
     python -m yallasql_b200.profile_cases join     # 30M-row fact table joined to the 2,556-row date table + SUM
     python -m yallasql_b200.profile_cases order    # 16M rows (key f32, id, 16-byte txt, date), 116,480-row runs
     python -m yallasql_b200.profile_cases cross    # 20K x 20K cross product with < (198M output pairs)
-    python -m yallasql_b200.profile_cases csv      # 4M-row sales table as CSV text (~205 MB): index + parse
+    python -m yallasql_b200.profile_cases csv      # 4M-row sales table as CSV text (~205 MB): index + parse + write
 
 An optional second argument sets the row count (rows per side for cross).
 
@@ -80,7 +80,8 @@ def cross_case(rows: int = 20_000) -> None:
 def csv_case(rows: int = 4_000_000) -> None:
     _, body = datagen.sales_csv(rows, seed=0)
     text = torch.from_numpy(body).cuda()
-    ops.csv_scan(text, [A.INT32, A.FLOAT32, A.INT32, A.INT32, A.TEXT, A.DATETIME], text_width=16)
+    batch = ops.csv_scan(text, [A.INT32, A.FLOAT32, A.INT32, A.INT32, A.TEXT, A.DATETIME], text_width=16)
+    ops.csv_format(batch)  # and back to text (the writer's two kernels)
     torch.cuda.synchronize()
 
 
