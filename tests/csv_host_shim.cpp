@@ -111,7 +111,22 @@ int64_t hs_record_starts(const uint8_t* text, uint64_t n, uint32_t* starts, uint
   return (int64_t)a.size();
 }
 
-// The device scan's semantics on the host (the same walk and conversions).
+// The device scan on the host: the same record split and the same
+// per-record routine (convert_record) as k_csv_parse.
+struct HostEmit {
+  void** data;
+  unsigned char** nulls;
+  const int* width;
+  uint64_t row;
+  void i32(int f, int32_t x, bool n) { static_cast<int32_t*>(data[f])[row] = x; nulls[f][row] = n; }
+  void f32(int f, float x, bool n) { static_cast<float*>(data[f])[row] = x; nulls[f][row] = n; }
+  void i64(int f, int64_t x, bool n) { static_cast<int64_t*>(data[f])[row] = x; nulls[f][row] = n; }
+  void word(int f, uint32_t k, uint32_t w) {
+    std::memcpy(static_cast<char*>(data[f]) + row * (uint64_t)width[f] + 4 * k, &w, 4);
+  }
+  void null(int f, bool n) { nulls[f][row] = n; }
+};
+
 int64_t hs_csv_scan(const uint8_t* text, uint64_t n, int nfields, const int* field_type, const int* field_width,
                     void** out_data, unsigned char** out_nulls, uint64_t capacity, uint64_t* bad,
                     int64_t* first_bad_row, int* first_bad_field, int* first_bad_kind) {
@@ -122,50 +137,36 @@ int64_t hs_csv_scan(const uint8_t* text, uint64_t n, int nfields, const int* fie
   *first_bad_row = -1;
   *first_bad_field = -1;
   *first_bad_kind = 0;
+  // records convert into scratch rows (like the kernel, which writes every
+  // record's row and drops the short/long ones afterwards)
+  std::vector<std::vector<uint8_t>> vals(nfields), nul(nfields);
+  std::vector<void*> vp(nfields);
+  std::vector<unsigned char*> np(nfields);
+  std::vector<int> width(nfields);
+  for (int f = 0; f < nfields; ++f) {
+    const int ty = field_type[f];
+    width[f] = ty == 3 ? field_width[f] : ty == 2 ? 8 : 4;
+    vals[f].assign((size_t)(nrec + 1) * width[f], 0xee);
+    nul[f].assign((size_t)nrec + 1, 7);
+    vp[f] = vals[f].data();
+    np[f] = nul[f].data();
+  }
+  auto desc = [&](int f) { return FieldOut{field_type[f] < 0 ? -1 : 0, field_type[f], field_width[f]}; };
   uint64_t rows = 0;
-  std::vector<std::vector<uint8_t>> tmp(nfields);
   for (int64_t r = 0; r < nrec; ++r) {
     const uint64_t st = starts[r], en = r + 1 < nrec ? starts[r + 1] : n;
+    HostEmit emit{vp.data(), np.data(), width.data(), (uint64_t)r};
+    uint32_t b = 0, first = ~0u;
+    if (!convert_record(text + st, (uint32_t)(en - st), nfields, desc, emit, &b, &first)) continue;
     if (rows >= capacity) return -1;
-    struct Cell { int type, width; int kind; } cells[64];
-    int64_t vals[64];
-    unsigned char nul[64];
-    std::vector<uint32_t> text_words[64];
-    auto sink = [&](uint32_t f, View v, bool escapes) {
-      if ((int)f >= nfields || field_type[f] < 0) return;
-      const int ty = field_type[f];
-      cells[f].kind = 0;
-      nul[f] = v.len == 0;
-      if (ty == 0) {
-        int32_t x = INT_MIN;
-        if (v.len) cells[f].kind = parse_int32(v, &x);
-        vals[f] = cells[f].kind ? 0 : x;
-      } else if (ty == 1) {
-        float x = FLT_MIN;
-        if (v.len) cells[f].kind = parse_float32(v, &x);
-        vals[f] = cells[f].kind ? 0 : float_bits(x);
-      } else if (ty == 2) {
-        vals[f] = v.len ? parse_datetime(v) : 0;
-      } else {
-        text_words[f].assign(field_width[f] / 4, 0xdeadbeefu);
-        auto store = [&](uint32_t k, uint32_t w) { text_words[f][k] = w; };
-        copy_text(v, escapes, (uint32_t)field_width[f], store);
-      }
-    };
-    uint32_t nf = walk_record(text + st, (uint32_t)(en - st), sink);
-    if ((int)nf != nfields) continue;
     for (int f = 0; f < nfields; ++f) {
-      const int ty = field_type[f];
-      if (ty < 0) continue;
-      out_nulls[f][rows] = nul[f];
-      if (ty == 0) static_cast<int32_t*>(out_data[f])[rows] = (int32_t)vals[f];
-      else if (ty == 1) static_cast<uint32_t*>(out_data[f])[rows] = (uint32_t)vals[f];
-      else if (ty == 2) static_cast<int64_t*>(out_data[f])[rows] = vals[f];
-      else std::memcpy(static_cast<char*>(out_data[f]) + rows * field_width[f], text_words[f].data(), field_width[f]);
-      if (ty <= 1 && cells[f].kind) {
-        if (*bad == 0) { *first_bad_row = (int64_t)rows; *first_bad_field = f; *first_bad_kind = cells[f].kind; }
-        ++*bad;
-      }
+      if (field_type[f] < 0) continue;
+      std::memcpy(static_cast<char*>(out_data[f]) + rows * width[f], vals[f].data() + r * width[f], width[f]);
+      out_nulls[f][rows] = nul[f][r];
+    }
+    if (b) {
+      if (*bad == 0) { *first_bad_row = (int64_t)rows; *first_bad_field = (int)(first >> 2); *first_bad_kind = (int)(first & 3); }
+      *bad += b;
     }
     ++rows;
   }

@@ -276,40 +276,40 @@ struct ParseParams {
   FieldDesc f[YQ_CSV_MAX_FIELDS];
 };
 
-// Converts one field into row `row` of its output column; returns CONV_*.
-__device__ __forceinline__ int32_t convert_cell(const FieldDesc& fd, uint32_t row, View v, bool escapes) {
-  const bool empty = v.len == 0;
-  fd.nulls[row] = empty ? 1 : 0;
-  int32_t st = CONV_OK;
-  switch (fd.type) {
-    case YQ_INT32: {
-      int32_t x = INT32_MIN;
-      if (!empty) st = parse_int32(v, &x);
-      static_cast<int32_t*>(fd.data)[row] = st == CONV_OK ? x : 0;
-      break;
-    }
-    case YQ_FLOAT32: {
-      float x = bits_float(0x00800000u);  // FLT_MIN, the reference's NULL sentinel
-      if (!empty) st = parse_float32(v, &x);
-      static_cast<float*>(fd.data)[row] = st == CONV_OK ? x : 0.0f;
-      break;
-    }
-    case YQ_DATETIME:
-      static_cast<long long*>(fd.data)[row] = empty ? 0 : parse_datetime(v);
-      break;
-    default: {  // YQ_TEXT
-      uint32_t* slot = reinterpret_cast<uint32_t*>(static_cast<char*>(fd.data) + (size_t)row * fd.width);
-      auto store = [slot](uint32_t k, uint32_t w) { slot[k] = w; };
-      copy_text(v, escapes, (uint32_t)fd.width, store);
-      break;
-    }
+// Output of one record's cells into row `row` of the projected columns.
+struct DevEmit {
+  const ParseParams* P;
+  uint32_t row;
+  __device__ __forceinline__ void i32(int f, int32_t x, bool null) {
+    static_cast<int32_t*>(P->f[f].data)[row] = x;
+    P->f[f].nulls[row] = null;
   }
-  return st;
-}
+  __device__ __forceinline__ void f32(int f, float x, bool null) {
+    static_cast<float*>(P->f[f].data)[row] = x;
+    P->f[f].nulls[row] = null;
+  }
+  __device__ __forceinline__ void i64(int f, int64_t x, bool null) {
+    static_cast<long long*>(P->f[f].data)[row] = x;
+    P->f[f].nulls[row] = null;
+  }
+  __device__ __forceinline__ void word(int f, uint32_t k, uint32_t w) {
+    reinterpret_cast<uint32_t*>(static_cast<char*>(P->f[f].data) + (size_t)row * P->f[f].width)[k] = w;
+  }
+  __device__ __forceinline__ void null(int f, bool null) { P->f[f].nulls[row] = null; }
+};
 
-// One thread per record, fields in lockstep: every lane of a warp walks to the
-// end of field f of its own record and then converts it with the same
-// field type, so the conversions run converged.
+struct DevDesc {
+  const ParseParams* P;
+  __device__ __forceinline__ FieldOut operator()(int f) const {
+    const FieldDesc& d = P->f[f];
+    return FieldOut{d.data ? 0 : -1, d.type, d.width};
+  }
+};
+
+// One thread per record, fields in lockstep: every lane of a warp takes field
+// f of its own record at the same time with the same field type, so the
+// conversions run converged (convert_record: typed one-pass fast paths, the
+// exact general path for every other form).
 __global__ void __launch_bounds__(kParseThreads) k_csv_parse(const __grid_constant__ ParseParams P) {
   extern __shared__ __align__(16) uint8_t s_span[];
   const uint32_t r0 = blockIdx.x * kParseThreads;
@@ -334,31 +334,16 @@ __global__ void __launch_bounds__(kParseThreads) k_csv_parse(const __grid_consta
   if (r >= rend) return;
   const uint64_t st = P.starts[r];
   const uint64_t en = r + 1 < P.nrec ? P.starts[r + 1] : P.nbytes;
-  FieldCursor cur;
-  cur.init(staged ? s_span + (st - a0) : P.data + st, (uint32_t)(en - st));
-  uint32_t bad = 0;
-  unsigned long long first_bad = ~0ull;
-  bool ok = true;
-  for (int f = 0; f < P.nfields; ++f) {
-    View v;
-    bool esc;
-    if (!cur.next(&v, &esc)) { ok = false; break; }  // fewer fields than the header
-    const FieldDesc& fd = P.f[f];
-    if (!fd.data) continue;
-    const int32_t cs = convert_cell(fd, r, v, esc);
-    if (cs != CONV_OK) {
-      ++bad;
-      const unsigned long long key = (unsigned long long)r << 12 | (unsigned long long)f << 2 | (unsigned)cs;
-      if (key < first_bad) first_bad = key;
-    }
-  }
-  if (cur.more()) ok = false;  // more fields than the header
+  DevEmit emit{&P, r};
+  uint32_t bad = 0, first = ~0u;
+  const bool ok = convert_record(staged ? s_span + (st - a0) : P.data + st, (uint32_t)(en - st), P.nfields,
+                                 DevDesc{&P}, emit, &bad, &first);
   P.valid[r] = ok ? 1 : 0;
   if (!ok) {
     atomicAdd(&P.counters[0], 1ull);
   } else if (bad) {
     atomicAdd(&P.counters[1], (unsigned long long)bad);
-    atomicMin(&P.counters[2], first_bad);
+    atomicMin(&P.counters[2], (unsigned long long)r << 12 | first);
   }
 }
 

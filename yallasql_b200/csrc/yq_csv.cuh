@@ -232,6 +232,7 @@ YQ_CSV_HD bool is_digit(uint32_t c) { return c - '0' < 10u; }
 YQ_CSV_HD uint32_t lower(uint32_t c) { return (c - 'A' < 26u) ? c + 32 : c; }
 
 enum : int32_t { CONV_OK = 0, CONV_INVALID = 1, CONV_RANGE = 2 };
+constexpr int32_t INT32_MIN_ = -2147483647 - 1;
 
 // ------------------------------------------------------------------ stoi
 // std::stoi(s) = strtol(s, &end, 10) on a 64-bit long: leading white space,
@@ -785,6 +786,208 @@ struct FieldCursor {
   }
   YQ_CSV_HD bool more() const { return !done; }
 };
+
+// ------------------------------------------------------ typed fast paths
+// One pass over an unquoted field in its common written form: find its end
+// and convert it together. Each returns false, with the cursor unmoved, when
+// the field is in any other form (quoted, empty, signs or spaces where the
+// general conversion decides, too many digits, a float needing exact
+// rounding, a date outside the canonical layout...); the caller then takes
+// the general path (next() + parse_*), which is exact for every input.
+
+// Consumes the terminator at rec[j] (',', newline or the end), if it is one.
+YQ_CSV_HD bool FieldCursor_end(FieldCursor& c, uint32_t j) {
+  if (j >= c.len) { c.i = j; c.done = true; return true; }
+  const uint32_t t = c.rec[j];
+  if (t == ',') { c.i = j + 1; return true; }
+  if (t == '\n' || t == '\r') { c.i = j; c.done = true; return true; }
+  return false;
+}
+
+// [+-]digits (at most 9) then a terminator.
+YQ_CSV_HD bool fast_int32(FieldCursor& c, int32_t* out) {
+  if (c.done) return false;
+  uint32_t j = c.i;
+  bool neg = false;
+  if (j < c.len && (c.rec[j] == '-' || c.rec[j] == '+')) { neg = c.rec[j] == '-'; ++j; }
+  uint32_t v = 0, nd = 0;
+  while (j < c.len && (uint32_t)c.rec[j] - '0' < 10u && nd < 10) { v = v * 10 + (c.rec[j] - '0'); ++j; ++nd; }
+  if (nd == 0 || nd > 9) return false;
+  if (!FieldCursor_end(c, j)) return false;
+  *out = neg ? (int32_t)(0u - v) : (int32_t)v;
+  return true;
+}
+
+// [+-]digits[.digits] (at most 19 significant digits) then a terminator, when
+// one double operation on exact operands rounds it exactly (the parse_float32
+// fast path's conditions).
+YQ_CSV_HD bool fast_float32(FieldCursor& c, float* out) {
+  if (c.done) return false;
+  uint32_t j = c.i;
+  uint32_t sign = 0;
+  if (j < c.len && (c.rec[j] == '-' || c.rec[j] == '+')) { sign = c.rec[j] == '-' ? 0x80000000u : 0u; ++j; }
+  uint64_t w = 0;
+  int nd = 0, frac = 0, digits = 0;
+  bool dot = false;
+  for (; j < c.len; ++j) {
+    const uint32_t ch = c.rec[j];
+    if (ch - '0' < 10u) {
+      ++digits;
+      if (w == 0 && ch == '0') { if (dot) ++frac; continue; }
+      if (nd == 19) return false;
+      w = w * 10 + (ch - '0');
+      ++nd;
+      if (dot) ++frac;
+    } else if (ch == '.' && !dot) {
+      dot = true;
+    } else {
+      break;
+    }
+  }
+  if (digits == 0) return false;
+  if (j < c.len && (c.rec[j] == 'e' || c.rec[j] == 'E')) return false;
+  const uint32_t j_end = j;
+  if (w == 0) {
+    if (!FieldCursor_end(c, j_end)) return false;
+    *out = bits_float(sign);
+    return true;
+  }
+  const int q = -frac;                     // value = w * 10^q
+  const int lead = nd - 1 + q;             // decimal position of the leading digit
+  if (w >= (1ull << 53) || q < -22 || lead <= -36 || lead >= 37) return false;
+  const double dv = (double)w / pow10_exact(-q);
+  union { double d; uint64_t u; } x;
+  x.d = dv;
+  if ((uint32_t)(x.u & ((1ull << 29) - 1)) == (1u << 28)) return false;  // a float midpoint
+  if (!FieldCursor_end(c, j_end)) return false;
+  *out = bits_float(sign | float_bits((float)dv));
+  return true;
+}
+
+// "YYYY-MM-DD HH:MM:SS" exactly, each part a value strptime's field rule
+// accepts with that many digits, then a terminator.
+YQ_CSV_HD bool fast_datetime(FieldCursor& c, int64_t* out) {
+  if (c.done || c.i + 19 > c.len) return false;
+  const uint8_t* p = c.rec + c.i;
+  const uint8_t sep[6] = {'-', '-', ' ', ':', ':', 0};
+  const int at[5] = {4, 7, 10, 13, 16};
+  for (int k = 0; k < 5; ++k)
+    if (p[at[k]] != sep[k]) return false;
+  const int dpos[14] = {0, 1, 2, 3, 5, 6, 8, 9, 11, 12, 14, 15, 17, 18};
+  for (int k = 0; k < 14; ++k)
+    if ((uint32_t)p[dpos[k]] - '0' >= 10u) return false;
+  const int Y = (p[0] - '0') * 1000 + (p[1] - '0') * 100 + (p[2] - '0') * 10 + (p[3] - '0');
+  const int M0 = p[5] - '0', D0 = p[8] - '0', h0 = p[11] - '0', m0 = p[14] - '0', s0 = p[17] - '0';
+  // a two-digit field is read as two digits only when its first digit * 10 <= the maximum
+  if (M0 > 1 || D0 > 3 || h0 > 2 || m0 > 5 || s0 > 6) return false;
+  const int M = M0 * 10 + (p[6] - '0'), D = D0 * 10 + (p[9] - '0'), h = h0 * 10 + (p[12] - '0');
+  const int mi = m0 * 10 + (p[15] - '0'), se = s0 * 10 + (p[18] - '0');
+  if (M < 1 || M > 12 || D < 1 || D > 31 || h > 23 || mi > 59 || se > 61) return false;
+  if (!FieldCursor_end(c, c.i + 19)) return false;
+  *out = days_from_civil(Y, M, D) * 86400 + h * 3600 + mi * 60 + se;
+  return true;
+}
+
+// An unquoted text field copied while it is scanned (String::set: up to the
+// first NUL, at most width-1 bytes, NUL padded).
+template <class Store>
+YQ_CSV_HD bool fast_text(FieldCursor& c, uint32_t width, Store& store) {
+  if (c.done || (c.i < c.len && c.rec[c.i] == '"')) return false;
+  uint32_t j = c.i, o = 0, word = 0;
+  bool stop = false;
+  for (; j < c.len; ++j) {
+    const uint32_t ch = c.rec[j];
+    if (ch == ',' || ch == '\n' || ch == '\r') break;
+    if (stop) continue;
+    if (ch == 0 || o >= width - 1) { stop = true; continue; }
+    word |= ch << (8 * (o & 3));
+    ++o;
+    if ((o & 3) == 0) { store(o / 4 - 1, word); word = 0; }
+  }
+  for (; o < width; ++o)
+    if ((o & 3) == 3) { store(o / 4, word); word = 0; }
+  FieldCursor_end(c, j);
+  return true;
+}
+
+// Every field of one record into its output through `emit` (fields in
+// order; types uniform across a warp). desc(f) gives {projected, type,
+// width}. Returns the field count check: true when the record has exactly
+// nfields fields. Conversion failures go to *bad / *first_bad (key: field << 2
+// | kind, the smallest field first).
+template <class Desc, class Emit>
+YQ_CSV_HD bool convert_record(const uint8_t* rec, uint32_t len, int nfields, const Desc& desc, Emit& emit,
+                              uint32_t* bad, uint32_t* first_bad) {
+  FieldCursor cur;
+  cur.init(rec, len);
+  for (int f = 0; f < nfields; ++f) {
+    const FieldOut d = desc(f);
+    View v;
+    bool esc;
+    if (d.column < 0) {
+      if (!cur.next(&v, &esc)) return false;
+      continue;
+    }
+    switch (d.type) {
+      case 0: {
+        int32_t x;
+        if (fast_int32(cur, &x)) { emit.i32(f, x, false); continue; }
+        break;
+      }
+      case 1: {
+        float x;
+        if (fast_float32(cur, &x)) { emit.f32(f, x, false); continue; }
+        break;
+      }
+      case 2: {
+        int64_t x;
+        if (fast_datetime(cur, &x)) { emit.i64(f, x, false); continue; }
+        break;
+      }
+      default: {
+        auto store = [&emit, f](uint32_t k, uint32_t w) { emit.word(f, k, w); };
+        if (cur.i < cur.len && cur.rec[cur.i] != ',' && cur.rec[cur.i] != '\n' && cur.rec[cur.i] != '\r' &&
+            fast_text(cur, (uint32_t)d.width, store)) {
+          emit.null(f, false);
+          continue;
+        }
+        break;
+      }
+    }
+    if (!cur.next(&v, &esc)) return false;  // fewer fields than the header
+    const bool empty = v.len == 0;
+    int32_t st = CONV_OK;
+    switch (d.type) {
+      case 0: {
+        int32_t x = INT32_MIN_;
+        if (!empty) st = parse_int32(v, &x);
+        emit.i32(f, st == CONV_OK ? x : 0, empty);
+        break;
+      }
+      case 1: {
+        float x = bits_float(0x00800000u);  // FLT_MIN, the reference's NULL sentinel
+        if (!empty) st = parse_float32(v, &x);
+        emit.f32(f, st == CONV_OK ? x : 0.0f, empty);
+        break;
+      }
+      case 2:
+        emit.i64(f, empty ? 0 : parse_datetime(v), empty);
+        break;
+      default: {
+        auto store = [&emit, f](uint32_t k, uint32_t w) { emit.word(f, k, w); };
+        copy_text(v, esc, (uint32_t)d.width, store);
+        emit.null(f, empty);
+        break;
+      }
+    }
+    if (st != CONV_OK) {
+      ++*bad;
+      const uint32_t key = (uint32_t)f << 2 | (uint32_t)st;
+      if (key < *first_bad) *first_bad = key;
+    }
+  }
+  return !cur.more();  // more fields than the header when the record goes on
+}
 
 // Calls sink(field_index, content_view, has_escapes) for every field of the
 // record; returns the field count.
