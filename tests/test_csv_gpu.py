@@ -68,6 +68,19 @@ def test_random_tables(cuda):
         same(gpu_scan(body, types), oracle.csv_scan(body, types))
 
 
+def test_many_tiles_with_quotes(cuda):
+    """Quote-heavy text of many 16 KiB tiles: record index look-back across
+    tiles that start inside quoted fields, escaped quotes and CR/LF runs."""
+    rng = np.random.default_rng(24)
+    done = 0
+    while done < 3:
+        types, header, body = csv_cases.random_csv(rng, max_rows=12000)
+        if len(body) < 200_000:
+            continue
+        same(gpu_scan(body, types), oracle.csv_scan(body, types))
+        done += 1
+
+
 def test_unaligned_text_and_wide_slots(cuda):
     rng = np.random.default_rng(22)
     for off in (1, 3, 7, 13):
