@@ -52,6 +52,16 @@ void yq_plan_destroy(yq_plan* plan);
 /* Node builders return the new node id (>= 0) or -yq_status. */
 int yq_plan_scan(yq_plan* plan, const yq_host_column* cols, int32_t ncols, uint64_t rows,
                  uint32_t batch_rows /* 0 = 4 MB batches */);
+/* A table read from CSV text, GetOperator's place in the tree
+ * (src/engine/operators/get_operator.cpp:17-109): `text` (host, nbytes) is
+ * the file after its header line; field_types[f] is CSV field f's type (the
+ * header-tag rule of Table::inferDBSchema); `project` lists the fields to
+ * keep, in output order; text columns get `text_width`-byte slots. The text
+ * goes to the device once and is converted batch by batch (yq_csv_index,
+ * yq_csv_parse). Must stay valid until the plan executes. */
+int yq_plan_scan_csv(yq_plan* plan, const uint8_t* text, uint64_t nbytes, const int32_t* field_types,
+                     int32_t nfields, const int32_t* project, int32_t nproj, int32_t text_width,
+                     uint32_t batch_rows /* 0 = 4 MB batches */);
 int yq_plan_filter(yq_plan* plan, int32_t child, const yq_program* predicate,
                    const yq_constants* constants);
 int yq_plan_project(yq_plan* plan, int32_t child, const yq_projection* proj, int32_t nproj,

@@ -231,3 +231,53 @@ def test_scan_then_write_round_trip(cuda):
                              1_000_000)
     assert got == want
     assert got.count(b"\n") == 1_000_000
+
+
+# ------------------------------------------------- in the operator tree
+def test_plan_csv_scan_filter_aggregate(cuda):
+    """GetOperator's place in the C++ operator tree: CSV text -> device scan
+    batch by batch -> filter -> aggregate (the benchmark query), against the
+    oracle's parse and evaluation."""
+    from yallasql_b200.plan import Plan
+    from test_filter_gpu import sales_query_exprs
+    from helpers import rel_close
+    header, body = datagen.sales_csv(300_000, seed=4)
+    data = header + body.tobytes()
+    pred, aggs = sales_query_exprs()
+    for batch_rows in (0, 50_000):
+        p = Plan()
+        root = p.aggregate(p.filter(p.scan_csv(data, ["price", "qty", "discount", "category"], text_width=16,
+                                               batch_rows=batch_rows), pred), aggs)
+        res = p.execute(root)
+        got = [v[0] for v, n in res]
+        o = oracle.csv_scan(body.tobytes(), [-1, 1, 0, 0, 3, -1], width=16)
+        cols = {0: (o["cols"][1][0], None, A.FLOAT32), 1: (o["cols"][2][0], None, A.INT32),
+                2: (o["cols"][3][0], None, A.INT32), 3: (o["cols"][4][0], None, A.TEXT)}
+        want = expr_eval.aggregate(pred, aggs, cols, o["rows"])
+        assert int(got[1]) == want[1]
+        assert float(got[2]) == want[2] and float(got[3]) == want[3]
+        assert rel_close(float(got[0]), want[0], 1e-6)
+
+
+def test_plan_csv_scan_batches_and_errors(cuda):
+    """Batches of 1,000 records over a file with ragged rows: the result
+    equals the oracle's parse; a cell stoi rejects fails the plan."""
+    from yallasql_b200.plan import Plan
+    rng = np.random.default_rng(25)
+    lines = []
+    for i in range(5000):
+        if i % 97 == 0:
+            lines.append(f"{i},only-two")
+        else:
+            lines.append(f'{i},"t{i},x",{rng.uniform(-50, 50):.3f},2020-0{1 + i % 9}-1{i % 10} 0{i % 10}:00:00')
+    body = ("\n".join(lines) + "\n").encode()
+    data = b"id (N),t (T),v (N),d (D)\n" + body
+    p = Plan()
+    res = p.execute(p.scan_csv(data, ["d", "id", "v", "t"], text_width=16, batch_rows=1000))
+    o = oracle.csv_scan(body, [0, 3, 1, 2], width=16)
+    for (gv, gn), (ov, on) in zip(res, [o["cols"][3], o["cols"][0], o["cols"][2], o["cols"][1]]):
+        assert gv.tobytes() == ov.tobytes() and np.array_equal(gn, on)
+    bad = b"a (N)\n1\n2\nx\n"
+    p2 = Plan()
+    with pytest.raises(A.YQError):
+        p2.execute(p2.scan_csv(bad))

@@ -266,6 +266,100 @@ class ScanOperator final : public Operator {
   uint64_t issued_ = 0, taken_ = 0;
 };
 
+// --------------------------------------------------------- CsvScanOperator
+// GetOperator (src/engine/operators/get_operator.cpp:17-109) over CSV text:
+// the file's body (header line removed) goes to the device once, one record
+// index splits it (yq_csv_index), and each next() converts the next batch of
+// records into a Batch (yq_csv_parse) instead of the reference's host
+// csv-parser loop and per-column synchronous copies. Batch rows follow
+// calculateOptimalBatchSize over the projected columns (include/config.hpp:28-36).
+// A cell that std::stoi / std::stof would reject raises YQ_ERR_INVALID_ARG
+// (the reference's process exits there).
+class CsvScanOperator final : public Operator {
+ public:
+  CsvScanOperator(const uint8_t* text, uint64_t nbytes, const int32_t* types, int nfields, const int32_t* project,
+                  int nproj, int32_t text_width, uint32_t batch_rows)
+      : host_(text), nbytes_(nbytes), types_(types, types + nfields), project_(project, project + nproj) {
+    uint64_t row_bytes = 0;
+    field_col_.assign(nfields, -1);
+    for (int i = 0; i < nproj; ++i) {
+      const int f = project_[i];
+      if (f < 0 || f >= nfields || field_col_[f] >= 0) throw Error(YQ_ERR_INVALID_ARG, "csv projection");
+      field_col_[f] = i;
+      const int32_t w = width_of(types_[f], text_width);
+      columns.push_back(std::make_shared<Column>(Column{types_[f], w}));
+      row_bytes += w;
+    }
+    if (batch_rows) {
+      batch_rows_ = batch_rows;
+    } else {
+      const uint64_t per = (4ull << 20) / std::max<uint64_t>(1, row_bytes);
+      batch_rows_ = std::max<uint64_t>(256, per / 256 * 256);
+    }
+  }
+  ~CsvScanOperator() override {
+    if (text_) cudaFree(text_);
+    if (starts_) cudaFree(starts_);
+  }
+  const char* kind() const override { return "csv_scan"; }
+  void init() override {
+    if (isInitialized_) return;
+    if (nbytes_) {
+      check_cuda(cudaMalloc(&text_, nbytes_), "csv text");
+      check_cuda(cudaMemcpyAsync(text_, host_, nbytes_, cudaMemcpyHostToDevice, ctx_->compute), "csv H2D");
+      ctx_->stats.h2d_bytes += nbytes_;
+      uint64_t n = 0;
+      int st = yq_csv_index(text_, nbytes_, nullptr, 0, &n, nullptr, 0, ctx_->compute);
+      if (st != YQ_OK && st != YQ_ERR_CAPACITY) check(st, "yq_csv_index");
+      records_ = n;
+      check_cuda(cudaMalloc(&starts_, std::max<uint64_t>(1, n) * sizeof(uint32_t)), "csv record starts");
+      check(yq_csv_index(text_, nbytes_, starts_, n, &n, nullptr, 0, ctx_->compute), "yq_csv_index");
+    }
+    isInitialized_ = true;
+  }
+  BatchID next(CacheManager& cache) override {
+    if (!isInitialized_) init();
+    if (isFinished || pos_ >= records_) {
+      isFinished = true;
+      return 0;
+    }
+    const uint64_t n = std::min<uint64_t>(batch_rows_, records_ - pos_);
+    // records [pos_, pos_+n) end where the next one starts (or at the end of the text)
+    uint64_t end = nbytes_;
+    if (pos_ + n < records_) {
+      uint32_t e = 0;
+      check_cuda(cudaMemcpyAsync(&e, starts_ + pos_ + n, sizeof(e), cudaMemcpyDeviceToHost, ctx_->compute), "csv end");
+      check_cuda(cudaStreamSynchronize(ctx_->compute), "csv end");
+      end = e;
+    }
+    auto b = std::make_unique<Batch>(columns, n, ctx_->compute, true);
+    std::vector<yq_column> out(columns.size());
+    for (size_t c = 0; c < columns.size(); ++c) out[c] = b->column(c);
+    uint32_t rows = 0;
+    yq_csv_error err{};
+    const int st = yq_csv_parse(text_, end, starts_ + pos_, (uint32_t)n, field_col_.data(), (int32_t)types_.size(),
+                                out.data(), (int32_t)out.size(), &rows, &err, nullptr, 0, ctx_->compute);
+    if (st != YQ_OK) {
+      if (st == YQ_ERR_INVALID_ARG && err.bad_cells)
+        throw Error(st, "csv scan: a field std::stoi/std::stof rejects, batch row " + std::to_string(err.first_row) +
+                            ", field " + std::to_string(err.first_field));
+      check(st, "yq_csv_parse");
+    }
+    b->rows = rows;  // rows with another field count are dropped (csv-parser IGNORE_ROW)
+    pos_ += n;
+    ++ctx_->stats.batches;
+    return cache.putBatch(std::move(b));
+  }
+
+ private:
+  const uint8_t* host_;
+  uint64_t nbytes_;
+  std::vector<int32_t> types_, project_, field_col_;
+  uint64_t batch_rows_ = 0, records_ = 0, pos_ = 0;
+  uint8_t* text_ = nullptr;
+  uint32_t* starts_ = nullptr;
+};
+
 static bool has_nulls(const Batch& b) {
   for (auto* n : b.nulls)
     if (n) return true;
@@ -713,6 +807,19 @@ void yq_plan_destroy(yq_plan* p) {
 int yq_plan_scan(yq_plan* p, const yq_host_column* cols, int32_t ncols, uint64_t rows, uint32_t batch_rows) {
   if (!p || !cols || ncols <= 0 || ncols > YQ_MAX_BATCH_COLUMNS) return -YQ_ERR_INVALID_ARG;
   return guarded([&] { return add(p, std::make_unique<ScanOperator>(cols, ncols, rows, batch_rows)); });
+}
+
+int yq_plan_scan_csv(yq_plan* p, const uint8_t* text, uint64_t nbytes, const int32_t* field_types,
+                     int32_t nfields, const int32_t* project, int32_t nproj, int32_t text_width,
+                     uint32_t batch_rows) {
+  if (!p || (nbytes && !text) || !field_types || nfields <= 0 || nfields > YQ_CSV_MAX_FIELDS || !project ||
+      nproj <= 0 || nproj > YQ_MAX_BATCH_COLUMNS || text_width < 4 || text_width > YQ_MAX_TEXT_WIDTH ||
+      text_width % 4 || nbytes >= (1ull << 32))
+    return -YQ_ERR_INVALID_ARG;
+  return guarded([&] {
+    return add(p, std::make_unique<CsvScanOperator>(text, nbytes, field_types, nfields, project, nproj, text_width,
+                                                    batch_rows));
+  });
 }
 
 int yq_plan_filter(yq_plan* p, int32_t child, const yq_program* pred, const yq_constants* k) {

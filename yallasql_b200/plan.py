@@ -35,6 +35,8 @@ PROTOTYPES = {
     "yq_plan_create": (C.c_void_p, [C.c_uint64]),
     "yq_plan_destroy": (None, [C.c_void_p]),
     "yq_plan_scan": (C.c_int, [C.c_void_p, C.POINTER(HostColumn), C.c_int32, C.c_uint64, C.c_uint32]),
+    "yq_plan_scan_csv": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_int32), C.c_int32,
+                                   C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.c_uint32]),
     "yq_plan_filter": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(A.Program), C.POINTER(A.Constants)]),
     "yq_plan_project": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(A.Projection), C.c_int32,
                                   C.POINTER(A.Constants)]),
@@ -120,6 +122,30 @@ class Plan:
         self._keep.append(arr)
         n = _node(lib().yq_plan_scan(self.h, arr, len(cols), rows, batch_rows), "yq_plan_scan")
         self.types[n] = ts
+        return n
+
+    def scan_csv(self, data: bytes, project: list[str] | None = None, text_width: int = 256, batch_rows: int = 0):
+        """A CSV file (header line included) as the plan's table: schema from
+        the header tags on the host, the body converted on the device batch by
+        batch (GetOperator's place in the tree). Returns the node id; the
+        output columns are the projected fields in `project` order."""
+        from .ops import csv_schema
+        if data.startswith(b"\xef\xbb\xbf"):
+            data = data[3:]
+        nl = data.find(b"\n")
+        header = data[: nl if nl >= 0 else len(data)].decode("utf-8", "replace")
+        body = data[nl + 1:] if nl >= 0 else b""
+        nl2 = body.find(b"\n")
+        schema = csv_schema(header, body[: nl2 if nl2 >= 0 else len(body)].decode("utf-8", "replace"))
+        names = [c.name for c in schema]
+        fields = list(range(len(schema))) if project is None else [names.index(p) for p in project]
+        buf = np.frombuffer(body, dtype=np.uint8).copy() if body else np.zeros(1, np.uint8)
+        types = (C.c_int32 * len(schema))(*[c.type for c in schema])
+        proj = (C.c_int32 * len(fields))(*fields)
+        self._keep += [buf, types, proj]
+        n = _node(lib().yq_plan_scan_csv(self.h, buf.ctypes.data, len(body), types, len(schema), proj, len(fields),
+                                         text_width, batch_rows), "yq_plan_scan_csv")
+        self.types[n] = [schema[f].type for f in fields]
         return n
 
     def filter(self, child: int, pred: Expr):
