@@ -266,7 +266,7 @@ def test_plan_csv_scan_batches_and_errors(cuda):
     rng = np.random.default_rng(25)
     lines = []
     for i in range(5000):
-        if i % 97 == 0:
+        if i % 97 == 5:  # the first data line stays whole: the schema's types come from it
             lines.append(f"{i},only-two")
         else:
             lines.append(f'{i},"t{i},x",{rng.uniform(-50, 50):.3f},2020-0{1 + i % 9}-1{i % 10} 0{i % 10}:00:00')
