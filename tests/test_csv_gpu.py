@@ -269,12 +269,18 @@ def test_plan_csv_scan_batches_and_errors(cuda):
         if i % 97 == 5:  # the first data line stays whole: the schema's types come from it
             lines.append(f"{i},only-two")
         else:
-            lines.append(f'{i},"t{i},x",{rng.uniform(-50, 50):.3f},2020-0{1 + i % 9}-1{i % 10} 0{i % 10}:00:00')
+            # the header-tag rule splits the first data line at every ',' (quotes or not), so
+            # its text stays comma-free there and `v` is typed FLOAT from its '.'
+            t = f'"t{i},x"' if i else '"t0"'
+            lines.append(f'{i},{t},{rng.uniform(-50, 50):.3f},2020-0{1 + i % 9}-1{i % 10} 0{i % 10}:00:00')
     body = ("\n".join(lines) + "\n").encode()
-    data = b"id (N),t (T),v (N),d (D)\n" + body
+    header = "id (N),t (T),v (N),d (D)"
+    data = (header + "\n").encode() + body
+    types = [c.type for c in ops.csv_schema(header, lines[0])]
+    assert types == [A.INT32, A.TEXT, A.FLOAT32, A.DATETIME]
     p = Plan()
     res = p.execute(p.scan_csv(data, ["d", "id", "v", "t"], text_width=16, batch_rows=1000))
-    o = oracle.csv_scan(body, [0, 3, 1, 2], width=16)
+    o = oracle.csv_scan(body, types, width=16)
     for (gv, gn), (ov, on) in zip(res, [o["cols"][3], o["cols"][0], o["cols"][2], o["cols"][1]]):
         assert gv.tobytes() == ov.tobytes() and np.array_equal(gn, on)
     bad = b"a (N)\n1\n2\nx\n"
