@@ -281,6 +281,25 @@ def operator_suite(lib, peak: float) -> dict:
              lambda: lib.yq_join_project(C.byref(lbc), C.byref(rbc), conds, 1, outs_c, 2, oc, pairs, C.byref(n64),
                                          None, 0, torch.cuda.current_stream().cuda_stream),
              pairs, 5, "join_nested_loop")
+    # GROUP BY discount over the 64M-row sales table (sort + group kernels)
+    t = datagen.sales_table(64_000_000, seed=0)
+    gb = ops.DeviceBatch([dev(t["discount"], A.INT32), dev(t["price"], A.FLOAT32), dev(t["qty"], A.INT32)])
+    del t
+    gaggs = [(A.AGG_COUNT_STAR, 0), (A.AGG_SUM, 1), (A.AGG_AVG, 2), (A.AGG_MIN, 1), (A.AGG_MAX, 1)]
+    g_out = ops.group_by(gb, 0, gaggs, capacity=64)
+    gws = torch.empty(lib.yq_group_by_workspace_size(C.byref(gb.columns[0].c()), gb.rows, len(gaggs), 64),
+                      dtype=torch.uint8, device="cuda")
+    gbc, gkeep = gb.c()
+    gag = (A.GroupAgg * len(gaggs))(*[A.GroupAgg(k, c) for k, c in gaggs])
+    gout = [ops.DeviceColumn.empty(c.type, 64, nulls=True) for c in g_out.columns]
+    goc = (A.Column * len(gout))(*[c.c() for c in gout])
+    ng = C.c_uint32()
+    profiled("group_by_discount_64M",
+             lambda: A.check(lib.yq_group_by(C.byref(gbc), 0, gag, len(gaggs), goc, 64, C.byref(ng), gws.data_ptr(),
+                                             gws.numel(), torch.cuda.current_stream().cuda_stream), "yq_group_by"),
+             64_000_000, 3, "group_accumulate")
+    out["group_by_discount_64M"]["groups"] = int(ng.value)
+    del gb, gws, gkeep
     out["cross_product_lt_20Kx20K"]["output_pairs"] = pairs
     out["cross_product_lt_20Kx20K"]["output_bytes_per_s"] = pairs * 8 / (out["cross_product_lt_20Kx20K"]["ms"] / 1e3)
     out["cross_product_lt_20Kx20K"]["frac_of_measured_hbm_output"] = round(

@@ -524,6 +524,34 @@ int yq_merge_path(const void* a, const void* b, int32_t type, int32_t width,
 int yq_cross_product_col(const yq_column* col, uint32_t left_rows, uint32_t right_rows,
                          int32_t is_left, yq_column* out, void* stream);
 
+/* ---------------------------------------------------------------- GROUP BY
+ * SELECT key, agg, ... GROUP BY key. The reference plans GROUP BY but folds
+ * every row into one result (AggregateOperator ignores the groups,
+ * include/engine/operators/aggregate_operator.hpp:84-104); this follows SQL
+ * semantics: one output row per distinct key, NULL keys one group, in
+ * ascending key order with the NULL group last (-0.0 equals +0.0, NaNs form
+ * one group above +inf). Aggregates skip NULL inputs; COUNT(*) counts rows and
+ * COUNT(col) non-NULL inputs (INT64); SUM of integers is INT64 (wrapping), of
+ * floats FLOAT64 accumulated in FP64 (order of additions not fixed: within
+ * 1e-15 relative between runs); AVG is FLOAT64; MIN/MAX keep the input type
+ * (floats ordered -0.0 < +0.0, NaN above +inf). SUM/AVG/MIN/MAX over no
+ * non-NULL input is NULL. */
+typedef struct yq_group_agg {
+  int32_t kind;    /* yq_agg_kind                              */
+  int32_t column;  /* input column; ignored for YQ_AGG_COUNT_STAR */
+} yq_group_agg;
+
+size_t yq_group_by_workspace_size(const yq_column* key, uint32_t rows, int32_t nagg, uint32_t capacity);
+/* out[0]: the key column (the key's type and width); out[1 + a]: aggregate a
+ * (types above; a NULL-byte array is required except for COUNT). Every output
+ * column has room for `capacity` rows. *groups = the number of groups; the
+ * call synchronises `stream` to read it and returns YQ_ERR_CAPACITY (outputs
+ * not written) when it exceeds `capacity`. Keys: INT32, INT64, DATETIME,
+ * FLOAT32, FLOAT64, TEXT; aggregate inputs: the numeric types (DATETIME for
+ * MIN/MAX/COUNT). */
+int yq_group_by(const yq_batch* batch, int32_t key_col, const yq_group_agg* aggs, int32_t nagg, yq_column* out,
+                uint32_t capacity, uint32_t* groups, void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------- CSV scan
  * Device-side replacement of GetOperator::next's per-row loop
  * (src/engine/operators/get_operator.cpp:56-109): csv-parser's tokenizer

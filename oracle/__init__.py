@@ -268,3 +268,91 @@ def csv_format(cols: list, rows: int) -> bytes:
     buf = C.create_string_buffer(int(need) + 1)
     L.orc_csv_format(n, ty, wd, dp, npp, C.c_uint64(rows), buf, C.c_uint64(need))
     return buf.raw[: int(need)]
+
+
+# ------------------------------------------------------------------ GROUP BY
+def _ordered_f64(x: np.ndarray) -> np.ndarray:
+    """Order-preserving int64 of doubles (NaN above +inf, -0.0 below +0.0)."""
+    d = np.asarray(x, dtype=np.float64).copy()
+    u = d.view(np.uint64).copy()
+    u[np.isnan(d)] = np.uint64(0x7ff8000000000000)
+    neg = (u >> np.uint64(63)) == 1
+    u = np.where(neg, ~u, u | np.uint64(1 << 63))
+    return (u ^ np.uint64(1 << 63)).view(np.int64)
+
+
+def _unordered_f64(k: np.ndarray) -> np.ndarray:
+    u = k.view(np.uint64) ^ np.uint64(1 << 63)
+    pos = (u >> np.uint64(63)) == 1
+    u = np.where(pos, u & ~np.uint64(1 << 63), ~u)
+    return u.view(np.float64)
+
+
+def group_by(key, key_nulls, key_type, aggs):
+    """SQL GROUP BY (the device operator's semantics, numpy): groups in
+    ascending key order (stable: a group's key is its first row's), the NULL
+    group last, -0.0 equal to +0.0 and NaNs one group above +inf. aggs: list of
+    (kind, values|None, nulls|None, type) with kind 0 COUNT(*), 1 COUNT, 2 SUM,
+    3 AVG, 4 MIN, 5 MAX. Returns (key values, key nulls, [(values, nulls)])."""
+    n = len(key)
+    kn = np.zeros(n, bool) if key_nulls is None else np.asarray(key_nulls).astype(bool)
+    # NULL keys are all equal: the NULL group keeps row order
+    if key_type == 3:  # text: byte strings
+        k = np.ascontiguousarray(key)
+        sk = np.where(kn, b"", k.view(f"S{k.shape[1]}").ravel())
+        order = np.lexsort((np.arange(n), sk, kn))
+        sorted_k = sk[order]
+        eq = sorted_k[1:] == sorted_k[:-1]
+    elif key_type in (1, 5):
+        kf = np.asarray(key, dtype=np.float64)
+        canon = np.where(kf == 0, 0.0, kf)
+        nanm = np.isnan(canon)
+        sortable = np.where(kn, 0.0, np.where(nanm, np.inf, canon))
+        order = np.lexsort((np.arange(n), np.where(kn, False, nanm), sortable, kn))
+        c, nm = canon[order], nanm[order]
+        eq = (c[1:] == c[:-1]) | (nm[1:] & nm[:-1])
+    else:
+        kv = np.where(kn, 0, np.asarray(key).astype(np.int64))
+        order = np.lexsort((np.arange(n), kv, kn))
+        s = kv[order]
+        eq = s[1:] == s[:-1]
+    skn = kn[order]
+    same = eq & (skn[1:] == skn[:-1])
+    same = np.where(skn[1:] & skn[:-1], True, same)
+    head = np.concatenate([[True], ~same]) if n else np.zeros(0, bool)
+    starts = np.flatnonzero(head)
+    out_key = np.asarray(key)[order[starts]]
+    out_kn = kn[order[starts]]
+    res = []
+    for kind, vals, nulls, typ in aggs:
+        if kind == 0:
+            res.append((np.diff(np.concatenate([starts, [n]])).astype(np.int64), None))
+            continue
+        vn = np.zeros(n, bool) if nulls is None else np.asarray(nulls).astype(bool)
+        ok = ~vn[order]
+        cnt = np.add.reduceat(ok.astype(np.int64), starts) if n else np.zeros(0, np.int64)
+        if kind == 1:
+            res.append((cnt, None))
+            continue
+        v = np.asarray(vals)[order]
+        isf = typ in (1, 5)
+        if kind in (2, 3):
+            if isf:
+                s = np.add.reduceat(np.where(ok, v.astype(np.float64), 0.0), starts)
+            else:
+                s = np.add.reduceat(np.where(ok, v.astype(np.int64), 0), starts)
+            if kind == 3:
+                with np.errstate(invalid="ignore", divide="ignore"):
+                    s = s.astype(np.float64) / cnt
+            res.append((np.where(cnt > 0, s, 0), cnt == 0))
+            continue
+        enc = _ordered_f64(v) if isf else v.astype(np.int64)
+        fill = np.iinfo(np.int64).max if kind == 4 else np.iinfo(np.int64).min
+        enc = np.where(ok, enc, fill)
+        red = (np.minimum if kind == 4 else np.maximum).reduceat(enc, starts)
+        if isf:
+            outv = _unordered_f64(red).astype(np.float32 if typ == 1 else np.float64)
+        else:
+            outv = red.astype({0: np.int32, 4: np.int64, 2: np.int64}[typ])
+        res.append((np.where(cnt > 0, outv, 0).astype(outv.dtype), cnt == 0))
+    return out_key, out_kn, res

@@ -89,6 +89,10 @@ class Operand(C.Structure):
     _fields_ = [("data", C.c_void_p), ("type", C.c_int32), ("width", C.c_int32), ("is_scalar", C.c_int32)]
 
 
+class GroupAgg(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("column", C.c_int32)]
+
+
 class CsvError(C.Structure):
     _fields_ = [("bad_cells", C.c_uint64), ("first_row", C.c_uint32), ("first_field", C.c_int32),
                 ("kind", C.c_int32)]
@@ -157,6 +161,8 @@ PROTOTYPES = {
     "yq_key_transform": (C.c_int, [vp, i32, vp, u32, i32, vp]),
     "yq_merge_path": (C.c_int, [vp, vp, i32, i32, i32, u32, u32, u32, vp, vp, vp, vp, vp]),
     "yq_cross_product_col": (C.c_int, [P(Column), u32, u32, i32, P(Column), vp]),
+    "yq_group_by_workspace_size": (sz, [P(Column), u32, i32, u32]),
+    "yq_group_by": (C.c_int, [P(Batch), i32, P(GroupAgg), i32, P(Column), u32, P(u32), vp, sz, vp]),
     "yq_csv_index_workspace_size": (sz, [u64]),
     "yq_csv_index": (C.c_int, [vp, u64, vp, u64, P(u64), vp, sz, vp]),
     "yq_csv_parse_workspace_size": (sz, [u32]),

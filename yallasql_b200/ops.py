@@ -686,3 +686,36 @@ def write_csv(names: list[str], batch: DeviceBatch, stream=None) -> bytes:
     names joined by ',') and the formatted rows, copied to the host."""
     text = csv_format(batch, stream)
     return (",".join(names) + "\n").encode() + bytes(text.cpu().numpy().tobytes())
+
+
+# ------------------------------------------------------------------ GROUP BY
+def group_by_out_type(kind: int, in_type: int) -> int:
+    if kind in (A.AGG_COUNT, A.AGG_COUNT_STAR):
+        return A.INT64
+    if kind == A.AGG_SUM:
+        return A.FLOAT64 if in_type in (A.FLOAT32, A.FLOAT64) else A.INT64
+    if kind == A.AGG_AVG:
+        return A.FLOAT64
+    return in_type
+
+
+def group_by(batch: DeviceBatch, key: int, aggs: list[tuple[int, int]], capacity: int | None = None,
+             stream=None) -> DeviceBatch:
+    """SELECT key, aggs... GROUP BY key over a device batch (yq_group_by):
+    `aggs` are (yq_agg_kind, input column) pairs; returns the key column then
+    one column per aggregate, one row per group in ascending key order."""
+    L = lib()
+    s = _stream(stream)
+    kc = batch.columns[key]
+    cap = batch.rows if capacity is None else capacity
+    outs = [DeviceColumn.empty(kc.type, max(cap, 1), kc.width if kc.type == A.TEXT else None, nulls=True)]
+    for kind, col in aggs:
+        t = group_by_out_type(kind, batch.columns[col].type if kind != A.AGG_COUNT_STAR else A.INT64)
+        outs.append(DeviceColumn.empty(t, max(cap, 1), nulls=True))
+    bc, keep = batch.c()
+    ga = (A.GroupAgg * max(1, len(aggs)))(*[A.GroupAgg(k, c) for k, c in aggs])
+    oc = (A.Column * len(outs))(*[c.c() for c in outs])
+    g = C.c_uint32(0)
+    _check(L.yq_group_by(C.byref(bc), key, ga, len(aggs), oc, cap, C.byref(g), None, 0, s), "yq_group_by")
+    n = int(g.value)
+    return DeviceBatch([DeviceColumn(c.data[:n], c.type, c.nulls[:n]) for c in outs])
