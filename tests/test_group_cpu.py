@@ -71,3 +71,13 @@ def test_group_by_oracle_matches_python():
                 assert abs(res[3][0][gi] - w[5]) <= 1e-9 * max(1.0, abs(w[5]))
                 assert struct.pack("<d", res[4][0][gi]) == struct.pack("<d", w[6])
                 assert struct.pack("<d", res[5][0][gi]) == struct.pack("<d", w[7])
+
+
+def test_group_by_wrapper_rejects_more_aggregates_than_the_limit():
+    """yq_group_by takes at most YQ_MAX_AGGREGATES (8) aggregates a call; the
+    Python wrapper says so before touching the device."""
+    import pytest
+    from yallasql_b200 import _abi as A
+    from yallasql_b200 import ops
+    with pytest.raises(ValueError, match="at most 8"):
+        ops.group_by(None, 0, [(A.AGG_COUNT_STAR, 0)] * 9)

@@ -704,6 +704,8 @@ def group_by(batch: DeviceBatch, key: int, aggs: list[tuple[int, int]], capacity
     """SELECT key, aggs... GROUP BY key over a device batch (yq_group_by):
     `aggs` are (yq_agg_kind, input column) pairs; returns the key column then
     one column per aggregate, one row per group in ascending key order."""
+    if len(aggs) > A.MAX_AGGREGATES:
+        raise ValueError(f"group_by takes at most {A.MAX_AGGREGATES} aggregates a call, got {len(aggs)}")
     L = lib()
     s = _stream(stream)
     kc = batch.columns[key]
