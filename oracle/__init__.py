@@ -9,6 +9,21 @@ expression trees with numpy. Parity status: the reference ships no golden
 vectors or known-answer tests; the oracle is pinned against the reference's
 own GPU kernels run on the same inputs (``oracle/_ref``, built by
 ``oracle/Makefile`` from the reference sources) by ``tests/test_ref_pin_gpu.py``.
+
+CSV scan (``csv_scan``, ``convert_batch``): pinned against the reference's own
+reader, csv-parser plus std::stoi / std::stof / strptime
+(``oracle/_ref/libcsvref.so`` from ``csv_ref_harness.cpp``), live in
+``tests/test_csv_cpu.py`` and through the golden fixtures it wrote
+(``tests/golden/csv_ref.npz``).
+
+CSV writer (``csv_format``): snprintf / gmtime_r + strftime, the C library
+routines behind the reference writer's std::to_chars and strftime, checked
+against std::to_chars itself in ``tests/test_csv_cpu.py``.
+
+GROUP BY (``group_by``): parity unpinned. The reference ignores GROUP BY and
+the DuckDB it defers to is not available here, so this numpy restatement of
+SQL semantics is checked only against a plain-Python restatement of the same
+semantics (``tests/test_group_cpu.py``).
 """
 from __future__ import annotations
 
