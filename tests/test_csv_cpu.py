@@ -232,3 +232,27 @@ def test_writer_cells_match_the_reference_routines(shim):
     secs = [int(x) for x in rng.integers(-62167219200 - 86400 * 366 * 50, 253402300800 + 86400 * 366 * 50, 5000)]
     secs += [int(x) for x in rng.integers(-2**40, 2**40, 2000)] + [0, -1, -62167219200, -62167219201, 253402300800]
     assert shim_cells(2, secs) == oracle_cells(2, secs, np.int64)
+
+
+def test_generated_csv_matches_python_formatting():
+    """The benchmark CSV generator's vectorised fields (variable-width ids and
+    prices, "YYYY-MM-DD HH:MM:SS" dates) against Python's own formatting of
+    the same values."""
+    import datetime
+
+    from yallasql_b200 import datagen
+    rng = np.random.default_rng(17)
+    secs = np.concatenate([rng.integers(-2_000_000_000, 4_000_000_000, 5000), [0, -1, 86399, 951782400]])
+    got = datagen._date_text(secs)
+    epoch = datetime.datetime(1970, 1, 1)
+    for s, row in zip(secs, got):
+        want = (epoch + datetime.timedelta(seconds=int(s))).strftime("%Y-%m-%d %H:%M:%S")
+        assert bytes(row).decode() == want
+    header, body = datagen.sales_csv(2000, seed=3)
+    lines = bytes(body).decode().splitlines()
+    assert len(lines) == 2000 and header.decode().count(",") == 5
+    for i, line in enumerate(lines):
+        f = line.split(",")
+        assert int(f[0]) == i and len(f) == 6
+        assert f[1] == f"{float(f[1]):.2f}" and 1.0 <= float(f[1]) < 1000.0
+        assert 1 <= int(f[2]) <= 50 and 0 <= int(f[3]) <= 10 and f[4] in datagen.CATEGORIES
