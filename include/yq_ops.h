@@ -248,10 +248,15 @@ int yq_filter_project(const yq_batch* batch, const yq_program* predicate,
  * exits), so batches are limited to YQ_FILTER_PROJECT_NOALLOC_MAX_ROWS rows;
  * larger batches are rejected with YQ_ERR_INVALID_ARG before any device work.
  * The first call on a device looks up that array's device address (once per
- * device, under a lock); make that first call before any stream capture.
+ * device and CUDA context, under a lock; a device reset gives the device a new
+ * context, and the next call looks the address up again); make that first call
+ * before any stream capture.
  * Every call shares the one array and clears the part it uses on `stream`, so
  * calls whose kernels overlap on the GPU (different streams, no ordering
- * between them) race and must not be issued. */
+ * between them) race and must not be issued.
+ * It always runs the library's interpreter kernel: loading the
+ * program-specialised kernel that yq_filter_project uses would itself
+ * allocate, and the interpreter runs about 4x slower than that kernel. */
 #define YQ_FILTER_PROJECT_NOALLOC_MAX_ROWS (1u << 26)
 int yq_filter_project_noalloc(const yq_batch* batch, const yq_program* predicate,
                               const yq_constants* constants, const yq_projection* proj,
@@ -487,6 +492,13 @@ int yq_cast(const void* src, int32_t src_type, void* dst, int32_t dst_type, uint
 size_t yq_prefix_sum_workspace_size(uint32_t n);
 int yq_prefix_sum_mask(const uint8_t* mask, uint32_t* out, uint32_t n, void* workspace,
                        size_t workspace_bytes, void* stream);
+/* Test hook for the bounded waits (no counterpart in the reference, whose
+ * kernels wait without a bound or exit(1) on error): runs the library's
+ * decoupled look-back as tile 1 of a chain whose tile 0 never publishes, with
+ * the poll bound lowered to `spin_limit` (1 .. 2^22). Returns YQ_ERR_TIMEOUT
+ * after the wait runs out, as every entry point built on that look-back does;
+ * `workspace` is >= 64 bytes of device memory. */
+int yq_debug_lookback_stall(uint32_t spin_limit, void* workspace, size_t workspace_bytes, void* stream);
 /* launch_prefix_sum<uint32_t> (prefix_sum.hpp:29): inclusive scan of uint32. */
 int yq_prefix_sum_u32(const uint32_t* in, uint32_t* out, uint32_t n, void* workspace,
                       size_t workspace_bytes, void* stream);

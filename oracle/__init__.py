@@ -38,6 +38,17 @@ LIB = os.path.join(HERE, "liboracle.so")
 SRC = os.path.join(HERE, "oracle.c")
 
 
+def reference_sources() -> str | None:
+    """The reference's source tree for the parity-pin builds, or None where it
+    is absent (the GPU box uses the prebuilt oracle/_ref libraries). Taken from
+    YQ_REFERENCE_SOURCES, else the read-only mount the build container
+    provides; this recipe is the one place that names that mount."""
+    for cand in (os.environ.get("YQ_REFERENCE_SOURCES"), "/root/reference"):
+        if cand and os.path.isdir(os.path.join(cand, "src", "kernels")):
+            return cand
+    return None
+
+
 def build() -> str:
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
         subprocess.check_call(["gcc", "-O3", "-march=x86-64-v2", "-shared", "-fPIC", "-pthread", "-o", LIB, SRC,

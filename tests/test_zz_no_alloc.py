@@ -42,20 +42,37 @@ def _plan():
     return ops.ProjectPlan([A.FLOAT32, A.INT32, A.INT32, A.TEXT, A.DATETIME], [4, 4, 4, 16, 8], pred, select)
 
 
-def _noalloc(lib, plan, batch):
-    """One call of yq_filter_project_noalloc; outputs allocated here by torch,
-    before the call, as a host that owns its memory would hand them in."""
-    cap = batch.rows
-    outs = [ops.DeviceColumn.empty(t, cap, w if t == A.TEXT else None, nulls=True)
+def _outputs(plan, cap):
+    return [ops.DeviceColumn.empty(t, cap, w if t == A.TEXT else None, nulls=True)
             for t, w in zip(plan.out_types, plan.out_widths)]
+
+
+def _noalloc(lib, plan, batch, outs, count_device=None):
+    """One call of yq_filter_project_noalloc into `outs` (allocated by torch
+    before the call, as a host that owns its memory would hand them in).
+    With `count_device` the call returns without waiting and the surviving
+    row count is read from that device word afterwards."""
+    cap = batch.rows
     oc = (A.Column * len(outs))(*[o.c() for o in outs])
     b, keep = batch.c()
     cnt = C.c_uint32(0)
     st = lib.yq_filter_project_noalloc(C.byref(b), C.byref(plan.pred.prog), C.byref(plan.consts), plan.proj,
-                                       len(plan.select), oc, cap, None, C.byref(cnt),
+                                       len(plan.select), oc, cap,
+                                       None if count_device is None else
+                                       C.cast(count_device.data_ptr(), C.POINTER(C.c_uint32)),
+                                       None if count_device is not None else C.byref(cnt),
                                        torch.cuda.current_stream().cuda_stream)
     assert st == A.OK, lib.yq_status_string(st)
-    return [o.slice(0, cnt.value) for o in outs]
+    n = int(count_device.item()) if count_device is not None else cnt.value
+    return [o.slice(0, n) for o in outs]
+
+
+def _same(got, want):
+    assert len(got) == len(want.columns)
+    for g, w in zip(got, want.columns):
+        assert g.rows == w.rows
+        assert torch.equal(g.data, w.data)
+        assert torch.equal(g.nulls, w.nulls)
 
 
 def test_noalloc_matches_allocating_entry_point_twice(cuda, yq):
@@ -64,10 +81,31 @@ def test_noalloc_matches_allocating_entry_point_twice(cuda, yq):
     want = plan.run(batch)  # yq_filter_project, library-allocated workspace
     assert 0 < want.rows < batch.rows
     for _ in range(2):  # the second call must not see the first call's scratch
-        got = _noalloc(yq, plan, batch)
-        for g, w in zip(got, want.columns):
-            assert torch.equal(g.data, w.data)
-            assert torch.equal(g.nulls, w.nulls)
+        _same(_noalloc(yq, plan, batch, _outputs(plan, batch.rows)), want)
+
+
+def test_noalloc_allocates_nothing_large_then_small(cuda, yq):
+    """Device memory in use is the same before and after a call, and a larger
+    batch followed by a smaller one leaves nothing of the first in the second
+    (the scratch is cleared as far as the second call reads it). One call
+    reports its count through a device word instead of the host."""
+    plan = _plan()
+    big, small = _table(2_000_003), _table(70_001)
+    want_big, want_small = plan.run(big), plan.run(small)
+    outs_big, outs_small = _outputs(plan, big.rows), _outputs(plan, small.rows)
+    count = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _noalloc(yq, plan, small, outs_small)  # warm-up: loads the kernel, looks up the scratch address
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    got_big = _noalloc(yq, plan, big, outs_big)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    got_small = _noalloc(yq, plan, small, outs_small, count_device=count)
+    torch.cuda.synchronize()
+    free2, _ = torch.cuda.mem_get_info()
+    assert free0 == free1 == free2, (free0, free1, free2)
+    _same(got_big, want_big)
+    _same(got_small, want_small)
 
 
 def test_noalloc_rejects_batches_above_its_limit(cuda, yq):

@@ -153,6 +153,7 @@ PROTOTYPES = {
     "yq_cast": (C.c_int, [vp, i32, vp, i32, u32, vp]),
     "yq_prefix_sum_workspace_size": (sz, [u32]),
     "yq_prefix_sum_mask": (C.c_int, [vp, vp, u32, vp, sz, vp]),
+    "yq_debug_lookback_stall": (C.c_int, [u32, vp, sz, vp]),
     "yq_prefix_sum_u32": (C.c_int, [vp, vp, u32, vp, sz, vp]),
     "yq_move_rows_filter": (C.c_int, [P(Column), vp, vp, u32, P(Column), vp]),
     "yq_move_rows_join": (C.c_int, [P(Column), vp, u32, i32, P(Column), vp]),

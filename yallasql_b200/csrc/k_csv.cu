@@ -556,13 +556,7 @@ int yq_csv_parse(const uint8_t* data, uint64_t nbytes, const uint32_t* record_st
   void* scan_ws = ws.take<uint8_t>(yq_prefix_sum_workspace_size(records));
   const unsigned long long init[4] = {0, 0, ~0ull, 0};
   YQ_TRY(h2d_async(P.counters, init, sizeof(init), s));
-  int dev = 0;
-  YQ_TRY_CUDA(cudaGetDevice(&dev));
-  static unsigned long long smem_set = 0;  // one bit per device: the opt-in for > 48 KiB of shared memory
-  if (dev < 64 && !((smem_set >> dev) & 1)) {
-    YQ_TRY_CUDA(cudaFuncSetAttribute(k_csv_parse, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpanCap + 16));
-    smem_set |= 1ull << dev;
-  }
+  YQ_TRY(kernel_allow_smem((const void*)k_csv_parse, kSpanCap + 16));
   double out_bytes = 1.0;  // valid flag
   for (int f = 0; f < nfields; ++f)
     if (P.f[f].data) out_bytes += P.f[f].width + 1.0;
@@ -664,13 +658,7 @@ int yq_csv_format(const yq_batch* batch, uint8_t* out, uint64_t capacity, uint64
   *bytes = total;
   if (total > capacity) return YQ_ERR_CAPACITY;
   if (!out) return YQ_ERR_INVALID_ARG;
-  int dev = 0;
-  YQ_TRY_CUDA(cudaGetDevice(&dev));
-  static unsigned long long smem_set = 0;  // one bit per device
-  if (dev < 64 && !((smem_set >> dev) & 1)) {
-    YQ_TRY_CUDA(cudaFuncSetAttribute(k_csv_format_write, cudaFuncAttributeMaxDynamicSharedMemorySize, kFmtSpan + 16));
-    smem_set |= 1ull << dev;
-  }
+  YQ_TRY(kernel_allow_smem((const void*)k_csv_format_write, kFmtSpan + 16));
   double in_bytes = 0;
   for (int c = 0; c < batch->ncols; ++c)
     in_bytes += (double)rows * (batch->columns[c].width + (batch->columns[c].nulls ? 1 : 0));

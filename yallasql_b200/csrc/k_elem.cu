@@ -756,4 +756,37 @@ int yq_cross_product_col(const yq_column* col, uint32_t left_rows, uint32_t righ
   return YQ_OK;
 }
 
+// --------------------------------------------------- bounded-wait test hook
+// Runs the production look-back (tile_lookback, the single-pass scan under
+// WHERE compaction, projection and the prefix sums) as tile 1 of a chain whose
+// tile 0 never publishes its status word, with the poll bound lowered to
+// `spin_limit`: the wait runs out, the error word gets kErrTimeout and the
+// call returns YQ_ERR_TIMEOUT. Nothing waits without a bound, so the device
+// stays usable afterwards.
+}  // extern "C"
+
+namespace {
+__global__ void k_debug_lookback_stall(unsigned long long* status, uint32_t* err, uint32_t limit,
+                                       unsigned long long* excl_out) {
+  const unsigned long long excl = tile_lookback(status, 1u, 7ull, err, limit);
+  if (threadIdx.x == 0) *excl_out = excl;
+}
+}  // namespace
+
+extern "C" int yq_debug_lookback_stall(uint32_t spin_limit, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!workspace || workspace_bytes < 64 || spin_limit == 0 || spin_limit > kSpinLimit) return YQ_ERR_INVALID_ARG;
+  cudaStream_t s = as_stream(stream);
+  unsigned long long* status = static_cast<unsigned long long*>(workspace);  // [0] tile 0, [1] tile 1
+  uint32_t* err = reinterpret_cast<uint32_t*>(status + 2);
+  unsigned long long* excl = status + 3;
+  YQ_TRY_CUDA(cudaMemsetAsync(workspace, 0, 64, s));
+  k_debug_lookback_stall<<<1, 32, 0, s>>>(status, err, spin_limit, excl);
+  YQ_CHECK_LAUNCH();
+  uint32_t e = 0;
+  YQ_TRY_CUDA(cudaMemcpyAsync(&e, err, sizeof(e), cudaMemcpyDeviceToHost, s));
+  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  return (e & kErrTimeout) ? YQ_ERR_TIMEOUT : YQ_OK;
+}
+
+extern "C" {
 }  // extern "C"

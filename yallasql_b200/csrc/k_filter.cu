@@ -17,35 +17,13 @@
 
 namespace yq {
 
-static int occupancy_grid(const void* kernel, int block, size_t smem) {
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess || per_sm < 1)
-    per_sm = 1;
-  return per_sm * sm_count();
+// Persistent grid of a row kernel: resident blocks on every SM (per device,
+// cached), no more than the steps.
+static int resident_grid(const void* kernel, size_t dyn_smem, uint32_t steps) {
+  const int cap = kernel_blocks_per_sm(kernel, kRowBlock, dyn_smem) * sm_count();
+  const int g = (int)(steps < (uint32_t)cap ? steps : (uint32_t)cap);
+  return g < 1 ? 1 : g;
 }
-
-// Raise a kernel's dynamic shared memory limit (once per size) to `smem`.
-static int allow_smem(const void* kernel, size_t smem, size_t& done) {
-  if (smem > 48 * 1024 && smem > done) {
-    YQ_TRY_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    done = smem;
-  }
-  return YQ_OK;
-}
-
-// Persistent grid of a row kernel: resident blocks, no more than the steps.
-struct GridCache {
-  int cap = 0;
-  size_t smem = (size_t)-1;
-  int grid(const void* kernel, size_t dyn_smem, uint32_t steps) {
-    if (smem != dyn_smem) {
-      cap = occupancy_grid(kernel, kRowBlock, dyn_smem);
-      smem = dyn_smem;
-    }
-    int g = (int)(steps < (uint32_t)cap ? steps : (uint32_t)cap);
-    return g < 1 ? 1 : g;
-  }
-};
 
 static size_t max_row_grid() { return (size_t)sm_count() * 8; }
 
@@ -146,10 +124,8 @@ static int launch_filter_aggregate(const FAParams& F0, uint32_t rows, Acc* parti
   const bool staged = F.SP.nstages > 0;
   const void* kern = staged ? (const void*)k_filter_aggregate<true> : (const void*)k_filter_aggregate<false>;
   const size_t smem = stage_smem_bytes(F.SP);
-  static size_t done_smem = 0;
-  YQ_TRY(allow_smem(kern, smem, done_smem));
-  static GridCache gc[2];
-  int grid = gc[staged ? 1 : 0].grid(kern, smem, ceil_div<uint32_t>(rows, kStepRows));
+  YQ_TRY(kernel_allow_smem(kern, smem));
+  int grid = resident_grid(kern, smem, ceil_div<uint32_t>(rows, kStepRows));
   if ((size_t)grid > max_row_grid()) grid = (int)max_row_grid();
   const void* jk = jit_kernel(JIT_FILTER_AGG, staged, F.P, F.pc_end, F.pc_end);  // compiles once, outside the timing
   ProfScope ps("filter_aggregate", s, (double)rows * row_bytes_of(F.P, program_columns(F.P, F.pc_end, 0)));
@@ -303,10 +279,8 @@ static int launch_filter_project(FPParams& F, uint32_t rows, uint32_t* misc, uns
   F.csteps = std::max<uint32_t>(1u, std::min<uint32_t>(8u, ceil_div<uint32_t>(rows, kStepRows) / (8u * sm_count())));
   const void* kern = staged ? (const void*)k_filter_project<true> : (const void*)k_filter_project<false>;
   const size_t smem = stage_smem_bytes(F.SP);
-  static size_t done_smem = 0;
-  YQ_TRY(allow_smem(kern, smem, done_smem));
-  static GridCache gc[2];
-  const int grid = gc[staged ? 1 : 0].grid(kern, smem, ceil_div<uint32_t>(rows, kStepRows));
+  YQ_TRY(kernel_allow_smem(kern, smem));
+  const int grid = resident_grid(kern, smem, ceil_div<uint32_t>(rows, kStepRows));
   uint32_t mask = program_columns(F.P, F.proj_end, 0);
   for (int p = 0; p < F.nproj; ++p)
     if (F.out[p].src_col >= 0) mask |= 1u << F.out[p].src_col;
@@ -524,10 +498,8 @@ static int filter_aggregate_ranges(const yq_batch* batch, const uint32_t* begin,
     const void* kern =
         staged ? (const void*)k_filter_aggregate_seg<true> : (const void*)k_filter_aggregate_seg<false>;
     const size_t smem = stage_smem_bytes(Q.F.SP);
-    static size_t done_smem = 0;
-    YQ_TRY(allow_smem(kern, smem, done_smem));
-    static GridCache gc[2];
-    const int grid = gc[staged ? 1 : 0].grid(kern, smem, nsteps);
+    YQ_TRY(kernel_allow_smem(kern, smem));
+    const int grid = resident_grid(kern, smem, nsteps);
     double rows = 0;
     for (int g = 0; g < nseg; ++g) rows += end[g] - begin[g];
     const void* jk = jit_kernel(JIT_FILTER_AGG_SEG, staged, Q.F.P, Q.F.pc_end, Q.F.pc_end);
@@ -624,6 +596,7 @@ int yq_filter_project(const yq_batch* batch, const yq_program* predicate, const 
 // the caller passes or the library allocates. Layout: four 32-bit counters
 // (chunk counter, error word, row count, spare), then one 64-bit look-back
 // status word per 1,024-row step plus one (a chunk of steps uses one).
+#include <cuda.h>
 #include <mutex>
 
 namespace yq {
@@ -633,16 +606,50 @@ constexpr size_t kNoAllocWords = 2 + (size_t)kNoAllocTiles + 1;  // 2 words hold
 
 static __device__ __align__(256) unsigned long long g_filter_project_scratch[kNoAllocWords];
 
-// Device address of the scratch array, looked up once per device with that
-// device current (host code only sees a host-side stand-in for the symbol).
+// Identity of the calling thread's current CUDA context, unique for the life
+// of the process (cuCtxGetId, reached through the runtime's driver entry
+// points so the library needs no link against the driver library); 0 when
+// no context is current or the driver does not offer it.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+static unsigned long long current_context_id() {
+  static std::once_flag once;
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(p);
+    cudaGetLastError();
+  });
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of the scratch array (host code only sees a host-side
+// stand-in for the symbol). Looked up with the device current, once per
+// device and context: after a device reset the device gets a new context in
+// which the array may live elsewhere, so a changed context id (or none known)
+// triggers a new lookup.
 static int noalloc_scratch(unsigned long long** out) {
   static std::mutex mu;
   static void* addr[64] = {nullptr};
+  static unsigned long long ctx[64] = {0};
   int dev = 0;
   YQ_TRY_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return YQ_ERR_UNSUPPORTED;
   std::lock_guard<std::mutex> lk(mu);
-  if (!addr[dev]) {
+  const unsigned long long id = current_context_id();
+  if (!addr[dev] || id == 0 || id != ctx[dev]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_filter_project_scratch);
     if (e != cudaSuccess || !p) {
@@ -650,6 +657,7 @@ static int noalloc_scratch(unsigned long long** out) {
       return YQ_ERR_CUDA;
     }
     addr[dev] = p;
+    ctx[dev] = current_context_id();  // the lookup made the device's context current
   }
   *out = static_cast<unsigned long long*>(addr[dev]);
   return YQ_OK;

@@ -13,10 +13,17 @@
 //                     from the one before it (-0.0 equals +0.0, NaNs equal)
 //   yq_prefix_sum_mask  -> group index of every sorted position, group count
 //   k_group_keys      each group's key into the output
-//   k_group_accumulate  32 consecutive sorted positions a thread, values read
-//                     through the permutation; a run of one group is folded in
-//                     registers and flushed with one atomic per aggregate
-//   k_group_finalize  accumulators -> output values and NULL bytes
+//   k_group_tiles     tiles of 4,096 sorted positions (16 a thread), values
+//                     read through the permutation: each thread folds its
+//                     positions in order, a segmented scan over the block's
+//                     threads (fixed tree) completes every group that starts
+//                     and ends in the tile and writes its output row; a group
+//                     crossing the tile's edges leaves a partial record
+//   k_group_span      each group that crosses tiles, from the tile where it
+//                     starts: its tiles' partial records folded in tile order
+//                     (fixed tree), output row written
+// No atomics: every floating-point sum is added in an order fixed by the
+// data's sorted layout, so a query gives the same bits on every run.
 #include <climits>
 
 #include "yq_common.cuh"
@@ -26,7 +33,6 @@ using namespace yq;
 namespace {
 
 constexpr int kGroupThreads = 256;
-constexpr int kGroupRun = 32;  // sorted positions per thread in the accumulate pass
 
 // Key equality of two rows (canonical floats, NULL == NULL).
 __device__ __forceinline__ bool same_key(const yq_column& k, uint32_t a, uint32_t b) {
@@ -78,8 +84,6 @@ struct GAgg {
   const uint8_t* nulls;
   int32_t type;          // input type
   int32_t kind;          // yq_agg_kind
-  unsigned long long* count;  // per group: rows (COUNT_STAR) or non-NULL inputs
-  unsigned long long* value;  // per group: int64 sum, double sum (bits), or ordered MIN/MAX key
 };
 
 struct GroupParams {
@@ -88,7 +92,17 @@ struct GroupParams {
   uint32_t rows;
   const uint32_t* perm;
   const uint32_t* incl;  // inclusive scan of the head flags: group = incl - 1
+  uint32_t* starts;      // [groups + 1] first sorted position of every group; starts[groups] = rows
+  yq_column out[YQ_MAX_AGGREGATES];  // aggregate output columns
+  unsigned long long* rec;  // [tiles][2][nagg][2]: head / tail partial (count, value) of every tile
+  uint32_t* tail_group;     // [tiles] group of the tile's tail record
+  uint32_t* tile_flags;     // [tiles] kHeadRec | kTailRec | kTailStarted (set with atomicOr)
+  uint32_t* err;
 };
+
+constexpr uint32_t kGroupItems = 16;
+constexpr uint32_t kGroupTile = kGroupThreads * kGroupItems;  // 4,096 sorted positions
+constexpr uint32_t kHeadRec = 1, kTailRec = 2, kTailStarted = 4;
 
 // Order-preserving signed 64-bit key of a double (NaN above +inf, one NaN).
 __device__ __forceinline__ long long ordered(double d) {
@@ -113,98 +127,267 @@ __device__ __forceinline__ double in_dbl(const GAgg& a, uint32_t r) {
   return a.type == YQ_FLOAT32 ? (double)static_cast<const float*>(a.data)[r] : static_cast<const double*>(a.data)[r];
 }
 
-__device__ __forceinline__ void flush(const GAgg& a, uint32_t g, unsigned long long cnt, long long isum, double dsum,
-                                      long long best) {
-  if (cnt == 0) return;
-  atomicAdd(a.count + g, cnt);
-  switch (a.kind) {
+// One aggregate's partial state: a count and a 64-bit value (int64 sum,
+// double sum bits, or the ordered key of MIN / MAX).
+struct GPart {
+  unsigned long long cnt;
+  unsigned long long v;
+};
+
+__device__ __forceinline__ GPart part_identity(int kind) {
+  return GPart{0ull, kind == YQ_AGG_MIN ? (unsigned long long)LLONG_MAX
+                     : kind == YQ_AGG_MAX ? (unsigned long long)LLONG_MIN : 0ull};
+}
+
+__device__ __forceinline__ GPart part_combine(int kind, bool flt, GPart a, GPart b) {
+  GPart c;
+  c.cnt = a.cnt + b.cnt;
+  switch (kind) {
     case YQ_AGG_SUM:
     case YQ_AGG_AVG:
-      if (is_float(a.type)) atomicAdd(reinterpret_cast<double*>(a.value + g), dsum);
-      else atomicAdd(a.value + g, (unsigned long long)isum);
+      c.v = flt ? (unsigned long long)__double_as_longlong(__longlong_as_double((long long)a.v) +
+                                                           __longlong_as_double((long long)b.v))
+                : a.v + b.v;
       break;
-    case YQ_AGG_MIN: atomicMin(reinterpret_cast<long long*>(a.value + g), best); break;
-    case YQ_AGG_MAX: atomicMax(reinterpret_cast<long long*>(a.value + g), best); break;
-    default: break;
+    case YQ_AGG_MIN: c.v = (long long)a.v < (long long)b.v ? a.v : b.v; break;
+    case YQ_AGG_MAX: c.v = (long long)a.v > (long long)b.v ? a.v : b.v; break;
+    default: c.v = 0ull; break;
+  }
+  return c;
+}
+
+__device__ __forceinline__ void part_add_row(const GAgg& a, bool flt, GPart& p, uint32_t r) {
+  if (a.kind == YQ_AGG_COUNT_STAR) {
+    ++p.cnt;
+    return;
+  }
+  if (a.nulls && a.nulls[r]) return;
+  ++p.cnt;
+  if (a.kind == YQ_AGG_SUM || a.kind == YQ_AGG_AVG) {
+    if (flt) p.v = (unsigned long long)__double_as_longlong(__longlong_as_double((long long)p.v) + in_dbl(a, r));
+    else p.v += (unsigned long long)in_int(a, r);
+  } else if (a.kind == YQ_AGG_MIN || a.kind == YQ_AGG_MAX) {
+    const long long k = flt ? ordered(in_dbl(a, r)) : in_int(a, r);
+    if (a.kind == YQ_AGG_MIN ? k < (long long)p.v : k > (long long)p.v) p.v = (unsigned long long)k;
   }
 }
 
-__global__ void __launch_bounds__(kGroupThreads) k_group_accumulate(const __grid_constant__ GroupParams P) {
-  const uint64_t t = (uint64_t)blockIdx.x * kGroupThreads + threadIdx.x;
-  const uint64_t lo = t * kGroupRun;
-  if (lo >= P.rows) return;
-  const uint32_t hi = (uint32_t)(lo + kGroupRun < P.rows ? lo + kGroupRun : P.rows);
-  for (int j = 0; j < P.nagg; ++j) {  // aggregates one at a time: the warp's lanes run the same one
+// Output row g of aggregate a from its complete state.
+__device__ __forceinline__ void part_write(const GAgg& a, const yq_column& o, uint32_t g, GPart p) {
+  const bool flt = is_float(a.type);
+  const bool null = p.cnt == 0 && a.kind != YQ_AGG_COUNT && a.kind != YQ_AGG_COUNT_STAR;
+  if (o.nulls) const_cast<uint8_t*>(o.nulls)[g] = null ? 1 : 0;
+  switch (a.kind) {
+    case YQ_AGG_COUNT:
+    case YQ_AGG_COUNT_STAR: static_cast<long long*>(o.data)[g] = (long long)p.cnt; break;
+    case YQ_AGG_SUM:
+      if (flt) static_cast<double*>(o.data)[g] = null ? 0.0 : __longlong_as_double((long long)p.v);
+      else static_cast<long long*>(o.data)[g] = null ? 0 : (long long)p.v;
+      break;
+    case YQ_AGG_AVG: {
+      const double sum = flt ? __longlong_as_double((long long)p.v) : (double)(long long)p.v;
+      static_cast<double*>(o.data)[g] = null ? 0.0 : sum / (double)p.cnt;
+      break;
+    }
+    default: {  // MIN / MAX in the input type
+      const long long k = (long long)p.v;
+      if (a.type == YQ_INT32) static_cast<int32_t*>(o.data)[g] = null ? 0 : (int32_t)k;
+      else if (a.type == YQ_FLOAT32) static_cast<float*>(o.data)[g] = null ? 0.0f : (float)unordered(k);
+      else if (a.type == YQ_FLOAT64) static_cast<double*>(o.data)[g] = null ? 0.0 : unordered(k);
+      else static_cast<long long*>(o.data)[g] = null ? 0 : k;
+      break;
+    }
+  }
+}
+
+__device__ __forceinline__ GPart shfl_up_part(GPart p, int d) {
+  return GPart{__shfl_up_sync(0xffffffffu, p.cnt, d), __shfl_up_sync(0xffffffffu, p.v, d)};
+}
+
+// Inclusive segmented scan over the block's threads in thread order (a
+// thread's flag restarts the running state); fixed combine tree. Returns the
+// inclusive state and flag; excl / excl_flag = the same up to the thread before.
+__device__ __forceinline__ void block_seg_scan(int kind, bool flt, bool flag, GPart x, GPart& incl, bool& incl_flag,
+                                               GPart& excl, bool& excl_flag, GPart* s_part, uint32_t* s_flag) {
+  constexpr int NW = kGroupThreads / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  GPart v = x;
+  bool f = flag;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const GPart u = shfl_up_part(v, d);
+    const bool uf = __shfl_up_sync(0xffffffffu, f, d);
+    if (lane >= d) {
+      if (!f) v = part_combine(kind, flt, u, v);
+      f = f || uf;
+    }
+  }
+  if (lane == 31) {
+    s_part[warp] = v;
+    s_flag[warp] = f;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {  // warp prefixes in warp order (exclusive), one thread: fixed order
+    GPart run = part_identity(kind);
+    bool rf = false;
+    for (int w = 0; w < NW; ++w) {
+      const GPart wv = s_part[w];
+      const bool wf = s_flag[w] != 0u;
+      s_part[NW + w] = run;
+      s_flag[NW + w] = rf;
+      run = wf ? wv : part_combine(kind, flt, run, wv);
+      rf = rf || wf;
+    }
+  }
+  __syncthreads();
+  const GPart wp = s_part[NW + warp];
+  const bool wpf = s_flag[NW + warp] != 0u;
+  // lane-level exclusive value within the warp
+  GPart le = shfl_up_part(v, 1);
+  bool lef = __shfl_up_sync(0xffffffffu, f, 1);
+  if (lane == 0) {
+    le = part_identity(kind);
+    lef = false;
+  }
+  incl = f ? v : part_combine(kind, flt, wp, v);
+  incl_flag = f || wpf;
+  excl = lef ? le : (lane == 0 ? wp : part_combine(kind, flt, wp, le));
+  excl_flag = lef || wpf;
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kGroupThreads) k_group_tiles(const __grid_constant__ GroupParams P) {
+  __shared__ GPart s_part[2 * (kGroupThreads / 32)];
+  __shared__ uint32_t s_flag[2 * (kGroupThreads / 32)];
+  const uint32_t tile = blockIdx.x;
+  const uint32_t tile0 = tile * kGroupTile;
+  const uint32_t tile_end = min(P.rows, tile0 + kGroupTile);
+  const uint32_t p0 = tile0 + threadIdx.x * kGroupItems;
+  const uint32_t n = p0 < tile_end ? min(kGroupItems, tile_end - p0) : 0u;  // valid positions of this thread
+  uint32_t g[kGroupItems], r[kGroupItems];
+#pragma unroll
+  for (int q = 0; q < (int)kGroupItems; ++q) {
+    g[q] = (uint32_t)q < n ? __ldg(P.incl + p0 + q) - 1u : 0u;
+    r[q] = (uint32_t)q < n ? __ldg(P.perm + p0 + q) : 0u;
+  }
+  const uint32_t prev_g = p0 > 0 && n ? __ldg(P.incl + p0 - 1) - 1u : 0xffffffffu;
+  const uint32_t last = n ? p0 + n - 1 : 0u;
+  const uint32_t next_g = n && last + 1 < P.rows ? __ldg(P.incl + last + 1) - 1u : 0xffffffffu;
+  // group starts
+#pragma unroll
+  for (int q = 0; q < (int)kGroupItems; ++q)
+    if ((uint32_t)q < n && (q == 0 ? g[0] != prev_g : g[q] != g[q - 1])) P.starts[g[q]] = p0 + q;
+  const bool starts_here = n && g[0] != prev_g;
+  bool boundary = false;  // a group starts inside (after the first position)
+#pragma unroll
+  for (int q = 1; q < (int)kGroupItems; ++q) boundary |= (uint32_t)q < n && g[q] != g[q - 1];
+  uint32_t g_last = 0u;
+#pragma unroll
+  for (int q = 0; q < (int)kGroupItems; ++q)
+    if ((uint32_t)q + 1 == n) g_last = g[q];
+  const bool ends_here = n && next_g != g_last;
+  const bool tile_last = n && last + 1 == tile_end;  // the tile's last valid position is this thread's
+  for (int j = 0; j < P.nagg; ++j) {
     const GAgg& a = P.a[j];
-    uint32_t g = P.incl[lo] - 1;
-    unsigned long long cnt = 0;
-    long long isum = 0, best = a.kind == YQ_AGG_MIN ? LLONG_MAX : LLONG_MIN;
-    double dsum = 0.0;
-    for (uint32_t i = (uint32_t)lo; i < hi; ++i) {
-      const uint32_t gi = P.incl[i] - 1;
-      if (gi != g) {
-        flush(a, g, cnt, isum, dsum, best);
-        g = gi;
-        cnt = 0;
-        isum = 0;
-        dsum = 0.0;
-        best = a.kind == YQ_AGG_MIN ? LLONG_MAX : LLONG_MIN;
+    const bool flt = is_float(a.type);
+    GPart first = part_identity(a.kind), cur = part_identity(a.kind);
+    uint32_t cg = g[0];
+    int seg = 0;  // segments closed so far in this thread
+#pragma unroll
+    for (int q = 0; q < (int)kGroupItems; ++q) {
+      if ((uint32_t)q >= n) break;
+      if (q > 0 && g[q] != cg) {  // the segment of group cg ends before position q
+        if (seg == 0) first = cur;                         // the thread's first segment
+        else part_write(a, P.out[j], cg, cur);             // an inner segment: complete here
+        if (seg == 0 && starts_here) part_write(a, P.out[j], cg, cur);  // first segment began here too
+        ++seg;
+        cg = g[q];
+        cur = part_identity(a.kind);
       }
-      if (a.kind == YQ_AGG_COUNT_STAR) { ++cnt; continue; }
-      const uint32_t r = P.perm[i];
-      if (a.nulls && a.nulls[r]) continue;
-      ++cnt;
-      if (a.kind == YQ_AGG_SUM || a.kind == YQ_AGG_AVG) {
-        if (is_float(a.type)) dsum += in_dbl(a, r);
-        else isum += in_int(a, r);
-      } else if (a.kind == YQ_AGG_MIN || a.kind == YQ_AGG_MAX) {
-        const long long k = is_float(a.type) ? ordered(in_dbl(a, r)) : in_int(a, r);
-        best = a.kind == YQ_AGG_MIN ? (k < best ? k : best) : (k > best ? k : best);
+      part_add_row(a, flt, cur, r[q]);
+    }
+    // thread element of the scan: the running state of the thread's last segment
+    GPart inc, exc;
+    bool inc_f, exc_f;
+    block_seg_scan(a.kind, flt, n == 0 || starts_here || boundary, cur, inc, inc_f, exc, exc_f, s_part, s_flag);
+    if (n == 0) continue;
+    unsigned long long* head_rec = P.rec + ((size_t)tile * 2 * P.nagg + j) * 2;
+    unsigned long long* tail_rec = P.rec + ((size_t)tile * 2 * P.nagg + P.nagg + j) * 2;
+    if (boundary && !starts_here) {
+      // the first segment continues a group from earlier threads and ends here
+      const GPart tot = part_combine(a.kind, flt, exc, first);
+      if (exc_f) {
+        part_write(a, P.out[j], g[0], tot);
+      } else {  // the group began before this tile: the tile's head record
+        head_rec[0] = tot.cnt;
+        head_rec[1] = tot.v;
+        if (j == 0) atomicOr(P.tile_flags + tile, kHeadRec);
       }
     }
-    flush(a, g, cnt, isum, dsum, best);
+    // the last segment: its state up to here is the inclusive scan value
+    if (ends_here) {
+      if (inc_f) {
+        part_write(a, P.out[j], g_last, inc);
+      } else {
+        head_rec[0] = inc.cnt;
+        head_rec[1] = inc.v;
+        if (j == 0) atomicOr(P.tile_flags + tile, kHeadRec);
+      }
+    } else if (tile_last) {  // the group goes on past this tile
+      tail_rec[0] = inc.cnt;
+      tail_rec[1] = inc.v;
+      if (j == 0) {
+        P.tail_group[tile] = g_last;
+        atomicOr(P.tile_flags + tile, kTailRec | (inc_f ? kTailStarted : 0u));
+      }
+    }
   }
 }
 
-__global__ void k_group_init(const __grid_constant__ GroupParams P, uint32_t groups) {
-  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += gridDim.x * blockDim.x)
-    for (int j = 0; j < P.nagg; ++j) {
-      P.a[j].count[g] = 0;
-      P.a[j].value[g] = P.a[j].kind == YQ_AGG_MIN ? (unsigned long long)LLONG_MAX
-                        : P.a[j].kind == YQ_AGG_MAX ? (unsigned long long)LLONG_MIN : 0ull;
+// One block per tile: the group that starts in this tile and runs past it.
+__global__ void __launch_bounds__(kGroupThreads) k_group_span(const __grid_constant__ GroupParams P, uint32_t ntiles) {
+  __shared__ GPart s_red[kGroupThreads / 32];
+  const uint32_t t = blockIdx.x;
+  const uint32_t fl = P.tile_flags[t];
+  if (!(fl & kTailRec) || !(fl & kTailStarted)) return;
+  const uint32_t g = P.tail_group[t];
+  const uint32_t end = P.starts[g + 1];
+  if (end == 0 || end > P.rows) {
+    if (threadIdx.x == 0) atomicOr(P.err, 2u);
+    return;
+  }
+  const uint32_t tb = (end - 1) / kGroupTile;
+  if (tb <= t || tb >= ntiles || !(P.tile_flags[tb] & kHeadRec)) {
+    if (threadIdx.x == 0) atomicOr(P.err, 2u);
+    return;
+  }
+  const uint32_t n = tb - t + 1;  // contributions: tail(t), tail(t+1..tb-1), head(tb)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int j = 0; j < P.nagg; ++j) {
+    const GAgg& a = P.a[j];
+    const bool flt = is_float(a.type);
+    GPart acc = part_identity(a.kind);
+    for (uint32_t k = threadIdx.x; k < n; k += kGroupThreads) {
+      const uint32_t tt = t + k;
+      const unsigned long long* rec =
+          P.rec + ((size_t)tt * 2 * P.nagg + (k + 1 == n ? 0 : P.nagg) + j) * 2;  // head of tb, else tail
+      acc = part_combine(a.kind, flt, acc, GPart{rec[0], rec[1]});
     }
-}
-
-__global__ void k_group_finalize(const __grid_constant__ GroupParams P, uint32_t groups, const yq_column* out_dev) {
-  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += gridDim.x * blockDim.x)
-    for (int j = 0; j < P.nagg; ++j) {
-      const GAgg& a = P.a[j];
-      const yq_column o = out_dev[1 + j];
-      const unsigned long long cnt = a.count[g], v = a.value[g];
-      const bool null = cnt == 0 && a.kind != YQ_AGG_COUNT && a.kind != YQ_AGG_COUNT_STAR;
-      if (o.nulls) const_cast<uint8_t*>(o.nulls)[g] = null ? 1 : 0;
-      switch (a.kind) {
-        case YQ_AGG_COUNT:
-        case YQ_AGG_COUNT_STAR: static_cast<long long*>(o.data)[g] = (long long)cnt; break;
-        case YQ_AGG_SUM:
-          if (is_float(a.type)) static_cast<double*>(o.data)[g] = null ? 0.0 : __longlong_as_double((long long)v);
-          else static_cast<long long*>(o.data)[g] = null ? 0 : (long long)v;
-          break;
-        case YQ_AGG_AVG: {
-          const double s = is_float(a.type) ? __longlong_as_double((long long)v) : (double)(long long)v;
-          static_cast<double*>(o.data)[g] = null ? 0.0 : s / (double)cnt;
-          break;
-        }
-        default: {  // MIN / MAX in the input type
-          const long long k = (long long)v;
-          if (a.type == YQ_INT32) static_cast<int32_t*>(o.data)[g] = null ? 0 : (int32_t)k;
-          else if (a.type == YQ_FLOAT32) static_cast<float*>(o.data)[g] = null ? 0.0f : (float)unordered(k);
-          else if (a.type == YQ_FLOAT64) static_cast<double*>(o.data)[g] = null ? 0.0 : unordered(k);
-          else static_cast<long long*>(o.data)[g] = null ? 0 : k;
-          break;
-        }
-      }
+    // fixed tree: lanes pairwise in index order, then warps in order
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const GPart o{__shfl_down_sync(0xffffffffu, acc.cnt, d), __shfl_down_sync(0xffffffffu, acc.v, d)};
+      if ((lane & (2 * d - 1)) == 0) acc = part_combine(a.kind, flt, acc, o);
     }
+    if (lane == 0) s_red[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      GPart tot = s_red[0];
+      for (int w = 1; w < kGroupThreads / 32; ++w) tot = part_combine(a.kind, flt, tot, s_red[w]);
+      part_write(a, P.out[j], g, tot);
+    }
+    __syncthreads();
+  }
 }
 
 int out_type(int32_t kind, int32_t in) {
@@ -230,14 +413,18 @@ extern "C" {
 
 size_t yq_group_by_workspace_size(const yq_column* key, uint32_t rows, int32_t nagg, uint32_t capacity) {
   if (!key) return 0;
+  const size_t tiles = ((size_t)rows + kGroupTile - 1) / kGroupTile + 1;
   WsSize w;
   w.add<uint8_t>(yq_sort_workspace_size(key, rows));
   w.add<uint32_t>((size_t)rows + 1);          // permutation
   w.add<uint8_t>((size_t)rows + 16);          // head flags
   w.add<uint32_t>((size_t)rows + 1);          // group of every sorted position
   w.add<uint8_t>(yq_prefix_sum_workspace_size(rows));
-  w.add<unsigned long long>((size_t)2 * (nagg > 0 ? nagg : 1) * ((size_t)capacity + 1));  // accumulators
-  w.add<yq_column>(YQ_MAX_AGGREGATES + 1);
+  w.add<uint32_t>((size_t)capacity + 2);      // group starts
+  w.add<unsigned long long>(tiles * 4 * (size_t)(nagg > 0 ? nagg : 1));  // tile head / tail records
+  w.add<uint32_t>(tiles);                     // tail group of every tile
+  w.add<uint32_t>(tiles);                     // tile flags
+  w.add<uint32_t>(4);                         // error word
   return w.total();
 }
 
@@ -254,6 +441,7 @@ int yq_group_by(const yq_batch* batch, int32_t key_col, const yq_group_agg* aggs
     return YQ_ERR_UNSUPPORTED;
   if (out[0].type != key.type || out[0].width != key.width || (rows && !out[0].data)) return YQ_ERR_INVALID_ARG;
   GroupParams P;
+  memset(&P, 0, sizeof(P));
   P.nagg = nagg;
   P.rows = rows;
   for (int j = 0; j < nagg; ++j) {
@@ -271,20 +459,25 @@ int yq_group_by(const yq_batch* batch, int32_t key_col, const yq_group_agg* aggs
     const yq_column& o = out[1 + j];
     if (o.type != ot || o.width != type_width(ot) || (rows && !o.data)) return YQ_ERR_INVALID_ARG;
     if (!o.nulls && g.kind != YQ_AGG_COUNT && g.kind != YQ_AGG_COUNT_STAR && rows) return YQ_ERR_INVALID_ARG;
-    P.a[j] = GAgg{in.data, in.nulls, it, g.kind, nullptr, nullptr};
+    P.a[j] = GAgg{in.data, in.nulls, it, g.kind};
+    P.out[j] = o;
   }
   if (rows == 0) return YQ_OK;
   cudaStream_t s = as_stream(stream);
   Workspace ws;
   YQ_TRY(ws.acquire(workspace, workspace_bytes, yq_group_by_workspace_size(&key, rows, nagg, capacity), s));
+  const uint32_t ntiles = (uint32_t)(((size_t)rows + kGroupTile - 1) / kGroupTile);
   const size_t sort_ws = yq_sort_workspace_size(&key, rows);
   void* d_sort = ws.take<uint8_t>(sort_ws);
   uint32_t* perm = ws.take<uint32_t>((size_t)rows + 1);
   uint8_t* head = ws.take<uint8_t>((size_t)rows + 16);
   uint32_t* incl = ws.take<uint32_t>((size_t)rows + 1);
   void* scan_ws = ws.take<uint8_t>(yq_prefix_sum_workspace_size(rows));
-  unsigned long long* acc = ws.take<unsigned long long>((size_t)2 * (nagg > 0 ? nagg : 1) * ((size_t)capacity + 1));
-  yq_column* out_dev = ws.take<yq_column>(YQ_MAX_AGGREGATES + 1);
+  uint32_t* starts = ws.take<uint32_t>((size_t)capacity + 2);
+  unsigned long long* rec = ws.take<unsigned long long>(((size_t)ntiles + 1) * 4 * (size_t)(nagg > 0 ? nagg : 1));
+  uint32_t* tail_group = ws.take<uint32_t>((size_t)ntiles + 1);
+  uint32_t* tile_flags = ws.take<uint32_t>((size_t)ntiles + 1);
+  uint32_t* d_err = ws.take<uint32_t>(4);
   yq_sort_config cfg{0, 0, 256, 1};  // every pass kept: no host read-back inside the sort
   YQ_TRY(yq_sort_indices(&key, rows, 0, 0, perm, &cfg, d_sort, sort_ws, stream));
   {
@@ -298,29 +491,34 @@ int yq_group_by(const yq_batch* batch, int32_t key_col, const yq_group_agg* aggs
   YQ_TRY_CUDA(cudaStreamSynchronize(s));
   *groups = G;
   if (G > capacity) return YQ_ERR_CAPACITY;
-  for (int j = 0; j < nagg; ++j) {
-    P.a[j].count = acc + (size_t)2 * j * ((size_t)capacity + 1);
-    P.a[j].value = P.a[j].count + capacity + 1;
-  }
   P.perm = perm;
   P.incl = incl;
-  YQ_TRY(h2d_async(out_dev, out, sizeof(yq_column) * (size_t)(nagg + 1), s));
+  P.starts = starts;
+  P.rec = rec;
+  P.tail_group = tail_group;
+  P.tile_flags = tile_flags;
+  P.err = d_err;
   k_group_keys<<<grid_for(rows, kGroupThreads), kGroupThreads, 0, s>>>(key, perm, rows, head, incl, out[0]);
   YQ_CHECK_LAUNCH();
   if (nagg) {
-    k_group_init<<<grid_for(G, kGroupThreads), kGroupThreads, 0, s>>>(P, G);
-    YQ_CHECK_LAUNCH();
-    double in_bytes = 4.0 * rows;
+    const uint32_t end_word[1] = {rows};
+    YQ_TRY(h2d_async(starts + G, end_word, sizeof(uint32_t), s));  // starts[G] = rows
+    YQ_TRY_CUDA(cudaMemsetAsync(tile_flags, 0, ((size_t)ntiles + 1) * sizeof(uint32_t), s));
+    YQ_TRY_CUDA(cudaMemsetAsync(d_err, 0, 4 * sizeof(uint32_t), s));
+    double in_bytes = 8.0 * rows;  // group index + permutation
     for (int j = 0; j < nagg; ++j)
       if (P.a[j].data) in_bytes += (double)rows * (type_width(P.a[j].type) + (P.a[j].nulls ? 1 : 0));
     {
       ProfScope ps("group_accumulate", s, in_bytes);
-      const uint64_t threads = ((uint64_t)rows + kGroupRun - 1) / kGroupRun;
-      k_group_accumulate<<<(unsigned)((threads + kGroupThreads - 1) / kGroupThreads), kGroupThreads, 0, s>>>(P);
+      k_group_tiles<<<ntiles, kGroupThreads, 0, s>>>(P);
+      YQ_CHECK_LAUNCH();
+      k_group_span<<<ntiles, kGroupThreads, 0, s>>>(P, ntiles);
       YQ_CHECK_LAUNCH();
     }
-    k_group_finalize<<<grid_for(G, kGroupThreads), kGroupThreads, 0, s>>>(P, G, out_dev);
-    YQ_CHECK_LAUNCH();
+    uint32_t err = 0;
+    YQ_TRY_CUDA(cudaMemcpyAsync(&err, d_err, sizeof(err), cudaMemcpyDeviceToHost, s));
+    YQ_TRY_CUDA(cudaStreamSynchronize(s));
+    if (err) return YQ_ERR_INVALID_ARG;
   }
   return YQ_OK;
 }

@@ -613,11 +613,7 @@ static int build_table(const yq_batch* right, const yq_program* pred, const yq_c
   B.hrows = hrows;
   B.counts = counts;
   const size_t smem = sizeof(uint32_t) * (nbuckets + kHashMaxRows + 40);
-  static size_t attr = 0;
-  if (smem > 48 * 1024 && smem > attr) {
-    YQ_TRY_CUDA(cudaFuncSetAttribute(k_hash_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = smem;
-  }
+  YQ_TRY(kernel_allow_smem((const void*)k_hash_build, smem));
   ProfScope ps("join_hash_build", s, (double)right->rows * right->columns[key_col].width);
   k_hash_build<<<1, kBuildBlock, smem, s>>>(B);
   YQ_CHECK_LAUNCH();
@@ -724,11 +720,7 @@ static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_
     J.nbuckets = nbuckets;
     J.hrows_n = J.R;
     const size_t smem = table_smem(nbuckets, J.R, true);
-    static size_t attr = 0;
-    if (smem > 48 * 1024 && smem > attr) {
-      YQ_TRY_CUDA(cudaFuncSetAttribute(k_join_hash, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr = smem;
-    }
+    YQ_TRY(kernel_allow_smem((const void*)k_join_hash, smem));
     ProfScope ps("join_hash_probe", s, (double)J.L * left->columns[conds[J.eq].left_col].width);
     k_join_hash<<<ntiles, kJoinBlock, smem, s>>>(J);
     YQ_CHECK_LAUNCH();
@@ -894,14 +886,8 @@ int yq_join_aggregate(const yq_batch* fact, const yq_program* fact_predicate, in
   F.table_off = (uint32_t)align_up(stage_smem_bytes(F.SP), 16);
   const size_t smem = F.table_off + table;
   const void* kern = staged ? (const void*)k_join_aggregate<true> : (const void*)k_join_aggregate<false>;
-  static size_t attr[2] = {0, 0};
-  if (smem > 48 * 1024 && smem > attr[staged]) {
-    YQ_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr[staged] = smem;
-  }
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kRowBlock, smem) != cudaSuccess || per_sm < 1)
-    per_sm = 1;
+  YQ_TRY(kernel_allow_smem(kern, smem));
+  int per_sm = kernel_blocks_per_sm(kern, kRowBlock, smem);
   if (per_sm > 8) per_sm = 8;
   const uint32_t tiles = ceil_div<uint32_t>(fact->rows, kStepRows);
   int grid = sm_count() * per_sm;

@@ -312,11 +312,7 @@ template <int KW>
 static int launch_merge(const MergeParams& M, cudaStream_t s, double bytes) {
   const int W = M.key.width;
   const size_t smem = (size_t)kMergeTile * 4 + 128 + (M.staged ? 2 * ((size_t)kMergeTile * W + 32) : 0);
-  static size_t attr = 0;
-  if (smem > 48 * 1024 && smem > attr) {
-    YQ_TRY_CUDA(cudaFuncSetAttribute(k_merge_tiles<KW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = smem;
-  }
+  YQ_TRY(kernel_allow_smem((const void*)k_merge_tiles<KW>, smem));
   {
     ProfScope ps("merge_partition", s, 0.0);
     k_merge_partition<KW><<<ceil_div<uint32_t>(M.ntiles, 128), 128, 0, s>>>(M);
@@ -674,20 +670,8 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
 template <int KW>
 static int launch_raw_level(const RawLevel& L, cudaStream_t s, double bytes) {
   using G = RawGeom<KW>;
-  static bool attr = false;
-  if (!attr) {
-    YQ_TRY_CUDA(cudaFuncSetAttribute(k_merge_raw_tiles<KW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem));
-    attr = true;
-  }
-  static int cap = 0;
-  if (!cap) {
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_merge_raw_tiles<KW>, kMergeBlock, G::smem) !=
-            cudaSuccess ||
-        per_sm < 1)
-      per_sm = 1;
-    cap = per_sm * sm_count();
-  }
+  YQ_TRY(kernel_allow_smem((const void*)k_merge_raw_tiles<KW>, G::smem));
+  const int cap = kernel_blocks_per_sm((const void*)k_merge_raw_tiles<KW>, kMergeBlock, G::smem) * sm_count();
   {
     ProfScope ps("merge_partition", s, 0.0);
     k_merge_raw_partition<KW><<<ceil_div<uint32_t>(L.ntiles, 128), 128, 0, s>>>(L);

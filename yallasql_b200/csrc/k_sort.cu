@@ -517,12 +517,7 @@ static size_t sweep_smem() {
 template <int KW, int D, int ITEMS>
 static int launch_sweep(const SweepParams& P, uint32_t ntiles, cudaStream_t s) {
   const size_t smem = sweep_smem<KW, D, ITEMS>();
-  static bool attr = false;
-  if (!attr) {
-    YQ_TRY_CUDA(cudaFuncSetAttribute(k_sort_onesweep<KW, D, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-    attr = true;
-  }
+  YQ_TRY(kernel_allow_smem((const void*)k_sort_onesweep<KW, D, ITEMS>, smem));
   k_sort_onesweep<KW, D, ITEMS><<<ntiles, kSortBlock, smem, s>>>(P);
   YQ_CHECK_LAUNCH();
   return YQ_OK;
@@ -533,11 +528,7 @@ static int launch_hist(const KeySrc& src, const SegInfo& seg, uint32_t tile_rows
                        cudaStream_t s) {
   constexpr int P = (KW * 32 + D - 1) / D;
   const size_t smem = sizeof(uint32_t) * P * (1 << D);
-  static bool attr = false;
-  if (!attr) {
-    YQ_TRY_CUDA(cudaFuncSetAttribute(k_sort_histogram<KW, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
+  YQ_TRY(kernel_allow_smem((const void*)k_sort_histogram<KW, D>, smem));
   int grid = sm_count() * 4;
   if ((uint32_t)grid > ntiles) grid = (int)ntiles;
   if (grid < 1) grid = 1;

@@ -3,6 +3,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 #include <stdio.h>
 #include <string.h>
@@ -130,15 +131,57 @@ void prof_end(cudaStream_t s) {
 }
 
 int sm_count() {
-  static int cached[64] = {0};
+  static std::atomic<int> cached[64] = {};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-  if (!cached[dev]) {
-    int v = 0;
+  int v = cached[dev].load(std::memory_order_relaxed);
+  if (!v) {
     if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
-    cached[dev] = v;
+    cached[dev].store(v, std::memory_order_relaxed);
   }
-  return cached[dev];
+  return v;
+}
+
+// ------------------------------------------------- per-device launch settings
+// cudaFuncSetAttribute applies to the current device only, and host threads
+// may launch concurrently: the shared-memory opt-in and the occupancy of each
+// kernel are kept per (device, kernel[, block, smem]) under one lock.
+namespace {
+std::mutex g_kattr_mu;
+std::map<std::pair<int, const void*>, size_t> g_kattr_smem;
+std::map<std::tuple<int, const void*, int, size_t>, int> g_kattr_blocks;
+}  // namespace
+
+int kernel_allow_smem(const void* kernel, size_t smem) {
+  if (smem <= 48 * 1024) return YQ_OK;
+  int dev = 0;
+  YQ_TRY_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_kattr_mu);
+  size_t& cap = g_kattr_smem[{dev, kernel}];
+  if (smem <= cap) return YQ_OK;  // the cap only rises: a smaller launch never lowers it
+  YQ_TRY_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  cap = smem;
+  return YQ_OK;
+}
+
+int kernel_blocks_per_sm(const void* kernel, int block, size_t smem) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 1;
+  }
+  if (kernel_allow_smem(kernel, smem) != YQ_OK) return 1;
+  std::lock_guard<std::mutex> lk(g_kattr_mu);
+  const auto key = std::make_tuple(dev, kernel, block, smem);
+  auto it = g_kattr_blocks.find(key);
+  if (it != g_kattr_blocks.end()) return it->second;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess || per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  g_kattr_blocks.emplace(key, per_sm);
+  return per_sm;
 }
 
 }  // namespace yq

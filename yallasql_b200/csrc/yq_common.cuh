@@ -78,6 +78,12 @@ int h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s);
 
 int sm_count();
 
+// Per-device, thread-safe launch settings (runtime.cu): raise `kernel`'s
+// dynamic shared-memory limit on the current device to at least `smem`, and
+// the number of `block`-thread blocks with `smem` bytes resident per SM (>= 1).
+int kernel_allow_smem(const void* kernel, size_t smem);
+int kernel_blocks_per_sm(const void* kernel, int block, size_t smem);
+
 #endif  // !__CUDACC_RTC__
 
 template <typename T>

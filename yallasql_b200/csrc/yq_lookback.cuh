@@ -28,13 +28,16 @@ constexpr int kLookbackWindow = 32 * kLookbackPerLane;
 
 // Called by all 32 lanes of one warp. Publishes `agg` for `tile`, walks back
 // over predecessors and returns the exclusive prefix of this tile (all lanes).
+// `limit` bounds the polls of one unpublished word (kSpinLimit unless a test
+// lowers it); running out sets kErrTimeout in *err.
 // Window position p (0 = nearest predecessor) is word base - p, read by lane
 // p / kLookbackPerLane. The walk waits while a word nearer than the nearest
 // inclusive one is unpublished; otherwise it adds the window's values up to
 // and including that inclusive word and stops, or adds the whole window and
 // moves it back.
 __device__ __forceinline__ unsigned long long tile_lookback(unsigned long long* status, uint32_t tile,
-                                                            unsigned long long agg, uint32_t* err) {
+                                                            unsigned long long agg, uint32_t* err,
+                                                            uint32_t limit = kSpinLimit) {
   const int lane = threadIdx.x & 31;
   if (tile == 0) {
     if (lane == 0) st_relaxed_u64(status, kFlagIncl | agg);
@@ -67,7 +70,7 @@ __device__ __forceinline__ unsigned long long tile_lookback(unsigned long long* 
     const int gi = il ? li * kLookbackPerLane + fi_at : kLookbackWindow;
     if (gz < gi) {
       // Give up at the bound, or early once another tile has already failed.
-      if (++spins > kSpinLimit || ((spins & 63u) == 0u && ld_relaxed_u32(err) != 0u)) {
+      if (++spins > limit || ((spins & 63u) == 0u && ld_relaxed_u32(err) != 0u)) {
         timed_out = true;
         break;
       }
