@@ -70,6 +70,19 @@ int yq_plan_aggregate(yq_plan* plan, int32_t child, const yq_agg_spec* aggs, int
                       const yq_constants* constants);
 int yq_plan_order(yq_plan* plan, int32_t child, int32_t key_col, int32_t descending,
                   int32_t nulls_first);
+/* ORDER BY several keys, most significant first (the reference sorts by
+ * `orders[0]` only, include/engine/operators/order_operator.hpp:277). One key
+ * takes the out-of-core merge path (yq_order_by); several keys, or a text key
+ * longer than 32 significant bytes, sort the whole input at once
+ * (yq_sort_indices_multi) and gather. */
+int yq_plan_order_multi(yq_plan* plan, int32_t child, const int32_t* keys, const int32_t* descending,
+                        const int32_t* nulls_first, int32_t nkeys);
+/* SELECT key, aggregates GROUP BY key (the reference's AggregateOperator
+ * ignores the groups, include/engine/operators/aggregate_operator.hpp:84-104):
+ * one output row per distinct key, ascending, NULL group last; columns = the
+ * key, then one per aggregate with yq_group_by's types (COUNT INT64, SUM of
+ * integers INT64, SUM of floats and AVG FLOAT64, MIN/MAX the input type). */
+int yq_plan_group_by(yq_plan* plan, int32_t child, int32_t key_col, const yq_group_agg* aggs, int32_t nagg);
 int yq_plan_join(yq_plan* plan, int32_t left, int32_t right, const yq_join_cond* conds,
                  int32_t ncond);
 int yq_plan_cross(yq_plan* plan, int32_t left, int32_t right);

@@ -522,7 +522,10 @@ int yq_move_rows_merge(const yq_column* a, const yq_column* b, const uint32_t* i
 int yq_reduce(const void* values, int32_t type, const uint8_t* nulls, uint32_t n,
               int32_t kind, void* result, void* stream);
 /* Order-preserving key transforms (src/kernels/radix_sort_utils.cu:4-53):
- * INT32 -> x ^ 0x80000000, FLOAT32 -> sign flip; inverse = 1 restores. */
+ * INT32 -> x ^ 0x80000000, FLOAT32 -> sign flip; inverse = 1 restores.
+ * INT64 / DATETIME -> x ^ 2^63 on each 64-bit value (dst holds two words per
+ * value): the signed order of the result is the unsigned order of x, the
+ * order the reference's sort gives int64 keys (radix_sort_kernel.cu:173). */
 int yq_key_transform(const void* src, int32_t type, uint32_t* dst, uint32_t n,
                      int32_t inverse, void* stream);
 /* launch_merge_sorted_array_kernel<T,Op> (include/kernels/merge_batchs.hpp:51):

@@ -97,3 +97,62 @@ def test_join_and_cross_product_queries(cuda):
     assert len(res2[0][0]) == 300 * 300
     np.testing.assert_array_equal(res2[0][0], np.repeat(x, 300))
     np.testing.assert_array_equal(res2[1][0], np.tile(y, 300))
+
+
+@pytest.mark.parametrize("batch_rows", [0, 7_000])
+def test_group_by_node(cuda, batch_rows):
+    """GROUP BY as an operator-tree node over scanned batches (the reference's
+    AggregateOperator ignores the groups): scan -> WHERE -> GROUP BY discount
+    with COUNT(*), SUM(price), AVG(qty), MIN(price), MAX(price), against the
+    oracle's GROUP BY of the filtered rows."""
+    rng = np.random.default_rng(31)
+    t, cols = sales_cols(300_001, seed=5)
+    pnull = rng.random(len(t["price"])) < 0.05
+    p = Plan()
+    scan = p.scan(cols, nulls=[pnull, None, None, None], batch_rows=batch_rows)
+    where = p.filter(scan, Compare(A.LT, ColumnRef(1, A.INT32), Constant(40, A.INT32)))
+    aggs = [(A.AGG_COUNT_STAR, 0), (A.AGG_SUM, 0), (A.AGG_AVG, 1), (A.AGG_MIN, 0), (A.AGG_MAX, 0)]
+    res = p.execute(p.group_by(where, 2, aggs))
+    keep = t["qty"] < 40
+    price, pn, qty, disc = t["price"][keep], pnull[keep], t["qty"][keep], t["discount"][keep]
+    okey, okn, ores = oracle.group_by(disc, None, A.INT32, [(0, None, None, 0), (2, price, pn, 1), (3, qty, None, 0),
+                                                            (4, price, pn, 1), (5, price, pn, 1)])
+    np.testing.assert_array_equal(res[0][0], okey)
+    for j, (w, wn) in enumerate(ores):
+        got, gn = res[1 + j]
+        if wn is None:
+            np.testing.assert_array_equal(got, w)
+            continue
+        np.testing.assert_array_equal(gn, wn)
+        if got.dtype == np.float64 and j in (1, 2):
+            np.testing.assert_allclose(np.where(wn, 0, got), np.where(wn, 0, w), rtol=1e-9)
+        else:
+            np.testing.assert_array_equal(np.where(wn, 0, got), np.where(wn, 0, w))
+
+
+@pytest.mark.parametrize("batch_rows", [0, 50_000])
+def test_order_by_several_keys_node(cuda, batch_rows):
+    """ORDER BY discount DESC, qty ASC, price DESC as one node (the reference
+    sorts by its first key only): stable, every column moved."""
+    t, cols = sales_cols(400_003, seed=6)
+    p = Plan()
+    root = p.order_multi(p.scan(cols, batch_rows=batch_rows), [2, 1, 0], [True, False, True])
+    res = p.execute(root)
+    perm = oracle.sort_perm_multi([t["discount"], t["qty"], t["price"]], [True, False, True])
+    for (got, _), want in zip(res, cols):
+        np.testing.assert_array_equal(got, want[perm])
+
+
+def test_order_by_long_text_key_node(cuda):
+    """One text key longer than the merge path's 32 bytes: the node sorts the
+    whole input by its chunked text key instead of merging runs."""
+    rng = np.random.default_rng(7)
+    n = 60_000
+    words = ["k" * int(rng.integers(20, 60)) + "".join(rng.choice(list("xyz"), 5)) for _ in range(n)]
+    txt = datagen.text_slots(words, 96)
+    ids = np.arange(n, dtype=np.int64)
+    p = Plan()
+    res = p.execute(p.order(p.scan([txt, ids], batch_rows=8_192), 0, descending=False))
+    perm = oracle.sort_perm(txt)
+    np.testing.assert_array_equal(res[1][0], ids[perm])
+    np.testing.assert_array_equal(res[0][0], txt[perm])

@@ -133,3 +133,25 @@ def test_large_sort_properties(cuda):
     # stability: among equal keys the row ids ascend
     eq = s[:-1] == s[1:]
     assert bool((perm[:-1][eq] < perm[1:][eq]).all())
+
+
+@pytest.mark.parametrize("width", [64, 256])
+@pytest.mark.parametrize("desc", [False, True])
+@pytest.mark.parametrize("with_nulls", [False, True])
+def test_long_text_keys_sort_in_chunks(cuda, width, desc, with_nulls):
+    """Text keys with more significant bytes than one pass carries (32, or 28
+    with a NULL word) sort as a chain of 32-byte chunk keys: values that agree
+    on their first 32..200 bytes still order by the bytes after them, NULLs
+    keep their input order."""
+    rng = np.random.default_rng(width + 2 * desc + with_nulls)
+    n = 50_000
+    prefix = "p" * (width - 24)
+    words = [prefix[: int(rng.integers(0, len(prefix) + 1))] + "".join(rng.choice(list("abc"), 6))
+             for _ in range(n)]
+    words = [w[: width - 1] for w in words]
+    k = datagen.text_slots(words, width)
+    nulls = (rng.random(n) < 0.1) if with_nulls else None
+    col = dev_col(k, A.TEXT, nulls)
+    perm = ops.sort_indices(col, descending=desc).cpu().numpy()
+    want = oracle.sort_perm(k, desc=desc, nulls=nulls)
+    np.testing.assert_array_equal(perm.astype(np.int64), want.astype(np.int64))

@@ -397,6 +397,15 @@ __global__ void k_key_transform(const uint32_t* __restrict__ src, int is_float, 
   }
 }
 
+// 64-bit integers (INT64 / DATETIME read as uint64 by the reference's sort,
+// radix_sort_kernel.cu:173): flipping the top bit maps signed order to
+// unsigned order and back.
+__global__ void k_key_transform64(const unsigned long long* __restrict__ src, unsigned long long* __restrict__ dst,
+                                  uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    dst[i] = src[i] ^ 0x8000000000000000ull;
+}
+
 // -------------------------------------------------------------- merge path
 // merge_sorted_array_kernel_v1 (merge_batchs.cu:33-77): compares raw values
 // (AscSortMergeOp / DescSortMergeOp), ties take A; emits keys, source index,
@@ -700,9 +709,17 @@ int yq_reduce(const void* values, int32_t type, const uint8_t* nulls, uint32_t n
 }
 
 int yq_key_transform(const void* src, int32_t type, uint32_t* dst, uint32_t n, int32_t inverse, void* stream) {
-  if (!src || !dst || (type != YQ_INT32 && type != YQ_FLOAT32)) return YQ_ERR_INVALID_ARG;
+  if (!src || !dst || (type != YQ_INT32 && type != YQ_FLOAT32 && type != YQ_INT64 && type != YQ_DATETIME))
+    return YQ_ERR_INVALID_ARG;
   if (n == 0) return YQ_OK;
   cudaStream_t s = as_stream(stream);
+  if (type == YQ_INT64 || type == YQ_DATETIME) {
+    ProfScope ps("elem_key_transform", s, (double)n * 16.0);
+    k_key_transform64<<<elem_grid(n, 4), kElemBlock, 0, s>>>((const unsigned long long*)src,
+                                                             reinterpret_cast<unsigned long long*>(dst), n);
+    YQ_CHECK_LAUNCH();
+    return YQ_OK;
+  }
   ProfScope ps("elem_key_transform", s, (double)n * 8.0);
   k_key_transform<<<elem_grid(n, 4), kElemBlock, 0, s>>>((const uint32_t*)src, type == YQ_FLOAT32, inverse, dst, n);
   YQ_CHECK_LAUNCH();

@@ -630,9 +630,9 @@ struct KeyPlan {
 // segment size (yq_sort_autotune), else 8-bit digits with the default items.
 // `sizing`: tile count for the variant with the fewest items (workspace bound).
 static int plan_key(const yq_column& c, int vwords_override, int want_d, int want_items, const uint32_t* seg_offsets,
-                    int nseg, KeyPlan& kp, bool sizing = false) {
+                    int nseg, KeyPlan& kp, bool sizing = false, int null_word_override = -1) {
   kp.sh.vwords = vwords_override >= 0 ? vwords_override : key_value_words(c);
-  kp.sh.null_word = c.nulls != nullptr;
+  kp.sh.null_word = null_word_override >= 0 ? null_word_override : c.nulls != nullptr;
   kp.sh.kw = round_kw(kp.sh.vwords + kp.sh.null_word);
   if (kp.sh.kw < 0) return YQ_ERR_UNSUPPORTED;
   kp.D = want_d;
@@ -777,8 +777,30 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
       vw = (int)tw;
       if (vw == 0 && !c.nulls) continue;  // every key equal: order unchanged
     }
+    // A text key longer than one pass's key (8 words, 7 with a NULL word) is
+    // sorted as a chain of chunk keys, its last chunk first (stable LSD over
+    // chunks): chunk 0 holds the leading words and the NULL word; NULL rows
+    // read as zero in the other chunks, so their order among themselves is
+    // kept. Every chunk reads the same slots at an offset (row stride = width).
+    const int lead = 8 - (c.nulls ? 1 : 0);
+    int nchunks = 1;
+    if (c.type == YQ_TEXT && vw > lead) {
+      if (keys_out) return YQ_ERR_UNSUPPORTED;  // merges carry one key of at most 8 words
+      nchunks = 1 + (vw - lead + 7) / 8;
+    }
+    for (int ch = nchunks - 1; ch >= 0; --ch) {
+    yq_column cc = c;
+    int cvw = vw;
+    int cnull = c.nulls != nullptr;
+    if (nchunks > 1) {
+      const int w0 = ch == 0 ? 0 : lead + (ch - 1) * 8;
+      const int w1 = ch == 0 ? lead : (w0 + 8 < vw ? w0 + 8 : vw);
+      cc.data = const_cast<char*>(static_cast<const char*>(c.data)) + 4 * w0;
+      cvw = w1 - w0;
+      cnull = (ch == 0 && c.nulls) ? 1 : 0;
+    }
     KeyPlan kp;
-    YQ_TRY(plan_key(c, vw, want_d, want_items, seg_offsets_host, nseg, kp));
+    YQ_TRY(plan_key(cc, cvw, want_d, want_items, seg_offsets_host, nseg, kp, false, cnull));
     SegPlan sp;
     plan_segments(seg_offsets_host, nseg, kp.tile_rows, sp);
     YQ_TRY(h2d_async(d_seg, sp.seg.data(), (nseg + 1) * sizeof(uint32_t), s));
@@ -788,7 +810,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
     YQ_TRY_CUDA(cudaMemsetAsync(d_misc, 0, 64 * sizeof(uint32_t), s));
 
     KeySrc src;
-    src.data = static_cast<const char*>(c.data);
+    src.data = static_cast<const char*>(cc.data);
     src.nulls = c.nulls;
     src.in_perm = perm_in;
     src.type = c.type;
@@ -900,6 +922,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
       YQ_TRY(kq.K.sweep(Sp, sp.ntiles, s));
     }
     perm_in = dst_perm;
+    }  // chunks of a long text key
   }
   if (perm_in != out_perm) {
     if (perm_in) {

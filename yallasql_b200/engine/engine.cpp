@@ -576,14 +576,57 @@ class AggregateOperator final : public Operator {
   Operator* source_ = nullptr;
 };
 
+// Every batch of `child` back to back in one device batch (the merge path and
+// the sort-based GROUP BY read contiguous rows); run r of the result is rows
+// [offs[r], offs[r+1]) and holds child batch r.
+static std::unique_ptr<Batch> collect_runs(Operator* child, CacheManager& cache, const std::vector<ColumnPtr>& columns,
+                                           cudaStream_t s, std::vector<uint32_t>& offs) {
+  std::vector<std::unique_ptr<Batch>> runs;
+  uint64_t total = 0;
+  bool nullable = false;
+  for (BatchID id = child->next(cache); id; id = child->next(cache)) {
+    auto b = cache.getBatch(id);
+    if (b->rows == 0) continue;
+    total += b->rows;
+    nullable |= has_nulls(*b);
+    runs.push_back(std::move(b));
+  }
+  offs.assign(1, 0u);
+  if (runs.empty()) return nullptr;
+  if (total > 0xffffffffull) throw Error(YQ_ERR_UNSUPPORTED, "more than 2^32 rows in one sorted table");
+  auto all = std::make_unique<Batch>(columns, total, s, nullable);
+  for (auto& r : runs) {
+    const uint64_t o = offs.back();
+    for (size_t c = 0; c < columns.size(); ++c) {
+      const size_t w = columns[c]->width;
+      check_cuda(cudaMemcpyAsync((char*)all->data[c] + o * w, r->data[c], r->rows * w, cudaMemcpyDeviceToDevice, s),
+                 "concat");
+      if (all->nulls[c]) {
+        if (r->nulls[c])
+          check_cuda(cudaMemcpyAsync(all->nulls[c] + o, r->nulls[c], r->rows, cudaMemcpyDeviceToDevice, s), "concat");
+        else
+          check_cuda(cudaMemsetAsync(all->nulls[c] + o, 0, r->rows, s), "concat");
+      }
+    }
+    offs.push_back((uint32_t)(o + r->rows));
+  }
+  return all;
+}
+
 // ----------------------------------------------------------- OrderOperator
 // Every child batch becomes a run; yq_order_by sorts the runs (segmented radix
 // sort), merges them pairwise by merge path until one remains and gathers the
 // rows (OrderOperator::firstPass / merge_all_sorted, order_operator.hpp:89-193).
+// The reference sorts by its first ORDER BY key only (`orders[0]`,
+// order_operator.hpp:277); here every key counts: with more than one key (or a
+// text key longer than the merge path's 32-byte key) the concatenated runs are
+// sorted at once by all keys (stable LSD over the keys, yq_sort_indices_multi)
+// and gathered.
 class OrderOperator final : public Operator {
  public:
-  OrderOperator(std::unique_ptr<Operator> child, int key, int desc, int nulls_first)
-      : key_(key), desc_(desc), nulls_first_(nulls_first) {
+  OrderOperator(std::unique_ptr<Operator> child, std::vector<int32_t> keys, std::vector<int32_t> desc,
+                std::vector<int32_t> nulls_first)
+      : keys_(std::move(keys)), desc_(std::move(desc)), nulls_first_(std::move(nulls_first)) {
     children_.push_back(std::move(child));
   }
   const char* kind() const override { return "order"; }
@@ -591,60 +634,112 @@ class OrderOperator final : public Operator {
     if (isInitialized_) return;
     children_[0]->init();
     columns = children_[0]->columns;
-    if (key_ < 0 || key_ >= (int)columns.size()) throw Error(YQ_ERR_INVALID_ARG, "OrderOperator key");
+    if (keys_.empty() || keys_.size() > YQ_MAX_BATCH_COLUMNS) throw Error(YQ_ERR_INVALID_ARG, "OrderOperator keys");
+    for (int k : keys_)
+      if (k < 0 || k >= (int)columns.size()) throw Error(YQ_ERR_INVALID_ARG, "OrderOperator key");
     isInitialized_ = true;
   }
   BatchID next(CacheManager& cache) override {
     if (!isInitialized_) init();
     if (isFinished) return 0;
     isFinished = true;
-    std::vector<std::unique_ptr<Batch>> runs;
-    uint64_t total = 0;
-    bool nullable = false;
-    for (BatchID id = children_[0]->next(cache); id; id = children_[0]->next(cache)) {
-      auto b = cache.getBatch(id);
-      if (b->rows == 0) continue;
-      total += b->rows;
-      nullable |= has_nulls(*b);
-      runs.push_back(std::move(b));
-    }
-    if (runs.empty()) return 0;
-    if (total > 0xffffffffull) throw Error(YQ_ERR_UNSUPPORTED, "OrderOperator: more than 2^32 rows");
     cudaStream_t s = ctx_->compute;
-    // gather the runs back to back (the merge path reads contiguous runs)
-    auto all = std::make_unique<Batch>(columns, total, s, nullable);
-    std::vector<uint32_t> offs{0};
-    for (auto& r : runs) {
-      const uint64_t o = offs.back();
-      for (size_t c = 0; c < columns.size(); ++c) {
-        const size_t w = columns[c]->width;
-        check_cuda(cudaMemcpyAsync((char*)all->data[c] + o * w, r->data[c], r->rows * w, cudaMemcpyDeviceToDevice, s),
-                   "order concat");
-        if (all->nulls[c]) {
-          if (r->nulls[c])
-            check_cuda(cudaMemcpyAsync(all->nulls[c] + o, r->nulls[c], r->rows, cudaMemcpyDeviceToDevice, s), "concat");
-          else
-            check_cuda(cudaMemsetAsync(all->nulls[c] + o, 0, r->rows, s), "concat");
-        }
-      }
-      offs.push_back((uint32_t)(o + r->rows));
-    }
-    runs.clear();
-    // Sort every run, merge the runs level by level as (key words, row id)
-    // pairs and gather every column once (yq_order_by).
+    std::vector<uint32_t> offs;
+    auto all = collect_runs(children_[0].get(), cache, columns, s, offs);
+    if (!all) return 0;
+    const uint64_t total = all->rows;
+    const bool nullable = has_nulls(*all);
     std::vector<yq_column> av, rv;
     all->view(av);
     auto result = std::make_unique<Batch>(columns, total, s, nullable);
     result->view(rv);
     yq_batch ib{av.data(), (int32_t)av.size(), (uint32_t)total};
     yq_batch ob{rv.data(), (int32_t)rv.size(), (uint32_t)total};
-    check(yq_order_by(&ib, key_, desc_, nulls_first_, offs.data(), (int32_t)offs.size() - 1, &ob, nullptr, 0, s),
-          "OrderOperator");
+    int st = YQ_ERR_UNSUPPORTED;
+    if (keys_.size() == 1)  // sort every run, merge (key words, row id) level by level, gather once
+      st = yq_order_by(&ib, keys_[0], desc_[0], nulls_first_[0], offs.data(), (int32_t)offs.size() - 1, &ob, nullptr,
+                       0, s);
+    if (st == YQ_ERR_UNSUPPORTED) {
+      std::vector<yq_column> kc;
+      for (int k : keys_) kc.push_back(av[k]);
+      uint32_t* perm = nullptr;
+      check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&perm), total * sizeof(uint32_t), s), "order perm");
+      st = yq_sort_indices_multi(kc.data(), desc_.data(), nulls_first_.data(), (int32_t)kc.size(), (uint32_t)total,
+                                 perm, nullptr, nullptr, 0, s);
+      if (st == YQ_OK) st = yq_gather(av.data(), (int32_t)av.size(), perm, (uint32_t)total, rv.data(), s);
+      cudaFreeAsync(perm, s);
+    }
+    check(st, "OrderOperator");
     return cache.putBatch(std::move(result));
   }
 
  private:
-  int key_, desc_, nulls_first_;
+  std::vector<int32_t> keys_, desc_, nulls_first_;
+};
+
+// --------------------------------------------------------- GroupByOperator
+// SELECT key, aggregates ... GROUP BY key. The reference's AggregateOperator
+// ignores the groups and folds every row into one result
+// (include/engine/operators/aggregate_operator.hpp:84-104); this operator
+// returns one row per distinct key in ascending key order (NULL group last)
+// with SQL aggregate semantics (yq_group_by): the child's batches are
+// concatenated and grouped in one call.
+class GroupByOperator final : public Operator {
+ public:
+  GroupByOperator(std::unique_ptr<Operator> child, int key, const yq_group_agg* aggs, int nagg)
+      : key_(key), aggs_(aggs, aggs + nagg) {
+    children_.push_back(std::move(child));
+  }
+  const char* kind() const override { return "group_by"; }
+  void init() override {
+    if (isInitialized_) return;
+    children_[0]->init();
+    const auto& in = children_[0]->columns;
+    if (key_ < 0 || key_ >= (int)in.size() || aggs_.size() > YQ_MAX_AGGREGATES)
+      throw Error(YQ_ERR_INVALID_ARG, "GroupByOperator");
+    columns.push_back(in[key_]);
+    for (const auto& a : aggs_) {
+      if (a.kind != YQ_AGG_COUNT_STAR && (a.column < 0 || a.column >= (int)in.size()))
+        throw Error(YQ_ERR_INVALID_ARG, "GroupByOperator aggregate column");
+      const int32_t it = a.kind == YQ_AGG_COUNT_STAR ? YQ_INT64 : in[a.column]->type;
+      int32_t t;
+      switch (a.kind) {
+        case YQ_AGG_COUNT_STAR:
+        case YQ_AGG_COUNT: t = YQ_INT64; break;
+        case YQ_AGG_AVG: t = YQ_FLOAT64; break;
+        case YQ_AGG_SUM: t = (it == YQ_FLOAT32 || it == YQ_FLOAT64) ? YQ_FLOAT64 : YQ_INT64; break;
+        default: t = it;
+      }
+      columns.push_back(std::make_shared<Column>(Column{t, width_of(t)}));
+    }
+    isInitialized_ = true;
+  }
+  BatchID next(CacheManager& cache) override {
+    if (!isInitialized_) init();
+    if (isFinished) return 0;
+    isFinished = true;
+    cudaStream_t s = ctx_->compute;
+    std::vector<uint32_t> offs;
+    auto all = collect_runs(children_[0].get(), cache, children_[0]->columns, s, offs);
+    if (!all) return 0;
+    const uint64_t total = all->rows;
+    std::vector<yq_column> av, rv;
+    all->view(av);
+    // at most one group per row: outputs sized for every row, trimmed to the group count
+    auto result = std::make_unique<Batch>(columns, total, s, true);
+    result->view(rv);
+    yq_batch ib{av.data(), (int32_t)av.size(), (uint32_t)total};
+    uint32_t groups = 0;
+    check(yq_group_by(&ib, key_, aggs_.data(), (int32_t)aggs_.size(), rv.data(), (uint32_t)total, &groups, nullptr, 0,
+                      s),
+          "GroupByOperator");
+    result->rows = groups;
+    return cache.putBatch(std::move(result));
+  }
+
+ private:
+  int key_;
+  std::vector<yq_group_agg> aggs_;
 };
 
 // ---------------------------------------- JoinOperator / CrossProductOperator
@@ -839,7 +934,28 @@ int yq_plan_aggregate(yq_plan* p, int32_t child, const yq_agg_spec* aggs, int32_
 
 int yq_plan_order(yq_plan* p, int32_t child, int32_t key, int32_t desc, int32_t nulls_first) {
   if (!p) return -YQ_ERR_INVALID_ARG;
-  return guarded([&] { return add(p, std::make_unique<OrderOperator>(take(p, child), key, desc, nulls_first)); });
+  return guarded([&] {
+    return add(p, std::make_unique<OrderOperator>(take(p, child), std::vector<int32_t>{key},
+                                                  std::vector<int32_t>{desc != 0}, std::vector<int32_t>{nulls_first != 0}));
+  });
+}
+
+int yq_plan_order_multi(yq_plan* p, int32_t child, const int32_t* keys, const int32_t* descending,
+                        const int32_t* nulls_first, int32_t nkeys) {
+  if (!p || !keys || nkeys <= 0 || nkeys > YQ_MAX_BATCH_COLUMNS) return -YQ_ERR_INVALID_ARG;
+  return guarded([&] {
+    std::vector<int32_t> k(keys, keys + nkeys), d(nkeys, 0), nf(nkeys, 0);
+    for (int i = 0; i < nkeys; ++i) {
+      d[i] = descending ? descending[i] != 0 : 0;
+      nf[i] = nulls_first ? nulls_first[i] != 0 : 0;
+    }
+    return add(p, std::make_unique<OrderOperator>(take(p, child), k, d, nf));
+  });
+}
+
+int yq_plan_group_by(yq_plan* p, int32_t child, int32_t key_col, const yq_group_agg* aggs, int32_t nagg) {
+  if (!p || nagg < 0 || nagg > YQ_MAX_AGGREGATES || (nagg && !aggs)) return -YQ_ERR_INVALID_ARG;
+  return guarded([&] { return add(p, std::make_unique<GroupByOperator>(take(p, child), key_col, aggs, nagg)); });
 }
 
 int yq_plan_join(yq_plan* p, int32_t left, int32_t right, const yq_join_cond* conds, int32_t ncond) {

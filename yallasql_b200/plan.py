@@ -43,6 +43,9 @@ PROTOTYPES = {
     "yq_plan_aggregate": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(A.AggSpec), C.c_int32,
                                     C.POINTER(A.Constants)]),
     "yq_plan_order": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "yq_plan_order_multi": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                      C.POINTER(C.c_int32), C.c_int32]),
+    "yq_plan_group_by": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(A.GroupAgg), C.c_int32]),
     "yq_plan_join": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(A.JoinCond), C.c_int32]),
     "yq_plan_cross": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "yq_plan_execute": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
@@ -197,6 +200,26 @@ class Plan:
     def order(self, child: int, key: int, descending=False, nulls_first=False):
         n = _node(lib().yq_plan_order(self.h, child, key, int(descending), int(nulls_first)), "yq_plan_order")
         self.types[n] = self.types[child]
+        return n
+
+    def order_multi(self, child: int, keys: list[int], descending: list[bool], nulls_first: list[bool] | None = None):
+        """ORDER BY several keys, most significant first."""
+        k = (C.c_int32 * len(keys))(*keys)
+        d = (C.c_int32 * len(keys))(*[int(x) for x in descending])
+        nf = (C.c_int32 * len(keys))(*[int(x) for x in (nulls_first or [False] * len(keys))])
+        self._keep += [k, d, nf]
+        n = _node(lib().yq_plan_order_multi(self.h, child, k, d, nf, len(keys)), "yq_plan_order_multi")
+        self.types[n] = self.types[child]
+        return n
+
+    def group_by(self, child: int, key: int, aggs: list[tuple[int, int]]):
+        """SELECT key, aggs GROUP BY key; aggs are (yq_agg_kind, input column)."""
+        from .ops import group_by_out_type
+        arr = (A.GroupAgg * max(1, len(aggs)))(*[A.GroupAgg(k, c) for k, c in aggs])
+        self._keep.append(arr)
+        n = _node(lib().yq_plan_group_by(self.h, child, key, arr, len(aggs)), "yq_plan_group_by")
+        ct = self.types[child]
+        self.types[n] = [ct[key]] + [group_by_out_type(k, A.INT64 if k == A.AGG_COUNT_STAR else ct[c]) for k, c in aggs]
         return n
 
     def join(self, left: int, right: int, conds: list):

@@ -5,6 +5,7 @@
     python -m yallasql_b200.profile_cases order    # 16M rows (key f32, id, 16-byte txt, date), 116,480-row runs
     python -m yallasql_b200.profile_cases cross    # 20K x 20K cross product with < (198M output pairs)
     python -m yallasql_b200.profile_cases csv      # 4M-row sales table as CSV text (~205 MB): index + parse + write
+    python -m yallasql_b200.profile_cases group    # 16M sales rows GROUP BY discount: COUNT(*), SUM, AVG, MIN, MAX
 
 An optional second argument sets the row count (rows per side for cross).
 
@@ -85,7 +86,16 @@ def csv_case(rows: int = 4_000_000) -> None:
     torch.cuda.synchronize()
 
 
-CASES = {"filter": filter_case, "join": join_case, "order": order_case, "cross": cross_case, "csv": csv_case}
+def group_case(rows: int = 16_000_000) -> None:
+    t = datagen.sales_table(rows, seed=0)
+    b = ops.DeviceBatch([_dev(t["discount"], A.INT32), _dev(t["price"], A.FLOAT32), _dev(t["qty"], A.INT32)])
+    ops.group_by(b, 0, [(A.AGG_COUNT_STAR, 0), (A.AGG_SUM, 1), (A.AGG_AVG, 2), (A.AGG_MIN, 1), (A.AGG_MAX, 1)],
+                 capacity=64)
+    torch.cuda.synchronize()
+
+
+CASES = {"filter": filter_case, "join": join_case, "order": order_case, "cross": cross_case, "csv": csv_case,
+         "group": group_case}
 
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "filter"
