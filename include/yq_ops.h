@@ -399,6 +399,13 @@ size_t yq_order_by_segments_workspace_size(const yq_column* key, uint32_t rows, 
 int yq_order_by_segments(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
                          const uint32_t* seg_offsets, int32_t nseg, yq_batch* out, const yq_sort_config* config,
                          void* workspace, size_t workspace_bytes, void* stream);
+/* The same, writing the permutation it gathers by into `perm_out` (`rows`
+ * device words): a host that keeps it can serve a repeat of the query with
+ * yq_gather alone (the serving loop keeps it as a resident intermediate). */
+int yq_order_by_segments_perm(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
+                              const uint32_t* seg_offsets, int32_t nseg, yq_batch* out, uint32_t* perm_out,
+                              const yq_sort_config* config, void* workspace, size_t workspace_bytes,
+                              void* stream);
 int yq_sort_autotune(const yq_column* key, uint32_t rows, const uint32_t* seg_offsets, int32_t nseg,
                      int32_t descending, yq_sort_config* best, void* stream);
 
@@ -456,6 +463,26 @@ int yq_join_aggregate(const yq_batch* fact, const yq_program* fact_predicate,
                       const yq_constants* constants, const yq_agg_spec* aggs,
                       int32_t nagg, void* state, void* workspace,
                       size_t workspace_bytes, void* stream);
+
+/* The same join against a dimension table prepared once and kept resident:
+ * yq_join_dim_table_build hashes the rows of `dim` that pass `dim_predicate`
+ * on `dim_key` into `table` (yq_join_dim_table_size bytes of device memory),
+ * waits for it once and writes the number of rows it kept to *kept (host);
+ * YQ_ERR_UNSUPPORTED when kept keys repeat. yq_join_aggregate_prepared then
+ * probes that table from the fact side with no host synchronisation (the
+ * reference rebuilds nothing either: it nests loops over every batch pair,
+ * join_operator.hpp:36-100); `dim_rows`, `kept` and `key_type` are those of
+ * the build. The table must stay valid while calls that read it run. */
+size_t yq_join_dim_table_size(uint32_t dim_rows);
+int yq_join_dim_table_build(const yq_batch* dim, const yq_program* dim_predicate, int32_t dim_key,
+                            const yq_constants* constants, void* table, size_t table_bytes,
+                            uint32_t* kept, void* stream);
+size_t yq_join_aggregate_prepared_workspace_size(int32_t nagg);
+int yq_join_aggregate_prepared(const yq_batch* fact, const yq_program* fact_predicate,
+                               int32_t fact_key, const void* table, uint32_t dim_rows,
+                               uint32_t kept, int32_t key_type, const yq_constants* constants,
+                               const yq_agg_spec* aggs, int32_t nagg, void* state,
+                               void* workspace, size_t workspace_bytes, void* stream);
 
 /* ====================================================================
  * Reference-compatible element kernels: one entry per YallaSQL::Kernel::launch_*

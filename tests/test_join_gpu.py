@@ -161,3 +161,28 @@ def test_star_join_rejects_repeated_dimension_keys(cuda):
     with pytest.raises(A.YQError) as e:
         plan.run(fb, db, ops.AggState(aggs))
     assert e.value.status == A.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("rows", [1, 4097, 3_000_000])
+def test_star_join_prepared_dimension(cuda, rows):
+    """The dimension side built once (yq_join_dim_table_build) and probed by
+    several aggregates with no host synchronisation: the same result as the
+    one-call join and the oracle, on every repetition."""
+    fact, dim = datagen.star_tables(rows, seed=3)
+    fb = dev_batch([fact["datekey"], fact["quantity"], fact["discount"], fact["extendedprice"]])
+    db = dev_batch([dim["datekey"], dim["year"], dim["month"]])
+    fp, dp, aggs = star_exprs(1994)
+    plan = ops.JoinAggPlan([A.INT32, A.INT32, A.INT32, A.FLOAT32], [A.INT32] * 3, fp, 0, dp, 0, aggs)
+    prep = plan.prepare(db)
+    assert prep.kept == int((dim["year"] == 1994).sum())
+    s, c = oracle.star_query(fact, dim, 1994)
+    one = ops.AggState(aggs)
+    plan.run(fb, db, one)
+    want = one.read()
+    for _ in range(3):
+        st = ops.AggState(aggs)
+        plan.run_prepared(fb, prep, st)
+        got = st.read()
+        assert got[1] == c == want[1]
+        assert rel_close(got[0], want[0], 1e-9) or (c == 0 and got[0] is None)
+        assert rel_close(got[0], s if c else None, 1e-6) or (c == 0 and got[0] is None)

@@ -23,15 +23,19 @@ def close(a, b):
     return a == b
 
 
+@pytest.mark.parametrize("share", [True, False])
 @pytest.mark.parametrize("rate", [0.0, 2000.0])
-def test_results_same_alone_and_in_mix(cuda, rate):
+def test_results_same_alone_and_in_mix(cuda, rate, share):
+    """With `share`, identical pending requests ride on one dispatch, filter
+    requests on one table share a scan and ORDER BY reuses a table's resident
+    permutation: every request's result is still the one it gets alone."""
     cat = serving.Catalog(ntables=4, lo=1_000, hi=200_000, seed=4)
     plans = serving.Plans()
     trace = serving.make_trace(80, rate, cat, seed=4)
     alone = copy.deepcopy(trace)
     serving.serve_plain(alone, cat, plans, keep=True)
     mixed = copy.deepcopy(trace)
-    stats = serving.serve_continuous(mixed, cat, plans, slots=4, keep=True)
+    stats = serving.serve_continuous(mixed, cat, plans, slots=4, keep=True, share=share)
     assert stats["queries"] == len(trace)
     seen = set()
     for a, m in zip(alone, mixed):

@@ -138,6 +138,8 @@ PROTOTYPES = {
                                               i32, vp, vp, sz, vp]),
     "yq_order_by_segments_workspace_size": (sz, [P(Column), u32, P(u32), i32]),
     "yq_order_by_segments": (C.c_int, [P(Batch), i32, i32, i32, P(u32), i32, P(Batch), P(SortConfig), vp, sz, vp]),
+    "yq_order_by_segments_perm": (C.c_int, [P(Batch), i32, i32, i32, P(u32), i32, P(Batch), vp, P(SortConfig), vp,
+                                            sz, vp]),
     "yq_sort_autotune": (C.c_int, [P(Column), u32, P(u32), i32, i32, P(SortConfig), vp]),
     "yq_order_by": (C.c_int, [P(Batch), i32, i32, i32, P(u32), i32, P(Batch), vp, sz, vp]),
     "yq_join_workspace_size": (sz, [u32, u32]),
@@ -145,6 +147,11 @@ PROTOTYPES = {
     "yq_join_project": (C.c_int, [P(Batch), P(Batch), P(JoinCond), i32, P(JoinOutput), i32, P(Column), u64,
                                   P(u64), vp, sz, vp]),
     "yq_join_aggregate_workspace_size": (sz, [u32, u32, i32]),
+    "yq_join_dim_table_size": (sz, [u32]),
+    "yq_join_dim_table_build": (C.c_int, [P(Batch), P(Program), i32, P(Constants), vp, sz, P(u32), vp]),
+    "yq_join_aggregate_prepared_workspace_size": (sz, [i32]),
+    "yq_join_aggregate_prepared": (C.c_int, [P(Batch), P(Program), i32, vp, u32, u32, i32, P(Constants),
+                                             P(AggSpec), i32, vp, vp, sz, vp]),
     "yq_join_aggregate": (C.c_int, [P(Batch), P(Program), i32, P(Batch), P(Program), i32, P(Constants),
                                     P(AggSpec), i32, vp, vp, sz, vp]),
     "yq_compare": (C.c_int, [Operand, Operand, i32, i32, vp, u32, vp]),

@@ -492,8 +492,7 @@ int yq_csv_index(const uint8_t* data, uint64_t nbytes, uint32_t* record_starts, 
     YQ_CHECK_LAUNCH();
   }
   unsigned long long h = 0;
-  YQ_TRY_CUDA(cudaMemcpyAsync(&h, total, sizeof(h), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  YQ_TRY(d2h_sync(&h, total, sizeof(h), s));
   *records = h;
   if (h > capacity) return YQ_ERR_CAPACITY;
   if (!record_starts) return h ? YQ_ERR_INVALID_ARG : YQ_OK;
@@ -566,8 +565,7 @@ int yq_csv_parse(const uint8_t* data, uint64_t nbytes, const uint32_t* record_st
     YQ_CHECK_LAUNCH();
   }
   unsigned long long h[3];
-  YQ_TRY_CUDA(cudaMemcpyAsync(h, P.counters, sizeof(h), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  YQ_TRY(d2h_sync(h, P.counters, sizeof(h), s));
   const unsigned long long invalid = h[0];
   if (invalid) {
     // rare path: drop the rows with a different field count, keeping order
@@ -595,8 +593,7 @@ int yq_csv_parse(const uint8_t* data, uint64_t nbytes, const uint32_t* record_st
       uint32_t first = (uint32_t)(h[2] >> 12);  // record index of the first bad cell
       if (invalid) {                           // -> its output row once dropped rows are gone
         uint32_t p = 0;
-        YQ_TRY_CUDA(cudaMemcpyAsync(&p, pos + first, sizeof(p), cudaMemcpyDeviceToHost, s));
-        YQ_TRY_CUDA(cudaStreamSynchronize(s));
+        YQ_TRY(d2h_sync(&p, pos + first, sizeof(p), s));
         first = p - 1;
       }
       *error = yq_csv_error{h[1], first, (int32_t)((h[2] >> 2) & 1023), (int32_t)(h[2] & 3)};
@@ -653,8 +650,7 @@ int yq_csv_format(const yq_batch* batch, uint8_t* out, uint64_t capacity, uint64
   }
   YQ_TRY(yq_prefix_sum_u32(P.len, end, rows, scan_ws, yq_prefix_sum_workspace_size(rows), stream));
   uint32_t total = 0;
-  YQ_TRY_CUDA(cudaMemcpyAsync(&total, end + rows - 1, sizeof(total), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  YQ_TRY(d2h_sync(&total, end + rows - 1, sizeof(total), s));
   *bytes = total;
   if (total > capacity) return YQ_ERR_CAPACITY;
   if (!out) return YQ_ERR_INVALID_ARG;

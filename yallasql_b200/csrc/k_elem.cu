@@ -800,8 +800,7 @@ extern "C" int yq_debug_lookback_stall(uint32_t spin_limit, void* workspace, siz
   k_debug_lookback_stall<<<1, 32, 0, s>>>(status, err, spin_limit, excl);
   YQ_CHECK_LAUNCH();
   uint32_t e = 0;
-  YQ_TRY_CUDA(cudaMemcpyAsync(&e, err, sizeof(e), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  YQ_TRY(d2h_sync(&e, err, sizeof(e), s));
   return (e & kErrTimeout) ? YQ_ERR_TIMEOUT : YQ_OK;
 }
 

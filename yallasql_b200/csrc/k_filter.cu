@@ -354,9 +354,7 @@ int yq_agg_state_read(const void* state, const yq_agg_spec* aggs, int32_t nagg, 
   YQ_TRY(check_aggs(aggs, nagg));
   Acc host[YQ_MAX_AGGREGATES + 1];
   cudaStream_t s = as_stream(stream);
-  YQ_TRY_CUDA(
-      cudaMemcpyAsync(host, state, sizeof(Acc) * YQ_MAX_AGGREGATES + sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  YQ_TRY(d2h_sync(host, state, sizeof(Acc) * YQ_MAX_AGGREGATES + sizeof(uint32_t), s));
   if (*agg_state_err(host)) return YQ_ERR_TIMEOUT;
   for (int a = 0; a < nagg; ++a) {
     const Acc& h = host[a];
@@ -409,8 +407,7 @@ int yq_agg_states_read(const void* states, int32_t count, const yq_agg_spec* agg
   if (count == 0) return YQ_OK;
   std::vector<char> host((size_t)count * kAggStateBytes);
   cudaStream_t s = as_stream(stream);
-  YQ_TRY_CUDA(cudaMemcpyAsync(host.data(), states, host.size(), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  YQ_TRY(d2h_sync(host.data(), states, host.size(), s));
   int status = YQ_OK;
   for (int g = 0; g < count; ++g) {
     Acc* st = reinterpret_cast<Acc*>(host.data() + (size_t)g * kAggStateBytes);
@@ -578,9 +575,8 @@ int yq_filter_project(const yq_batch* batch, const yq_program* predicate, const 
   YQ_TRY(launch_filter_project(F, rows, misc, status, cnt_dev, s));
   if (count_host) {
     uint32_t h[2];
-    YQ_TRY_CUDA(cudaMemcpyAsync(&h[0], cnt_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    YQ_TRY_CUDA(cudaMemcpyAsync(&h[1], misc + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    YQ_TRY_CUDA(cudaStreamSynchronize(s));
+    YQ_TRY(d2h_sync(&h[0], cnt_dev, sizeof(uint32_t), s));
+    YQ_TRY(d2h_sync(&h[1], misc + 1, sizeof(uint32_t), s));
     *count_host = h[0];
     if (h[1] & kErrTimeout) return YQ_ERR_TIMEOUT;
     if (h[0] > capacity) return YQ_ERR_CAPACITY;

@@ -487,8 +487,7 @@ int yq_group_by(const yq_batch* batch, int32_t key_col, const yq_group_agg* aggs
   }
   YQ_TRY(yq_prefix_sum_mask(head, incl, rows, scan_ws, yq_prefix_sum_workspace_size(rows), stream));
   uint32_t G = 0;
-  YQ_TRY_CUDA(cudaMemcpyAsync(&G, incl + rows - 1, sizeof(G), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  YQ_TRY(d2h_sync(&G, incl + rows - 1, sizeof(G), s));
   *groups = G;
   if (G > capacity) return YQ_ERR_CAPACITY;
   P.perm = perm;
@@ -516,8 +515,7 @@ int yq_group_by(const yq_batch* batch, int32_t key_col, const yq_group_agg* aggs
       YQ_CHECK_LAUNCH();
     }
     uint32_t err = 0;
-    YQ_TRY_CUDA(cudaMemcpyAsync(&err, d_err, sizeof(err), cudaMemcpyDeviceToHost, s));
-    YQ_TRY_CUDA(cudaStreamSynchronize(s));
+    YQ_TRY(d2h_sync(&err, d_err, sizeof(err), s));
     if (err) return YQ_ERR_INVALID_ARG;
   }
   return YQ_OK;

@@ -745,9 +745,8 @@ static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_
   }
   unsigned long long h_total = 0;
   uint32_t h_err = 0;
-  YQ_TRY_CUDA(cudaMemcpyAsync(&h_total, J.total, sizeof(h_total), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaMemcpyAsync(&h_err, J.err, sizeof(h_err), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  YQ_TRY(d2h_sync(&h_total, J.total, sizeof(h_total), s));
+  YQ_TRY(d2h_sync(&h_err, J.err, sizeof(h_err), s));
   if (count_host) *count_host = h_total;
   if (h_err & kErrTimeout) return YQ_ERR_TIMEOUT;
   return h_total > capacity ? YQ_ERR_CAPACITY : YQ_OK;
@@ -800,19 +799,12 @@ size_t yq_join_aggregate_workspace_size(uint32_t fact_rows, uint32_t dim_rows, i
   return w.total();
 }
 
-int yq_join_aggregate(const yq_batch* fact, const yq_program* fact_predicate, int32_t fact_key, const yq_batch* dim,
-                      const yq_program* dim_predicate, int32_t dim_key, const yq_constants* constants,
-                      const yq_agg_spec* aggs, int32_t nagg, void* state, void* workspace, size_t workspace_bytes,
-                      void* stream) {
-  if (!fact || !dim || !state || fact_key < 0 || fact_key >= fact->ncols || dim_key < 0 || dim_key >= dim->ncols ||
-      nagg < 0 || nagg > YQ_MAX_AGGREGATES || (nagg > 0 && !aggs))
-    return YQ_ERR_INVALID_ARG;
-  const yq_column& fk = fact->columns[fact_key];
-  const yq_column& dk = dim->columns[dim_key];
-  if (!join_col_ok(fk) || !join_col_ok(dk) || fk.type != dk.type || !hashable(fk.type)) return YQ_ERR_INVALID_ARG;
-  if (dim->rows > kHashMaxRows) return YQ_ERR_UNSUPPORTED;
-  cudaStream_t s = as_stream(stream);
-  JAParams F;
+}  // extern "C"
+
+// The fact side of a star-join aggregate: predicate and aggregate inputs as
+// one program over the fact columns.
+static int join_agg_params(const yq_batch* fact, const yq_program* fact_predicate, int32_t fact_key,
+                           const yq_constants* constants, const yq_agg_spec* aggs, int32_t nagg, JAParams& F) {
   memset(&F, 0, sizeof(F));
   {
     ProgramBuilder B;
@@ -853,22 +845,16 @@ int yq_join_aggregate(const yq_batch* fact, const yq_program* fact_predicate, in
     F.pc_end = B.len;
     F.A.nagg = nagg;
   }
-  if (fact->rows == 0 || nagg == 0) return YQ_OK;
-  const uint32_t nbuckets = pow2_at_least(dim->rows ? dim->rows : 1);
-  Workspace ws;
-  YQ_TRY(ws.acquire(workspace, workspace_bytes, yq_join_aggregate_workspace_size(fact->rows, dim->rows, nagg), s));
-  uint32_t* d_bstart = ws.take<uint32_t>(nbuckets + 1);
-  unsigned long long* d_hkeys = ws.take<unsigned long long>(dim->rows ? dim->rows : 1);
-  uint32_t* d_hrows = ws.take<uint32_t>(dim->rows ? dim->rows : 1);
-  uint32_t* d_misc = ws.take<uint32_t>(8);  // [0] ticket [2] kept rows [3] duplicate keys
+  return YQ_OK;
+}
+
+// Probe launch over a built dimension table (nbuckets buckets, `kept` rows).
+static int join_agg_launch(JAParams& F, const yq_batch* fact, int32_t fact_key, uint32_t nbuckets, uint32_t kept,
+                           uint32_t* d_bstart, unsigned long long* d_hkeys, Acc* partials, uint32_t* d_misc,
+                           void* state, cudaStream_t s) {
+  const yq_column& fk = fact->columns[fact_key];
   const int grid_cap = sm_count() * 8;
-  Acc* partials = ws.take<Acc>((size_t)grid_cap * YQ_MAX_AGGREGATES);
-  YQ_TRY_CUDA(cudaMemsetAsync(d_misc, 0, 8 * sizeof(uint32_t), s));
-  YQ_TRY(build_table(dim, dim_predicate, constants, dim_key, nbuckets, d_bstart, d_hkeys, d_hrows, d_misc + 2, s));
-  uint32_t counts[2] = {0, 0};
-  YQ_TRY_CUDA(cudaMemcpyAsync(counts, d_misc + 2, sizeof(counts), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaStreamSynchronize(s));
-  if (counts[1] != 0) return YQ_ERR_UNSUPPORTED;  // dimension keys repeat: use yq_join_pairs + an aggregate
+  const uint32_t counts[1] = {kept};
   F.fkey = jcol(fk);
   F.nbuckets = nbuckets;
   F.hrows_n = counts[0];
@@ -913,6 +899,118 @@ int yq_join_aggregate(const yq_batch* fact, const yq_program* fact_predicate, in
     k_join_aggregate<false><<<grid, kRowBlock, smem, s>>>(F, fact->rows, partials, d_misc, static_cast<Acc*>(state));
   YQ_CHECK_LAUNCH();
   return YQ_OK;
+}
+
+
+extern "C" {
+
+int yq_join_aggregate(const yq_batch* fact, const yq_program* fact_predicate, int32_t fact_key, const yq_batch* dim,
+                      const yq_program* dim_predicate, int32_t dim_key, const yq_constants* constants,
+                      const yq_agg_spec* aggs, int32_t nagg, void* state, void* workspace, size_t workspace_bytes,
+                      void* stream) {
+  if (!fact || !dim || !state || fact_key < 0 || fact_key >= fact->ncols || dim_key < 0 || dim_key >= dim->ncols ||
+      nagg < 0 || nagg > YQ_MAX_AGGREGATES || (nagg > 0 && !aggs))
+    return YQ_ERR_INVALID_ARG;
+  const yq_column& fk = fact->columns[fact_key];
+  const yq_column& dk = dim->columns[dim_key];
+  if (!join_col_ok(fk) || !join_col_ok(dk) || fk.type != dk.type || !hashable(fk.type)) return YQ_ERR_INVALID_ARG;
+  if (dim->rows > kHashMaxRows) return YQ_ERR_UNSUPPORTED;
+  cudaStream_t s = as_stream(stream);
+  JAParams F;
+  YQ_TRY(join_agg_params(fact, fact_predicate, fact_key, constants, aggs, nagg, F));
+  if (fact->rows == 0 || nagg == 0) return YQ_OK;
+  const uint32_t nbuckets = pow2_at_least(dim->rows ? dim->rows : 1);
+  Workspace ws;
+  YQ_TRY(ws.acquire(workspace, workspace_bytes, yq_join_aggregate_workspace_size(fact->rows, dim->rows, nagg), s));
+  uint32_t* d_bstart = ws.take<uint32_t>(nbuckets + 1);
+  unsigned long long* d_hkeys = ws.take<unsigned long long>(dim->rows ? dim->rows : 1);
+  uint32_t* d_hrows = ws.take<uint32_t>(dim->rows ? dim->rows : 1);
+  uint32_t* d_misc = ws.take<uint32_t>(8);  // [0] ticket [2] kept rows [3] duplicate keys
+  const int grid_cap = sm_count() * 8;
+  Acc* partials = ws.take<Acc>((size_t)grid_cap * YQ_MAX_AGGREGATES);
+  YQ_TRY_CUDA(cudaMemsetAsync(d_misc, 0, 8 * sizeof(uint32_t), s));
+  YQ_TRY(build_table(dim, dim_predicate, constants, dim_key, nbuckets, d_bstart, d_hkeys, d_hrows, d_misc + 2, s));
+  uint32_t counts[2] = {0, 0};
+  YQ_TRY(d2h_sync(counts, d_misc + 2, sizeof(counts), s));
+  if (counts[1] != 0) return YQ_ERR_UNSUPPORTED;  // dimension keys repeat: use yq_join_pairs + an aggregate
+  return join_agg_launch(F, fact, fact_key, nbuckets, counts[0], d_bstart, d_hkeys, partials, d_misc, state, s);
+}
+
+// ------------------------------------------------ prepared dimension table
+// Table layout: [8 counters][bucket starts nb+1][keys dim_rows][rows dim_rows].
+static size_t dim_table_layout(uint32_t dim_rows, WsSize& w) {
+  const uint32_t nb = pow2_at_least(dim_rows ? dim_rows : 1);
+  w.add<uint32_t>(8);
+  w.add<uint32_t>(nb + 1);
+  w.add<unsigned long long>(dim_rows ? dim_rows : 1);
+  w.add<uint32_t>(dim_rows ? dim_rows : 1);
+  return w.total();
+}
+
+size_t yq_join_dim_table_size(uint32_t dim_rows) {
+  WsSize w;
+  return dim_table_layout(dim_rows, w);
+}
+
+int yq_join_dim_table_build(const yq_batch* dim, const yq_program* dim_predicate, int32_t dim_key,
+                            const yq_constants* constants, void* table, size_t table_bytes, uint32_t* kept,
+                            void* stream) {
+  if (!dim || !table || !kept || dim_key < 0 || dim_key >= dim->ncols) return YQ_ERR_INVALID_ARG;
+  const yq_column& dk = dim->columns[dim_key];
+  if (!join_col_ok(dk) || !hashable(dk.type)) return YQ_ERR_INVALID_ARG;
+  if (dim->rows > kHashMaxRows) return YQ_ERR_UNSUPPORTED;
+  if (table_bytes < yq_join_dim_table_size(dim->rows)) return YQ_ERR_CAPACITY;
+  cudaStream_t s = as_stream(stream);
+  const uint32_t nbuckets = pow2_at_least(dim->rows ? dim->rows : 1);
+  Workspace ws;
+  YQ_TRY(ws.acquire(table, table_bytes, yq_join_dim_table_size(dim->rows), s));
+  uint32_t* d_misc = ws.take<uint32_t>(8);
+  uint32_t* d_bstart = ws.take<uint32_t>(nbuckets + 1);
+  unsigned long long* d_hkeys = ws.take<unsigned long long>(dim->rows ? dim->rows : 1);
+  uint32_t* d_hrows = ws.take<uint32_t>(dim->rows ? dim->rows : 1);
+  YQ_TRY_CUDA(cudaMemsetAsync(d_misc, 0, 8 * sizeof(uint32_t), s));
+  YQ_TRY(build_table(dim, dim_predicate, constants, dim_key, nbuckets, d_bstart, d_hkeys, d_hrows, d_misc + 2, s));
+  uint32_t counts[2] = {0, 0};
+  YQ_TRY(d2h_sync(counts, d_misc + 2, sizeof(counts), s));
+  if (counts[1] != 0) return YQ_ERR_UNSUPPORTED;
+  *kept = counts[0];
+  return YQ_OK;
+}
+
+size_t yq_join_aggregate_prepared_workspace_size(int32_t nagg) {
+  (void)nagg;
+  WsSize w;
+  w.add<uint32_t>(8);
+  w.add<Acc>((size_t)sm_count() * 8 * YQ_MAX_AGGREGATES);
+  return w.total();
+}
+
+int yq_join_aggregate_prepared(const yq_batch* fact, const yq_program* fact_predicate, int32_t fact_key,
+                               const void* table, uint32_t dim_rows, uint32_t kept, int32_t key_type,
+                               const yq_constants* constants, const yq_agg_spec* aggs, int32_t nagg, void* state,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+  if (!fact || !table || !state || fact_key < 0 || fact_key >= fact->ncols || nagg < 0 ||
+      nagg > YQ_MAX_AGGREGATES || (nagg > 0 && !aggs) || kept > dim_rows || dim_rows > kHashMaxRows)
+    return YQ_ERR_INVALID_ARG;
+  const yq_column& fk = fact->columns[fact_key];
+  if (!join_col_ok(fk) || fk.type != key_type || !hashable(fk.type)) return YQ_ERR_INVALID_ARG;
+  cudaStream_t s = as_stream(stream);
+  JAParams F;
+  YQ_TRY(join_agg_params(fact, fact_predicate, fact_key, constants, aggs, nagg, F));
+  if (fact->rows == 0 || nagg == 0) return YQ_OK;
+  const uint32_t nbuckets = pow2_at_least(dim_rows ? dim_rows : 1);
+  const size_t tbytes = yq_join_dim_table_size(dim_rows);
+  Workspace tw;  // the caller's table, carved as yq_join_dim_table_build laid it out
+  YQ_TRY(tw.acquire(const_cast<void*>(table), tbytes, tbytes, s));
+  tw.take<uint32_t>(8);
+  uint32_t* d_bstart = tw.take<uint32_t>(nbuckets + 1);
+  unsigned long long* d_hkeys = tw.take<unsigned long long>(dim_rows ? dim_rows : 1);
+  Workspace ws;
+  YQ_TRY(ws.acquire(workspace, workspace_bytes, yq_join_aggregate_prepared_workspace_size(nagg), s));
+  uint32_t* d_misc = ws.take<uint32_t>(8);
+  Acc* partials = ws.take<Acc>((size_t)sm_count() * 8 * YQ_MAX_AGGREGATES);
+  YQ_TRY_CUDA(cudaMemsetAsync(d_misc, 0, 8 * sizeof(uint32_t), s));
+  return join_agg_launch(F, fact, fact_key, nbuckets, kept, d_bstart, d_hkeys, partials, d_misc, state, s);
 }
 
 }  // extern "C"

@@ -834,10 +834,10 @@ extern "C" size_t yq_order_by_segments_workspace_size(const yq_column* key, uint
   return w.total();
 }
 
-extern "C" int yq_order_by_segments(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
-                                    const uint32_t* seg_offsets, int32_t nseg, yq_batch* out,
-                                    const yq_sort_config* config, void* workspace, size_t workspace_bytes,
-                                    void* stream) {
+static int order_by_segments_impl(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
+                                  const uint32_t* seg_offsets, int32_t nseg, yq_batch* out, uint32_t* perm_out,
+                                  const yq_sort_config* config, void* workspace, size_t workspace_bytes,
+                                  void* stream) {
   if (!in || !out || !seg_offsets || nseg <= 0 || key_col < 0 || key_col >= in->ncols || out->ncols != in->ncols ||
       in->ncols > YQ_MAX_BATCH_COLUMNS)
     return YQ_ERR_INVALID_ARG;
@@ -859,6 +859,7 @@ extern "C" int yq_order_by_segments(const yq_batch* in, int32_t key_col, int32_t
   YQ_TRY(sort_segments_impl(&j, 1, rows, seg_offsets, nseg, nullptr, nullptr, nullptr, 0, nullptr, &sort_bytes));
   char* sort_ws = ws.take<char>(sort_bytes);
   uint32_t* perm = ws.take<uint32_t>((size_t)rows + 16);
+  if (perm_out) perm = perm_out;  // the caller keeps the permutation
   if (rows == 0) return YQ_OK;
   uint32_t* sort_err = nullptr;
   YQ_TRY(sort_segments_impl(&j, 1, rows, seg_offsets, nseg, perm, config, sort_ws, sort_bytes, s, nullptr, nullptr,
@@ -869,11 +870,27 @@ extern "C" int yq_order_by_segments(const yq_batch* in, int32_t key_col, int32_t
   YQ_TRY_CUDA(cudaMemcpyAsync(d_err, sort_err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
   if (no_wait) return YQ_OK;
   uint32_t e = 0;
-  YQ_TRY_CUDA(cudaMemcpyAsync(&e, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  YQ_TRY(d2h_sync(&e, d_err, sizeof(uint32_t), s));
   if (e & kErrTimeout) return YQ_ERR_TIMEOUT;
   if (e & kErrBounds) return YQ_ERR_INVALID_ARG;
   return YQ_OK;
+}
+
+extern "C" int yq_order_by_segments(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
+                                    const uint32_t* seg_offsets, int32_t nseg, yq_batch* out,
+                                    const yq_sort_config* config, void* workspace, size_t workspace_bytes,
+                                    void* stream) {
+  return order_by_segments_impl(in, key_col, descending, nulls_first, seg_offsets, nseg, out, nullptr, config,
+                                workspace, workspace_bytes, stream);
+}
+
+extern "C" int yq_order_by_segments_perm(const yq_batch* in, int32_t key_col, int32_t descending,
+                                         int32_t nulls_first, const uint32_t* seg_offsets, int32_t nseg,
+                                         yq_batch* out, uint32_t* perm_out, const yq_sort_config* config,
+                                         void* workspace, size_t workspace_bytes, void* stream) {
+  if (!perm_out) return YQ_ERR_INVALID_ARG;
+  return order_by_segments_impl(in, key_col, descending, nulls_first, seg_offsets, nseg, out, perm_out, config,
+                                workspace, workspace_bytes, stream);
 }
 
 extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
@@ -995,9 +1012,8 @@ extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descendi
   // 3. every column (the key included) gathered once by the final row ids
   YQ_TRY(gather_impl(staged ? stage : in->columns, in->ncols, ids[cur], rows, out->columns, only_if, s));
   uint32_t err[2] = {0, 0};
-  YQ_TRY_CUDA(cudaMemcpyAsync(&err[0], sort_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaMemcpyAsync(&err[1], d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  YQ_TRY(d2h_sync(&err[0], sort_err, sizeof(uint32_t), s));
+  YQ_TRY(d2h_sync(&err[1], d_err, sizeof(uint32_t), s));
   const uint32_t e = err[0] | err[1];
   if (e & kErrTimeout) return YQ_ERR_TIMEOUT;
   if (e & kErrBounds) return YQ_ERR_INVALID_ARG;
@@ -1104,8 +1120,7 @@ int yq_merge_pass(const yq_column* cols, int32_t ncols, int32_t key_col, int32_t
     default: YQ_TRY(launch_merge<8>(M, s, bytes)); break;
   }
   uint32_t err = 0;
-  YQ_TRY_CUDA(cudaMemcpyAsync(&err, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  YQ_TRY(d2h_sync(&err, d_err, sizeof(uint32_t), s));
   if (err & kErrTimeout) return YQ_ERR_TIMEOUT;
   if (err & kErrBounds) return YQ_ERR_INVALID_ARG;
   return YQ_OK;

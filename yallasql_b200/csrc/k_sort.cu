@@ -34,6 +34,7 @@ constexpr uint32_t kMaxSortRows = (1u << 30) - 1u;
 struct SegInfo {
   const uint32_t* seg_start;   // nseg + 1 row offsets
   const uint32_t* tile_start;  // nseg + 1 tile offsets
+  const uint32_t* tile_seg;    // segment of every tile (null: binary search of tile_start)
   int32_t nseg;
 };
 
@@ -52,6 +53,7 @@ __device__ __forceinline__ uint32_t digit_of(const uint32_t (&k)[KW], int shift)
 }
 
 __device__ __forceinline__ int find_segment(const SegInfo& g, uint32_t tile) {
+  if (g.tile_seg) return (int)__ldg(g.tile_seg + tile);  // one load instead of a chain of dependent ones
   int lo = 0, hi = g.nseg - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
@@ -342,6 +344,53 @@ __global__ void __launch_bounds__(kSortBlock, sweep_min_blocks(KW, D, ITEMS)) k_
       }
     }
     S.vals_out[g] = s_vals[i];
+  }
+}
+
+// Which passes change the order, decided on the device so the host reads 16
+// bytes per pass instead of every segment's histogram. Per pass p:
+// sum[4p] = 1 while every non-empty segment's keys share one digit,
+// sum[4p+1] / sum[4p+2] = the least / greatest such digit, sum[4p+3] = 1 when a
+// non-empty segment exists. Block (p, b): its warps take segments
+// b*64 + warp, + 8, ...; a warp's lanes look at 8 bins each.
+__global__ void k_pass_summary_init(int32_t* sum, int P) {
+  for (int p = threadIdx.x; p < P; p += blockDim.x) {
+    sum[4 * p] = 1;
+    sum[4 * p + 1] = 0x7fffffff;
+    sum[4 * p + 2] = -1;
+    sum[4 * p + 3] = 0;
+  }
+}
+
+__global__ void k_pass_summary(const uint32_t* __restrict__ hist, const uint32_t* __restrict__ seg_start, int nseg,
+                               int P, int R, int32_t* sum) {
+  const int p = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g_end = min(nseg, (int)(blockIdx.y + 1) * 64);
+  for (int g = blockIdx.y * 64 + warp; g < g_end; g += blockDim.x / 32) {
+    const uint32_t len = __ldg(seg_start + g + 1) - __ldg(seg_start + g);
+    if (len == 0) continue;
+    const uint32_t* hp = hist + ((size_t)g * P + p) * R;
+    int one = -1;
+    for (int d = lane; d < R; d += 32)
+      if (__ldg(hp + d) == len) one = d;  // at most one bin can hold every key
+    const uint32_t hit = __ballot_sync(0xffffffffu, one >= 0);
+    if (lane == 0) {
+      atomicOr(sum + 4 * p + 3, 1);
+      if (!hit) atomicAnd(sum + 4 * p, 0);
+    }
+    if (hit && lane == __ffs(hit) - 1) {
+      atomicMin(sum + 4 * p + 1, one);
+      atomicMax(sum + 4 * p + 2, one);
+    }
+  }
+}
+
+// tile_seg[t] = the segment tile t belongs to: block g fills segment g's tiles.
+__global__ void k_fill_tile_seg(const uint32_t* __restrict__ tile_start, int nseg, uint32_t* __restrict__ tile_seg) {
+  for (int g = blockIdx.x; g < nseg; g += gridDim.x) {
+    const uint32_t t0 = __ldg(tile_start + g), t1 = __ldg(tile_start + g + 1);
+    for (uint32_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) tile_seg[t] = (uint32_t)g;
   }
 }
 
@@ -709,7 +758,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
   // Size buffers for the widest plan any key can take (text keys are sized
   // for their full slot, up to 8 words; their significant width is measured
   // on the device before they are sorted).
-  size_t max_kw = 1, max_hist = 1, max_status = 1;
+  size_t max_kw = 1, max_hist = 1, max_status = 1, max_tiles = 1;
   for (int j = 0; j < njobs; ++j) {
     const yq_column& c = jobs[j].key;
     if (!valid_key_column(c)) return YQ_ERR_INVALID_ARG;
@@ -726,6 +775,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
     const size_t h = (size_t)nseg * kp.P * kp.R, sz = (size_t)kp.P * kp.ntiles * kp.R;
     if (h > max_hist) max_hist = h;
     if (sz > max_status) max_status = sz;
+    if (kp.ntiles > max_tiles) max_tiles = kp.ntiles;
   }
 
   WsSize w;
@@ -733,12 +783,13 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
   w.add<uint32_t>(nseg + 1);
   w.add<uint32_t>(max_hist);
   w.add<uint32_t>(max_status);
-  w.add<uint32_t>(80);
+  w.add<uint32_t>(80 + 4 * 64);
   w.add<uint32_t>((size_t)rows * max_kw);
   w.add<uint32_t>((size_t)rows * max_kw);
   w.add<uint32_t>(rows);
   w.add<uint32_t>(rows);
   w.add<uint32_t>(rows);
+  w.add<uint32_t>(max_tiles + 1);  // segment of every tile
   if (size_only) {
     *size_only = w.total();
     return YQ_OK;
@@ -752,10 +803,21 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
   uint32_t* d_tiles = ws.take<uint32_t>(nseg + 1);
   uint32_t* d_hist = ws.take<uint32_t>(max_hist);
   uint32_t* d_status = ws.take<uint32_t>(max_status);
-  uint32_t* d_misc = ws.take<uint32_t>(80);  // [0..63] tile counters, [64] error, [65] text words
+  uint32_t* d_misc = ws.take<uint32_t>(80 + 4 * 64);  // [0..63] tile counters, [64] error, [65] text words,
+                                                       // [66..] pass summary
   uint32_t* d_keys[2] = {ws.take<uint32_t>((size_t)rows * max_kw), ws.take<uint32_t>((size_t)rows * max_kw)};
   uint32_t* d_vals[2] = {ws.take<uint32_t>(rows), ws.take<uint32_t>(rows)};
   uint32_t* d_perm_tmp = ws.take<uint32_t>(rows);
+  uint32_t* d_tile_seg = ws.take<uint32_t>(max_tiles + 1);
+  // tile offsets of a plan on the device, with the segment of every tile
+  auto upload_tiles = [&](const SegPlan& p) -> int {
+    YQ_TRY(h2d_async(d_tiles, p.tiles.data(), (nseg + 1) * sizeof(uint32_t), s));
+    if (p.ntiles > max_tiles) return YQ_ERR_UNSUPPORTED;
+    const int g = nseg < 4096 ? nseg : 4096;
+    k_fill_tile_seg<<<g, 256, 0, s>>>(d_tiles, nseg, d_tile_seg);
+    YQ_CHECK_LAUNCH();
+    return YQ_OK;
+  };
   uint32_t* d_err = d_misc + 64;
   uint32_t* d_textw = d_misc + 65;
   YQ_TRY_CUDA(cudaMemsetAsync(d_misc, 0, 80 * sizeof(uint32_t), s));
@@ -772,8 +834,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
       YQ_TRY_CUDA(cudaMemsetAsync(d_textw, 0, sizeof(uint32_t), s));
       k_text_words<<<sm_count() * 4, 256, 0, s>>>(static_cast<const char*>(c.data), c.nulls, c.width, rows, d_textw);
       YQ_CHECK_LAUNCH();
-      YQ_TRY_CUDA(cudaMemcpyAsync(&tw, d_textw, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-      YQ_TRY_CUDA(cudaStreamSynchronize(s));
+      YQ_TRY(d2h_sync(&tw, d_textw, sizeof(uint32_t), s));
       vw = (int)tw;
       if (vw == 0 && !c.nulls) continue;  // every key equal: order unchanged
     }
@@ -804,7 +865,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
     SegPlan sp;
     plan_segments(seg_offsets_host, nseg, kp.tile_rows, sp);
     YQ_TRY(h2d_async(d_seg, sp.seg.data(), (nseg + 1) * sizeof(uint32_t), s));
-    YQ_TRY(h2d_async(d_tiles, sp.tiles.data(), (nseg + 1) * sizeof(uint32_t), s));
+    YQ_TRY(upload_tiles(sp));
     YQ_TRY_CUDA(cudaMemsetAsync(d_hist, 0, (size_t)nseg * kp.P * kp.R * sizeof(uint32_t), s));
     YQ_TRY_CUDA(cudaMemsetAsync(d_status, 0, (size_t)kp.P * sp.ntiles * kp.R * sizeof(uint32_t), s));
     YQ_TRY_CUDA(cudaMemsetAsync(d_misc, 0, 64 * sizeof(uint32_t), s));
@@ -822,6 +883,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
     SegInfo seg;
     seg.seg_start = d_seg;
     seg.tile_start = d_tiles;
+    seg.tile_seg = d_tile_seg;
     seg.nseg = nseg;
     {
       // algorithmic bytes: each key read once (+ the incoming permutation)
@@ -838,23 +900,20 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
       // A pass whose digit is the same for every key of every segment leaves
       // the order unchanged and is skipped. common[p] = that digit when it is
       // also the same across segments, else -1.
-      std::vector<uint32_t> h((size_t)nseg * kp.P * kp.R);
-      YQ_TRY_CUDA(cudaMemcpyAsync(h.data(), d_hist, h.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-      YQ_TRY_CUDA(cudaStreamSynchronize(s));
+      if (kp.P > 64) return YQ_ERR_UNSUPPORTED;
+      int32_t* d_sum = reinterpret_cast<int32_t*>(d_misc + 66);  // [4 * P] summary words (P <= 64 here)
+      k_pass_summary_init<<<1, 64, 0, s>>>(d_sum, kp.P);
+      YQ_CHECK_LAUNCH();
+      k_pass_summary<<<dim3((unsigned)kp.P, (unsigned)ceil_div(nseg, 64)), 256, 0, s>>>(d_hist, d_seg, nseg, kp.P,
+                                                                                          kp.R, d_sum);
+      YQ_CHECK_LAUNCH();
+      int32_t sum[4 * 64];
+      YQ_TRY(d2h_sync(sum, d_sum, (size_t)kp.P * 4 * sizeof(int32_t), s));
       std::vector<int> common(kp.P, -1);
       for (int p = 0; p < kp.P; ++p) {
-        bool trivial = true;
-        int digit = -2;  // -2: no non-empty segment seen yet
-        for (int g = 0; g < nseg && trivial; ++g) {
-          const uint32_t len = seg_offsets_host[g + 1] - seg_offsets_host[g];
-          if (len == 0) continue;
-          const uint32_t* hp = h.data() + ((size_t)g * kp.P + p) * kp.R;
-          int one = -1;
-          for (int d = 0; d < kp.R && one < 0; ++d)
-            if (hp[d] == len) one = d;
-          trivial = one >= 0;
-          digit = (digit == -2 || digit == one) ? one : -1;
-        }
+        const bool trivial = sum[4 * p] != 0;
+        // -2: no non-empty segment; -1: segments disagree on the digit
+        const int digit = !sum[4 * p + 3] ? -2 : (sum[4 * p + 1] == sum[4 * p + 2] ? sum[4 * p + 1] : -1);
         if (!trivial) passes.push_back(p);
         else common[p] = digit;
       }
@@ -893,7 +952,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
     }
     if (kq.sh.kw != kp.sh.kw) {  // tiles of the narrower kernels
       plan_segments(seg_offsets_host, nseg, kq.tile_rows, sp);
-      YQ_TRY(h2d_async(d_tiles, sp.tiles.data(), (nseg + 1) * sizeof(uint32_t), s));
+      YQ_TRY(upload_tiles(sp));
       YQ_TRY_CUDA(cudaMemsetAsync(d_status, 0, passes.size() * sp.ntiles * kq.R * sizeof(uint32_t), s));
     }
     if (passes.size() > 64) return YQ_ERR_UNSUPPORTED;
@@ -935,8 +994,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
   if (err_out) *err_out = d_err;
   if (!keep_trivial && !defer_err) {
     uint32_t err = 0;
-    YQ_TRY_CUDA(cudaMemcpyAsync(&err, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    YQ_TRY_CUDA(cudaStreamSynchronize(s));
+    YQ_TRY(d2h_sync(&err, d_err, sizeof(uint32_t), s));
     if (err & kErrTimeout) return YQ_ERR_TIMEOUT;
     if (err & kErrBounds) return YQ_ERR_INVALID_ARG;
   }

@@ -43,11 +43,17 @@ __global__ void k_param_copy(uint32_t* __restrict__ dst, const __grid_constant__
   for (uint32_t i = threadIdx.x; i < nwords; i += blockDim.x) dst[i] = c.words[i];
 }
 
+// Uploads up to kParamPathBytes travel as kernel parameters rather than
+// through a copy engine: an operator's small uploads then never queue behind a
+// bulk transfer another stream has in flight on the same engine.
+constexpr size_t kParamPathBytes = 16 * 1024;
+
 int h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   if (bytes == 0) return YQ_OK;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   YQ_TRY_CUDA(cudaStreamIsCapturing(s, &cap));
-  if (cap != cudaStreamCaptureStatusNone) {
+  if (cap != cudaStreamCaptureStatusNone || (bytes <= kParamPathBytes && !(bytes & 3u) &&
+                                            !(reinterpret_cast<uintptr_t>(dst) & 3u))) {
     if ((bytes & 3u) || (reinterpret_cast<uintptr_t>(dst) & 3u)) return YQ_ERR_UNSUPPORTED;
     const uint32_t* w = static_cast<const uint32_t*>(src);
     const size_t nw = bytes / 4;
@@ -81,6 +87,48 @@ int h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   memcpy(h, src, bytes);
   YQ_TRY_CUDA(cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, s));
   YQ_TRY_CUDA(cudaEventRecord(g_stage_ev[slot], s));
+  return YQ_OK;
+}
+
+// -------------------------------------------------------- small read-backs
+// A small device -> host read that the host needs now: a kernel copies the
+// words into mapped pinned host memory (stores over the link, not a copy
+// engine), the stream is synchronised, the bytes are copied out. Larger reads
+// take cudaMemcpyAsync. One mapped buffer per device, under a lock.
+namespace {
+constexpr size_t kMappedBytes = 64 * 1024;
+std::mutex g_mapped_mu;
+uint32_t* g_mapped[64] = {nullptr};
+}  // namespace
+
+__global__ void k_to_host(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, uint32_t nwords) {
+  for (uint32_t i = threadIdx.x; i < nwords; i += blockDim.x) dst[i] = src[i];
+  __threadfence_system();
+}
+
+int d2h_sync(void* host_dst, const void* dev_src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return YQ_OK;
+  int dev = 0;
+  YQ_TRY_CUDA(cudaGetDevice(&dev));
+  const bool small = bytes <= kMappedBytes && dev >= 0 && dev < 64 && !(bytes & 3u) &&
+                     !(reinterpret_cast<uintptr_t>(dev_src) & 3u);
+  if (!small) {
+    YQ_TRY_CUDA(cudaMemcpyAsync(host_dst, dev_src, bytes, cudaMemcpyDeviceToHost, s));
+    YQ_TRY_CUDA(cudaStreamSynchronize(s));
+    return YQ_OK;
+  }
+  std::lock_guard<std::mutex> lk(g_mapped_mu);
+  if (!g_mapped[dev]) {
+    void* h = nullptr;
+    YQ_TRY_CUDA(cudaHostAlloc(&h, kMappedBytes, cudaHostAllocMapped | cudaHostAllocPortable));
+    g_mapped[dev] = static_cast<uint32_t*>(h);
+  }
+  uint32_t* dptr = nullptr;
+  YQ_TRY_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&dptr), g_mapped[dev], 0));
+  k_to_host<<<1, 256, 0, s>>>(dptr, static_cast<const uint32_t*>(dev_src), (uint32_t)(bytes / 4));
+  YQ_CHECK_LAUNCH();
+  YQ_TRY_CUDA(cudaStreamSynchronize(s));
+  memcpy(host_dst, g_mapped[dev], bytes);
   return YQ_OK;
 }
 

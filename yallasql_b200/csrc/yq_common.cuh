@@ -76,6 +76,10 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 // the stream (staged through pinned memory; runtime.cu).
 int h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s);
 
+// Device -> host read of `bytes` that the host waits for (synchronises `s`);
+// small reads bypass the copy engines (runtime.cu).
+int d2h_sync(void* host_dst, const void* dev_src, size_t bytes, cudaStream_t s);
+
 int sm_count();
 
 // Per-device, thread-safe launch settings (runtime.cu): raise `kernel`'s

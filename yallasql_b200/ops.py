@@ -95,7 +95,11 @@ class AggState:
         self.aggs = aggs
         self.buf = torch.empty(max(256, lib().yq_agg_state_bytes(len(aggs))), dtype=torch.uint8, device="cuda")
         self._specs = _agg_specs_stub(aggs)
-        _check(lib().yq_agg_state_init(self.buf.data_ptr(), self._specs, len(aggs), _stream(stream)),
+        self.reset(stream)
+
+    def reset(self, stream=None):
+        """Back to the aggregates' identities, so the state serves another query."""
+        _check(lib().yq_agg_state_init(self.buf.data_ptr(), self._specs, len(self.aggs), _stream(stream)),
                "yq_agg_state_init")
 
     def read(self, stream=None) -> list:
@@ -184,17 +188,23 @@ class AggStates:
         self._specs = _agg_specs_stub(aggs)
         self.reset(stream)
 
-    def reset(self, stream=None):
-        _check(lib().yq_agg_states_init(self.buf.data_ptr(), self.count, self._specs, len(self.aggs),
+    def reset(self, stream=None, count: int | None = None):
+        """The first `count` states (all by default) back to the identities."""
+        k = self.count if count is None else count
+        if k < 0 or k > self.count:
+            raise ValueError("count beyond the states allocated")
+        _check(lib().yq_agg_states_init(self.buf.data_ptr(), k, self._specs, len(self.aggs),
                                         _stream(stream)), "yq_agg_states_init")
 
-    def read(self, stream=None) -> list:
+    def read(self, stream=None, count: int | None = None) -> list:
+        """Results of the first `count` states (all by default)."""
+        k = self.count if count is None else count
         n = len(self.aggs)
-        out = (A.AggResult * max(1, self.count * n))()
-        _check(lib().yq_agg_states_read(self.buf.data_ptr(), self.count, self._specs, n, out, _stream(stream)),
+        out = (A.AggResult * max(1, k * n))()
+        _check(lib().yq_agg_states_read(self.buf.data_ptr(), k, self._specs, n, out, _stream(stream)),
                "yq_agg_states_read")
         res = []
-        for g in range(self.count):
+        for g in range(k):
             vals = []
             for i, a in enumerate(self.aggs):
                 r = out[g * n + i]
@@ -458,6 +468,37 @@ class JoinAggPlan:
                                        len(self.aggs), state.buf.data_ptr(), None, 0, _stream(stream)),
                "yq_join_aggregate")
 
+    def prepare(self, dim: DeviceBatch, stream=None) -> "PreparedDim":
+        """Build the dimension side once (filtered, hashed, kept resident)."""
+        return PreparedDim(self, dim, stream)
+
+    def run_prepared(self, fact: DeviceBatch, prepared: "PreparedDim", state: AggState, stream=None,
+                     workspace: torch.Tensor | None = None):
+        """Probe a prepared dimension table: no host synchronisation."""
+        fb, fk = fact.c()
+        ws = workspace.data_ptr() if workspace is not None else None
+        wsb = workspace.numel() if workspace is not None else 0
+        _check(lib().yq_join_aggregate_prepared(C.byref(fb), C.byref(self.fpred.prog), self.fact_key,
+                                                prepared.table.data_ptr(), prepared.dim_rows, prepared.kept,
+                                                prepared.key_type, C.byref(self.consts), self.specs, len(self.aggs),
+                                                state.buf.data_ptr(), ws, wsb, _stream(stream)),
+               "yq_join_aggregate_prepared")
+
+
+class PreparedDim:
+    """A star join's dimension side built once and kept in device memory."""
+
+    def __init__(self, plan: JoinAggPlan, dim: DeviceBatch, stream=None):
+        self.dim_rows = dim.rows
+        self.key_type = dim.columns[plan.dim_key].type
+        self.table = torch.empty(int(lib().yq_join_dim_table_size(dim.rows)), dtype=torch.uint8, device="cuda")
+        db, dk = dim.c()
+        kept = C.c_uint32(0)
+        _check(lib().yq_join_dim_table_build(C.byref(db), C.byref(plan.dpred.prog), plan.dim_key,
+                                             C.byref(plan.consts), self.table.data_ptr(), self.table.numel(),
+                                             C.byref(kept), _stream(stream)), "yq_join_dim_table_build")
+        self.kept = int(kept.value)
+
 
 def order_by_workspace_bytes(col: DeviceColumn, offsets: list[int]) -> int:
     """Least workspace of yq_order_by (one-level gather)."""
@@ -519,16 +560,23 @@ def order_by_segments_workspace_bytes(col: DeviceColumn, offsets) -> int:
 
 
 def order_by_segments(batch: DeviceBatch, key: int, descending: bool, offsets, out: DeviceBatch, config=None,
-                      workspace: torch.Tensor | None = None, nulls_first=False, stream=None) -> DeviceBatch:
-    """ORDER BY per task: task g = rows [offsets[g], offsets[g+1]) (yq_order_by_segments)."""
+                      workspace: torch.Tensor | None = None, nulls_first=False, stream=None,
+                      perm_out: torch.Tensor | None = None) -> DeviceBatch:
+    """ORDER BY per task: task g = rows [offsets[g], offsets[g+1]) (yq_order_by_segments);
+    with `perm_out` the permutation is kept there (yq_order_by_segments_perm)."""
     offs = offsets if isinstance(offsets, C.Array) else (C.c_uint32 * len(offsets))(*offsets)
     ib, _ia = batch.c()
     ob, _oa = out.c()
     ws = workspace.data_ptr() if workspace is not None else None
     wsb = workspace.numel() if workspace is not None else 0
-    _check(lib().yq_order_by_segments(C.byref(ib), key, int(descending), int(nulls_first), offs, len(offs) - 1,
-                                      C.byref(ob), C.byref(config) if config is not None else None, ws, wsb,
-                                      _stream(stream)), "yq_order_by_segments")
+    cfg = C.byref(config) if config is not None else None
+    if perm_out is not None:
+        _check(lib().yq_order_by_segments_perm(C.byref(ib), key, int(descending), int(nulls_first), offs,
+                                               len(offs) - 1, C.byref(ob), perm_out.data_ptr(), cfg, ws, wsb,
+                                               _stream(stream)), "yq_order_by_segments_perm")
+    else:
+        _check(lib().yq_order_by_segments(C.byref(ib), key, int(descending), int(nulls_first), offs, len(offs) - 1,
+                                          C.byref(ob), cfg, ws, wsb, _stream(stream)), "yq_order_by_segments")
     return out
 
 

@@ -36,9 +36,11 @@ from . import batched, datagen, ops
 from .expr import Aggregate, And, Arith, Cast, ColumnRef, Compare, Constant, between
 
 CLASSES = ("filter", "order", "join", "subquery")
+MAX_GROUP = 64  # filter requests co-launched in one segmented call at most
 MIX = (0.4, 0.3, 0.2, 0.1)
 ORDER_TYPES = [A.FLOAT32, A.INT64, A.TEXT, A.DATETIME]
 ORDER_WIDTHS = [4, 8, 16, 8]
+THRESHOLD_MARK = -3.0e38  # placeholder of the subquery's threshold in its compiled plan
 SALES_TYPES = [A.FLOAT32, A.INT32, A.INT32, A.TEXT]  # price qty discount category
 
 
@@ -145,10 +147,39 @@ class Plans:
             [Aggregate(A.AGG_SUM, Arith(A.MUL, ColumnRef(3, A.FLOAT32), Cast(ColumnRef(2, A.INT32), A.FLOAT32)))])
         self.revenue = Arith(A.MUL, ColumnRef(0, A.FLOAT32), Cast(ColumnRef(2, A.INT32), A.FLOAT32))
         self.avg = {}
+        self.rows_gt = {}  # stage 2 of the subquery per category, its threshold patched per request
+        mark = Constant(THRESHOLD_MARK, A.FLOAT32)
         for c in range(len(datagen.CATEGORIES)):
             eq = Compare(A.EQ, ColumnRef(3, A.TEXT), Constant(datagen.CATEGORIES[c], A.TEXT))
             self.avg[c] = ops.AggPlan(SALES_TYPES, eq, [Aggregate(A.AGG_AVG, self.revenue)])
+            plan = ops.ProjectPlan(SALES_TYPES, [4, 4, 4, 16], And(eq, Compare(A.GT, self.revenue, mark)),
+                                   [self.revenue, 1])
+            slot = [w for _, w in plan.pool.words].index(mark.word())
+            self.rows_gt[c] = (plan, slot)
+        # AVG over no rows is NULL, so no row qualifies: a predicate false on every row
+        self.rows_none = ops.ProjectPlan(SALES_TYPES, [4, 4, 4, 16],
+                                         Compare(A.NE, ColumnRef(1, A.INT32), ColumnRef(1, A.INT32)),
+                                         [self.revenue, 1])
         self.order_cfg = ops.sort_config(digit_bits=0, keep_trivial=True)
+        self.join_dim = None
+        self._join_dim_of = None
+
+    def prepared_dim(self, cat: "Catalog") -> ops.PreparedDim:
+        """The join's dimension side (date rows of year 1993, hashed), built once
+        per catalog and kept resident for every join request."""
+        if self._join_dim_of is not cat:
+            self.join_dim = self.join.prepare(cat.dim)
+            self._join_dim_of = cat
+        return self.join_dim
+
+    def subquery_rows_plan(self, category: int, avg) -> ops.ProjectPlan:
+        """Stage 2 of the subquery: category = c AND revenue > avg (the compiled
+        plan of category c with `avg` written into its threshold constant)."""
+        if avg is None:
+            return self.rows_none
+        plan, slot = self.rows_gt[category]
+        plan._keep[0][slot] = Constant(float(np.float32(avg)), A.FLOAT32).word()
+        return plan
 
 
 # ------------------------------------------------------------------- jobs
@@ -165,12 +196,27 @@ class SlotBuffers:
         self.cat = cat
         self._order = None
         self._sub = None
+        self._states = None
 
-    def ensure(self):
-        """Allocate both buffers now (before a timed run)."""
+    def ensure(self, plans: "Plans | None" = None):
+        """Allocate the buffers now (before a timed run)."""
         self.order(0, 0)
         self.subquery(0)
+        if plans is not None:
+            self.states(plans)
         return self
+
+    def states(self, plans: "Plans"):
+        """Aggregate states and workspaces the slot reuses: up to MAX_GROUP
+        co-launched filter states, one join state with its probe workspace, one
+        subquery AVG state and the subquery's row counter."""
+        if self._states is None:
+            jws = torch.empty(max(256, int(ops.lib().yq_join_aggregate_prepared_workspace_size(
+                len(plans.join.aggs)))), dtype=torch.uint8, device="cuda")
+            self._states = {"filter": ops.AggStates(plans.aggs, MAX_GROUP), "join": ops.AggState(plans.join.aggs),
+                            "join_ws": jws, "avg": ops.AggState(plans.avg[0].aggs),
+                            "count": torch.zeros(1, dtype=torch.int32, device="cuda")}
+        return self._states
 
     def order(self, n: int, ws_bytes: int):
         if self._order is None:
@@ -208,35 +254,56 @@ class Job:
 
 
 class FilterGroup(Job):
-    def __init__(self, cat: Catalog, plans: Plans, reqs: list[Request]):
+    """Filter requests co-launched as one segmented filter+aggregate over their
+    tables' row ranges. With `shared`, requests on the same table share one
+    range (the query has no parameters: their results are the same)."""
+
+    def __init__(self, cat: Catalog, plans: Plans, reqs: list[Request], shared: bool = False):
         self.cat, self.plans, self.reqs = cat, plans, reqs
-        self.begin = [cat.sales_begin[r.table] for r in reqs]
-        self.end = [cat.sales_end[r.table] for r in reqs]
-        self.mem = 256 * len(reqs) + 8 * sum(e - b for b, e in zip(self.begin, self.end)) // 1024 + (1 << 16)
+        tables = []
+        self.slot_of = []
+        for r in reqs:
+            if not shared or r.table not in tables:
+                tables.append(r.table)
+            self.slot_of.append(tables.index(r.table) if shared else len(tables) - 1)
+        self.begin = [cat.sales_begin[t] for t in tables]
+        self.end = [cat.sales_end[t] for t in tables]
+        self.mem = 256 * len(tables) + 8 * sum(e - b for b, e in zip(self.begin, self.end)) // 1024 + (1 << 16)
 
     def launch(self, stream, bufs=None):
         self.stream = stream
+        n = len(self.begin)
         with torch.cuda.stream(stream):
-            self.states = ops.AggStates(self.plans.aggs, len(self.reqs), stream=stream.cuda_stream)
+            if bufs is not None and n <= MAX_GROUP:
+                self.states = bufs.states(self.plans)["filter"]
+                self.states.reset(stream.cuda_stream, count=n)
+            else:
+                self.states = ops.AggStates(self.plans.aggs, n, stream=stream.cuda_stream)
             self.plans.filter.run_ranges(self.cat.arena, self.begin, self.end, self.states, stream=stream.cuda_stream)
             self.event = torch.cuda.Event()
             self.event.record(stream)
 
     def finish(self):
-        res = self.states.read(self.stream)
-        for r, v in zip(self.reqs, res):
-            r.result = v
+        res = self.states.read(self.stream, count=len(self.begin))
+        for r, k in zip(self.reqs, self.slot_of):
+            r.result = res[k]
         self.states = None
 
 
 class OrderJob(Job):
-    def __init__(self, cat: Catalog, plans: Plans, req: Request, keep: bool):
+    """ORDER BY key DESC over one table. With `perms` (the serving loop's
+    resident intermediates), the first request on a table keeps its sort
+    permutation; later ones wait for it and only gather."""
+
+    def __init__(self, cat: Catalog, plans: Plans, req: Request, keep: bool, perms: dict | None = None):
         self.cat, self.plans, self.reqs, self.keep = cat, plans, [req], keep
         self.tbl = cat.order[req.table]
+        self.perms = perms
         n = self.tbl.rows
         self.offs = (C.c_uint32 * 2)(0, n)
         self.ws_bytes = max(256, ops.order_by_segments_workspace_bytes(self.tbl.columns[0], [0, n]))
         self.mem = 36 * n + self.ws_bytes
+        self.gather_only = perms is not None and req.table in perms
 
     def launch(self, stream, bufs: SlotBuffers | None = None):
         n = self.tbl.rows
@@ -248,17 +315,32 @@ class OrderJob(Job):
                 self.out = ops.DeviceBatch([ops.DeviceColumn.empty(t, n, w if t == A.TEXT else None)
                                             for t, w in zip(ORDER_TYPES, ORDER_WIDTHS)])
                 self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device="cuda")
-            ops.order_by_segments(self.tbl, 0, True, self.offs, self.out, config=self.plans.order_cfg,
-                                  workspace=self.ws, stream=stream.cuda_stream)
+            t = self.reqs[0].table
+            if self.gather_only:
+                perm, ready = self.perms[t]
+                stream.wait_event(ready)  # the permutation's sort may still run on another stream
+                ops.gather(self.tbl, perm, stream=stream.cuda_stream, out=self.out)
+            elif self.perms is not None:
+                perm = torch.empty(n, dtype=torch.int32, device="cuda")
+                ops.order_by_segments(self.tbl, 0, True, self.offs, self.out, config=self.plans.order_cfg,
+                                      workspace=self.ws, stream=stream.cuda_stream, perm_out=perm)
+                ready = torch.cuda.Event()
+                ready.record(stream)
+                self.perms[t] = (perm, ready)
+            else:
+                ops.order_by_segments(self.tbl, 0, True, self.offs, self.out, config=self.plans.order_cfg,
+                                      workspace=self.ws, stream=stream.cuda_stream)
             self.event = torch.cuda.Event()
             self.event.record(stream)
 
     def finish(self):
-        with torch.cuda.stream(self.stream):
-            err = int(self.ws[:4].view(torch.int32)[0].item())
-        if err:
-            raise RuntimeError(f"ORDER BY request {self.reqs[0].rid}: device error word {err}")
-        self.reqs[0].result = self.out if self.keep else ("ok", self.tbl.rows)
+        if not self.gather_only:
+            with torch.cuda.stream(self.stream):
+                err = int(self.ws[:4].view(torch.int32)[0].item())
+            if err:
+                raise RuntimeError(f"ORDER BY request {self.reqs[0].rid}: device error word {err}")
+        for r in self.reqs:
+            r.result = self.out if self.keep else ("ok", self.tbl.rows)
         self.out = self.ws = None
 
 
@@ -270,14 +352,23 @@ class JoinJob(Job):
     def launch(self, stream, bufs=None):
         self.stream = stream
         with torch.cuda.stream(stream):
-            self.state = ops.AggState(self.plans.join.aggs, stream=stream.cuda_stream)
-            self.plans.join.run(self.cat.facts[self.reqs[0].table], self.cat.dim, self.state,
-                                stream=stream.cuda_stream)
+            fact = self.cat.facts[self.reqs[0].table]
+            if bufs is not None:  # the slot's state, the resident dimension table: no host wait
+                st = bufs.states(self.plans)
+                self.state = st["join"]
+                self.state.reset(stream.cuda_stream)
+                self.plans.join.run_prepared(fact, self.plans.prepared_dim(self.cat), self.state,
+                                             stream=stream.cuda_stream, workspace=st["join_ws"])
+            else:
+                self.state = ops.AggState(self.plans.join.aggs, stream=stream.cuda_stream)
+                self.plans.join.run(fact, self.cat.dim, self.state, stream=stream.cuda_stream)
             self.event = torch.cuda.Event()
             self.event.record(stream)
 
     def finish(self):
-        self.reqs[0].result = self.state.read(self.stream)
+        res = self.state.read(self.stream)
+        for r in self.reqs:
+            r.result = res
         self.state = None
 
 
@@ -293,7 +384,11 @@ class SubqueryJob(Job):
         self.stream = stream
         with torch.cuda.stream(stream):
             plan = self.plans.avg[self.reqs[0].param]
-            self.state = ops.AggState(plan.aggs, stream=stream.cuda_stream)
+            if bufs is not None:
+                self.state = bufs.states(self.plans)["avg"]
+                self.state.reset(stream.cuda_stream)
+            else:
+                self.state = ops.AggState(plan.aggs, stream=stream.cuda_stream)
             plan.run(self.tbl, self.state, stream=stream.cuda_stream)
             self.event = torch.cuda.Event()
             self.event.record(stream)
@@ -314,21 +409,17 @@ class SubqueryRows(Job):
 
     def launch(self, stream, bufs=None):
         p = self.first.plans
-        c = self.reqs[0].param
-        eq = Compare(A.EQ, ColumnRef(3, A.TEXT), Constant(datagen.CATEGORIES[c], A.TEXT))
         # AVG over no rows is NULL: then no row qualifies (the comparison is NULL)
-        thr = Constant(float(np.float32(self.avg)) if self.avg is not None else 0.0, A.FLOAT32)
-        pred = And(eq, Compare(A.GT, p.revenue, thr)) if self.avg is not None else \
-            And(eq, Compare(A.NE, ColumnRef(1, A.INT32), ColumnRef(1, A.INT32)))
-        self.plan = ops.ProjectPlan(SALES_TYPES, [4, 4, 4, 16], pred, [p.revenue, 1])
+        self.plan = p.subquery_rows_plan(self.reqs[0].param, self.avg)
         n = max(1, self.tbl.rows)
         self.stream = stream
         with torch.cuda.stream(stream):
             if bufs is not None and not self.first.keep:
                 self.outs = bufs.subquery(n)
+                self.cnt = bufs.states(p)["count"]
             else:
                 self.outs = [ops.DeviceColumn.empty(A.FLOAT32, n), ops.DeviceColumn.empty(A.INT32, n)]
-            self.cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+                self.cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
             oc = (A.Column * 2)(*[o.c() for o in self.outs])
             b, keep = self.tbl.c()
             self._keep = (oc, b, keep)
@@ -343,15 +434,17 @@ class SubqueryRows(Job):
         with torch.cuda.stream(self.stream):
             n = int(self.cnt.item())
             if self.first.keep:
-                self.reqs[0].result = (n, self.outs[0].data[:n].clone(), self.outs[1].data[:n].clone())
+                res = (n, self.outs[0].data[:n].clone(), self.outs[1].data[:n].clone())
             else:
-                self.reqs[0].result = (n,)
+                res = (n,)
+            for r in self.reqs:
+                r.result = res
         self.outs = None
 
 
-def make_job(cat, plans, req: Request, keep: bool) -> Job:
+def make_job(cat, plans, req: Request, keep: bool, perms: dict | None = None) -> Job:
     if req.klass == "order":
-        return OrderJob(cat, plans, req, keep)
+        return OrderJob(cat, plans, req, keep, perms)
     if req.klass == "join":
         return JoinJob(cat, plans, req)
     if req.klass == "subquery":
@@ -368,7 +461,8 @@ def _wait_until(t0: float, at: float):
 def serve_plain(trace: list[Request], cat: Catalog, plans: Plans, keep: bool = False) -> dict:
     """One request at a time, in arrival order, on one stream."""
     stream = torch.cuda.Stream()
-    bufs = cat.slot_buffers(0).ensure()
+    bufs = cat.slot_buffers(0).ensure(plans)
+    plans.prepared_dim(cat)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for r in trace:
@@ -384,12 +478,21 @@ def serve_plain(trace: list[Request], cat: Catalog, plans: Plans, keep: bool = F
 
 
 def serve_continuous(trace: list[Request], cat: Catalog, plans: Plans, slots: int = 8, budget: float = 40e9,
-                     max_group: int = 64, keep: bool = False) -> dict:
+                     max_group: int = MAX_GROUP, keep: bool = False, share: bool = True) -> dict:
     """Admit requests as streams and budget free up; overlap their work on the
-    device; co-launch pending filter requests as one segmented launch."""
+    device; co-launch pending filter requests as one segmented launch.
+
+    With `share` (the default) the loop also shares work between requests:
+    pending requests identical to the one being dispatched (same class, table
+    and parameter) ride on its dispatch and complete with it; co-launched
+    filter requests on one table share one scan; and the sort permutation of
+    each ORDER BY table is kept resident (counted in the budget) once a request
+    has sorted it, so later ORDER BY requests on that table only gather."""
     streams = [torch.cuda.Stream() for _ in range(slots)]
+    perms: dict | None = {} if share else None
     for sl in range(slots):
-        cat.slot_buffers(sl).ensure()
+        cat.slot_buffers(sl).ensure(plans)
+    plans.prepared_dim(cat)
     free = list(range(slots))
     pending: deque[Request] = deque()
     ready: deque[Job] = deque()  # later stages of admitted requests (go first)
@@ -431,21 +534,30 @@ def serve_continuous(trace: list[Request], cat: Catalog, plans: Plans, slots: in
             else:
                 head = pending[0]
                 if head.klass == "filter":
-                    group = [r for r in pending if r.klass == "filter"][:max_group]
-                    job = FilterGroup(cat, plans, group)
+                    group = [r for r in pending if r.klass == "filter"]
+                    if not share:
+                        group = group[:max_group]
+                    job = FilterGroup(cat, plans, group, shared=share)
+                    if len(job.begin) > max_group:  # more distinct tables than states: the first max_group
+                        keep_t = set(sorted({r.table for r in group}, key=[r.table for r in group].index)[:max_group])
+                        job = FilterGroup(cat, plans, [r for r in group if r.table in keep_t], shared=share)
                 else:
-                    job = make_job(cat, plans, head, keep)
+                    job = make_job(cat, plans, head, keep, perms)
+                    if share:  # identical pending requests complete with this one
+                        key = (head.klass, head.table, head.param)
+                        job.reqs = [r for r in pending if (r.klass, r.table, r.param) == key]
             if used + job.mem > budget and inflight:
                 break  # wait for memory (first-come first-served)
             if ready and job is ready[0]:
                 ready.popleft()
-            elif isinstance(job, FilterGroup):
+            else:
                 ids = {id(r) for r in job.reqs}
                 pending = deque(r for r in pending if id(r) not in ids)
-            else:
-                pending.popleft()
             sl = free.pop()
+            had = set(perms) if perms is not None else None
             job.launch(streams[sl], cat.slot_buffers(sl))
+            if perms is not None and len(perms) > len(had):  # a permutation became resident
+                used += 4.0 * job.tbl.rows
             used += job.mem
             inflight.append((job, sl))
             peak_inflight = max(peak_inflight, len(inflight))
