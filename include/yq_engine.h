@@ -48,6 +48,16 @@ typedef struct yq_host_column {
  * reference's MAX_LIMIT_GPU_CACHE, include/config.hpp:19). Batches beyond the
  * budget move to pinned host memory and come back on demand. */
 yq_plan* yq_plan_create(uint64_t gpu_budget_bytes);
+/* The host tier's budget and the directory of the file tier (the reference's
+ * MAX_LIMIT_CPU_CACHE and cacheDir, include/config.hpp:17 and
+ * CacheManager::handleOverflow(Device::CPU),
+ * include/engine/cache_manager.hpp:82-85). When the batches spilled to pinned
+ * host memory exceed `host_budget_bytes`, the oldest move to files in
+ * `cache_dir`, written by a background task, null bytes included; they are
+ * read back (and the file removed) when an operator asks for them. 0 (the
+ * default) keeps spilled batches in host memory without limit. Returns
+ * YQ_ERR_INVALID_ARG for a budget without a directory. */
+int yq_plan_set_spill(yq_plan* plan, uint64_t host_budget_bytes, const char* cache_dir);
 void yq_plan_destroy(yq_plan* plan);
 /* Node builders return the new node id (>= 0) or -yq_status. */
 int yq_plan_scan(yq_plan* plan, const yq_host_column* cols, int32_t ncols, uint64_t rows,
@@ -85,6 +95,11 @@ int yq_plan_order_multi(yq_plan* plan, int32_t child, const int32_t* keys, const
 int yq_plan_group_by(yq_plan* plan, int32_t child, int32_t key_col, const yq_group_agg* aggs, int32_t nagg);
 int yq_plan_join(yq_plan* plan, int32_t left, int32_t right, const yq_join_cond* conds,
                  int32_t ncond);
+/* A join whose condition is an OR of ANDs: conds[i] belongs to disjunct group
+ * disjunct[i] (yq_join_project_or). The reference throws on OR in a join
+ * condition (include/engine/operators/expressions/filters/conjunction_join.hpp:113-114). */
+int yq_plan_join_or(yq_plan* plan, int32_t left, int32_t right, const yq_join_cond* conds,
+                    const int32_t* disjunct, int32_t ncond);
 int yq_plan_cross(yq_plan* plan, int32_t left, int32_t right);
 
 /* Pull every batch from `root` (ExecutorEngine::execute's loop,
@@ -99,13 +114,15 @@ int yq_result_column(const yq_result* r, int32_t c, yq_host_column* out);
 void yq_result_destroy(yq_result* r);
 
 /* Statistics of the last execute: batches pulled, bytes copied host->device
- * and device->host, device milliseconds of the compute stream. */
+ * and device->host, device milliseconds of the compute stream, and the moves
+ * of the cache manager's spill tiers. */
 typedef struct yq_plan_stats {
   uint64_t batches;
   uint64_t h2d_bytes;
   uint64_t d2h_bytes;
   double compute_ms;
-  uint64_t spilled_batches;
+  uint64_t spilled_batches; /* device -> pinned host moves */
+  uint64_t disk_batches;    /* pinned host -> file moves */
 } yq_plan_stats;
 int yq_plan_stats_read(const yq_plan* plan, yq_plan_stats* out);
 

@@ -279,7 +279,7 @@ int yq_filter_project_noalloc(const yq_batch* batch, const yq_program* predicate
 typedef struct yq_sort_config {
   int32_t digit_bits;        /* 4, 6 or 8; 0 = autotuned (yq_sort_autotune), else 8 */
   int32_t items_per_thread;  /* 0 = autotuned / the variant's default          */
-  int32_t block_threads;     /* fixed at 256 (kept for layout)                 */
+  int32_t block_threads;     /* 128, 256 or 512; 0 = autotuned / 256          */
   int32_t keep_trivial;      /* 1 = never skip passes (no host read-back)      */
 } yq_sort_config;
 
@@ -357,6 +357,23 @@ size_t yq_order_by_batch_workspace_size(const yq_batch* in, int32_t key_col, con
 int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
                 const uint32_t* run_offsets, int32_t nruns, yq_batch* out, void* workspace,
                 size_t workspace_bytes, void* stream);
+/* yq_order_by with the merge-path tile given: merge_items outputs per
+ * thread (4, 8 or 16; 16 needs a key of at most two words, else
+ * YQ_ERR_UNSUPPORTED; 0 = the tuned or default choice). */
+int yq_order_by_tiled(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
+                      const uint32_t* run_offsets, int32_t nruns, yq_batch* out, int32_t merge_items,
+                      void* workspace, size_t workspace_bytes, void* stream);
+/* Tunes yq_order_by for this input: the run-formation sort through
+ * yq_sort_autotune (digit bits, items per thread, block threads; returned in
+ * *best_sort) and the merge-path tile (outputs per thread, 4, 8 or 16; 16 for
+ * keys of up to two words) by timing the whole ORDER BY once per tile; the
+ * fastest tile is remembered for this key width and row count (log2) and
+ * used by later yq_order_by calls. The reference fixes the merge tile at
+ * compile time (ELE_PER_TH 6, src/kernels/merge_batchs.cu:8). Allocates its
+ * own output and workspace (stream-ordered) and synchronises `stream`. */
+int yq_order_by_autotune(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
+                         const uint32_t* run_offsets, int32_t nruns, yq_sort_config* best_sort,
+                         int32_t* best_merge_items, void* stream);
 
 /* ---- Batched forms: many independent tasks in one set of launches.
  * The tasks' rows sit back to back in one batch (task g = rows
@@ -374,10 +391,12 @@ int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descending, int32_t
  * With config->keep_trivial set it enqueues device work only and never waits
  * (it can be captured in a CUDA graph); an error is then left as a non-zero
  * 32-bit word at offset 0 of `workspace` (required in that mode).
- * yq_sort_autotune: times every instantiated (digit bits, items per thread)
- * variant on the given key and segments, remembers the fastest for this key
- * width and segment size (used whenever a sort's config leaves those fields 0)
- * and returns it. */
+ * yq_sort_autotune: times every instantiated (digit bits, items per thread,
+ * block threads) variant on the given key and segments, remembers the fastest
+ * for this key width and segment size (used whenever a sort's config leaves
+ * those fields 0) and returns it. The reference fixes these at compile time:
+ * OUR_RADIX 4 (include/kernels/radix_sort_kernel.hpp:9) and BLOCK_DIM 256
+ * (include/kernels/constants.hpp:7). */
 int yq_agg_states_init(void* states, int32_t count, const yq_agg_spec* aggs, int32_t nagg, void* stream);
 int yq_agg_states_read(const void* states, int32_t count, const yq_agg_spec* aggs, int32_t nagg,
                        yq_agg_result* out, void* stream);
@@ -451,6 +470,23 @@ int yq_join_project(const yq_batch* left, const yq_batch* right, const yq_join_c
                     int32_t ncond, const yq_join_output* outputs, int32_t nout,
                     yq_column* out, uint64_t capacity, uint64_t* count_host,
                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* Join conditions as an OR of ANDs (the reference rejects OR in a join
+ * condition, include/engine/operators/expressions/filters/conjunction_join.hpp:113-114,
+ * and evaluates AND chains with and_join_batches,
+ * src/kernels/comparison_operators_kernel.cu:24-54): condition i belongs to
+ * disjunct group disjunct[i] (0..G-1, every group used); a pair matches when
+ * all conditions of at least one group hold. A comparison with a NULL side
+ * does not hold. Same output order, capacity and workspace contract as
+ * yq_join_pairs / yq_join_project; always the nested-loop kernel. */
+int yq_join_pairs_or(const yq_batch* left, const yq_batch* right, const yq_join_cond* conds,
+                     const int32_t* disjunct, int32_t ncond, uint32_t* out_left, uint32_t* out_right,
+                     uint64_t capacity, uint64_t* count_host, void* workspace, size_t workspace_bytes,
+                     void* stream);
+int yq_join_project_or(const yq_batch* left, const yq_batch* right, const yq_join_cond* conds,
+                       const int32_t* disjunct, int32_t ncond, const yq_join_output* outputs, int32_t nout,
+                       yq_column* out, uint64_t capacity, uint64_t* count_host, void* workspace,
+                       size_t workspace_bytes, void* stream);
 
 /* Fused star-join aggregate: rows of `fact` passing `fact_predicate` are
  * probed against the rows of `dim` passing `dim_predicate` on

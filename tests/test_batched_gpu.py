@@ -89,5 +89,41 @@ def test_sort_autotune_choice_is_used(cuda):
     offs = [0, 100_000, 300_000]
     best = ops.sort_autotune(col, offs, descending=True)
     assert best.digit_bits in (4, 6, 8) and best.items_per_thread in (8, 12, 16)
+    assert best.block_threads in (128, 256, 512)
     perm = ops.sort_segments(col, offs, True, config=ops.sort_config(digit_bits=0))
     np.testing.assert_array_equal(perm.cpu().numpy().astype(np.int64), oracle.sort_perm(key, desc=True, segments=offs))
+
+
+@pytest.mark.parametrize("variant", [(8, 8, 512), (8, 12, 512), (6, 16, 128), (4, 16, 128), (8, 12, 256),
+                                     (6, 16, 256)])
+@pytest.mark.parametrize("kind", ["f32", "i64", "f32_nulls"])
+def test_every_block_size_variant(cuda, variant, kind):
+    """Each instantiated (digit bits, items per thread, block threads) sort
+    variant, asked for explicitly, gives the stable segmented sort; a variant
+    that is not instantiated for the key width falls back to 8-bit digits."""
+    d, items, block = variant
+    rng = np.random.default_rng(d * 100 + items + block)
+    n = 250_003
+    nulls = None
+    if kind == "f32":
+        key = rng.integers(-5000, 5000, n).astype(np.float32)
+    elif kind == "i64":
+        key = rng.integers(-(1 << 40), 1 << 40, n).astype(np.int64)
+    else:
+        key = rng.normal(0, 1, n).astype(np.float32)
+        nulls = rng.random(n) < 0.1
+    col = ops.DeviceColumn(torch.from_numpy(key).cuda(), A.FLOAT32 if key.dtype == np.float32 else A.INT64,
+                           None if nulls is None else torch.from_numpy(nulls.astype(np.uint8)).cuda())
+    offs = [0, 7, 100_000, 100_000, 250_003]
+    cfg = ops.sort_config(digit_bits=d, items_per_thread=items, block_threads=block)
+    perm = ops.sort_segments(col, offs, True, config=cfg)
+    want = oracle.sort_perm(key, desc=True, nulls=nulls, segments=offs)
+    np.testing.assert_array_equal(perm.cpu().numpy().astype(np.int64), want)
+
+
+def test_block_threads_validated(cuda):
+    key = np.arange(1000, dtype=np.float32)
+    col = ops.DeviceColumn(torch.from_numpy(key).cuda(), A.FLOAT32)
+    with pytest.raises(A.YQError) as e:
+        ops.sort_segments(col, [0, 1000], False, config=ops.sort_config(block_threads=96))
+    assert e.value.status == A.ERR_INVALID_ARG

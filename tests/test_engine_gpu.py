@@ -79,6 +79,60 @@ def test_order_by_query_with_spills(cuda, budget):
         assert p.stats().spilled_batches > 0
 
 
+@pytest.mark.parametrize("host_budget", [1 << 20, 1])
+def test_order_by_query_spills_to_files(cuda, tmp_path, host_budget):
+    """Device budget 1 MB and a host budget: spilled batches move on to files
+    in the cache directory (the reference's FS tier) with their null bytes,
+    come back for the merge, and the files are gone afterwards. The key and
+    a payload column carry nulls."""
+    rng = np.random.default_rng(12)
+    t = datagen.order_table(150_000, seed=3, dist="zipf")
+    knull = rng.random(len(t["key"])) < 0.03
+    inull = rng.random(len(t["key"])) < 0.1
+    cols = [t["key"], t["id"], t["txt"], t["d"]]
+    p = Plan(gpu_budget=1 << 20, host_budget=host_budget, cache_dir=str(tmp_path))
+    root = p.order(p.scan(cols, types=[A.FLOAT32, A.INT64, A.TEXT, A.DATETIME], nulls=[knull, inull, None, None],
+                          batch_rows=6000), 0, descending=True)
+    res = p.execute(root)
+    st = p.stats()
+    assert st.spilled_batches > 0 and st.disk_batches > 0
+    assert list(tmp_path.iterdir()) == []
+    perm = oracle.sort_perm(t["key"], desc=True, nulls=knull)
+    np.testing.assert_array_equal(res[0][1].astype(bool), knull[perm])
+    np.testing.assert_array_equal(res[1][1].astype(bool), inull[perm])
+    np.testing.assert_array_equal(np.where(knull[perm], 0, res[0][0]), np.where(knull[perm], 0, t["key"][perm]))
+    for (v, _), name in zip(res[1:], ["id", "txt", "d"]):
+        np.testing.assert_array_equal(v, t[name][perm])
+
+
+def test_spill_needs_a_directory(cuda):
+    from yallasql_b200.plan import lib as plan_lib
+    p = Plan()
+    assert plan_lib().yq_plan_set_spill(p.h, 1 << 20, None) == A.ERR_INVALID_ARG
+    assert plan_lib().yq_plan_set_spill(p.h, 0, None) == 0
+
+
+def test_or_join_query(cuda):
+    """JoinOperator with an OR of ANDs (the reference throws on OR in a join
+    condition): fact.datekey = dim.datekey OR fact.quantity > dim.year - 1945,
+    over several batches on both sides, against the union of the groups'
+    oracle pairs."""
+    fact, dim = datagen.star_tables(6_000, seed=4)
+    dyear = (dim["year"] - 1945).astype(np.int32)
+    p = Plan()
+    f = p.scan([fact["datekey"], fact["quantity"]], batch_rows=2048)
+    d = p.scan([dim["datekey"], dyear], batch_rows=700)
+    res = p.execute(p.join(f, d, [(0, 0, A.EQ), (1, 1, A.GT)], disjunct=[0, 1]))
+    got = sorted(zip(*[r[0].tolist() for r in res]))
+    pairs = set()
+    for conds in ([(0, 0, A.EQ)], [(1, 1, A.GT)]):
+        wl, wr = oracle.join_pairs([fact["datekey"], fact["quantity"]], [dim["datekey"], dyear], conds)
+        pairs.update(zip(wl.tolist(), wr.tolist()))
+    want = sorted((int(fact["datekey"][l]), int(fact["quantity"][l]), int(dim["datekey"][r]), int(dyear[r]))
+                  for l, r in pairs)
+    assert got == want
+
+
 def test_join_and_cross_product_queries(cuda):
     fact, dim = datagen.star_tables(50_000, seed=2)
     p = Plan()

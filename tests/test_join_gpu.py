@@ -49,6 +49,63 @@ def test_join_pairs_match_oracle(cuda, L, R, conds):
     np.testing.assert_array_equal(gr, wr)
 
 
+def union_pairs(lc, rc, conds, disjunct, ln, rn):
+    """Oracle of an OR of ANDs: the union of each group's conjunction pairs,
+    in (left, right) order."""
+    got = set()
+    for g in range(max(disjunct) + 1):
+        wl, wr = oracle.join_pairs(lc, rc, [c for c, d in zip(conds, disjunct) if d == g], ln, rn)
+        got.update(zip(wl.tolist(), wr.tolist()))
+    pairs = sorted(got)
+    return (np.array([p[0] for p in pairs], dtype=np.uint32), np.array([p[1] for p in pairs], dtype=np.uint32))
+
+
+@pytest.mark.parametrize("L,R", [(1, 1), (33, 17), (1025, 300), (3000, 9000)])
+@pytest.mark.parametrize("conds,disjunct", [
+    ([(0, 0, A.EQ), (1, 1, A.LT)], [0, 1]),                          # a.k = b.k OR a.v < b.v
+    ([(0, 0, A.EQ), (2, 2, A.GT), (3, 3, A.EQ)], [0, 0, 1]),         # (k = k AND f > f) OR t = t
+    ([(3, 3, A.NE), (1, 1, A.EQ), (0, 0, A.LE), (2, 2, A.LT)], [1, 0, 1, 2]),
+])
+def test_or_join_pairs_match_union_of_conjunctions(cuda, L, R, conds, disjunct):
+    """Join conditions as an OR of ANDs, NULL keys included (a comparison
+    with a NULL side does not hold in any group)."""
+    rng = np.random.default_rng(L * 7 + R)
+    lc, ln = random_side(rng, L, 0.05)
+    rc, rn = random_side(rng, R, 0.05)
+    lb = ops.DeviceBatch([dev_col(c, None, n) for c, n in zip(lc, ln)])
+    rb = ops.DeviceBatch([dev_col(c, None, n) for c, n in zip(rc, rn)])
+    gl, gr = pairs_np(*ops.join_pairs(lb, rb, conds, disjunct=disjunct))
+    wl, wr = union_pairs(lc, rc, conds, disjunct, ln, rn)
+    np.testing.assert_array_equal(gl, wl)
+    np.testing.assert_array_equal(gr, wr)
+    # the projecting form writes the same pairs' columns
+    out = ops.join_project(lb, rb, conds, [(0, 1), (1, 1)], disjunct=disjunct)
+    np.testing.assert_array_equal(out.columns[0].data.cpu().numpy(), lc[1][wl])
+    np.testing.assert_array_equal(out.columns[1].data.cpu().numpy(), rc[1][wr])
+
+
+def test_or_join_one_group_is_the_conjunction(cuda):
+    rng = np.random.default_rng(5)
+    lc, ln = random_side(rng, 2000, 0.05)
+    rc, rn = random_side(rng, 700, 0.05)
+    lb = ops.DeviceBatch([dev_col(c, None, n) for c, n in zip(lc, ln)])
+    rb = ops.DeviceBatch([dev_col(c, None, n) for c, n in zip(rc, rn)])
+    conds = [(0, 0, A.EQ), (1, 1, A.LT)]
+    a = pairs_np(*ops.join_pairs(lb, rb, conds, disjunct=[0, 0]))
+    b = pairs_np(*ops.join_pairs(lb, rb, conds))
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+
+
+def test_or_join_rejects_unused_group(cuda):
+    rng = np.random.default_rng(6)
+    lc, ln = random_side(rng, 10)
+    lb = ops.DeviceBatch([dev_col(c) for c in lc])
+    with pytest.raises(A.YQError) as e:
+        ops.join_pairs(lb, lb, [(0, 0, A.EQ), (1, 1, A.LT)], disjunct=[0, 2])
+    assert e.value.status == A.ERR_INVALID_ARG
+
+
 _NP_CMP = {A.LT: np.less, A.LE: np.less_equal, A.GT: np.greater, A.GE: np.greater_equal, A.EQ: np.equal,
            A.NE: np.not_equal}
 

@@ -173,3 +173,51 @@ def test_order_by_entry_matches_stable_sort(cuda, nruns, kind, desc, nulls_first
     np.testing.assert_array_equal(out.columns[2].data.cpu().numpy(), txt[perm])
     if nulls is not None:
         np.testing.assert_array_equal(out.columns[0].nulls.cpu().numpy().astype(bool), nulls[perm])
+
+
+@pytest.mark.parametrize("merge_items", [4, 8, 16])
+@pytest.mark.parametrize("kind", ["f32", "i64", "text32", "f32_nulls"])
+def test_order_by_every_merge_tile(cuda, merge_items, kind):
+    """yq_order_by_tiled: every merge-path tile (4, 8 or 16 outputs per thread)
+    gives the stable sort; 16 is refused for keys wider than two words."""
+    rng = np.random.default_rng(merge_items * 13 + len(kind))
+    sizes = rng.integers(1, 40_000, 9)
+    n = int(sizes.sum())
+    offs = [0] + list(np.cumsum(sizes).astype(int))
+    nulls = None
+    if kind == "f32":
+        k, t = rng.integers(-300, 300, n).astype(np.float32), A.FLOAT32
+    elif kind == "i64":
+        k, t = rng.integers(-(1 << 40), 1 << 40, n).astype(np.int64), A.INT64
+    elif kind == "text32":
+        k = np.zeros((n, 32), np.uint8)
+        k[:, :20] = rng.integers(97, 100, (n, 20))
+        t = A.TEXT
+    else:
+        k, t = rng.normal(0, 10, n).astype(np.float32), A.FLOAT32
+        nulls = rng.random(n) < 0.2
+    payload = np.arange(n, dtype=np.int64)
+    b = ops.DeviceBatch([dev_col(k, t, nulls), dev_col(payload)])
+    if kind == "text32" and merge_items == 16:
+        with pytest.raises(A.YQError) as e:
+            ops.order_by(b, 0, True, offs, merge_items=merge_items)
+        assert e.value.status == A.ERR_UNSUPPORTED
+        return
+    out = ops.order_by(b, 0, True, offs, merge_items=merge_items)
+    perm = oracle.sort_perm(k, desc=True, nulls=nulls)
+    np.testing.assert_array_equal(out.columns[1].data.cpu().numpy(), payload[perm])
+
+
+def test_order_by_autotune_then_order_by(cuda):
+    """The tuner returns a sort variant and a merge tile; later yq_order_by
+    calls on that shape use them and still give the stable sort."""
+    rows = 600_000
+    t = datagen.order_table(rows, seed=9, dist="zipf")
+    b = table_batch(t)
+    offs = list(range(0, rows, 116_480)) + [rows]
+    best, items = ops.order_by_autotune(b, 0, True, offs)
+    assert best.digit_bits in (4, 6, 8) and best.block_threads in (128, 256, 512) and items in (4, 8, 16)
+    out = ops.order_by(b, 0, True, offs)
+    perm = oracle.sort_perm(t["key"], desc=True)
+    for col, n in zip(out.columns, ["key", "id", "txt", "d"]):
+        np.testing.assert_array_equal(col.data.cpu().numpy(), t[n][perm])

@@ -141,11 +141,16 @@ PROTOTYPES = {
     "yq_order_by_segments_perm": (C.c_int, [P(Batch), i32, i32, i32, P(u32), i32, P(Batch), vp, P(SortConfig), vp,
                                             sz, vp]),
     "yq_sort_autotune": (C.c_int, [P(Column), u32, P(u32), i32, i32, P(SortConfig), vp]),
+    "yq_order_by_tiled": (C.c_int, [P(Batch), i32, i32, i32, P(u32), i32, P(Batch), i32, vp, sz, vp]),
+    "yq_order_by_autotune": (C.c_int, [P(Batch), i32, i32, i32, P(u32), i32, P(SortConfig), P(i32), vp]),
     "yq_order_by": (C.c_int, [P(Batch), i32, i32, i32, P(u32), i32, P(Batch), vp, sz, vp]),
     "yq_join_workspace_size": (sz, [u32, u32]),
     "yq_join_pairs": (C.c_int, [P(Batch), P(Batch), P(JoinCond), i32, vp, vp, u64, P(u64), vp, sz, vp]),
     "yq_join_project": (C.c_int, [P(Batch), P(Batch), P(JoinCond), i32, P(JoinOutput), i32, P(Column), u64,
                                   P(u64), vp, sz, vp]),
+    "yq_join_pairs_or": (C.c_int, [P(Batch), P(Batch), P(JoinCond), vp, i32, vp, vp, u64, P(u64), vp, sz, vp]),
+    "yq_join_project_or": (C.c_int, [P(Batch), P(Batch), P(JoinCond), vp, i32, P(JoinOutput), i32, P(Column), u64,
+                                     P(u64), vp, sz, vp]),
     "yq_join_aggregate_workspace_size": (sz, [u32, u32, i32]),
     "yq_join_dim_table_size": (sz, [u32]),
     "yq_join_dim_table_build": (C.c_int, [P(Batch), P(Program), i32, P(Constants), vp, sz, P(u32), vp]),

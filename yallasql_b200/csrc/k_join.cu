@@ -51,6 +51,10 @@ struct JOut {
 struct JoinParams {
   JCond cond[kMaxConds];
   int32_t ncond;
+  // OR of ANDs: condition i belongs to disjunct group[i]; a pair matches when
+  // every condition of at least one group holds. ngroups <= 1: one conjunction.
+  int8_t group[kMaxConds];
+  int32_t ngroups;
   int32_t eq;  // index of the equality condition used for hashing (-1: nested loop)
   JOut out[kMaxJoinOut];
   int32_t nout;          // 0: write pairs
@@ -126,7 +130,26 @@ __device__ __forceinline__ bool cond_holds(const JCond& c, uint32_t l, uint32_t 
   return cmp_holds(s, c.cmp);
 }
 
+// A disjunction of conjunctions: a group fails at its first condition that
+// does not hold (a comparison with a NULL side does not hold), later
+// conditions of a failed group are skipped, and the pair matches while some
+// group has not failed. Only TRUE selects a pair, so this two-valued
+// evaluation gives the rows SQL's three-valued OR/AND selects.
+__device__ __forceinline__ bool any_group(const JoinParams& J, uint32_t l, uint32_t r) {
+  const uint32_t all = (1u << J.ngroups) - 1u;
+  uint32_t failed = 0u;
+  for (int i = 0; i < J.ncond; ++i) {
+    const uint32_t bit = 1u << J.group[i];
+    if (!(failed & bit) && !cond_holds(J.cond[i], l, r)) {
+      failed |= bit;
+      if (failed == all) return false;
+    }
+  }
+  return true;
+}
+
 __device__ __forceinline__ bool all_conds(const JoinParams& J, uint32_t l, uint32_t r, int skip) {
+  if (J.ngroups > 1) return any_group(J, l, r);
   for (int i = 0; i < J.ncond; ++i)
     if (i != skip && !cond_holds(J.cond[i], l, r)) return false;
   return true;
@@ -621,8 +644,8 @@ static int build_table(const yq_batch* right, const yq_program* pred, const yq_c
 }
 
 // Shared by yq_join_pairs / yq_join_project.
-static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_cond* conds, int32_t ncond,
-                     const yq_join_output* outputs, int32_t nout, yq_column* out, uint32_t* out_left,
+static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_cond* conds, const int32_t* disjunct,
+                     int32_t ncond, const yq_join_output* outputs, int32_t nout, yq_column* out, uint32_t* out_left,
                      uint32_t* out_right, uint64_t capacity, uint64_t* count_host, void* workspace,
                      size_t workspace_bytes, cudaStream_t s) {
   if (!left || !right || ncond < 0 || ncond > kMaxConds || (ncond > 0 && !conds) || nout < 0 || nout > kMaxJoinOut ||
@@ -634,6 +657,19 @@ static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_
   J.R = right->rows;
   J.ncond = ncond;
   J.eq = -1;
+  J.ngroups = 1;
+  if (disjunct && ncond > 0) {  // groups numbered 0..G-1, each used by some condition
+    int g = 0;
+    uint32_t used = 0u;
+    for (int i = 0; i < ncond; ++i) {
+      if (disjunct[i] < 0 || disjunct[i] >= kMaxConds) return YQ_ERR_INVALID_ARG;
+      J.group[i] = (int8_t)disjunct[i];
+      used |= 1u << disjunct[i];
+      g = disjunct[i] + 1 > g ? disjunct[i] + 1 : g;
+    }
+    if (used != (1u << g) - 1u) return YQ_ERR_INVALID_ARG;
+    J.ngroups = g;
+  }
   for (int i = 0; i < ncond; ++i) {
     const yq_join_cond& c = conds[i];
     if (c.left_col < 0 || c.left_col >= left->ncols || c.right_col < 0 || c.right_col >= right->ncols ||
@@ -645,7 +681,7 @@ static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_
     J.cond[i].l = jcol(a);
     J.cond[i].r = jcol(b);
     J.cond[i].cmp = c.cmp;
-    if (J.eq < 0 && c.cmp == YQ_EQ && hashable(a.type)) J.eq = i;
+    if (J.eq < 0 && J.ngroups == 1 && c.cmp == YQ_EQ && hashable(a.type)) J.eq = i;
   }
   for (int o = 0; o < nout; ++o) {
     const yq_join_output& w = outputs[o];
@@ -727,7 +763,7 @@ static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_
   } else {
     ProfScope ps("join_nested_loop", s, (double)J.L * J.R * 0.0);
     const JCond& c0 = J.cond[0];
-    const bool typed = J.ncond == 1 && c0.l.type == c0.r.type && !c0.l.nulls && !c0.r.nulls &&
+    const bool typed = J.ncond == 1 && J.ngroups == 1 && c0.l.type == c0.r.type && !c0.l.nulls && !c0.r.nulls &&
                        c0.l.width == c0.r.width && (c0.l.type == YQ_INT32 || c0.l.type == YQ_FLOAT32 ||
                                                      c0.l.type == YQ_INT64 || c0.l.type == YQ_DATETIME ||
                                                      c0.l.type == YQ_FLOAT64);
@@ -774,16 +810,33 @@ size_t yq_join_workspace_size(uint32_t left_rows, uint32_t right_rows) {
 int yq_join_pairs(const yq_batch* left, const yq_batch* right, const yq_join_cond* conds, int32_t ncond,
                   uint32_t* out_left, uint32_t* out_right, uint64_t capacity, uint64_t* count_host, void* workspace,
                   size_t workspace_bytes, void* stream) {
-  return join_impl(left, right, conds, ncond, nullptr, 0, nullptr, out_left, out_right, capacity, count_host,
-                   workspace, workspace_bytes, as_stream(stream));
+  return join_impl(left, right, conds, nullptr, ncond, nullptr, 0, nullptr, out_left, out_right, capacity,
+                   count_host, workspace, workspace_bytes, as_stream(stream));
 }
 
 int yq_join_project(const yq_batch* left, const yq_batch* right, const yq_join_cond* conds, int32_t ncond,
                     const yq_join_output* outputs, int32_t nout, yq_column* out, uint64_t capacity,
                     uint64_t* count_host, void* workspace, size_t workspace_bytes, void* stream) {
   if (nout <= 0) return YQ_ERR_INVALID_ARG;
-  return join_impl(left, right, conds, ncond, outputs, nout, out, nullptr, nullptr, capacity, count_host, workspace,
-                   workspace_bytes, as_stream(stream));
+  return join_impl(left, right, conds, nullptr, ncond, outputs, nout, out, nullptr, nullptr, capacity, count_host,
+                   workspace, workspace_bytes, as_stream(stream));
+}
+
+int yq_join_pairs_or(const yq_batch* left, const yq_batch* right, const yq_join_cond* conds, const int32_t* disjunct,
+                     int32_t ncond, uint32_t* out_left, uint32_t* out_right, uint64_t capacity, uint64_t* count_host,
+                     void* workspace, size_t workspace_bytes, void* stream) {
+  if (ncond <= 0 || !disjunct) return YQ_ERR_INVALID_ARG;
+  return join_impl(left, right, conds, disjunct, ncond, nullptr, 0, nullptr, out_left, out_right, capacity,
+                   count_host, workspace, workspace_bytes, as_stream(stream));
+}
+
+int yq_join_project_or(const yq_batch* left, const yq_batch* right, const yq_join_cond* conds,
+                       const int32_t* disjunct, int32_t ncond, const yq_join_output* outputs, int32_t nout,
+                       yq_column* out, uint64_t capacity, uint64_t* count_host, void* workspace,
+                       size_t workspace_bytes, void* stream) {
+  if (nout <= 0 || ncond <= 0 || !disjunct) return YQ_ERR_INVALID_ARG;
+  return join_impl(left, right, conds, disjunct, ncond, outputs, nout, out, nullptr, nullptr, capacity, count_host,
+                   workspace, workspace_bytes, as_stream(stream));
 }
 
 size_t yq_join_aggregate_workspace_size(uint32_t fact_rows, uint32_t dim_rows, int32_t nagg) {

@@ -13,6 +13,8 @@
 //      on an mbarrier, merges there (ties take run A, so the merge is stable),
 //      and moves every payload column with coalesced writes.
 #include <string.h>
+#include <map>
+#include <mutex>
 #include <vector>
 #include "yq_sort.cuh"
 
@@ -399,14 +401,15 @@ __device__ __forceinline__ uint32_t raw_corank(const uint32_t* keys, const RawPa
   return lo;
 }
 
-template <int KW>
+template <int KW, int ITEMS>
 __global__ void k_merge_raw_partition(const __grid_constant__ RawLevel L) {
+  constexpr uint32_t TILE = kMergeBlock * ITEMS;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= L.ntiles) return;
   const RawPair p = L.pairs[raw_pair_of_tile(L.pairs, L.npairs, t)];
   const uint32_t total = p.m + p.n;
-  const uint32_t k0 = (t - p.tile0) * kMergeTile;
-  const uint32_t k1 = min(k0 + kMergeTile, total);
+  const uint32_t k0 = (t - p.tile0) * TILE;
+  const uint32_t k1 = min(k0 + TILE, total);
   if (k0 >= total) {  // a descriptor with no work (never produced by the host plan)
     L.tiles[t] = RawTile{0, 0, 0, 0, 0, 0, 0, 0};
     atomicOr(L.err, kErrBounds);
@@ -431,11 +434,15 @@ struct RawSlot {
   uint32_t ka, kb, ia, ib;  // byte offsets of the first A / B key and id in the slot
 };
 
-template <int KW>
+// ITEMS outputs per thread: a tile of kMergeBlock * ITEMS outputs. Variants
+// (KW, ITEMS) whose kRawStages slots fit the 227 KB of shared memory:
+// ITEMS 4 and 8 for every key width, 16 for one and two key words.
+template <int KW, int ITEMS>
 struct RawGeom {
   static constexpr uint32_t W = 4u * KW;
-  static constexpr uint32_t kreg = kMergeTile * W + 64;  // keys of both windows + alignment slack
-  static constexpr uint32_t ireg = kMergeTile * 4 + 64;  // ids of both windows + alignment slack
+  static constexpr uint32_t TILE = kMergeBlock * ITEMS;
+  static constexpr uint32_t kreg = TILE * W + 64;  // keys of both windows + alignment slack
+  static constexpr uint32_t ireg = TILE * 4 + 64;  // ids of both windows + alignment slack
   static constexpr uint32_t slot = kreg + ireg;
   static constexpr size_t smem = (size_t)kRawStages * slot + kRawStages * 8;
 };
@@ -456,10 +463,10 @@ __device__ __forceinline__ uint32_t raw_window(unsigned char* region, uint32_t& 
 }
 
 // Thread 0: start the copies of tile descriptor d into `slot`.
-template <int KW>
+template <int KW, int ITEMS>
 __device__ __forceinline__ void raw_issue(const RawLevel& L, const RawTile& d, int slot, unsigned char* smem,
                                           RawSlot* s_slot) {
-  using G = RawGeom<KW>;
+  using G = RawGeom<KW, ITEMS>;
   unsigned char* kreg = smem + (size_t)slot * G::slot;
   unsigned char* ireg = kreg + G::kreg;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + (size_t)kRawStages * G::slot) + slot;
@@ -554,9 +561,9 @@ __device__ __forceinline__ void decode_store(const KeyDecode& d, size_t row, con
   }
 }
 
-template <int KW>
+template <int KW, int ITEMS>
 __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_constant__ RawLevel L) {
-  using G = RawGeom<KW>;
+  using G = RawGeom<KW, ITEMS>;
   extern __shared__ __align__(128) unsigned char raw_smem[];
   __shared__ RawSlot s_slot[kRawStages];
   uint64_t* bars = reinterpret_cast<uint64_t*>(raw_smem + (size_t)kRawStages * G::slot);
@@ -568,7 +575,7 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
   if (threadIdx.x == 0) {
     for (int j = 0; j < kRawStages - 1; ++j) {
       const uint32_t t = blockIdx.x + (uint32_t)j * GR;
-      if (t < NT) raw_issue<KW>(L, L.tiles[t], j, raw_smem, s_slot);
+      if (t < NT) raw_issue<KW, ITEMS>(L, L.tiles[t], j, raw_smem, s_slot);
     }
     const uint32_t t = blockIdx.x + (uint32_t)(kRawStages - 1) * GR;
     if (t < NT) next = L.tiles[t];
@@ -581,7 +588,7 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
       const uint32_t tn = t + (uint32_t)(kRawStages - 1) * GR;
       const int ns = slot == 0 ? kRawStages - 1 : slot - 1;
       if (tn < NT) {
-        raw_issue<KW>(L, next, ns, raw_smem, s_slot);
+        raw_issue<KW, ITEMS>(L, next, ns, raw_smem, s_slot);
         const uint32_t tf = tn + GR;  // descriptor for the next issue, loaded a tile ahead
         if (tf < NT) next = L.tiles[tf];
       }
@@ -593,10 +600,10 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
     const unsigned char* kA = kreg + r.ka;
     const unsigned char* kB = kreg + r.kb;
 
-    // Each thread merges kMergeItems consecutive outputs of the tile in
+    // Each thread merges ITEMS consecutive outputs of the tile in
     // registers and stores them itself: a warp's stores cover one contiguous
-    // run of 32 x kMergeItems outputs (16-byte stores when aligned).
-    const uint32_t kk = threadIdx.x * kMergeItems;
+    // run of 32 x ITEMS outputs (16-byte stores when aligned).
+    const uint32_t kk = threadIdx.x * ITEMS;
     if (kk < r.cnt) {
       uint32_t lo = kk > r.nb ? kk - r.nb : 0u, hi = kk < r.na ? kk : r.na;
       while (lo < hi) {
@@ -615,10 +622,10 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
       if (jb < r.nb) raw_key_s<KW>(kB + (size_t)jb * G::W, kb);
       const uint32_t* idA = reinterpret_cast<const uint32_t*>(ireg + r.ia);
       const uint32_t* idB = reinterpret_cast<const uint32_t*>(ireg + r.ib);
-      uint32_t okey[kMergeItems][KW], oid[kMergeItems];
-      const uint32_t m = r.cnt - kk < (uint32_t)kMergeItems ? r.cnt - kk : (uint32_t)kMergeItems;
+      uint32_t okey[ITEMS][KW], oid[ITEMS];
+      const uint32_t m = r.cnt - kk < (uint32_t)ITEMS ? r.cnt - kk : (uint32_t)ITEMS;
 #pragma unroll
-      for (int x = 0; x < kMergeItems; ++x) {
+      for (int x = 0; x < ITEMS; ++x) {
         if ((uint32_t)x >= m) break;
         const bool takeA = ia < r.na && (jb >= r.nb || key_le<KW>(ka, kb));
         if (takeA) {
@@ -634,29 +641,29 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
         }
       }
       const size_t o0 = (size_t)r.out0 + kk;
-      if (m == (uint32_t)kMergeItems && (o0 & 3u) == 0u) {
+      if (m == (uint32_t)ITEMS && (o0 & 3u) == 0u) {
 #pragma unroll
-        for (int x = 0; x < kMergeItems; x += 4)
+        for (int x = 0; x < ITEMS; x += 4)
           *reinterpret_cast<uint4*>(L.ids_out + o0 + x) = make_uint4(oid[x], oid[x + 1], oid[x + 2], oid[x + 3]);
       } else {
 #pragma unroll
-        for (int x = 0; x < kMergeItems; ++x)
+        for (int x = 0; x < ITEMS; ++x)
           if ((uint32_t)x < m) L.ids_out[o0 + x] = oid[x];
       }
       if (L.keys_out) {
-        if (KW == 1 && m == (uint32_t)kMergeItems && (o0 & 3u) == 0u) {
+        if (KW == 1 && m == (uint32_t)ITEMS && (o0 & 3u) == 0u) {
 #pragma unroll
-          for (int x = 0; x < kMergeItems; x += 4)
+          for (int x = 0; x < ITEMS; x += 4)
             *reinterpret_cast<uint4*>(L.keys_out + o0 + x) =
                 make_uint4(okey[x][0], okey[x + 1][0], okey[x + 2][0], okey[x + 3][0]);
         } else {
 #pragma unroll
-          for (int x = 0; x < kMergeItems; ++x)
+          for (int x = 0; x < ITEMS; ++x)
             if ((uint32_t)x < m) raw_key_store<KW>(L.keys_out, o0 + x, okey[x]);
         }
       } else if (L.dec.out) {
 #pragma unroll
-        for (int x = 0; x < kMergeItems; ++x)
+        for (int x = 0; x < ITEMS; ++x)
           if ((uint32_t)x < m) decode_store<KW>(L.dec, o0 + x, okey[x]);
       }
     }
@@ -667,21 +674,62 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
   }
 }
 
-template <int KW>
+template <int KW, int ITEMS>
 static int launch_raw_level(const RawLevel& L, cudaStream_t s, double bytes) {
-  using G = RawGeom<KW>;
-  YQ_TRY(kernel_allow_smem((const void*)k_merge_raw_tiles<KW>, G::smem));
-  const int cap = kernel_blocks_per_sm((const void*)k_merge_raw_tiles<KW>, kMergeBlock, G::smem) * sm_count();
+  using G = RawGeom<KW, ITEMS>;
+  static_assert(G::smem <= 227 * 1024, "stage slots exceed shared memory");
+  YQ_TRY(kernel_allow_smem((const void*)k_merge_raw_tiles<KW, ITEMS>, G::smem));
+  const int cap = kernel_blocks_per_sm((const void*)k_merge_raw_tiles<KW, ITEMS>, kMergeBlock, G::smem) * sm_count();
   {
     ProfScope ps("merge_partition", s, 0.0);
-    k_merge_raw_partition<KW><<<ceil_div<uint32_t>(L.ntiles, 128), 128, 0, s>>>(L);
+    k_merge_raw_partition<KW, ITEMS><<<ceil_div<uint32_t>(L.ntiles, 128), 128, 0, s>>>(L);
     YQ_CHECK_LAUNCH();
   }
   const int grid = (int)(L.ntiles < (uint32_t)cap ? L.ntiles : (uint32_t)cap);
   ProfScope ps("merge_tiles", s, bytes);
-  k_merge_raw_tiles<KW><<<grid, kMergeBlock, G::smem, s>>>(L);
+  k_merge_raw_tiles<KW, ITEMS><<<grid, kMergeBlock, G::smem, s>>>(L);
   YQ_CHECK_LAUNCH();
   return YQ_OK;
+}
+
+static bool merge_items_ok(int kw, int items) {
+  return items == 4 || items == 8 || (items == 16 && kw <= 2);
+}
+
+static int launch_raw_level_items(int kw, int items, const RawLevel& L, cudaStream_t s, double bytes) {
+  switch (kw * 100 + items) {
+    case 104: return launch_raw_level<1, 4>(L, s, bytes);
+    case 108: return launch_raw_level<1, 8>(L, s, bytes);
+    case 116: return launch_raw_level<1, 16>(L, s, bytes);
+    case 204: return launch_raw_level<2, 4>(L, s, bytes);
+    case 208: return launch_raw_level<2, 8>(L, s, bytes);
+    case 216: return launch_raw_level<2, 16>(L, s, bytes);
+    case 404: return launch_raw_level<4, 4>(L, s, bytes);
+    case 408: return launch_raw_level<4, 8>(L, s, bytes);
+    case 804: return launch_raw_level<8, 4>(L, s, bytes);
+    case 808: return launch_raw_level<8, 8>(L, s, bytes);
+    default: return YQ_ERR_UNSUPPORTED;
+  }
+}
+
+// Merge-path tile (outputs per thread) per (key words, log2 of rows), set by
+// yq_order_by_autotune; kMergeItems where none was tuned.
+static std::mutex g_merge_tune_mu;
+static std::map<std::pair<int, int>, int> g_merge_tuned;
+
+static int log2_rows(uint32_t rows) {
+  int b = 0;
+  while (rows > 1) {
+    rows >>= 1;
+    ++b;
+  }
+  return b;
+}
+
+static int merge_items_for(int kw, uint32_t rows) {
+  std::lock_guard<std::mutex> lk(g_merge_tune_mu);
+  auto it = g_merge_tuned.find({kw, log2_rows(rows)});
+  return it == g_merge_tuned.end() ? kMergeItems : it->second;
 }
 
 // *flag |= 1 when a key value would not survive the key-word round trip
@@ -710,7 +758,7 @@ struct OrderPlan {
   std::vector<uint32_t> level_tiles;  // tiles per level
 };
 
-static void plan_order_levels(const uint32_t* offsets, int nruns, OrderPlan& P) {
+static void plan_order_levels(const uint32_t* offsets, int nruns, uint32_t tile, OrderPlan& P) {
   std::vector<uint32_t> offs(offsets, offsets + nruns + 1);
   P.pairs.clear();
   P.level_first.clear();
@@ -728,7 +776,7 @@ static void plan_order_levels(const uint32_t* offsets, int nruns, OrderPlan& P) 
       p.n = (r + 1 < runs) ? offs[r + 2] - offs[r + 1] : 0u;
       p.tile0 = tiles;
       next.push_back(offs[r]);
-      const uint32_t t = ceil_div<uint32_t>(p.m + p.n, kMergeTile);
+      const uint32_t t = ceil_div<uint32_t>(p.m + p.n, tile);
       if (t == 0) continue;  // empty pair
       tiles += t;
       P.pairs.push_back(p);
@@ -782,7 +830,7 @@ static int order_ws_layout(const yq_column& key, uint32_t rows, const uint32_t* 
   if (o.kw_max < 0) return YQ_ERR_INVALID_ARG;
   KeyJob j{key, 0, 0};
   YQ_TRY(sort_segments_impl(&j, 1, rows, offsets, nruns, nullptr, nullptr, nullptr, 0, nullptr, &o.sort_bytes));
-  o.max_tiles = ceil_div<uint32_t>(rows, kMergeTile) + (uint32_t)nruns + 1;
+  o.max_tiles = ceil_div<uint32_t>(rows, kMergeBlock * 4u) + (uint32_t)nruns + 1;  // the smallest merge tile
   o.npairs = (size_t)nruns + 64;
   w.add<char>(o.sort_bytes);
   w.add<uint32_t>((size_t)rows * o.kw_max + 16);  // keys, two buffers
@@ -893,9 +941,11 @@ extern "C" int yq_order_by_segments_perm(const yq_batch* in, int32_t key_col, in
                                 workspace, workspace_bytes, stream);
 }
 
-extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
-                           const uint32_t* run_offsets, int32_t nruns, yq_batch* out, void* workspace,
-                           size_t workspace_bytes, void* stream) {
+// merge_items: outputs per thread of the merge tiles (0 = the tuned or default
+// choice); *kw_used (optional): the key words the merge levels compared.
+static int order_by_run(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
+                        const uint32_t* run_offsets, int32_t nruns, yq_batch* out, void* workspace,
+                        size_t workspace_bytes, void* stream, int merge_items, int* kw_used = nullptr) {
   if (!in || !out || !run_offsets || nruns <= 0 || key_col < 0 || key_col >= in->ncols || out->ncols != in->ncols ||
       in->ncols > YQ_MAX_BATCH_COLUMNS)
     return YQ_ERR_INVALID_ARG;
@@ -969,8 +1019,11 @@ extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descendi
   // 2. merge levels over (key words, row id)
   int cur = 0;
   if (merged) {
+    if (kw_used) *kw_used = kw;
+    const int mi = merge_items ? merge_items : merge_items_for(kw, rows);
+    if (!merge_items_ok(kw, mi)) return YQ_ERR_UNSUPPORTED;
     OrderPlan P;
-    plan_order_levels(run_offsets, nruns, P);
+    plan_order_levels(run_offsets, nruns, kMergeBlock * (uint32_t)mi, P);
     if (P.pairs.size() > o.npairs) return YQ_ERR_UNSUPPORTED;
     YQ_TRY(h2d_async(d_pairs, P.pairs.data(), P.pairs.size() * sizeof(RawPair), s));
     const int levels = (int)P.level_tiles.size();
@@ -999,13 +1052,7 @@ extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descendi
       if (L.ntiles == 0) continue;
       // algorithmic bytes: key words + id in and out (ids only out on the last level)
       const double bytes = (double)rows * (4.0 * kw + 4.0 + (last ? 4.0 : 4.0 * kw + 4.0));
-      switch (kw) {
-        case 1: YQ_TRY(launch_raw_level<1>(L, s, bytes)); break;
-        case 2: YQ_TRY(launch_raw_level<2>(L, s, bytes)); break;
-        case 4: YQ_TRY(launch_raw_level<4>(L, s, bytes)); break;
-        case 8: YQ_TRY(launch_raw_level<8>(L, s, bytes)); break;
-        default: return YQ_ERR_UNSUPPORTED;
-      }
+      YQ_TRY(launch_raw_level_items(kw, mi, L, s, bytes));
       cur ^= 1;
     }
   }
@@ -1017,6 +1064,93 @@ extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descendi
   const uint32_t e = err[0] | err[1];
   if (e & kErrTimeout) return YQ_ERR_TIMEOUT;
   if (e & kErrBounds) return YQ_ERR_INVALID_ARG;
+  return YQ_OK;
+}
+
+extern "C" int yq_order_by(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
+                           const uint32_t* run_offsets, int32_t nruns, yq_batch* out, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+  return order_by_run(in, key_col, descending, nulls_first, run_offsets, nruns, out, workspace, workspace_bytes,
+                      stream, 0);
+}
+
+extern "C" int yq_order_by_tiled(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
+                                 const uint32_t* run_offsets, int32_t nruns, yq_batch* out, int32_t merge_items,
+                                 void* workspace, size_t workspace_bytes, void* stream) {
+  if (merge_items != 0 && merge_items != 4 && merge_items != 8 && merge_items != 16) return YQ_ERR_INVALID_ARG;
+  return order_by_run(in, key_col, descending, nulls_first, run_offsets, nruns, out, workspace, workspace_bytes,
+                      stream, merge_items);
+}
+
+extern "C" int yq_order_by_autotune(const yq_batch* in, int32_t key_col, int32_t descending, int32_t nulls_first,
+                                    const uint32_t* run_offsets, int32_t nruns, yq_sort_config* best_sort,
+                                    int32_t* best_merge_items, void* stream) {
+  if (!in || !run_offsets || nruns <= 0 || key_col < 0 || key_col >= in->ncols || in->ncols > YQ_MAX_BATCH_COLUMNS ||
+      !best_sort || !best_merge_items)
+    return YQ_ERR_INVALID_ARG;
+  cudaStream_t s = as_stream(stream);
+  // run formation: the sort's own tuner over the runs as segments
+  YQ_TRY(yq_sort_autotune(&in->columns[key_col], in->rows, run_offsets, nruns, descending, best_sort, stream));
+  *best_merge_items = kMergeItems;
+  const int kw = sort_key_words_max(in->columns[key_col]);
+  if (nruns < 2 || in->rows == 0 || kw <= 0) return YQ_OK;
+  // merge levels: time the whole ORDER BY for each merge tile (an output
+  // batch and a workspace of its own, freed before returning)
+  yq_column oc[YQ_MAX_BATCH_COLUMNS];
+  void* bufs[2 * YQ_MAX_BATCH_COLUMNS + 1] = {nullptr};
+  int nb = 0;
+  int status = YQ_OK;
+  for (int c = 0; c < in->ncols && status == YQ_OK; ++c) {
+    oc[c] = in->columns[c];
+    void* d = nullptr;
+    void* n = nullptr;
+    if (cudaMallocAsync(&d, (size_t)in->rows * oc[c].width + 16, s) != cudaSuccess) status = YQ_ERR_ALLOC;
+    bufs[nb++] = d;
+    if (status == YQ_OK && oc[c].nulls && cudaMallocAsync(&n, (size_t)in->rows + 16, s) != cudaSuccess)
+      status = YQ_ERR_ALLOC;
+    bufs[nb++] = n;
+    oc[c].data = d;
+    oc[c].nulls = static_cast<const uint8_t*>(n);
+  }
+  yq_batch out{oc, in->ncols, in->rows};
+  const size_t wsb = yq_order_by_batch_workspace_size(in, key_col, run_offsets, nruns);
+  void* ws = nullptr;
+  if (status == YQ_OK && (wsb == 0 || cudaMallocAsync(&ws, wsb, s) != cudaSuccess)) status = YQ_ERR_ALLOC;
+  bufs[nb++] = ws;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (status == YQ_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+    status = YQ_ERR_CUDA;
+  float best_ms = 1e30f;
+  int pick = kMergeItems;
+  int kw_merge = 0;
+  for (int items : {8, 4, 16}) {
+    if (status != YQ_OK) break;
+    if (!merge_items_ok(kw, items)) continue;
+    status = order_by_run(in, key_col, descending, nulls_first, run_offsets, nruns, &out, ws, wsb, stream, items,
+                          &kw_merge);
+    if (status != YQ_OK) break;
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 2 && status == YQ_OK; ++r)
+      status = order_by_run(in, key_col, descending, nulls_first, run_offsets, nruns, &out, ws, wsb, stream, items);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (status == YQ_OK && ms < best_ms) {
+      best_ms = ms;
+      pick = items;
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  for (int i = 0; i < nb; ++i)
+    if (bufs[i]) cudaFreeAsync(bufs[i], s);
+  if (status != YQ_OK) return status;
+  if (kw_merge > 0) {  // keyed by the key words the merge levels compare
+    std::lock_guard<std::mutex> lk(g_merge_tune_mu);
+    g_merge_tuned[{kw_merge, log2_rows(in->rows)}] = pick;
+  }
+  *best_merge_items = pick;
   return YQ_OK;
 }
 

@@ -154,16 +154,22 @@ struct SweepParams {
 // Blocks per SM the registers are sized for: four for the variants whose
 // keys, values and ranks fit 64 registers without spilling (one key word, up
 // to 12 items per thread, or 8 items of two words), three otherwise.
+// Blocks of 512 threads get half as many blocks per SM and blocks of 128
+// twice as many, so the per-thread register budget stays the same.
 constexpr int sweep_min_blocks(int kw, int d, int items) { return (kw * items <= 12 && d == 8) || (kw == 2 && items <= 8 && d == 8) ? 4 : 3; }
+constexpr int sweep_min_blocks(int kw, int d, int items, int block) {
+  return block == 256 ? sweep_min_blocks(kw, d, items)
+                      : (block > 256 ? (sweep_min_blocks(kw, d, items) + 1) / 2 : 2 * sweep_min_blocks(kw, d, items));
+}
 
-template <int KW, int D, int ITEMS>
-__global__ void __launch_bounds__(kSortBlock, sweep_min_blocks(KW, D, ITEMS)) k_sort_onesweep(const __grid_constant__ SweepParams S) {
+// BLOCK threads, ITEMS keys per thread: a tile of BLOCK * ITEMS rows. Every
+// digit has its own thread in the per-digit steps (RADIX <= BLOCK).
+template <int KW, int D, int ITEMS, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, sweep_min_blocks(KW, D, ITEMS, BLOCK)) k_sort_onesweep(const __grid_constant__ SweepParams S) {
   constexpr int RADIX = 1 << D;
-  constexpr int NW = kSortBlock / 32;
-  constexpr uint32_t TILE = kSortBlock * ITEMS;
-  constexpr int DPT = (RADIX + kSortBlock - 1) / kSortBlock;  // digits per thread (1 here)
-  static_assert(RADIX <= kSortBlock, "one digit per thread");
-  (void)DPT;
+  constexpr int NW = BLOCK / 32;
+  constexpr uint32_t TILE = BLOCK * ITEMS;
+  static_assert(RADIX <= BLOCK, "one digit per thread");
 
   extern __shared__ uint32_t smem[];
   uint32_t* s_whist = smem;                       // [NW][RADIX]
@@ -176,7 +182,7 @@ __global__ void __launch_bounds__(kSortBlock, sweep_min_blocks(KW, D, ITEMS)) k_
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) s_misc[0] = atomicAdd(S.tile_counter, 1u);
-  for (int i = threadIdx.x; i < NW * RADIX; i += kSortBlock) s_whist[i] = 0u;
+  for (int i = threadIdx.x; i < NW * RADIX; i += BLOCK) s_whist[i] = 0u;
   __syncthreads();
   const uint32_t tile = s_misc[0];
   const int sg = find_segment(S.seg, tile);
@@ -265,8 +271,8 @@ __global__ void __launch_bounds__(kSortBlock, sweep_min_blocks(KW, D, ITEMS)) k_
     seg_count = __ldg(S.hist + ((size_t)sg * S.npass + S.pass) * RADIX + t);
   }
   uint32_t total;
-  const uint32_t tile_excl = block_exclusive_sum<kSortBlock>(t < RADIX ? tile_count : 0u, s_scan, total);
-  const uint32_t seg_excl = block_exclusive_sum<kSortBlock>(t < RADIX ? seg_count : 0u, s_scan, total);
+  const uint32_t tile_excl = block_exclusive_sum<BLOCK>(t < RADIX ? tile_count : 0u, s_scan, total);
+  const uint32_t seg_excl = block_exclusive_sum<BLOCK>(t < RADIX ? seg_count : 0u, s_scan, total);
 
   // 4. decoupled look-back per digit over the segment's earlier tiles
   if (t < RADIX) {
@@ -321,7 +327,7 @@ __global__ void __launch_bounds__(kSortBlock, sweep_min_blocks(KW, D, ITEMS)) k_
   __syncthreads();
 
   // 6. contiguous scatter per digit run
-  for (uint32_t i = threadIdx.x; i < tile_n; i += kSortBlock) {
+  for (uint32_t i = threadIdx.x; i < tile_n; i += BLOCK) {
     uint32_t kk[KW];
 #pragma unroll
     for (int j = 0; j < KW; ++j) kk[j] = s_keys[i * KW + j];
@@ -556,18 +562,18 @@ static bool valid_key_column(const yq_column& c) {
 
 static int round_kw(int w) { return w <= 1 ? 1 : (w <= 2 ? 2 : (w <= 4 ? 4 : (w <= 8 ? 8 : -1))); }
 
-template <int KW, int D, int ITEMS>
+template <int KW, int D, int ITEMS, int BLOCK>
 static size_t sweep_smem() {
   constexpr int RADIX = 1 << D;
-  constexpr int NW = kSortBlock / 32;
-  return sizeof(uint32_t) * ((size_t)NW * RADIX + 2 * RADIX + NW + 1 + 4 + (size_t)kSortBlock * ITEMS * (KW + 1));
+  constexpr int NW = BLOCK / 32;
+  return sizeof(uint32_t) * ((size_t)NW * RADIX + 2 * RADIX + NW + 1 + 4 + (size_t)BLOCK * ITEMS * (KW + 1));
 }
 
-template <int KW, int D, int ITEMS>
+template <int KW, int D, int ITEMS, int BLOCK>
 static int launch_sweep(const SweepParams& P, uint32_t ntiles, cudaStream_t s) {
-  const size_t smem = sweep_smem<KW, D, ITEMS>();
-  YQ_TRY(kernel_allow_smem((const void*)k_sort_onesweep<KW, D, ITEMS>, smem));
-  k_sort_onesweep<KW, D, ITEMS><<<ntiles, kSortBlock, smem, s>>>(P);
+  const size_t smem = sweep_smem<KW, D, ITEMS, BLOCK>();
+  YQ_TRY(kernel_allow_smem((const void*)k_sort_onesweep<KW, D, ITEMS, BLOCK>, smem));
+  k_sort_onesweep<KW, D, ITEMS, BLOCK><<<ntiles, BLOCK, smem, s>>>(P);
   YQ_CHECK_LAUNCH();
   return YQ_OK;
 }
@@ -586,25 +592,47 @@ static int launch_hist(const KeySrc& src, const SegInfo& seg, uint32_t tile_rows
   return YQ_OK;
 }
 
-// Dispatch table over (KW, D).
+// Dispatch table over (KW, D, ITEMS, BLOCK).
 struct SortKernels {
   int (*hist)(const KeySrc&, const SegInfo&, uint32_t, uint32_t, uint32_t*, cudaStream_t);
   int (*sweep)(const SweepParams&, uint32_t, cudaStream_t);
   int items;
+  int block;
+  uint32_t tile_rows() const { return (uint32_t)(items * block); }
 };
 
-template <int KW, int D, int ITEMS>
+template <int KW, int D, int ITEMS, int BLOCK = kSortBlock>
 static SortKernels make_kernels() {
   SortKernels k;
   k.hist = &launch_hist<KW, D>;
-  k.sweep = &launch_sweep<KW, D, ITEMS>;
+  k.sweep = &launch_sweep<KW, D, ITEMS, BLOCK>;
   k.items = ITEMS;
+  k.block = BLOCK;
   return k;
 }
 
-// Instantiated (key words, digit bits, items per thread) variants; items = 0
-// picks the default for (kw, d), the case that lists digit bits x 100 + 0.
-static bool pick_kernels(int kw, int d, int items, SortKernels& k) {
+// Instantiated (key words, digit bits, items per thread, block threads)
+// variants; items = 0 picks the default for (kw, d) and block = 0 the
+// 256-thread block. Every variant's tile (items x block) is at least
+// min_tile_rows(kw), which sizes the look-back status.
+static bool pick_kernels(int kw, int d, int items, int block, SortKernels& k) {
+  if (block == 512) {
+    switch (kw * 10000 + d * 100 + items) {
+      case 10808: case 10800: k = make_kernels<1, 8, 8, 512>(); return true;
+      case 10812: k = make_kernels<1, 8, 12, 512>(); return true;
+      case 20808: case 20800: k = make_kernels<2, 8, 8, 512>(); return true;
+      default: return false;
+    }
+  }
+  if (block == 128) {
+    switch (kw * 10000 + d * 100 + items) {
+      case 10616: case 10600: k = make_kernels<1, 6, 16, 128>(); return true;
+      case 10416: case 10400: k = make_kernels<1, 4, 16, 128>(); return true;
+      case 20616: case 20600: k = make_kernels<2, 6, 16, 128>(); return true;
+      default: return false;
+    }
+  }
+  if (block != 0 && block != kSortBlock) return false;
   switch (kw * 10000 + d * 100 + items) {
     case 10816: k = make_kernels<1, 8, 16>(); return true;
     case 10812: case 10800: k = make_kernels<1, 8, 12>(); return true;  // 12 items: four blocks per SM
@@ -620,14 +648,18 @@ static bool pick_kernels(int kw, int d, int items, SortKernels& k) {
     default: return false;
   }
 }
+static bool pick_kernels(int kw, int d, int items, SortKernels& k) { return pick_kernels(kw, d, items, 0, k); }
 
-// Fewest items per thread any variant of key width kw uses (sizes the
-// look-back status of the most tiles a tuned choice can make).
-static int min_items(int kw) { return kw == 1 ? 8 : (kw == 2 ? 8 : (kw == 4 ? 8 : 4)); }
+// Fewest rows per tile any variant of key width kw uses (sizes the look-back
+// status of the most tiles a tuned choice can make).
+static uint32_t min_tile_rows(int kw) { return (uint32_t)kSortBlock * (kw == 8 ? 4 : 8); }
 
-// Autotuned (digit bits, items) per (key words, log2 of rows per segment).
+// Autotuned variant per (key words, log2 of rows per segment).
+struct TunedSort {
+  int d = 8, items = 0, block = 0;
+};
 static std::mutex g_tune_mu;
-static std::map<std::pair<int, int>, std::pair<int, int>> g_tuned;
+static std::map<std::pair<int, int>, TunedSort> g_tuned;
 
 static int rows_bucket(uint32_t rows, int nseg) {
   uint32_t avg = nseg > 0 ? rows / (uint32_t)nseg : rows;
@@ -639,10 +671,10 @@ static int rows_bucket(uint32_t rows, int nseg) {
   return b;
 }
 
-static std::pair<int, int> tuned_choice(int kw, uint32_t rows, int nseg) {
+static TunedSort tuned_choice(int kw, uint32_t rows, int nseg) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   auto it = g_tuned.find({kw, rows_bucket(rows, nseg)});
-  if (it == g_tuned.end()) return {8, 0};
+  if (it == g_tuned.end()) return TunedSort{};
   return it->second;
 }
 
@@ -675,29 +707,32 @@ struct KeyPlan {
   uint32_t tile_rows, ntiles;
 };
 
-// want_d / want_items = 0: the autotuned choice for this key width and
-// segment size (yq_sort_autotune), else 8-bit digits with the default items.
-// `sizing`: tile count for the variant with the fewest items (workspace bound).
-static int plan_key(const yq_column& c, int vwords_override, int want_d, int want_items, const uint32_t* seg_offsets,
-                    int nseg, KeyPlan& kp, bool sizing = false, int null_word_override = -1) {
+// want_d / want_items / want_block = 0: the autotuned choice for this key
+// width and segment size (yq_sort_autotune), else 8-bit digits with the
+// default items and 256-thread blocks. `sizing`: tile count for the smallest
+// tile any variant uses (workspace bound).
+static int plan_key(const yq_column& c, int vwords_override, int want_d, int want_items, int want_block,
+                    const uint32_t* seg_offsets, int nseg, KeyPlan& kp, bool sizing = false,
+                    int null_word_override = -1) {
   kp.sh.vwords = vwords_override >= 0 ? vwords_override : key_value_words(c);
   kp.sh.null_word = null_word_override >= 0 ? null_word_override : c.nulls != nullptr;
   kp.sh.kw = round_kw(kp.sh.vwords + kp.sh.null_word);
   if (kp.sh.kw < 0) return YQ_ERR_UNSUPPORTED;
   kp.D = want_d;
-  int items = want_items;
+  int items = want_items, block = want_block;
   if (kp.D == 0) {
-    const std::pair<int, int> t = tuned_choice(kp.sh.kw, seg_offsets[nseg] - seg_offsets[0], nseg);
-    kp.D = t.first;
-    if (items == 0) items = t.second;
+    const TunedSort t = tuned_choice(kp.sh.kw, seg_offsets[nseg] - seg_offsets[0], nseg);
+    kp.D = t.d;
+    if (items == 0) items = t.items;
+    if (block == 0) block = t.block;
   }
-  if (!pick_kernels(kp.sh.kw, kp.D, items, kp.K)) {
+  if (!pick_kernels(kp.sh.kw, kp.D, items, block, kp.K)) {
     kp.D = 8;
     if (!pick_kernels(kp.sh.kw, 8, 0, kp.K)) return YQ_ERR_UNSUPPORTED;
   }
   kp.P = (kp.sh.kw * 32 + kp.D - 1) / kp.D;
   kp.R = 1 << kp.D;
-  kp.tile_rows = (uint32_t)kSortBlock * (sizing ? min_items(kp.sh.kw) : kp.K.items);
+  kp.tile_rows = sizing ? min_tile_rows(kp.sh.kw) : kp.K.tile_rows();
   kp.ntiles = 0;
   for (int i = 0; i < nseg; ++i) kp.ntiles += ceil_div<uint32_t>(seg_offsets[i + 1] - seg_offsets[i], kp.tile_rows);
   return YQ_OK;
@@ -751,8 +786,10 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
     if (seg_offsets_host[i + 1] < seg_offsets_host[i]) return YQ_ERR_INVALID_ARG;
   const int want_d = cfg ? cfg->digit_bits : 0;
   const int want_items = cfg ? cfg->items_per_thread : 0;
+  const int want_block = cfg ? cfg->block_threads : 0;
   if (want_d != 0 && want_d != 4 && want_d != 6 && want_d != 8) return YQ_ERR_INVALID_ARG;
   if (want_items < 0 || want_items > 16) return YQ_ERR_INVALID_ARG;
+  if (want_block != 0 && want_block != 128 && want_block != 256 && want_block != 512) return YQ_ERR_INVALID_ARG;
   const bool keep_trivial = cfg && cfg->keep_trivial;
 
   // Size buffers for the widest plan any key can take (text keys are sized
@@ -767,7 +804,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
     if (c.type == YQ_TEXT && vw > 8 - (c.nulls ? 1 : 0)) vw = 8 - (c.nulls ? 1 : 0);
     // Sized for 8-bit digits (the largest passes x bins) and the fewest items
     // per thread (the most tiles), which bound every variant's buffers.
-    int st = plan_key(c, vw, 8, 0, seg_offsets_host, nseg, kp, true);
+    int st = plan_key(c, vw, 8, 0, 0, seg_offsets_host, nseg, kp, true);
     if (st != YQ_OK) return st;
     // For a text key this is the plan at its full (clamped) width, which
     // bounds every narrower plan: fewer words mean fewer passes and larger tiles.
@@ -861,7 +898,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
       cnull = (ch == 0 && c.nulls) ? 1 : 0;
     }
     KeyPlan kp;
-    YQ_TRY(plan_key(cc, cvw, want_d, want_items, seg_offsets_host, nseg, kp, false, cnull));
+    YQ_TRY(plan_key(cc, cvw, want_d, want_items, want_block, seg_offsets_host, nseg, kp, false, cnull));
     SegPlan sp;
     plan_segments(seg_offsets_host, nseg, kp.tile_rows, sp);
     YQ_TRY(h2d_async(d_seg, sp.seg.data(), (nseg + 1) * sizeof(uint32_t), s));
@@ -932,7 +969,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
         if (kw_eff > 0 && kw_eff < kp.sh.kw && pick_kernels(kw_eff, kp.D, 0, kq.K)) {
           kq.sh.kw = kw_eff;
           kq.P = kw_eff * ppw;
-          kq.tile_rows = (uint32_t)kSortBlock * kq.K.items;
+          kq.tile_rows = kq.K.tile_rows();
           for (int w = kw_eff; w < kp.sh.kw; ++w)
             for (int q = 0; q < ppw; ++q) high[w - kw_eff] |= (uint32_t)common[w * ppw + q] << (q * kp.D);
           std::vector<int> kept;
@@ -1107,13 +1144,15 @@ int yq_sort_autotune(const yq_column* key, uint32_t rows, const uint32_t* seg_of
   if (!key || !seg_offsets || nseg <= 0 || !best || !valid_key_column(*key)) return YQ_ERR_INVALID_ARG;
   const int kw = round_kw(key_value_words(*key) + (key->nulls ? 1 : 0));
   if (kw < 0) return YQ_ERR_UNSUPPORTED;
-  // Every instantiated (digit bits, items per thread) variant of this key width.
-  std::vector<std::pair<int, int>> cand;
+  // Every instantiated (digit bits, items per thread, block threads) variant
+  // of this key width.
+  std::vector<TunedSort> cand;
   for (int d : {8, 6, 4})
-    for (int it : {16, 12, 8, 4}) {
-      SortKernels k;
-      if (pick_kernels(kw, d, it, k) && k.items == it) cand.push_back({d, it});
-    }
+    for (int it : {16, 12, 8, 4})
+      for (int b : {256, 512, 128}) {
+        SortKernels k;
+        if (pick_kernels(kw, d, it, b, k) && k.items == it && k.block == b) cand.push_back(TunedSort{d, it, b});
+      }
   if (cand.empty()) return YQ_ERR_UNSUPPORTED;
   cudaStream_t s = as_stream(stream);
   KeyJob j{*key, descending != 0, 0};
@@ -1127,10 +1166,10 @@ int yq_sort_autotune(const yq_column* key, uint32_t rows, const uint32_t* seg_of
   YQ_TRY_CUDA(cudaEventCreate(&e0));
   YQ_TRY_CUDA(cudaEventCreate(&e1));
   float best_ms = 1e30f;
-  std::pair<int, int> pick = cand[0];
+  TunedSort pick = cand[0];
   int status = YQ_OK;
   for (const auto& c : cand) {
-    yq_sort_config cfg{c.first, c.second, 0, 1};
+    yq_sort_config cfg{c.d, c.items, c.block, 1};
     status = sort_segments_impl(&j, 1, rows, seg_offsets, nseg, perm, &cfg, ws, wsb, s, nullptr);  // warm-up
     if (status != YQ_OK) break;
     cudaEventRecord(e0, s);
@@ -1154,9 +1193,9 @@ int yq_sort_autotune(const yq_column* key, uint32_t rows, const uint32_t* seg_of
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tuned[{kw, rows_bucket(rows, nseg)}] = pick;
   }
-  best->digit_bits = pick.first;
-  best->items_per_thread = pick.second;
-  best->block_threads = kSortBlock;
+  best->digit_bits = pick.d;
+  best->items_per_thread = pick.items;
+  best->block_threads = pick.block;
   best->keep_trivial = 0;
   return YQ_OK;
 }

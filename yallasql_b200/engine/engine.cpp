@@ -3,8 +3,11 @@
 #include "engine.hpp"
 
 #include <string.h>
+#include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
+#include <cstdio>
 #include <numeric>
 
 namespace yq::engine {
@@ -35,56 +38,168 @@ Batch::Batch(std::vector<ColumnPtr> cols, uint64_t n, cudaStream_t s, bool with_
 }
 
 Batch::~Batch() {
+  waitWrite();
   for (size_t c = 0; c < columns.size(); ++c) {
     if (location == Device::GPU) {
       if (data[c]) cudaFreeAsync(data[c], stream);
       if (nulls[c]) cudaFreeAsync(nulls[c], stream);
-    } else {
+    } else if (location == Device::CPU) {
       if (data[c]) cudaFreeHost(data[c]);
       if (nulls[c]) cudaFreeHost(nulls[c]);
     }
   }
+  if (location == Device::FS && !file_.empty()) std::remove(file_.c_str());
 }
 
 uint64_t Batch::bytes() const {
   uint64_t b = 0;
-  for (size_t c = 0; c < columns.size(); ++c) b += rows * columns[c]->width + (nulls[c] ? rows : 0);
+  for (size_t c = 0; c < columns.size(); ++c) b += rows * columns[c]->width + (nullable(c) ? rows : 0);
   return b;
 }
 
-// GPU <-> pinned host (Batch::moveGpuToCpu / moveCpuToGpu, src/batch.cu:28-73).
-void Batch::moveTo(Device target) {
+// GPU <-> pinned host (Batch::moveGpuToCpu / moveCpuToGpu, src/batch.cu:28-73),
+// pinned host <-> file (moveCpuToFs / moveFsToCpu, src/batch.cu:75-110).
+void Batch::moveTo(Device target, const std::string& path) {
   if (target == location) return;
+  if (location == Device::FS) fsToCpu();
+  if (location == Device::GPU && target != Device::GPU) gpuToCpu();
+  if (target == Device::GPU && location == Device::CPU) cpuToGpu();
+  if (target == Device::FS && location == Device::CPU) cpuToFs(path);
+}
+
+void Batch::gpuToCpu() {
   for (size_t c = 0; c < columns.size(); ++c) {
     const size_t b = std::max<uint64_t>(1, rows) * columns[c]->width;
     const size_t nb = std::max<uint64_t>(1, rows);
     void* p = nullptr;
     void* q = nullptr;
-    if (target == Device::CPU) {
-      check_cuda(cudaMallocHost(&p, b), "spill alloc");
-      check_cuda(cudaMemcpyAsync(p, data[c], b, cudaMemcpyDeviceToHost, stream), "spill copy");
-      if (nulls[c]) {
-        check_cuda(cudaMallocHost(&q, nb), "spill alloc");
-        check_cuda(cudaMemcpyAsync(q, nulls[c], nb, cudaMemcpyDeviceToHost, stream), "spill copy");
-      }
-      check_cuda(cudaStreamSynchronize(stream), "spill sync");
-      cudaFreeAsync(data[c], stream);
-      if (nulls[c]) cudaFreeAsync(nulls[c], stream);
-    } else {
-      check_cuda(cudaMallocAsync(&p, b, stream), "reload alloc");
-      check_cuda(cudaMemcpyAsync(p, data[c], b, cudaMemcpyHostToDevice, stream), "reload copy");
-      if (nulls[c]) {
-        check_cuda(cudaMallocAsync(&q, nb, stream), "reload alloc");
-        check_cuda(cudaMemcpyAsync(q, nulls[c], nb, cudaMemcpyHostToDevice, stream), "reload copy");
-      }
-      check_cuda(cudaStreamSynchronize(stream), "reload sync");
-      cudaFreeHost(data[c]);
-      if (nulls[c]) cudaFreeHost(nulls[c]);
+    check_cuda(cudaMallocHost(&p, b), "spill alloc");
+    check_cuda(cudaMemcpyAsync(p, data[c], b, cudaMemcpyDeviceToHost, stream), "spill copy");
+    if (nulls[c]) {
+      check_cuda(cudaMallocHost(&q, nb), "spill alloc");
+      check_cuda(cudaMemcpyAsync(q, nulls[c], nb, cudaMemcpyDeviceToHost, stream), "spill copy");
     }
+    check_cuda(cudaStreamSynchronize(stream), "spill sync");
+    cudaFreeAsync(data[c], stream);
+    if (nulls[c]) cudaFreeAsync(nulls[c], stream);
     data[c] = p;
     nulls[c] = static_cast<uint8_t*>(q);
   }
-  location = target;
+  location = Device::CPU;
+}
+
+void Batch::cpuToGpu() {
+  for (size_t c = 0; c < columns.size(); ++c) {
+    const size_t b = std::max<uint64_t>(1, rows) * columns[c]->width;
+    const size_t nb = std::max<uint64_t>(1, rows);
+    void* p = nullptr;
+    void* q = nullptr;
+    check_cuda(cudaMallocAsync(&p, b, stream), "reload alloc");
+    check_cuda(cudaMemcpyAsync(p, data[c], b, cudaMemcpyHostToDevice, stream), "reload copy");
+    if (nulls[c]) {
+      check_cuda(cudaMallocAsync(&q, nb, stream), "reload alloc");
+      check_cuda(cudaMemcpyAsync(q, nulls[c], nb, cudaMemcpyHostToDevice, stream), "reload copy");
+    }
+    check_cuda(cudaStreamSynchronize(stream), "reload sync");
+    cudaFreeHost(data[c]);
+    if (nulls[c]) cudaFreeHost(nulls[c]);
+    data[c] = p;
+    nulls[c] = static_cast<uint8_t*>(q);
+  }
+  location = Device::GPU;
+}
+
+// File layout: a header (magic, rows, column count, then per column type,
+// width and a null flag) followed, per column, by rows * width data bytes and,
+// for a nullable column, rows null bytes. The reference writes the data only
+// and so loses the null bytes on this tier.
+namespace {
+constexpr uint64_t kBatchFileMagic = 0x3148435441425159ull;  // "YQBATCH1"
+}
+
+void Batch::cpuToFs(const std::string& path) {
+  if (path.empty()) throw Error(YQ_ERR_INVALID_ARG, "spill to disk: no cache directory");
+  file_ = path;
+  std::vector<void*> d = data;
+  std::vector<uint8_t*> nl = nulls;
+  std::vector<std::pair<int32_t, int32_t>> meta;
+  for (auto& c : columns) meta.emplace_back(c->type, c->width);
+  const uint64_t n = rows;
+  null_flag_.assign(columns.size(), 0);
+  // The host buffers now belong to the write task: it frees them once the
+  // file is complete (or failed), and the batch forgets them.
+  for (size_t c = 0; c < columns.size(); ++c) {
+    data[c] = nullptr;
+    null_flag_[c] = nulls[c] != nullptr;
+    nulls[c] = nullptr;
+  }
+  location = Device::FS;
+  write_ = std::async(std::launch::async, [path, d, nl, meta, n]() -> bool {
+    bool ok = false;
+    if (FILE* f = std::fopen(path.c_str(), "wb")) {
+      const uint64_t head[3] = {kBatchFileMagic, n, (uint64_t)meta.size()};
+      ok = std::fwrite(head, sizeof(head), 1, f) == 1;
+      for (size_t c = 0; ok && c < meta.size(); ++c) {
+        const int32_t m[3] = {meta[c].first, meta[c].second, nl[c] != nullptr};
+        ok = std::fwrite(m, sizeof(m), 1, f) == 1;
+      }
+      for (size_t c = 0; ok && c < meta.size(); ++c) {
+        const size_t b = std::max<uint64_t>(1, n) * meta[c].second;
+        ok = std::fwrite(d[c], 1, b, f) == b;
+        if (ok && nl[c]) ok = std::fwrite(nl[c], 1, std::max<uint64_t>(1, n), f) == std::max<uint64_t>(1, n);
+      }
+      ok = (std::fclose(f) == 0) && ok;
+    }
+    for (size_t c = 0; c < d.size(); ++c) {
+      if (d[c]) cudaFreeHost(d[c]);
+      if (nl[c]) cudaFreeHost(nl[c]);
+    }
+    return ok;
+  });
+}
+
+void Batch::waitWrite() {
+  if (!write_.valid()) return;
+  const bool ok = write_.get();
+  if (!ok && location == Device::FS) write_failed_ = true;
+}
+
+void Batch::fsToCpu() {
+  waitWrite();
+  if (write_failed_) throw Error(YQ_ERR_CUDA, "spill to disk: writing " + file_ + " failed");
+  FILE* f = std::fopen(file_.c_str(), "rb");
+  if (!f) throw Error(YQ_ERR_INVALID_ARG, "reload from disk: cannot open " + file_);
+  bool ok = true;
+  uint64_t head[3] = {0, 0, 0};
+  ok = std::fread(head, sizeof(head), 1, f) == 1 && head[0] == kBatchFileMagic && head[1] == rows &&
+       head[2] == columns.size();
+  std::vector<int32_t> has(columns.size(), 0);
+  for (size_t c = 0; ok && c < columns.size(); ++c) {
+    int32_t m[3];
+    ok = std::fread(m, sizeof(m), 1, f) == 1 && m[0] == columns[c]->type && m[1] == columns[c]->width;
+    has[c] = m[2];
+  }
+  for (size_t c = 0; ok && c < columns.size(); ++c) {
+    const size_t b = std::max<uint64_t>(1, rows) * columns[c]->width;
+    const size_t nb = std::max<uint64_t>(1, rows);
+    void* p = nullptr;
+    check_cuda(cudaMallocHost(&p, b), "reload alloc");
+    data[c] = p;
+    ok = std::fread(p, 1, b, f) == b;
+    if (ok && has[c]) {
+      void* q = nullptr;
+      check_cuda(cudaMallocHost(&q, nb), "reload alloc");
+      nulls[c] = static_cast<uint8_t*>(q);
+      ok = std::fread(q, 1, nb, f) == nb;
+    }
+  }
+  std::fclose(f);
+  location = Device::CPU;  // buffers read so far are freed as host memory by the destructor
+  null_flag_.clear();
+  const std::string name = file_;
+  std::remove(file_.c_str());
+  file_.clear();
+  if (!ok) throw Error(YQ_ERR_INVALID_ARG, "reload from disk: " + name + " is truncated or not this batch");
 }
 
 yq_column Batch::column(size_t c) const {
@@ -101,6 +216,7 @@ yq_batch Batch::view(std::vector<yq_column>& storage) const {
 BatchID CacheManager::putBatch(std::unique_ptr<Batch> b) {
   const BatchID id = next_++;
   if (b->location == Device::GPU) gpu_bytes_ += b->bytes();
+  else if (b->location == Device::CPU) host_bytes_ += b->bytes();
   batches_[id] = std::move(b);
   handleOverflow();
   return id;
@@ -111,15 +227,23 @@ std::unique_ptr<Batch> CacheManager::getBatch(BatchID id) {
   if (it == batches_.end()) throw Error(YQ_ERR_INVALID_ARG, "getBatch: unknown batch");
   std::unique_ptr<Batch> b = std::move(it->second);
   batches_.erase(it);
-  if (b->location == Device::GPU) gpu_bytes_ -= std::min(gpu_bytes_, b->bytes());
-  else b->moveTo(Device::GPU);
+  const uint64_t bytes = b->bytes();
+  if (b->location == Device::GPU) gpu_bytes_ -= std::min(gpu_bytes_, bytes);
+  else if (b->location == Device::CPU) host_bytes_ -= std::min(host_bytes_, bytes);
+  b->moveTo(Device::GPU);
   return b;
 }
 
 Batch& CacheManager::refBatch(BatchID id) { return *batches_.at(id); }
 
+std::string CacheManager::filePath(BatchID id) const {
+  static std::atomic<uint64_t> seq{0};
+  return dir_ + "/yq_batch_" + std::to_string((unsigned long)getpid()) + "_" +
+         std::to_string((unsigned long long)seq.fetch_add(1)) + "_" + std::to_string((unsigned long long)id) + ".bin";
+}
+
 void CacheManager::handleOverflow() {
-  // Oldest device batches (lowest id) move to pinned host memory first.
+  // Oldest device batches (lowest id) move to pinned host memory first ...
   for (auto& kv : batches_) {
     if (gpu_bytes_ <= budget_) break;
     Batch& b = *kv.second;
@@ -127,7 +251,19 @@ void CacheManager::handleOverflow() {
     const uint64_t bytes = b.bytes();
     b.moveTo(Device::CPU);
     gpu_bytes_ -= std::min(gpu_bytes_, bytes);
+    host_bytes_ += bytes;
     ++spilled_;
+  }
+  // ... and the oldest host batches to files when host memory is over its budget.
+  if (host_budget_ == 0 || dir_.empty()) return;
+  for (auto& kv : batches_) {
+    if (host_bytes_ <= host_budget_) break;
+    Batch& b = *kv.second;
+    if (b.location != Device::CPU) continue;
+    const uint64_t bytes = b.bytes();
+    b.moveTo(Device::FS, filePath(kv.first));
+    host_bytes_ -= std::min(host_bytes_, bytes);
+    ++disk_;
   }
 }
 
@@ -748,8 +884,10 @@ class GroupByOperator final : public Operator {
 // yields one output batch with all left columns followed by all right columns.
 class JoinOperator final : public Operator {
  public:
-  JoinOperator(std::unique_ptr<Operator> l, std::unique_ptr<Operator> r, const yq_join_cond* conds, int ncond)
+  JoinOperator(std::unique_ptr<Operator> l, std::unique_ptr<Operator> r, const yq_join_cond* conds, int ncond,
+               const int32_t* disjunct = nullptr)
       : conds_(conds, conds + ncond) {
+    if (disjunct) disjunct_.assign(disjunct, disjunct + ncond);
     children_.push_back(std::move(l));
     children_.push_back(std::move(r));
   }
@@ -802,8 +940,12 @@ class JoinOperator final : public Operator {
       std::vector<yq_column> ov;
       out->view(ov);
       uint64_t count = 0;
-      const int st = yq_join_project(&L, &R, conds_.data(), (int32_t)conds_.size(), outs.data(), (int32_t)outs.size(),
-                                     ov.data(), cap, &count, nullptr, 0, ctx_->compute);
+      const int st =
+          disjunct_.empty()
+              ? yq_join_project(&L, &R, conds_.data(), (int32_t)conds_.size(), outs.data(), (int32_t)outs.size(),
+                                ov.data(), cap, &count, nullptr, 0, ctx_->compute)
+              : yq_join_project_or(&L, &R, conds_.data(), disjunct_.data(), (int32_t)conds_.size(), outs.data(),
+                                   (int32_t)outs.size(), ov.data(), cap, &count, nullptr, 0, ctx_->compute);
       if (st == YQ_ERR_CAPACITY) {
         cap = count;
         continue;
@@ -817,6 +959,7 @@ class JoinOperator final : public Operator {
   }
 
   std::vector<yq_join_cond> conds_;
+  std::vector<int32_t> disjunct_;  // empty: all conditions ANDed
   std::vector<BatchID> left_;
   bool cached_ = false;
   std::unique_ptr<Batch> right_;
@@ -833,6 +976,8 @@ struct yq_plan {
   std::vector<Operator*> nodes;
   ExecContext ctx;
   uint64_t budget;
+  uint64_t host_budget = 0;
+  std::string cache_dir;
 };
 
 struct yq_result {
@@ -887,6 +1032,13 @@ yq_plan* yq_plan_create(uint64_t gpu_budget_bytes) {
     return nullptr;
   }
   return p;
+}
+
+int yq_plan_set_spill(yq_plan* p, uint64_t host_budget_bytes, const char* cache_dir) {
+  if (!p || (host_budget_bytes && (!cache_dir || !*cache_dir))) return YQ_ERR_INVALID_ARG;
+  p->host_budget = host_budget_bytes;
+  p->cache_dir = host_budget_bytes ? std::string(cache_dir) : std::string();
+  return YQ_OK;
 }
 
 void yq_plan_destroy(yq_plan* p) {
@@ -967,6 +1119,16 @@ int yq_plan_join(yq_plan* p, int32_t left, int32_t right, const yq_join_cond* co
   });
 }
 
+int yq_plan_join_or(yq_plan* p, int32_t left, int32_t right, const yq_join_cond* conds, const int32_t* disjunct,
+                    int32_t ncond) {
+  if (!p || ncond <= 0 || !conds || !disjunct) return -YQ_ERR_INVALID_ARG;
+  return guarded([&] {
+    auto l = take(p, left);
+    auto r = take(p, right);
+    return add(p, std::make_unique<JoinOperator>(std::move(l), std::move(r), conds, ncond, disjunct));
+  });
+}
+
 int yq_plan_cross(yq_plan* p, int32_t left, int32_t right) {
   if (!p) return -YQ_ERR_INVALID_ARG;
   return guarded([&] {
@@ -982,7 +1144,7 @@ int yq_plan_execute(yq_plan* p, int32_t root, yq_result** out) {
     Operator* op = p->nodes[root];
     p->ctx.stats = yq_plan_stats{};
     op->setContext(&p->ctx);
-    CacheManager cache(p->budget);
+    CacheManager cache(p->budget, p->host_budget, p->cache_dir);
     cudaEvent_t e0, e1;
     check_cuda(cudaEventCreate(&e0), "event");
     check_cuda(cudaEventCreate(&e1), "event");
@@ -1031,6 +1193,7 @@ int yq_plan_execute(yq_plan* p, int32_t root, yq_result** out) {
     cudaEventElapsedTime(&ms, e0, e1);
     p->ctx.stats.compute_ms = ms;
     p->ctx.stats.spilled_batches = cache.spilled();
+    p->ctx.stats.disk_batches = cache.spilledToDisk();
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     batches.clear();

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <future>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -34,7 +35,10 @@ namespace yq::engine {
 
 using BatchID = uint64_t;
 
-enum class Device : uint8_t { CPU, GPU };
+// Where a batch's columns live: the device, pinned host memory, or a file in
+// the plan's cache directory (the reference's Device::GPU / CPU / FS,
+// include/enums/device.hpp).
+enum class Device : uint8_t { CPU, GPU, FS };
 
 struct Column {
   int32_t type;
@@ -57,8 +61,9 @@ inline void check_cuda(cudaError_t e, const char* where) {
 }
 
 // Columnar batch: per column a buffer of rows * width bytes and an optional
-// null-byte array; on the device (stream-ordered allocations on `stream`) or
-// in pinned host memory after a spill.
+// null-byte array; on the device (stream-ordered allocations on `stream`), in
+// pinned host memory after a spill, or in a file after a second spill (the
+// null bytes travel with the data on every tier).
 class Batch {
  public:
   std::vector<ColumnPtr> columns;
@@ -74,29 +79,56 @@ class Batch {
   Batch& operator=(const Batch&) = delete;
 
   uint64_t bytes() const;
-  void moveTo(Device target);
+  bool nullable(size_t c) const { return nulls[c] != nullptr || (c < null_flag_.size() && null_flag_[c]); }
+  // Move between tiers. To FS: the file `path` is written by a background
+  // task that then frees the host buffers (Batch::moveCpuToFs with
+  // serializeBatchAsync, src/batch.cu:75-95); any later move or the
+  // destructor waits for that task first. From FS: the file is read back
+  // into pinned memory and removed.
+  void moveTo(Device target, const std::string& path = std::string());
   yq_batch view(std::vector<yq_column>& storage) const;
   yq_column column(size_t c) const;
+
+ private:
+  void gpuToCpu();
+  void cpuToGpu();
+  void cpuToFs(const std::string& path);
+  void fsToCpu();
+  void waitWrite();
+  std::string file_;
+  std::future<bool> write_;
+  std::vector<uint8_t> null_flag_;  // per column: nullable, while the null bytes are in the file
+  bool write_failed_ = false;
 };
 
-// BatchID -> Batch with a device budget; the oldest device batches move to
-// pinned host memory when the budget is exceeded (CacheManager::handleOverflow,
-// include/engine/cache_manager.hpp:67-88; accounting here is 64-bit).
+// BatchID -> Batch with a device budget and a host budget; when the device
+// budget is exceeded the oldest device batches move to pinned host memory, and
+// when the host budget is exceeded the oldest host batches move to files in
+// `cache_dir` (CacheManager::handleOverflow,
+// include/engine/cache_manager.hpp:67-88; accounting here is 64-bit). A host
+// budget of 0, or no cache directory, keeps every spilled batch in host memory.
 class CacheManager {
  public:
-  explicit CacheManager(uint64_t gpu_budget) : budget_(gpu_budget) {}
+  explicit CacheManager(uint64_t gpu_budget, uint64_t host_budget = 0, std::string cache_dir = std::string())
+      : budget_(gpu_budget), host_budget_(host_budget), dir_(std::move(cache_dir)) {}
   BatchID putBatch(std::unique_ptr<Batch> b);
   std::unique_ptr<Batch> getBatch(BatchID id);  // ownership back to the caller, on the device
   Batch& refBatch(BatchID id);
   uint64_t spilled() const { return spilled_; }
+  uint64_t spilledToDisk() const { return disk_; }
 
  private:
   void handleOverflow();
+  std::string filePath(BatchID id) const;
   std::map<BatchID, std::unique_ptr<Batch>> batches_;
   BatchID next_ = 1;
   uint64_t budget_;
+  uint64_t host_budget_;
+  std::string dir_;
   uint64_t gpu_bytes_ = 0;
+  uint64_t host_bytes_ = 0;
   uint64_t spilled_ = 0;
+  uint64_t disk_ = 0;
 };
 
 struct ExecContext {

@@ -276,9 +276,11 @@ def filter_project(batch: DeviceBatch, predicate: Expr | None, select: list, str
 
 
 # ----------------------------------------------------------------- sort
-def sort_config(digit_bits=0, keep_trivial=False):
+def sort_config(digit_bits=0, keep_trivial=False, items_per_thread=0, block_threads=0):
     c = A.SortConfig()
     c.digit_bits = digit_bits
+    c.items_per_thread = items_per_thread
+    c.block_threads = block_threads
     c.keep_trivial = 1 if keep_trivial else 0
     return c
 
@@ -393,18 +395,31 @@ def _conds(conds):
     return arr
 
 
-def join_pairs(left: DeviceBatch, right: DeviceBatch, conds: list, capacity: int | None = None, stream=None):
+def _disjunct(disjunct, conds):
+    if len(disjunct) != len(conds):
+        raise ValueError("one disjunct group per condition")
+    return (C.c_int32 * len(conds))(*disjunct)
+
+
+def join_pairs(left: DeviceBatch, right: DeviceBatch, conds: list, capacity: int | None = None, stream=None,
+               disjunct: list | None = None):
     """Inner join pairs (left row, right row) in (left, right) order; conds =
-    [(left_col, right_col, yq_cmp)], all ANDed (JoinOperator + ComparisonJoinExpression)."""
+    [(left_col, right_col, yq_cmp)], all ANDed (JoinOperator + ComparisonJoinExpression);
+    with `disjunct` (a group per condition) an OR of the groups' ANDs."""
     lb, lk = left.c()
     rb, rk = right.c()
     cap = capacity if capacity is not None else max(1, left.rows * right.rows if len(conds) == 0 else left.rows * 4)
+    dj = None if disjunct is None else _disjunct(disjunct, conds)
     while True:
         ol = torch.empty(max(1, cap), dtype=torch.int32, device="cuda")
         orr = torch.empty(max(1, cap), dtype=torch.int32, device="cuda")
         cnt = C.c_uint64(0)
-        st = lib().yq_join_pairs(C.byref(lb), C.byref(rb), _conds(conds), len(conds), ol.data_ptr(), orr.data_ptr(),
-                                 cap, C.byref(cnt), None, 0, _stream(stream))
+        if dj is None:
+            st = lib().yq_join_pairs(C.byref(lb), C.byref(rb), _conds(conds), len(conds), ol.data_ptr(),
+                                     orr.data_ptr(), cap, C.byref(cnt), None, 0, _stream(stream))
+        else:
+            st = lib().yq_join_pairs_or(C.byref(lb), C.byref(rb), _conds(conds), C.cast(dj, C.c_void_p), len(conds),
+                                        ol.data_ptr(), orr.data_ptr(), cap, C.byref(cnt), None, 0, _stream(stream))
         if st == A.ERR_CAPACITY and capacity is None:
             cap = int(cnt.value)  # count-then-retry with the exact size
             continue
@@ -414,20 +429,27 @@ def join_pairs(left: DeviceBatch, right: DeviceBatch, conds: list, capacity: int
 
 
 def join_project(left: DeviceBatch, right: DeviceBatch, conds: list, outputs: list, capacity: int | None = None,
-                 stream=None) -> DeviceBatch:
-    """Join and write the chosen columns [(side, column)] of every matching pair."""
+                 stream=None, disjunct: list | None = None) -> DeviceBatch:
+    """Join and write the chosen columns [(side, column)] of every matching
+    pair; `disjunct` as in join_pairs."""
     lb, lk = left.c()
     rb, rk = right.c()
     srcs = [(right if s else left).columns[c] for s, c in outputs]
     cap = capacity if capacity is not None else (left.rows * right.rows if not conds else max(1, left.rows * 4))
     outs_c = (A.JoinOutput * len(outputs))(*[A.JoinOutput(s, c) for s, c in outputs])
+    dj = None if disjunct is None else _disjunct(disjunct, conds)
     while True:
         outs = [DeviceColumn.empty(c.type, max(1, cap), c.width if c.type == A.TEXT else None,
                                    nulls=c.nulls is not None) for c in srcs]
         oc = (A.Column * len(outs))(*[o.c() for o in outs])
         cnt = C.c_uint64(0)
-        st = lib().yq_join_project(C.byref(lb), C.byref(rb), _conds(conds), len(conds), outs_c, len(outputs), oc,
-                                   cap, C.byref(cnt), None, 0, _stream(stream))
+        if dj is None:
+            st = lib().yq_join_project(C.byref(lb), C.byref(rb), _conds(conds), len(conds), outs_c, len(outputs),
+                                       oc, cap, C.byref(cnt), None, 0, _stream(stream))
+        else:
+            st = lib().yq_join_project_or(C.byref(lb), C.byref(rb), _conds(conds), C.cast(dj, C.c_void_p),
+                                          len(conds), outs_c, len(outputs), oc, cap, C.byref(cnt), None, 0,
+                                          _stream(stream))
         if st == A.ERR_CAPACITY and capacity is None:
             cap = int(cnt.value)
             continue
@@ -541,15 +563,20 @@ class OrderByRuns:
 
 
 def order_by(batch: DeviceBatch, key: int, descending: bool, offsets: list[int], nulls_first=False,
-             stream=None) -> DeviceBatch:
-    """One-shot yq_order_by into a new batch (workspace from the library)."""
+             stream=None, merge_items: int | None = None) -> DeviceBatch:
+    """One-shot yq_order_by into a new batch (workspace from the library);
+    `merge_items` picks the merge tile (yq_order_by_tiled)."""
     out = DeviceBatch([DeviceColumn.empty(c.type, c.rows, c.width if c.type == A.TEXT else None,
                                           nulls=c.nulls is not None) for c in batch.columns])
     offs = (C.c_uint32 * len(offsets))(*offsets)
     ib, _ia = batch.c()
     ob, _oa = out.c()
-    _check(lib().yq_order_by(C.byref(ib), key, int(descending), int(nulls_first), offs, len(offsets) - 1,
-                             C.byref(ob), None, 0, _stream(stream)), "yq_order_by")
+    if merge_items is None:
+        _check(lib().yq_order_by(C.byref(ib), key, int(descending), int(nulls_first), offs, len(offsets) - 1,
+                                 C.byref(ob), None, 0, _stream(stream)), "yq_order_by")
+    else:
+        _check(lib().yq_order_by_tiled(C.byref(ib), key, int(descending), int(nulls_first), offs, len(offsets) - 1,
+                                       C.byref(ob), merge_items, None, 0, _stream(stream)), "yq_order_by_tiled")
     return out
 
 
@@ -589,6 +616,20 @@ def sort_autotune(col: DeviceColumn, offsets, descending=False, stream=None) -> 
     _check(lib().yq_sort_autotune(C.byref(cc), col.rows, offs, len(offsets) - 1, int(descending), C.byref(best),
                                   _stream(stream)), "yq_sort_autotune")
     return best
+
+
+def order_by_autotune(batch: DeviceBatch, key: int, descending: bool, offsets, nulls_first=False,
+                      stream=None) -> tuple["A.SortConfig", int]:
+    """Tune yq_order_by for this input (yq_order_by_autotune): the run sort's
+    (digit bits, items per thread, block threads) and the merge tile's outputs
+    per thread, remembered for later calls on inputs of this shape."""
+    offs = offsets if isinstance(offsets, C.Array) else (C.c_uint32 * len(offsets))(*offsets)
+    ib, _ia = batch.c()
+    best = A.SortConfig()
+    items = C.c_int32(0)
+    _check(lib().yq_order_by_autotune(C.byref(ib), key, int(descending), int(nulls_first), offs, len(offs) - 1,
+                                      C.byref(best), C.byref(items), _stream(stream)), "yq_order_by_autotune")
+    return best, int(items.value)
 
 
 # ------------------------------------------------------------------ CSV scan

@@ -26,7 +26,8 @@ class HostColumn(C.Structure):
 
 class PlanStats(C.Structure):
     _fields_ = [("batches", C.c_uint64), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
-                ("compute_ms", C.c_double), ("spilled_batches", C.c_uint64)]
+                ("compute_ms", C.c_double), ("spilled_batches", C.c_uint64),
+                ("disk_batches", C.c_uint64)]
 
 
 _lib = None
@@ -34,6 +35,7 @@ _lib = None
 PROTOTYPES = {
     "yq_plan_create": (C.c_void_p, [C.c_uint64]),
     "yq_plan_destroy": (None, [C.c_void_p]),
+    "yq_plan_set_spill": (C.c_int, [C.c_void_p, C.c_uint64, C.c_char_p]),
     "yq_plan_scan": (C.c_int, [C.c_void_p, C.POINTER(HostColumn), C.c_int32, C.c_uint64, C.c_uint32]),
     "yq_plan_scan_csv": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_int32), C.c_int32,
                                    C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.c_uint32]),
@@ -47,6 +49,8 @@ PROTOTYPES = {
                                       C.POINTER(C.c_int32), C.c_int32]),
     "yq_plan_group_by": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(A.GroupAgg), C.c_int32]),
     "yq_plan_join": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(A.JoinCond), C.c_int32]),
+    "yq_plan_join_or": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(A.JoinCond), C.POINTER(C.c_int32),
+                                  C.c_int32]),
     "yq_plan_cross": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "yq_plan_execute": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
     "yq_result_rows": (C.c_uint64, [C.c_void_p]),
@@ -87,10 +91,17 @@ def _node(st: int, what: str) -> int:
 class Plan:
     """One query: build nodes, then execute once."""
 
-    def __init__(self, gpu_budget: int = 0):
+    def __init__(self, gpu_budget: int = 0, host_budget: int = 0, cache_dir: str | None = None):
+        """gpu_budget: device bytes before batches spill to pinned host memory
+        (0 = 1 GiB); host_budget with cache_dir: host bytes before spilled
+        batches move on to files in cache_dir (0 = no file tier)."""
         self.h = lib().yq_plan_create(gpu_budget)
         if not self.h:
             raise A.YQError(A.ERR_CUDA, "yq_plan_create")
+        if host_budget:
+            st = lib().yq_plan_set_spill(self.h, host_budget, (cache_dir or "").encode())
+            if st:
+                raise A.YQError(st, "yq_plan_set_spill")
         self._keep = []
         self.types: dict[int, list[int]] = {}
 
@@ -222,10 +233,17 @@ class Plan:
         self.types[n] = [ct[key]] + [group_by_out_type(k, A.INT64 if k == A.AGG_COUNT_STAR else ct[c]) for k, c in aggs]
         return n
 
-    def join(self, left: int, right: int, conds: list):
+    def join(self, left: int, right: int, conds: list, disjunct: list | None = None):
+        """Inner join on conds [(left_col, right_col, cmp)], ANDed; with
+        `disjunct` (a group per condition) an OR of the groups' ANDs."""
         arr = (A.JoinCond * len(conds))(*[A.JoinCond(l, r, c) for l, r, c in conds])
         self._keep.append(arr)
-        n = _node(lib().yq_plan_join(self.h, left, right, arr, len(conds)), "yq_plan_join")
+        if disjunct is None:
+            n = _node(lib().yq_plan_join(self.h, left, right, arr, len(conds)), "yq_plan_join")
+        else:
+            dj = (C.c_int32 * len(conds))(*disjunct)
+            self._keep.append(dj)
+            n = _node(lib().yq_plan_join_or(self.h, left, right, arr, dj, len(conds)), "yq_plan_join_or")
         self.types[n] = self.types[left] + self.types[right]
         return n
 
