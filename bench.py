@@ -491,11 +491,19 @@ def serving_form(args) -> dict:
     serving.serve_plain(copy.deepcopy(warm), cat, plans)
     serving.serve_continuous(copy.deepcopy(warm), cat, plans)
     burst = serving.make_trace(n, 0.0, cat, seed=4)
-    plain_sat = serving.serve_plain(copy.deepcopy(burst), cat, plans)
-    cont_sat = serving.serve_continuous(copy.deepcopy(burst), cat, plans, slots=8, budget=40e9)
+
+    def median_of(fn, trace, k=3):
+        """The run with the median throughput of k runs of the same trace (a
+        single run can lose hundreds of ms to a host stall)."""
+        outs = sorted((fn(copy.deepcopy(trace)) for _ in range(k)), key=lambda d: d["queries_per_s"])
+        return outs[k // 2]
+
+    plain_sat = median_of(lambda tr: serving.serve_plain(tr, cat, plans), burst)
+    cont_sat = median_of(lambda tr: serving.serve_continuous(tr, cat, plans, slots=8, budget=40e9), burst)
     # the same loop without sharing work between requests (no coalescing of
     # identical requests, one scan per filter request, no resident permutations)
-    cont_sat_noshare = serving.serve_continuous(copy.deepcopy(burst), cat, plans, slots=8, budget=40e9, share=False)
+    cont_sat_noshare = median_of(
+        lambda tr: serving.serve_continuous(tr, cat, plans, slots=8, budget=40e9, share=False), burst)
     rate = 0.7 * plain_sat["queries_per_s"]
     trace = serving.make_trace(n, rate, cat, seed=4)
     plain_open = serving.serve_plain(copy.deepcopy(trace), cat, plans)
@@ -503,14 +511,16 @@ def serving_form(args) -> dict:
     # Poisson-rate sweep: a form "sustains" a rate when it completes the trace
     # at >= 95% of the offered rate; at a p99 budget, each form's best rate is
     # the highest sustained rate whose p99 stays within the budget
+    # (rates from a quarter of the plain form's saturation throughput up to
+    # 90% of the continuous form's; each point the median of three runs)
     grid = sorted({round(f * plain_sat["queries_per_s"]) for f in (0.25, 0.5, 0.75, 1.0)} |
-                  {round(f * cont_sat["queries_per_s"]) for f in (0.5, 0.75, 0.9)})
+                  {round(f * cont_sat["queries_per_s"]) for f in (0.4, 0.55, 0.7, 0.8, 0.9)})
     sweep = []
     for rr in grid:
         tr = serving.make_trace(n, float(rr), cat, seed=6)
-        pl = serving.serve_plain(copy.deepcopy(tr), cat, plans)
-        co = serving.serve_continuous(copy.deepcopy(tr), cat, plans, slots=8, budget=40e9)
-        cn = serving.serve_continuous(copy.deepcopy(tr), cat, plans, slots=8, budget=40e9, share=False)
+        pl = median_of(lambda x: serving.serve_plain(x, cat, plans), tr)
+        co = median_of(lambda x: serving.serve_continuous(x, cat, plans, slots=8, budget=40e9), tr)
+        cn = median_of(lambda x: serving.serve_continuous(x, cat, plans, slots=8, budget=40e9, share=False), tr)
         pick = lambda d: {k: round(d[k], 3) for k in ("queries_per_s", "p50_ms", "p99_ms")}
         sweep.append({"offered_per_s": rr, "plain": pick(pl), "continuous": pick(co),
                       "continuous_without_sharing": pick(cn)})
