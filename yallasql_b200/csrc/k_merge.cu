@@ -334,7 +334,9 @@ static int launch_merge(const MergeParams& M, cudaStream_t s, double bytes) {
 // gives every output tile its A and B windows (merge-path co-ranks at both
 // ends of the tile); the tile kernel is persistent, and thread 0 of a block
 // starts the bulk copies of the key and id windows of the tiles kRawStages - 1
-// ahead of the one the block merges, so the copies overlap the merging.
+// ahead of the one the block merges, so the copies overlap the merging. A
+// level whose ids are the row positions (right after the first gather level)
+// copies no ids.
 // Windows are copied from their 16-byte aligned hull (buffers are padded).
 constexpr int kRawStages = 3;
 
@@ -401,6 +403,10 @@ __device__ __forceinline__ uint32_t raw_corank(const uint32_t* keys, const RawPa
   return lo;
 }
 
+// Tile t's A and B windows: merge-path co-ranks at both ends of the tile,
+// one thread per tile. (Finding them in the tile kernel's blocks instead, all
+// of a block's tiles before its first merge, measured 70 us per level slower
+// than this launch.)
 template <int KW, int ITEMS>
 __global__ void k_merge_raw_partition(const __grid_constant__ RawLevel L) {
   constexpr uint32_t TILE = kMergeBlock * ITEMS;
@@ -432,6 +438,7 @@ __global__ void k_merge_raw_partition(const __grid_constant__ RawLevel L) {
 struct RawSlot {
   uint32_t na, nb, cnt, out0;
   uint32_t ka, kb, ia, ib;  // byte offsets of the first A / B key and id in the slot
+  uint32_t a_row, b_row;    // first A / B row (the ids themselves when the level has no id input)
 };
 
 // ITEMS outputs per thread: a tile of kMergeBlock * ITEMS outputs. Variants
@@ -477,19 +484,27 @@ __device__ __forceinline__ void raw_issue(const RawLevel& L, const RawTile& d, i
   r.nb = d.nb;
   r.cnt = d.cnt;
   r.out0 = d.out0;
+  r.a_row = d.a_row;
+  r.b_row = d.b_row;
   {
     uint32_t k2 = 0, i2 = 0, b2 = 0;
     r.ka = raw_window(kreg, k2, L.keys_in, d.a_row, d.na, G::W, bar, b2, false);
     r.kb = raw_window(kreg, k2, L.keys_in, d.b_row, d.nb, G::W, bar, b2, false);
-    r.ia = raw_window(ireg, i2, L.ids_in, d.a_row, d.na, 4u, bar, b2, false);
-    r.ib = raw_window(ireg, i2, L.ids_in, d.b_row, d.nb, 4u, bar, b2, false);
+    if (L.ids_in) {  // no id input: every row's id is its row number
+      r.ia = raw_window(ireg, i2, L.ids_in, d.a_row, d.na, 4u, bar, b2, false);
+      r.ib = raw_window(ireg, i2, L.ids_in, d.b_row, d.nb, 4u, bar, b2, false);
+    } else {
+      r.ia = r.ib = 0u;
+    }
     mbar_arrive_expect_tx(bar, b2);
   }
   s_slot[slot] = r;
   raw_window(kreg, ko, L.keys_in, d.a_row, d.na, G::W, bar, bytes, true);
   raw_window(kreg, ko, L.keys_in, d.b_row, d.nb, G::W, bar, bytes, true);
-  raw_window(ireg, io, L.ids_in, d.a_row, d.na, 4u, bar, bytes, true);
-  raw_window(ireg, io, L.ids_in, d.b_row, d.nb, 4u, bar, bytes, true);
+  if (L.ids_in) {
+    raw_window(ireg, io, L.ids_in, d.a_row, d.na, 4u, bar, bytes, true);
+    raw_window(ireg, io, L.ids_in, d.b_row, d.nb, 4u, bar, bytes, true);
+  }
 }
 
 template <int KW>
@@ -526,7 +541,7 @@ __device__ __forceinline__ void raw_key_store(uint32_t* out, size_t row, const u
 }
 
 // Inverse of make_key_ptr for a key without nulls (exact when the column holds
-// no -0.0, non-canonical NaN or bool byte other than 0/1: see k_key_lossy).
+// no -0.0, non-canonical NaN or bool byte other than 0/1: see key_value_lossy).
 template <int KW>
 __device__ __forceinline__ void decode_store(const KeyDecode& d, size_t row, const uint32_t (&k0)[KW]) {
   // the whole key: the merged words, then the words every row shares
@@ -631,12 +646,14 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
         if (takeA) {
 #pragma unroll
           for (int j = 0; j < KW; ++j) okey[x][j] = ka[j];
-          oid[x] = idA[ia++];
+          oid[x] = L.ids_in ? idA[ia] : r.a_row + ia;
+          ++ia;
           if (ia < r.na) raw_key_s<KW>(kA + (size_t)ia * G::W, ka);
         } else {
 #pragma unroll
           for (int j = 0; j < KW; ++j) okey[x][j] = kb[j];
-          oid[x] = idB[jb++];
+          oid[x] = L.ids_in ? idB[jb] : r.b_row + jb;
+          ++jb;
           if (jb < r.nb) raw_key_s<KW>(kB + (size_t)jb * G::W, kb);
         }
       }
@@ -730,25 +747,6 @@ static int merge_items_for(int kw, uint32_t rows) {
   std::lock_guard<std::mutex> lk(g_merge_tune_mu);
   auto it = g_merge_tuned.find({kw, log2_rows(rows)});
   return it == g_merge_tuned.end() ? kMergeItems : it->second;
-}
-
-// *flag |= 1 when a key value would not survive the key-word round trip
-// (-0.0, a NaN other than the canonical one, a bool byte other than 0/1).
-__global__ void k_key_lossy(const char* __restrict__ data, int type, uint32_t rows, uint32_t* flag) {
-  bool lossy = false;
-  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
-    if (type == YQ_FLOAT32) {
-      const uint32_t b = __ldg(reinterpret_cast<const uint32_t*>(data) + r);
-      lossy |= b == 0x80000000u || (((b & 0x7f800000u) == 0x7f800000u) && (b & 0x007fffffu) && b != 0x7fc00000u);
-    } else if (type == YQ_FLOAT64) {
-      const unsigned long long b = __ldg(reinterpret_cast<const unsigned long long*>(data) + r);
-      lossy |= b == 0x8000000000000000ull || (((b & 0x7ff0000000000000ull) == 0x7ff0000000000000ull) &&
-                                              (b & 0x000fffffffffffffull) && b != 0x7ff8000000000000ull);
-    } else if (type == YQ_BOOL) {
-      lossy |= (uint8_t)data[r] > 1u;
-    }
-  }
-  if (__any_sync(0xffffffffu, lossy) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
 }
 
 // Merge levels of one ORDER BY: host plan of every level's pairs.
@@ -989,8 +987,12 @@ static int order_by_run(const yq_batch* in, int32_t key_col, int32_t descending,
     }
   YQ_TRY_CUDA(cudaMemsetAsync(d_err, 0, 4 * sizeof(uint32_t), s));
 
-  // 1. every run sorted; the sort hands over its key words and row ids
+  // 1. every run sorted; the sort hands over its key words and row ids, and
+  // its histogram pass flags key values the key words cannot restore
+  const bool may_decode = nruns > 1 && !key.nulls && key.type != YQ_TEXT;
+  uint32_t* d_lossy = d_err + 1;
   KeyJob job{key, descending != 0, nulls_first != 0};
+  if (may_decode && (key.type == YQ_FLOAT32 || key.type == YQ_FLOAT64 || key.type == YQ_BOOL)) job.lossy = d_lossy;
   int kw = 0;
   uint32_t* sort_err = nullptr;
   uint32_t high[8];
@@ -999,22 +1001,18 @@ static int order_by_run(const yq_batch* in, int32_t key_col, int32_t descending,
   // The last merge level writes the key column itself when the key has no
   // nulls; the gather then moves the key column only if some value would not
   // round-trip through its key words (flag set on the device).
-  const bool decode = kw > 0 && nruns > 1 && !key.nulls && key.type != YQ_TEXT;
-  uint32_t* d_lossy = d_err + 1;
-  if (decode && (key.type == YQ_FLOAT32 || key.type == YQ_FLOAT64 || key.type == YQ_BOOL)) {
-    k_key_lossy<<<sm_count() * 4, 256, 0, s>>>(static_cast<const char*>(key.data), key.type, rows, d_lossy);
-    YQ_CHECK_LAUNCH();
-  }
+  const bool decode = kw > 0 && may_decode;
   const uint32_t* only_if[YQ_MAX_BATCH_COLUMNS] = {nullptr};
   if (decode) only_if[key_col] = d_lossy;  // zero unless a value would not round-trip
   // 1b. two-level gather, first level: every column into sorted-run order;
-  // the row ids become positions in that copy
+  // the row ids become positions in that copy, so the first merge level
+  // reads no ids (a row's id is its position)
   const bool merged = kw > 0 && nruns > 1;
   staged = staged && merged;
+  bool ids_are_positions = false;
   if (staged) {
     YQ_TRY(gather_impl(in->columns, in->ncols, ids[0], rows, stage, only_if, s));
-    k_iota<<<sm_count() * 4, 256, 0, s>>>(ids[0], rows);
-    YQ_CHECK_LAUNCH();
+    ids_are_positions = true;
   }
   // 2. merge levels over (key words, row id)
   int cur = 0;
@@ -1031,7 +1029,7 @@ static int order_by_run(const yq_batch* in, int32_t key_col, int32_t descending,
       const bool last = l + 1 == levels;
       RawLevel L;
       L.keys_in = keys[cur];
-      L.ids_in = ids[cur];
+      L.ids_in = ids_are_positions ? nullptr : ids[cur];
       L.keys_out = last ? nullptr : keys[cur ^ 1];
       memset(&L.dec, 0, sizeof(L.dec));
       if (last && decode) {
@@ -1050,11 +1048,18 @@ static int order_by_run(const yq_batch* in, int32_t key_col, int32_t descending,
       L.err = d_err;
       if (L.ntiles > o.max_tiles) return YQ_ERR_UNSUPPORTED;
       if (L.ntiles == 0) continue;
-      // algorithmic bytes: key words + id in and out (ids only out on the last level)
-      const double bytes = (double)rows * (4.0 * kw + 4.0 + (last ? 4.0 : 4.0 * kw + 4.0));
+      // algorithmic bytes: key words + id in and out (ids only out on the
+      // last level; no ids in when they are the row positions)
+      const double bytes =
+          (double)rows * (4.0 * kw + (L.ids_in ? 4.0 : 0.0) + (last ? 4.0 : 4.0 * kw + 4.0));
       YQ_TRY(launch_raw_level_items(kw, mi, L, s, bytes));
+      ids_are_positions = false;
       cur ^= 1;
     }
+  }
+  if (ids_are_positions) {  // no level ran: the final gather still needs the positions written out
+    k_iota<<<sm_count() * 4, 256, 0, s>>>(ids[cur], rows);
+    YQ_CHECK_LAUNCH();
   }
   // 3. every column (the key included) gathered once by the final row ids
   YQ_TRY(gather_impl(staged ? stage : in->columns, in->ncols, ids[cur], rows, out->columns, only_if, s));

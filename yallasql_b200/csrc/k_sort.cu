@@ -100,10 +100,16 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_histogram(const KeySrc src,
       const uint32_t e = base + threadIdx.x;
       const bool valid = e < r1;
       uint32_t k[KW];
-      if (valid) make_key<KW>(src, src.in_perm ? __ldg(src.in_perm + e) : e, k);
+      const uint32_t row = valid ? (src.in_perm ? __ldg(src.in_perm + e) : e) : 0u;
+      if (valid) make_key<KW>(src, row, k);
       else {
 #pragma unroll
         for (int j = 0; j < KW; ++j) k[j] = 0u;
+      }
+      if (src.lossy) {  // the key column is read here anyway: flag values the key words cannot restore
+        const bool l = valid && !(src.nulls && src.nulls[row]) &&
+                       key_value_lossy(src.type, src.data + (size_t)row * src.width);
+        if (__any_sync(0xffffffffu, l) && lane == 0) atomicOr(src.lossy, 1u);
       }
       const uint32_t vb = __ballot_sync(0xffffffffu, valid);
       const int first = __ffs(vb) - 1;
@@ -917,6 +923,7 @@ int sort_segments_impl(const KeyJob* jobs, int njobs, uint32_t rows, const uint3
     src.desc = job.desc;
     src.nulls_first = job.nulls_first;
     src.null_word = kp.sh.null_word;
+    src.lossy = nchunks == 1 ? job.lossy : nullptr;
     SegInfo seg;
     seg.seg_start = d_seg;
     seg.tile_start = d_tiles;

@@ -19,7 +19,25 @@ struct KeySrc {
   int32_t desc;
   int32_t nulls_first;
   int32_t null_word;    // 1: word `vwords` is the null flag
+  uint32_t* lossy;      // optional: the histogram sets it when a value would not survive the key words
 };
+
+// A value whose key words decode to a different bit pattern: -0.0, a NaN
+// other than the canonical one, a bool byte other than 0/1.
+__device__ __forceinline__ bool key_value_lossy(int type, const char* p) {
+  if (type == YQ_FLOAT32) {
+    const uint32_t b = *reinterpret_cast<const uint32_t*>(p);
+    return b == 0x80000000u || (((b & 0x7f800000u) == 0x7f800000u) && (b & 0x007fffffu) && b != 0x7fc00000u);
+  }
+  if (type == YQ_FLOAT64) {
+    const unsigned long long b = *reinterpret_cast<const unsigned long long*>(p);
+    return b == 0x8000000000000000ull ||
+           (((b & 0x7ff0000000000000ull) == 0x7ff0000000000000ull) && (b & 0x000fffffffffffffull) &&
+            b != 0x7ff8000000000000ull);
+  }
+  if (type == YQ_BOOL) return (uint8_t)*p > 1u;
+  return false;
+}
 
 __device__ __forceinline__ uint32_t bswap(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
 

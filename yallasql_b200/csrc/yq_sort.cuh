@@ -10,6 +10,7 @@ namespace yq {
 struct KeyJob {
   yq_column key;
   int desc, nulls_first;
+  uint32_t* lossy = nullptr;  // set to non-zero when a key value would not round-trip its key words
 };
 
 // Words of the order-preserving key the sort builds for column `c` at most
