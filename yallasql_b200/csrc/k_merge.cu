@@ -331,8 +331,8 @@ static int launch_merge(const MergeParams& M, cudaStream_t s, double bytes) {
 // ORDER BY over sorted runs as the radix sort leaves them: each row is its
 // order-preserving key words (yq_keys.cuh) plus its row id, so the merge
 // compares unsigned words only. A level is two launches: the partition kernel
-// gives every output tile its A and B windows (merge-path co-ranks at both
-// ends of the tile); the tile kernel is persistent, and thread 0 of a block
+// gives every output tile its A and B windows (the merge-path co-rank at its
+// first output; the next tile's gives its end); the tile kernel is persistent, and thread 0 of a block
 // starts the bulk copies of the key and id windows of the tiles kRawStages - 1
 // ahead of the one the block merges, so the copies overlap the merging. A
 // level whose ids are the row positions (right after the first gather level)
@@ -344,9 +344,21 @@ struct RawPair {
   uint32_t a0, m, b0, n, tile0;
 };
 
+// A tile's windows. The partition kernel searches one co-rank per tile (at
+// the tile's first output): `i0` is it, and `done` says whether na / nb are
+// final (the pair's last tile, whose end co-rank is the pair's A length);
+// otherwise the tile kernel completes them from the next tile's i0.
 struct RawTile {
-  uint32_t a_row, na, b_row, nb, out0, cnt, pad0, pad1;
+  uint32_t a_row, na, b_row, nb, out0, cnt, i0, done;
 };
+
+__device__ __forceinline__ RawTile raw_tile_fix(RawTile d, uint32_t next_i0) {
+  if (!d.done) {
+    d.na = next_i0 - d.i0;
+    d.nb = d.cnt - d.na;
+  }
+  return d;
+}
 
 // Decoding of key words back into the key column's values (the last level
 // writes the sorted key column itself instead of its words).
@@ -403,10 +415,10 @@ __device__ __forceinline__ uint32_t raw_corank(const uint32_t* keys, const RawPa
   return lo;
 }
 
-// Tile t's A and B windows: merge-path co-ranks at both ends of the tile,
-// one thread per tile. (Finding them in the tile kernel's blocks instead, all
-// of a block's tiles before its first merge, measured 70 us per level slower
-// than this launch.)
+// Tile t's merge-path co-rank at its first output, one thread per tile (the
+// tile's end co-rank is the next tile's start). Finding the co-ranks in the
+// tile kernel's blocks instead, all of a block's tiles before its first merge,
+// measured 70 us per level slower than this launch.
 template <int KW, int ITEMS>
 __global__ void k_merge_raw_partition(const __grid_constant__ RawLevel L) {
   constexpr uint32_t TILE = kMergeBlock * ITEMS;
@@ -417,20 +429,20 @@ __global__ void k_merge_raw_partition(const __grid_constant__ RawLevel L) {
   const uint32_t k0 = (t - p.tile0) * TILE;
   const uint32_t k1 = min(k0 + TILE, total);
   if (k0 >= total) {  // a descriptor with no work (never produced by the host plan)
-    L.tiles[t] = RawTile{0, 0, 0, 0, 0, 0, 0, 0};
+    L.tiles[t] = RawTile{0, 0, 0, 0, 0, 0, 0, 1};
     atomicOr(L.err, kErrBounds);
     return;
   }
   const uint32_t i0 = raw_corank<KW>(L.keys_in, p, k0);
-  const uint32_t i1 = (k1 == total) ? p.m : raw_corank<KW>(L.keys_in, p, k1);
   RawTile d;
   d.a_row = p.a0 + i0;
-  d.na = i1 - i0;
   d.b_row = p.b0 + (k0 - i0);
-  d.nb = (k1 - i1) - (k0 - i0);
   d.out0 = p.a0 + k0;
   d.cnt = k1 - k0;
-  d.pad0 = d.pad1 = 0;
+  d.i0 = i0;
+  d.done = k1 == total;  // the end co-rank of a pair's last tile is p.m; others take the next tile's i0
+  d.na = d.done ? p.m - i0 : 0u;
+  d.nb = d.done ? d.cnt - d.na : 0u;
   L.tiles[t] = d;
 }
 
@@ -587,13 +599,18 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
     for (int s = 0; s < kRawStages; ++s) mbar_init(bars + s, 1);
   __syncthreads();
   RawTile next{};
+  uint32_t next_i1 = 0u;  // the following tile's first co-rank (ends `next` unless it is done)
   if (threadIdx.x == 0) {
     for (int j = 0; j < kRawStages - 1; ++j) {
       const uint32_t t = blockIdx.x + (uint32_t)j * GR;
-      if (t < NT) raw_issue<KW, ITEMS>(L, L.tiles[t], j, raw_smem, s_slot);
+      if (t < NT)
+        raw_issue<KW, ITEMS>(L, raw_tile_fix(L.tiles[t], t + 1 < NT ? L.tiles[t + 1].i0 : 0u), j, raw_smem, s_slot);
     }
     const uint32_t t = blockIdx.x + (uint32_t)(kRawStages - 1) * GR;
-    if (t < NT) next = L.tiles[t];
+    if (t < NT) {
+      next = L.tiles[t];
+      next_i1 = t + 1 < NT ? L.tiles[t + 1].i0 : 0u;
+    }
   }
   int slot = 0;
   uint32_t parity = 0;
@@ -603,9 +620,12 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_raw_tiles(const __grid_co
       const uint32_t tn = t + (uint32_t)(kRawStages - 1) * GR;
       const int ns = slot == 0 ? kRawStages - 1 : slot - 1;
       if (tn < NT) {
-        raw_issue<KW, ITEMS>(L, next, ns, raw_smem, s_slot);
+        raw_issue<KW, ITEMS>(L, raw_tile_fix(next, next_i1), ns, raw_smem, s_slot);
         const uint32_t tf = tn + GR;  // descriptor for the next issue, loaded a tile ahead
-        if (tf < NT) next = L.tiles[tf];
+        if (tf < NT) {
+          next = L.tiles[tf];
+          next_i1 = tf + 1 < NT ? L.tiles[tf + 1].i0 : 0u;
+        }
       }
     }
     mbar_wait_bounded(bars + slot, parity, L.err);
