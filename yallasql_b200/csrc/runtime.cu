@@ -94,11 +94,13 @@ int h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s) {
 // A small device -> host read that the host needs now: a kernel copies the
 // words into mapped pinned host memory (stores over the link, not a copy
 // engine), the stream is synchronised, the bytes are copied out. Larger reads
-// take cudaMemcpyAsync. One mapped buffer per device, under a lock.
+// take cudaMemcpyAsync. Each call takes a mapped buffer from its device's free
+// list (allocated on first need, never freed) and gives it back after the
+// copy, so calls from several host threads wait on their own streams only.
 namespace {
 constexpr size_t kMappedBytes = 64 * 1024;
 std::mutex g_mapped_mu;
-uint32_t* g_mapped[64] = {nullptr};
+std::vector<uint32_t*> g_mapped_free[64];
 }  // namespace
 
 __global__ void k_to_host(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, uint32_t nwords) {
@@ -117,18 +119,35 @@ int d2h_sync(void* host_dst, const void* dev_src, size_t bytes, cudaStream_t s) 
     YQ_TRY_CUDA(cudaStreamSynchronize(s));
     return YQ_OK;
   }
-  std::lock_guard<std::mutex> lk(g_mapped_mu);
-  if (!g_mapped[dev]) {
+  uint32_t* buf = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mapped_mu);
+    if (!g_mapped_free[dev].empty()) {
+      buf = g_mapped_free[dev].back();
+      g_mapped_free[dev].pop_back();
+    }
+  }
+  if (!buf) {
     void* h = nullptr;
     YQ_TRY_CUDA(cudaHostAlloc(&h, kMappedBytes, cudaHostAllocMapped | cudaHostAllocPortable));
-    g_mapped[dev] = static_cast<uint32_t*>(h);
+    buf = static_cast<uint32_t*>(h);
   }
   uint32_t* dptr = nullptr;
-  YQ_TRY_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&dptr), g_mapped[dev], 0));
-  k_to_host<<<1, 256, 0, s>>>(dptr, static_cast<const uint32_t*>(dev_src), (uint32_t)(bytes / 4));
-  YQ_CHECK_LAUNCH();
-  YQ_TRY_CUDA(cudaStreamSynchronize(s));
-  memcpy(host_dst, g_mapped[dev], bytes);
+  cudaError_t e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&dptr), buf, 0);
+  if (e == cudaSuccess) {
+    k_to_host<<<1, 256, 0, s>>>(dptr, static_cast<const uint32_t*>(dev_src), (uint32_t)(bytes / 4));
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) memcpy(host_dst, buf, bytes);
+  {
+    std::lock_guard<std::mutex> lk(g_mapped_mu);
+    g_mapped_free[dev].push_back(buf);
+  }
+  if (e != cudaSuccess) {
+    set_cuda_error(e);
+    return YQ_ERR_CUDA;
+  }
   return YQ_OK;
 }
 
