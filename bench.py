@@ -470,7 +470,10 @@ def batched_form(args) -> dict:
             "plain_tasks_per_s": ntasks / (plain_ms / 1e3), "batched_tasks_per_s": ntasks / (batched_ms / 1e3),
             "speedup": round(plain_ms / batched_ms, 3),
             "batched_algorithmic_gbs": round(ts.algorithmic_bytes / (batched_ms / 1e3) / 1e9, 1),
-            "sort_autotuned": {"digit_bits": pipe.tuned[0], "items_per_thread": pipe.tuned[1]},
+            "sort_autotuned": {"digit_bits": pipe.tuned[0], "items_per_thread": pipe.tuned[1],
+                               "block_threads": pipe.tuned[2],
+                               "swept": "digit bits {4,6,8} x items {4,8,12,16} x block {128,256,512}, "
+                                        "instantiated variants"},
             "graph": True, "setup_s": round(setup_s, 2), "results_equal_plain": bool(same_sorted and same_aggs),
             "error_word": pipe.error_word()}
 

@@ -150,7 +150,7 @@ class BatchedPipeline:
         self.sws = torch.empty(max(256, ops.order_by_segments_workspace_bytes(ts.sarena.columns[1], ts.soffs)),
                                dtype=torch.uint8, device="cuda")
         tuned = ops.sort_autotune(ts.sarena.columns[1], ts.soffs, descending=True)
-        self.tuned = (tuned.digit_bits, tuned.items_per_thread)
+        self.tuned = (tuned.digit_bits, tuned.items_per_thread, tuned.block_threads)
         # digit width / items from the autotuner's cache, no host read-back: capturable
         self.cfg = ops.sort_config(digit_bits=0, keep_trivial=True)
         self.graph = None
