@@ -140,6 +140,41 @@ def test_single_inequality_nested_loop_types(cuda, kind, cmp):
     np.testing.assert_array_equal(gr, wr.astype(np.uint32))
 
 
+@pytest.mark.parametrize("kind", ["i32", "f32", "i64", "f64"])
+@pytest.mark.parametrize("cmp", [A.LT, A.GE, A.EQ, A.NE])
+def test_typed_nested_loop_projection_counted(cuda, kind, cmp):
+    """Right side long enough that each left row's matches are counted up
+    front (the right key sorted once, two binary searches per left row), then
+    written in left-major, right-ascending order; outputs are the condition's
+    right column (written from the staged value) or another right column."""
+    rng = np.random.default_rng(len(kind) * 11 + cmp)
+    L, R = 257, 12_345
+    if kind in ("i32", "i64"):
+        dt = np.int32 if kind == "i32" else np.int64
+        x, y = rng.integers(-40, 40, L).astype(dt), rng.integers(-40, 40, R).astype(dt)
+    else:
+        dt = np.float32 if kind == "f32" else np.float64
+        pool = np.array([0.0, -0.0, 1.5, -2.5, np.nan, 3.0, -7.25], dt)
+        x, y = rng.choice(pool, L), rng.choice(pool, R)
+    z = rng.integers(0, 1 << 30, R).astype(np.int32)
+    lb = ops.DeviceBatch([dev_col(x)])
+    rb = ops.DeviceBatch([dev_col(y), dev_col(z)])
+    with np.errstate(invalid="ignore"):
+        m = _NP_CMP[cmp](x[:, None], y[None, :])
+    wl, wr = np.nonzero(m)
+    out = ops.join_project(lb, rb, [(0, 0, cmp)], [(0, 0), (1, 0)])
+    np.testing.assert_array_equal(out.columns[0].data.cpu().numpy().view(x.dtype).view(np.uint8),
+                                  x[wl].view(np.uint8))
+    np.testing.assert_array_equal(out.columns[1].data.cpu().numpy().view(y.dtype).view(np.uint8),
+                                  y[wr].view(np.uint8))
+    out2 = ops.join_project(lb, rb, [(0, 0, cmp)], [(1, 1), (0, 0)])
+    np.testing.assert_array_equal(out2.columns[0].data.cpu().numpy(), z[wr])
+    if len(wl) > 1:
+        with pytest.raises(A.YQError) as e:
+            ops.join_project(lb, rb, [(0, 0, cmp)], [(0, 0), (1, 0)], capacity=len(wl) // 2)
+        assert e.value.status == A.ERR_CAPACITY
+
+
 def test_join_project_writes_pair_columns(cuda):
     rng = np.random.default_rng(5)
     lc, _ = random_side(rng, 4000)

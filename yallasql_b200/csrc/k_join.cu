@@ -24,6 +24,7 @@
 #include "vm_host.cuh"
 #include "row_kernels.cuh"
 #include "yq_jit.cuh"
+#include "yq_sort.cuh"
 
 namespace yq {
 
@@ -71,6 +72,8 @@ struct JoinParams {
   uint32_t* tile_counter;
   unsigned long long* total;
   uint32_t* err;
+  const uint32_t* counts;  // typed nested loop: matches per left row, counted up front (null: count in the kernel)
+  char* vdst[2];           // typed nested loop writing the condition's own values: left / right output (or null)
 };
 
 
@@ -426,6 +429,59 @@ __device__ __forceinline__ bool nl_cmp(T a, T b) {
   else return a != b;
 }
 
+// Matches per left row of one typed comparison, from the right column sorted
+// ascending with its NaNs (float columns) at the end, `nvalid` values before
+// them: two binary searches per left row instead of a pass over the right
+// side. A NaN compares false except under <>, as in nl_cmp.
+template <typename T>
+__device__ __forceinline__ bool nan_of(T v) {
+  return v != v;
+}
+
+template <typename T>
+__global__ void k_join_count_valid(const T* __restrict__ sorted, uint32_t R, uint32_t* nvalid) {
+  uint32_t nan = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x)
+    nan += nan_of(__ldg(sorted + i)) ? 1u : 0u;
+  for (int d = 16; d > 0; d >>= 1) nan += __shfl_xor_sync(0xffffffffu, nan, d);
+  if ((threadIdx.x & 31) == 0 && nan) atomicSub(nvalid, nan);
+}
+
+template <typename T, int OP>
+__global__ void k_join_count_sorted(const T* __restrict__ lcol, uint32_t L, const T* __restrict__ sorted,
+                                    const uint32_t* __restrict__ nvalid_p, uint32_t R, uint32_t* __restrict__ counts) {
+  const uint32_t nvalid = *nvalid_p;
+  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < L; l += gridDim.x * blockDim.x) {
+    const T v = __ldg(lcol + l);
+    uint32_t c;
+    if (nan_of(v)) {
+      c = OP == YQ_NE ? R : 0u;
+    } else {
+      uint32_t lo = 0, hi = nvalid;  // first position holding a value >= v
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(sorted + mid) < v) lo = mid + 1;
+        else hi = mid;
+      }
+      const uint32_t lb = lo;
+      hi = nvalid;  // first position holding a value > v
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (!(v < __ldg(sorted + mid))) lo = mid + 1;
+        else hi = mid;
+      }
+      const uint32_t ub = lo;
+      if constexpr (OP == YQ_LT) c = nvalid - ub;
+      else if constexpr (OP == YQ_LE) c = nvalid - lb;
+      else if constexpr (OP == YQ_GT) c = lb;
+      else if constexpr (OP == YQ_GE) c = ub;
+      else if constexpr (OP == YQ_EQ) c = ub - lb;
+      else c = R - (ub - lb);
+    }
+    counts[l] = c;
+  }
+}
+
 // Outputs of a join that are all 4- or 8-byte cells without null bytes (at
 // most kSimpleOut of them, e.g. one column of each side): the typed kernel
 // writes them directly, reading each left row's cells once.
@@ -435,8 +491,12 @@ __device__ __forceinline__ unsigned long long cell_bits(const char* p, int w) {
   return w == 8 ? __ldg(reinterpret_cast<const unsigned long long*>(p)) : (unsigned long long)__ldg(reinterpret_cast<const uint32_t*>(p));
 }
 
-template <typename T, int OP, bool SIMPLE>
+// MODE 0: writes (left row, right row) pairs; 1: writes up to kSimpleOut
+// 4- or 8-byte cells of either side; 2: the outputs are the condition's own
+// two columns (SELECT a.x, b.y ... WHERE a.x < b.y), written from registers.
+template <typename T, int OP, int MODE>
 __global__ void __launch_bounds__(kJoinBlock) k_join_nested_typed(const __grid_constant__ JoinParams J) {
+  constexpr bool SIMPLE = MODE == 1;
   __shared__ T s_r[kNlChunk];
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_cnt[kNlTile];
@@ -458,29 +518,37 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_nested_typed(const __grid_c
     lok[i] = l < J.L;
     lv[i] = lok[i] ? __ldg(lcol + l) : T(0);
   }
-  // pass 1: matches per left row
-  uint32_t cnt[kNlRowsPerWarp];
+  // pass 1: matches per left row (counted up front from the sorted right
+  // side when J.counts is given, else here over the whole right side)
+  if (J.counts) {
+    if (lane == 0)
 #pragma unroll
-  for (int i = 0; i < kNlRowsPerWarp; ++i) cnt[i] = 0;
-  for (uint32_t r0 = 0; r0 < J.R; r0 += kNlChunk) {
-    const uint32_t n = min(kNlChunk, J.R - r0);
-    __syncthreads();
-    for (uint32_t x = threadIdx.x; x < n; x += kJoinBlock) s_r[x] = __ldg(rcol + r0 + x);
-    __syncthreads();
-    // per-lane counts (one predicated add a comparison), summed over the warp below
-    for (uint32_t x = lane; x < n; x += 32) {
-      const T rv = s_r[x];
+      for (int i = 0; i < kNlRowsPerWarp; ++i)
+        s_cnt[warp * kNlRowsPerWarp + i] = lok[i] ? __ldg(J.counts + tile * kNlTile + warp * kNlRowsPerWarp + i) : 0u;
+  } else {
+    uint32_t cnt[kNlRowsPerWarp];
 #pragma unroll
-      for (int i = 0; i < kNlRowsPerWarp; ++i) cnt[i] += (lok[i] && nl_cmp<T, OP>(lv[i], rv)) ? 1u : 0u;
+    for (int i = 0; i < kNlRowsPerWarp; ++i) cnt[i] = 0;
+    for (uint32_t r0 = 0; r0 < J.R; r0 += kNlChunk) {
+      const uint32_t n = min(kNlChunk, J.R - r0);
+      __syncthreads();
+      for (uint32_t x = threadIdx.x; x < n; x += kJoinBlock) s_r[x] = __ldg(rcol + r0 + x);
+      __syncthreads();
+      // per-lane counts (one predicated add a comparison), summed over the warp below
+      for (uint32_t x = lane; x < n; x += 32) {
+        const T rv = s_r[x];
+#pragma unroll
+        for (int i = 0; i < kNlRowsPerWarp; ++i) cnt[i] += (lok[i] && nl_cmp<T, OP>(lv[i], rv)) ? 1u : 0u;
+      }
     }
+#pragma unroll
+    for (int i = 0; i < kNlRowsPerWarp; ++i)
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) cnt[i] += __shfl_xor_sync(0xffffffffu, cnt[i], d);
+    if (lane == 0)
+#pragma unroll
+      for (int i = 0; i < kNlRowsPerWarp; ++i) s_cnt[warp * kNlRowsPerWarp + i] = cnt[i];
   }
-#pragma unroll
-  for (int i = 0; i < kNlRowsPerWarp; ++i)
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) cnt[i] += __shfl_xor_sync(0xffffffffu, cnt[i], d);
-  if (lane == 0)
-#pragma unroll
-    for (int i = 0; i < kNlRowsPerWarp; ++i) s_cnt[warp * kNlRowsPerWarp + i] = cnt[i];
   __syncthreads();
   const uint32_t mine = threadIdx.x < kNlTile ? s_cnt[threadIdx.x] : 0u;
   uint32_t total;
@@ -496,7 +564,16 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_nested_typed(const __grid_c
 #pragma unroll
   for (int i = 0; i < kNlRowsPerWarp; ++i) pos[i] = s_prefix + s_cnt[warp * kNlRowsPerWarp + i];
   unsigned long long lcell[kNlRowsPerWarp][SIMPLE ? kSimpleOut : 1];  // left-side output cells of each row
+  const bool room = s_prefix + total <= J.capacity;  // every pair of this tile fits: no per-pair check
+  T* const vl = reinterpret_cast<T*>(J.vdst[0]);
+  T* const vr = reinterpret_cast<T*>(J.vdst[1]);
+  uint32_t from_rv = 0u;  // outputs that are the condition's right column: written from the staged value
   if constexpr (SIMPLE) {
+#pragma unroll
+    for (int o = 0; o < kSimpleOut; ++o)
+      if (o < J.nout && J.out[o].side == 1 && J.out[o].src == static_cast<const char*>(c.r.data) &&
+          J.out[o].width == (int)sizeof(T))
+        from_rv |= 1u << o;
 #pragma unroll
     for (int i = 0; i < kNlRowsPerWarp; ++i)
 #pragma unroll
@@ -521,16 +598,26 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_nested_typed(const __grid_c
         if (m) {
           const unsigned long long at = pos[i] + __popc(bal & lt);
           if constexpr (SIMPLE) {
-            if (at < J.capacity) {
+            if (room || at < J.capacity) {
 #pragma unroll
               for (int o = 0; o < kSimpleOut; ++o) {
                 if (o >= J.nout) break;
                 const JOut& w = J.out[o];
+                unsigned long long rb = 0ull;
+                if (from_rv >> o & 1u) {
+                  if constexpr (sizeof(T) == 8) rb = *reinterpret_cast<const unsigned long long*>(&rv);
+                  else rb = (unsigned long long)*reinterpret_cast<const uint32_t*>(&rv);
+                }
                 const unsigned long long v =
-                    w.side ? cell_bits(w.src + (size_t)(r0 + x) * w.width, w.width) : lcell[i][o];
+                    !w.side ? lcell[i][o] : ((from_rv >> o & 1u) ? rb : cell_bits(w.src + (size_t)(r0 + x) * w.width, w.width));
                 if (w.width == 8) reinterpret_cast<unsigned long long*>(w.dst)[at] = v;
                 else reinterpret_cast<uint32_t*>(w.dst)[at] = (uint32_t)v;
               }
+            }
+          } else if constexpr (MODE == 2) {
+            if (room || at < J.capacity) {
+              if (vl) vl[at] = lv[i];
+              if (vr) vr[at] = rv;
             }
           } else {
             emit_pair(J, at, tile * kNlTile + warp * kNlRowsPerWarp + i, r0 + x);
@@ -543,24 +630,34 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_nested_typed(const __grid_c
   if (tile == gridDim.x - 1 && threadIdx.x == 0) *J.total = s_prefix + total;
 }
 
-template <typename T, bool SIMPLE>
+template <typename T, int MODE>
 static void launch_nested_typed_op(int op, unsigned grid, const JoinParams& J, cudaStream_t s) {
   switch (op) {
-    case YQ_LT: k_join_nested_typed<T, YQ_LT, SIMPLE><<<grid, kJoinBlock, 0, s>>>(J); break;
-    case YQ_LE: k_join_nested_typed<T, YQ_LE, SIMPLE><<<grid, kJoinBlock, 0, s>>>(J); break;
-    case YQ_GT: k_join_nested_typed<T, YQ_GT, SIMPLE><<<grid, kJoinBlock, 0, s>>>(J); break;
-    case YQ_GE: k_join_nested_typed<T, YQ_GE, SIMPLE><<<grid, kJoinBlock, 0, s>>>(J); break;
-    case YQ_EQ: k_join_nested_typed<T, YQ_EQ, SIMPLE><<<grid, kJoinBlock, 0, s>>>(J); break;
-    default: k_join_nested_typed<T, YQ_NE, SIMPLE><<<grid, kJoinBlock, 0, s>>>(J); break;
+    case YQ_LT: k_join_nested_typed<T, YQ_LT, MODE><<<grid, kJoinBlock, 0, s>>>(J); break;
+    case YQ_LE: k_join_nested_typed<T, YQ_LE, MODE><<<grid, kJoinBlock, 0, s>>>(J); break;
+    case YQ_GT: k_join_nested_typed<T, YQ_GT, MODE><<<grid, kJoinBlock, 0, s>>>(J); break;
+    case YQ_GE: k_join_nested_typed<T, YQ_GE, MODE><<<grid, kJoinBlock, 0, s>>>(J); break;
+    case YQ_EQ: k_join_nested_typed<T, YQ_EQ, MODE><<<grid, kJoinBlock, 0, s>>>(J); break;
+    default: k_join_nested_typed<T, YQ_NE, MODE><<<grid, kJoinBlock, 0, s>>>(J); break;
   }
 }
 
 template <typename T>
-static void launch_nested_typed(int op, unsigned grid, const JoinParams& J, cudaStream_t s) {
+static void launch_nested_typed(int op, unsigned grid, JoinParams J, cudaStream_t s) {
   bool simple = J.nout >= 1 && J.nout <= kSimpleOut;
   for (int o = 0; o < J.nout && simple; ++o) simple = (J.out[o].width == 4 || J.out[o].width == 8) && !J.out[o].dst_nulls;
-  if (simple) launch_nested_typed_op<T, true>(op, grid, J, s);
-  else launch_nested_typed_op<T, false>(op, grid, J, s);
+  // the outputs are the condition's own left and right columns, each at most once
+  bool values = simple;
+  J.vdst[0] = J.vdst[1] = nullptr;
+  for (int o = 0; o < J.nout && values; ++o) {
+    const JOut& w = J.out[o];
+    const JCol& cc = w.side ? J.cond[0].r : J.cond[0].l;
+    values = w.src == cc.data && w.width == (int)sizeof(T) && !J.vdst[w.side];
+    if (values) J.vdst[w.side] = w.dst;
+  }
+  if (values) launch_nested_typed_op<T, 2>(op, grid, J, s);
+  else if (simple) launch_nested_typed_op<T, 1>(op, grid, J, s);
+  else launch_nested_typed_op<T, 0>(op, grid, J, s);
 }
 
 // ------------------------------------------------------- cross product
@@ -639,6 +736,67 @@ static int build_table(const yq_batch* right, const yq_program* pred, const yq_c
   YQ_TRY(kernel_allow_smem((const void*)k_hash_build, smem));
   ProfScope ps("join_hash_build", s, (double)right->rows * right->columns[key_col].width);
   k_hash_build<<<1, kBuildBlock, smem, s>>>(B);
+  YQ_CHECK_LAUNCH();
+  return YQ_OK;
+}
+
+// The typed nested loop counts each left row's matches up front when the
+// right side is at least this long: one sort of the right key and two
+// binary searches per left row, instead of a comparison pass over L x R.
+constexpr uint32_t kCountFirstRows = 4096;
+
+// Sort workspace for a right side of R rows (an 8-byte key bounds the typed
+// path's 4- and 8-byte keys).
+static size_t count_sort_bytes(uint32_t R) {
+  yq_column dummy{reinterpret_cast<void*>(static_cast<uintptr_t>(256)), nullptr, YQ_INT64, 8};
+  KeyJob j{dummy, 0, 0};
+  uint32_t offs[2] = {0, R};
+  size_t sb = 0;
+  if (sort_segments_impl(&j, 1, R, offs, 1, nullptr, nullptr, nullptr, 0, nullptr, &sb) != YQ_OK) return 0;
+  return sb;
+}
+
+struct CountWs {
+  char* sort_ws;
+  size_t sort_bytes;
+  uint32_t* perm;     // [R]
+  char* sorted;       // [R] values of the right key, ascending
+  uint32_t* nvalid;   // [1] values before the NaNs
+  uint32_t* counts;   // [L]
+};
+
+static void count_ws_layout(uint32_t L, uint32_t R, size_t sort_bytes, WsSize& w) {
+  w.add<char>(sort_bytes);
+  w.add<uint32_t>(R ? R : 1);
+  w.add<unsigned long long>(R ? R : 1);
+  w.add<uint32_t>(4);
+  w.add<uint32_t>(L ? L : 1);
+}
+
+template <typename T>
+static int count_matches_typed(const JoinParams& J, const CountWs& c, cudaStream_t s) {
+  const JCond& c0 = J.cond[0];
+  const yq_column rc{const_cast<char*>(c0.r.data), nullptr, c0.r.type, c0.r.width};
+  KeyJob j{rc, 0, 0};
+  uint32_t offs[2] = {0, J.R};
+  YQ_TRY(sort_segments_impl(&j, 1, J.R, offs, 1, c.perm, nullptr, c.sort_ws, c.sort_bytes, s, nullptr));
+  const yq_column sc{c.sorted, nullptr, rc.type, rc.width};
+  YQ_TRY(gather_impl(&rc, 1, c.perm, J.R, &sc, nullptr, s));
+  const uint32_t R = J.R;
+  YQ_TRY(h2d_async(c.nvalid, &R, sizeof(R), s));
+  const int grid = sm_count() * 4;
+  const T* sorted = reinterpret_cast<const T*>(c.sorted);
+  const T* lcol = reinterpret_cast<const T*>(c0.l.data);
+  k_join_count_valid<T><<<grid, 256, 0, s>>>(sorted, J.R, c.nvalid);
+  YQ_CHECK_LAUNCH();
+  switch (c0.cmp) {
+    case YQ_LT: k_join_count_sorted<T, YQ_LT><<<grid, 256, 0, s>>>(lcol, J.L, sorted, c.nvalid, R, c.counts); break;
+    case YQ_LE: k_join_count_sorted<T, YQ_LE><<<grid, 256, 0, s>>>(lcol, J.L, sorted, c.nvalid, R, c.counts); break;
+    case YQ_GT: k_join_count_sorted<T, YQ_GT><<<grid, 256, 0, s>>>(lcol, J.L, sorted, c.nvalid, R, c.counts); break;
+    case YQ_GE: k_join_count_sorted<T, YQ_GE><<<grid, 256, 0, s>>>(lcol, J.L, sorted, c.nvalid, R, c.counts); break;
+    case YQ_EQ: k_join_count_sorted<T, YQ_EQ><<<grid, 256, 0, s>>>(lcol, J.L, sorted, c.nvalid, R, c.counts); break;
+    default: k_join_count_sorted<T, YQ_NE><<<grid, 256, 0, s>>>(lcol, J.L, sorted, c.nvalid, R, c.counts); break;
+  }
   YQ_CHECK_LAUNCH();
   return YQ_OK;
 }
@@ -725,6 +883,14 @@ static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_
   const bool use_hash = J.eq >= 0 && J.R <= kHashMaxRows;
   const uint32_t nbuckets = use_hash ? pow2_at_least(J.R) : 0u;
   const uint32_t ntiles = use_hash ? ceil_div<uint32_t>(J.L, kJoinTile) : ceil_div<uint32_t>(J.L, kNlTile);
+  const JCond& t0 = J.cond[0];
+  const bool typed = !use_hash && J.ncond == 1 && J.ngroups == 1 && t0.l.type == t0.r.type && !t0.l.nulls &&
+                     !t0.r.nulls && t0.l.width == t0.r.width &&
+                     (t0.l.type == YQ_INT32 || t0.l.type == YQ_FLOAT32 || t0.l.type == YQ_INT64 ||
+                      t0.l.type == YQ_DATETIME || t0.l.type == YQ_FLOAT64);
+  const bool count_first = typed && J.R >= kCountFirstRows;
+  const size_t sort_bytes = count_first ? count_sort_bytes(J.R) : 0;
+  if (count_first && sort_bytes == 0) return YQ_ERR_UNSUPPORTED;
   WsSize w;
   w.add<uint32_t>(nbuckets + 1);
   w.add<unsigned long long>(use_hash ? J.R : 1);
@@ -732,6 +898,7 @@ static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_
   w.add<unsigned long long>((size_t)ntiles + 1);
   w.add<uint32_t>(8);
   w.add<unsigned long long>(2);
+  if (count_first) count_ws_layout(J.L, J.R, sort_bytes, w);
   Workspace ws;
   YQ_TRY(ws.acquire(workspace, workspace_bytes, w.total(), s));
   uint32_t* d_bstart = ws.take<uint32_t>(nbuckets + 1);
@@ -742,6 +909,15 @@ static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_
   J.total = ws.take<unsigned long long>(2);
   J.tile_counter = d_misc;
   J.err = d_misc + 1;
+  CountWs cw{};
+  if (count_first) {
+    cw.sort_ws = ws.take<char>(sort_bytes);
+    cw.sort_bytes = sort_bytes;
+    cw.perm = ws.take<uint32_t>(J.R ? J.R : 1);
+    cw.sorted = reinterpret_cast<char*>(ws.take<unsigned long long>(J.R ? J.R : 1));
+    cw.nvalid = ws.take<uint32_t>(4);
+    cw.counts = ws.take<uint32_t>(J.L ? J.L : 1);
+  }
   YQ_TRY_CUDA(cudaMemsetAsync(J.status, 0, ((size_t)ntiles + 1) * sizeof(unsigned long long), s));
   YQ_TRY_CUDA(cudaMemsetAsync(d_misc, 0, 8 * sizeof(uint32_t), s));
   YQ_TRY_CUDA(cudaMemsetAsync(J.total, 0, 2 * sizeof(unsigned long long), s));
@@ -763,11 +939,16 @@ static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_
   } else {
     ProfScope ps("join_nested_loop", s, (double)J.L * J.R * 0.0);
     const JCond& c0 = J.cond[0];
-    const bool typed = J.ncond == 1 && J.ngroups == 1 && c0.l.type == c0.r.type && !c0.l.nulls && !c0.r.nulls &&
-                       c0.l.width == c0.r.width && (c0.l.type == YQ_INT32 || c0.l.type == YQ_FLOAT32 ||
-                                                     c0.l.type == YQ_INT64 || c0.l.type == YQ_DATETIME ||
-                                                     c0.l.type == YQ_FLOAT64);
     if (typed) {
+      if (count_first) {
+        switch (c0.l.type) {
+          case YQ_INT32: YQ_TRY(count_matches_typed<int32_t>(J, cw, s)); break;
+          case YQ_FLOAT32: YQ_TRY(count_matches_typed<float>(J, cw, s)); break;
+          case YQ_FLOAT64: YQ_TRY(count_matches_typed<double>(J, cw, s)); break;
+          default: YQ_TRY(count_matches_typed<long long>(J, cw, s)); break;  // INT64, DATETIME
+        }
+        J.counts = cw.counts;
+      }
       switch (c0.l.type) {
         case YQ_INT32: launch_nested_typed<int32_t>(c0.cmp, ntiles, J, s); break;
         case YQ_FLOAT32: launch_nested_typed<float>(c0.cmp, ntiles, J, s); break;
@@ -804,6 +985,7 @@ size_t yq_join_workspace_size(uint32_t left_rows, uint32_t right_rows) {
   w.add<unsigned long long>((size_t)ntiles + 1);
   w.add<uint32_t>(8);
   w.add<unsigned long long>(2);
+  if (right_rows >= kCountFirstRows) count_ws_layout(left_rows, right_rows, count_sort_bytes(right_rows), w);
   return w.total();
 }
 
