@@ -554,6 +554,95 @@ def serving_form(args) -> dict:
             "rate_sweep": sweep, "matched_p99": matched}
 
 
+def reference_gpu_kernels() -> dict:
+    """The reference's own GPU kernels (its src/kernels built for sm_100a into
+    oracle/_ref/libyqref.so) timed on this GPU with CUDA events, on the config
+    workloads in the reference's own batch shapes. Its filter compaction and
+    radix sort are not run (their prefix-sum kernels shift by 32 or more bits and
+    faulted on this GPU); the timed sequences leave out the reference's per-batch
+    allocations and host syncs, which favours the reference."""
+    import torch
+    from yallasql_b200 import datagen
+    path = os.path.join(ROOT, "oracle", "_ref", "libyqref.so")
+    if not torch.cuda.is_available() or not os.path.exists(path):
+        return {"unavailable": "no GPU or oracle/_ref/libyqref.so not built"}
+    L = C.CDLL(path)
+    vp, u32, i32, fp = C.c_void_p, C.c_uint32, C.c_int, C.POINTER(C.c_float)
+    L.ref_time_aggregate.argtypes = [vp, vp, vp, u32, u32, vp, vp, vp, i32, fp]
+    L.ref_time_merge_window.argtypes = [vp, vp, u32, vp, vp, vp, vp, i32, fp]
+    L.ref_time_join_batch.argtypes = [vp, u32, vp, u32, vp, vp, i32, fp]
+    L.ref_time_cross.argtypes = [vp, vp, u32, vp, vp, u32, u32, vp, vp, vp, vp, i32, fp]
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    ms = C.c_float()
+    out = {}
+
+    def check(rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what}: CUDA error {rc}")
+
+    # filter+aggregate query's aggregates (cast, mul, SUM/MIN/MAX/COUNT per 15,616-row batch: 268 B/row layout)
+    for rows, name in ((1_000_000, "aggregate_1M"), (64_000_000, "aggregate_64M")):
+        t = datagen.sales_table(rows, seed=0)
+        price, disc = dev(t["price"]), dev(t["discount"])
+        nulls = torch.zeros(rows, dtype=torch.uint8, device="cuda")
+        fd, prod = torch.empty(rows, dtype=torch.float32, device="cuda"), torch.empty(rows, dtype=torch.float32,
+                                                                                         device="cuda")
+        acc = torch.zeros(8, dtype=torch.int32, device="cuda")
+        check(L.ref_time_aggregate(price.data_ptr(), disc.data_ptr(), nulls.data_ptr(), rows, 15_616, fd.data_ptr(),
+                                   prod.data_ptr(), acc.data_ptr(), 3 if rows > 1_000_000 else 10, C.byref(ms)), name)
+        out[name] = {"rows": rows, "batch_rows": 15_616, "ms": round(ms.value, 4),
+                     "rows_per_s": rows / (ms.value / 1e3),
+                     "launches": "cast, mul, reduction_sum_wrap SUM/MIN/MAX, reduction_count_notnull per batch",
+                     "note": "no WHERE compaction (the reference's prefix-sum kernels are not run): aggregates over "
+                             "every row"}
+        del t, price, disc, nulls, fd, prod
+    # ORDER BY merge: one 15,360-row window (272 B/row layout) of merge_sorted_array_kernel_v1
+    w = 15_360
+    rng = np.random.default_rng(1)
+    a = -np.sort(-rng.uniform(-1e6, 1e6, w).astype(np.float32))
+    b = -np.sort(-rng.uniform(-1e6, 1e6, w).astype(np.float32))
+    da, db = dev(a), dev(b)
+    c = torch.empty(w, dtype=torch.float32, device="cuda")
+    idx = torch.empty(w, dtype=torch.int32, device="cuda")
+    fa = torch.empty(w, dtype=torch.uint8, device="cuda")
+    la = torch.zeros(1, dtype=torch.int32, device="cuda")
+    check(L.ref_time_merge_window(da.data_ptr(), db.data_ptr(), w, c.data_ptr(), idx.data_ptr(), fa.data_ptr(),
+                                  la.data_ptr(), 200, C.byref(ms)), "merge")
+    runs = -(-64_000_000 // w)
+    levels = int(np.ceil(np.log2(runs)))
+    out["merge_window_15360"] = {"window_rows": w, "ms_per_window": round(ms.value, 5),
+                                 "merged_rows_per_s": w / (ms.value / 1e3),
+                                 "orderby_64M_merge_phase_ms_est": round(levels * (64_000_000 / w) * ms.value, 1),
+                                 "estimate": f"{levels} merge levels x 64M rows / {w}-row windows x the window's "
+                                             "kernel time (key merge only; the host loop, its blocking copies and "
+                                             "the per-window column moves not counted)"}
+    # star join: one 262,144-row fact batch (16 B/row layout) x the 2,556-row date table
+    fact, dim = datagen.star_tables(262_144, seed=2)
+    fk, dk = dev(fact["datekey"]), dev(dim["datekey"])
+    pairs = torch.empty(2 * 1_048_576, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    check(L.ref_time_join_batch(fk.data_ptr(), 262_144, dk.data_ptr(), 2556, pairs.data_ptr(), cnt.data_ptr(), 5,
+                                C.byref(ms)), "join")
+    nb = -(-60_000_000 // 262_144)
+    out["join_batch_262144x2556"] = {"ms_per_batch": round(ms.value, 4), "pairs_per_batch": int(cnt.item()),
+                                     "star_join_60M_join_phase_ms_est": round(nb * ms.value, 1),
+                                     "estimate": f"{nb} fact batches x the batch's outer_join_batches time (the "
+                                                 "pair gathers, filters and the aggregate not counted)"}
+    # cross product 20K x 20K, right side in 256-row chunks
+    x, y = datagen.cross_tables(20_000, seed=2)
+    dx, dy = dev(x), dev(y)
+    zn = torch.zeros(20_000, dtype=torch.uint8, device="cuda")
+    ol, orr = (torch.empty(20_000 * 256, dtype=torch.int32, device="cuda") for _ in range(2))
+    oln, orn = (torch.empty(20_000 * 256, dtype=torch.uint8, device="cuda") for _ in range(2))
+    check(L.ref_time_cross(dx.data_ptr(), zn.data_ptr(), 20_000, dy.data_ptr(), zn.data_ptr(), 20_000, 256,
+                           ol.data_ptr(), oln.data_ptr(), orr.data_ptr(), orn.data_ptr(), 2, C.byref(ms)), "cross")
+    out["cross_product_20Kx20K"] = {"ms": round(ms.value, 3), "output_rows": 400_000_000,
+                                    "note": "materialisation only (both columns + null bytes, 256-row right chunks); "
+                                            "the reference then filters a.x < b.y with its compaction, not run"}
+    torch.cuda.synchronize()
+    return out
+
+
 def run_reference(args, rank: int):
     """Reference arm: the CPU port of the operator (oracle/ stable ORDER BY +
     row gather), all host threads, the whole table every step (a sample
