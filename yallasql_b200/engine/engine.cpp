@@ -134,7 +134,10 @@ void Batch::cpuToFs(const std::string& path) {
     nulls[c] = nullptr;
   }
   location = Device::FS;
-  write_ = std::async(std::launch::async, [path, d, nl, meta, n]() -> bool {
+  int dev = 0;
+  cudaGetDevice(&dev);  // the task frees the host buffers with the caller's device current
+  write_ = std::async(std::launch::async, [path, d, nl, meta, n, dev]() -> bool {
+    cudaSetDevice(dev);
     bool ok = false;
     if (FILE* f = std::fopen(path.c_str(), "wb")) {
       const uint64_t head[3] = {kBatchFileMagic, n, (uint64_t)meta.size()};
