@@ -132,6 +132,23 @@ def test_prefix_sums(cuda, yq, n):
     np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), np.cumsum(u, dtype=np.uint32))
 
 
+@pytest.mark.parametrize("offset", [1, 3, 4])
+def test_prefix_sums_unaligned_input(cuda, yq, offset):
+    """Inputs that start off a 16-byte boundary take the element-wise loads;
+    several tiles, a partial last tile."""
+    n = 300_001
+    rng = np.random.default_rng(offset)
+    m = rng.integers(0, 2, n + offset).astype(np.uint8)
+    dm = dev(m)
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    assert yq.yq_prefix_sum_mask(dm.data_ptr() + offset, out.data_ptr(), n, None, 0, s()) == A.OK
+    np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), np.cumsum(m[offset:], dtype=np.uint32))
+    u = rng.integers(0, 1000, n + offset).astype(np.uint32)
+    du = dev(u)
+    assert yq.yq_prefix_sum_u32(du.data_ptr() + 4 * offset, out.data_ptr(), n, None, 0, s()) == A.OK
+    np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), np.cumsum(u[offset:], dtype=np.uint32))
+
+
 def test_move_rows_filter_skips_null_cells(cuda, yq):
     rng = np.random.default_rng(1)
     n = 10_000

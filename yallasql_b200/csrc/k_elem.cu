@@ -153,23 +153,56 @@ __global__ void k_cast(const S* __restrict__ src, D* __restrict__ dst, uint32_t 
 }
 
 // --------------------------------------------------------- prefix sums
-constexpr int kScanItems = 8;
+// Inclusive scan in tiles of kScanTile elements, one decoupled look-back per
+// tile. Each thread scans kScanItems consecutive elements in registers (one
+// 16-byte load per thread for masks, four for 32-bit values, when the input
+// is 16-byte aligned and the tile is full); the results go through shared
+// memory so that each warp's stores cover 128 contiguous bytes.
+constexpr int kScanItems = 16;
 constexpr uint32_t kScanTile = kElemBlock * kScanItems;
+constexpr int kScanPitch = kScanItems + 1;  // padded row of a thread's results in shared memory
+
+template <typename T>
+__device__ __forceinline__ void scan_load(const T* __restrict__ in, uint32_t i0, uint32_t n, bool vec,
+                                          uint32_t (&v)[kScanItems]) {
+  if (vec && i0 + kScanItems <= n) {
+    if constexpr (sizeof(T) == 1) {
+      const uint4 q = __ldg(reinterpret_cast<const uint4*>(in + i0));
+      const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int k = 0; k < kScanItems; ++k) v[k] = (w[k >> 2] >> (8 * (k & 3))) & 0xffu;
+      return;
+    } else {
+#pragma unroll
+      for (int c = 0; c < kScanItems / 4; ++c) {
+        const uint4 q = __ldg(reinterpret_cast<const uint4*>(in + i0) + c);
+        v[4 * c] = q.x;
+        v[4 * c + 1] = q.y;
+        v[4 * c + 2] = q.z;
+        v[4 * c + 3] = q.w;
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) v[k] = (i0 + k < n) ? (uint32_t)in[i0 + k] : 0u;
+}
 
 template <typename T>
 __global__ void __launch_bounds__(kElemBlock) k_scan(const T* __restrict__ in, uint32_t* __restrict__ out, uint32_t n,
                                                      uint32_t* tile_counter, unsigned long long* status,
-                                                     uint32_t* err) {
+                                                     uint32_t* err, int vec) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kElemBlock / 32 + 1];
   __shared__ unsigned long long s_prefix;
+  __shared__ uint32_t s_out[kElemBlock * kScanPitch];
   if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
   __syncthreads();
   const uint32_t tile = s_tile;
-  const uint32_t i0 = tile * kScanTile + threadIdx.x * kScanItems;
+  const uint32_t t0 = tile * kScanTile;
+  const uint32_t i0 = t0 + threadIdx.x * kScanItems;
   uint32_t v[kScanItems];
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) v[k] = (i0 + k < n) ? (uint32_t)in[i0 + k] : 0u;
+  scan_load<T>(in, i0, n, vec != 0, v);
 #pragma unroll
   for (int k = 1; k < kScanItems; ++k) v[k] += v[k - 1];
   uint32_t total;
@@ -178,11 +211,15 @@ __global__ void __launch_bounds__(kElemBlock) k_scan(const T* __restrict__ in, u
     const unsigned long long p = tile_lookback(status, tile, total, err);
     if (threadIdx.x == 0) s_prefix = p;
   }
-  __syncthreads();
-  const uint32_t base = (uint32_t)s_prefix + excl;
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k)
-    if (i0 + k < n) out[i0 + k] = base + v[k];
+  for (int k = 0; k < kScanItems; ++k) s_out[threadIdx.x * kScanPitch + k] = excl + v[k];
+  __syncthreads();
+  const uint32_t base = (uint32_t)s_prefix;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    const uint32_t e = (uint32_t)j * kElemBlock + threadIdx.x;  // element of the tile
+    if (t0 + e < n) out[t0 + e] = base + s_out[(e / kScanItems) * kScanPitch + (e % kScanItems)];
+  }
 }
 
 // ------------------------------------------------------------ row moves
@@ -495,7 +532,8 @@ static int prefix_sum(const T* in, uint32_t* out, uint32_t n, void* workspace, s
   YQ_TRY_CUDA(cudaMemsetAsync(status, 0, ((size_t)ntiles + 1) * sizeof(unsigned long long), s));
   YQ_TRY_CUDA(cudaMemsetAsync(misc, 0, 4 * sizeof(uint32_t), s));
   ProfScope ps("prefix_sum", s, (double)n * (sizeof(T) + 4.0));
-  k_scan<T><<<ntiles, kElemBlock, 0, s>>>(in, out, n, misc, status, misc + 1);
+  const int vec = (reinterpret_cast<uintptr_t>(in) & 15u) == 0u;
+  k_scan<T><<<ntiles, kElemBlock, 0, s>>>(in, out, n, misc, status, misc + 1, vec);
   YQ_CHECK_LAUNCH();
   return YQ_OK;
 }

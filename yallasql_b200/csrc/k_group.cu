@@ -27,6 +27,7 @@
 #include <climits>
 
 #include "yq_common.cuh"
+#include "yq_sort.cuh"
 
 using namespace yq;
 
@@ -65,6 +66,18 @@ __global__ void k_group_heads(const yq_column key, const uint32_t* __restrict__ 
                               uint8_t* __restrict__ head) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x)
     head[i] = (i == 0 || !same_key(key, perm[i], perm[i - 1])) ? 1 : 0;
+}
+
+// Head flags from the sorted key words (kw words a row, in sorted order): a
+// sequential read instead of two reads through the permutation. Key words
+// already equate -0.0 with +0.0 and every NaN, and carry the NULL flag.
+__global__ void k_group_heads_words(const uint32_t* __restrict__ words, int kw, uint32_t rows,
+                                    uint8_t* __restrict__ head) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+    bool h = i == 0;
+    for (int j = 0; j < kw && !h; ++j) h = __ldg(words + (size_t)i * kw + j) != __ldg(words + (size_t)(i - 1) * kw + j);
+    head[i] = h ? 1 : 0;
+  }
 }
 
 __global__ void k_group_keys(const yq_column key, const uint32_t* __restrict__ perm, uint32_t rows,
@@ -417,6 +430,8 @@ size_t yq_group_by_workspace_size(const yq_column* key, uint32_t rows, int32_t n
   WsSize w;
   w.add<uint8_t>(yq_sort_workspace_size(key, rows));
   w.add<uint32_t>((size_t)rows + 1);          // permutation
+  const int kwm = sort_key_words_max(*key);
+  w.add<uint32_t>((size_t)rows * (kwm > 0 ? kwm : 1) + 16);  // sorted key words
   w.add<uint8_t>((size_t)rows + 16);          // head flags
   w.add<uint32_t>((size_t)rows + 1);          // group of every sorted position
   w.add<uint8_t>(yq_prefix_sum_workspace_size(rows));
@@ -470,6 +485,8 @@ int yq_group_by(const yq_batch* batch, int32_t key_col, const yq_group_agg* aggs
   const size_t sort_ws = yq_sort_workspace_size(&key, rows);
   void* d_sort = ws.take<uint8_t>(sort_ws);
   uint32_t* perm = ws.take<uint32_t>((size_t)rows + 1);
+  const int kwm = sort_key_words_max(key);
+  uint32_t* words = ws.take<uint32_t>((size_t)rows * (kwm > 0 ? kwm : 1) + 16);
   uint8_t* head = ws.take<uint8_t>((size_t)rows + 16);
   uint32_t* incl = ws.take<uint32_t>((size_t)rows + 1);
   void* scan_ws = ws.take<uint8_t>(yq_prefix_sum_workspace_size(rows));
@@ -478,9 +495,23 @@ int yq_group_by(const yq_batch* batch, int32_t key_col, const yq_group_agg* aggs
   uint32_t* tail_group = ws.take<uint32_t>((size_t)ntiles + 1);
   uint32_t* tile_flags = ws.take<uint32_t>((size_t)ntiles + 1);
   uint32_t* d_err = ws.take<uint32_t>(4);
-  yq_sort_config cfg{0, 0, 256, 1};  // every pass kept: no host read-back inside the sort
-  YQ_TRY(yq_sort_indices(&key, rows, 0, 0, perm, &cfg, d_sort, sort_ws, stream));
-  {
+  // The sort skips the passes whose digit every key shares (a key of few
+  // distinct values sorts in one or two passes) and hands over its key words
+  // in sorted order; a text key too long for one pass's words sorts without
+  // them, and its heads compare the rows through the permutation.
+  KeyJob job{key, 0, 0};
+  const uint32_t offs[2] = {0, rows};
+  int kw = 0;
+  int st = sort_segments_impl(&job, 1, rows, offs, 1, perm, nullptr, d_sort, sort_ws, s, nullptr, words, &kw);
+  const bool have_words = st == YQ_OK;
+  if (st == YQ_ERR_UNSUPPORTED)
+    st = sort_segments_impl(&job, 1, rows, offs, 1, perm, nullptr, d_sort, sort_ws, s, nullptr);
+  YQ_TRY(st);
+  if (have_words) {
+    ProfScope ps("group_heads", s, (double)rows * 4.0 * (kw > 0 ? kw : 1));
+    k_group_heads_words<<<grid_for(rows, kGroupThreads), kGroupThreads, 0, s>>>(words, kw, rows, head);
+    YQ_CHECK_LAUNCH();
+  } else {
     ProfScope ps("group_heads", s, (double)rows * (key.width + 4));
     k_group_heads<<<grid_for(rows, kGroupThreads), kGroupThreads, 0, s>>>(key, perm, rows, head);
     YQ_CHECK_LAUNCH();
