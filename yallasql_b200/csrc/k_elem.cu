@@ -154,11 +154,11 @@ __global__ void k_cast(const S* __restrict__ src, D* __restrict__ dst, uint32_t 
 
 // --------------------------------------------------------- prefix sums
 // Inclusive scan in tiles of kScanTile elements, one decoupled look-back per
-// tile. Each thread scans kScanItems consecutive elements in registers (one
-// 16-byte load per thread for masks, four for 32-bit values, when the input
-// is 16-byte aligned and the tile is full); the results go through shared
+// tile. Each thread scans kScanItems consecutive elements in registers
+// (16-byte loads when the input is 16-byte aligned and the tile is full: two
+// per thread for masks, eight for 32-bit values); the results go through shared
 // memory so that each warp's stores cover 128 contiguous bytes.
-constexpr int kScanItems = 16;
+constexpr int kScanItems = 32;
 constexpr uint32_t kScanTile = kElemBlock * kScanItems;
 constexpr int kScanPitch = kScanItems + 1;  // padded row of a thread's results in shared memory
 
@@ -167,10 +167,13 @@ __device__ __forceinline__ void scan_load(const T* __restrict__ in, uint32_t i0,
                                           uint32_t (&v)[kScanItems]) {
   if (vec && i0 + kScanItems <= n) {
     if constexpr (sizeof(T) == 1) {
-      const uint4 q = __ldg(reinterpret_cast<const uint4*>(in + i0));
-      const uint32_t w[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-      for (int k = 0; k < kScanItems; ++k) v[k] = (w[k >> 2] >> (8 * (k & 3))) & 0xffu;
+      for (int c = 0; c < kScanItems / 16; ++c) {
+        const uint4 q = __ldg(reinterpret_cast<const uint4*>(in + i0) + c);
+        const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[16 * c + k] = (w[k >> 2] >> (8 * (k & 3))) & 0xffu;
+      }
       return;
     } else {
 #pragma unroll

@@ -68,6 +68,14 @@ __global__ void k_group_heads(const yq_column key, const uint32_t* __restrict__ 
     head[i] = (i == 0 || !same_key(key, perm[i], perm[i - 1])) ? 1 : 0;
 }
 
+// First input row of every tile of sorted positions (the tiles run in the
+// order of these rows: see yq_group_by).
+__global__ void k_tile_first_row(const uint32_t* __restrict__ perm, uint32_t ntiles, uint32_t tile_rows,
+                                 uint32_t* __restrict__ first) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x)
+    first[t] = __ldg(perm + (size_t)t * tile_rows);
+}
+
 // Head flags from the sorted key words (kw words a row, in sorted order): a
 // sequential read instead of two reads through the permutation. Key words
 // already equate -0.0 with +0.0 and every NaN, and carry the NULL flag.
@@ -108,6 +116,7 @@ struct GroupParams {
   uint32_t* starts;      // [groups + 1] first sorted position of every group; starts[groups] = rows
   yq_column out[YQ_MAX_AGGREGATES];  // aggregate output columns
   unsigned long long* rec;  // [tiles][2][nagg][2]: head / tail partial (count, value) of every tile
+  const uint32_t* tile_order;  // [tiles] the tile block b works on (null: tile b)
   uint32_t* tail_group;     // [tiles] group of the tile's tail record
   uint32_t* tile_flags;     // [tiles] kHeadRec | kTailRec | kTailStarted (set with atomicOr)
   uint32_t* err;
@@ -272,7 +281,7 @@ __device__ __forceinline__ void block_seg_scan(int kind, bool flt, bool flag, GP
 __global__ void __launch_bounds__(kGroupThreads) k_group_tiles(const __grid_constant__ GroupParams P) {
   __shared__ GPart s_part[2 * (kGroupThreads / 32)];
   __shared__ uint32_t s_flag[2 * (kGroupThreads / 32)];
-  const uint32_t tile = blockIdx.x;
+  const uint32_t tile = P.tile_order ? __ldg(P.tile_order + blockIdx.x) : blockIdx.x;
   const uint32_t tile0 = tile * kGroupTile;
   const uint32_t tile_end = min(P.rows, tile0 + kGroupTile);
   const uint32_t p0 = tile0 + threadIdx.x * kGroupItems;
@@ -424,6 +433,12 @@ unsigned grid_for(uint64_t n, unsigned per_block) {
 
 extern "C" {
 
+// Sort workspace for ordering `ntiles` tiles by their first row (4-byte keys).
+static size_t tile_order_sort_bytes(uint32_t ntiles) {
+  const yq_column c{reinterpret_cast<void*>(static_cast<uintptr_t>(256)), nullptr, YQ_INT32, 4};
+  return yq_sort_workspace_size(&c, ntiles);
+}
+
 size_t yq_group_by_workspace_size(const yq_column* key, uint32_t rows, int32_t nagg, uint32_t capacity) {
   if (!key) return 0;
   const size_t tiles = ((size_t)rows + kGroupTile - 1) / kGroupTile + 1;
@@ -438,6 +453,8 @@ size_t yq_group_by_workspace_size(const yq_column* key, uint32_t rows, int32_t n
   w.add<uint32_t>((size_t)capacity + 2);      // group starts
   w.add<unsigned long long>(tiles * 4 * (size_t)(nagg > 0 ? nagg : 1));  // tile head / tail records
   w.add<uint32_t>(tiles);                     // tail group of every tile
+  w.add<uint32_t>(2 * tiles);                 // first row of every tile, tile order
+  w.add<uint8_t>(tile_order_sort_bytes((uint32_t)tiles));
   w.add<uint32_t>(tiles);                     // tile flags
   w.add<uint32_t>(4);                         // error word
   return w.total();
@@ -493,6 +510,10 @@ int yq_group_by(const yq_batch* batch, int32_t key_col, const yq_group_agg* aggs
   uint32_t* starts = ws.take<uint32_t>((size_t)capacity + 2);
   unsigned long long* rec = ws.take<unsigned long long>(((size_t)ntiles + 1) * 4 * (size_t)(nagg > 0 ? nagg : 1));
   uint32_t* tail_group = ws.take<uint32_t>((size_t)ntiles + 1);
+  uint32_t* first_row = ws.take<uint32_t>((size_t)ntiles + 1);
+  uint32_t* tile_order = ws.take<uint32_t>((size_t)ntiles + 1);
+  const size_t order_ws_bytes = tile_order_sort_bytes(ntiles + 1);
+  void* order_ws = ws.take<uint8_t>(order_ws_bytes);
   uint32_t* tile_flags = ws.take<uint32_t>((size_t)ntiles + 1);
   uint32_t* d_err = ws.take<uint32_t>(4);
   // The sort skips the passes whose digit every key shares (a key of few
@@ -538,6 +559,21 @@ int yq_group_by(const yq_batch* batch, int32_t key_col, const yq_group_agg* aggs
     double in_bytes = 8.0 * rows;  // group index + permutation
     for (int j = 0; j < nagg; ++j)
       if (P.a[j].data) in_bytes += (double)rows * (type_width(P.a[j].type) + (P.a[j].nulls ? 1 : 0));
+    // Tiles run in the order of their first input row. The rows of one group
+    // ascend through its sorted positions, so the tiles resident together
+    // (one stretch of every group) read values from one stretch of rows,
+    // which L2 then holds for all of them; in position order they would be
+    // one group's tiles reading rows spread over the whole table. The
+    // results do not depend on the order: each tile writes its own records.
+    if (ntiles >= 64) {
+      k_tile_first_row<<<grid_for(ntiles, kGroupThreads), kGroupThreads, 0, s>>>(perm, ntiles, kGroupTile, first_row);
+      YQ_CHECK_LAUNCH();
+      const yq_column fc{first_row, nullptr, YQ_INT32, 4};
+      KeyJob oj{fc, 0, 0};
+      const uint32_t oo[2] = {0, ntiles};
+      YQ_TRY(sort_segments_impl(&oj, 1, ntiles, oo, 1, tile_order, nullptr, order_ws, order_ws_bytes, s, nullptr));
+      P.tile_order = tile_order;
+    }
     {
       ProfScope ps("group_accumulate", s, in_bytes);
       k_group_tiles<<<ntiles, kGroupThreads, 0, s>>>(P);
