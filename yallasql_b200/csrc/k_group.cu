@@ -13,7 +13,7 @@
 //                     from the one before it (-0.0 equals +0.0, NaNs equal)
 //   yq_prefix_sum_mask  -> group index of every sorted position, group count
 //   k_group_keys      each group's key into the output
-//   k_group_tiles     tiles of 4,096 sorted positions (16 a thread), values
+//   k_group_tiles     tiles of 2,048 sorted positions (8 a thread), values
 //                     read through the permutation: each thread folds its
 //                     positions in order, a segmented scan over the block's
 //                     threads (fixed tree) completes every group that starts
@@ -122,8 +122,8 @@ struct GroupParams {
   uint32_t* err;
 };
 
-constexpr uint32_t kGroupItems = 16;
-constexpr uint32_t kGroupTile = kGroupThreads * kGroupItems;  // 4,096 sorted positions
+constexpr uint32_t kGroupItems = 8;
+constexpr uint32_t kGroupTile = kGroupThreads * kGroupItems;  // 2,048 sorted positions
 constexpr uint32_t kHeadRec = 1, kTailRec = 2, kTailStarted = 4;
 
 // Order-preserving signed 64-bit key of a double (NaN above +inf, one NaN).
