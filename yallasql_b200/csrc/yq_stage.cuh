@@ -108,10 +108,14 @@ __device__ __forceinline__ void stage_issue(const StagePlan& SP, int slot, uint3
   uint64_t* bar = stage_bar(SP, slot);
   mbar_arrive_expect_tx(bar, SP.tx_bytes[pass]);
   unsigned char* dst = yq_dyn_smem + (size_t)slot * SP.stage_bytes;
+  // A column the second pass reads again stays in L2 from its first read;
+  // everything else streams through.
+  const uint64_t keep = l2_evict_last_policy(), stream = l2_evict_first_policy();
   for (int i = 0; i < SP.ncopy; ++i) {
     const StageCopy& c = SP.c[i];
     if (c.passes >> pass & 1u)
-      tma_load_1d(dst + c.soff, c.src + (size_t)row0 * c.row_bytes, kStepRows * c.row_bytes, bar);
+      tma_load_1d_hint(dst + c.soff, c.src + (size_t)row0 * c.row_bytes, kStepRows * c.row_bytes, bar,
+                       (pass == 0 && (c.passes & 2u)) ? keep : stream);
   }
 }
 
