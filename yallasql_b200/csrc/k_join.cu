@@ -888,9 +888,8 @@ static int join_impl(const yq_batch* left, const yq_batch* right, const yq_join_
                      !t0.r.nulls && t0.l.width == t0.r.width &&
                      (t0.l.type == YQ_INT32 || t0.l.type == YQ_FLOAT32 || t0.l.type == YQ_INT64 ||
                       t0.l.type == YQ_DATETIME || t0.l.type == YQ_FLOAT64);
-  const bool count_first = typed && J.R >= kCountFirstRows;
-  const size_t sort_bytes = count_first ? count_sort_bytes(J.R) : 0;
-  if (count_first && sort_bytes == 0) return YQ_ERR_UNSUPPORTED;
+  const size_t sort_bytes = typed && J.R >= kCountFirstRows ? count_sort_bytes(J.R) : 0;
+  const bool count_first = sort_bytes != 0;  // else (a right side too long to sort) the kernel counts
   WsSize w;
   w.add<uint32_t>(nbuckets + 1);
   w.add<unsigned long long>(use_hash ? J.R : 1);
