@@ -132,6 +132,19 @@ def make_trace(n: int, rate: float, catalog: Catalog, seed: int = 4) -> list[Req
             enumerate(zip(kinds, tables, t, cats))]
 
 
+def warm_trace(catalog: Catalog) -> list[Request]:
+    """Every request class on every table, with two parameters each, all
+    arriving at once. Each distinct expression program compiles its kernel
+    once per variant (staged or not, by size), so serving this trace before a
+    timed run keeps compilations out of it."""
+    out = []
+    for k in CLASSES:
+        for t in range(catalog.ntables):
+            for c in (0, 1):
+                out.append(Request(len(out), k, t, 0.0, c))
+    return out
+
+
 class Plans:
     """Compiled programs shared by every request."""
 
