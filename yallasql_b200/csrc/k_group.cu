@@ -286,6 +286,63 @@ __global__ void __launch_bounds__(kGroupThreads) k_group_tiles(const __grid_cons
   const uint32_t tile_end = min(P.rows, tile0 + kGroupTile);
   const uint32_t p0 = tile0 + threadIdx.x * kGroupItems;
   const uint32_t n = p0 < tile_end ? min(kGroupItems, tile_end - p0) : 0u;  // valid positions of this thread
+  // A tile inside one group (with few groups, nearly every tile): every
+  // aggregate folds over the whole tile by a fixed-order block reduction,
+  // with one barrier instead of a segmented scan per aggregate.
+  if (tile0 < tile_end && __ldg(P.incl + tile0) == __ldg(P.incl + tile_end - 1)) {
+    __shared__ GPart s_u[YQ_MAX_AGGREGATES][kGroupThreads / 32];
+    const uint32_t G = __ldg(P.incl + tile0) - 1u;
+    const bool starts = tile0 == 0 || __ldg(P.incl + tile0 - 1) - 1u != G;
+    const bool ends = tile_end == P.rows || __ldg(P.incl + tile_end) - 1u != G;
+    if (threadIdx.x == 0 && starts) P.starts[G] = tile0;
+    uint32_t rr[kGroupItems];
+#pragma unroll
+    for (int q = 0; q < (int)kGroupItems; ++q) rr[q] = (uint32_t)q < n ? __ldg(P.perm + p0 + q) : 0u;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int j = 0; j < P.nagg; ++j) {
+      const GAgg& a = P.a[j];
+      const bool flt = is_float(a.type);
+      GPart acc = part_identity(a.kind);
+#pragma unroll
+      for (int q = 0; q < (int)kGroupItems; ++q)
+        if ((uint32_t)q < n) part_add_row(a, flt, acc, rr[q]);
+      // fixed tree: lanes pairwise in index order
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const GPart o{__shfl_down_sync(0xffffffffu, acc.cnt, d), __shfl_down_sync(0xffffffffu, acc.v, d)};
+        if ((lane & (2 * d - 1)) == 0) acc = part_combine(a.kind, flt, acc, o);
+      }
+      if (lane == 0) s_u[j][warp] = acc;
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < P.nagg) {  // thread j: aggregate j, warps in order
+      const int j = threadIdx.x;
+      const GAgg& a = P.a[j];
+      const bool flt = is_float(a.type);
+      GPart tot = s_u[j][0];
+      for (int w = 1; w < kGroupThreads / 32; ++w) tot = part_combine(a.kind, flt, tot, s_u[j][w]);
+      unsigned long long* head_rec = P.rec + ((size_t)tile * 2 * P.nagg + j) * 2;
+      unsigned long long* tail_rec = P.rec + ((size_t)tile * 2 * P.nagg + P.nagg + j) * 2;
+      if (starts && ends) {
+        part_write(a, P.out[j], G, tot);
+      } else if (ends) {  // the group began before this tile and ends at its last position
+        head_rec[0] = tot.cnt;
+        head_rec[1] = tot.v;
+      } else {  // the group goes on past this tile
+        tail_rec[0] = tot.cnt;
+        tail_rec[1] = tot.v;
+      }
+    }
+    if (threadIdx.x == 0 && P.nagg > 0 && !(starts && ends)) {
+      if (ends) {
+        atomicOr(P.tile_flags + tile, kHeadRec);
+      } else {
+        P.tail_group[tile] = G;
+        atomicOr(P.tile_flags + tile, kTailRec | (starts ? kTailStarted : 0u));
+      }
+    }
+    return;
+  }
   uint32_t g[kGroupItems], r[kGroupItems];
 #pragma unroll
   for (int q = 0; q < (int)kGroupItems; ++q) {
