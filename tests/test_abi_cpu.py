@@ -111,3 +111,42 @@ def test_workspace_sizes_are_host_only(yq):
     col = A.Column(0x1000, None, A.FLOAT32, 4)
     assert yq.yq_sort_workspace_size(C.byref(col), 1_000_000) >= 4 * 1_000_000 * 5
     assert yq.yq_agg_state_bytes(4) >= 4 * 24
+
+
+def test_bad_or_join_arguments(yq):
+    """OR-of-AND join conditions: groups numbered 0..G-1 with every group
+    used; rejected before any device work otherwise."""
+    lb, lk = _batch([(A.INT32, 4), (A.INT32, 4)])
+    rb, rk = _batch([(A.INT32, 4), (A.INT32, 4)])
+    conds = (A.JoinCond * 2)(A.JoinCond(0, 0, A.EQ), A.JoinCond(1, 1, A.LT))
+    cnt = C.c_uint64()
+    for groups in ([0, 2], [1, 1], [0, 9], [-1, 0]):
+        g = (C.c_int32 * 2)(*groups)
+        st = yq.yq_join_pairs_or(C.byref(lb), C.byref(rb), conds, C.cast(g, C.c_void_p), 2, 0x3000, 0x4000, 100,
+                                 C.byref(cnt), None, 0, None)
+        assert st == A.ERR_INVALID_ARG, groups
+    assert yq.yq_join_pairs_or(C.byref(lb), C.byref(rb), conds, None, 2, 0x3000, 0x4000, 100, C.byref(cnt), None, 0,
+                               None) == A.ERR_INVALID_ARG
+    g = (C.c_int32 * 2)(0, 1)
+    assert yq.yq_join_pairs_or(C.byref(lb), C.byref(rb), conds, C.cast(g, C.c_void_p), 0, 0x3000, 0x4000, 100,
+                               C.byref(cnt), None, 0, None) == A.ERR_INVALID_ARG
+
+
+def test_bad_tuning_arguments(yq):
+    col = A.Column(0x1000, None, A.FLOAT32, 4)
+    for block in (96, 1024, -1):
+        cfg = A.SortConfig(8, 0, block, 0)
+        assert yq.yq_sort_indices(C.byref(col), 10, 0, 0, 0x2000, C.byref(cfg), None, 0, None) == A.ERR_INVALID_ARG
+    b, keep = _batch([(A.FLOAT32, 4), (A.INT64, 8)])
+    offs = (C.c_uint32 * 3)(0, 5, 10)
+    for items in (3, 12, 32):
+        assert yq.yq_order_by_tiled(C.byref(b), 0, 0, 0, offs, 2, C.byref(b), items, None, 0, None) == \
+            A.ERR_INVALID_ARG
+
+
+def test_join_workspace_covers_counting(yq):
+    """With a right side long enough for the up-front match counts, the join
+    workspace also holds the right key's sort and one count per left row."""
+    small = yq.yq_join_workspace_size(50_000, 1_000)
+    big = yq.yq_join_workspace_size(50_000, 100_000)
+    assert big >= small + 4 * 50_000 + 12 * 100_000
