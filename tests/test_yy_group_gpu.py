@@ -104,3 +104,24 @@ def test_capacity_error(cuda):
     got = ops.group_by(b, 0, [(A.AGG_COUNT_STAR, 0)], capacity=10)
     assert got.columns[0].data.cpu().tolist() == list(range(10))
     assert got.columns[1].data.cpu().tolist() == [10] * 10
+
+
+@pytest.mark.parametrize("layout", ["one_group", "tile_edges", "short_groups"])
+def test_tiles_inside_one_group(cuda, layout):
+    """Tiles of 2,048 sorted positions that lie inside one group fold it with
+    a block reduction: one group over ~500 tiles; groups whose boundaries
+    fall exactly on tile edges; groups shorter than a tile. NULL inputs."""
+    rng = np.random.default_rng(len(layout))
+    n = 1_000_000
+    if layout == "one_group":
+        k = np.full(n, 7, np.int32)
+    elif layout == "tile_edges":
+        k = (np.arange(n) // (2048 * 3)).astype(np.int32)  # every group ends on a tile edge
+        k = rng.permutation(k)
+    else:
+        k = rng.integers(0, 3000, n).astype(np.int32)
+    v = rng.normal(0, 100, n).astype(np.float32)
+    vn = rng.random(n) < 0.05
+    q = rng.integers(-1000, 1000, n).astype(np.int64)
+    check([(k, A.INT32, None), (v, A.FLOAT32, vn), (q, A.INT64, None)], 0,
+          ALL_AGGS([1]) + [(A.AGG_SUM, 2), (A.AGG_MIN, 2)])  # eight aggregates, the most a call takes
