@@ -491,6 +491,7 @@ unsigned grid_for(uint64_t n, unsigned per_block) {
 extern "C" {
 
 // Sort workspace for ordering `ntiles` tiles by their first row (4-byte keys).
+// Sizing reads no column data: the placeholder pointer only has to be non-null.
 static size_t tile_order_sort_bytes(uint32_t ntiles) {
   const yq_column c{reinterpret_cast<void*>(static_cast<uintptr_t>(256)), nullptr, YQ_INT32, 4};
   return yq_sort_workspace_size(&c, ntiles);

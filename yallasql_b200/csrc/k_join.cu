@@ -746,7 +746,8 @@ static int build_table(const yq_batch* right, const yq_program* pred, const yq_c
 constexpr uint32_t kCountFirstRows = 4096;
 
 // Sort workspace for a right side of R rows (an 8-byte key bounds the typed
-// path's 4- and 8-byte keys).
+// path's 4- and 8-byte keys). Sizing reads no column data: the placeholder
+// pointer only has to be non-null.
 static size_t count_sort_bytes(uint32_t R) {
   yq_column dummy{reinterpret_cast<void*>(static_cast<uintptr_t>(256)), nullptr, YQ_INT64, 8};
   KeyJob j{dummy, 0, 0};
